@@ -1,0 +1,328 @@
+"""Benchmark of the pressure-projection step (computeSource -> solveFPS ->
+makeVelocityDivFree -> computeContinuityError) on the 512x384x256 channel.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one projection of the whole channel.  ``value`` is measured with all
+inputs resident in HBM (device entry point, out-of-place velocity so every step
+projects the same u*); ``e2e`` goes through the host entry point with pinned
+host buffers, host<->device copies inside the timed region.  Inputs (~0.4 GB
+per field) are larger than L2, so no flush is needed between steps.
+
+With N > 1 (torchrun, one rank per GPU) every rank projects its own,
+independently seeded channel: the ensemble shards as independent channels per
+GPU with no data-path collective (weak scaling); the time is the max over ranks.
+
+``--impl reference`` times the CPU restatement of the reference path (the
+oracle; the Fortran reference cannot be built here) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "projection solves/s and Gcell/s, mixed vs FP64 on 1 B200 at rel. residual 1e-10"
+UNIT = "Gcell/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def alg_bytes(nx, ny, nz):
+    """Compulsory HBM bytes of the stage sequence (FP64, no surface tension)."""
+    N = nx * ny * nz
+    K = (nx // 2 + 1) * ny * nz
+    return {
+        "recip": 16.0 * N,
+        "rhs_fftx": 48.0 * N + 16.0 * K,
+        "fftz_fwd": 32.0 * K,
+        "tridiag": 32.0 * K,
+        "fftz_inv": 32.0 * K,
+        "fftx_inv": 16.0 * K + 8.0 * N,
+        "correct": 80.0 * N,
+        "div": 24.0 * N,
+        "b_alg": 128.0 * N + 64.0 * K,
+    }
+
+
+def cpu_baseline_sample(seed: int):
+    """The oracle projection on a bounded sample (the same recipe at 128x128x64),
+    timed on this host; returns (Gcell/s, cores, kind, sample)."""
+    import numpy as np  # noqa: F401
+    from oracle import tbfp_oracle as O
+    from tbfsolver_b200 import synth
+
+    spec = synth.CONFIGS["c1"]
+    inp = synth.make_inputs(spec, seed=seed)
+    g = inp.grid
+    m = O.Mesh(g.nx, g.ny, g.nz, g.Lx, g.Ly, g.Lz, y_uniform=not g.y_stretched, gamma=g.gamma)
+    F = lambda f: O.FField(f.kind, f.hd, g.nx, g.ny, g.nz, f.a.numpy().copy())  # noqa: E731
+    args = [F(f) for f in (inp.u.ux, inp.u.uy, inp.u.uz, inp.rho, inp.psi_n, inp.psi_nm1)]
+    O.projection(m, *args, inp.dt, inp.alpha, inp.rho0, tridiag="thomas")
+    reps, t0 = 0, time.perf_counter()
+    while reps < 3 or time.perf_counter() - t0 < 10.0:
+        O.projection(m, *args, inp.dt, inp.alpha, inp.rho0, tridiag="thomas")
+        reps += 1
+    dt = (time.perf_counter() - t0) / reps
+    return g.ncells / dt / 1e9, 1, "port", f"numpy oracle, {spec.name}, {reps} projections, {dt * 1e3:.0f} ms each"
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    gcell, cores, kind, sample = cpu_baseline_sample(args.seed)
+    from tbfsolver_b200 import synth
+
+    spec = synth.CONFIGS[args.config]
+    line = {"metric": METRIC, "value": gcell, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": spec.ncells / (gcell * 1e9) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": spec.name, "cells": spec.ncells, "sample": "bounded CPU sample"},
+            "impl": "reference",
+            "cpu_baseline": {"value": gcell, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": gcell, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from tbfsolver_b200 import synth
+    from tbfsolver_b200._native import STAGES
+    from tbfsolver_b200.fields import Field, VField
+    from tbfsolver_b200.solver import PoissonEqn
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    spec = synth.CONFIGS[args.config]
+    inp = synth.make_inputs(spec, seed=args.seed + rank, device="cuda")
+    g = inp.grid
+    stream = torch.cuda.Stream()
+    eqn = PoissonEqn(g, spec.rhol, spec.rhog, stream=stream.cuda_stream, asynchronous=True, timing=True)
+    dt, alpha = inp.dt, inp.alpha
+    new = lambda: Field("cl", 1, g.nx, g.ny, g.nz, torch.zeros_like(inp.psi_n.a))  # noqa: E731
+    u_in = inp.u
+    u_out = VField(*[Field.like(f, torch.empty_like(f.a)) for f in u_in.components()])
+    # calls 1 and 2 of the chain: builds psi^n, psi^{n-1} so the split term is active
+    pn, pnm1 = inp.psi_n, inp.psi_nm1
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            psi = new()
+            eqn.projection(psi, pn, pnm1, inp.rho, u_in, dt, alpha, u_out=u_out, want_stats=False)
+            pnm1, pn = pn, psi
+    stream.synchronize()
+    psi = new()
+
+    def step():
+        eqn.projection(psi, pn, pnm1, inp.rho, u_in, dt, alpha, u_out=u_out, want_stats=False)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+
+    # per-stage device times (CUDA events recorded by the library between its launches)
+    nstat = 5
+    acc = [0.0] * 8
+    last = None
+    for _ in range(nstat):
+        last = eqn.projection(psi, pn, pnm1, inp.rho, u_in, dt, alpha, u_out=u_out)
+        for i in range(8):
+            acc[i] += last.ms_stage[i] / nstat
+    stage_ms = dict(zip(STAGES, acc))
+
+    # end to end through the host entry point, pinned host buffers
+    def pinned(f):
+        h = torch.empty(f.a.shape, dtype=torch.float64, pin_memory=True)
+        h.copy_(f.a)
+        return Field.like(f, h.numpy())
+
+    hu = VField(*[pinned(f) for f in u_in.components()])
+    hrho, hpn, hpnm1 = pinned(inp.rho), pinned(pn), pinned(pnm1)
+    hpsi = pinned(psi)
+    hu0 = [f.a.copy() for f in hu.components()]
+    h2d = sum(f.a.nbytes for f in (*hu.components(), hrho, hpn, hpnm1))
+    d2h = sum(f.a.nbytes for f in (*hu.components(), hpsi))
+    eqn.projection(hpsi, hpn, hpnm1, hrho, hu, dt, alpha, want_stats=False)  # warm the host path
+    e2e_ms = []
+    for _ in range(args.e2e_steps):
+        for f, a0 in zip(hu.components(), hu0):
+            f.a[...] = a0
+        a0e, a1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0e.record(stream)
+        eqn.projection(hpsi, hpn, hpnm1, hrho, hu, dt, alpha, want_stats=False)
+        a1e.record(stream)
+        stream.synchronize()
+        e2e_ms.append(a0e.elapsed_time(a1e))
+    e2e = statistics.median(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = float(t.item())
+
+    N = g.ncells
+    value = world * N / (ms * 1e-3) / 1e9
+    e2e_value = world * N / (e2e * 1e-3) / 1e9
+    pk, pk_kind = peaks()
+    ab = alg_bytes(g.nx, g.ny, g.nz)
+    dom = max((k for k in stage_ms if stage_ms[k] > 0), key=lambda k: stage_ms[k])
+    achieved = ab[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        try:
+            with open(prof) as f:
+                traffic = json.load(f).get(args.config, {}).get(dom)
+        except Exception:
+            traffic = None
+    stages = {k: {"ms": round(v, 4), "alg_GBps": round(ab[k] / (v * 1e-3) / 1e9, 1) if v > 0 else None,
+                  "frac": round(ab[k] / (v * 1e-3) / 1e9 / pk, 3) if v > 0 else None}
+              for k, v in stage_ms.items() if v > 0}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        gcell, cores, kind, sample = cpu_baseline_sample(args.seed)
+        cpu = {"value": gcell, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": spec.name, "cells": N, "precision": "fp64", "parallelism":
+                   f"independent channel per GPU x{world}", "l2": "inputs larger than L2 (0.4 GB per field)"},
+        "solves_per_s": world * 1e3 / ms,
+        "max_div": last.max_div, "cont_err": last.cont_err,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk, "unit": "GB/s",
+                     "frac": achieved / pk, "traffic": traffic, "peak_kind": pk_kind,
+                     "alg_bytes_per_launch": ab[dom]},
+        "step_roofline": {"b_alg_bytes": ab["b_alg"], "achieved": ab["b_alg"] / (ms * 1e-3) / 1e9,
+                          "frac": ab["b_alg"] / (ms * 1e-3) / 1e9 / pk},
+        "stages": stages,
+        "gpu_launches": 7 * args.steps,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

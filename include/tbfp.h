@@ -1,0 +1,191 @@
+/*
+ * tbfp.h -- C ABI of the B200-native pressure-projection library for
+ * TBFsolver-style bubbly channel flow.
+ *
+ * The library replaces, behind plain C calls, the Fortran subroutines of the
+ * reference's FAST_MODE projection step:
+ *
+ *   fastPoissonSolverCTOR   src/fastPoissonSolver/fastPoissonSolver.f90:123  -> tbfp_create
+ *   solveFPS                src/fastPoissonSolver/fastPoissonSolver.f90:337  -> tbfp_solve_fps[_dev]
+ *   computeSource (FAST)    src/poissonEqn/poissonEqn.f90:193                -> tbfp_rhs_split[_dev]
+ *   makeVelocityDivFree     src/momentumEqn/momentumEqn.f90:999              -> tbfp_correct[_dev]
+ *   computeContinuityError  src/auxiliaryRoutines/auxiliaryRoutines.f90:42   -> tbfp_continuity_error[_dev]
+ *   solvePoissonEqn + makeVelocityDivFree + computeContinuityError
+ *                           src/main.f90:197-212                             -> tbfp_projection[_dev]
+ *
+ * Array convention.  Every field argument is the base address of a Fortran
+ * allocatable WITH its halo, exactly as the reference allocates it
+ * (field.f90:271-273): a cell field ('cl') is f(1-hd:nx+hd, 1-hd:ny+hd,
+ * 1-hd:nz+hd); the staggered velocity components are ux(-hd:nx+hd, ...) ('sx'),
+ * uy(.., -hd:ny+hd, ..) ('sy'), uz(.., .., -hd:nz+hd) ('sz'), column-major
+ * (i fastest).  The halo widths are given once in tbfp_desc.  Host-pointer
+ * entry points copy to and from device buffers owned by the handle; the
+ * *_dev entry points take device pointers with the same layout.
+ *
+ * Return convention (mirrors the reference's error handling, errorHandler.f90):
+ *   0   TBFP_OK
+ *   >0  soft condition; results are valid (e.g. an iteration cap was reached,
+ *       the reference's warning at pcg.f90:366-373)
+ *   <0  hard error; a Fortran caller maps it to mpiABORT(tbfp_strerror(rc)).
+ * A singular tridiagonal pivot is NOT an error (fastPoissonSolver.f90:318-322).
+ *
+ * Threading: one handle per host thread; calls on one handle are not
+ * re-entrant.  All calls are synchronous (they return after the device work
+ * has completed) unless TBFP_FLAG_ASYNC is set at create time.
+ */
+#ifndef TBFP_H
+#define TBFP_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TBFP_ABI_VERSION 1
+
+/* status codes */
+#define TBFP_OK 0
+#define TBFP_ENOTCONVERGED 1 /* soft: iteration cap reached */
+#define TBFP_EINVAL (-1)     /* invalid descriptor or argument */
+#define TBFP_ENULL (-2)      /* a required pointer is NULL */
+#define TBFP_ECUDA (-3)      /* CUDA runtime error */
+#define TBFP_ENOMEM (-4)     /* device allocation failed */
+#define TBFP_EUNSUPPORTED (-5) /* size or feature not supported */
+#define TBFP_ENODEVICE (-6)  /* no usable CUDA device */
+
+/* precision modes */
+#define TBFP_FP64 0  /* plain FP64: the drop-in for solveFPS */
+#define TBFP_MIXED 1 /* FP32 transforms + FP64 defect correction */
+
+/* create-time flags */
+#define TBFP_FLAG_ASYNC 1u  /* do not synchronise the stream before returning */
+#define TBFP_FLAG_TIMING 2u /* record per-stage device times into tbfp_stats.ms_stage */
+
+/* stages of one projection, indices into tbfp_stats.ms_stage */
+#define TBFP_STAGE_RECIP 0      /* 1/rho */
+#define TBFP_STAGE_RHS_FFTX 1   /* split RHS + forward x transform */
+#define TBFP_STAGE_FFTZ_FWD 2   /* forward z transform */
+#define TBFP_STAGE_TRIDIAG 3    /* y tridiagonal systems + gauge */
+#define TBFP_STAGE_FFTZ_INV 4   /* backward z transform */
+#define TBFP_STAGE_FFTX_INV 5   /* backward x transform, psi + ghosts */
+#define TBFP_STAGE_CORRECT 6    /* velocity correction (+ continuity check) */
+#define TBFP_STAGE_DIV 7        /* separate continuity check (in-place path) */
+#define TBFP_NSTAGES 8
+
+typedef struct tbfp_handle tbfp_handle;
+
+/*
+ * Create-time descriptor.  Grid metrics are the reference mesh arrays
+ * (grid.f90:334-399) for the interior index ranges given below; they are
+ * copied at create time.  x and z must be uniform and periodic, y
+ * wall-bounded (grid.f90:219-230, mpiControl.f90:206-228).
+ */
+typedef struct {
+  int nx, ny, nz;      /* global cell counts */
+  int hd_psi;          /* halo of psi, its old levels and s (reference: 1) */
+  int hd_u;            /* halo of ux, uy, uz (reference: 2) */
+  int hd_rho;          /* halo of rho (reference: 1) */
+  int hd_st;           /* halo of the surface-tension components (reference: 1) */
+  double dx_fft;       /* xc(2)-xc(1), spacing of the x eigenvalues (fastPoissonSolver.f90:222) */
+  double dz_fft;       /* zc(2)-zc(1) (fastPoissonSolver.f90:223) */
+  const double *dxf;   /* dxf(1..nx)   */
+  const double *dxc;   /* dxc(1..nx+1) */
+  const double *dyf;   /* dyf(1..ny)   */
+  const double *dyc;   /* dyc(1..ny+1) */
+  const double *dzf;   /* dzf(1..nz)   */
+  const double *dzc;   /* dzc(1..nz+1) */
+  double s_Vg;         /* total volume (grid.f90:933-951); <= 0: computed from dxf,dyf,dzf */
+  int precision;       /* TBFP_FP64 or TBFP_MIXED */
+  double tol;          /* TBFP_MIXED: target ||s - L psi||_2 / ||s||_2 */
+  int max_iter;        /* TBFP_MIXED: cap on defect-correction sweeps */
+  int device;          /* CUDA device ordinal; < 0 selects the current device */
+  void *stream;        /* cudaStream_t to run on; NULL: the library creates one */
+  unsigned flags;      /* TBFP_FLAG_* */
+} tbfp_desc;
+
+/* Per-call statistics (the reference prints these to stdout). */
+typedef struct {
+  int iterations;       /* defect-correction sweeps (1 for TBFP_FP64) */
+  double rel_residual;  /* ||s - L psi||_2/||s||_2 when computed, else -1 */
+  double max_div;       /* max|div u| after the correction (auxiliaryRoutines.f90:75) */
+  double cont_err;      /* dt * max_div, the reference's "continuity error" (:82) */
+  double ms_device;     /* device time of the call, ms (CUDA events) */
+  double ms_stage[8];   /* per-stage device time (TBFP_FLAG_TIMING), else 0 */
+} tbfp_stats;
+
+/* --- lifecycle --------------------------------------------------------- */
+int tbfp_abi_version(void);
+const char *tbfp_strerror(int status);
+/* Last error message of a handle (or of the last failed tbfp_create if h is NULL). */
+const char *tbfp_last_error(const tbfp_handle *h);
+/* fastPoissonSolverCTOR (fastPoissonSolver.f90:123-156): eigenvalues, off-diagonals,
+   transform plans and device work buffers. */
+int tbfp_create(const tbfp_desc *d, tbfp_handle **h);
+int tbfp_destroy(tbfp_handle *h);
+/* Bytes of device memory the handle holds. */
+size_t tbfp_device_bytes(const tbfp_handle *h);
+
+/* --- solveFPS (fastPoissonSolver.f90:337-384) -------------------------- */
+/* s: cell field (hd_psi), read on the interior.  psi: cell field (hd_psi),
+   written on the interior and on the ghost cells (the updateBoundaries of
+   fastPoissonSolver.f90:381: Neumann at the y walls, periodic in x and z). */
+int tbfp_solve_fps(tbfp_handle *h, const double *s, double *psi);
+int tbfp_solve_fps_dev(tbfp_handle *h, const double *s, double *psi);
+
+/* --- computeSource, FAST_MODE (poissonEqn.f90:193-305) ----------------- */
+/* psi_n = psi%ptrf_, psi_nm1 = psi%ptrf_%ptrf_.  st_n / st_nm1: arrays of the
+   three staggered surface-tension components at the old levels, or NULL for
+   zero surface tension.  s: cell field (hd_psi), interior written. */
+int tbfp_rhs_split(tbfp_handle *h, const double *ux, const double *uy, const double *uz,
+                   const double *rho, const double *psi_n, const double *psi_nm1,
+                   const double *const *st_n, const double *const *st_nm1,
+                   double dt, double alpha, double rho0, double *s);
+int tbfp_rhs_split_dev(tbfp_handle *h, const double *ux, const double *uy, const double *uz,
+                       const double *rho, const double *psi_n, const double *psi_nm1,
+                       const double *const *st_n, const double *const *st_nm1,
+                       double dt, double alpha, double rho0, double *s);
+
+/* --- makeVelocityDivFree, FAST_MODE (momentumEqn.f90:999-1127) --------- */
+/* In place on ux, uy, uz: faces of setEqnBounds (momentumEqn.f90:1134-1190)
+   are corrected and the periodic duplicate faces are equated
+   (vfield.f90:124-189).  The remaining ghost/halo refresh of u is left to the
+   caller's updateBoundariesV, as in the reference. */
+int tbfp_correct(tbfp_handle *h, double *ux, double *uy, double *uz, const double *psi,
+                 const double *psi_n, const double *psi_nm1, const double *rho,
+                 const double *const *st_n, const double *const *st_nm1,
+                 double dt, double alpha, double rho0);
+int tbfp_correct_dev(tbfp_handle *h, double *ux, double *uy, double *uz, const double *psi,
+                     const double *psi_n, const double *psi_nm1, const double *rho,
+                     const double *const *st_n, const double *const *st_nm1,
+                     double dt, double alpha, double rho0);
+
+/* --- computeContinuityError (auxiliaryRoutines.f90:42-91) -------------- */
+/* max_div = max|div u| over the interior; cont_err = dt * max_div.  Either
+   output pointer may be NULL. */
+int tbfp_continuity_error(tbfp_handle *h, const double *ux, const double *uy, const double *uz,
+                          double dt, double *max_div, double *cont_err);
+int tbfp_continuity_error_dev(tbfp_handle *h, const double *ux, const double *uy,
+                              const double *uz, double dt, double *max_div, double *cont_err);
+
+/* --- one projection (main.f90:197-212) ---------------------------------- */
+/* computeSource -> solveFPS -> makeVelocityDivFree -> computeContinuityError.
+   ux, uy, uz are read as u* and overwritten with the projected velocity; psi
+   receives the new pressure (interior + ghosts).  stats may be NULL. */
+int tbfp_projection(tbfp_handle *h, double *ux, double *uy, double *uz, const double *rho,
+                    const double *psi_n, const double *psi_nm1,
+                    const double *const *st_n, const double *const *st_nm1,
+                    double dt, double alpha, double rho0, double *psi, tbfp_stats *stats);
+/* Device-pointer form.  u*_in are read, u*_out written: they may be the same
+   arrays (in place).  Every interior face of u*_out is written; halos are not. */
+int tbfp_projection_dev(tbfp_handle *h, const double *ux_in, const double *uy_in,
+                        const double *uz_in, double *ux_out, double *uy_out, double *uz_out,
+                        const double *rho, const double *psi_n, const double *psi_nm1,
+                        const double *const *st_n, const double *const *st_nm1,
+                        double dt, double alpha, double rho0, double *psi, tbfp_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TBFP_H */

@@ -1,0 +1,504 @@
+"""CPU oracle for the TBFsolver pressure-projection step (numpy/scipy restatement).
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the shipped library imports or calls this
+module; only ``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` /
+``--impl reference`` legs of ``bench.py`` use it, and only as the checker.
+
+Every function restates the reference Fortran (cifanip/TBFsolver) line by line
+and cites the file:line it follows.  The reference itself cannot be built in
+this environment (no Fortran compiler, MPI, FFTW, LAPACK or MUMPS), and the
+reference ships no tests, golden vectors or fixtures for this path
+(its example case ``channel_18`` has its input fields missing).  PARITY IS
+UNPINNED against reference outputs; the restatement is pinned instead by
+analytic known-answer tests (manufactured discrete solutions, single Fourier
+modes, post-projection divergence) and by the fact that the tridiagonal step
+calls the very LAPACK routines (``zgttrf``/``zgttrs``) the reference calls.
+
+Array convention
+----------------
+A Fortran array ``f_(ilo:ihi, jlo:jhi, klo:khi)`` is held as a C-ordered numpy
+array of shape ``(khi-klo+1, jhi-jlo+1, ihi-ilo+1)`` -- byte-for-byte the same
+memory image as the Fortran column-major array.  ``FField`` carries the lower
+bounds so code can index with the reference's (i, j, k) ranges.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field as dc_field
+
+import numpy as np
+from scipy.linalg import lapack
+
+EPS64 = float(np.finfo(np.float64).eps)  # Fortran epsilon(0.d0)
+TINY64 = float(np.finfo(np.float64).tiny)  # Fortran tiny(0.d0)
+
+# field.f90:28-30 boundary types
+FIXED_VALUE, NORMAL_GRADIENT, PERIODIC = 1, 2, 3
+
+
+# ---------------------------------------------------------------------------
+# 1-D arrays with Fortran lower bounds
+# ---------------------------------------------------------------------------
+class FArr1:
+    """1-D array with a Fortran lower bound: ``a[i]`` and ``a.r(i0, i1)`` (inclusive)."""
+
+    def __init__(self, lb: int, values: np.ndarray):
+        self.lb = int(lb)
+        self.v = np.asarray(values, dtype=np.float64)
+
+    @property
+    def ub(self) -> int:
+        return self.lb + self.v.size - 1
+
+    def __getitem__(self, i: int) -> float:
+        return float(self.v[i - self.lb])
+
+    def r(self, i0: int, i1: int) -> np.ndarray:
+        return self.v[i0 - self.lb : i1 - self.lb + 1]
+
+
+# ---------------------------------------------------------------------------
+# grid.f90 restatement (single rank: local mesh == global mesh)
+# ---------------------------------------------------------------------------
+def _coord_unif_c(lb, ub, L, n):
+    # grid.f90:235-257  q(i) = 0.5*delta + (n-1)*delta, n starting at i0-gHD == lb
+    delta = L / n
+    idx = np.arange(lb, ub + 1, dtype=np.float64)
+    return 0.5 * delta + (idx - 1.0) * delta
+
+
+def _coord_unif_f(lb, ub, L, n):
+    # grid.f90:261-283  q(i) = n*delta, n starting at i0-1-gHD == lb
+    delta = L / n
+    idx = np.arange(lb, ub + 1, dtype=np.float64)
+    return idx * delta
+
+
+def _coord_hyper_c(lb, ub, L, n, gamma):
+    # grid.f90:288-307 (the reference hard-codes s_gamma=1.4 at grid.f90:27;
+    # the restatement takes gamma as a parameter)
+    idx = np.arange(lb, ub + 1, dtype=np.float64)
+    return 0.5 * L * (1.0 + np.tanh(-gamma + 2.0 * gamma * (idx - 0.5) / n) / math.tanh(gamma))
+
+
+def _coord_hyper_f(lb, ub, L, n, gamma):
+    # grid.f90:311-330
+    idx = np.arange(lb, ub + 1, dtype=np.float64)
+    return 0.5 * L * (1.0 + np.tanh(-gamma + 2.0 * gamma * idx / n) / math.tanh(gamma))
+
+
+@dataclass
+class Mesh:
+    """Restatement of ``gridCTOR`` (grid.f90:156-215) for one rank, halo gHD=3."""
+
+    nx: int
+    ny: int
+    nz: int
+    Lx: float
+    Ly: float
+    Lz: float
+    y_uniform: bool = True
+    gamma: float = 1.4
+    hd: int = 3
+    xc: FArr1 = dc_field(init=False)
+    yc: FArr1 = dc_field(init=False)
+    zc: FArr1 = dc_field(init=False)
+    xf: FArr1 = dc_field(init=False)
+    yf: FArr1 = dc_field(init=False)
+    zf: FArr1 = dc_field(init=False)
+    dxc: FArr1 = dc_field(init=False)
+    dyc: FArr1 = dc_field(init=False)
+    dzc: FArr1 = dc_field(init=False)
+    dxf: FArr1 = dc_field(init=False)
+    dyf: FArr1 = dc_field(init=False)
+    dzf: FArr1 = dc_field(init=False)
+    s_Vg: float = dc_field(init=False)
+
+    def __post_init__(self):
+        g = self.hd
+        nx, ny, nz = self.nx, self.ny, self.nz
+        # computeCoordinates grid.f90:633-688 (x, z uniform: checkGridSpacing :219-230)
+        self.xc = FArr1(1 - g, _coord_unif_c(1 - g, nx + g, self.Lx, nx))
+        self.zc = FArr1(1 - g, _coord_unif_c(1 - g, nz + g, self.Lz, nz))
+        self.xf = FArr1(0 - g, _coord_unif_f(0 - g, nx + g, self.Lx, nx))
+        self.zf = FArr1(0 - g, _coord_unif_f(0 - g, nz + g, self.Lz, nz))
+        if self.y_uniform:
+            self.yc = FArr1(1 - g, _coord_unif_c(1 - g, ny + g, self.Ly, ny))
+            self.yf = FArr1(0 - g, _coord_unif_f(0 - g, ny + g, self.Ly, ny))
+        else:
+            self.yc = FArr1(1 - g, _coord_hyper_c(1 - g, ny + g, self.Ly, ny, self.gamma))
+            self.yf = FArr1(0 - g, _coord_hyper_f(0 - g, ny + g, self.Ly, ny, self.gamma))
+        # metrics_centroids grid.f90:334-364: dxc(i) = xc(i)-xc(i-1), i = lb+1..ub
+        self.dxc = FArr1(self.xc.lb + 1, np.diff(self.xc.v))
+        self.dyc = FArr1(self.yc.lb + 1, np.diff(self.yc.v))
+        self.dzc = FArr1(self.zc.lb + 1, np.diff(self.zc.v))
+        # metrics_faces grid.f90:368-399
+        self.dxf = FArr1(self.xf.lb + 1, np.diff(self.xf.v))
+        self.dyf = FArr1(self.yf.lb + 1, np.diff(self.yf.v))
+        self.dzf = FArr1(self.zf.lb + 1, np.diff(self.zf.v))
+        # computeVolume grid.f90:784-807 and totalVolume :933-951 (loop order k, j, i)
+        s = 0.0
+        dxf = self.dxf.r(1, nx)
+        dyf = self.dyf.r(1, ny)
+        dzf = self.dzf.r(1, nz)
+        for k in range(nz):
+            # sequential accumulation in the Fortran loop order (cumsum is strictly
+            # left to right; the carry is prepended)
+            blk = ((dxf[None, :] * dyf[:, None]) * dzf[k]).ravel()
+            s = float(np.cumsum(np.concatenate(([s], blk)))[-1])
+        self.s_Vg = s
+
+    def volume(self) -> np.ndarray:
+        """V(i,j,k) = dxf(i)*dyf(j)*dzf(k) on the interior, shape (nz, ny, nx) (grid.f90:801)."""
+        dxf = self.dxf.r(1, self.nx)
+        dyf = self.dyf.r(1, self.ny)
+        dzf = self.dzf.r(1, self.nz)
+        return (dxf[None, None, :] * dyf[None, :, None]) * dzf[:, None, None]
+
+
+# ---------------------------------------------------------------------------
+# field.f90 restatement: storage with halos
+# ---------------------------------------------------------------------------
+_KIND_LO = {"cl": (1, 1, 1), "sx": (0, 1, 1), "sy": (1, 0, 1), "sz": (1, 1, 0)}
+
+
+class FField:
+    """Field ``f_(is-hd:ie+hd, js-hd:je+hd, ks-hd:ke+hd)`` (field.f90:271-273, :1746-1789)."""
+
+    def __init__(self, kind: str, hd: int, nx: int, ny: int, nz: int, data: np.ndarray | None = None):
+        lo = _KIND_LO[kind]
+        self.kind, self.hd = kind, hd
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.lb = (lo[0] - hd, lo[1] - hd, lo[2] - hd)
+        self.ub = (nx + hd, ny + hd, nz + hd)
+        shape = (self.ub[2] - self.lb[2] + 1, self.ub[1] - self.lb[1] + 1, self.ub[0] - self.lb[0] + 1)
+        if data is None:
+            self.a = np.zeros(shape, dtype=np.float64)
+        else:
+            assert data.shape == shape, (data.shape, shape)
+            self.a = data
+
+    def v(self, i0, i1, j0, j1, k0, k1) -> np.ndarray:
+        """View of the inclusive Fortran range (i0:i1, j0:j1, k0:k1)."""
+        lb = self.lb
+        return self.a[k0 - lb[2] : k1 - lb[2] + 1, j0 - lb[1] : j1 - lb[1] + 1, i0 - lb[0] : i1 - lb[0] + 1]
+
+    def copy(self) -> "FField":
+        return FField(self.kind, self.hd, self.nx, self.ny, self.nz, self.a.copy())
+
+    def interior(self) -> np.ndarray:
+        lo = _KIND_LO[self.kind]
+        return self.v(lo[0], self.nx, lo[1], self.ny, lo[2], self.nz)
+
+
+def update_boundaries_cl_channel(f: FField) -> None:
+    """updateBoundaries (field.f90:950-974) for a cell field of the channel:
+    normalGradient (bf=0) at the y walls (boundaryField_S.f90:694-727, one ghost
+    layer on the interior i,k range), then the periodic halo exchange in x and
+    then z over the full extended ranges (field.f90:708-788 with a single rank,
+    whose Cartesian neighbours are itself)."""
+    nx, ny, nz, hd = f.nx, f.ny, f.nz, f.hd
+    f.v(1, nx, 0, 0, 1, nz)[...] = f.v(1, nx, 1, 1, 1, nz)
+    f.v(1, nx, ny + 1, ny + 1, 1, nz)[...] = f.v(1, nx, ny, ny, 1, nz)
+    jl, jh, kl, kh = 1 - hd, ny + hd, 1 - hd, nz + hd
+    il, ih = 1 - hd, nx + hd
+    # x: recv from right into ie+1.. <- is..is+hd-1 ; recv from left into is-hd.. <- ie-hd+1..ie
+    f.v(nx + 1, nx + hd, jl, jh, kl, kh)[...] = f.v(1, hd, jl, jh, kl, kh)
+    f.v(1 - hd, 0, jl, jh, kl, kh)[...] = f.v(nx - hd + 1, nx, jl, jh, kl, kh)
+    # z (front-back) over all i, j
+    f.v(il, ih, jl, jh, nz + 1, nz + hd)[...] = f.v(il, ih, jl, jh, 1, hd)
+    f.v(il, ih, jl, jh, 1 - hd, 0)[...] = f.v(il, ih, jl, jh, nz - hd + 1, nz)
+
+
+def equate_periodic_bc(ux: FField, uz: FField) -> None:
+    """equatePeriodicBC (vfield.f90:124-189) on one rank: ux(0,:,:) = ux(nx,:,:),
+    uz(:,:,0) = uz(:,:,nz) (y is wall-bounded, so uy is left alone)."""
+    ux.v(0, 0, ux.lb[1], ux.ub[1], ux.lb[2], ux.ub[2])[...] = ux.v(ux.nx, ux.nx, ux.lb[1], ux.ub[1], ux.lb[2], ux.ub[2])
+    uz.v(uz.lb[0], uz.ub[0], uz.lb[1], uz.ub[1], 0, 0)[...] = uz.v(uz.lb[0], uz.ub[0], uz.lb[1], uz.ub[1], uz.nz, uz.nz)
+
+
+# ---------------------------------------------------------------------------
+# poissonEqn.f90 (FAST_MODE): split right-hand side
+# ---------------------------------------------------------------------------
+def compute_source_fast(mesh: Mesh, psi_n: FField, psi_nm1: FField, rho: FField,
+                        ux: FField, uy: FField, uz: FField, dt: float, alpha: float, rho0: float,
+                        st_n=None, st_nm1=None) -> np.ndarray:
+    """computeSource (poissonEqn.f90:193-256) + computeOldPressDiv (:258-305), nl=2.
+
+    ``st_n``/``st_nm1`` are (stx, sty, stz) FField triples or None (zero surface
+    tension).  Returns the interior source s, shape (nz, ny, nx)."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    r = 1.0 / (alpha * dt)
+    dxf1, dzf1 = mesh.dxf[1], mesh.dzf[1]
+    dxc1, dzc1 = mesh.dxc[1], mesh.dzc[1]
+    dyf = mesh.dyf.r(1, ny)[None, :, None]
+    dycp = mesh.dyc.r(2, ny + 1)[None, :, None]  # dyc(j+1)
+    dycm = mesh.dyc.r(1, ny)[None, :, None]  # dyc(j)
+
+    def P(f, di=0, dj=0, dk=0):
+        return f.v(1 + di, nx + di, 1 + dj, ny + dj, 1 + dk, nz + dk)
+
+    ddx = (P(ux) - P(ux, di=-1)) / dxf1
+    ddy = (P(uy) - P(uy, dj=-1)) / dyf
+    ddz = (P(uz) - P(uz, dk=-1)) / dzf1
+    s = ((ddx + ddy) + ddz) * r * rho0
+
+    irc = 1.0 / P(rho)
+    apx = 1.0 - rho0 * 0.5 * (1.0 / P(rho, di=1) + irc)
+    amx = 1.0 - rho0 * 0.5 * (1.0 / P(rho, di=-1) + irc)
+    apy = 1.0 - rho0 * 0.5 * (1.0 / P(rho, dj=1) + irc)
+    amy = 1.0 - rho0 * 0.5 * (1.0 / P(rho, dj=-1) + irc)
+    apz = 1.0 - rho0 * 0.5 * (1.0 / P(rho, dk=1) + irc)
+    amz = 1.0 - rho0 * 0.5 * (1.0 / P(rho, dk=-1) + irc)
+
+    def grad(dc, sh_p, sh_m):
+        # 2*(pn(+)-pn(-)) - (pnm1(+)-pnm1(-)), divided by the centroid spacing
+        g = 2.0 * (P(psi_n, **sh_p) - P(psi_n, **sh_m))
+        g = g - (P(psi_nm1, **sh_p) - P(psi_nm1, **sh_m))
+        return g / dc
+
+    dpxp = grad(dxc1, dict(di=1), {})
+    dpxm = grad(dxc1, {}, dict(di=-1))
+    dpyp = grad(dycp, dict(dj=1), {})
+    dpym = grad(dycm, {}, dict(dj=-1))
+    dpzp = grad(dzc1, dict(dk=1), {})
+    dpzm = grad(dzc1, {}, dict(dk=-1))
+    if st_n is not None:
+        sxn, syn, szn = st_n
+        sxo, syo, szo = st_nm1
+        dpxp = dpxp - 2.0 * P(sxn) + P(sxo)
+        dpxm = dpxm - 2.0 * P(sxn, di=-1) + P(sxo, di=-1)
+        dpyp = dpyp - 2.0 * P(syn) + P(syo)
+        dpym = dpym - 2.0 * P(syn, dj=-1) + P(syo, dj=-1)
+        dpzp = dpzp - 2.0 * P(szn) + P(szo)
+        dpzm = dpzm - 2.0 * P(szn, dk=-1) + P(szo, dk=-1)
+
+    ddx = (apx * dpxp - amx * dpxm) / dxf1
+    ddy = (apy * dpyp - amy * dpym) / dyf
+    ddz = (apz * dpzp - amz * dpzm) / dzf1
+    return ((s + ddx) + ddy) + ddz
+
+
+# ---------------------------------------------------------------------------
+# fastPoissonSolver.f90: FFT(x,z) + tridiagonal(y) direct solve
+# ---------------------------------------------------------------------------
+def fps_eigenvalues(mesh: Mesh):
+    """computeEigenvalues (fastPoissonSolver.f90:215-251): lx(i), i=1..nx, and lz(k)."""
+    dx = mesh.xc[2] - mesh.xc[1]
+    dz = mesh.zc[2] - mesh.zc[1]
+    vx = np.arange(mesh.nx, dtype=np.float64) * 2.0 * math.pi
+    vz = np.arange(mesh.nz, dtype=np.float64) * 2.0 * math.pi
+    lx = 2.0 * (np.cos(vx / mesh.nx) - 1.0) / (dx * dx)
+    lz = 2.0 * (np.cos(vz / mesh.nz) - 1.0) / (dz * dz)
+    return lx, lz
+
+
+def fps_offdiag(mesh: Mesh):
+    """initOffDiagMatrix (fastPoissonSolver.f90:255-276): am(j), ap(j), j=1..ny."""
+    ny = mesh.ny
+    am = 1.0 / (mesh.dyc.r(1, ny) * mesh.dyf.r(1, ny))
+    am[0] = 0.0
+    ap = 1.0 / (mesh.dyc.r(2, ny + 1) * mesh.dyf.r(1, ny))
+    ap[-1] = 0.0
+    return am, ap
+
+
+def solve_tridiag_lapack(spec: np.ndarray, lx: np.ndarray, lz: np.ndarray, am: np.ndarray, ap: np.ndarray) -> None:
+    """solveTriDiag (fastPoissonSolver.f90:280-333) with the LAPACK routines the
+    reference calls.  ``spec`` has shape (nz, ny, nkx) (complex, modified in place);
+    system (kx, kz) runs along axis 1.  Row scaling by r=1/(lx+lz-am-ap) so the
+    diagonal is 1; ``zgttrf``; if info != 0 the last U pivot becomes epsilon
+    (:318-322); ``zgttrs``."""
+    nz, ny, nkx = spec.shape
+    for kz in range(nz):
+        for kx in range(nkx):
+            r = 1.0 / (lx[kx] + lz[kz] - am - ap)
+            am_s = (am * r).astype(np.complex128)
+            ap_s = (ap * r).astype(np.complex128)
+            ac = np.ones(ny, dtype=np.complex128)
+            fy = spec[kz, :, kx] * r
+            dl, d, du, du2, ipiv, info = lapack.zgttrf(am_s[1:].copy(), ac, ap_s[:-1].copy())
+            if info != 0:
+                d[ny - 1] = EPS64
+            x, info2 = lapack.zgttrs(dl, d, du, du2, ipiv, fy)
+            spec[kz, :, kx] = x
+
+
+def solve_tridiag_thomas(spec: np.ndarray, lx: np.ndarray, lz: np.ndarray, am: np.ndarray, ap: np.ndarray) -> None:
+    """Vectorised no-pivoting LU of the same scaled systems (a faster stand-in for
+    the LAPACK call on large grids).  The singular (kx,kz)=(0,0) system gets the
+    same epsilon-pivot rule as :318-322 when its last pivot is exactly zero."""
+    nz, ny, nkx = spec.shape
+    lam = lz[:, None] + lx[None, :nkx]  # (nz, nkx)
+    cp = np.empty((ny, nz, nkx))
+    dp = np.empty((ny, nz, nkx), dtype=np.complex128)
+    r0 = 1.0 / (lam - am[0] - ap[0])
+    c_prev = ap[0] * r0  # U(1,1) = 1
+    d_prev = spec[:, 0, :] * r0
+    cp[0] = c_prev
+    dp[0] = d_prev
+    piv = np.ones_like(lam)
+    for j in range(1, ny):
+        r = 1.0 / (lam - am[j] - ap[j])
+        a = am[j] * r
+        den = 1.0 - a * c_prev
+        if j == ny - 1:
+            den = np.where(den == 0.0, EPS64, den)
+        c_prev = (ap[j] * r) / den
+        d_prev = (spec[:, j, :] * r - a * d_prev) / den
+        cp[j] = c_prev
+        dp[j] = d_prev
+    x = dp[ny - 1]
+    spec[:, ny - 1, :] = x
+    for j in range(ny - 2, -1, -1):
+        x = dp[j] - cp[j] * x
+        spec[:, j, :] = x
+    del piv
+
+
+def solve_fps(mesh: Mesh, s: np.ndarray, psi: FField, tridiag: str = "lapack") -> None:
+    """solveFPS (fastPoissonSolver.f90:337-384): r2c along x (:353), c2c along z
+    (:357), tridiagonal along y (:363), inverse z (:367) and c2r x (:371), scale by
+    1/(nx*nz) (:374), zero volume-weighted mean (:380, :388-423), then
+    updateBoundaries (:381).  All transforms unnormalised as FFTW's."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    spec = np.fft.rfft(s, axis=2)  # (nz, ny, nx/2+1), unnormalised forward
+    spec = np.fft.fft(spec, axis=0)
+    lx, lz = fps_eigenvalues(mesh)
+    am, ap = fps_offdiag(mesh)
+    if tridiag == "lapack":
+        solve_tridiag_lapack(spec, lx, lz, am, ap)
+    elif tridiag == "thomas":
+        solve_tridiag_thomas(spec, lx, lz, am, ap)
+    else:
+        raise ValueError(tridiag)
+    spec = np.fft.ifft(spec, axis=0, norm="forward")  # unnormalised backward
+    p = np.fft.irfft(spec, n=nx, axis=2, norm="forward")
+    p = p / (nx * nz)
+    psi.v(1, nx, 1, ny, 1, nz)[...] = p
+    zero_average_pressure(mesh, psi)
+    update_boundaries_cl_channel(psi)
+
+
+def zero_average_pressure(mesh: Mesh, p: FField) -> None:
+    """zeroAveragePressure (fastPoissonSolver.f90:388-423): p -= sum(p*V)/s_Vg,
+    applied to the whole array including the halo (:421)."""
+    av = float(np.sum(p.interior() * mesh.volume()))
+    avg = av / mesh.s_Vg
+    p.a -= avg
+
+
+# ---------------------------------------------------------------------------
+# momentumEqn.f90 (FAST_MODE) velocity correction
+# ---------------------------------------------------------------------------
+def make_velocity_div_free(mesh: Mesh, ux: FField, uy: FField, uz: FField, psi: FField,
+                           psi_n: FField, psi_nm1: FField, rho: FField,
+                           dt: float, alpha: float, rho0: float, st_n=None, st_nm1=None) -> None:
+    """makeVelocityDivFree FAST (momentumEqn.f90:999-1090) + computeOldPressGrad
+    (:1092-1127), in place.  Loop ranges follow setEqnBounds (:1134-1190) for the
+    channel: ux i=0..nx (periodic), uy j=1..ny-1 (fixedValue walls excluded), uz
+    k=0..nz.  Ends with the periodic equate of updateBoundariesV (vfield.f90:118,
+    :124-189); the remaining ghost/halo refresh of u is the caller's."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    r = dt * alpha
+    invrho0 = 1.0 / rho0
+
+    def upd(u, i0, i1, j0, j1, k0, k1, di, dj, dk, dc, stc):
+        def S(f, o=0):
+            return f.v(i0 + di * o, i1 + di * o, j0 + dj * o, j1 + dj * o, k0 + dk * o, k1 + dk * o)
+
+        invrho = 0.5 * (1.0 / S(rho, 1) + 1.0 / S(rho))
+        dpr = (S(psi, 1) - S(psi)) / dc
+        dpr0 = (2.0 * (S(psi_n, 1) - S(psi_n)) - (S(psi_nm1, 1) - S(psi_nm1))) / dc
+        if st_n is not None:
+            dpr0 = dpr0 - 2.0 * S(st_n[stc]) + S(st_nm1[stc])
+        tgt = u.v(i0, i1, j0, j1, k0, k1)
+        tgt -= r * (invrho0 * dpr + (invrho - invrho0) * dpr0)
+
+    upd(ux, 0, nx, 1, ny, 1, nz, 1, 0, 0, mesh.dxc[1], 0)
+    upd(uy, 1, nx, 1, ny - 1, 1, nz, 0, 1, 0, mesh.dyc.r(2, ny)[None, :, None], 1)
+    upd(uz, 1, nx, 1, ny, 0, nz, 0, 0, 1, mesh.dzc[1], 2)
+    equate_periodic_bc(ux, uz)
+
+
+def compute_continuity_error(mesh: Mesh, ux: FField, uy: FField, uz: FField) -> float:
+    """max|div u| over the interior (auxiliaryRoutines.f90:42-91), WITHOUT the
+    final multiplication by dt (:82) so both forms can be reported."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    dxf = mesh.dxf.r(1, nx)[None, None, :]
+    dyf = mesh.dyf.r(1, ny)[None, :, None]
+    dzf = mesh.dzf.r(1, nz)[:, None, None]
+    d = (ux.v(1, nx, 1, ny, 1, nz) - ux.v(0, nx - 1, 1, ny, 1, nz)) / dxf
+    d = d + (uy.v(1, nx, 1, ny, 1, nz) - uy.v(1, nx, 0, ny - 1, 1, nz)) / dyf
+    d = d + (uz.v(1, nx, 1, ny, 1, nz) - uz.v(1, nx, 1, ny, 0, nz - 1)) / dzf
+    return float(np.max(np.abs(d))) if d.size else -1.0
+
+
+def divergence(mesh: Mesh, ux: FField, uy: FField, uz: FField) -> np.ndarray:
+    """The cell divergence field used by compute_continuity_error (auxiliaryRoutines.f90:71-75)."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    dxf = mesh.dxf.r(1, nx)[None, None, :]
+    dyf = mesh.dyf.r(1, ny)[None, :, None]
+    dzf = mesh.dzf.r(1, nz)[:, None, None]
+    d = (ux.v(1, nx, 1, ny, 1, nz) - ux.v(0, nx - 1, 1, ny, 1, nz)) / dxf
+    d = d + (uy.v(1, nx, 1, ny, 1, nz) - uy.v(1, nx, 0, ny - 1, 1, nz)) / dyf
+    return d + (uz.v(1, nx, 1, ny, 1, nz) - uz.v(1, nx, 1, ny, 0, nz - 1)) / dzf
+
+
+# ---------------------------------------------------------------------------
+# The 7-point operator the split solve inverts (beta == 1 form of pcg.f90:163-176
+# with the am/ap of fastPoissonSolver.f90:265-273 and periodic x, z).
+# ---------------------------------------------------------------------------
+def laplacian_fps(mesh: Mesh, psi: FField) -> np.ndarray:
+    """L_h psi on the interior for a psi whose ghosts are up to date (Neumann walls
+    via the ghost rows, periodic x/z via halos).  x and z use the uniform spacing
+    dx=xc(2)-xc(1) exactly as the eigenvalues do; y uses am/ap."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    dx = mesh.xc[2] - mesh.xc[1]
+    dz = mesh.zc[2] - mesh.zc[1]
+    am, ap = fps_offdiag(mesh)
+    c = psi.v(1, nx, 1, ny, 1, nz)
+    lx = (psi.v(2, nx + 1, 1, ny, 1, nz) - 2.0 * c + psi.v(0, nx - 1, 1, ny, 1, nz)) / (dx * dx)
+    lz = (psi.v(1, nx, 1, ny, 2, nz + 1) - 2.0 * c + psi.v(1, nx, 1, ny, 0, nz - 1)) / (dz * dz)
+    ly = ap[None, :, None] * (psi.v(1, nx, 2, ny + 1, 1, nz) - c) - am[None, :, None] * (c - psi.v(1, nx, 0, ny - 1, 1, nz))
+    return lx + ly + lz
+
+
+# ---------------------------------------------------------------------------
+# one projection, as called from main.f90:197-215 (FAST_MODE)
+# ---------------------------------------------------------------------------
+@dataclass
+class ProjectionResult:
+    psi: FField
+    ux: FField
+    uy: FField
+    uz: FField
+    s: np.ndarray
+    max_div: float  # max|div u| (raw)
+    cont_err: float  # dt * max|div u| (auxiliaryRoutines.f90:82)
+
+
+def projection(mesh: Mesh, ux: FField, uy: FField, uz: FField, rho: FField, psi_n: FField,
+               psi_nm1: FField, dt: float, alpha: float, rho0: float, st_n=None, st_nm1=None,
+               tridiag: str = "lapack") -> ProjectionResult:
+    """solvePoissonEqn (poissonEqn.f90:347-370) -> makeVelocityDivFree
+    (momentumEqn.f90:999) -> computeContinuityError (auxiliaryRoutines.f90:42)
+    on copies of the inputs.  psi_n / psi_nm1 are psi%ptrf_ and psi%ptrf_%ptrf_."""
+    s = compute_source_fast(mesh, psi_n, psi_nm1, rho, ux, uy, uz, dt, alpha, rho0, st_n, st_nm1)
+    psi = FField("cl", psi_n.hd, mesh.nx, mesh.ny, mesh.nz)
+    solve_fps(mesh, s, psi, tridiag=tridiag)
+    uxo, uyo, uzo = ux.copy(), uy.copy(), uz.copy()
+    make_velocity_div_free(mesh, uxo, uyo, uzo, psi, psi_n, psi_nm1, rho, dt, alpha, rho0, st_n, st_nm1)
+    md = compute_continuity_error(mesh, uxo, uyo, uzo)
+    return ProjectionResult(psi, uxo, uyo, uzo, s, md, md * dt)
+
+
+def alpha_rks(scheme: int, substep: int = 1) -> float:
+    """alphaRKS (time.f90:99-105) with the tables of initRK3coef (time.f90:365-405)."""
+    if scheme == 0:
+        gamma, xi = (1.5, 0.0, 0.0), (-0.5, 0.0, 0.0)
+    elif scheme == 1:
+        gamma, xi = (8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0), (0.0, -17.0 / 60.0, -5.0 / 12.0)
+    else:
+        raise ValueError("invalid time integration scheme")
+    return gamma[substep - 1] + xi[substep - 1]

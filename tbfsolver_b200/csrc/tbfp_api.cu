@@ -1,0 +1,749 @@
+// C ABI of the projection library: handle lifecycle, set-up tables and the
+// orchestration of the kernels in tbfp_kernels.cu.  See include/tbfp.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tbfp.h"
+#include "tbfp_kernels.cuh"
+
+using namespace tbfp;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct tbfp_handle {
+  int nx = 0, ny = 0, nz = 0, nkx = 0;
+  long R = 0;
+  int hd_psi = 1, hd_u = 2, hd_rho = 1, hd_st = 1;
+  Lay Lpsi{}, Lux{}, Luy{}, Luz{}, Lrho{}, Lst[3]{};
+  size_t n_psi = 0, n_ux = 0, n_uy = 0, n_uz = 0, n_rho = 0, n_st[3]{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  unsigned flags = 0;
+  int precision = TBFP_FP64;
+  double tol = 1e-10;
+  int max_iter = 8;
+
+  GridK g{};
+  FftPlan plx{}, plz{};
+  double s_Vg = 0.0, dx_fft = 0.0, dz_fft = 0.0, mean_c = 0.0, nxnz = 0.0, scale = 0.0;
+
+  // device tables
+  double *d_lamx = nullptr, *d_lamz = nullptr, *d_am = nullptr, *d_ap = nullptr, *d_dyf = nullptr;
+  double *d_idyf = nullptr, *d_idyc = nullptr, *d_idxf = nullptr, *d_idzf = nullptr;
+  double2 *d_twx = nullptr, *d_twz = nullptr;
+  // work
+  double2 *d_spec = nullptr;
+  double *d_irho = nullptr;
+  unsigned long long *d_maxdiv = nullptr;
+  // device copies used by the host-pointer entry points
+  double *h_ux = nullptr, *h_uy = nullptr, *h_uz = nullptr;
+  double *h_rho = nullptr, *h_pn = nullptr, *h_pnm1 = nullptr, *h_psi = nullptr, *h_s = nullptr;
+  double *h_st[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t evs[TBFP_NSTAGES + 1] = {};
+  size_t dev_bytes = 0;
+  std::vector<void *> allocs;
+  std::string err;
+};
+
+namespace {
+
+int set_err(tbfp_handle *h, int code, const std::string &msg) {
+  if (h) h->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+int cuda_err(tbfp_handle *h, cudaError_t e, const char *where) {
+  std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return set_err(h, TBFP_ENOMEM, m);
+  return set_err(h, TBFP_ECUDA, m);
+}
+
+#define TBFP_CK(h, call)                                  \
+  do {                                                    \
+    cudaError_t _e = (call);                              \
+    if (_e != cudaSuccess) return cuda_err((h), _e, #call); \
+  } while (0)
+
+template <typename T>
+int dev_alloc(tbfp_handle *h, T **p, size_t count) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, count * sizeof(T) > 0 ? count * sizeof(T) : 16);
+  if (e != cudaSuccess) return cuda_err(h, e, "cudaMalloc");
+  h->allocs.push_back(q);
+  h->dev_bytes += count * sizeof(T);
+  *p = static_cast<T *>(q);
+  return TBFP_OK;
+}
+
+template <typename T>
+int upload(tbfp_handle *h, T **p, const std::vector<T> &v) {
+  int rc = dev_alloc(h, p, v.size());
+  if (rc) return rc;
+  TBFP_CK(h, cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return TBFP_OK;
+}
+
+// Fortran array layout: interior lower bounds lo, halo hd.
+Lay make_lay(int ilo, int jlo, int klo, int ni, int nj, int hd, size_t *count, int nk) {
+  Lay L;
+  L.ilo = ilo - hd;
+  L.jlo = jlo - hd;
+  L.klo = klo - hd;
+  const long ei = ni + 2 * hd, ej = nj + 2 * hd, ek = nk + 2 * hd;
+  L.sj = ei;
+  L.sk = ei * ej;
+  *count = (size_t)(ei * ej * ek);
+  return L;
+}
+
+bool make_plan(int n, FftPlan *pl) {
+  std::memset(pl, 0, sizeof(*pl));
+  pl->n = n;
+  int m = n, k = 0;
+  while (m % 8 == 0 && m > 1 && k < 16) { pl->rad[k++] = 8; m /= 8; }
+  while (m % 4 == 0 && k < 16) { pl->rad[k++] = 4; m /= 4; }
+  while (m % 2 == 0 && k < 16) { pl->rad[k++] = 2; m /= 2; }
+  if (m % 3 == 0) { pl->rad[k++] = 3; m /= 3; }  // at most one factor 3, as the last pass
+  pl->nrad = k;
+  return m == 1;
+}
+
+// exp(-2*pi*i*m/n) for m = 0..n-1, evaluated in extended precision and rounded.
+std::vector<double2> twiddles(int n) {
+  std::vector<double2> t(n);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int m = 0; m < n; ++m) {
+    const long double a = 2.0L * pi * (long double)m / (long double)n;
+    t[m].x = (double)cosl(a);
+    t[m].y = (double)(-sinl(a));
+  }
+  return t;
+}
+
+int ensure_host_bufs(tbfp_handle *h, bool st) {
+  if (!h->h_ux) {
+    int rc;
+    if ((rc = dev_alloc(h, &h->h_ux, h->n_ux))) return rc;
+    if ((rc = dev_alloc(h, &h->h_uy, h->n_uy))) return rc;
+    if ((rc = dev_alloc(h, &h->h_uz, h->n_uz))) return rc;
+    if ((rc = dev_alloc(h, &h->h_rho, h->n_rho))) return rc;
+    if ((rc = dev_alloc(h, &h->h_pn, h->n_psi))) return rc;
+    if ((rc = dev_alloc(h, &h->h_pnm1, h->n_psi))) return rc;
+    if ((rc = dev_alloc(h, &h->h_psi, h->n_psi))) return rc;
+    if ((rc = dev_alloc(h, &h->h_s, h->n_psi))) return rc;
+  }
+  if (st && !h->h_st[0]) {
+    for (int c = 0; c < 6; ++c) {
+      int rc = dev_alloc(h, &h->h_st[c], h->n_st[c % 3]);
+      if (rc) return rc;
+    }
+  }
+  return TBFP_OK;
+}
+
+int h2d(tbfp_handle *h, double *dst, const double *src, size_t n) {
+  TBFP_CK(h, cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  return TBFP_OK;
+}
+int d2h(tbfp_handle *h, double *dst, const double *src, size_t n) {
+  TBFP_CK(h, cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return TBFP_OK;
+}
+
+int finish(tbfp_handle *h, const char *where) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(h, e, where);
+  if (!(h->flags & TBFP_FLAG_ASYNC)) {
+    e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_err(h, e, where);
+  }
+  return TBFP_OK;
+}
+
+bool st_present(const double *const *st_n, const double *const *st_nm1) {
+  return st_n != nullptr && st_nm1 != nullptr;
+}
+
+RhsArgs rhs_args(tbfp_handle *h, const double *ux, const double *uy, const double *uz, const double *psi_n,
+                 const double *psi_nm1, const double *const *st_n, const double *const *st_nm1, double dt,
+                 double alpha, double rho0) {
+  RhsArgs a{};
+  a.ux = ux;
+  a.uy = uy;
+  a.uz = uz;
+  a.irho = h->d_irho;
+  a.pn = psi_n;
+  a.pnm1 = psi_nm1;
+  for (int c = 0; c < 3; ++c) {
+    a.stn[c] = st_n ? st_n[c] : nullptr;
+    a.sto[c] = st_nm1 ? st_nm1[c] : nullptr;
+    a.Lst[c] = h->Lst[c];
+  }
+  a.Lux = h->Lux;
+  a.Luy = h->Luy;
+  a.Luz = h->Luz;
+  a.Lrho = h->Lrho;
+  a.Lpsi = h->Lpsi;
+  a.r = 1.0 / (alpha * dt);  // poissonEqn.f90:215
+  a.rho0 = rho0;
+  return a;
+}
+
+CorrArgs corr_args(tbfp_handle *h, const double *uxi, const double *uyi, const double *uzi, double *uxo,
+                   double *uyo, double *uzo, const double *psi, const double *psi_n, const double *psi_nm1,
+                   const double *const *st_n, const double *const *st_nm1, double dt, double alpha,
+                   double rho0) {
+  CorrArgs a{};
+  a.uxi = uxi;
+  a.uyi = uyi;
+  a.uzi = uzi;
+  a.uxo = uxo;
+  a.uyo = uyo;
+  a.uzo = uzo;
+  a.psi = psi;
+  a.pn = psi_n;
+  a.pnm1 = psi_nm1;
+  a.irho = h->d_irho;
+  for (int c = 0; c < 3; ++c) {
+    a.stn[c] = st_n ? st_n[c] : nullptr;
+    a.sto[c] = st_nm1 ? st_nm1[c] : nullptr;
+    a.Lst[c] = h->Lst[c];
+  }
+  a.Lux = h->Lux;
+  a.Luy = h->Luy;
+  a.Luz = h->Luz;
+  a.Lpsi = h->Lpsi;
+  a.Lrho = h->Lrho;
+  a.r = dt * alpha;  // momentumEqn.f90:1012
+  a.invrho0 = 1.0 / rho0;
+  return a;
+}
+
+// solveFPS body on device data: spectrum already holds the forward x transform.
+void fps_spectral_solve(tbfp_handle *h) {
+  launch_fftz(h->d_spec, h->g, h->plz, h->d_twz, false, h->stream);
+  launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, h->stream);
+  launch_fftz(h->d_spec, h->g, h->plz, h->d_twz, true, h->stream);
+}
+
+bool aliased(const void *a, const void *b) { return a == b; }
+
+int check_ptrs(tbfp_handle *h, std::initializer_list<const void *> ps) {
+  if (!h) return TBFP_ENULL;
+  for (const void *p : ps)
+    if (!p) return set_err(h, TBFP_ENULL, "a required array pointer is NULL");
+  return TBFP_OK;
+}
+
+int check_st(tbfp_handle *h, const double *const *st_n, const double *const *st_nm1) {
+  if ((st_n == nullptr) != (st_nm1 == nullptr))
+    return set_err(h, TBFP_EINVAL, "st_n and st_nm1 must both be given or both be NULL");
+  if (st_n)
+    for (int c = 0; c < 3; ++c)
+      if (!st_n[c] || !st_nm1[c]) return set_err(h, TBFP_ENULL, "a surface-tension component pointer is NULL");
+  return TBFP_OK;
+}
+
+int device_projection(tbfp_handle *h, const double *uxi, const double *uyi, const double *uzi, double *uxo,
+                      double *uyo, double *uzo, const double *rho, const double *psi_n, const double *psi_nm1,
+                      const double *const *st_n, const double *const *st_nm1, double dt, double alpha,
+                      double rho0, double *psi, tbfp_stats *stats) {
+  const bool st = st_present(st_n, st_nm1);
+  const bool timing = (h->flags & TBFP_FLAG_TIMING) != 0;
+  cudaStream_t s = h->stream;
+  auto mark = [&](int i) {
+    if (timing) cudaEventRecord(h->evs[i], s);
+  };
+  TBFP_CK(h, cudaEventRecord(h->ev0, s));
+  TBFP_CK(h, cudaMemsetAsync(h->d_maxdiv, 0, sizeof(unsigned long long), s));
+  mark(0);
+  launch_recip(rho, h->d_irho, (long)h->n_rho, s);
+  mark(1);
+  RhsArgs ra = rhs_args(h, uxi, uyi, uzi, psi_n, psi_nm1, st_n, st_nm1, dt, alpha, rho0);
+  launch_fftx_fwd_rhs(ra, st, h->g, h->plx, h->d_twx, h->d_spec, s);
+  mark(2);
+  launch_fftz(h->d_spec, h->g, h->plz, h->d_twz, false, s);
+  mark(3);
+  launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, s);
+  mark(4);
+  launch_fftz(h->d_spec, h->g, h->plz, h->d_twz, true, s);
+  mark(5);
+  launch_fftx_inv(h->d_spec, psi, h->Lpsi, h->hd_psi, h->g, h->plx, h->d_twx, h->scale, s);
+  mark(6);
+  CorrArgs ca = corr_args(h, uxi, uyi, uzi, uxo, uyo, uzo, psi, psi_n, psi_nm1, st_n, st_nm1, dt, alpha, rho0);
+  const bool inplace = aliased(uxi, uxo) || aliased(uyi, uyo) || aliased(uzi, uzo);
+  if (!inplace) {
+    launch_correct_div(ca, st, h->g, h->d_maxdiv, s);
+    mark(7);
+    mark(8);
+  } else {
+    launch_correct_inplace(ca, st, h->g, s);
+    mark(7);
+    launch_div(uxo, uyo, uzo, h->Lux, h->Luy, h->Luz, h->g, h->d_maxdiv, s);
+    mark(8);
+  }
+  TBFP_CK(h, cudaEventRecord(h->ev1, s));
+  if (stats) {
+    unsigned long long bits = 0;
+    TBFP_CK(h, cudaMemcpyAsync(&bits, h->d_maxdiv, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+    TBFP_CK(h, cudaStreamSynchronize(h->stream));
+    double md;
+    std::memcpy(&md, &bits, sizeof(md));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    stats->iterations = 1;
+    stats->rel_residual = -1.0;
+    stats->max_div = md;
+    stats->cont_err = md * dt;
+    stats->ms_device = ms;
+    for (int i = 0; i < TBFP_NSTAGES; ++i) {
+      float m = 0.f;
+      if (timing) cudaEventElapsedTime(&m, h->evs[i], h->evs[i + 1]);
+      stats->ms_stage[i] = m;
+    }
+  }
+  return finish(h, "tbfp_projection");
+}
+
+}  // namespace
+
+extern "C" {
+
+int tbfp_abi_version(void) { return TBFP_ABI_VERSION; }
+
+const char *tbfp_strerror(int status) {
+  switch (status) {
+    case TBFP_OK: return "success";
+    case TBFP_ENOTCONVERGED: return "iteration cap reached before the tolerance (results valid)";
+    case TBFP_EINVAL: return "invalid descriptor or argument";
+    case TBFP_ENULL: return "a required pointer is NULL";
+    case TBFP_ECUDA: return "CUDA runtime error";
+    case TBFP_ENOMEM: return "device memory allocation failed";
+    case TBFP_EUNSUPPORTED: return "size or feature not supported";
+    case TBFP_ENODEVICE: return "no usable CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char *tbfp_last_error(const tbfp_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+size_t tbfp_device_bytes(const tbfp_handle *h) { return h ? h->dev_bytes : 0; }
+
+int tbfp_destroy(tbfp_handle *h) {
+  if (!h) return TBFP_OK;
+  int dev_prev = 0;
+  cudaGetDevice(&dev_prev);
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (void *p : h->allocs) cudaFree(p);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  for (cudaEvent_t e : h->evs)
+    if (e) cudaEventDestroy(e);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  cudaSetDevice(dev_prev);
+  delete h;
+  return TBFP_OK;
+}
+
+int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
+  g_create_error.clear();
+  if (!d || !out) return set_err(nullptr, TBFP_ENULL, "tbfp_create: NULL descriptor or output");
+  *out = nullptr;
+  if (d->nx < 4 || d->ny < 4 || d->nz < 2 || (d->nx % 2) != 0)
+    return set_err(nullptr, TBFP_EINVAL, "tbfp_create: need nx even >= 4, ny >= 4, nz >= 2");
+  if (d->hd_psi < 1 || d->hd_rho < 1 || d->hd_u < 0 || d->hd_st < 0)
+    return set_err(nullptr, TBFP_EINVAL, "tbfp_create: halo widths must be hd_psi>=1, hd_rho>=1, hd_u>=0, hd_st>=0");
+  if (!d->dxf || !d->dxc || !d->dyf || !d->dyc || !d->dzf || !d->dzc)
+    return set_err(nullptr, TBFP_ENULL, "tbfp_create: a grid metric array is NULL");
+  if (!(d->dx_fft > 0.0) || !(d->dz_fft > 0.0))
+    return set_err(nullptr, TBFP_EINVAL, "tbfp_create: dx_fft and dz_fft must be positive");
+  if (d->precision != TBFP_FP64 && d->precision != TBFP_MIXED)
+    return set_err(nullptr, TBFP_EINVAL, "tbfp_create: unknown precision mode");
+  if (d->precision == TBFP_MIXED)
+    return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_create: TBFP_MIXED is not available in this build");
+  for (int i = 0; i < d->nx; ++i)
+    if (!(d->dxf[i] > 0.0)) return set_err(nullptr, TBFP_EINVAL, "tbfp_create: dxf must be positive");
+  for (int j = 0; j < d->ny; ++j)
+    if (!(d->dyf[j] > 0.0)) return set_err(nullptr, TBFP_EINVAL, "tbfp_create: dyf must be positive");
+  for (int j = 0; j <= d->ny; ++j)
+    if (!(d->dyc[j] > 0.0)) return set_err(nullptr, TBFP_EINVAL, "tbfp_create: dyc must be positive");
+  for (int k = 0; k < d->nz; ++k)
+    if (!(d->dzf[k] > 0.0)) return set_err(nullptr, TBFP_EINVAL, "tbfp_create: dzf must be positive");
+  if (!(d->dxc[0] > 0.0) || !(d->dzc[0] > 0.0))
+    return set_err(nullptr, TBFP_EINVAL, "tbfp_create: dxc(1), dzc(1) must be positive");
+
+  FftPlan plx, plz;
+  if (!make_plan(d->nx / 2, &plx) || !make_plan(d->nz, &plz))
+    return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_create: nx/2 and nz must be 2^a or 3*2^a");
+  if (d->nx / 2 > fft_max_length() || d->nz > fft_max_length())
+    return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_create: nx/2 and nz must not exceed the transform tile length");
+  if (fftx_smem_bytes(d->nx / 2) > 227 * 1024 || fftz_smem_bytes(d->nz) > 227 * 1024 ||
+      tridiag_smem_bytes(d->ny) > 227 * 1024)
+    return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_create: grid too large for the shared-memory tiles");
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_err(nullptr, TBFP_ENODEVICE, "tbfp_create: no CUDA device");
+
+  tbfp_handle *h = new tbfp_handle();
+  h->nx = d->nx;
+  h->ny = d->ny;
+  h->nz = d->nz;
+  h->nkx = d->nx / 2 + 1;
+  h->R = (long)d->ny * d->nz;
+  h->hd_psi = d->hd_psi;
+  h->hd_u = d->hd_u;
+  h->hd_rho = d->hd_rho;
+  h->hd_st = d->hd_st;
+  h->flags = d->flags;
+  h->precision = d->precision;
+  h->tol = d->tol;
+  h->max_iter = d->max_iter;
+  h->plx = plx;
+  h->plz = plz;
+  if (d->device >= 0) h->device = d->device;
+  else cudaGetDevice(&h->device);
+  int dev_prev = 0;
+  cudaGetDevice(&dev_prev);
+  if (cudaSetDevice(h->device) != cudaSuccess) {
+    delete h;
+    return set_err(nullptr, TBFP_ENODEVICE, "tbfp_create: cannot select the CUDA device");
+  }
+  const int nx = h->nx, ny = h->ny, nz = h->nz;
+  h->Lpsi = make_lay(1, 1, 1, nx, ny, h->hd_psi, &h->n_psi, nz);
+  h->Lrho = make_lay(1, 1, 1, nx, ny, h->hd_rho, &h->n_rho, nz);
+  h->Lux = make_lay(0, 1, 1, nx + 1, ny, h->hd_u, &h->n_ux, nz);
+  h->Luy = make_lay(1, 0, 1, nx, ny + 1, h->hd_u, &h->n_uy, nz);
+  h->Luz = make_lay(1, 1, 0, nx, ny, h->hd_u, &h->n_uz, nz + 1);
+  h->Lst[0] = make_lay(0, 1, 1, nx + 1, ny, h->hd_st, &h->n_st[0], nz);
+  h->Lst[1] = make_lay(1, 0, 1, nx, ny + 1, h->hd_st, &h->n_st[1], nz);
+  h->Lst[2] = make_lay(1, 1, 0, nx, ny, h->hd_st, &h->n_st[2], nz + 1);
+
+  int rc = TBFP_OK;
+  auto fail = [&](int code) {
+    std::string m = h->err;
+    tbfp_destroy(h);
+    cudaSetDevice(dev_prev);
+    return set_err(nullptr, code, m);
+  };
+  cudaError_t ce = prepare_kernels();
+  if (ce != cudaSuccess) {
+    cuda_err(h, ce, "cudaFuncSetAttribute");
+    return fail(TBFP_ECUDA);
+  }
+  if (d->stream) {
+    h->stream = static_cast<cudaStream_t>(d->stream);
+  } else {
+    if ((ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+      cuda_err(h, ce, "cudaStreamCreate");
+      return fail(TBFP_ECUDA);
+    }
+    h->own_stream = true;
+  }
+  if ((ce = cudaEventCreate(&h->ev0)) != cudaSuccess || (ce = cudaEventCreate(&h->ev1)) != cudaSuccess) {
+    cuda_err(h, ce, "cudaEventCreate");
+    return fail(TBFP_ECUDA);
+  }
+  if (h->flags & TBFP_FLAG_TIMING) {
+    for (cudaEvent_t &e : h->evs) {
+      if ((ce = cudaEventCreate(&e)) != cudaSuccess) {
+        cuda_err(h, ce, "cudaEventCreate");
+        return fail(TBFP_ECUDA);
+      }
+    }
+  }
+
+  // --- tables: computeEigenvalues (fastPoissonSolver.f90:215-251) and
+  //     initOffDiagMatrix (:255-276); reciprocal metrics for the stencils.
+  const double pi = 3.14159265358979323846;
+  h->dx_fft = d->dx_fft;
+  h->dz_fft = d->dz_fft;
+  std::vector<double> lamx(h->nkx), lamz(nz), am(ny), ap(ny), dyf(ny), idyf(ny), idyc(ny + 1), idxf(nx), idzf(nz);
+  for (int i = 0; i < h->nkx; ++i)
+    lamx[i] = 2.0 * (std::cos(((double)i * 2.0 * pi) / nx) - 1.0) / (d->dx_fft * d->dx_fft);
+  for (int k = 0; k < nz; ++k)
+    lamz[k] = 2.0 * (std::cos(((double)k * 2.0 * pi) / nz) - 1.0) / (d->dz_fft * d->dz_fft);
+  for (int j = 0; j < ny; ++j) {
+    am[j] = 1.0 / (d->dyc[j] * d->dyf[j]);
+    ap[j] = 1.0 / (d->dyc[j + 1] * d->dyf[j]);
+    dyf[j] = d->dyf[j];
+    idyf[j] = 1.0 / d->dyf[j];
+  }
+  am[0] = 0.0;
+  ap[ny - 1] = 0.0;
+  for (int j = 0; j <= ny; ++j) idyc[j] = 1.0 / d->dyc[j];
+  for (int i = 0; i < nx; ++i) idxf[i] = 1.0 / d->dxf[i];
+  for (int k = 0; k < nz; ++k) idzf[k] = 1.0 / d->dzf[k];
+  double sVg = d->s_Vg;
+  if (!(sVg > 0.0)) {  // totalVolume (grid.f90:933-951), loop order k, j, i
+    sVg = 0.0;
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) sVg += d->dxf[i] * d->dyf[j] * d->dzf[k];
+  }
+  h->s_Vg = sVg;
+  h->mean_c = d->dx_fft * d->dz_fft / sVg;
+  h->nxnz = (double)nx * (double)nz;
+  h->scale = 1.0 / ((double)nx * (double)nz);
+
+  if ((rc = upload(h, &h->d_lamx, lamx)) || (rc = upload(h, &h->d_lamz, lamz)) || (rc = upload(h, &h->d_am, am)) ||
+      (rc = upload(h, &h->d_ap, ap)) || (rc = upload(h, &h->d_dyf, dyf)) || (rc = upload(h, &h->d_idyf, idyf)) ||
+      (rc = upload(h, &h->d_idyc, idyc)) || (rc = upload(h, &h->d_idxf, idxf)) || (rc = upload(h, &h->d_idzf, idzf)) ||
+      (rc = upload(h, &h->d_twx, twiddles(nx))) || (rc = upload(h, &h->d_twz, twiddles(nz))))
+    return fail(rc);
+  if ((rc = dev_alloc(h, &h->d_spec, (size_t)h->nkx * h->R)) || (rc = dev_alloc(h, &h->d_irho, h->n_rho)) ||
+      (rc = dev_alloc(h, &h->d_maxdiv, 1)))
+    return fail(rc);
+
+  GridK &g = h->g;
+  g.nx = nx;
+  g.ny = ny;
+  g.nz = nz;
+  g.nkx = h->nkx;
+  g.M = nx / 2;
+  g.R = h->R;
+  g.idxf1 = 1.0 / d->dxf[0];
+  g.idzf1 = 1.0 / d->dzf[0];
+  g.idxc1 = 1.0 / d->dxc[0];
+  g.idzc1 = 1.0 / d->dzc[0];
+  g.idyf = h->d_idyf;
+  g.idyc = h->d_idyc;
+  g.idxf = h->d_idxf;
+  g.idzf = h->d_idzf;
+  cudaSetDevice(dev_prev);
+  *out = h;
+  return TBFP_OK;
+}
+
+// ---------------------------------------------------------------------------
+int tbfp_solve_fps_dev(tbfp_handle *h, const double *s, double *psi) {
+  int rc = check_ptrs(h, {s, psi});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  launch_fftx_fwd_from_s(s, h->Lpsi, h->g, h->plx, h->d_twx, h->d_spec, h->stream);
+  fps_spectral_solve(h);
+  launch_fftx_inv(h->d_spec, psi, h->Lpsi, h->hd_psi, h->g, h->plx, h->d_twx, h->scale, h->stream);
+  return finish(h, "tbfp_solve_fps");
+}
+
+int tbfp_solve_fps(tbfp_handle *h, const double *s, double *psi) {
+  int rc = check_ptrs(h, {s, psi});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  if ((rc = ensure_host_bufs(h, false))) return rc;
+  if ((rc = h2d(h, h->h_s, s, h->n_psi))) return rc;
+  // keep the caller's untouched entries (deep y ghost layers) as they are
+  if (h->hd_psi > 1 && (rc = h2d(h, h->h_psi, psi, h->n_psi))) return rc;
+  const unsigned fl = h->flags;
+  h->flags |= TBFP_FLAG_ASYNC;
+  rc = tbfp_solve_fps_dev(h, h->h_s, h->h_psi);
+  h->flags = fl;
+  if (rc) return rc;
+  if ((rc = d2h(h, psi, h->h_psi, h->n_psi))) return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return TBFP_OK;
+}
+
+int tbfp_rhs_split_dev(tbfp_handle *h, const double *ux, const double *uy, const double *uz, const double *rho,
+                       const double *psi_n, const double *psi_nm1, const double *const *st_n,
+                       const double *const *st_nm1, double dt, double alpha, double rho0, double *s) {
+  int rc = check_ptrs(h, {ux, uy, uz, rho, psi_n, psi_nm1, s});
+  if (rc) return rc;
+  if ((rc = check_st(h, st_n, st_nm1))) return rc;
+  if (!(dt > 0.0) || !(alpha > 0.0) || !(rho0 > 0.0))
+    return set_err(h, TBFP_EINVAL, "tbfp_rhs_split: dt, alpha and rho0 must be positive");
+  cudaSetDevice(h->device);
+  launch_recip(rho, h->d_irho, (long)h->n_rho, h->stream);
+  RhsArgs ra = rhs_args(h, ux, uy, uz, psi_n, psi_nm1, st_n, st_nm1, dt, alpha, rho0);
+  launch_rhs(ra, st_present(st_n, st_nm1), h->g, s, h->Lpsi, h->stream);
+  return finish(h, "tbfp_rhs_split");
+}
+
+int tbfp_rhs_split(tbfp_handle *h, const double *ux, const double *uy, const double *uz, const double *rho,
+                   const double *psi_n, const double *psi_nm1, const double *const *st_n,
+                   const double *const *st_nm1, double dt, double alpha, double rho0, double *s) {
+  int rc = check_ptrs(h, {ux, uy, uz, rho, psi_n, psi_nm1, s});
+  if (rc) return rc;
+  if ((rc = check_st(h, st_n, st_nm1))) return rc;
+  cudaSetDevice(h->device);
+  const bool st = st_present(st_n, st_nm1);
+  if ((rc = ensure_host_bufs(h, st))) return rc;
+  if ((rc = h2d(h, h->h_ux, ux, h->n_ux)) || (rc = h2d(h, h->h_uy, uy, h->n_uy)) ||
+      (rc = h2d(h, h->h_uz, uz, h->n_uz)) || (rc = h2d(h, h->h_rho, rho, h->n_rho)) ||
+      (rc = h2d(h, h->h_pn, psi_n, h->n_psi)) || (rc = h2d(h, h->h_pnm1, psi_nm1, h->n_psi)) ||
+      (rc = h2d(h, h->h_s, s, h->n_psi)))
+    return rc;
+  const double *dn[3] = {nullptr, nullptr, nullptr}, *do_[3] = {nullptr, nullptr, nullptr};
+  if (st) {
+    for (int c = 0; c < 3; ++c) {
+      if ((rc = h2d(h, h->h_st[c], st_n[c], h->n_st[c])) || (rc = h2d(h, h->h_st[3 + c], st_nm1[c], h->n_st[c])))
+        return rc;
+      dn[c] = h->h_st[c];
+      do_[c] = h->h_st[3 + c];
+    }
+  }
+  const unsigned fl = h->flags;
+  h->flags |= TBFP_FLAG_ASYNC;
+  rc = tbfp_rhs_split_dev(h, h->h_ux, h->h_uy, h->h_uz, h->h_rho, h->h_pn, h->h_pnm1, st ? dn : nullptr,
+                          st ? do_ : nullptr, dt, alpha, rho0, h->h_s);
+  h->flags = fl;
+  if (rc) return rc;
+  if ((rc = d2h(h, s, h->h_s, h->n_psi))) return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return TBFP_OK;
+}
+
+int tbfp_correct_dev(tbfp_handle *h, double *ux, double *uy, double *uz, const double *psi, const double *psi_n,
+                     const double *psi_nm1, const double *rho, const double *const *st_n,
+                     const double *const *st_nm1, double dt, double alpha, double rho0) {
+  int rc = check_ptrs(h, {ux, uy, uz, psi, psi_n, psi_nm1, rho});
+  if (rc) return rc;
+  if ((rc = check_st(h, st_n, st_nm1))) return rc;
+  if (!(dt > 0.0) || !(alpha > 0.0) || !(rho0 > 0.0))
+    return set_err(h, TBFP_EINVAL, "tbfp_correct: dt, alpha and rho0 must be positive");
+  cudaSetDevice(h->device);
+  launch_recip(rho, h->d_irho, (long)h->n_rho, h->stream);
+  CorrArgs ca = corr_args(h, ux, uy, uz, ux, uy, uz, psi, psi_n, psi_nm1, st_n, st_nm1, dt, alpha, rho0);
+  launch_correct_inplace(ca, st_present(st_n, st_nm1), h->g, h->stream);
+  return finish(h, "tbfp_correct");
+}
+
+int tbfp_correct(tbfp_handle *h, double *ux, double *uy, double *uz, const double *psi, const double *psi_n,
+                 const double *psi_nm1, const double *rho, const double *const *st_n, const double *const *st_nm1,
+                 double dt, double alpha, double rho0) {
+  int rc = check_ptrs(h, {ux, uy, uz, psi, psi_n, psi_nm1, rho});
+  if (rc) return rc;
+  if ((rc = check_st(h, st_n, st_nm1))) return rc;
+  cudaSetDevice(h->device);
+  const bool st = st_present(st_n, st_nm1);
+  if ((rc = ensure_host_bufs(h, st))) return rc;
+  if ((rc = h2d(h, h->h_ux, ux, h->n_ux)) || (rc = h2d(h, h->h_uy, uy, h->n_uy)) ||
+      (rc = h2d(h, h->h_uz, uz, h->n_uz)) || (rc = h2d(h, h->h_rho, rho, h->n_rho)) ||
+      (rc = h2d(h, h->h_psi, psi, h->n_psi)) || (rc = h2d(h, h->h_pn, psi_n, h->n_psi)) ||
+      (rc = h2d(h, h->h_pnm1, psi_nm1, h->n_psi)))
+    return rc;
+  const double *dn[3] = {nullptr, nullptr, nullptr}, *do_[3] = {nullptr, nullptr, nullptr};
+  if (st) {
+    for (int c = 0; c < 3; ++c) {
+      if ((rc = h2d(h, h->h_st[c], st_n[c], h->n_st[c])) || (rc = h2d(h, h->h_st[3 + c], st_nm1[c], h->n_st[c])))
+        return rc;
+      dn[c] = h->h_st[c];
+      do_[c] = h->h_st[3 + c];
+    }
+  }
+  const unsigned fl = h->flags;
+  h->flags |= TBFP_FLAG_ASYNC;
+  rc = tbfp_correct_dev(h, h->h_ux, h->h_uy, h->h_uz, h->h_psi, h->h_pn, h->h_pnm1, h->h_rho, st ? dn : nullptr,
+                        st ? do_ : nullptr, dt, alpha, rho0);
+  h->flags = fl;
+  if (rc) return rc;
+  if ((rc = d2h(h, ux, h->h_ux, h->n_ux)) || (rc = d2h(h, uy, h->h_uy, h->n_uy)) || (rc = d2h(h, uz, h->h_uz, h->n_uz)))
+    return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return TBFP_OK;
+}
+
+int tbfp_continuity_error_dev(tbfp_handle *h, const double *ux, const double *uy, const double *uz, double dt,
+                              double *max_div, double *cont_err) {
+  int rc = check_ptrs(h, {ux, uy, uz});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  TBFP_CK(h, cudaMemsetAsync(h->d_maxdiv, 0, sizeof(unsigned long long), h->stream));
+  launch_div(ux, uy, uz, h->Lux, h->Luy, h->Luz, h->g, h->d_maxdiv, h->stream);
+  unsigned long long bits = 0;
+  TBFP_CK(h, cudaMemcpyAsync(&bits, h->d_maxdiv, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(h, e, "tbfp_continuity_error");
+  double md;
+  std::memcpy(&md, &bits, sizeof(md));
+  if (max_div) *max_div = md;
+  if (cont_err) *cont_err = md * dt;  // auxiliaryRoutines.f90:82
+  return TBFP_OK;
+}
+
+int tbfp_continuity_error(tbfp_handle *h, const double *ux, const double *uy, const double *uz, double dt,
+                          double *max_div, double *cont_err) {
+  int rc = check_ptrs(h, {ux, uy, uz});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  if ((rc = ensure_host_bufs(h, false))) return rc;
+  if ((rc = h2d(h, h->h_ux, ux, h->n_ux)) || (rc = h2d(h, h->h_uy, uy, h->n_uy)) || (rc = h2d(h, h->h_uz, uz, h->n_uz)))
+    return rc;
+  return tbfp_continuity_error_dev(h, h->h_ux, h->h_uy, h->h_uz, dt, max_div, cont_err);
+}
+
+int tbfp_projection_dev(tbfp_handle *h, const double *ux_in, const double *uy_in, const double *uz_in,
+                        double *ux_out, double *uy_out, double *uz_out, const double *rho, const double *psi_n,
+                        const double *psi_nm1, const double *const *st_n, const double *const *st_nm1, double dt,
+                        double alpha, double rho0, double *psi, tbfp_stats *stats) {
+  int rc = check_ptrs(h, {ux_in, uy_in, uz_in, ux_out, uy_out, uz_out, rho, psi_n, psi_nm1, psi});
+  if (rc) return rc;
+  if ((rc = check_st(h, st_n, st_nm1))) return rc;
+  if (!(dt > 0.0) || !(alpha > 0.0) || !(rho0 > 0.0))
+    return set_err(h, TBFP_EINVAL, "tbfp_projection: dt, alpha and rho0 must be positive");
+  cudaSetDevice(h->device);
+  return device_projection(h, ux_in, uy_in, uz_in, ux_out, uy_out, uz_out, rho, psi_n, psi_nm1, st_n, st_nm1, dt,
+                           alpha, rho0, psi, stats);
+}
+
+int tbfp_projection(tbfp_handle *h, double *ux, double *uy, double *uz, const double *rho, const double *psi_n,
+                    const double *psi_nm1, const double *const *st_n, const double *const *st_nm1, double dt,
+                    double alpha, double rho0, double *psi, tbfp_stats *stats) {
+  int rc = check_ptrs(h, {ux, uy, uz, rho, psi_n, psi_nm1, psi});
+  if (rc) return rc;
+  if ((rc = check_st(h, st_n, st_nm1))) return rc;
+  if (!(dt > 0.0) || !(alpha > 0.0) || !(rho0 > 0.0))
+    return set_err(h, TBFP_EINVAL, "tbfp_projection: dt, alpha and rho0 must be positive");
+  cudaSetDevice(h->device);
+  const bool st = st_present(st_n, st_nm1);
+  if ((rc = ensure_host_bufs(h, st))) return rc;
+  // u is corrected in place in the device copy, so the caller's halos come back
+  // unchanged.  With hd_psi == 1 every entry of psi (interior and ghosts) is
+  // written; deeper halos are preserved by uploading psi first.
+  if ((rc = h2d(h, h->h_ux, ux, h->n_ux)) || (rc = h2d(h, h->h_uy, uy, h->n_uy)) ||
+      (rc = h2d(h, h->h_uz, uz, h->n_uz)) || (rc = h2d(h, h->h_rho, rho, h->n_rho)) ||
+      (rc = h2d(h, h->h_pn, psi_n, h->n_psi)) || (rc = h2d(h, h->h_pnm1, psi_nm1, h->n_psi)))
+    return rc;
+  if (h->hd_psi > 1 && (rc = h2d(h, h->h_psi, psi, h->n_psi))) return rc;
+  const double *dn[3] = {nullptr, nullptr, nullptr}, *do_[3] = {nullptr, nullptr, nullptr};
+  if (st) {
+    for (int c = 0; c < 3; ++c) {
+      if ((rc = h2d(h, h->h_st[c], st_n[c], h->n_st[c])) || (rc = h2d(h, h->h_st[3 + c], st_nm1[c], h->n_st[c])))
+        return rc;
+      dn[c] = h->h_st[c];
+      do_[c] = h->h_st[3 + c];
+    }
+  }
+  const unsigned fl = h->flags;
+  h->flags |= TBFP_FLAG_ASYNC;
+  rc = device_projection(h, h->h_ux, h->h_uy, h->h_uz, h->h_ux, h->h_uy, h->h_uz, h->h_rho, h->h_pn, h->h_pnm1,
+                         st ? dn : nullptr, st ? do_ : nullptr, dt, alpha, rho0, h->h_psi, stats);
+  h->flags = fl;
+  if (rc) return rc;
+  if ((rc = d2h(h, ux, h->h_ux, h->n_ux)) || (rc = d2h(h, uy, h->h_uy, h->n_uy)) ||
+      (rc = d2h(h, uz, h->h_uz, h->n_uz)) || (rc = d2h(h, psi, h->h_psi, h->n_psi)))
+    return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return TBFP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,644 @@
+// FP64 kernels of the split-pressure projection (FAST_MODE of the reference).
+//
+// Spectrum layout in HBM: S[kx][row], row = (k-1)*ny + (j-1), kx = 0..nx/2.
+// For a fixed kx the x rows are contiguous, so
+//   * the x transforms (one CTA per tile of consecutive rows) write/read
+//     contiguous runs of the tile's rows for every kx,
+//   * the z transform of a fixed (kx, j) column strides by ny (a CTA stages a
+//     tile of consecutive j columns for all k in shared memory),
+//   * the y system of a fixed (kx, kz) is the contiguous run S[kx][kz*ny ...].
+// This replaces the six pencil transposes of pencilDec.f90:359-562.
+#include <cuda_runtime.h>
+
+#include "tbfp_kernels.cuh"
+
+namespace tbfp {
+
+constexpr int kNT = 256;    // threads per CTA of the transform kernels
+constexpr int kEMAX = 8;    // complex elements per thread in the transform kernels
+constexpr int kWPB = 4;     // warps per CTA of the tridiagonal kernel
+
+static int pow2_floor(int v) {
+  int p = 1;
+  while (2 * p <= v) p *= 2;
+  return p;
+}
+// Longest transform one CTA holds (all of it must fit the register budget).
+int fft_max_length() { return kEMAX * kNT; }
+// Rows (x) or columns (z) per CTA: the largest power of two keeping
+// n*rows <= kEMAX*kNT complex elements in the tile.
+int fftx_rows_per_cta(int M) { return (kEMAX * kNT) / M > 0 ? pow2_floor((kEMAX * kNT) / M) : 1; }
+int fftz_cols_per_cta(int nz) { return (kEMAX * kNT) / nz > 0 ? pow2_floor((kEMAX * kNT) / nz) : 1; }
+size_t fftx_smem_bytes(int M) { return (size_t)fftx_rows_per_cta(M) * (M + 1) * sizeof(double2); }
+size_t fftz_smem_bytes(int nz) { return (size_t)fftz_cols_per_cta(nz) * nz * sizeof(double2); }
+size_t tridiag_smem_bytes(int ny) { return (size_t)kWPB * ny * (sizeof(double2) + 2 * sizeof(double)); }
+
+// ---------------------------------------------------------------------------
+// 1/rho over the whole (halo-inclusive) density array.
+// ---------------------------------------------------------------------------
+__global__ void k_recip(const double *__restrict__ rho, double *__restrict__ irho, long n) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
+    irho[t] = 1.0 / rho[t];
+}
+
+void launch_recip(const double *rho, double *irho, long n, cudaStream_t st) {
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_recip<<<blocks, 256, 0, st>>>(rho, irho, n);
+}
+
+// ---------------------------------------------------------------------------
+// Split right-hand side at one cell: computeSource (poissonEqn.f90:224-253) with
+// computeOldPressDiv (:270-301), nl = 2.  Divisions by metrics are products with
+// host-computed reciprocals; 1/rho comes from the precomputed array.
+// ---------------------------------------------------------------------------
+template <bool ST>
+__device__ __forceinline__ double rhs_cell(const RhsArgs &a, const GridK &g, int i, int j, int k) {
+  const double ddx = (a.ux[at(a.Lux, i, j, k)] - a.ux[at(a.Lux, i - 1, j, k)]) * g.idxf1;
+  const double ddy = (a.uy[at(a.Luy, i, j, k)] - a.uy[at(a.Luy, i, j - 1, k)]) * g.idyf[j - 1];
+  const double ddz = (a.uz[at(a.Luz, i, j, k)] - a.uz[at(a.Luz, i, j, k - 1)]) * g.idzf1;
+  double s = ((ddx + ddy) + ddz) * a.r * a.rho0;
+
+  const long c = at(a.Lrho, i, j, k);
+  const double irc = a.irho[c];
+  const double h = a.rho0 * 0.5;
+  const double apx = 1.0 - h * (a.irho[c + 1] + irc);
+  const double amx = 1.0 - h * (a.irho[c - 1] + irc);
+  const double apy = 1.0 - h * (a.irho[c + a.Lrho.sj] + irc);
+  const double amy = 1.0 - h * (a.irho[c - a.Lrho.sj] + irc);
+  const double apz = 1.0 - h * (a.irho[c + a.Lrho.sk] + irc);
+  const double amz = 1.0 - h * (a.irho[c - a.Lrho.sk] + irc);
+
+  const long p = at(a.Lpsi, i, j, k);
+  const long sj = a.Lpsi.sj, sk = a.Lpsi.sk;
+  const double pc = a.pn[p], oc = a.pnm1[p];
+  double dpxp = (2.0 * (a.pn[p + 1] - pc) - (a.pnm1[p + 1] - oc)) * g.idxc1;
+  double dpxm = (2.0 * (pc - a.pn[p - 1]) - (oc - a.pnm1[p - 1])) * g.idxc1;
+  double dpyp = (2.0 * (a.pn[p + sj] - pc) - (a.pnm1[p + sj] - oc)) * g.idyc[j];
+  double dpym = (2.0 * (pc - a.pn[p - sj]) - (oc - a.pnm1[p - sj])) * g.idyc[j - 1];
+  double dpzp = (2.0 * (a.pn[p + sk] - pc) - (a.pnm1[p + sk] - oc)) * g.idzc1;
+  double dpzm = (2.0 * (pc - a.pn[p - sk]) - (oc - a.pnm1[p - sk])) * g.idzc1;
+  if constexpr (ST) {
+    const long x0 = at(a.Lst[0], i, j, k), y0 = at(a.Lst[1], i, j, k), z0 = at(a.Lst[2], i, j, k);
+    dpxp = dpxp - 2.0 * a.stn[0][x0] + a.sto[0][x0];
+    dpxm = dpxm - 2.0 * a.stn[0][x0 - 1] + a.sto[0][x0 - 1];
+    dpyp = dpyp - 2.0 * a.stn[1][y0] + a.sto[1][y0];
+    dpym = dpym - 2.0 * a.stn[1][y0 - a.Lst[1].sj] + a.sto[1][y0 - a.Lst[1].sj];
+    dpzp = dpzp - 2.0 * a.stn[2][z0] + a.sto[2][z0];
+    dpzm = dpzm - 2.0 * a.stn[2][z0 - a.Lst[2].sk] + a.sto[2][z0 - a.Lst[2].sk];
+  }
+  s = s + (apx * dpxp - amx * dpxm) * g.idxf1;
+  s = s + (apy * dpyp - amy * dpym) * g.idyf[j - 1];
+  s = s + (apz * dpzp - amz * dpzm) * g.idzf1;
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// Forward x transform of a tile of rows: real rows (from s, or computed by the
+// split RHS) -> half-length complex FFT -> r2c post-processing -> S[kx][row].
+// ---------------------------------------------------------------------------
+template <int MODE, bool ST>
+__global__ void __launch_bounds__(kNT, 2) k_fftx_fwd(const double *__restrict__ s_in, Lay Ls, RhsArgs ra, GridK g,
+                                                  FftPlan pl, const double2 *__restrict__ twx,
+                                                  double2 *__restrict__ spec, int TJ) {
+  extern __shared__ double2 sm[];
+  const int M = g.M, nx = g.nx, ld = M + 1;
+  const long r0 = (long)blockIdx.x * TJ;
+  const int nrows = (int)min((long)TJ, g.R - r0);
+  double *smr = reinterpret_cast<double *>(sm);
+
+  for (int t = threadIdx.x; t < TJ * nx; t += blockDim.x) {
+    const int row = t / nx, ii = t - row * nx;
+    double v = 0.0;
+    if (row < nrows) {
+      const long rr = r0 + row;
+      const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
+      if constexpr (MODE == 0) v = s_in[at(Ls, ii + 1, j, k)];
+      else v = rhs_cell<ST>(ra, g, ii + 1, j, k);
+    }
+    smr[(long)row * 2 * ld + ii] = v;
+  }
+  __syncthreads();
+  fft_smem<double2, kEMAX, false>(sm, pl, __ffs(TJ) - 1, 1, ld, twx, 2);
+
+  // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx)
+  const int npair = M / 2 + 1;
+  for (int t = threadIdx.x; t < TJ * npair; t += blockDim.x) {
+    const int row = t / npair, kk = t - row * npair;
+    double2 *Z = sm + (long)row * ld;
+    if (kk == 0) {
+      const double2 z0 = Z[0];
+      Z[0] = mk<double2>(z0.x + z0.y, 0.0);
+      Z[M] = mk<double2>(z0.x - z0.y, 0.0);
+    } else {
+      const int km = M - kk;
+      const double2 a = Z[kk], b = Z[km];
+      const double2 wa = twx[kk], wb = twx[km];
+      // for index kk
+      double2 ep = mk<double2>(a.x + b.x, a.y - b.y);   // Z_k + conj Z_{M-k}
+      double2 em = mk<double2>(a.x - b.x, a.y + b.y);   // Z_k - conj Z_{M-k}
+      double2 t1 = cmul(wa, em);                         // W^k * em
+      Z[kk] = mk<double2>(0.5 * (ep.x + t1.y), 0.5 * (ep.y - t1.x));  // (ep - i t1)/2
+      if (km != kk) {
+        double2 fp = mk<double2>(b.x + a.x, b.y - a.y);
+        double2 fm = mk<double2>(b.x - a.x, b.y + a.y);
+        double2 t2 = cmul(wb, fm);
+        Z[km] = mk<double2>(0.5 * (fp.x + t2.y), 0.5 * (fp.y - t2.x));
+      }
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < TJ * ld; t += blockDim.x) {
+    const int kx = t / TJ, row = t - kx * TJ;
+    if (row < nrows) spec[(long)kx * g.R + r0 + row] = sm[(long)row * ld + kx];
+  }
+}
+
+void launch_fftx_fwd_from_s(const double *s, Lay Ls, const GridK &g, const FftPlan &pl, const double2 *twx,
+                            double2 *spec, cudaStream_t st) {
+  const int TJ = fftx_rows_per_cta(g.M);
+  const long nblk = (g.R + TJ - 1) / TJ;
+  RhsArgs ra{};
+  k_fftx_fwd<0, false><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(s, Ls, ra, g, pl, twx, spec, TJ);
+}
+
+void launch_fftx_fwd_rhs(const RhsArgs &ra, bool has_st, const GridK &g, const FftPlan &pl, const double2 *twx,
+                         double2 *spec, cudaStream_t st) {
+  const int TJ = fftx_rows_per_cta(g.M);
+  const long nblk = (g.R + TJ - 1) / TJ;
+  Lay Ls{};
+  if (has_st)
+    k_fftx_fwd<1, true><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(nullptr, Ls, ra, g, pl, twx, spec, TJ);
+  else
+    k_fftx_fwd<1, false><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(nullptr, Ls, ra, g, pl, twx, spec, TJ);
+}
+
+// Standalone split RHS (tbfp_rhs_split): s on the interior.
+template <bool ST>
+__global__ void k_rhs(RhsArgs ra, GridK g, double *__restrict__ s, Lay Ls) {
+  const long n = (long)g.nx * g.R;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.nx) + 1;
+    const long rr = t / g.nx;
+    const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
+    s[at(Ls, i, j, k)] = rhs_cell<ST>(ra, g, i, j, k);
+  }
+}
+
+void launch_rhs(const RhsArgs &ra, bool has_st, const GridK &g, double *s, Lay Ls, cudaStream_t st) {
+  const long n = (long)g.nx * g.R;
+  int blocks = (int)min((n + 255) / 256, 148L * 16);
+  if (has_st) k_rhs<true><<<blocks, 256, 0, st>>>(ra, g, s, Ls);
+  else k_rhs<false><<<blocks, 256, 0, st>>>(ra, g, s, Ls);
+}
+
+// ---------------------------------------------------------------------------
+// z transform (forward or backward) of a tile of TJz consecutive j columns of
+// one kx plane: S[kx][(k-1)*ny + j-1], k = 1..nz, staged in shared memory.
+// ---------------------------------------------------------------------------
+template <bool INV>
+__global__ void __launch_bounds__(kNT, 2) k_fftz(double2 *__restrict__ spec, GridK g, FftPlan pl,
+                                              const double2 *__restrict__ twz, int TJz) {
+  extern __shared__ double2 sm[];
+  const int kx = blockIdx.y;
+  const int j0 = blockIdx.x * TJz;
+  const int nj = min(TJz, g.ny - j0);
+  double2 *base = spec + (long)kx * g.R + j0;
+  const int nz = g.nz, ny = g.ny;
+  for (int t = threadIdx.x; t < nz * TJz; t += blockDim.x) {
+    const int k = t / TJz, jj = t - k * TJz;
+    sm[t] = (jj < nj) ? base[(long)k * ny + jj] : mk<double2>(0.0, 0.0);
+  }
+  __syncthreads();
+  fft_smem<double2, kEMAX, INV>(sm, pl, __ffs(TJz) - 1, TJz, 1, twz, 1);
+  for (int t = threadIdx.x; t < nz * TJz; t += blockDim.x) {
+    const int k = t / TJz, jj = t - k * TJz;
+    if (jj < nj) base[(long)k * ny + jj] = sm[t];
+  }
+}
+
+void launch_fftz(double2 *spec, const GridK &g, const FftPlan &pl, const double2 *twz, bool inverse,
+                 cudaStream_t st) {
+  const int TJz = fftz_cols_per_cta(g.nz);
+  dim3 grid((g.ny + TJz - 1) / TJz, g.nkx);
+  if (inverse) k_fftz<true><<<grid, kNT, fftz_smem_bytes(g.nz), st>>>(spec, g, pl, twz, TJz);
+  else k_fftz<false><<<grid, kNT, fftz_smem_bytes(g.nz), st>>>(spec, g, pl, twz, TJz);
+}
+
+// ---------------------------------------------------------------------------
+// y systems (solveTriDiag, fastPoissonSolver.f90:280-333): one warp per (kx,kz).
+// Row j (0-based) scaled as in the reference, r = 1/(lam - am - ap):
+//     a_j x_{j-1} + x_j + c_j x_{j+1} = d_j,  a = am*r, c = ap*r, d = f*r.
+// Each lane owns a contiguous block [s,e] of rows (partition method):
+//   forward within the block:  at_i x_{s-1} + x_i + ct_i x_{i+1} = dt_i
+//   running backward pass:     x_s = hd - ha x_{s-1} - hc x_e
+// which gives one reduced equation per lane in y_l = x_{e_l}:
+//   at_e y_{l-1} + (1 - ct_e ha') y_l - ct_e hc' y_{l+1} = dt_e - ct_e hd'
+// (primes: the next lane's hat values), solved by parallel cyclic reduction
+// over the warp; then x_i = dt_i - at_i y_{l-1} - ct_i x_{i+1}.
+// The singular (0,0) system (Neumann walls) is gauged by pinning its last
+// unknown to zero, then its volume-weighted mean is removed in spectral space:
+// sum_{i,k} p(i,j,k) = X(0,j,0), so zeroAveragePressure (:388-423) is
+// X(0,j,0) -= nx*nz * dx*dz*sum_j dyf(j) X(0,j,0) / s_Vg.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+__device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+
+__global__ void __launch_bounds__(kWPB * 32) k_tridiag(double2 *__restrict__ spec, GridK g,
+                                                       const double *__restrict__ lamx,
+                                                       const double *__restrict__ lamz,
+                                                       const double *__restrict__ am, const double *__restrict__ ap,
+                                                       const double *__restrict__ dyf, double mean_c, double nxnz) {
+  extern __shared__ unsigned char smraw[];
+  const int ny = g.ny;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *d = reinterpret_cast<double2 *>(smraw) + (long)warp * ny;
+  double *ca = reinterpret_cast<double *>(reinterpret_cast<double2 *>(smraw) + (long)kWPB * ny) + (long)warp * 2 * ny;
+  double *cc = ca + ny;
+  const long q = (long)blockIdx.x * kWPB + warp;
+  if (q >= (long)g.nkx * g.nz) return;  // whole warp leaves; no block-level barrier follows
+  const int kx = (int)(q / g.nz), kz = (int)(q % g.nz);
+  double2 *S = spec + (long)kx * g.R + (long)kz * ny;
+  for (int e = lane; e < ny; e += 32) d[e] = S[e];
+  __syncwarp();
+
+  const double lam = lamx[kx] + lamz[kz];
+  const bool pin = (kx == 0 && kz == 0);
+  const int NL = min(32, ny / 2);
+  const int nb = ny / NL, rem = ny - nb * NL;
+  const bool active = lane < NL;
+  const int s = lane * nb + min(lane, rem);
+  const int len = active ? nb + (lane < rem ? 1 : 0) : 0;
+  const int e = s + len - 1;
+
+  double at_e = 0.0, ct_e = 0.0;
+  double2 dt_e = mk<double2>(0.0, 0.0);
+  if (active) {
+    double at_p = 0.0, ct_p = 0.0;
+    double2 dt_p = mk<double2>(0.0, 0.0);
+    for (int i = s; i <= e; ++i) {
+      const double r = 1.0 / (lam - am[i] - ap[i]);
+      double a = am[i] * r, c = ap[i] * r;
+      double2 dd = cscale(d[i], r);
+      if (pin && i == ny - 1) {
+        a = 0.0;
+        c = 0.0;
+        dd = mk<double2>(0.0, 0.0);
+      }
+      double at, ct;
+      double2 dt;
+      if (i == s) {
+        at = a;
+        ct = c;
+        dt = dd;
+      } else {
+        const double inv = 1.0 / (1.0 - a * ct_p);
+        at = -a * at_p * inv;
+        ct = c * inv;
+        dt = mk<double2>((dd.x - a * dt_p.x) * inv, (dd.y - a * dt_p.y) * inv);
+      }
+      ca[i] = at;
+      cc[i] = ct;
+      d[i] = dt;
+      at_p = at;
+      ct_p = ct;
+      dt_p = dt;
+    }
+    at_e = at_p;
+    ct_e = ct_p;
+    dt_e = dt_p;
+  }
+  // running backward pass for x_s in terms of x_{s-1} and x_e
+  double ha = 0.0, hc = -1.0;
+  double2 hd = mk<double2>(0.0, 0.0);
+  if (active && len >= 2) {
+    hd = d[e - 1];
+    ha = ca[e - 1];
+    hc = cc[e - 1];
+    for (int i = e - 2; i >= s; --i) {
+      const double ct = cc[i];
+      hd = mk<double2>(d[i].x - ct * hd.x, d[i].y - ct * hd.y);
+      ha = ca[i] - ct * ha;
+      hc = -ct * hc;
+    }
+  }
+  const double ha_n = shdn(ha, 1), hc_n = shdn(hc, 1);
+  const double hdx_n = shdn(hd.x, 1), hdy_n = shdn(hd.y, 1);
+  double A = 0.0, B = 1.0, C = 0.0, Dx = 0.0, Dy = 0.0;
+  if (active) {
+    A = at_e;
+    if (lane + 1 < NL) {
+      B = 1.0 - ct_e * ha_n;
+      C = -ct_e * hc_n;
+      Dx = dt_e.x - ct_e * hdx_n;
+      Dy = dt_e.y - ct_e * hdy_n;
+    } else {
+      Dx = dt_e.x;
+      Dy = dt_e.y;
+    }
+  }
+  // parallel cyclic reduction over the 32 reduced equations
+#pragma unroll
+  for (int h = 1; h < 32; h <<= 1) {
+    double Am = shup(A, h), Bm = shup(B, h), Cm = shup(C, h), Dxm = shup(Dx, h), Dym = shup(Dy, h);
+    double Ap = shdn(A, h), Bp = shdn(B, h), Cp = shdn(C, h), Dxp = shdn(Dx, h), Dyp = shdn(Dy, h);
+    if (lane < h) {
+      Am = 0.0; Bm = 1.0; Cm = 0.0; Dxm = 0.0; Dym = 0.0;
+    }
+    if (lane + h >= 32) {
+      Ap = 0.0; Bp = 1.0; Cp = 0.0; Dxp = 0.0; Dyp = 0.0;
+    }
+    const double k1 = A / Bm, k2 = C / Bp;
+    const double nA = -k1 * Am, nC = -k2 * Cp;
+    const double nB = B - k1 * Cm - k2 * Ap;
+    const double nDx = Dx - k1 * Dxm - k2 * Dxp, nDy = Dy - k1 * Dym - k2 * Dyp;
+    A = nA; B = nB; C = nC; Dx = nDx; Dy = nDy;
+  }
+  const double iB = 1.0 / B;
+  const double yx = Dx * iB, yy = Dy * iB;
+  double xsx = shup(yx, 1), xsy = shup(yy, 1);
+  if (lane == 0) { xsx = 0.0; xsy = 0.0; }
+  if (active) {
+    double2 xn = mk<double2>(yx, yy);
+    d[e] = xn;
+    for (int i = e - 1; i >= s; --i) {
+      const double a = ca[i], c = cc[i];
+      xn = mk<double2>(d[i].x - a * xsx - c * xn.x, d[i].y - a * xsy - c * xn.y);
+      d[i] = xn;
+    }
+  }
+  __syncwarp();
+  if (pin) {
+    double sx = 0.0, sy = 0.0;
+    for (int i = lane; i < ny; i += 32) {
+      sx += d[i].x * dyf[i];
+      sy += d[i].y * dyf[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sx += __shfl_xor_sync(0xffffffffu, sx, o);
+      sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    const double subx = sx * mean_c * nxnz, suby = sy * mean_c * nxnz;
+    for (int i = lane; i < ny; i += 32) d[i] = mk<double2>(d[i].x - subx, d[i].y - suby);
+    __syncwarp();
+  }
+  for (int i = lane; i < ny; i += 32) S[i] = d[i];
+}
+
+void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
+                    const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st) {
+  const long nsys = (long)g.nkx * g.nz;
+  const long nblk = (nsys + kWPB - 1) / kWPB;
+  k_tridiag<<<(unsigned)nblk, kWPB * 32, tridiag_smem_bytes(g.ny), st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c,
+                                                                         nxnz);
+}
+
+// ---------------------------------------------------------------------------
+// Inverse x transform of a tile of rows: S[kx][row] -> c2r -> psi rows scaled
+// by 1/(nx*nz) (fastPoissonSolver.f90:371-378), written with every ghost image
+// of updateBoundaries (field.f90:950-974 on one rank): the first y ghost layer
+// copies the wall cell (normalGradient, bf=0), x and z ghosts are periodic.
+// The imaginary parts of X[0] and X[nx/2] are ignored, as FFTW's c2r does.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kNT, 2) k_fftx_inv(const double2 *__restrict__ spec, double *__restrict__ psi, Lay Lp,
+                                                  int hd, GridK g, FftPlan pl, const double2 *__restrict__ twx,
+                                                  double scale, int TJ) {
+  extern __shared__ double2 sm[];
+  const int M = g.M, nx = g.nx, ld = M + 1;
+  const long r0 = (long)blockIdx.x * TJ;
+  const int nrows = (int)min((long)TJ, g.R - r0);
+  for (int t = threadIdx.x; t < TJ * ld; t += blockDim.x) {
+    const int kx = t / TJ, row = t - kx * TJ;
+    sm[(long)row * ld + kx] = (row < nrows) ? spec[(long)kx * g.R + r0 + row] : mk<double2>(0.0, 0.0);
+  }
+  __syncthreads();
+  // Z[k] = (X_k + conj X_{M-k}) + i conj(W^k) (X_k - conj X_{M-k}),  k = 0..M-1
+  const int npair = M / 2 + 1;
+  for (int t = threadIdx.x; t < TJ * npair; t += blockDim.x) {
+    const int row = t / npair, kk = t - row * npair;
+    double2 *X = sm + (long)row * ld;
+    if (kk == 0) {
+      const double a = X[0].x, b = X[M].x;
+      X[0] = mk<double2>(a + b, a - b);
+    } else {
+      const int km = M - kk;
+      const double2 a = X[kk], b = X[km];
+      const double2 wa = cconj(twx[kk]), wb = cconj(twx[km]);
+      double2 ep = mk<double2>(a.x + b.x, a.y - b.y);
+      double2 em = mk<double2>(a.x - b.x, a.y + b.y);
+      double2 t1 = cmul(wa, em);
+      X[kk] = mk<double2>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
+      if (km != kk) {
+        double2 fp = mk<double2>(b.x + a.x, b.y - a.y);
+        double2 fm = mk<double2>(b.x - a.x, b.y + a.y);
+        double2 t2 = cmul(wb, fm);
+        X[km] = mk<double2>(fp.x - t2.y, fp.y + t2.x);
+      }
+    }
+  }
+  __syncthreads();
+  fft_smem<double2, kEMAX, true>(sm, pl, __ffs(TJ) - 1, 1, ld, twx, 2);
+  const double *smr = reinterpret_cast<const double *>(sm);
+  for (int t = threadIdx.x; t < TJ * nx; t += blockDim.x) {
+    const int row = t / nx, ii = t - row * nx;
+    if (row >= nrows) continue;
+    const double v = smr[(long)row * 2 * ld + ii] * scale;
+    const long rr = r0 + row;
+    const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
+    const int i = ii + 1;
+    // images of (i, j, k)
+    int is[2], js[2], ks[2];
+    int ni = 1, nj = 1, nk = 1;
+    is[0] = i; js[0] = j; ks[0] = k;
+    if (i <= hd) is[ni++] = i + nx;
+    else if (i > nx - hd) is[ni++] = i - nx;
+    if (j == 1) js[nj++] = 0;
+    else if (j == g.ny) js[nj++] = g.ny + 1;
+    if (k <= hd) ks[nk++] = k + g.nz;
+    else if (k > g.nz - hd) ks[nk++] = k - g.nz;
+    for (int c = 0; c < nk; ++c)
+      for (int b = 0; b < nj; ++b)
+        for (int a = 0; a < ni; ++a) psi[at(Lp, is[a], js[b], ks[c])] = v;
+  }
+}
+
+void launch_fftx_inv(const double2 *spec, double *psi, Lay Lp, int hd, const GridK &g, const FftPlan &pl,
+                     const double2 *twx, double scale, cudaStream_t st) {
+  const int TJ = fftx_rows_per_cta(g.M);
+  const long nblk = (g.R + TJ - 1) / TJ;
+  k_fftx_inv<<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(spec, psi, Lp, hd, g, pl, twx, scale, TJ);
+}
+
+// ---------------------------------------------------------------------------
+// Velocity correction (makeVelocityDivFree FAST, momentumEqn.f90:999-1127):
+//   u_d -= dt*alpha*[ (1/rho0) d psi + (1/rho_f - 1/rho0)(2 d psi^n - d psi^{n-1} - (2 st^n - st^{n-1})) ]
+// One face value per helper; faces are indexed like the staggered arrays.
+// ---------------------------------------------------------------------------
+template <bool ST>
+__device__ __forceinline__ double corr_x(const CorrArgs &a, const GridK &g, int i, int j, int k) {
+  const long pc = at(a.Lpsi, i, j, k), rc = at(a.Lrho, i, j, k);
+  const double invrho = 0.5 * (a.irho[rc + 1] + a.irho[rc]);
+  const double dpr = (a.psi[pc + 1] - a.psi[pc]) * g.idxc1;
+  double dpr0 = (2.0 * (a.pn[pc + 1] - a.pn[pc]) - (a.pnm1[pc + 1] - a.pnm1[pc])) * g.idxc1;
+  if constexpr (ST) {
+    const long q = at(a.Lst[0], i, j, k);
+    dpr0 = dpr0 - 2.0 * a.stn[0][q] + a.sto[0][q];
+  }
+  return a.uxi[at(a.Lux, i, j, k)] - a.r * (a.invrho0 * dpr + (invrho - a.invrho0) * dpr0);
+}
+template <bool ST>
+__device__ __forceinline__ double corr_y(const CorrArgs &a, const GridK &g, int i, int j, int k) {
+  const long pc = at(a.Lpsi, i, j, k), rc = at(a.Lrho, i, j, k);
+  const long sj = a.Lpsi.sj;
+  const double invrho = 0.5 * (a.irho[rc + a.Lrho.sj] + a.irho[rc]);
+  const double idy = g.idyc[j];  // 1/dyc(j+1)
+  const double dpr = (a.psi[pc + sj] - a.psi[pc]) * idy;
+  double dpr0 = (2.0 * (a.pn[pc + sj] - a.pn[pc]) - (a.pnm1[pc + sj] - a.pnm1[pc])) * idy;
+  if constexpr (ST) {
+    const long q = at(a.Lst[1], i, j, k);
+    dpr0 = dpr0 - 2.0 * a.stn[1][q] + a.sto[1][q];
+  }
+  return a.uyi[at(a.Luy, i, j, k)] - a.r * (a.invrho0 * dpr + (invrho - a.invrho0) * dpr0);
+}
+template <bool ST>
+__device__ __forceinline__ double corr_z(const CorrArgs &a, const GridK &g, int i, int j, int k) {
+  const long pc = at(a.Lpsi, i, j, k), rc = at(a.Lrho, i, j, k);
+  const long sk = a.Lpsi.sk;
+  const double invrho = 0.5 * (a.irho[rc + a.Lrho.sk] + a.irho[rc]);
+  const double dpr = (a.psi[pc + sk] - a.psi[pc]) * g.idzc1;
+  double dpr0 = (2.0 * (a.pn[pc + sk] - a.pn[pc]) - (a.pnm1[pc + sk] - a.pnm1[pc])) * g.idzc1;
+  if constexpr (ST) {
+    const long q = at(a.Lst[2], i, j, k);
+    dpr0 = dpr0 - 2.0 * a.stn[2][q] + a.sto[2][q];
+  }
+  return a.uzi[at(a.Luz, i, j, k)] - a.r * (a.invrho0 * dpr + (invrho - a.invrho0) * dpr0);
+}
+
+__device__ __forceinline__ void block_max_atomic(double v, unsigned long long *out) {
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (l == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// Out-of-place correction fused with the continuity check: every thread owns
+// cell (i,j,k), computes its six corrected faces (the three "minus" faces are
+// recomputed with the neighbour's arithmetic, so they equal what that
+// neighbour writes) and reduces |div u| (auxiliaryRoutines.f90:71-75).
+// The periodic duplicates ux(0)=ux(nx), uz(.,.,0)=uz(.,.,nz) are the equated
+// values of vfield.f90:124-189; the uy wall faces are copied through.
+template <bool ST>
+__global__ void __launch_bounds__(256) k_correct_div(CorrArgs a, GridK g, unsigned long long *__restrict__ maxdiv) {
+  const long n = (long)g.nx * g.R;
+  double vmax = 0.0;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.nx) + 1;
+    const long rr = t / g.nx;
+    const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
+    const double uxp = corr_x<ST>(a, g, i, j, k);
+    const double uxm = corr_x<ST>(a, g, i == 1 ? g.nx : i - 1, j, k);
+    const double uyp = (j < g.ny) ? corr_y<ST>(a, g, i, j, k) : a.uyi[at(a.Luy, i, j, k)];
+    const double uym = (j > 1) ? corr_y<ST>(a, g, i, j - 1, k) : a.uyi[at(a.Luy, i, 0, k)];
+    const double uzp = corr_z<ST>(a, g, i, j, k);
+    const double uzm = corr_z<ST>(a, g, i, j, k == 1 ? g.nz : k - 1);
+    a.uxo[at(a.Lux, i, j, k)] = uxp;
+    if (i == g.nx) a.uxo[at(a.Lux, 0, j, k)] = uxp;
+    a.uyo[at(a.Luy, i, j, k)] = uyp;
+    if (j == 1) a.uyo[at(a.Luy, i, 0, k)] = uym;
+    a.uzo[at(a.Luz, i, j, k)] = uzp;
+    if (k == g.nz) a.uzo[at(a.Luz, i, j, 0)] = uzp;
+    double dv = (uxp - uxm) * g.idxf[i - 1];
+    dv = dv + (uyp - uym) * g.idyf[j - 1];
+    dv = dv + (uzp - uzm) * g.idzf[k - 1];
+    vmax = fmax(vmax, fabs(dv));
+  }
+  block_max_atomic(vmax, maxdiv);
+}
+
+void launch_correct_div(const CorrArgs &ca, bool has_st, const GridK &g, unsigned long long *maxdiv,
+                        cudaStream_t st) {
+  const long n = (long)g.nx * g.R;
+  int blocks = (int)min((n + 255) / 256, 148L * 16);
+  if (has_st) k_correct_div<true><<<blocks, 256, 0, st>>>(ca, g, maxdiv);
+  else k_correct_div<false><<<blocks, 256, 0, st>>>(ca, g, maxdiv);
+}
+
+// In-place correction: each thread reads and writes only the faces it owns.
+template <bool ST>
+__global__ void __launch_bounds__(256) k_correct_inplace(CorrArgs a, GridK g) {
+  const long n = (long)g.nx * g.R;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.nx) + 1;
+    const long rr = t / g.nx;
+    const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
+    const double uxp = corr_x<ST>(a, g, i, j, k);
+    const double uyp = (j < g.ny) ? corr_y<ST>(a, g, i, j, k) : 0.0;
+    const double uzp = corr_z<ST>(a, g, i, j, k);
+    a.uxo[at(a.Lux, i, j, k)] = uxp;
+    if (i == g.nx) a.uxo[at(a.Lux, 0, j, k)] = uxp;
+    if (j < g.ny) a.uyo[at(a.Luy, i, j, k)] = uyp;
+    a.uzo[at(a.Luz, i, j, k)] = uzp;
+    if (k == g.nz) a.uzo[at(a.Luz, i, j, 0)] = uzp;
+  }
+}
+
+void launch_correct_inplace(const CorrArgs &ca, bool has_st, const GridK &g, cudaStream_t st) {
+  const long n = (long)g.nx * g.R;
+  int blocks = (int)min((n + 255) / 256, 148L * 16);
+  if (has_st) k_correct_inplace<true><<<blocks, 256, 0, st>>>(ca, g);
+  else k_correct_inplace<false><<<blocks, 256, 0, st>>>(ca, g);
+}
+
+// computeContinuityError (auxiliaryRoutines.f90:67-80), max|div u| only.
+__global__ void __launch_bounds__(256) k_div(const double *__restrict__ ux, const double *__restrict__ uy,
+                                             const double *__restrict__ uz, Lay Lux, Lay Luy, Lay Luz, GridK g,
+                                             unsigned long long *__restrict__ maxdiv) {
+  const long n = (long)g.nx * g.R;
+  double vmax = 0.0;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.nx) + 1;
+    const long rr = t / g.nx;
+    const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
+    double dv = (ux[at(Lux, i, j, k)] - ux[at(Lux, i - 1, j, k)]) * g.idxf[i - 1];
+    dv = dv + (uy[at(Luy, i, j, k)] - uy[at(Luy, i, j - 1, k)]) * g.idyf[j - 1];
+    dv = dv + (uz[at(Luz, i, j, k)] - uz[at(Luz, i, j, k - 1)]) * g.idzf[k - 1];
+    vmax = fmax(vmax, fabs(dv));
+  }
+  block_max_atomic(vmax, maxdiv);
+}
+
+void launch_div(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz, const GridK &g,
+                unsigned long long *maxdiv, cudaStream_t st) {
+  const long n = (long)g.nx * g.R;
+  int blocks = (int)min((n + 255) / 256, 148L * 16);
+  k_div<<<blocks, 256, 0, st>>>(ux, uy, uz, Lux, Luy, Luz, g, maxdiv);
+}
+
+// Raise the dynamic shared-memory limits once per process.
+cudaError_t prepare_kernels() {
+  const int big = 227 * 1024;
+  cudaError_t e = cudaSuccess;
+#define TBFP_ATTR(fn)                                                                 \
+  do {                                                                                \
+    cudaError_t ee = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, big); \
+    if (ee != cudaSuccess) e = ee;                                                    \
+  } while (0)
+  TBFP_ATTR((k_fftx_fwd<0, false>));
+  TBFP_ATTR((k_fftx_fwd<1, false>));
+  TBFP_ATTR((k_fftx_fwd<1, true>));
+  TBFP_ATTR(k_fftz<false>);
+  TBFP_ATTR(k_fftz<true>);
+  TBFP_ATTR(k_tridiag);
+  TBFP_ATTR(k_fftx_inv);
+#undef TBFP_ATTR
+  return e;
+}
+
+}  // namespace tbfp

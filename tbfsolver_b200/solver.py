@@ -1,0 +1,223 @@
+"""Python mirror of the reference's projection-step interface over the C ABI.
+
+Names and argument meaning follow the Fortran modules they replace:
+
+* ``FastPoissonSolver``  -- fastPoissonSolverMod (src/fastPoissonSolver/fastPoissonSolver.f90):
+  ``FastPoissonSolver(mesh)`` is fastPoissonSolverCTOR (:123), ``solve_fps(p, s)`` is solveFPS (:337).
+* ``PoissonEqn``         -- poissonEqnMod in FAST_MODE (src/poissonEqn/poissonEqn.f90):
+  ``compute_source`` (:193), ``solve_poisson_eqn`` (:347), ``update_pressure`` (:374).
+* ``make_velocity_div_free`` -- momentumEqn.f90:999 (FAST_MODE).
+* ``compute_continuity_error`` -- auxiliaryRoutines.f90:42 (returns the value
+  instead of printing it).
+
+The reference's old time levels ``psi%ptrf_`` and ``psi%ptrf_%ptrf_`` are
+passed explicitly as ``psi_n`` and ``psi_nm1``; the surface-tension old levels
+as ``st_n``/``st_nm1`` triples (or None for zero surface tension).  Errors the
+reference turns into mpiABORT raise ``TbfpError``; soft conditions are returned.
+
+Fields holding numpy arrays go through the host entry points (copies in and
+out); fields holding CUDA tensors go through the ``*_dev`` entry points.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._native import (TBFP_EINVAL, TBFP_FLAG_ASYNC, TBFP_FLAG_TIMING, TBFP_FP64, TBFP_MIXED, TbfpDesc, TbfpError,
+                      TbfpStats, check, load)
+from .fields import Field, VField
+from .grid import Grid
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _placement(fields) -> bool:
+    """True if every field is on a CUDA device, False if every one is on the host."""
+    flags = {f.on_cuda for f in fields if f is not None}
+    if len(flags) != 1:
+        raise TbfpError(TBFP_EINVAL, "fields must all live on the host or all on the device")
+    return flags.pop()
+
+
+class _PtrTriple:
+    """A ``const double *const[3]`` argument kept alive for one call."""
+
+    def __init__(self, st):
+        if st is None:
+            self.arr = None
+            self.addr = None
+        else:
+            if len(st) != 3:
+                raise ValueError("surface tension must be a (x, y, z) triple of fields")
+            self.arr = (C.c_void_p * 3)(*[f.address() for f in st])
+            self.addr = C.cast(self.arr, C.c_void_p).value
+
+
+class FastPoissonSolver:
+    """The split-constant-coefficient direct Poisson solver on one GPU."""
+
+    def __init__(self, mesh: Grid, hd_psi: int = 1, hd_u: int = 2, hd_rho: int = 1, hd_st: int = 1,
+                 precision: str = "fp64", tol: float = 1e-10, max_iter: int = 8, device: int = -1,
+                 stream: int | None = None, asynchronous: bool = False, timing: bool = False):
+        self.lib = load()
+        self.mesh = mesh
+        self.hd_psi, self.hd_u, self.hd_rho, self.hd_st = hd_psi, hd_u, hd_rho, hd_st
+        nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+        # keep the metric arrays alive while the descriptor is read
+        self._m = {
+            "dxf": np.ascontiguousarray(mesh.dxf.r(1, nx)), "dxc": np.ascontiguousarray(mesh.dxc.r(1, nx + 1)),
+            "dyf": np.ascontiguousarray(mesh.dyf.r(1, ny)), "dyc": np.ascontiguousarray(mesh.dyc.r(1, ny + 1)),
+            "dzf": np.ascontiguousarray(mesh.dzf.r(1, nz)), "dzc": np.ascontiguousarray(mesh.dzc.r(1, nz + 1)),
+        }
+        prec = {"fp64": TBFP_FP64, "mixed": TBFP_MIXED}[precision]
+        d = TbfpDesc(nx=nx, ny=ny, nz=nz, hd_psi=hd_psi, hd_u=hd_u, hd_rho=hd_rho, hd_st=hd_st,
+                     dx_fft=mesh.dx_fft, dz_fft=mesh.dz_fft,
+                     dxf=_dptr(self._m["dxf"]), dxc=_dptr(self._m["dxc"]), dyf=_dptr(self._m["dyf"]),
+                     dyc=_dptr(self._m["dyc"]), dzf=_dptr(self._m["dzf"]), dzc=_dptr(self._m["dzc"]),
+                     s_Vg=mesh.s_Vg, precision=prec, tol=tol, max_iter=max_iter, device=device,
+                     stream=stream, flags=(TBFP_FLAG_ASYNC if asynchronous else 0) | (TBFP_FLAG_TIMING if timing else 0))
+        h = C.c_void_p()
+        check(self.lib.tbfp_create(C.byref(d), C.byref(h)), None)
+        self.h = h
+
+    # --- lifecycle -------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.tbfp_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover - interpreter shutdown
+            pass
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.lib.tbfp_device_bytes(self.h))
+
+    # --- fields ----------------------------------------------------------
+    def new_field(self, kind: str, hd: int | None = None) -> Field:
+        m = self.mesh
+        if hd is None:
+            hd = {"cl": self.hd_psi, "sx": self.hd_u, "sy": self.hd_u, "sz": self.hd_u}[kind]
+        return Field(kind, hd, m.nx, m.ny, m.nz)
+
+    def _check_psi(self, *fs):
+        for f in fs:
+            if f.kind != "cl" or f.hd != self.hd_psi:
+                raise TbfpError(TBFP_EINVAL, f"expected a 'cl' field with halo {self.hd_psi}")
+
+    # --- solveFPS ----------------------------------------------------------
+    def solve_fps(self, p: Field, s: Field) -> None:
+        """solveFPS (fastPoissonSolver.f90:337-384): p <- L^{-1} s with zero volume-weighted
+        mean, ghosts updated."""
+        self._check_psi(p, s)
+        dev = _placement([p, s])
+        fn = self.lib.tbfp_solve_fps_dev if dev else self.lib.tbfp_solve_fps
+        check(fn(self.h, s.address(), p.address()), self.h)
+
+
+class PoissonEqn:
+    """The FAST_MODE pressure equation (poissonEqnCTOR, poissonEqn.f90:89-150)."""
+
+    def __init__(self, mesh: Grid, rhol: float, rhog: float, **solver_kw):
+        self.mesh = mesh
+        self.rho0 = min(rhol, rhog)  # poissonEqn.f90:127
+        self.nl = 2  # number of pressure levels (:145)
+        self.solver = FastPoissonSolver(mesh, **solver_kw)
+
+    def close(self):
+        self.solver.close()
+
+    def compute_source(self, s: Field, psi_n: Field, psi_nm1: Field, rho: Field, u: VField, dt: float,
+                       alpha: float, st_n=None, st_nm1=None) -> None:
+        """computeSource FAST (poissonEqn.f90:193-305) into s."""
+        sv = self.solver
+        fields = [s, psi_n, psi_nm1, rho, *u.components()] + list(st_n or []) + list(st_nm1 or [])
+        dev = _placement(fields)
+        a, b = _PtrTriple(st_n), _PtrTriple(st_nm1)
+        fn = sv.lib.tbfp_rhs_split_dev if dev else sv.lib.tbfp_rhs_split
+        check(fn(sv.h, u.ux.address(), u.uy.address(), u.uz.address(), rho.address(), psi_n.address(),
+                 psi_nm1.address(), a.addr, b.addr, dt, alpha, self.rho0, s.address()), sv.h)
+
+    def solve_poisson_eqn(self, psi: Field, psi_n: Field, psi_nm1: Field, rho: Field, u: VField, dt: float,
+                          alpha: float, st_n=None, st_nm1=None) -> None:
+        """solvePoissonEqn FAST (poissonEqn.f90:347-370): computeSource then solveFPS."""
+        s = Field.like(psi, _zeros_like(psi.a))
+        self.compute_source(s, psi_n, psi_nm1, rho, u, dt, alpha, st_n, st_nm1)
+        self.solver.solve_fps(psi, s)
+
+    def projection(self, psi: Field, psi_n: Field, psi_nm1: Field, rho: Field, u: VField, dt: float,
+                   alpha: float, st_n=None, st_nm1=None, u_out: VField | None = None,
+                   want_stats: bool = True) -> TbfpStats | None:
+        """One projection as main.f90:197-212 calls it: solvePoissonEqn, makeVelocityDivFree
+        and computeContinuityError in one library call.  u is overwritten with the
+        projected velocity unless u_out is given (device fields only).  With
+        want_stats=False no statistics are read back, so an asynchronous solver
+        does not synchronise."""
+        sv = self.solver
+        fields = [psi, psi_n, psi_nm1, rho, *u.components()] + list(st_n or []) + list(st_nm1 or [])
+        dev = _placement(fields)
+        a, b = _PtrTriple(st_n), _PtrTriple(st_nm1)
+        st = TbfpStats() if want_stats else None
+        stp = C.byref(st) if want_stats else None
+        if dev:
+            uo = u_out or u
+            check(sv.lib.tbfp_projection_dev(sv.h, u.ux.address(), u.uy.address(), u.uz.address(),
+                                             uo.ux.address(), uo.uy.address(), uo.uz.address(), rho.address(),
+                                             psi_n.address(), psi_nm1.address(), a.addr, b.addr, dt, alpha,
+                                             self.rho0, psi.address(), stp), sv.h)
+        else:
+            if u_out is not None:
+                raise TbfpError(TBFP_EINVAL, "u_out is only supported for device fields")
+            check(sv.lib.tbfp_projection(sv.h, u.ux.address(), u.uy.address(), u.uz.address(), rho.address(),
+                                         psi_n.address(), psi_nm1.address(), a.addr, b.addr, dt, alpha,
+                                         self.rho0, psi.address(), stp), sv.h)
+        return st
+
+    @staticmethod
+    def update_pressure(psi: Field, psi_n: Field, psi_nm1: Field):
+        """updatePressure's history shift (poissonEqn.f90:400-401, storeOldField
+        field.f90:1590-1603) as a rotation of buffers: returns the new
+        (psi_n, psi_nm1, spare) -- psi becomes psi^n, psi^n becomes psi^{n-1}."""
+        return psi, psi_n, psi_nm1
+
+
+def make_velocity_div_free(eqn: PoissonEqn, u: VField, psi: Field, psi_n: Field, psi_nm1: Field, rho: Field,
+                           dt: float, alpha: float, st_n=None, st_nm1=None) -> None:
+    """makeVelocityDivFree FAST (momentumEqn.f90:999-1127), in place on u."""
+    sv = eqn.solver
+    fields = [psi, psi_n, psi_nm1, rho, *u.components()] + list(st_n or []) + list(st_nm1 or [])
+    dev = _placement(fields)
+    a, b = _PtrTriple(st_n), _PtrTriple(st_nm1)
+    fn = sv.lib.tbfp_correct_dev if dev else sv.lib.tbfp_correct
+    check(fn(sv.h, u.ux.address(), u.uy.address(), u.uz.address(), psi.address(), psi_n.address(),
+             psi_nm1.address(), rho.address(), a.addr, b.addr, dt, alpha, eqn.rho0), sv.h)
+
+
+def compute_continuity_error(solver: FastPoissonSolver, u: VField, dt: float):
+    """computeContinuityError (auxiliaryRoutines.f90:42-91): returns
+    (max|div u|, dt*max|div u|)."""
+    dev = _placement(list(u.components()))
+    md, ce = C.c_double(), C.c_double()
+    fn = solver.lib.tbfp_continuity_error_dev if dev else solver.lib.tbfp_continuity_error
+    check(fn(solver.h, u.ux.address(), u.uy.address(), u.uz.address(), dt, C.byref(md), C.byref(ce)), solver.h)
+    return md.value, ce.value
+
+
+def _zeros_like(a):
+    if isinstance(a, np.ndarray):
+        return np.zeros_like(a)
+    import torch  # noqa: PLC0415
+
+    return torch.zeros_like(a)

@@ -1,0 +1,236 @@
+"""GPU parity tests: the CUDA path, called through the C ABI, against the CPU
+oracle and the golden fixtures.
+
+Tolerances (the floating-point bar of the task): pressure and velocity within
+1e-12 relative (L-infinity, relative to the field's max magnitude), max|div u|
+within 1e-12 absolute.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import tbfp_oracle as O
+from tbfsolver_b200 import synth
+from tbfsolver_b200._native import TbfpError
+from tbfsolver_b200.fields import Field, VField
+from tbfsolver_b200.grid import Grid
+from tbfsolver_b200.solver import FastPoissonSolver, PoissonEqn, compute_continuity_error, make_velocity_div_free
+from tests._helpers import mesh_of, rel_linf, to_oracle
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL_P = 1e-12
+TOL_DIV = 1e-12
+
+
+def _grid_from(z):
+    return Grid(int(z["nx"]), int(z["ny"]), int(z["nz"]), float(z["Lx"]), float(z["Ly"]), float(z["Lz"]),
+                bool(z["stretched"]), float(z["gamma"]))
+
+
+def _cuda(f: Field) -> Field:
+    a = f.a if isinstance(f.a, torch.Tensor) else torch.from_numpy(np.asarray(f.a))
+    return Field.like(f, a.to("cuda").contiguous())
+
+
+def _np(f: Field) -> Field:
+    a = f.a.detach().cpu().numpy() if isinstance(f.a, torch.Tensor) else np.asarray(f.a)
+    return Field.like(f, np.ascontiguousarray(a, dtype=np.float64).copy())
+
+
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "kat_*.npz"))))
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_golden_kat_solve_fps(path, where):
+    """Manufactured solution: solve_fps(s = L_h psi*) == psi* - mean, ghosts included."""
+    z = np.load(path)
+    g = _grid_from(z)
+    with FastPoissonSolver(g) as fps:
+        s = Field("cl", 1, g.nx, g.ny, g.nz, z["s"].copy())
+        p = Field("cl", 1, g.nx, g.ny, g.nz)
+        if where == "device":
+            s, p = _cuda(s), _cuda(p)
+        fps.solve_fps(p, s)
+        got = _np(p).a
+    assert rel_linf(got, z["psi_expected"]) < TOL_P
+
+
+def _golden_fields(z, device):
+    nx, ny, nz = int(z["nx"]), int(z["ny"]), int(z["nz"])
+    hu = int(z["hd_u"])
+    mk = lambda kind, key, hd: Field(kind, hd, nx, ny, nz, z[key].copy())  # noqa: E731
+    u = VField(mk("sx", "ux", hu), mk("sy", "uy", hu), mk("sz", "uz", hu))
+    rest = [mk("cl", k, 1) for k in ("rho", "psi_n", "psi_nm1")]
+    st_n = st_nm1 = None
+    if "stn_x" in z:
+        st_n = [mk(k, "stn_" + c, 1) for k, c in zip(("sx", "sy", "sz"), "xyz")]
+        st_nm1 = [mk(k, "sto_" + c, 1) for k, c in zip(("sx", "sy", "sz"), "xyz")]
+    if device:
+        u = VField(*[_cuda(f) for f in u.components()])
+        rest = [_cuda(f) for f in rest]
+        if st_n:
+            st_n = [_cuda(f) for f in st_n]
+            st_nm1 = [_cuda(f) for f in st_nm1]
+    return u, rest, st_n, st_nm1
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "proj_*.npz"))))
+@pytest.mark.parametrize("mode", ["host", "device_inplace", "device_outofplace"])
+def test_golden_projection(path, mode):
+    """One projection (computeSource, solveFPS, makeVelocityDivFree, continuity check)."""
+    z = np.load(path)
+    g = _grid_from(z)
+    dev = mode != "host"
+    u, (rho, pn, pnm1), st_n, st_nm1 = _golden_fields(z, dev)
+    eqn = PoissonEqn(g, 1.0, float(z["rho0"]), hd_u=int(z["hd_u"]))
+    try:
+        psi = Field("cl", 1, g.nx, g.ny, g.nz)
+        if dev:
+            psi = _cuda(psi)
+        uo = None
+        if mode == "device_outofplace":
+            uo = VField(*[Field.like(f, torch.full_like(f.a, 7.0)) for f in u.components()])
+        st = eqn.projection(psi, pn, pnm1, rho, u, float(z["dt"]), float(z["alpha"]), st_n, st_nm1, u_out=uo)
+        res = uo or u
+        assert rel_linf(_np(psi).a, z["psi"]) < TOL_P
+        for c, f in zip("xyz", res.components()):
+            a = _np(f).a
+            want = z[f"u{c}_out"]
+            if mode == "device_outofplace":  # halos are not written out of place: compare interiors
+                a = Field.like(f, a).interior()
+                want = Field.like(f, want).interior()
+            assert rel_linf(a, want) < TOL_P, c
+        assert abs(st.max_div - float(z["max_div"])) < TOL_DIV
+        assert st.cont_err == pytest.approx(st.max_div * float(z["dt"]), rel=1e-15)
+    finally:
+        eqn.close()
+
+
+# ---------------------------------------------------------------------------
+def _case(nx, ny, nz, stretched, nb=2, radius=0.3, seed=5, rhog=0.05):
+    spec = synth.small_spec(nx, ny, nz, stretched=stretched, nbubbles=nb, radius=radius, rhog=rhog)
+    return synth.make_inputs(spec, seed=seed)
+
+
+@pytest.mark.parametrize("dims,stretched", [((32, 24, 16), True), ((64, 64, 32), False), ((96, 48, 48), True),
+                                            ((128, 96, 64), True), ((48, 100, 24), False), ((256, 40, 12), True)])
+def test_solve_fps_random_rhs(dims, stretched):
+    """solveFPS on a seeded random right-hand side vs the oracle (LAPACK path);
+    covers radix-2/4/8 and radix-3 lengths and ny not a multiple of 32."""
+    nx, ny, nz = dims
+    g = Grid(nx, ny, nz, 2 * np.pi, 2.0, np.pi, stretched, 1.5)
+    m = mesh_of(g)
+    rng = np.random.default_rng(nx + ny + nz)
+    s = Field("cl", 1, nx, ny, nz)
+    s.interior()[...] = rng.standard_normal((nz, ny, nx))
+    want = O.FField("cl", 1, nx, ny, nz)
+    O.solve_fps(m, s.interior().copy(), want, tridiag="lapack" if nx * nz <= 8192 else "thomas")
+    with FastPoissonSolver(g) as fps:
+        p = _cuda(Field("cl", 1, nx, ny, nz))
+        fps.solve_fps(p, _cuda(s))
+        got = _np(p).a
+    assert rel_linf(got, want.a) < TOL_P
+
+
+@pytest.mark.parametrize("stretched", [True, False])
+def test_rhs_correct_and_continuity_separately(stretched):
+    """tbfp_rhs_split, tbfp_correct and tbfp_continuity_error against
+    computeSource, makeVelocityDivFree and computeContinuityError."""
+    inp = _case(48, 32, 24, stretched, seed=11)
+    g = inp.grid
+    m = mesh_of(g)
+    rng = np.random.default_rng(2)
+    pn, pnm1 = _np(inp.psi_n), _np(inp.psi_nm1)
+    pn.a[...] = rng.standard_normal(pn.a.shape)
+    pnm1.a[...] = rng.standard_normal(pn.a.shape)
+    o = {k: to_oracle(f, g) for k, f in (("ux", inp.u.ux), ("uy", inp.u.uy), ("uz", inp.u.uz), ("rho", inp.rho))}
+    opn, opnm1 = to_oracle(pn, g), to_oracle(pnm1, g)
+    s_ref = O.compute_source_fast(m, opn, opnm1, o["rho"], o["ux"], o["uy"], o["uz"], inp.dt, inp.alpha, inp.rho0)
+    eqn = PoissonEqn(g, 1.0, inp.rho0)
+    try:
+        u = VField(*[_cuda(f) for f in inp.u.components()])
+        s = _cuda(Field("cl", 1, g.nx, g.ny, g.nz))
+        eqn.compute_source(s, _cuda(pn), _cuda(pnm1), _cuda(inp.rho), u, inp.dt, inp.alpha)
+        assert rel_linf(_np(s).interior(), s_ref) < TOL_P
+        # correction with a given psi
+        psi = _np(Field("cl", 1, g.nx, g.ny, g.nz))
+        psi.a[...] = rng.standard_normal(psi.a.shape)
+        opsi = to_oracle(psi, g)
+        O.update_boundaries_cl_channel(opsi)
+        psi.a[...] = opsi.a
+        ux, uy, uz = o["ux"].copy(), o["uy"].copy(), o["uz"].copy()
+        O.make_velocity_div_free(m, ux, uy, uz, opsi, opn, opnm1, o["rho"], inp.dt, inp.alpha, inp.rho0)
+        make_velocity_div_free(eqn, u, _cuda(psi), _cuda(pn), _cuda(pnm1), _cuda(inp.rho), inp.dt, inp.alpha)
+        for f, want in zip(u.components(), (ux, uy, uz)):
+            a = Field.like(f, _np(f).a)
+            assert rel_linf(a.interior(), Field.like(f, want.a).interior()) < TOL_P
+        md, ce = compute_continuity_error(eqn.solver, u, inp.dt)
+        md_ref = O.compute_continuity_error(m, ux, uy, uz)
+        assert abs(md - md_ref) <= 1e-12 * max(1.0, md_ref)
+        assert ce == pytest.approx(md * inp.dt, rel=1e-15)
+    finally:
+        eqn.close()
+
+
+@pytest.mark.parametrize("name", ["c1"])
+def test_projection_chain_full_config(name):
+    """Config 1 at full size (128x128x64, 18 bubbles): a 3-call projection chain on
+    the GPU vs the oracle chain, compared at every call."""
+    spec = synth.CONFIGS[name]
+    inp = synth.make_inputs(spec, seed=2024)
+    g = inp.grid
+    m = mesh_of(g)
+    ou = [to_oracle(f, g) for f in inp.u.components()]
+    orho, opn, opnm1 = to_oracle(inp.rho, g), to_oracle(inp.psi_n, g), to_oracle(inp.psi_nm1, g)
+    eqn = PoissonEqn(g, spec.rhol, spec.rhog)
+    try:
+        u0 = VField(*[_cuda(f) for f in inp.u.components()])
+        rho, pn, pnm1 = _cuda(inp.rho), _cuda(inp.psi_n), _cuda(inp.psi_nm1)
+        for call in range(3):
+            r = O.projection(m, *ou, orho, opn, opnm1, inp.dt, inp.alpha, inp.rho0)
+            psi = _cuda(Field("cl", 1, g.nx, g.ny, g.nz))
+            uo = VField(*[Field.like(f, torch.empty_like(f.a)) for f in u0.components()])
+            st = eqn.projection(psi, pn, pnm1, rho, u0, inp.dt, inp.alpha, u_out=uo)
+            assert rel_linf(_np(psi).a, r.psi.a) < TOL_P, call
+            for f, want in zip(uo.components(), (r.ux, r.uy, r.uz)):
+                assert rel_linf(Field.like(f, _np(f).a).interior(), Field.like(f, want.a).interior()) < TOL_P
+            assert abs(st.max_div - r.max_div) < TOL_DIV
+            opnm1, opn = opn, r.psi
+            pnm1, pn = pn, psi
+    finally:
+        eqn.close()
+
+
+def test_host_and_device_paths_identical():
+    inp = _case(32, 24, 16, True, seed=3)
+    g = inp.grid
+    eqn = PoissonEqn(g, 1.0, inp.rho0)
+    try:
+        uh = VField(*[_np(f) for f in inp.u.components()])
+        ph = Field("cl", 1, g.nx, g.ny, g.nz)
+        sh = eqn.projection(ph, _np(inp.psi_n), _np(inp.psi_nm1), _np(inp.rho), uh, inp.dt, inp.alpha)
+        ud = VField(*[_cuda(f) for f in inp.u.components()])
+        pd = _cuda(Field("cl", 1, g.nx, g.ny, g.nz))
+        sd = eqn.projection(pd, _cuda(inp.psi_n), _cuda(inp.psi_nm1), _cuda(inp.rho), ud, inp.dt, inp.alpha)
+        assert np.array_equal(ph.a, _np(pd).a)
+        for a, b in zip(uh.components(), ud.components()):
+            assert np.array_equal(a.a, _np(b).a)
+        assert sh.max_div == sd.max_div
+    finally:
+        eqn.close()
+
+
+def test_errors_are_raised_not_hidden():
+    g = Grid(16, 12, 8, 1.0, 2.0, 1.0)
+    with FastPoissonSolver(g) as fps:
+        with pytest.raises(TbfpError):
+            fps.solve_fps(_cuda(Field("cl", 1, 16, 12, 8)), Field("cl", 1, 16, 12, 8))  # mixed placement
+        eqn = PoissonEqn(g, 1.0, 0.1)
+        u = VField.zeros(2, 16, 12, 8)
+        f = Field("cl", 1, 16, 12, 8)
+        with pytest.raises(TbfpError):
+            eqn.projection(f, f, f, f, u, dt=-1.0, alpha=1.0)
+        eqn.close()
