@@ -303,12 +303,20 @@ def fps_offdiag(mesh: Mesh):
     return am, ap
 
 
-def solve_tridiag_lapack(spec: np.ndarray, lx: np.ndarray, lz: np.ndarray, am: np.ndarray, ap: np.ndarray) -> None:
+def solve_tridiag_lapack(spec: np.ndarray, lx: np.ndarray, lz: np.ndarray, am: np.ndarray, ap: np.ndarray,
+                         pin00: bool = False) -> None:
     """solveTriDiag (fastPoissonSolver.f90:280-333) with the LAPACK routines the
     reference calls.  ``spec`` has shape (nz, ny, nkx) (complex, modified in place);
     system (kx, kz) runs along axis 1.  Row scaling by r=1/(lx+lz-am-ap) so the
     diagonal is 1; ``zgttrf``; if info != 0 the last U pivot becomes epsilon
-    (:318-322); ``zgttrs``."""
+    (:318-322); ``zgttrs``.
+
+    pin00=True gauges the singular (0,0) system exactly instead: its last
+    equation is replaced by x_ny = 0.  In exact arithmetic the epsilon pivot
+    solves the same consistent system (the compatibility defect lands in the
+    last row) shifted by a constant of order defect/epsilon, which the zero-mean
+    step removes; in floating point that constant costs up to ~1e-11 relative
+    accuracy, so parity checks at 1e-12 use the exact gauge."""
     nz, ny, nkx = spec.shape
     for kz in range(nz):
         for kx in range(nkx):
@@ -317,6 +325,9 @@ def solve_tridiag_lapack(spec: np.ndarray, lx: np.ndarray, lz: np.ndarray, am: n
             ap_s = (ap * r).astype(np.complex128)
             ac = np.ones(ny, dtype=np.complex128)
             fy = spec[kz, :, kx] * r
+            if pin00 and kx == 0 and kz == 0:
+                am_s[ny - 1] = 0.0
+                fy[ny - 1] = 0.0
             dl, d, du, du2, ipiv, info = lapack.zgttrf(am_s[1:].copy(), ac, ap_s[:-1].copy())
             if info != 0:
                 d[ny - 1] = EPS64
@@ -324,12 +335,17 @@ def solve_tridiag_lapack(spec: np.ndarray, lx: np.ndarray, lz: np.ndarray, am: n
             spec[kz, :, kx] = x
 
 
-def solve_tridiag_thomas(spec: np.ndarray, lx: np.ndarray, lz: np.ndarray, am: np.ndarray, ap: np.ndarray) -> None:
+def solve_tridiag_thomas(spec: np.ndarray, lx: np.ndarray, lz: np.ndarray, am: np.ndarray, ap: np.ndarray,
+                         pin00: bool = True) -> None:
     """Vectorised no-pivoting LU of the same scaled systems (a faster stand-in for
-    the LAPACK call on large grids).  The singular (kx,kz)=(0,0) system gets the
-    same epsilon-pivot rule as :318-322 when its last pivot is exactly zero."""
+    the LAPACK call on large grids).  The singular (kx,kz)=(0,0) system is gauged
+    exactly (last unknown pinned, see solve_tridiag_lapack) unless pin00=False,
+    in which case it gets the epsilon-pivot rule of :318-322."""
     nz, ny, nkx = spec.shape
     lam = lz[:, None] + lx[None, :nkx]  # (nz, nkx)
+    pin = np.zeros(lam.shape, dtype=bool)
+    if pin00:
+        pin[0, 0] = True
     cp = np.empty((ny, nz, nkx))
     dp = np.empty((ny, nz, nkx), dtype=np.complex128)
     r0 = 1.0 / (lam - am[0] - ap[0])
@@ -341,11 +357,15 @@ def solve_tridiag_thomas(spec: np.ndarray, lx: np.ndarray, lz: np.ndarray, am: n
     for j in range(1, ny):
         r = 1.0 / (lam - am[j] - ap[j])
         a = am[j] * r
+        rhs = spec[:, j, :] * r
+        if j == ny - 1:
+            a = np.where(pin, 0.0, a)
+            rhs = np.where(pin, 0.0, rhs)
         den = 1.0 - a * c_prev
         if j == ny - 1:
             den = np.where(den == 0.0, EPS64, den)
         c_prev = (ap[j] * r) / den
-        d_prev = (spec[:, j, :] * r - a * d_prev) / den
+        d_prev = (rhs - a * d_prev) / den
         cp[j] = c_prev
         dp[j] = d_prev
     x = dp[ny - 1]
@@ -356,11 +376,13 @@ def solve_tridiag_thomas(spec: np.ndarray, lx: np.ndarray, lz: np.ndarray, am: n
     del piv
 
 
-def solve_fps(mesh: Mesh, s: np.ndarray, psi: FField, tridiag: str = "lapack") -> None:
+def solve_fps(mesh: Mesh, s: np.ndarray, psi: FField, tridiag: str = "lapack-pinned") -> None:
     """solveFPS (fastPoissonSolver.f90:337-384): r2c along x (:353), c2c along z
     (:357), tridiagonal along y (:363), inverse z (:367) and c2r x (:371), scale by
     1/(nx*nz) (:374), zero volume-weighted mean (:380, :388-423), then
-    updateBoundaries (:381).  All transforms unnormalised as FFTW's."""
+    updateBoundaries (:381).  All transforms unnormalised as FFTW's.
+    tridiag: "lapack" (the reference's epsilon pivot), "lapack-pinned" (same
+    routines, exact gauge of the (0,0) system; the default) or "thomas"."""
     nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
     spec = np.fft.rfft(s, axis=2)  # (nz, ny, nx/2+1), unnormalised forward
     spec = np.fft.fft(spec, axis=0)
@@ -368,6 +390,8 @@ def solve_fps(mesh: Mesh, s: np.ndarray, psi: FField, tridiag: str = "lapack") -
     am, ap = fps_offdiag(mesh)
     if tridiag == "lapack":
         solve_tridiag_lapack(spec, lx, lz, am, ap)
+    elif tridiag == "lapack-pinned":
+        solve_tridiag_lapack(spec, lx, lz, am, ap, pin00=True)
     elif tridiag == "thomas":
         solve_tridiag_thomas(spec, lx, lz, am, ap)
     else:
@@ -480,7 +504,7 @@ class ProjectionResult:
 
 def projection(mesh: Mesh, ux: FField, uy: FField, uz: FField, rho: FField, psi_n: FField,
                psi_nm1: FField, dt: float, alpha: float, rho0: float, st_n=None, st_nm1=None,
-               tridiag: str = "lapack") -> ProjectionResult:
+               tridiag: str = "lapack-pinned") -> ProjectionResult:
     """solvePoissonEqn (poissonEqn.f90:347-370) -> makeVelocityDivFree
     (momentumEqn.f90:999) -> computeContinuityError (auxiliaryRoutines.f90:42)
     on copies of the inputs.  psi_n / psi_nm1 are psi%ptrf_ and psi%ptrf_%ptrf_."""

@@ -99,59 +99,77 @@ __device__ __forceinline__ double rhs_cell(const RhsArgs &a, const GridK &g, int
 // ---------------------------------------------------------------------------
 template <int MODE, bool ST>
 __global__ void __launch_bounds__(kNT, 2) k_fftx_fwd(const double *__restrict__ s_in, Lay Ls, RhsArgs ra, GridK g,
-                                                  FftPlan pl, const double2 *__restrict__ twx,
-                                                  double2 *__restrict__ spec, int TJ) {
+                                                     FftPlan pl, const double2 *__restrict__ twx,
+                                                     double2 *__restrict__ spec, int logTJ, int logtpr) {
   extern __shared__ double2 sm[];
+  const int TJ = 1 << logTJ;
   const int M = g.M, nx = g.nx, ld = M + 1;
-  const long r0 = (long)blockIdx.x * TJ;
-  const int nrows = (int)min((long)TJ, g.R - r0);
+  const int r0 = blockIdx.x << logTJ;
+  const int nrows = min(TJ, (int)g.R - r0);
   double *smr = reinterpret_cast<double *>(sm);
+  const int tpr = 1 << logtpr;  // threads per row (power of two)
+  const int lane_r = threadIdx.x & (tpr - 1);
 
-  for (int t = threadIdx.x; t < TJ * nx; t += blockDim.x) {
-    const int row = t / nx, ii = t - row * nx;
-    double v = 0.0;
+  for (int row = threadIdx.x >> logtpr; row < TJ; row += (kNT >> logtpr)) {
+    double *dst = smr + (long)row * 2 * ld;
     if (row < nrows) {
-      const long rr = r0 + row;
-      const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
-      if constexpr (MODE == 0) v = s_in[at(Ls, ii + 1, j, k)];
-      else v = rhs_cell<ST>(ra, g, ii + 1, j, k);
+      const unsigned rr = (unsigned)(r0 + row);
+      const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
+      for (int ii = lane_r; ii < nx; ii += tpr) {
+        if constexpr (MODE == 0) dst[ii] = s_in[at(Ls, ii + 1, j, k)];
+        else dst[ii] = rhs_cell<ST>(ra, g, ii + 1, j, k);
+      }
+    } else {
+      for (int ii = lane_r; ii < nx; ii += tpr) dst[ii] = 0.0;
     }
-    smr[(long)row * 2 * ld + ii] = v;
   }
   __syncthreads();
-  fft_smem<double2, kEMAX, false>(sm, pl, __ffs(TJ) - 1, 1, ld, twx, 2);
+  fft_smem<double2, kEMAX, false>(sm, pl, logTJ, 1, ld, twx, 2);
 
   // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx)
   const int npair = M / 2 + 1;
-  for (int t = threadIdx.x; t < TJ * npair; t += blockDim.x) {
-    const int row = t / npair, kk = t - row * npair;
+  for (int row = threadIdx.x >> logtpr; row < TJ; row += (kNT >> logtpr)) {
     double2 *Z = sm + (long)row * ld;
-    if (kk == 0) {
-      const double2 z0 = Z[0];
-      Z[0] = mk<double2>(z0.x + z0.y, 0.0);
-      Z[M] = mk<double2>(z0.x - z0.y, 0.0);
-    } else {
-      const int km = M - kk;
-      const double2 a = Z[kk], b = Z[km];
-      const double2 wa = twx[kk], wb = twx[km];
-      // for index kk
-      double2 ep = mk<double2>(a.x + b.x, a.y - b.y);   // Z_k + conj Z_{M-k}
-      double2 em = mk<double2>(a.x - b.x, a.y + b.y);   // Z_k - conj Z_{M-k}
-      double2 t1 = cmul(wa, em);                         // W^k * em
-      Z[kk] = mk<double2>(0.5 * (ep.x + t1.y), 0.5 * (ep.y - t1.x));  // (ep - i t1)/2
-      if (km != kk) {
-        double2 fp = mk<double2>(b.x + a.x, b.y - a.y);
-        double2 fm = mk<double2>(b.x - a.x, b.y + a.y);
-        double2 t2 = cmul(wb, fm);
-        Z[km] = mk<double2>(0.5 * (fp.x + t2.y), 0.5 * (fp.y - t2.x));
+    for (int kk = lane_r; kk < npair; kk += tpr) {
+      if (kk == 0) {
+        const double2 z0 = Z[0];
+        Z[0] = mk<double2>(z0.x + z0.y, 0.0);
+        Z[M] = mk<double2>(z0.x - z0.y, 0.0);
+      } else {
+        const int km = M - kk;
+        const double2 a = Z[kk], b = Z[km];
+        const double2 wa = twx[kk], wb = twx[km];
+        double2 ep = mk<double2>(a.x + b.x, a.y - b.y);  // Z_k + conj Z_{M-k}
+        double2 em = mk<double2>(a.x - b.x, a.y + b.y);  // Z_k - conj Z_{M-k}
+        double2 t1 = cmul(wa, em);                        // W^k * em
+        Z[kk] = mk<double2>(0.5 * (ep.x + t1.y), 0.5 * (ep.y - t1.x));  // (ep - i t1)/2
+        if (km != kk) {
+          double2 fp = mk<double2>(b.x + a.x, b.y - a.y);
+          double2 fm = mk<double2>(b.x - a.x, b.y + a.y);
+          double2 t2 = cmul(wb, fm);
+          Z[km] = mk<double2>(0.5 * (fp.x + t2.y), 0.5 * (fp.y - t2.x));
+        }
       }
     }
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < TJ * ld; t += blockDim.x) {
-    const int kx = t / TJ, row = t - kx * TJ;
+  // S[kx][r0 + row]: consecutive threads take consecutive rows of one kx
+  for (int t = threadIdx.x; t < (ld << logTJ); t += kNT) {
+    const int kx = t >> logTJ, row = t & (TJ - 1);
     if (row < nrows) spec[(long)kx * g.R + r0 + row] = sm[(long)row * ld + kx];
   }
+}
+
+static int ilog2i(int v) {
+  int l = 0;
+  while ((2 << l) <= v) ++l;
+  return l;
+}
+// threads per x row: the smallest power of two >= nx/2, capped at the block size
+static int logtpr_for(int nx) {
+  int t = 1;
+  while (t < nx / 2 && t < kNT) t *= 2;
+  return ilog2i(t);
 }
 
 void launch_fftx_fwd_from_s(const double *s, Lay Ls, const GridK &g, const FftPlan &pl, const double2 *twx,
@@ -159,7 +177,8 @@ void launch_fftx_fwd_from_s(const double *s, Lay Ls, const GridK &g, const FftPl
   const int TJ = fftx_rows_per_cta(g.M);
   const long nblk = (g.R + TJ - 1) / TJ;
   RhsArgs ra{};
-  k_fftx_fwd<0, false><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(s, Ls, ra, g, pl, twx, spec, TJ);
+  k_fftx_fwd<0, false><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(s, Ls, ra, g, pl, twx, spec, ilog2i(TJ),
+                                                                         logtpr_for(g.nx));
 }
 
 void launch_fftx_fwd_rhs(const RhsArgs &ra, bool has_st, const GridK &g, const FftPlan &pl, const double2 *twx,
@@ -167,29 +186,25 @@ void launch_fftx_fwd_rhs(const RhsArgs &ra, bool has_st, const GridK &g, const F
   const int TJ = fftx_rows_per_cta(g.M);
   const long nblk = (g.R + TJ - 1) / TJ;
   Lay Ls{};
+  const int lt = ilog2i(TJ), lr = logtpr_for(g.nx);
   if (has_st)
-    k_fftx_fwd<1, true><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(nullptr, Ls, ra, g, pl, twx, spec, TJ);
+    k_fftx_fwd<1, true><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(nullptr, Ls, ra, g, pl, twx, spec, lt, lr);
   else
-    k_fftx_fwd<1, false><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(nullptr, Ls, ra, g, pl, twx, spec, TJ);
+    k_fftx_fwd<1, false><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(nullptr, Ls, ra, g, pl, twx, spec, lt, lr);
 }
 
-// Standalone split RHS (tbfp_rhs_split): s on the interior.
+// Standalone split RHS (tbfp_rhs_split): s on the interior; grid (x tiles, ny, nz).
 template <bool ST>
-__global__ void k_rhs(RhsArgs ra, GridK g, double *__restrict__ s, Lay Ls) {
-  const long n = (long)g.nx * g.R;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % g.nx) + 1;
-    const long rr = t / g.nx;
-    const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
-    s[at(Ls, i, j, k)] = rhs_cell<ST>(ra, g, i, j, k);
-  }
+__global__ void __launch_bounds__(128) k_rhs(RhsArgs ra, GridK g, double *__restrict__ s, Lay Ls) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  if (i <= g.nx) s[at(Ls, i, j, k)] = rhs_cell<ST>(ra, g, i, j, k);
 }
 
 void launch_rhs(const RhsArgs &ra, bool has_st, const GridK &g, double *s, Lay Ls, cudaStream_t st) {
-  const long n = (long)g.nx * g.R;
-  int blocks = (int)min((n + 255) / 256, 148L * 16);
-  if (has_st) k_rhs<true><<<blocks, 256, 0, st>>>(ra, g, s, Ls);
-  else k_rhs<false><<<blocks, 256, 0, st>>>(ra, g, s, Ls);
+  dim3 grid((g.nx + 127) / 128, g.ny, g.nz);
+  if (has_st) k_rhs<true><<<grid, 128, 0, st>>>(ra, g, s, Ls);
+  else k_rhs<false><<<grid, 128, 0, st>>>(ra, g, s, Ls);
 }
 
 // ---------------------------------------------------------------------------
@@ -401,65 +416,77 @@ void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const dou
 // copies the wall cell (normalGradient, bf=0), x and z ghosts are periodic.
 // The imaginary parts of X[0] and X[nx/2] are ignored, as FFTW's c2r does.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kNT, 2) k_fftx_inv(const double2 *__restrict__ spec, double *__restrict__ psi, Lay Lp,
-                                                  int hd, GridK g, FftPlan pl, const double2 *__restrict__ twx,
-                                                  double scale, int TJ) {
+__global__ void __launch_bounds__(kNT, 2) k_fftx_inv(const double2 *__restrict__ spec, double *__restrict__ psi,
+                                                     Lay Lp, int hd, GridK g, FftPlan pl,
+                                                     const double2 *__restrict__ twx, double scale, int logTJ,
+                                                     int logtpr) {
   extern __shared__ double2 sm[];
+  const int TJ = 1 << logTJ;
   const int M = g.M, nx = g.nx, ld = M + 1;
-  const long r0 = (long)blockIdx.x * TJ;
-  const int nrows = (int)min((long)TJ, g.R - r0);
-  for (int t = threadIdx.x; t < TJ * ld; t += blockDim.x) {
-    const int kx = t / TJ, row = t - kx * TJ;
+  const int r0 = blockIdx.x << logTJ;
+  const int nrows = min(TJ, (int)g.R - r0);
+  const int tpr = 1 << logtpr;
+  const int lane_r = threadIdx.x & (tpr - 1);
+  for (int t = threadIdx.x; t < (ld << logTJ); t += kNT) {
+    const int kx = t >> logTJ, row = t & (TJ - 1);
     sm[(long)row * ld + kx] = (row < nrows) ? spec[(long)kx * g.R + r0 + row] : mk<double2>(0.0, 0.0);
   }
   __syncthreads();
   // Z[k] = (X_k + conj X_{M-k}) + i conj(W^k) (X_k - conj X_{M-k}),  k = 0..M-1
   const int npair = M / 2 + 1;
-  for (int t = threadIdx.x; t < TJ * npair; t += blockDim.x) {
-    const int row = t / npair, kk = t - row * npair;
+  for (int row = threadIdx.x >> logtpr; row < TJ; row += (kNT >> logtpr)) {
     double2 *X = sm + (long)row * ld;
-    if (kk == 0) {
-      const double a = X[0].x, b = X[M].x;
-      X[0] = mk<double2>(a + b, a - b);
-    } else {
-      const int km = M - kk;
-      const double2 a = X[kk], b = X[km];
-      const double2 wa = cconj(twx[kk]), wb = cconj(twx[km]);
-      double2 ep = mk<double2>(a.x + b.x, a.y - b.y);
-      double2 em = mk<double2>(a.x - b.x, a.y + b.y);
-      double2 t1 = cmul(wa, em);
-      X[kk] = mk<double2>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
-      if (km != kk) {
-        double2 fp = mk<double2>(b.x + a.x, b.y - a.y);
-        double2 fm = mk<double2>(b.x - a.x, b.y + a.y);
-        double2 t2 = cmul(wb, fm);
-        X[km] = mk<double2>(fp.x - t2.y, fp.y + t2.x);
+    for (int kk = lane_r; kk < npair; kk += tpr) {
+      if (kk == 0) {
+        const double a = X[0].x, b = X[M].x;
+        X[0] = mk<double2>(a + b, a - b);
+      } else {
+        const int km = M - kk;
+        const double2 a = X[kk], b = X[km];
+        const double2 wa = cconj(twx[kk]), wb = cconj(twx[km]);
+        double2 ep = mk<double2>(a.x + b.x, a.y - b.y);
+        double2 em = mk<double2>(a.x - b.x, a.y + b.y);
+        double2 t1 = cmul(wa, em);
+        X[kk] = mk<double2>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
+        if (km != kk) {
+          double2 fp = mk<double2>(b.x + a.x, b.y - a.y);
+          double2 fm = mk<double2>(b.x - a.x, b.y + a.y);
+          double2 t2 = cmul(wb, fm);
+          X[km] = mk<double2>(fp.x - t2.y, fp.y + t2.x);
+        }
       }
     }
   }
   __syncthreads();
-  fft_smem<double2, kEMAX, true>(sm, pl, __ffs(TJ) - 1, 1, ld, twx, 2);
+  fft_smem<double2, kEMAX, true>(sm, pl, logTJ, 1, ld, twx, 2);
   const double *smr = reinterpret_cast<const double *>(sm);
-  for (int t = threadIdx.x; t < TJ * nx; t += blockDim.x) {
-    const int row = t / nx, ii = t - row * nx;
-    if (row >= nrows) continue;
-    const double v = smr[(long)row * 2 * ld + ii] * scale;
-    const long rr = r0 + row;
-    const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
-    const int i = ii + 1;
-    // images of (i, j, k)
-    int is[2], js[2], ks[2];
-    int ni = 1, nj = 1, nk = 1;
-    is[0] = i; js[0] = j; ks[0] = k;
-    if (i <= hd) is[ni++] = i + nx;
-    else if (i > nx - hd) is[ni++] = i - nx;
+  for (int row = threadIdx.x >> logtpr; row < nrows; row += (kNT >> logtpr)) {
+    const unsigned rr = (unsigned)(r0 + row);
+    const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
+    // ghost images of the row: first y ghost layer (wall copy), periodic z
+    int js[2], ks[2];
+    int nj = 1, nk = 1;
+    js[0] = j;
+    ks[0] = k;
     if (j == 1) js[nj++] = 0;
     else if (j == g.ny) js[nj++] = g.ny + 1;
     if (k <= hd) ks[nk++] = k + g.nz;
     else if (k > g.nz - hd) ks[nk++] = k - g.nz;
-    for (int c = 0; c < nk; ++c)
-      for (int b = 0; b < nj; ++b)
-        for (int a = 0; a < ni; ++a) psi[at(Lp, is[a], js[b], ks[c])] = v;
+    const double *src = smr + (long)row * 2 * ld;
+    for (int ii = lane_r; ii < nx; ii += tpr) {
+      const double v = src[ii] * scale;
+      const int i = ii + 1;
+      int is[2];
+      int ni = 1;
+      is[0] = i;
+      if (i <= hd) is[ni++] = i + nx;
+      else if (i > nx - hd) is[ni++] = i - nx;
+      for (int c = 0; c < nk; ++c)
+        for (int b = 0; b < nj; ++b) {
+          double *prow = psi + at(Lp, 0, js[b], ks[c]);
+          for (int a = 0; a < ni; ++a) prow[is[a] - Lp.ilo] = v;
+        }
+    }
   }
 }
 
@@ -467,7 +494,8 @@ void launch_fftx_inv(const double2 *spec, double *psi, Lay Lp, int hd, const Gri
                      const double2 *twx, double scale, cudaStream_t st) {
   const int TJ = fftx_rows_per_cta(g.M);
   const long nblk = (g.R + TJ - 1) / TJ;
-  k_fftx_inv<<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(spec, psi, Lp, hd, g, pl, twx, scale, TJ);
+  k_fftx_inv<<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(spec, psi, Lp, hd, g, pl, twx, scale, ilog2i(TJ),
+                                                               logtpr_for(g.nx));
 }
 
 // ---------------------------------------------------------------------------
@@ -528,97 +556,104 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long *o
   }
 }
 
-// Out-of-place correction fused with the continuity check: every thread owns
-// cell (i,j,k), computes its six corrected faces (the three "minus" faces are
-// recomputed with the neighbour's arithmetic, so they equal what that
-// neighbour writes) and reduces |div u| (auxiliaryRoutines.f90:71-75).
-// The periodic duplicates ux(0)=ux(nx), uz(.,.,0)=uz(.,.,nz) are the equated
-// values of vfield.f90:124-189; the uy wall faces are copied through.
+// Out-of-place correction fused with the continuity check.  Grid (x tiles of
+// 128, y chunks of kJC rows, nz); a thread owns column (i, k) of a y chunk and
+// walks it in j, so the lower y face of a cell is the upper face computed one
+// step before; the lower x face comes from the neighbouring lane (recomputed
+// by lane 0 and at i = 1).  The periodic duplicates ux(0)=ux(nx),
+// uz(.,.,0)=uz(.,.,nz) are the equated values of vfield.f90:124-189 and the uy
+// wall faces are copied through.  |div u| (auxiliaryRoutines.f90:71-75) is
+// reduced per block and folded into *maxdiv with one atomic.
+constexpr int kJC = 32;
+
 template <bool ST>
-__global__ void __launch_bounds__(256) k_correct_div(CorrArgs a, GridK g, unsigned long long *__restrict__ maxdiv) {
-  const long n = (long)g.nx * g.R;
+__global__ void __launch_bounds__(128) k_correct_div(CorrArgs a, GridK g, unsigned long long *__restrict__ maxdiv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.z + 1;
+  const int j0 = blockIdx.y * kJC + 1, j1 = min(j0 + kJC - 1, g.ny);
+  const bool valid = i <= g.nx;
+  const int lane = threadIdx.x & 31;
+  const int ic = valid ? i : g.nx;  // clamped index keeps every load in bounds
+  const int km = (k == 1) ? g.nz : k - 1;
   double vmax = 0.0;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % g.nx) + 1;
-    const long rr = t / g.nx;
-    const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
-    const double uxp = corr_x<ST>(a, g, i, j, k);
-    const double uxm = corr_x<ST>(a, g, i == 1 ? g.nx : i - 1, j, k);
-    const double uyp = (j < g.ny) ? corr_y<ST>(a, g, i, j, k) : a.uyi[at(a.Luy, i, j, k)];
-    const double uym = (j > 1) ? corr_y<ST>(a, g, i, j - 1, k) : a.uyi[at(a.Luy, i, 0, k)];
-    const double uzp = corr_z<ST>(a, g, i, j, k);
-    const double uzm = corr_z<ST>(a, g, i, j, k == 1 ? g.nz : k - 1);
-    a.uxo[at(a.Lux, i, j, k)] = uxp;
-    if (i == g.nx) a.uxo[at(a.Lux, 0, j, k)] = uxp;
-    a.uyo[at(a.Luy, i, j, k)] = uyp;
-    if (j == 1) a.uyo[at(a.Luy, i, 0, k)] = uym;
-    a.uzo[at(a.Luz, i, j, k)] = uzp;
-    if (k == g.nz) a.uzo[at(a.Luz, i, j, 0)] = uzp;
-    double dv = (uxp - uxm) * g.idxf[i - 1];
-    dv = dv + (uyp - uym) * g.idyf[j - 1];
-    dv = dv + (uzp - uzm) * g.idzf[k - 1];
-    vmax = fmax(vmax, fabs(dv));
+  double uym = (j0 > 1) ? corr_y<ST>(a, g, ic, j0 - 1, k) : a.uyi[at(a.Luy, ic, 0, k)];
+  if (valid && j0 == 1) a.uyo[at(a.Luy, i, 0, k)] = uym;
+  const double idx = g.idxf[ic - 1], idz = g.idzf[k - 1];
+  for (int j = j0; j <= j1; ++j) {
+    const double uxp = corr_x<ST>(a, g, ic, j, k);
+    const double up = __shfl_up_sync(0xffffffffu, uxp, 1);
+    const double uxm = (lane == 0 || i == 1) ? corr_x<ST>(a, g, i == 1 ? g.nx : ic - 1, j, k) : up;
+    const double uyp = (j < g.ny) ? corr_y<ST>(a, g, ic, j, k) : a.uyi[at(a.Luy, ic, j, k)];
+    const double uzp = corr_z<ST>(a, g, ic, j, k);
+    const double uzm = corr_z<ST>(a, g, ic, j, km);
+    if (valid) {
+      a.uxo[at(a.Lux, i, j, k)] = uxp;
+      if (i == g.nx) a.uxo[at(a.Lux, 0, j, k)] = uxp;
+      a.uyo[at(a.Luy, i, j, k)] = uyp;
+      a.uzo[at(a.Luz, i, j, k)] = uzp;
+      if (k == g.nz) a.uzo[at(a.Luz, i, j, 0)] = uzp;
+      double dv = (uxp - uxm) * idx;
+      dv = dv + (uyp - uym) * g.idyf[j - 1];
+      dv = dv + (uzp - uzm) * idz;
+      vmax = fmax(vmax, fabs(dv));
+    }
+    uym = uyp;
   }
   block_max_atomic(vmax, maxdiv);
 }
 
 void launch_correct_div(const CorrArgs &ca, bool has_st, const GridK &g, unsigned long long *maxdiv,
                         cudaStream_t st) {
-  const long n = (long)g.nx * g.R;
-  int blocks = (int)min((n + 255) / 256, 148L * 16);
-  if (has_st) k_correct_div<true><<<blocks, 256, 0, st>>>(ca, g, maxdiv);
-  else k_correct_div<false><<<blocks, 256, 0, st>>>(ca, g, maxdiv);
+  dim3 grid((g.nx + 127) / 128, (g.ny + kJC - 1) / kJC, g.nz);
+  if (has_st) k_correct_div<true><<<grid, 128, 0, st>>>(ca, g, maxdiv);
+  else k_correct_div<false><<<grid, 128, 0, st>>>(ca, g, maxdiv);
 }
 
 // In-place correction: each thread reads and writes only the faces it owns.
 template <bool ST>
-__global__ void __launch_bounds__(256) k_correct_inplace(CorrArgs a, GridK g) {
-  const long n = (long)g.nx * g.R;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % g.nx) + 1;
-    const long rr = t / g.nx;
-    const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
-    const double uxp = corr_x<ST>(a, g, i, j, k);
-    const double uyp = (j < g.ny) ? corr_y<ST>(a, g, i, j, k) : 0.0;
-    const double uzp = corr_z<ST>(a, g, i, j, k);
-    a.uxo[at(a.Lux, i, j, k)] = uxp;
-    if (i == g.nx) a.uxo[at(a.Lux, 0, j, k)] = uxp;
-    if (j < g.ny) a.uyo[at(a.Luy, i, j, k)] = uyp;
-    a.uzo[at(a.Luz, i, j, k)] = uzp;
-    if (k == g.nz) a.uzo[at(a.Luz, i, j, 0)] = uzp;
-  }
+__global__ void __launch_bounds__(128) k_correct_inplace(CorrArgs a, GridK g) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  if (i > g.nx) return;
+  const double uxp = corr_x<ST>(a, g, i, j, k);
+  const double uzp = corr_z<ST>(a, g, i, j, k);
+  if (j < g.ny) a.uyo[at(a.Luy, i, j, k)] = corr_y<ST>(a, g, i, j, k);
+  a.uxo[at(a.Lux, i, j, k)] = uxp;
+  if (i == g.nx) a.uxo[at(a.Lux, 0, j, k)] = uxp;
+  a.uzo[at(a.Luz, i, j, k)] = uzp;
+  if (k == g.nz) a.uzo[at(a.Luz, i, j, 0)] = uzp;
 }
 
 void launch_correct_inplace(const CorrArgs &ca, bool has_st, const GridK &g, cudaStream_t st) {
-  const long n = (long)g.nx * g.R;
-  int blocks = (int)min((n + 255) / 256, 148L * 16);
-  if (has_st) k_correct_inplace<true><<<blocks, 256, 0, st>>>(ca, g);
-  else k_correct_inplace<false><<<blocks, 256, 0, st>>>(ca, g);
+  dim3 grid((g.nx + 127) / 128, g.ny, g.nz);
+  if (has_st) k_correct_inplace<true><<<grid, 128, 0, st>>>(ca, g);
+  else k_correct_inplace<false><<<grid, 128, 0, st>>>(ca, g);
 }
 
 // computeContinuityError (auxiliaryRoutines.f90:67-80), max|div u| only.
-__global__ void __launch_bounds__(256) k_div(const double *__restrict__ ux, const double *__restrict__ uy,
+__global__ void __launch_bounds__(128) k_div(const double *__restrict__ ux, const double *__restrict__ uy,
                                              const double *__restrict__ uz, Lay Lux, Lay Luy, Lay Luz, GridK g,
                                              unsigned long long *__restrict__ maxdiv) {
-  const long n = (long)g.nx * g.R;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.z + 1;
+  const int j0 = blockIdx.y * kJC + 1, j1 = min(j0 + kJC - 1, g.ny);
   double vmax = 0.0;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % g.nx) + 1;
-    const long rr = t / g.nx;
-    const int j = (int)(rr % g.ny) + 1, k = (int)(rr / g.ny) + 1;
-    double dv = (ux[at(Lux, i, j, k)] - ux[at(Lux, i - 1, j, k)]) * g.idxf[i - 1];
-    dv = dv + (uy[at(Luy, i, j, k)] - uy[at(Luy, i, j - 1, k)]) * g.idyf[j - 1];
-    dv = dv + (uz[at(Luz, i, j, k)] - uz[at(Luz, i, j, k - 1)]) * g.idzf[k - 1];
-    vmax = fmax(vmax, fabs(dv));
+  if (i <= g.nx) {
+    const double idx = g.idxf[i - 1], idz = g.idzf[k - 1];
+    for (int j = j0; j <= j1; ++j) {
+      double dv = (ux[at(Lux, i, j, k)] - ux[at(Lux, i - 1, j, k)]) * idx;
+      dv = dv + (uy[at(Luy, i, j, k)] - uy[at(Luy, i, j - 1, k)]) * g.idyf[j - 1];
+      dv = dv + (uz[at(Luz, i, j, k)] - uz[at(Luz, i, j, k - 1)]) * idz;
+      vmax = fmax(vmax, fabs(dv));
+    }
   }
   block_max_atomic(vmax, maxdiv);
 }
 
 void launch_div(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz, const GridK &g,
                 unsigned long long *maxdiv, cudaStream_t st) {
-  const long n = (long)g.nx * g.R;
-  int blocks = (int)min((n + 255) / 256, 148L * 16);
-  k_div<<<blocks, 256, 0, st>>>(ux, uy, uz, Lux, Luy, Luz, g, maxdiv);
+  dim3 grid((g.nx + 127) / 128, (g.ny + kJC - 1) / kJC, g.nz);
+  k_div<<<grid, 128, 0, st>>>(ux, uy, uz, Lux, Luy, Luz, g, maxdiv);
 }
 
 // Raise the dynamic shared-memory limits once per process.

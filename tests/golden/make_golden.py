@@ -63,6 +63,15 @@ def make_proj(name, spec, seed, with_st=False):
         st_nm1 = tuple(O.FField(k, 1, g.nx, g.ny, g.nz) for k in ("sx", "sy", "sz"))
         for f in st_n + st_nm1:
             f.a[...] = 0.3 * rng.standard_normal(f.a.shape)
+        # clean_st_prev_bc (poissonEqn.f90:419-459): the old surface-tension levels
+        # are zero on the Neumann walls of psi (uy at j = lbj..lbj+hd and
+        # ubj-hd..ubj), which keeps the split source compatible
+        for f in (st_n[1], st_nm1[1]):
+            f.v(f.lb[0], f.ub[0], -1, 0, f.lb[2], f.ub[2])[...] = 0.0
+            f.v(f.lb[0], f.ub[0], g.ny, g.ny + 1, f.lb[2], f.ub[2])[...] = 0.0
+        # the periodic duplicate faces are equal (equatePeriodicBC, vfield.f90:124-189)
+        for lev in (st_n, st_nm1):
+            O.equate_periodic_bc(lev[0], lev[2])
     for _ in range(2):  # calls 1 and 2 of the chain, then rotate the history
         r = O.projection(m, ux, uy, uz, rho, pn, pnm1, inp.dt, inp.alpha, inp.rho0, st_n, st_nm1)
         pnm1, pn = pn, r.psi

@@ -119,20 +119,52 @@ def _case(nx, ny, nz, stretched, nb=2, radius=0.3, seed=5, rhog=0.05):
                                             ((128, 96, 64), True), ((48, 100, 24), False), ((256, 40, 12), True)])
 def test_solve_fps_random_rhs(dims, stretched):
     """solveFPS on a seeded random right-hand side vs the oracle (LAPACK path);
-    covers radix-2/4/8 and radix-3 lengths and ny not a multiple of 32."""
+    covers radix-2/4/8 and radix-3 lengths and ny not a multiple of 32.  The
+    right-hand side is made compatible with the Neumann walls (zero volume
+    integral), as every projection source is."""
     nx, ny, nz = dims
     g = Grid(nx, ny, nz, 2 * np.pi, 2.0, np.pi, stretched, 1.5)
     m = mesh_of(g)
     rng = np.random.default_rng(nx + ny + nz)
     s = Field("cl", 1, nx, ny, nz)
     s.interior()[...] = rng.standard_normal((nz, ny, nx))
+    s.interior()[...] -= np.sum(s.interior() * m.volume()) / m.s_Vg
     want = O.FField("cl", 1, nx, ny, nz)
-    O.solve_fps(m, s.interior().copy(), want, tridiag="lapack" if nx * nz <= 8192 else "thomas")
+    O.solve_fps(m, s.interior().copy(), want, tridiag="lapack-pinned" if nx * nz <= 8192 else "thomas")
     with FastPoissonSolver(g) as fps:
         p = _cuda(Field("cl", 1, nx, ny, nz))
         fps.solve_fps(p, _cuda(s))
         got = _np(p).a
     assert rel_linf(got, want.a) < TOL_P
+
+
+@pytest.mark.parametrize("stretched", [True, False])
+def test_incompatible_rhs_is_solved_with_the_defect_on_the_top_wall(stretched):
+    """A source with a non-zero volume integral has no Neumann solution.  The
+    reference's epsilon pivot (fastPoissonSolver.f90:318-322) then returns the
+    solution of the system whose defect is moved to the last y row (the top
+    wall), shifted by a constant of order defect/epsilon that the zero-mean
+    step cancels (losing most of its digits).  The library solves the same
+    consistent system with an exact gauge: the residual L psi - s vanishes
+    except on the top-wall plane, where it is uniform and equals
+    -sum(s V) / (dyf(ny) Lx Lz)."""
+    nx, ny, nz = 32, 24, 16
+    g = Grid(nx, ny, nz, 2 * np.pi, 2.0, np.pi, stretched, 1.5)
+    m = mesh_of(g)
+    rng = np.random.default_rng(5)
+    s = Field("cl", 1, nx, ny, nz)
+    s.interior()[...] = 1.0 + rng.standard_normal((nz, ny, nx))
+    with FastPoissonSolver(g) as fps:
+        p = _cuda(Field("cl", 1, nx, ny, nz))
+        fps.solve_fps(p, _cuda(s))
+        psi = O.FField("cl", 1, nx, ny, nz, _np(p).a)
+    res = O.laplacian_fps(m, psi) - s.interior()
+    scale = np.max(np.abs(s.interior()))
+    assert np.max(np.abs(res[:, :-1, :])) < 1e-12 * scale
+    defect = -np.sum(s.interior() * m.volume()) / (m.dyf[ny] * (nx * m.dx_fft if hasattr(m, "dx_fft") else g.Lx)
+                                                   * g.Lz)
+    assert np.max(np.abs(res[:, -1, :] - defect)) < 1e-11 * scale
+    assert abs(np.sum(psi.interior() * m.volume())) / m.s_Vg < 1e-12 * np.max(np.abs(psi.interior()))
 
 
 @pytest.mark.parametrize("stretched", [True, False])
