@@ -526,3 +526,328 @@ def alpha_rks(scheme: int, substep: int = 1) -> float:
     else:
         raise ValueError("invalid time integration scheme")
     return gamma[substep - 1] + xi[substep - 1]
+
+
+# ===========================================================================
+# MG_MODE: variable-coefficient oracle (PCG preconditioned by a red-black
+# Gauss-Seidel multigrid V-cycle with a direct coarsest-level solve)
+# ===========================================================================
+class Level:
+    """One multigrid level: grid metrics (coarsenGrid, grid.f90:490-544, halo 2
+    on coarse levels), red/black masks (rbgsCTOR, rbgs.f90:115-153) and the
+    1/(dc*df) metric tables (storeMetrics, rbgs.f90:489-521)."""
+
+    def __init__(self, mesh: Mesh):
+        self.m = mesh
+        nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+        i = np.arange(1, nx + 1)[None, None, :]
+        j = np.arange(1, ny + 1)[None, :, None]
+        k = np.arange(1, nz + 1)[:, None, None]
+        self.red = ((i + j + k) % 2 == 0)
+        self.black = ~self.red
+        self.invx1 = 1.0 / (mesh.dxc.r(2, nx + 1) * mesh.dxf.r(1, nx))  # invx(1,i)
+        self.invx2 = 1.0 / (mesh.dxc.r(1, nx) * mesh.dxf.r(1, nx))      # invx(2,i)
+        self.invy1 = 1.0 / (mesh.dyc.r(2, ny + 1) * mesh.dyf.r(1, ny))
+        self.invy2 = 1.0 / (mesh.dyc.r(1, ny) * mesh.dyf.r(1, ny))
+        self.invz1 = 1.0 / (mesh.dzc.r(2, nz + 1) * mesh.dzf.r(1, nz))
+        self.invz2 = 1.0 / (mesh.dzc.r(1, nz) * mesh.dzf.r(1, nz))
+
+    def coeffs(self, beta: FField):
+        """Face coefficients aR..aBa of rbgs.f90:215-220 (and pcg.f90:163-168)."""
+        nx, ny, nz = self.m.nx, self.m.ny, self.m.nz
+        B = lambda di=0, dj=0, dk=0: beta.v(1 + di, nx + di, 1 + dj, ny + dj, 1 + dk, nz + dk)  # noqa: E731
+        bc = B()
+        aR = 0.5 * (B(di=1) + bc) * self.invx1[None, None, :]
+        aL = 0.5 * (bc + B(di=-1)) * self.invx2[None, None, :]
+        aT = 0.5 * (B(dj=1) + bc) * self.invy1[None, :, None]
+        aBo = 0.5 * (bc + B(dj=-1)) * self.invy2[None, :, None]
+        aF = 0.5 * (B(dk=1) + bc) * self.invz1[:, None, None]
+        aBa = 0.5 * (bc + B(dk=-1)) * self.invz2[:, None, None]
+        return aR, aL, aT, aBo, aF, aBa
+
+
+def coarse_mesh(m: Mesh) -> Mesh:
+    """coarsenGrid (grid.f90:490-544): half the cells, same box and stretching,
+    coordinates recomputed with the reference formulas, halo 2."""
+    return Mesh(m.nx // 2, m.ny // 2, m.nz // 2, m.Lx, m.Ly, m.Lz, y_uniform=m.y_uniform, gamma=m.gamma, hd=2)
+
+
+def apply_L(lev: Level, p: FField, beta: FField, coeffs=None) -> np.ndarray:
+    """L_beta p on the interior: the operator of computeQv (pcg.f90:171-176) and
+    computeResiduals (rbgs.f90:308-317)."""
+    m = lev.m
+    nx, ny, nz = m.nx, m.ny, m.nz
+    aR, aL, aT, aBo, aF, aBa = coeffs or lev.coeffs(beta)
+    P = lambda di=0, dj=0, dk=0: p.v(1 + di, nx + di, 1 + dj, ny + dj, 1 + dk, nz + dk)  # noqa: E731
+    c = P()
+    return (aR * (P(di=1) - c) - aL * (c - P(di=-1)) + aT * (P(dj=1) - c) - aBo * (c - P(dj=-1))
+            + aF * (P(dk=1) - c) - aBa * (c - P(dk=-1)))
+
+
+def correct_full_neumann(m: Mesh, p: FField) -> None:
+    """correctFullNeumann (rbgs.f90:403-446): remove the unweighted interior mean
+    from the whole array (halo included)."""
+    avg = float(np.sum(p.interior())) / (m.nx * m.ny * m.nz)
+    p.a -= avg
+
+
+def rbgs_iterate(lev: Level, p: FField, beta: FField, q: np.ndarray, n_iter: int, reset: bool, coeffs=None) -> None:
+    """iterateGS (rbgs.f90:186-272): red sweep, boundary update, black sweep,
+    boundary update, full-Neumann mean removal; every colour is updated from the
+    values (and ghosts) left by the previous boundary update."""
+    m = lev.m
+    nx, ny, nz = m.nx, m.ny, m.nz
+    if reset:
+        p.a[...] = 0.0
+    aR, aL, aT, aBo, aF, aBa = coeffs or lev.coeffs(beta)
+    den = aR + aL + aT + aBo + aF + aBa
+    P = lambda di=0, dj=0, dk=0: p.v(1 + di, nx + di, 1 + dj, ny + dj, 1 + dk, nz + dk)  # noqa: E731
+    for _ in range(n_iter):
+        for mask in (lev.red, lev.black):
+            new = (-q + (aR * P(di=1) + aL * P(di=-1)) + (aT * P(dj=1) + aBo * P(dj=-1))
+                   + (aF * P(dk=1) + aBa * P(dk=-1))) / den
+            c = P()
+            c[mask] = new[mask]
+            update_boundaries_cl_channel(p)
+        correct_full_neumann(m, p)
+
+
+def compute_residuals(lev: Level, p: FField, beta: FField, q_full: FField, coeffs=None):
+    """computeResiduals (rbgs.f90:276-333): resV = q - L_beta p and
+    res = ||resV||_2 / (||q||_2 + tiny), the q norm over q's whole array."""
+    resV = q_full.interior() - apply_L(lev, p, beta, coeffs)
+    res = math.sqrt(float(np.sum(resV * resV))) / (math.sqrt(float(np.sum(q_full.a * q_full.a))) + TINY64)
+    return resV, res
+
+
+def restriction(mf: Mesh, mc: Mesh, qf: np.ndarray) -> np.ndarray:
+    """restrictionOp3D (interpolation.f90:80-124): trilinear restriction from the
+    fine centroids to the coarse centroids (interior arrays)."""
+    xf, yf, zf = mf.xc.r(1, mf.nx), mf.yc.r(1, mf.ny), mf.zc.r(1, mf.nz)
+    xc, yc, zc = mc.xc.r(1, mc.nx), mc.yc.r(1, mc.ny), mc.zc.r(1, mc.nz)
+    xo, xe = xf[0::2], xf[1::2]  # xf(2i-1), xf(2i)
+    yo, ye = yf[0::2], yf[1::2]
+    zo, ze = zf[0::2], zf[1::2]
+    X1, X2 = (xe - xc)[None, None, :], (xc - xo)[None, None, :]
+    Y1, Y2 = (ye - yc)[None, :, None], (yc - yo)[None, :, None]
+    Z1, Z2 = (ze - zc)[:, None, None], (zc - zo)[:, None, None]
+    V = ((xe - xo)[None, None, :] * (ye - yo)[None, :, None]) * (ze - zo)[:, None, None]
+    q = lambda a, b, c: qf[c::2, b::2, a::2]  # qf(2i-1+a, 2j-1+b, 2k-1+c)  # noqa: E731
+    s = (X1 * Y1) * Z1 * q(0, 0, 0)
+    s = s + (X2 * Y1) * Z1 * q(1, 0, 0)
+    s = s + (X1 * Y2) * Z1 * q(0, 1, 0)
+    s = s + (X2 * Y2) * Z1 * q(1, 1, 0)
+    s = s + (X1 * Y1) * Z2 * q(0, 0, 1)
+    s = s + (X2 * Y1) * Z2 * q(1, 0, 1)
+    s = s + (X1 * Y2) * Z2 * q(0, 1, 1)
+    s = s + (X2 * Y2) * Z2 * q(1, 1, 1)
+    return s / V
+
+
+def prolongation(mf: Mesh, mc: Mesh, pc: FField) -> np.ndarray:
+    """prolongationOp3D (interpolation.f90:129-181): trilinear interpolation of
+    the coarse field (ghosts included) to the fine centroids; fine cell i lies
+    between coarse centroids ih = i/2 (integer division) and ih+1."""
+    nxf, nyf, nzf = mf.nx, mf.ny, mf.nz
+    xf, yf, zf = mf.xc.r(1, nxf), mf.yc.r(1, nyf), mf.zc.r(1, nzf)
+    ih = np.arange(1, nxf + 1) // 2
+    jh = np.arange(1, nyf + 1) // 2
+    kh = np.arange(1, nzf + 1) // 2
+    xc0, xc1 = mc.xc.v[ih - mc.xc.lb], mc.xc.v[ih + 1 - mc.xc.lb]
+    yc0, yc1 = mc.yc.v[jh - mc.yc.lb], mc.yc.v[jh + 1 - mc.yc.lb]
+    zc0, zc1 = mc.zc.v[kh - mc.zc.lb], mc.zc.v[kh + 1 - mc.zc.lb]
+    X1, X2 = (xc1 - xf)[None, None, :], (xf - xc0)[None, None, :]
+    Y1, Y2 = (yc1 - yf)[None, :, None], (yf - yc0)[None, :, None]
+    Z1, Z2 = (zc1 - zf)[:, None, None], (zf - zc0)[:, None, None]
+    V = ((xc1 - xc0)[None, None, :] * (yc1 - yc0)[None, :, None]) * (zc1 - zc0)[:, None, None]
+    lb = pc.lb
+    Q = lambda a, b, c: pc.a[(kh + c - lb[2])[:, None, None], (jh + b - lb[1])[None, :, None],  # noqa: E731
+                             (ih + a - lb[0])[None, None, :]]
+    s = (X1 * Y1) * Z1 * Q(0, 0, 0)
+    s = s + (X2 * Y1) * Z1 * Q(1, 0, 0)
+    s = s + (X1 * Y2) * Z1 * Q(0, 1, 0)
+    s = s + (X2 * Y2) * Z1 * Q(1, 1, 0)
+    s = s + (X1 * Y1) * Z2 * Q(0, 0, 1)
+    s = s + (X2 * Y1) * Z2 * Q(1, 0, 1)
+    s = s + (X1 * Y2) * Z2 * Q(0, 1, 1)
+    s = s + (X2 * Y2) * Z2 * Q(1, 1, 1)
+    return s / V
+
+
+def coarse_direct_solve(lev: Level, p: FField, beta: FField, s: np.ndarray) -> None:
+    """solveMat (poissMat.f90:289-312): the coarsest-level system assembled as
+    V*(-L_beta) with true Neumann walls (computeInternalMatrixValues :714-772 and
+    the boundary values :802-971), right-hand side -V*s (computeRHS :1081-1118;
+    the homogeneous error boundary conditions add nothing), bordered by the
+    Lagrange-multiplier row sum(p) = 0 (:467-503, :776-798) and solved directly
+    (the reference factorises with MUMPS on every call)."""
+    m = lev.m
+    nx, ny, nz = m.nx, m.ny, m.nz
+    n = nx * ny * nz
+    idx = lambda i, j, k: ((k % nz) * ny + j) * nx + (i % nx)  # noqa: E731
+    aR, aL, aT, aBo, aF, aBa = lev.coeffs(beta)
+    V = m.volume()
+    A = np.zeros((n + 1, n + 1))
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                r = idx(i, j, k)
+                v = V[k, j, i]
+                terms = [(aR[k, j, i], idx(i + 1, j, k)), (aL[k, j, i], idx(i - 1, j, k)),
+                         (aF[k, j, i], idx(i, j, k + 1)), (aBa[k, j, i], idx(i, j, k - 1))]
+                if j < ny - 1:
+                    terms.append((aT[k, j, i], idx(i, j + 1, k)))
+                if j > 0:
+                    terms.append((aBo[k, j, i], idx(i, j - 1, k)))
+                for a, c in terms:
+                    A[r, c] -= v * a
+                    A[r, r] += v * a
+                A[r, n] = 1.0
+                A[n, r] = 1.0
+    b = np.zeros(n + 1)
+    b[:n] = (-V * s).reshape(-1)
+    x = np.linalg.solve(A, b)
+    p.v(1, nx, 1, ny, 1, nz)[...] = x[:n].reshape(nz, ny, nx)
+    update_boundaries_cl_channel(p)
+
+
+class MGOracle:
+    """multiGrid + rbgs + poissMat + pcg restated (multiGrid.f90, rbgs.f90,
+    poissMat.f90, pcg.f90) for one rank, all in FP64."""
+
+    def __init__(self, mesh: Mesh, n_levels: int = 6, n_pre: int = 2, n_post: int = 2, tol_mg: float = 0.4,
+                 max_iter_mg: int = 100, tol_pcg: float = 1e-10, max_iter_pcg: int = 100):
+        for l in range(1, n_levels):  # checkLevelsNumber (multiGrid.f90:116-145)
+            for n in (mesh.nx, mesh.ny, mesh.nz):
+                if n % (2 ** l):
+                    raise ValueError("grid not divisible for the requested multigrid levels")
+        self.n_levels, self.n_pre, self.n_post = n_levels, n_pre, n_post
+        self.tol_mg, self.max_iter_mg = tol_mg, max_iter_mg
+        self.tol_pcg, self.max_iter_pcg = tol_pcg, max_iter_pcg
+        meshes = [mesh]
+        for _ in range(n_levels - 1):
+            meshes.append(coarse_mesh(meshes[-1]))
+        self.levels = [Level(m) for m in meshes]  # index 0 = finest (level nLevels)
+        self.mg_iters = []
+
+    def _field(self, li):
+        m = self.levels[li].m
+        return FField("cl", 1, m.nx, m.ny, m.nz)
+
+    def restrict_beta(self, beta: FField):
+        """restrictField(beta) on every level (field.f90:1442-1470) with boundary updates."""
+        betas = [beta]
+        for li in range(1, self.n_levels):
+            mf, mc = self.levels[li - 1].m, self.levels[li].m
+            bc = self._field(li)
+            bc.v(1, mc.nx, 1, mc.ny, 1, mc.nz)[...] = restriction(mf, mc, betas[-1].interior())
+            update_boundaries_cl_channel(bc)
+            betas.append(bc)
+        return betas
+
+    def vcycle(self, li: int, p: FField, betas, s_full: FField, coeffs) -> None:
+        """mgVcycle (multiGrid.f90:186-232); li = 0 is the finest level."""
+        lev = self.levels[li]
+        if li == self.n_levels - 1:
+            coarse_direct_solve(lev, p, betas[li], s_full.interior())
+            return
+        rbgs_iterate(lev, p, betas[li], s_full.interior(), self.n_pre, reset=(li != 0), coeffs=coeffs[li])
+        resV, _ = compute_residuals(lev, p, betas[li], s_full, coeffs[li])
+        mc = self.levels[li + 1].m
+        sc = self._field(li + 1)
+        sc.v(1, mc.nx, 1, mc.ny, 1, mc.nz)[...] = restriction(lev.m, mc, resV)
+        update_boundaries_cl_channel(sc)
+        pc = self._field(li + 1)
+        self.vcycle(li + 1, pc, betas, sc, coeffs)
+        m = lev.m
+        p.v(1, m.nx, 1, m.ny, 1, m.nz)[...] += prolongation(m, mc, pc)
+        update_boundaries_cl_channel(p)
+        rbgs_iterate(lev, p, betas[li], s_full.interior(), self.n_post, reset=False, coeffs=coeffs[li])
+
+    def solve_mg(self, p: FField, betas, s_full: FField, coeffs) -> int:
+        """solveMG (multiGrid.f90:165-182) with continueIterating (:237-279)."""
+        lev = self.levels[0]
+        _, res = compute_residuals(lev, p, betas[0], s_full, coeffs[0])
+        it = 0
+        while True:
+            if it == self.max_iter_mg:
+                break
+            if not res > self.tol_mg:
+                break
+            it += 1
+            self.vcycle(0, p, betas, s_full, coeffs)
+            _, res = compute_residuals(lev, p, betas[0], s_full, coeffs[0])
+        return it
+
+    def solve_pcg(self, psi: FField, beta: FField, q: np.ndarray):
+        """solvePCG (pcg.f90:103-140): psi is the initial guess and the result
+        (ghosts updated); returns (iterations, ||r||/||q||)."""
+        lev = self.levels[0]
+        m = lev.m
+        nx, ny, nz = m.nx, m.ny, m.nz
+        betas = self.restrict_beta(beta)
+        coeffs = [lv.coeffs(b) for lv, b in zip(self.levels, betas)]
+        qf = FField("cl", 1, nx, ny, nz)
+        qf.v(1, nx, 1, ny, 1, nz)[...] = q
+        resV, _ = compute_residuals(lev, psi, beta, qf, coeffs[0])
+        r = FField("cl", 1, nx, ny, nz)
+        r.v(1, nx, 1, ny, 1, nz)[...] = resV
+        d = FField("cl", 1, nx, ny, nz)
+        self.mg_iters.append(self.solve_mg(d, betas, r, coeffs))
+        deltaN = float(np.sum(r.interior() * d.interior()))
+        qn = math.sqrt(float(np.sum(q * q)) + TINY64)
+        it = 0
+        res = math.sqrt(float(np.sum(r.interior() ** 2))) / qn
+        while True:
+            if it == self.max_iter_pcg:
+                break
+            res = math.sqrt(float(np.sum(r.interior() ** 2))) / qn
+            if not res > self.tol_pcg:
+                break
+            it += 1
+            qv = apply_L(lev, d, beta, coeffs[0])
+            alpha = deltaN / float(np.sum(d.interior() * qv))
+            psi.a += alpha * d.a
+            r.v(1, nx, 1, ny, 1, nz)[...] -= alpha * qv
+            d0 = d.interior().copy()
+            d.a[...] = 0.0
+            self.mg_iters.append(self.solve_mg(d, betas, r, coeffs))
+            delta0 = deltaN
+            deltaN = float(np.sum(r.interior() * d.interior()))
+            gamma = deltaN / delta0
+            d0 = d.interior() + gamma * d0
+            d.v(1, nx, 1, ny, 1, nz)[...] = d0
+            update_boundaries_cl_channel(d)
+        update_boundaries_cl_channel(psi)
+        return it, res
+
+
+def compute_source_mg(mesh: Mesh, ux: FField, uy: FField, uz: FField) -> np.ndarray:
+    """computeSource MG (poissonEqn.f90:155-190): s = div u* with per-index metrics."""
+    return divergence(mesh, ux, uy, uz)
+
+
+def compute_beta(mesh: Mesh, rho: FField, dt: float, alpha: float) -> FField:
+    """computeBeta (poissonEqn.f90:311-342): beta = dt*alpha/rho, then its boundary update."""
+    b = FField("cl", 1, mesh.nx, mesh.ny, mesh.nz)
+    b.v(1, mesh.nx, 1, mesh.ny, 1, mesh.nz)[...] = (dt * alpha) / rho.interior()
+    update_boundaries_cl_channel(b)
+    return b
+
+
+def add_pressure_grad(mesh: Mesh, ux: FField, uy: FField, uz: FField, p: FField, rho: FField,
+                      dt: float, alpha: float) -> None:
+    """makeVelocityDivFree MG = addPressureGrad (momentumEqn.f90:795-869, :980-993),
+    loop ranges of setEqnBounds, then the periodic equate."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+
+    def upd(u, i0, i1, j0, j1, k0, k1, di, dj, dk, dc):
+        S = lambda f, o=0: f.v(i0 + di * o, i1 + di * o, j0 + dj * o, j1 + dj * o, k0 + dk * o, k1 + dk * o)  # noqa: E731
+        invrho = 0.5 * (1.0 / S(rho, 1) + 1.0 / S(rho))
+        tgt = u.v(i0, i1, j0, j1, k0, k1)
+        tgt -= dt * alpha * invrho * (S(p, 1) - S(p)) / dc
+
+    upd(ux, 0, nx, 1, ny, 1, nz, 1, 0, 0, mesh.dxc.r(1, nx + 1)[None, None, :])
+    upd(uy, 1, nx, 1, ny - 1, 1, nz, 0, 1, 0, mesh.dyc.r(2, ny)[None, :, None])
+    upd(uz, 1, nx, 1, ny, 0, nz, 0, 0, 1, mesh.dzc.r(1, nz + 1)[:, None, None])
+    equate_periodic_bc(ux, uz)
