@@ -184,6 +184,23 @@ int tbfp_projection_dev(tbfp_handle *h, const double *ux_in, const double *uy_in
                         const double *const *st_n, const double *const *st_nm1,
                         double dt, double alpha, double rho0, double *psi, tbfp_stats *stats);
 
+/* --- solveFPS without device allocation ------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+   memory (inside a CUDA graph capture, under a memory pool another runtime
+   owns, or a driver that only hands over arrays it allocated itself): the same
+   solve as tbfp_solve_fps_dev, on the caller's device arrays s and psi, with no
+   handle.  Work spectrum and set-up tables live in one static device array that
+   every GPU loading the library holds until exit, which limits the grid to
+   (nx/2+1)*ny*nz <= TBFP_NOALLOC_MAX_SPECTRUM complex entries (64 MiB),
+   nx <= 4096, ny <= 2048, nz <= 2048 (else TBFP_EUNSUPPORTED).  The first call
+   on a device looks up the array's address; make it before any stream capture.
+   All calls share the array: calls that overlap on the GPU race.  Runs on
+   d->stream (NULL: the legacy default stream), synchronous; error text via
+   tbfp_last_error(NULL).  Only the fields nx, ny, nz, hd_psi, dx_fft, dz_fft,
+   dxf, dyf, dyc, dzf, s_Vg, device and stream of d are read. */
+#define TBFP_NOALLOC_MAX_SPECTRUM 4194304
+int tbfp_solve_fps_noalloc(const tbfp_desc *d, const double *s, double *psi);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,6 +87,7 @@ PROTOTYPES = {
     "tbfp_projection": (C.c_int, [_H, _P, _P, _P, _P, _P, _P, _PP, _PP, _D, _D, _D, _P, C.POINTER(TbfpStats)]),
     "tbfp_projection_dev": (C.c_int, [_H, _P, _P, _P, _P, _P, _P, _P, _P, _P, _PP, _PP, _D, _D, _D, _P,
                                       C.POINTER(TbfpStats)]),
+    "tbfp_solve_fps_noalloc": (C.c_int, [C.POINTER(TbfpDesc), _P, _P]),
 }
 
 _lib = None

@@ -16,7 +16,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "lib", "libtbfp.so")
-SOURCES = ["tbfp_api.cu", "tbfp_kernels.cu"]
+SOURCES = ["tbfp_api.cu", "tbfp_kernels.cu", "tbfp_noalloc.cu"]
 HEADERS = ["tbfp_kernels.cuh", "fft_smem.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

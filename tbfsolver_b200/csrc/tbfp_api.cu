@@ -24,6 +24,10 @@ struct DevBuf {
 
 }  // namespace
 
+namespace tbfp {
+void set_global_error(const std::string &msg) { g_create_error = msg; }
+}  // namespace tbfp
+
 struct tbfp_handle {
   int nx = 0, ny = 0, nz = 0, nkx = 0;
   long R = 0;

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "fft_smem.cuh"
 
 namespace tbfp {
@@ -50,6 +52,9 @@ struct CorrArgs {
   double r;  // dt*alpha
   double invrho0;
 };
+
+// Error text returned by tbfp_last_error(NULL) (defined in tbfp_api.cu).
+void set_global_error(const std::string &msg);
 
 // Kernel launchers (defined in tbfp_kernels.cu).
 void launch_recip(const double *rho, double *irho, long n, cudaStream_t st);
