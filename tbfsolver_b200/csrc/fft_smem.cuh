@@ -103,14 +103,26 @@ template <typename V, int R, bool INV> __device__ __forceinline__ void bfly(V *v
   else bfly8<V, INV>(v);
 }
 
-// One Stockham pass of radix R.  Butterfly b of a length-n transform reads
-// x[b + r*n/R], applies twiddle exp(-+2*pi*i*(b mod Ns)*r/(Ns*R)), transforms,
-// and writes y[(b/Ns)*Ns*R + b mod Ns + r*Ns].  Butterflies are numbered
-// batch-fastest (b = jj*nb + batch), nb and Ns are powers of two (the plan puts
-// its single radix-3 pass last), so all index arithmetic is shifts and masks.
-// QMAX bounds the butterflies a thread owns (ceil(elements per thread / R)).
-template <typename V, int R, int QMAX, bool INV>
-__device__ __forceinline__ void stockham_pass(V *buf, int n, int lognb, int es, int bs, int logNs,
+// Shared-memory slot of element e of a sequence: one empty slot after every 8
+// elements, which makes the stride-R writes of the early Stockham passes (and
+// the reads of the late ones) free of bank conflicts for 16-byte elements.
+__host__ __device__ __forceinline__ int pad8(int e) { return e + (e >> 3); }
+
+// One Stockham pass of radix R over a group of G threads (a warp, G = 32, or a
+// whole block).  Butterfly b of a length-n transform reads x[b + r*n/R],
+// applies twiddle exp(-+2*pi*i*(b mod Ns)*r/(Ns*R)), transforms, and writes
+// y[(b/Ns)*Ns*R + b mod Ns + r*Ns].  Butterflies are numbered batch-fastest
+// (b = jj*nb + batch), nb and Ns are powers of two (the plan puts its single
+// radix-3 pass last), so all index arithmetic is shifts and masks.  QMAX
+// bounds the butterflies a thread owns (ceil(elements per thread / R)).
+template <int G>
+__device__ __forceinline__ void group_sync() {
+  if constexpr (G == 32) __syncwarp();
+  else __syncthreads();
+}
+
+template <typename V, int R, int QMAX, bool INV, int G>
+__device__ __forceinline__ void stockham_pass(V *buf, int tid, int n, int lognb, int es, int bs, int logNs,
                                               const V *__restrict__ tw, int twmul) {
   const int per = n / R;
   const int total = per << lognb;
@@ -119,14 +131,14 @@ __device__ __forceinline__ void stockham_pass(V *buf, int n, int lognb, int es, 
   V v[QMAX][R];
 #pragma unroll
   for (int q = 0; q < QMAX; ++q) {
-    const int b = threadIdx.x + q * blockDim.x;
+    const int b = tid + q * G;
     if (b < total) {
       const int bt = b & nbm, jj = b >> lognb;
       const V *base = buf + bt * bs;
       const int k0 = jj & Nsm;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        V x = base[(jj + r * per) * es];
+        V x = base[pad8(jj + r * per) * es];
         if (r > 0) {
           V w = tw[(k0 * r * stride_tw) * twmul];
           if (INV) w.y = -w.y;
@@ -136,43 +148,44 @@ __device__ __forceinline__ void stockham_pass(V *buf, int n, int lognb, int es, 
       }
     }
   }
-  __syncthreads();
+  group_sync<G>();
 #pragma unroll
   for (int q = 0; q < QMAX; ++q) {
-    const int b = threadIdx.x + q * blockDim.x;
+    const int b = tid + q * G;
     if (b < total) {
       const int bt = b & nbm, jj = b >> lognb;
       bfly<V, R, INV>(v[q]);
       V *base = buf + bt * bs;
       const int d = (((jj >> logNs) * R) << logNs) + (jj & Nsm);
 #pragma unroll
-      for (int r = 0; r < R; ++r) base[(d + (r << logNs)) * es] = v[q][r];
+      for (int r = 0; r < R; ++r) base[pad8(d + (r << logNs)) * es] = v[q][r];
     }
   }
-  __syncthreads();
+  group_sync<G>();
 }
 
-// Full transform of nb = 2^lognb sequences.  EMAX = upper bound of n*nb/blockDim.x.
-template <typename V, int EMAX, bool INV>
-__device__ void fft_smem(V *buf, const FftPlan &pl, int lognb, int es, int bs, const V *__restrict__ tw,
-                         int twmul) {
+// Full transform of nb = 2^lognb sequences by a group of G threads (tid is the
+// thread's index in the group).  EMAX = upper bound of n*nb/G.
+template <typename V, int EMAX, bool INV, int G>
+__device__ void fft_group(V *buf, int tid, const FftPlan &pl, int lognb, int es, int bs, const V *__restrict__ tw,
+                          int twmul) {
   int logNs = 0;
   for (int p = 0; p < pl.nrad; ++p) {
     const int R = pl.rad[p];
     switch (R) {
       case 2:
-        stockham_pass<V, 2, (EMAX + 1) / 2, INV>(buf, pl.n, lognb, es, bs, logNs, tw, twmul);
+        stockham_pass<V, 2, (EMAX + 1) / 2, INV, G>(buf, tid, pl.n, lognb, es, bs, logNs, tw, twmul);
         logNs += 1;
         break;
       case 3:  // always the last pass
-        stockham_pass<V, 3, (EMAX + 2) / 3, INV>(buf, pl.n, lognb, es, bs, logNs, tw, twmul);
+        stockham_pass<V, 3, (EMAX + 2) / 3, INV, G>(buf, tid, pl.n, lognb, es, bs, logNs, tw, twmul);
         break;
       case 4:
-        stockham_pass<V, 4, (EMAX + 3) / 4, INV>(buf, pl.n, lognb, es, bs, logNs, tw, twmul);
+        stockham_pass<V, 4, (EMAX + 3) / 4, INV, G>(buf, tid, pl.n, lognb, es, bs, logNs, tw, twmul);
         logNs += 2;
         break;
       default:
-        stockham_pass<V, 8, (EMAX + 7) / 8, INV>(buf, pl.n, lognb, es, bs, logNs, tw, twmul);
+        stockham_pass<V, 8, (EMAX + 7) / 8, INV, G>(buf, tid, pl.n, lognb, es, bs, logNs, tw, twmul);
         logNs += 3;
         break;
     }

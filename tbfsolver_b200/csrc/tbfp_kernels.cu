@@ -14,24 +14,54 @@
 
 namespace tbfp {
 
-constexpr int kNT = 256;    // threads per CTA of the transform kernels
-constexpr int kEMAX = 8;    // complex elements per thread in the transform kernels
-constexpr int kWPB = 4;     // warps per CTA of the tridiagonal kernel
+constexpr int kNT = 256;   // threads per CTA of the transform kernels (8 warps)
+constexpr int kNW = kNT / 32;
+constexpr int kWPB = 4;    // warps per CTA of the tridiagonal kernel
 
 static int pow2_floor(int v) {
   int p = 1;
   while (2 * p <= v) p *= 2;
   return p;
 }
-// Longest transform one CTA holds (all of it must fit the register budget).
-int fft_max_length() { return kEMAX * kNT; }
-// Rows (x) or columns (z) per CTA: the largest power of two keeping
-// n*rows <= kEMAX*kNT complex elements in the tile.
-int fftx_rows_per_cta(int M) { return (kEMAX * kNT) / M > 0 ? pow2_floor((kEMAX * kNT) / M) : 1; }
-int fftz_cols_per_cta(int nz) { return (kEMAX * kNT) / nz > 0 ? pow2_floor((kEMAX * kNT) / nz) : 1; }
-size_t fftx_smem_bytes(int M) { return (size_t)fftx_rows_per_cta(M) * (M + 1) * sizeof(double2); }
-size_t fftz_smem_bytes(int nz) { return (size_t)fftz_cols_per_cta(nz) * nz * sizeof(double2); }
-size_t tridiag_smem_bytes(int ny) { return (size_t)kWPB * ny * (sizeof(double2) + 2 * sizeof(double)); }
+static int ilog2i(int v) {
+  int l = 0;
+  while ((2 << l) <= v) ++l;
+  return l;
+}
+// Each warp transforms its own sequences (rows of x, columns of z) with
+// __syncwarp only; a warp holds 8 complex values per lane (16 for lengths 512).
+// Sequences per warp: the largest power of two keeping n*spw <= 256, or 1.
+static int seq_per_warp(int n) { return n >= 256 ? 1 : pow2_floor(256 / n); }
+static int elems_per_lane(int n) { return n * seq_per_warp(n) / 32; }
+int fft_max_length() { return 512; }
+int fftx_rows_per_cta(int M) { return kNW * seq_per_warp(M); }
+int fftz_cols_per_cta(int nz) { return kNW * seq_per_warp(nz); }
+// Row stride of an x tile (complex slots): holds pad8(M)+1 slots; with nb rows
+// per warp interleaved in a phase of 8 lanes, rows must land on distinct
+// 16-byte bank groups: stride = (8/nb)*odd (mod 8) for nb < 8, odd for nb >= 8.
+static int x_row_stride(int M) {
+  const int nb = seq_per_warp(M);
+  int ld = pad8(M) + 1;
+  if (nb == 1) return ld;
+  const int want = nb >= 8 ? 1 : 8 / nb;  // required residue pattern
+  while (!((ld % 8) % want == 0 && ((ld % 8) / want) % 2 == 1)) ++ld;
+  return ld;
+}
+// Row stride of a z tile: the tile's 8*nb columns plus a skew for small nb.
+static int z_row_stride(int nz) {
+  const int nb = seq_per_warp(nz);
+  return 8 * nb + (nb <= 4 ? nb : 0);
+}
+size_t fftx_smem_bytes(int M) { return (size_t)fftx_rows_per_cta(M) * x_row_stride(M) * sizeof(double2); }
+size_t fftz_smem_bytes(int nz) { return (size_t)z_row_stride(nz) * (pad8(nz - 1) + 1) * sizeof(double2); }
+// per warp: (rows per lane + 1) x 33 slots of (complex rhs, two real coefficients)
+static int tri_rows_per_lane(int ny) {
+  const int NL = ny / 2 < 32 ? ny / 2 : 32;
+  return (ny + NL - 1) / NL;
+}
+size_t tridiag_smem_bytes(int ny) {
+  return (size_t)kWPB * 33 * tri_rows_per_lane(ny) * (sizeof(double2) + 2 * sizeof(double));
+}
 
 // ---------------------------------------------------------------------------
 // 1/rho over the whole (halo-inclusive) density array.
@@ -97,100 +127,97 @@ __device__ __forceinline__ double rhs_cell(const RhsArgs &a, const GridK &g, int
 // Forward x transform of a tile of rows: real rows (from s, or computed by the
 // split RHS) -> half-length complex FFT -> r2c post-processing -> S[kx][row].
 // ---------------------------------------------------------------------------
-template <int MODE, bool ST>
+template <int MODE, bool ST, int EMAX>
 __global__ void __launch_bounds__(kNT, 2) k_fftx_fwd(const double *__restrict__ s_in, Lay Ls, RhsArgs ra, GridK g,
-                                                     FftPlan pl, const double2 *__restrict__ twx,
-                                                     double2 *__restrict__ spec, int logTJ, int logtpr) {
+                                                  FftPlan pl, const double2 *__restrict__ twx,
+                                                  double2 *__restrict__ spec, int logrpw, int ld) {
   extern __shared__ double2 sm[];
+  const int RPW = 1 << logrpw;         // rows per warp
+  const int logTJ = logrpw + 3;        // kNW = 8 warps
   const int TJ = 1 << logTJ;
-  const int M = g.M, nx = g.nx, ld = M + 1;
+  const int M = g.M, nx = g.nx;
   const int r0 = blockIdx.x << logTJ;
   const int nrows = min(TJ, (int)g.R - r0);
-  double *smr = reinterpret_cast<double *>(sm);
-  const int tpr = 1 << logtpr;  // threads per row (power of two)
-  const int lane_r = threadIdx.x & (tpr - 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *wsm = sm + (long)warp * RPW * ld;  // this warp's rows
+  double *wsr = reinterpret_cast<double *>(wsm);
 
-  for (int row = threadIdx.x >> logtpr; row < TJ; row += (kNT >> logtpr)) {
-    double *dst = smr + (long)row * 2 * ld;
+  for (int rl = 0; rl < RPW; ++rl) {
+    const int row = warp * RPW + rl;
+    double *dst = wsr + (long)rl * 2 * ld;
     if (row < nrows) {
       const unsigned rr = (unsigned)(r0 + row);
       const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
-      for (int ii = lane_r; ii < nx; ii += tpr) {
-        if constexpr (MODE == 0) dst[ii] = s_in[at(Ls, ii + 1, j, k)];
-        else dst[ii] = rhs_cell<ST>(ra, g, ii + 1, j, k);
+#pragma unroll 4
+      for (int ii = lane; ii < nx; ii += 32) {
+        const int slot = 2 * pad8(ii >> 1) + (ii & 1);
+        if constexpr (MODE == 0) dst[slot] = s_in[at(Ls, ii + 1, j, k)];
+        else dst[slot] = rhs_cell<ST>(ra, g, ii + 1, j, k);
       }
     } else {
-      for (int ii = lane_r; ii < nx; ii += tpr) dst[ii] = 0.0;
+      for (int ii = lane; ii < nx; ii += 32) dst[2 * pad8(ii >> 1) + (ii & 1)] = 0.0;
     }
   }
-  __syncthreads();
-  fft_smem<double2, kEMAX, false>(sm, pl, logTJ, 1, ld, twx, 2);
+  __syncwarp();
+  fft_group<double2, EMAX, false, 32>(wsm, lane, pl, logrpw, 1, ld, twx, 2);
 
   // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx)
   const int npair = M / 2 + 1;
-  for (int row = threadIdx.x >> logtpr; row < TJ; row += (kNT >> logtpr)) {
-    double2 *Z = sm + (long)row * ld;
-    for (int kk = lane_r; kk < npair; kk += tpr) {
+  for (int rl = 0; rl < RPW; ++rl) {
+    double2 *Z = wsm + (long)rl * ld;
+    for (int kk = lane; kk < npair; kk += 32) {
       if (kk == 0) {
         const double2 z0 = Z[0];
         Z[0] = mk<double2>(z0.x + z0.y, 0.0);
-        Z[M] = mk<double2>(z0.x - z0.y, 0.0);
+        Z[pad8(M)] = mk<double2>(z0.x - z0.y, 0.0);
       } else {
         const int km = M - kk;
-        const double2 a = Z[kk], b = Z[km];
+        const double2 a = Z[pad8(kk)], b = Z[pad8(km)];
         const double2 wa = twx[kk], wb = twx[km];
         double2 ep = mk<double2>(a.x + b.x, a.y - b.y);  // Z_k + conj Z_{M-k}
         double2 em = mk<double2>(a.x - b.x, a.y + b.y);  // Z_k - conj Z_{M-k}
         double2 t1 = cmul(wa, em);                        // W^k * em
-        Z[kk] = mk<double2>(0.5 * (ep.x + t1.y), 0.5 * (ep.y - t1.x));  // (ep - i t1)/2
+        Z[pad8(kk)] = mk<double2>(0.5 * (ep.x + t1.y), 0.5 * (ep.y - t1.x));  // (ep - i t1)/2
         if (km != kk) {
           double2 fp = mk<double2>(b.x + a.x, b.y - a.y);
           double2 fm = mk<double2>(b.x - a.x, b.y + a.y);
           double2 t2 = cmul(wb, fm);
-          Z[km] = mk<double2>(0.5 * (fp.x + t2.y), 0.5 * (fp.y - t2.x));
+          Z[pad8(km)] = mk<double2>(0.5 * (fp.x + t2.y), 0.5 * (fp.y - t2.x));
         }
       }
     }
   }
   __syncthreads();
   // S[kx][r0 + row]: consecutive threads take consecutive rows of one kx
-  for (int t = threadIdx.x; t < (ld << logTJ); t += kNT) {
+  for (int t = threadIdx.x; t < ((M + 1) << logTJ); t += kNT) {
     const int kx = t >> logTJ, row = t & (TJ - 1);
-    if (row < nrows) spec[(long)kx * g.R + r0 + row] = sm[(long)row * ld + kx];
+    if (row < nrows) spec[(long)kx * g.R + r0 + row] = sm[(long)row * ld + pad8(kx)];
   }
 }
 
-static int ilog2i(int v) {
-  int l = 0;
-  while ((2 << l) <= v) ++l;
-  return l;
-}
-// threads per x row: the smallest power of two >= nx/2, capped at the block size
-static int logtpr_for(int nx) {
-  int t = 1;
-  while (t < nx / 2 && t < kNT) t *= 2;
-  return ilog2i(t);
+template <int MODE, bool ST>
+static void launch_x_fwd(const double *s, Lay Ls, const RhsArgs &ra, const GridK &g, const FftPlan &pl,
+                         const double2 *twx, double2 *spec, cudaStream_t st) {
+  const int TJ = fftx_rows_per_cta(g.M);
+  const long nblk = (g.R + TJ - 1) / TJ;
+  const int lr = ilog2i(seq_per_warp(g.M)), ld = x_row_stride(g.M);
+  if (elems_per_lane(g.M) <= 8)
+    k_fftx_fwd<MODE, ST, 8><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(s, Ls, ra, g, pl, twx, spec, lr, ld);
+  else
+    k_fftx_fwd<MODE, ST, 16><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(s, Ls, ra, g, pl, twx, spec, lr, ld);
 }
 
 void launch_fftx_fwd_from_s(const double *s, Lay Ls, const GridK &g, const FftPlan &pl, const double2 *twx,
                             double2 *spec, cudaStream_t st) {
-  const int TJ = fftx_rows_per_cta(g.M);
-  const long nblk = (g.R + TJ - 1) / TJ;
   RhsArgs ra{};
-  k_fftx_fwd<0, false><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(s, Ls, ra, g, pl, twx, spec, ilog2i(TJ),
-                                                                         logtpr_for(g.nx));
+  launch_x_fwd<0, false>(s, Ls, ra, g, pl, twx, spec, st);
 }
 
 void launch_fftx_fwd_rhs(const RhsArgs &ra, bool has_st, const GridK &g, const FftPlan &pl, const double2 *twx,
                          double2 *spec, cudaStream_t st) {
-  const int TJ = fftx_rows_per_cta(g.M);
-  const long nblk = (g.R + TJ - 1) / TJ;
   Lay Ls{};
-  const int lt = ilog2i(TJ), lr = logtpr_for(g.nx);
-  if (has_st)
-    k_fftx_fwd<1, true><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(nullptr, Ls, ra, g, pl, twx, spec, lt, lr);
-  else
-    k_fftx_fwd<1, false><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(nullptr, Ls, ra, g, pl, twx, spec, lt, lr);
+  if (has_st) launch_x_fwd<1, true>(nullptr, Ls, ra, g, pl, twx, spec, st);
+  else launch_x_fwd<1, false>(nullptr, Ls, ra, g, pl, twx, spec, st);
 }
 
 // Standalone split RHS (tbfp_rhs_split): s on the interior; grid (x tiles, ny, nz).
@@ -211,33 +238,46 @@ void launch_rhs(const RhsArgs &ra, bool has_st, const GridK &g, double *s, Lay L
 // z transform (forward or backward) of a tile of TJz consecutive j columns of
 // one kx plane: S[kx][(k-1)*ny + j-1], k = 1..nz, staged in shared memory.
 // ---------------------------------------------------------------------------
-template <bool INV>
+template <bool INV, int EMAX>
 __global__ void __launch_bounds__(kNT, 2) k_fftz(double2 *__restrict__ spec, GridK g, FftPlan pl,
-                                              const double2 *__restrict__ twz, int TJz) {
+                                              const double2 *__restrict__ twz, int logcpw, int ES) {
   extern __shared__ double2 sm[];
+  const int logT = logcpw + 3;  // columns per CTA (8 warps)
+  const int TJz = 1 << logT;
   const int kx = blockIdx.y;
-  const int j0 = blockIdx.x * TJz;
+  const int j0 = blockIdx.x << logT;
   const int nj = min(TJz, g.ny - j0);
   double2 *base = spec + (long)kx * g.R + j0;
   const int nz = g.nz, ny = g.ny;
-  for (int t = threadIdx.x; t < nz * TJz; t += blockDim.x) {
-    const int k = t / TJz, jj = t - k * TJz;
-    sm[t] = (jj < nj) ? base[(long)k * ny + jj] : mk<double2>(0.0, 0.0);
+  for (int t = threadIdx.x; t < (nz << logT); t += kNT) {
+    const int k = t >> logT, jj = t & (TJz - 1);
+    sm[pad8(k) * ES + jj] = (jj < nj) ? base[(long)k * ny + jj] : mk<double2>(0.0, 0.0);
   }
   __syncthreads();
-  fft_smem<double2, kEMAX, INV>(sm, pl, __ffs(TJz) - 1, TJz, 1, twz, 1);
-  for (int t = threadIdx.x; t < nz * TJz; t += blockDim.x) {
-    const int k = t / TJz, jj = t - k * TJz;
-    if (jj < nj) base[(long)k * ny + jj] = sm[t];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  fft_group<double2, EMAX, INV, 32>(sm + (warp << logcpw), lane, pl, logcpw, ES, 1, twz, 1);
+  __syncthreads();
+  for (int t = threadIdx.x; t < (nz << logT); t += kNT) {
+    const int k = t >> logT, jj = t & (TJz - 1);
+    if (jj < nj) base[(long)k * ny + jj] = sm[pad8(k) * ES + jj];
   }
 }
 
 void launch_fftz(double2 *spec, const GridK &g, const FftPlan &pl, const double2 *twz, bool inverse,
                  cudaStream_t st) {
   const int TJz = fftz_cols_per_cta(g.nz);
+  const int lc = ilog2i(seq_per_warp(g.nz));
   dim3 grid((g.ny + TJz - 1) / TJz, g.nkx);
-  if (inverse) k_fftz<true><<<grid, kNT, fftz_smem_bytes(g.nz), st>>>(spec, g, pl, twz, TJz);
-  else k_fftz<false><<<grid, kNT, fftz_smem_bytes(g.nz), st>>>(spec, g, pl, twz, TJz);
+  const size_t sb = fftz_smem_bytes(g.nz);
+  const int es = z_row_stride(g.nz);
+  const bool e8 = elems_per_lane(g.nz) <= 8;
+  if (inverse) {
+    if (e8) k_fftz<true, 8><<<grid, kNT, sb, st>>>(spec, g, pl, twz, lc, es);
+    else k_fftz<true, 16><<<grid, kNT, sb, st>>>(spec, g, pl, twz, lc, es);
+  } else {
+    if (e8) k_fftz<false, 8><<<grid, kNT, sb, st>>>(spec, g, pl, twz, lc, es);
+    else k_fftz<false, 16><<<grid, kNT, sb, st>>>(spec, g, pl, twz, lc, es);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -263,38 +303,57 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(double2 *__restrict__ spe
                                                        const double *__restrict__ lamx,
                                                        const double *__restrict__ lamz,
                                                        const double *__restrict__ am, const double *__restrict__ ap,
-                                                       const double *__restrict__ dyf, double mean_c, double nxnz) {
+                                                       const double *__restrict__ dyf, double mean_c, double nxnz,
+                                                       int T) {
   extern __shared__ unsigned char smraw[];
   const int ny = g.ny;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double2 *d = reinterpret_cast<double2 *>(smraw) + (long)warp * ny;
-  double *ca = reinterpret_cast<double *>(reinterpret_cast<double2 *>(smraw) + (long)kWPB * ny) + (long)warp * 2 * ny;
-  double *cc = ca + ny;
+  // per warp, interleaved by lane: row t of lane l at [t*33 + l]
+  const int W = 33 * T;
+  double2 *d = reinterpret_cast<double2 *>(smraw) + (long)warp * W;
+  double *ca = reinterpret_cast<double *>(reinterpret_cast<double2 *>(smraw) + (long)kWPB * W) + (long)warp * 2 * W;
+  double *cc = ca + W;
   const long q = (long)blockIdx.x * kWPB + warp;
   if (q >= (long)g.nkx * g.nz) return;  // whole warp leaves; no block-level barrier follows
   const int kx = (int)(q / g.nz), kz = (int)(q % g.nz);
   double2 *S = spec + (long)kx * g.R + (long)kz * ny;
-  for (int e = lane; e < ny; e += 32) d[e] = S[e];
+
+  const int NL = min(32, ny / 2);
+  const int nb = ny / NL, rem = ny - nb * NL;
+  const int split = rem * (nb + 1);  // rows owned by the lanes with nb+1 rows
+  // slot of global row e
+  auto slot = [&](int e) -> int {
+    int l, t;
+    if (e < split) {
+      l = e / (nb + 1);
+      t = e - l * (nb + 1);
+    } else {
+      const int f = e - split;
+      l = rem + f / nb;
+      t = f - (l - rem) * nb;
+    }
+    return t * 33 + l;
+  };
+  for (int e = lane; e < ny; e += 32) d[slot(e)] = S[e];
   __syncwarp();
 
   const double lam = lamx[kx] + lamz[kz];
   const bool pin = (kx == 0 && kz == 0);
-  const int NL = min(32, ny / 2);
-  const int nb = ny / NL, rem = ny - nb * NL;
   const bool active = lane < NL;
-  const int s = lane * nb + min(lane, rem);
+  const int s0 = lane * nb + min(lane, rem);  // first global row of this lane
   const int len = active ? nb + (lane < rem ? 1 : 0) : 0;
-  const int e = s + len - 1;
 
   double at_e = 0.0, ct_e = 0.0;
   double2 dt_e = mk<double2>(0.0, 0.0);
   if (active) {
     double at_p = 0.0, ct_p = 0.0;
     double2 dt_p = mk<double2>(0.0, 0.0);
-    for (int i = s; i <= e; ++i) {
+    for (int t = 0; t < len; ++t) {
+      const int i = s0 + t;
       const double r = 1.0 / (lam - am[i] - ap[i]);
       double a = am[i] * r, c = ap[i] * r;
-      double2 dd = cscale(d[i], r);
+      const int sl = t * 33 + lane;
+      double2 dd = cscale(d[sl], r);
       if (pin && i == ny - 1) {
         a = 0.0;
         c = 0.0;
@@ -302,7 +361,7 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(double2 *__restrict__ spe
       }
       double at, ct;
       double2 dt;
-      if (i == s) {
+      if (t == 0) {
         at = a;
         ct = c;
         dt = dd;
@@ -312,9 +371,9 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(double2 *__restrict__ spe
         ct = c * inv;
         dt = mk<double2>((dd.x - a * dt_p.x) * inv, (dd.y - a * dt_p.y) * inv);
       }
-      ca[i] = at;
-      cc[i] = ct;
-      d[i] = dt;
+      ca[sl] = at;
+      cc[sl] = ct;
+      d[sl] = dt;
       at_p = at;
       ct_p = ct;
       dt_p = dt;
@@ -327,13 +386,16 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(double2 *__restrict__ spe
   double ha = 0.0, hc = -1.0;
   double2 hd = mk<double2>(0.0, 0.0);
   if (active && len >= 2) {
-    hd = d[e - 1];
-    ha = ca[e - 1];
-    hc = cc[e - 1];
-    for (int i = e - 2; i >= s; --i) {
-      const double ct = cc[i];
-      hd = mk<double2>(d[i].x - ct * hd.x, d[i].y - ct * hd.y);
-      ha = ca[i] - ct * ha;
+    int sl = (len - 2) * 33 + lane;
+    hd = d[sl];
+    ha = ca[sl];
+    hc = cc[sl];
+    for (int t = len - 3; t >= 0; --t) {
+      sl = t * 33 + lane;
+      const double ct = cc[sl];
+      const double2 dv = d[sl];
+      hd = mk<double2>(dv.x - ct * hd.x, dv.y - ct * hd.y);
+      ha = ca[sl] - ct * ha;
       hc = -ct * hc;
     }
   }
@@ -375,19 +437,22 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(double2 *__restrict__ spe
   if (lane == 0) { xsx = 0.0; xsy = 0.0; }
   if (active) {
     double2 xn = mk<double2>(yx, yy);
-    d[e] = xn;
-    for (int i = e - 1; i >= s; --i) {
-      const double a = ca[i], c = cc[i];
-      xn = mk<double2>(d[i].x - a * xsx - c * xn.x, d[i].y - a * xsy - c * xn.y);
-      d[i] = xn;
+    d[(len - 1) * 33 + lane] = xn;
+    for (int t = len - 2; t >= 0; --t) {
+      const int sl = t * 33 + lane;
+      const double a = ca[sl], c = cc[sl];
+      const double2 dv = d[sl];
+      xn = mk<double2>(dv.x - a * xsx - c * xn.x, dv.y - a * xsy - c * xn.y);
+      d[sl] = xn;
     }
   }
   __syncwarp();
   if (pin) {
     double sx = 0.0, sy = 0.0;
-    for (int i = lane; i < ny; i += 32) {
-      sx += d[i].x * dyf[i];
-      sy += d[i].y * dyf[i];
+    for (int e = lane; e < ny; e += 32) {
+      const double2 v = d[slot(e)];
+      sx += v.x * dyf[e];
+      sy += v.y * dyf[e];
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -395,10 +460,13 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(double2 *__restrict__ spe
       sy += __shfl_xor_sync(0xffffffffu, sy, o);
     }
     const double subx = sx * mean_c * nxnz, suby = sy * mean_c * nxnz;
-    for (int i = lane; i < ny; i += 32) d[i] = mk<double2>(d[i].x - subx, d[i].y - suby);
+    for (int e = lane; e < ny; e += 32) {
+      const int sl = slot(e);
+      d[sl] = mk<double2>(d[sl].x - subx, d[sl].y - suby);
+    }
     __syncwarp();
   }
-  for (int i = lane; i < ny; i += 32) S[i] = d[i];
+  for (int e = lane; e < ny; e += 32) S[e] = d[slot(e)];
 }
 
 void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
@@ -406,7 +474,7 @@ void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const dou
   const long nsys = (long)g.nkx * g.nz;
   const long nblk = (nsys + kWPB - 1) / kWPB;
   k_tridiag<<<(unsigned)nblk, kWPB * 32, tridiag_smem_bytes(g.ny), st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c,
-                                                                         nxnz);
+                                                                         nxnz, tri_rows_per_lane(g.ny));
 }
 
 // ---------------------------------------------------------------------------
@@ -416,51 +484,56 @@ void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const dou
 // copies the wall cell (normalGradient, bf=0), x and z ghosts are periodic.
 // The imaginary parts of X[0] and X[nx/2] are ignored, as FFTW's c2r does.
 // ---------------------------------------------------------------------------
+template <int EMAX>
 __global__ void __launch_bounds__(kNT, 2) k_fftx_inv(const double2 *__restrict__ spec, double *__restrict__ psi,
-                                                     Lay Lp, int hd, GridK g, FftPlan pl,
-                                                     const double2 *__restrict__ twx, double scale, int logTJ,
-                                                     int logtpr) {
+                                                  Lay Lp, int hd, GridK g, FftPlan pl,
+                                                  const double2 *__restrict__ twx, double scale, int logrpw,
+                                                  int ld) {
   extern __shared__ double2 sm[];
+  const int RPW = 1 << logrpw;
+  const int logTJ = logrpw + 3;
   const int TJ = 1 << logTJ;
-  const int M = g.M, nx = g.nx, ld = M + 1;
+  const int M = g.M, nx = g.nx;
   const int r0 = blockIdx.x << logTJ;
   const int nrows = min(TJ, (int)g.R - r0);
-  const int tpr = 1 << logtpr;
-  const int lane_r = threadIdx.x & (tpr - 1);
-  for (int t = threadIdx.x; t < (ld << logTJ); t += kNT) {
+  for (int t = threadIdx.x; t < ((M + 1) << logTJ); t += kNT) {
     const int kx = t >> logTJ, row = t & (TJ - 1);
-    sm[(long)row * ld + kx] = (row < nrows) ? spec[(long)kx * g.R + r0 + row] : mk<double2>(0.0, 0.0);
+    sm[(long)row * ld + pad8(kx)] = (row < nrows) ? spec[(long)kx * g.R + r0 + row] : mk<double2>(0.0, 0.0);
   }
   __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *wsm = sm + (long)warp * RPW * ld;
   // Z[k] = (X_k + conj X_{M-k}) + i conj(W^k) (X_k - conj X_{M-k}),  k = 0..M-1
   const int npair = M / 2 + 1;
-  for (int row = threadIdx.x >> logtpr; row < TJ; row += (kNT >> logtpr)) {
-    double2 *X = sm + (long)row * ld;
-    for (int kk = lane_r; kk < npair; kk += tpr) {
+  for (int rl = 0; rl < RPW; ++rl) {
+    double2 *X = wsm + (long)rl * ld;
+    for (int kk = lane; kk < npair; kk += 32) {
       if (kk == 0) {
-        const double a = X[0].x, b = X[M].x;
+        const double a = X[0].x, b = X[pad8(M)].x;
         X[0] = mk<double2>(a + b, a - b);
       } else {
         const int km = M - kk;
-        const double2 a = X[kk], b = X[km];
+        const double2 a = X[pad8(kk)], b = X[pad8(km)];
         const double2 wa = cconj(twx[kk]), wb = cconj(twx[km]);
         double2 ep = mk<double2>(a.x + b.x, a.y - b.y);
         double2 em = mk<double2>(a.x - b.x, a.y + b.y);
         double2 t1 = cmul(wa, em);
-        X[kk] = mk<double2>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
+        X[pad8(kk)] = mk<double2>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
         if (km != kk) {
           double2 fp = mk<double2>(b.x + a.x, b.y - a.y);
           double2 fm = mk<double2>(b.x - a.x, b.y + a.y);
           double2 t2 = cmul(wb, fm);
-          X[km] = mk<double2>(fp.x - t2.y, fp.y + t2.x);
+          X[pad8(km)] = mk<double2>(fp.x - t2.y, fp.y + t2.x);
         }
       }
     }
   }
-  __syncthreads();
-  fft_smem<double2, kEMAX, true>(sm, pl, logTJ, 1, ld, twx, 2);
-  const double *smr = reinterpret_cast<const double *>(sm);
-  for (int row = threadIdx.x >> logtpr; row < nrows; row += (kNT >> logtpr)) {
+  __syncwarp();
+  fft_group<double2, EMAX, true, 32>(wsm, lane, pl, logrpw, 1, ld, twx, 2);
+  const double *wsr = reinterpret_cast<const double *>(wsm);
+  for (int rl = 0; rl < RPW; ++rl) {
+    const int row = warp * RPW + rl;
+    if (row >= nrows) break;
     const unsigned rr = (unsigned)(r0 + row);
     const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
     // ghost images of the row: first y ghost layer (wall copy), periodic z
@@ -472,9 +545,9 @@ __global__ void __launch_bounds__(kNT, 2) k_fftx_inv(const double2 *__restrict__
     else if (j == g.ny) js[nj++] = g.ny + 1;
     if (k <= hd) ks[nk++] = k + g.nz;
     else if (k > g.nz - hd) ks[nk++] = k - g.nz;
-    const double *src = smr + (long)row * 2 * ld;
-    for (int ii = lane_r; ii < nx; ii += tpr) {
-      const double v = src[ii] * scale;
+    const double *src = wsr + (long)rl * 2 * ld;
+    for (int ii = lane; ii < nx; ii += 32) {
+      const double v = src[2 * pad8(ii >> 1) + (ii & 1)] * scale;
       const int i = ii + 1;
       int is[2];
       int ni = 1;
@@ -494,8 +567,11 @@ void launch_fftx_inv(const double2 *spec, double *psi, Lay Lp, int hd, const Gri
                      const double2 *twx, double scale, cudaStream_t st) {
   const int TJ = fftx_rows_per_cta(g.M);
   const long nblk = (g.R + TJ - 1) / TJ;
-  k_fftx_inv<<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(spec, psi, Lp, hd, g, pl, twx, scale, ilog2i(TJ),
-                                                               logtpr_for(g.nx));
+  const int lr = ilog2i(seq_per_warp(g.M)), ld = x_row_stride(g.M);
+  if (elems_per_lane(g.M) <= 8)
+    k_fftx_inv<8><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(spec, psi, Lp, hd, g, pl, twx, scale, lr, ld);
+  else
+    k_fftx_inv<16><<<(unsigned)nblk, kNT, fftx_smem_bytes(g.M), st>>>(spec, psi, Lp, hd, g, pl, twx, scale, lr, ld);
 }
 
 // ---------------------------------------------------------------------------
@@ -566,8 +642,19 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long *o
 // reduced per block and folded into *maxdiv with one atomic.
 constexpr int kJC = 32;
 
+// Face update of makeVelocityDivFree FAST for one face: u - r*(invrho0*dpr + (invrho-invrho0)*dpr0),
+// dpr = (psi+ - psi)*idc, dpr0 = (2(pn+ - pn) - (po+ - po))*idc [- 2 st^n + st^{n-1}].
+__device__ __forceinline__ double face_update(double u, double r, double ir0, double irp, double irc, double idc,
+                                              double ps_p, double ps_c, double pn_p, double pn_c, double po_p,
+                                              double po_c, double st) {
+  const double invrho = 0.5 * (irp + irc);
+  const double dpr = (ps_p - ps_c) * idc;
+  const double dpr0 = (2.0 * (pn_p - pn_c) - (po_p - po_c)) * idc - st;
+  return u - r * (ir0 * dpr + (invrho - ir0) * dpr0);
+}
+
 template <bool ST>
-__global__ void __launch_bounds__(128) k_correct_div(CorrArgs a, GridK g, unsigned long long *__restrict__ maxdiv) {
+__global__ void __launch_bounds__(128, 7) k_correct_div(CorrArgs a, GridK g, unsigned long long *__restrict__ maxdiv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int k = blockIdx.z + 1;
   const int j0 = blockIdx.y * kJC + 1, j1 = min(j0 + kJC - 1, g.ny);
@@ -575,29 +662,100 @@ __global__ void __launch_bounds__(128) k_correct_div(CorrArgs a, GridK g, unsign
   const int lane = threadIdx.x & 31;
   const int ic = valid ? i : g.nx;  // clamped index keeps every load in bounds
   const int km = (k == 1) ? g.nz : k - 1;
-  double vmax = 0.0;
-  double uym = (j0 > 1) ? corr_y<ST>(a, g, ic, j0 - 1, k) : a.uyi[at(a.Luy, ic, 0, k)];
-  if (valid && j0 == 1) a.uyo[at(a.Luy, i, 0, k)] = uym;
+  const double *__restrict__ ps = a.psi;
+  const double *__restrict__ pn = a.pn;
+  const double *__restrict__ po = a.pnm1;
+  const double *__restrict__ ir = a.irho;
+  const double *__restrict__ uxi = a.uxi;
+  const double *__restrict__ uyi = a.uyi;
+  const double *__restrict__ uzi = a.uzi;
+  double *__restrict__ uxo = a.uxo;
+  double *__restrict__ uyo = a.uyo;
+  double *__restrict__ uzo = a.uzo;
+  const long pjs = a.Lpsi.sj, pks = a.Lpsi.sk, rjs = a.Lrho.sj, rks = a.Lrho.sk;
+  const double r = a.r, ir0 = a.invrho0;
+  const double idxc = g.idxc1, idzc = g.idzc1;
   const double idx = g.idxf[ic - 1], idz = g.idzf[k - 1];
+  // surface-tension terms of one face (zero without surface tension)
+  auto stx = [&](int ii, int jj, int kk) -> double {
+    if constexpr (ST) {
+      const long q = at(a.Lst[0], ii, jj, kk);
+      return 2.0 * a.stn[0][q] - a.sto[0][q];
+    } else return 0.0;
+  };
+  auto sty = [&](int ii, int jj, int kk) -> double {
+    if constexpr (ST) {
+      const long q = at(a.Lst[1], ii, jj, kk);
+      return 2.0 * a.stn[1][q] - a.sto[1][q];
+    } else return 0.0;
+  };
+  auto stz = [&](int ii, int jj, int kk) -> double {
+    if constexpr (ST) {
+      const long q = at(a.Lst[2], ii, jj, kk);
+      return 2.0 * a.stn[2][q] - a.sto[2][q];
+    } else return 0.0;
+  };
+
+  // centre values of the current cell, carried along j
+  long p = at(a.Lpsi, ic, j0, k), q = at(a.Lrho, ic, j0, k);
+  double psc = ps[p], pnc = pn[p], poc = po[p], irc = ir[q];
+  double uym;
+  if (j0 > 1) {
+    const double psm = ps[p - pjs], pnm = pn[p - pjs], pom = po[p - pjs], irm = ir[q - rjs];
+    uym = face_update(uyi[at(a.Luy, ic, j0 - 1, k)], r, ir0, irc, irm, g.idyc[j0 - 1], psc, psm, pnc, pnm, poc, pom,
+                      sty(ic, j0 - 1, k));
+  } else {
+    uym = uyi[at(a.Luy, ic, 0, k)];
+  }
+  if (valid && j0 == 1) uyo[at(a.Luy, i, 0, k)] = uym;
+  const long pxw = (i == 1) ? (long)(g.nx - 1) : -1;  // offset to the lower x neighbour's centre
+  double vmax = 0.0;
   for (int j = j0; j <= j1; ++j) {
-    const double uxp = corr_x<ST>(a, g, ic, j, k);
+    // every load of this step, issued together
+    const double psx = ps[p + 1], pnx = pn[p + 1], pox = po[p + 1], irx = ir[q + 1];
+    const double psy = ps[p + pjs], pny = pn[p + pjs], poy = po[p + pjs], iry = ir[q + rjs];
+    const double psz = ps[p + pks], pnz = pn[p + pks], poz = po[p + pks], irz = ir[q + rks];
+    const long pm = (k == 1) ? p + (long)(g.nz - 1) * pks : p - pks;
+    const long qm = (k == 1) ? q + (long)(g.nz - 1) * rks : q - rks;
+    const double psm = ps[pm], pnm = pn[pm], pom = po[pm], irm = ir[qm];
+    const double ux_c = uxi[at(a.Lux, ic, j, k)];
+    const double uy_c = uyi[at(a.Luy, ic, j, k)];
+    const double uz_c = uzi[at(a.Luz, ic, j, k)];
+    const double uz_m = uzi[at(a.Luz, ic, j, km)];
+
+    const double uxp = face_update(ux_c, r, ir0, irx, irc, idxc, psx, psc, pnx, pnc, pox, poc, stx(ic, j, k));
     const double up = __shfl_up_sync(0xffffffffu, uxp, 1);
-    const double uxm = (lane == 0 || i == 1) ? corr_x<ST>(a, g, i == 1 ? g.nx : ic - 1, j, k) : up;
-    const double uyp = (j < g.ny) ? corr_y<ST>(a, g, ic, j, k) : a.uyi[at(a.Luy, ic, j, k)];
-    const double uzp = corr_z<ST>(a, g, ic, j, k);
-    const double uzm = corr_z<ST>(a, g, ic, j, km);
+    double uxm = up;
+    if (lane == 0 || i == 1) {  // lower x face: recompute (periodic wrap at i = 1)
+      const long pw = (i == 1) ? p + pxw : p - 1;
+      const long qw = (i == 1) ? q + pxw : q - 1;
+      const int iw = (i == 1) ? g.nx : ic - 1;
+      uxm = face_update(uxi[at(a.Lux, iw, j, k)], r, ir0, ir[qw + 1], ir[qw], idxc, ps[pw + 1], ps[pw], pn[pw + 1],
+                        pn[pw], po[pw + 1], po[pw], stx(iw, j, k));
+    }
+    const double uyp = (j < g.ny) ? face_update(uy_c, r, ir0, iry, irc, g.idyc[j], psy, psc, pny, pnc, poy, poc,
+                                                sty(ic, j, k))
+                                  : uy_c;
+    const double uzp = face_update(uz_c, r, ir0, irz, irc, idzc, psz, psc, pnz, pnc, poz, poc, stz(ic, j, k));
+    const double uzm = face_update(uz_m, r, ir0, irc, irm, idzc, psc, psm, pnc, pnm, poc, pom, stz(ic, j, km));
     if (valid) {
-      a.uxo[at(a.Lux, i, j, k)] = uxp;
-      if (i == g.nx) a.uxo[at(a.Lux, 0, j, k)] = uxp;
-      a.uyo[at(a.Luy, i, j, k)] = uyp;
-      a.uzo[at(a.Luz, i, j, k)] = uzp;
-      if (k == g.nz) a.uzo[at(a.Luz, i, j, 0)] = uzp;
+      uxo[at(a.Lux, i, j, k)] = uxp;
+      if (i == g.nx) uxo[at(a.Lux, 0, j, k)] = uxp;
+      uyo[at(a.Luy, i, j, k)] = uyp;
+      uzo[at(a.Luz, i, j, k)] = uzp;
+      if (k == g.nz) uzo[at(a.Luz, i, j, 0)] = uzp;
       double dv = (uxp - uxm) * idx;
       dv = dv + (uyp - uym) * g.idyf[j - 1];
       dv = dv + (uzp - uzm) * idz;
       vmax = fmax(vmax, fabs(dv));
     }
     uym = uyp;
+    psc = psy;
+    pnc = pny;
+    poc = poy;
+    irc = iry;
+    p += pjs;
+    q += rjs;
   }
   block_max_atomic(vmax, maxdiv);
 }
@@ -665,13 +823,19 @@ cudaError_t prepare_kernels() {
     cudaError_t ee = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, big); \
     if (ee != cudaSuccess) e = ee;                                                    \
   } while (0)
-  TBFP_ATTR((k_fftx_fwd<0, false>));
-  TBFP_ATTR((k_fftx_fwd<1, false>));
-  TBFP_ATTR((k_fftx_fwd<1, true>));
-  TBFP_ATTR(k_fftz<false>);
-  TBFP_ATTR(k_fftz<true>);
+  TBFP_ATTR((k_fftx_fwd<0, false, 8>));
+  TBFP_ATTR((k_fftx_fwd<1, false, 8>));
+  TBFP_ATTR((k_fftx_fwd<1, true, 8>));
+  TBFP_ATTR((k_fftx_fwd<0, false, 16>));
+  TBFP_ATTR((k_fftx_fwd<1, false, 16>));
+  TBFP_ATTR((k_fftx_fwd<1, true, 16>));
+  TBFP_ATTR((k_fftz<false, 8>));
+  TBFP_ATTR((k_fftz<true, 8>));
+  TBFP_ATTR((k_fftz<false, 16>));
+  TBFP_ATTR((k_fftz<true, 16>));
   TBFP_ATTR(k_tridiag);
-  TBFP_ATTR(k_fftx_inv);
+  TBFP_ATTR(k_fftx_inv<8>);
+  TBFP_ATTR(k_fftx_inv<16>);
 #undef TBFP_ATTR
   return e;
 }
