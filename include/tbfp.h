@@ -56,11 +56,16 @@ extern "C" {
 
 /* precision modes */
 #define TBFP_FP64 0  /* plain FP64: the drop-in for solveFPS */
-#define TBFP_MIXED 1 /* FP32 transforms + FP64 defect correction */
+#define TBFP_MIXED 1 /* FP32 transforms + FP64 defect correction: psi = solve32(s), then
+                        psi += solve32(s - L psi) until ||s - L psi||_2/||s||_2 <= tol.
+                        The residual is that of the system the FP64 path solves (the
+                        incompatible part of s, sum s V != 0, sits on the top wall).
+                        Synchronises the stream once per correction sweep. */
 
 /* create-time flags */
 #define TBFP_FLAG_ASYNC 1u  /* do not synchronise the stream before returning */
 #define TBFP_FLAG_TIMING 2u /* record per-stage device times into tbfp_stats.ms_stage */
+#define TBFP_FLAG_RESIDUAL 4u /* TBFP_FP64: also compute tbfp_stats.rel_residual (one more pass) */
 
 /* stages of one projection, indices into tbfp_stats.ms_stage */
 #define TBFP_STAGE_RECIP 0      /* 1/rho */
@@ -114,6 +119,17 @@ typedef struct {
   double ms_stage[8];   /* per-stage device time (TBFP_FLAG_TIMING), else 0 */
 } tbfp_stats;
 
+/* MG_MODE settings (the reference's specs/pcg_solver file, read by pcgCTOR,
+ * pcg.f90:62-99, and multiGridCTOR, multiGrid.f90:60-112). */
+typedef struct {
+  int n_levels;       /* multigrid levels; nx, ny, nz divisible by 2^(n_levels-1) */
+  int n_pre, n_post;  /* red-black Gauss-Seidel sweeps before / after the coarse correction */
+  double tol_mg;      /* V-cycles repeat while ||q - L p||/||q|| > tol_mg (0.4 in channel_18) */
+  int max_iter_mg;    /* cap on V-cycles per preconditioner application */
+  double tol_pcg;     /* PCG stops at ||r||_2/||q||_2 <= tol_pcg */
+  int max_iter_pcg;   /* cap on PCG iterations (soft TBFP_ENOTCONVERGED) */
+} tbfp_mg_params;
+
 /* --- lifecycle --------------------------------------------------------- */
 int tbfp_abi_version(void);
 const char *tbfp_strerror(int status);
@@ -125,6 +141,10 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **h);
 int tbfp_destroy(tbfp_handle *h);
 /* Bytes of device memory the handle holds. */
 size_t tbfp_device_bytes(const tbfp_handle *h);
+/* Statistics of the handle's last solve or projection (iterations and
+ * rel_residual of TBFP_MIXED / TBFP_FLAG_RESIDUAL, device time).  No
+ * counterpart in the reference, which prints them (pcg.f90:366-373). */
+int tbfp_get_stats(const tbfp_handle *h, tbfp_stats *out);
 
 /* --- solveFPS (fastPoissonSolver.f90:337-384) -------------------------- */
 /* s: cell field (hd_psi), read on the interior.  psi: cell field (hd_psi),
@@ -183,6 +203,21 @@ int tbfp_projection_dev(tbfp_handle *h, const double *ux_in, const double *uy_in
                         const double *rho, const double *psi_n, const double *psi_nm1,
                         const double *const *st_n, const double *const *st_nm1,
                         double dt, double alpha, double rho0, double *psi, tbfp_stats *stats);
+
+/* --- MG_MODE: PCG with a multigrid preconditioner ----------------------- */
+/* pcgCTOR (pcg.f90:62-99) + multiGridCTOR (multiGrid.f90:60-112): builds the
+   level hierarchy on the handle's grid (metrics from its tbfp_desc). */
+int tbfp_pcg_setup(tbfp_handle *h, const tbfp_mg_params *p);
+/* solvePCG (pcg.f90:103-140): L_beta psi = q with face coefficient
+   (beta_P + beta_nb)/2/(dc df), periodic x/z, Neumann walls; FP64 CG
+   preconditioned by FP32 red-black Gauss-Seidel V-cycles (solveMG,
+   multiGrid.f90:165-232) with a direct coarsest solve (poissMat.f90:289-312).
+   psi (layout of psi, hd_psi) is the initial guess and the result, ghosts
+   updated; beta has rho's layout (hd_rho), q psi's.  stats: iterations = PCG
+   iterations, rel_residual = ||r||_2/||q||_2.  Returns TBFP_ENOTCONVERGED
+   (soft) at max_iter_pcg. */
+int tbfp_pcg_solve(tbfp_handle *h, double *psi, const double *beta, const double *q, tbfp_stats *stats);
+int tbfp_pcg_solve_dev(tbfp_handle *h, double *psi, const double *beta, const double *q, tbfp_stats *stats);
 
 /* --- solveFPS without device allocation ------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device

@@ -26,6 +26,7 @@ TBFP_FP64 = 0
 TBFP_MIXED = 1
 TBFP_FLAG_ASYNC = 1
 TBFP_FLAG_TIMING = 2
+TBFP_FLAG_RESIDUAL = 4
 STAGES = ("recip", "rhs_fftx", "fftz_fwd", "tridiag", "fftz_inv", "fftx_inv", "correct", "div")
 
 
@@ -49,6 +50,11 @@ class TbfpDesc(C.Structure):
         ("precision", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int),
         ("device", C.c_int), ("stream", C.c_void_p), ("flags", C.c_uint),
     ]
+
+
+class TbfpMgParams(C.Structure):
+    _fields_ = [("n_levels", C.c_int), ("n_pre", C.c_int), ("n_post", C.c_int), ("tol_mg", C.c_double),
+                ("max_iter_mg", C.c_int), ("tol_pcg", C.c_double), ("max_iter_pcg", C.c_int)]
 
 
 class TbfpStats(C.Structure):
@@ -76,6 +82,10 @@ PROTOTYPES = {
     "tbfp_create": (C.c_int, [C.POINTER(TbfpDesc), C.POINTER(_H)]),
     "tbfp_destroy": (C.c_int, [_H]),
     "tbfp_device_bytes": (C.c_size_t, [_H]),
+    "tbfp_get_stats": (C.c_int, [_H, C.POINTER(TbfpStats)]),
+    "tbfp_pcg_setup": (C.c_int, [_H, C.POINTER(TbfpMgParams)]),
+    "tbfp_pcg_solve": (C.c_int, [_H, _P, _P, _P, C.POINTER(TbfpStats)]),
+    "tbfp_pcg_solve_dev": (C.c_int, [_H, _P, _P, _P, C.POINTER(TbfpStats)]),
     "tbfp_solve_fps": (C.c_int, [_H, _P, _P]),
     "tbfp_solve_fps_dev": (C.c_int, [_H, _P, _P]),
     "tbfp_rhs_split": (C.c_int, [_H, _P, _P, _P, _P, _P, _P, _PP, _PP, _D, _D, _D, _P]),

@@ -1,22 +1,23 @@
-// Batched complex FFTs held in shared memory (Stockham autosort, radix 2/3/4/8).
+// Batched complex FFTs held in shared memory (Stockham autosort, radix 2/3/4/8),
+// specialised at compile time for each supported length.
 //
 // Replaces the FFTW guru plans of the reference (fastPoissonSolver.f90:160-211):
 // all transforms are unnormalised, forward = exp(-2*pi*i*k*n/N), exactly FFTW's
-// convention.  A CTA transforms `nb` sequences of length n that already sit in
-// shared memory with element stride `es` and batch stride `bs` (in complex
-// elements).  Each radix pass reads all of a thread's butterfly inputs into
-// registers, synchronises, and writes the outputs back in place, so no second
-// buffer is needed.  Twiddles come from a table tw[m] = exp(-2*pi*i*m/Ntab)
-// computed on the host in double precision; a length-n transform reads it with
-// stride twmul = Ntab/n.
+// convention.  One warp transforms NB = 2^LOGNB sequences of length N that sit in
+// shared memory with element stride ES and sequence stride BS (in complex
+// elements).  Each radix pass reads a lane's butterfly inputs into registers,
+// synchronises the warp, and writes the outputs back in place, so no second
+// buffer is needed.  N, NB, ES, BS and the radix sequence are template
+// constants, so every index is a shift, a mask or a constant offset.
+//
+// Twiddles come from a pass-ordered table (built on the host in extended
+// precision, staged in shared memory by the kernel): pass p with Ns_p > 1 reads
+// tw[Ns_p - R_0 + k0*(R_p-1) + r-1] = exp(-2*pi*i*k0*r/(Ns_p*R_p)); the table has
+// N - R_0 entries in total (sum over p of Ns_{p+1} - Ns_p).
 #pragma once
 #include <cuda_runtime.h>
 
 namespace tbfp {
-
-template <typename T> struct cplx_t;
-template <> struct cplx_t<double> { using type = double2; };
-template <> struct cplx_t<float> { using type = float2; };
 
 template <typename V> __device__ __forceinline__ V mk(decltype(V::x) a, decltype(V::x) b) {
   V r;
@@ -36,13 +37,36 @@ template <typename V, bool INV> __device__ __forceinline__ V rot90(V a) {
   return INV ? mk<V>(-a.y, a.x) : mk<V>(a.y, -a.x);
 }
 
-// A transform plan: length and radix sequence (product == n).  n = 2^a or
-// 3*2^a; powers of two first (radix 8, then 4, then 2), the radix 3 last.
-struct FftPlan {
-  int n;
-  int nrad;
-  int rad[16];
-};
+// --- compile-time radix plan: radix 8 while possible, then 4, then 2, and at
+// most one radix 3 as the last pass (n = 2^a or 3*2^a) -----------------------
+__host__ __device__ constexpr int ct_nrad(int n) {
+  int k = 0, m = n;
+  while (m % 8 == 0 && m > 1) { ++k; m /= 8; }
+  while (m % 4 == 0) { ++k; m /= 4; }
+  while (m % 2 == 0) { ++k; m /= 2; }
+  if (m % 3 == 0) { ++k; m /= 3; }
+  return m == 1 ? k : -1;
+}
+__host__ __device__ constexpr int ct_rad(int n, int p) {
+  int k = 0, m = n;
+  while (m % 8 == 0 && m > 1) { if (k == p) return 8; ++k; m /= 8; }
+  while (m % 4 == 0) { if (k == p) return 4; ++k; m /= 4; }
+  while (m % 2 == 0) { if (k == p) return 2; ++k; m /= 2; }
+  if (m % 3 == 0 && k == p) return 3;
+  return 1;
+}
+__host__ __device__ constexpr int ct_ns(int n, int p) {
+  int s = 1;
+  for (int q = 0; q < p; ++q) s *= ct_rad(n, q);
+  return s;
+}
+__host__ __device__ constexpr int ct_log2(int v) {
+  int l = 0;
+  while ((1 << (l + 1)) <= v) ++l;
+  return l;
+}
+// Entries of the pass-ordered twiddle table of a length-n transform.
+__host__ __device__ constexpr int ct_twiddle_len(int n) { return n - ct_rad(n, 0); }
 
 // --- radix butterflies (in registers) --------------------------------------
 template <typename V, bool INV> __device__ __forceinline__ void bfly2(V *v) {
@@ -106,89 +130,55 @@ template <typename V, int R, bool INV> __device__ __forceinline__ void bfly(V *v
 // Shared-memory slot of element e of a sequence: one empty slot after every 8
 // elements, which makes the stride-R writes of the early Stockham passes (and
 // the reads of the late ones) free of bank conflicts for 16-byte elements.
-__host__ __device__ __forceinline__ int pad8(int e) { return e + (e >> 3); }
+__host__ __device__ __forceinline__ constexpr int pad8(int e) { return e + (e >> 3); }
 
-// One Stockham pass of radix R over a group of G threads (a warp, G = 32, or a
-// whole block).  Butterfly b of a length-n transform reads x[b + r*n/R],
-// applies twiddle exp(-+2*pi*i*(b mod Ns)*r/(Ns*R)), transforms, and writes
-// y[(b/Ns)*Ns*R + b mod Ns + r*Ns].  Butterflies are numbered batch-fastest
-// (b = jj*nb + batch), nb and Ns are powers of two (the plan puts its single
-// radix-3 pass last), so all index arithmetic is shifts and masks.  QMAX
-// bounds the butterflies a thread owns (ceil(elements per thread / R)).
-template <int G>
-__device__ __forceinline__ void group_sync() {
-  if constexpr (G == 32) __syncwarp();
-  else __syncthreads();
-}
-
-template <typename V, int R, int QMAX, bool INV, int G>
-__device__ __forceinline__ void stockham_pass(V *buf, int tid, int n, int lognb, int es, int bs, int logNs,
-                                              const V *__restrict__ tw, int twmul) {
-  const int per = n / R;
-  const int total = per << lognb;
-  const int nbm = (1 << lognb) - 1, Nsm = (1 << logNs) - 1;
-  const int stride_tw = (n / R) >> logNs;  // n/(Ns*R)
-  V v[QMAX][R];
+// Pass P of a length-N transform of NB = 2^LOGNB sequences by one warp.
+// Butterfly b reads x[b + r*N/R], applies twiddle exp(-+2*pi*i*(b mod Ns)*r/(Ns*R)),
+// transforms, and writes y[(b/Ns)*Ns*R + b mod Ns + r*Ns].  Butterflies are
+// numbered sequence-fastest (b = jj*NB + sequence).
+template <typename V, int N, int LOGNB, int ES, int BS, bool INV, int P = 0>
+__device__ __forceinline__ void fft_warp(V *buf, int lane, const V *__restrict__ tw) {
+  if constexpr (P < ct_nrad(N)) {
+    constexpr int R = ct_rad(N, P), NS = ct_ns(N, P), LNS = ct_log2(NS), PER = N / R;
+    constexpr int NB = 1 << LOGNB, TOT = PER * NB, Q = (TOT + 31) / 32;
+    constexpr int TWO = NS - ct_rad(N, 0);  // this pass's offset in the twiddle table
+    V v[Q][R];
 #pragma unroll
-  for (int q = 0; q < QMAX; ++q) {
-    const int b = tid + q * G;
-    if (b < total) {
-      const int bt = b & nbm, jj = b >> lognb;
-      const V *base = buf + bt * bs;
-      const int k0 = jj & Nsm;
+    for (int q = 0; q < Q; ++q) {
+      const int b = lane + 32 * q;
+      if (TOT % 32 == 0 || b < TOT) {
+        const int bt = b & (NB - 1), jj = b >> LOGNB;
+        const V *base = buf + bt * BS;
+        const int k0 = jj & (NS - 1);
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        V x = base[pad8(jj + r * per) * es];
-        if (r > 0) {
-          V w = tw[(k0 * r * stride_tw) * twmul];
-          if (INV) w.y = -w.y;
-          x = cmul(x, w);
+        for (int r = 0; r < R; ++r) {
+          V x = base[pad8(jj + r * PER) * ES];
+          if constexpr (NS > 1) {
+            if (r > 0) {
+              V w = tw[TWO + k0 * (R - 1) + (r - 1)];
+              if constexpr (INV) w.y = -w.y;
+              x = cmul(x, w);
+            }
+          }
+          v[q][r] = x;
         }
-        v[q][r] = x;
       }
     }
-  }
-  group_sync<G>();
+    __syncwarp();
 #pragma unroll
-  for (int q = 0; q < QMAX; ++q) {
-    const int b = tid + q * G;
-    if (b < total) {
-      const int bt = b & nbm, jj = b >> lognb;
-      bfly<V, R, INV>(v[q]);
-      V *base = buf + bt * bs;
-      const int d = (((jj >> logNs) * R) << logNs) + (jj & Nsm);
+    for (int q = 0; q < Q; ++q) {
+      const int b = lane + 32 * q;
+      if (TOT % 32 == 0 || b < TOT) {
+        const int bt = b & (NB - 1), jj = b >> LOGNB;
+        bfly<V, R, INV>(v[q]);
+        V *base = buf + bt * BS;
+        const int d = (((jj >> LNS) * R) << LNS) + (jj & (NS - 1));
 #pragma unroll
-      for (int r = 0; r < R; ++r) base[pad8(d + (r << logNs)) * es] = v[q][r];
+        for (int r = 0; r < R; ++r) base[pad8(d + r * NS) * ES] = v[q][r];
+      }
     }
-  }
-  group_sync<G>();
-}
-
-// Full transform of nb = 2^lognb sequences by a group of G threads (tid is the
-// thread's index in the group).  EMAX = upper bound of n*nb/G.
-template <typename V, int EMAX, bool INV, int G>
-__device__ void fft_group(V *buf, int tid, const FftPlan &pl, int lognb, int es, int bs, const V *__restrict__ tw,
-                          int twmul) {
-  int logNs = 0;
-  for (int p = 0; p < pl.nrad; ++p) {
-    const int R = pl.rad[p];
-    switch (R) {
-      case 2:
-        stockham_pass<V, 2, (EMAX + 1) / 2, INV, G>(buf, tid, pl.n, lognb, es, bs, logNs, tw, twmul);
-        logNs += 1;
-        break;
-      case 3:  // always the last pass
-        stockham_pass<V, 3, (EMAX + 2) / 3, INV, G>(buf, tid, pl.n, lognb, es, bs, logNs, tw, twmul);
-        break;
-      case 4:
-        stockham_pass<V, 4, (EMAX + 3) / 4, INV, G>(buf, tid, pl.n, lognb, es, bs, logNs, tw, twmul);
-        logNs += 2;
-        break;
-      default:
-        stockham_pass<V, 8, (EMAX + 7) / 8, INV, G>(buf, tid, pl.n, lognb, es, bs, logNs, tw, twmul);
-        logNs += 3;
-        break;
-    }
+    __syncwarp();
+    fft_warp<V, N, LOGNB, ES, BS, INV, P + 1>(buf, lane, tw);
   }
 }
 

@@ -2,7 +2,10 @@
 // orchestration of the kernels in tbfp_kernels.cu.  See include/tbfp.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <climits>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -10,6 +13,7 @@
 
 #include "tbfp.h"
 #include "tbfp_kernels.cuh"
+#include "tbfp_mg.cuh"
 
 using namespace tbfp;
 
@@ -43,15 +47,23 @@ struct tbfp_handle {
   int max_iter = 8;
 
   GridK g{};
-  FftPlan plx{}, plz{};
   double s_Vg = 0.0, dx_fft = 0.0, dz_fft = 0.0, mean_c = 0.0, nxnz = 0.0, scale = 0.0;
 
   // device tables
   double *d_lamx = nullptr, *d_lamz = nullptr, *d_am = nullptr, *d_ap = nullptr, *d_dyf = nullptr;
   double *d_idyf = nullptr, *d_idyc = nullptr, *d_idxf = nullptr, *d_idzf = nullptr;
-  double2 *d_twx = nullptr, *d_twz = nullptr;
+  double2 *d_twx = nullptr;                     // exp(-2 pi i m/nx), the r2c/c2r factors
+  double2 *d_tpx = nullptr, *d_tpz = nullptr;  // pass-ordered twiddles of lengths nx/2 and nz
+  float2 *d_twx32 = nullptr, *d_tpx32 = nullptr, *d_tpz32 = nullptr;  // FP32 copies (TBFP_MIXED)
+  double *d_acc = nullptr;  // reductions of the residual passes: [0] sum s dyf, [1] sum s^2, [2..] sum r^2
+  double idx2 = 0.0, idz2 = 0.0, ctop_scale = 0.0;
+  tbfp_stats last{};        // statistics of the last solve or projection
+  MgSolver *mg = nullptr;   // MG_MODE hierarchy (tbfp_pcg_setup)
+  std::vector<double> mdxf, mdxc, mdyf, mdyc, mdzf, mdzc;  // caller's metrics, kept for tbfp_pcg_setup
+  double *h_beta = nullptr, *h_q = nullptr;                // device copies for tbfp_pcg_solve
   // work
   double2 *d_spec = nullptr;
+  double *d_s = nullptr;  // split right-hand side, laid out like psi
   double *d_irho = nullptr;
   unsigned long long *d_maxdiv = nullptr;
   // device copies used by the host-pointer entry points
@@ -117,27 +129,19 @@ Lay make_lay(int ilo, int jlo, int klo, int ni, int nj, int hd, size_t *count, i
   return L;
 }
 
-bool make_plan(int n, FftPlan *pl) {
-  std::memset(pl, 0, sizeof(*pl));
-  pl->n = n;
-  int m = n, k = 0;
-  while (m % 8 == 0 && m > 1 && k < 16) { pl->rad[k++] = 8; m /= 8; }
-  while (m % 4 == 0 && k < 16) { pl->rad[k++] = 4; m /= 4; }
-  while (m % 2 == 0 && k < 16) { pl->rad[k++] = 2; m /= 2; }
-  if (m % 3 == 0) { pl->rad[k++] = 3; m /= 3; }  // at most one factor 3, as the last pass
-  pl->nrad = k;
-  return m == 1;
-}
-
-// exp(-2*pi*i*m/n) for m = 0..n-1, evaluated in extended precision and rounded.
-std::vector<double2> twiddles(int n) {
+std::vector<double2> unit_twiddles(int n) {
   std::vector<double2> t(n);
-  const long double pi = 3.141592653589793238462643383279502884L;
-  for (int m = 0; m < n; ++m) {
-    const long double a = 2.0L * pi * (long double)m / (long double)n;
-    t[m].x = (double)cosl(a);
-    t[m].y = (double)(-sinl(a));
-  }
+  fft_unit_twiddles(n, t.data());
+  return t;
+}
+std::vector<double2> pass_twiddles(int n) {
+  std::vector<double2> t(n);
+  fft_pass_twiddles(n, t.data());
+  return t;
+}
+std::vector<float2> to_f32(const std::vector<double2> &v) {
+  std::vector<float2> t(v.size());
+  for (size_t i = 0; i < v.size(); ++i) t[i] = make_float2((float)v[i].x, (float)v[i].y);
   return t;
 }
 
@@ -242,9 +246,87 @@ CorrArgs corr_args(tbfp_handle *h, const double *uxi, const double *uyi, const d
 
 // solveFPS body on device data: spectrum already holds the forward x transform.
 void fps_spectral_solve(tbfp_handle *h) {
-  launch_fftz(h->d_spec, h->g, h->plz, h->d_twz, false, h->stream);
+  launch_fftz(h->d_spec, h->g, h->d_tpz, false, h->stream);
   launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, h->stream);
-  launch_fftz(h->d_spec, h->g, h->plz, h->d_twz, true, h->stream);
+  launch_fftz(h->d_spec, h->g, h->d_tpz, true, h->stream);
+}
+
+XSrc xsrc(tbfp_handle *h, const double *s, const double *psi) {
+  XSrc x{};
+  x.s = s;
+  x.Ls = h->Lpsi;
+  x.psi = psi;
+  x.Lp = h->Lpsi;
+  x.am = h->d_am;
+  x.ap = h->d_ap;
+  x.dyf = h->d_dyf;
+  x.idx2 = h->idx2;
+  x.idz2 = h->idz2;
+  x.ctop_scale = h->ctop_scale;
+  x.acc = h->d_acc;
+  return x;
+}
+
+// Read back acc[1] (sum s^2) and acc[slot] (sum r^2): the relative residual
+// ||r||_2/||s||_2 (pcg.f90:408-429 uses the same ratio of 2-norms).
+int read_rel_residual(tbfp_handle *h, int slot, double *rel) {
+  double v[2];
+  TBFP_CK(h, cudaMemcpyAsync(&v[0], h->d_acc + 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  TBFP_CK(h, cudaMemcpyAsync(&v[1], h->d_acc + slot, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  *rel = v[0] > 0.0 ? std::sqrt(v[1] / v[0]) : std::sqrt(v[1]);
+  return TBFP_OK;
+}
+
+// solveFPS (fastPoissonSolver.f90:337-384) on device arrays, including the
+// zero-mean gauge and the ghost update of psi.
+//   TBFP_FP64: one FP64 direct solve; with TBFP_FLAG_RESIDUAL one more pass
+//     computes ||s - L psi||/||s||.
+//   TBFP_MIXED: direct solves with an FP32 spectrum (FP64 tridiagonal
+//     arithmetic) and FP64 defect correction: psi = solve32(s), then while
+//     ||r||/||s|| > tol: psi += solve32(r), r = s - L psi recomputed in FP64 by
+//     the forward x pass.  The host reads the residual norm after each pass.
+int device_solve(tbfp_handle *h, const double *s, double *psi, int *iters, double *rel) {
+  cudaStream_t st = h->stream;
+  *iters = 1;
+  *rel = -1.0;
+  const bool want_res = h->precision == TBFP_MIXED || (h->flags & TBFP_FLAG_RESIDUAL);
+  if (want_res) TBFP_CK(h, cudaMemsetAsync(h->d_acc, 0, 64 * sizeof(double), st));
+  XSrc x = xsrc(h, s, psi);
+  if (!want_res) x.acc = nullptr;
+  if (h->precision == TBFP_FP64) {
+    launch_fftx_fwd(x, false, h->g, h->d_twx, h->d_tpx, h->d_spec, st);
+    fps_spectral_solve(h);
+    launch_fftx_inv(h->d_spec, psi, h->Lpsi, h->hd_psi, h->g, h->d_twx, h->d_tpx, h->scale, st);
+    if (want_res) {
+      x.acc_r = h->d_acc + 2;
+      launch_fftx_fwd(x, true, h->g, h->d_twx, h->d_tpx, h->d_spec, st);  // residual (spectrum is scratch)
+      int rc = read_rel_residual(h, 2, rel);
+      if (rc) return rc;
+    }
+    return TBFP_OK;
+  }
+  float2 *sp = reinterpret_cast<float2 *>(h->d_spec);
+  auto spectral32 = [&]() {
+    launch_fftz(sp, h->g, h->d_tpz32, false, st);
+    launch_tridiag(sp, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, st);
+    launch_fftz(sp, h->g, h->d_tpz32, true, st);
+  };
+  launch_fftx_fwd(x, false, h->g, h->d_twx32, h->d_tpx32, sp, st);
+  spectral32();
+  launch_fftx_inv(sp, psi, h->Lpsi, h->hd_psi, h->g, h->d_twx32, h->d_tpx32, h->scale, false, st);
+  for (int it = 0;; ++it) {
+    const int slot = 2 + (it < 60 ? it : 61);
+    x.acc_r = h->d_acc + slot;
+    launch_fftx_fwd(x, true, h->g, h->d_twx32, h->d_tpx32, sp, st);  // r of the current psi, transformed
+    int rc = read_rel_residual(h, slot, rel);
+    if (rc) return rc;
+    if (*rel <= h->tol) return TBFP_OK;
+    if (*iters >= h->max_iter) return TBFP_ENOTCONVERGED;
+    spectral32();
+    launch_fftx_inv(sp, psi, h->Lpsi, h->hd_psi, h->g, h->d_twx32, h->d_tpx32, h->scale, true, st);
+    ++*iters;
+  }
 }
 
 bool aliased(const void *a, const void *b) { return a == b; }
@@ -281,16 +363,29 @@ int device_projection(tbfp_handle *h, const double *uxi, const double *uyi, cons
   launch_recip(rho, h->d_irho, (long)h->n_rho, s);
   mark(1);
   RhsArgs ra = rhs_args(h, uxi, uyi, uzi, psi_n, psi_nm1, st_n, st_nm1, dt, alpha, rho0);
-  launch_fftx_fwd_rhs(ra, st, h->g, h->plx, h->d_twx, h->d_spec, s);
-  mark(2);
-  launch_fftz(h->d_spec, h->g, h->plz, h->d_twz, false, s);
-  mark(3);
-  launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, s);
-  mark(4);
-  launch_fftz(h->d_spec, h->g, h->plz, h->d_twz, true, s);
-  mark(5);
-  launch_fftx_inv(h->d_spec, psi, h->Lpsi, h->hd_psi, h->g, h->plx, h->d_twx, h->scale, s);
-  mark(6);
+  launch_rhs(ra, st, h->g, h->d_s, h->Lpsi, s);
+  int iters = 1, solve_rc = TBFP_OK;
+  double rel = -1.0;
+  if (h->precision == TBFP_FP64 && !(h->flags & TBFP_FLAG_RESIDUAL)) {
+    launch_fftx_fwd_from_s(h->d_s, h->Lpsi, h->g, h->d_twx, h->d_tpx, h->d_spec, s);
+    mark(2);
+    launch_fftz(h->d_spec, h->g, h->d_tpz, false, s);
+    mark(3);
+    launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, s);
+    mark(4);
+    launch_fftz(h->d_spec, h->g, h->d_tpz, true, s);
+    mark(5);
+    launch_fftx_inv(h->d_spec, psi, h->Lpsi, h->hd_psi, h->g, h->d_twx, h->d_tpx, h->scale, s);
+    mark(6);
+  } else {  // iterative or checked solve: its passes are timed as one stage (TRIDIAG)
+    mark(2);
+    mark(3);
+    solve_rc = device_solve(h, h->d_s, psi, &iters, &rel);
+    if (solve_rc < 0) return solve_rc;
+    mark(4);
+    mark(5);
+    mark(6);
+  }
   CorrArgs ca = corr_args(h, uxi, uyi, uzi, uxo, uyo, uzo, psi, psi_n, psi_nm1, st_n, st_nm1, dt, alpha, rho0);
   const bool inplace = aliased(uxi, uxo) || aliased(uyi, uyo) || aliased(uzi, uzo);
   if (!inplace) {
@@ -312,8 +407,8 @@ int device_projection(tbfp_handle *h, const double *uxi, const double *uyi, cons
     std::memcpy(&md, &bits, sizeof(md));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-    stats->iterations = 1;
-    stats->rel_residual = -1.0;
+    stats->iterations = iters;
+    stats->rel_residual = rel;
     stats->max_div = md;
     stats->cont_err = md * dt;
     stats->ms_device = ms;
@@ -323,7 +418,17 @@ int device_projection(tbfp_handle *h, const double *uxi, const double *uyi, cons
       stats->ms_stage[i] = m;
     }
   }
-  return finish(h, "tbfp_projection");
+  if (stats) {
+    h->last = *stats;
+  } else {
+    h->last = tbfp_stats{};
+    h->last.iterations = iters;
+    h->last.rel_residual = rel;
+    h->last.max_div = -1.0;
+    h->last.cont_err = -1.0;
+  }
+  const int frc = finish(h, "tbfp_projection");
+  return frc ? frc : solve_rc;
 }
 
 }  // namespace
@@ -350,12 +455,20 @@ const char *tbfp_last_error(const tbfp_handle *h) { return h ? h->err.c_str() : 
 
 size_t tbfp_device_bytes(const tbfp_handle *h) { return h ? h->dev_bytes : 0; }
 
+int tbfp_get_stats(const tbfp_handle *h, tbfp_stats *out) {
+  if (!h || !out) return TBFP_ENULL;
+  *out = h->last;
+  return TBFP_OK;
+}
+
 int tbfp_destroy(tbfp_handle *h) {
   if (!h) return TBFP_OK;
   int dev_prev = 0;
   cudaGetDevice(&dev_prev);
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  delete h->mg;
+  h->mg = nullptr;
   for (void *p : h->allocs) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -381,8 +494,8 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
     return set_err(nullptr, TBFP_EINVAL, "tbfp_create: dx_fft and dz_fft must be positive");
   if (d->precision != TBFP_FP64 && d->precision != TBFP_MIXED)
     return set_err(nullptr, TBFP_EINVAL, "tbfp_create: unknown precision mode");
-  if (d->precision == TBFP_MIXED)
-    return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_create: TBFP_MIXED is not available in this build");
+  if (d->precision == TBFP_MIXED && (!(d->tol > 0.0) || d->max_iter < 1))
+    return set_err(nullptr, TBFP_EINVAL, "tbfp_create: TBFP_MIXED needs tol > 0 and max_iter >= 1");
   for (int i = 0; i < d->nx; ++i)
     if (!(d->dxf[i] > 0.0)) return set_err(nullptr, TBFP_EINVAL, "tbfp_create: dxf must be positive");
   for (int j = 0; j < d->ny; ++j)
@@ -394,14 +507,11 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
   if (!(d->dxc[0] > 0.0) || !(d->dzc[0] > 0.0))
     return set_err(nullptr, TBFP_EINVAL, "tbfp_create: dxc(1), dzc(1) must be positive");
 
-  FftPlan plx, plz;
-  if (!make_plan(d->nx / 2, &plx) || !make_plan(d->nz, &plz))
-    return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_create: nx/2 and nz must be 2^a or 3*2^a");
-  if (d->nx / 2 > fft_max_length() || d->nz > fft_max_length())
-    return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_create: nx/2 and nz must not exceed the transform tile length");
-  if (fftx_smem_bytes(d->nx / 2) > 227 * 1024 || fftz_smem_bytes(d->nz) > 227 * 1024 ||
-      tridiag_smem_bytes(d->ny) > 227 * 1024)
-    return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_create: grid too large for the shared-memory tiles");
+  if (!fft_length_supported(d->nx / 2) || !fft_length_supported(d->nz))
+    return set_err(nullptr, TBFP_EUNSUPPORTED,
+                   "tbfp_create: nx/2 and nz must be 2^a or 3*2^a between 4 and 512");
+  if (tridiag_smem_bytes(d->ny) > 227 * 1024)
+    return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_create: ny too large for the shared-memory tiles");
 
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -421,8 +531,6 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
   h->precision = d->precision;
   h->tol = d->tol;
   h->max_iter = d->max_iter;
-  h->plx = plx;
-  h->plz = plz;
   if (d->device >= 0) h->device = d->device;
   else cudaGetDevice(&h->device);
   int dev_prev = 0;
@@ -440,6 +548,13 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
   h->Lst[0] = make_lay(0, 1, 1, nx + 1, ny, h->hd_st, &h->n_st[0], nz);
   h->Lst[1] = make_lay(1, 0, 1, nx, ny + 1, h->hd_st, &h->n_st[1], nz);
   h->Lst[2] = make_lay(1, 1, 0, nx, ny, h->hd_st, &h->n_st[2], nz + 1);
+  // the stencil kernels index fields with 32-bit element offsets
+  const size_t nmax = std::max({h->n_psi, h->n_rho, h->n_ux, h->n_uy, h->n_uz, h->n_st[0], h->n_st[1], h->n_st[2]});
+  if (nmax >= (size_t)INT32_MAX) {
+    delete h;
+    cudaSetDevice(dev_prev);
+    return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_create: a field has 2^31 or more elements");
+  }
 
   int rc = TBFP_OK;
   auto fail = [&](int code) {
@@ -479,12 +594,22 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
   //     initOffDiagMatrix (:255-276); reciprocal metrics for the stencils.
   const double pi = 3.14159265358979323846;
   h->dx_fft = d->dx_fft;
+  h->mdxf.assign(d->dxf, d->dxf + nx);
+  h->mdxc.assign(d->dxc, d->dxc + nx + 1);
+  h->mdyf.assign(d->dyf, d->dyf + ny);
+  h->mdyc.assign(d->dyc, d->dyc + ny + 1);
+  h->mdzf.assign(d->dzf, d->dzf + nz);
+  h->mdzc.assign(d->dzc, d->dzc + nz + 1);
   h->dz_fft = d->dz_fft;
   std::vector<double> lamx(h->nkx), lamz(nz), am(ny), ap(ny), dyf(ny), idyf(ny), idyc(ny + 1), idxf(nx), idzf(nz);
   for (int i = 0; i < h->nkx; ++i)
     lamx[i] = 2.0 * (std::cos(((double)i * 2.0 * pi) / nx) - 1.0) / (d->dx_fft * d->dx_fft);
-  for (int k = 0; k < nz; ++k)
-    lamz[k] = 2.0 * (std::cos(((double)k * 2.0 * pi) / nz) - 1.0) / (d->dz_fft * d->dz_fft);
+  // lamz(k) of fastPoissonSolver.f90:215-251, evaluated at min(k, nz-k) so the
+  // table is exactly even in k (the y solve pairs kz with nz-kz)
+  for (int k = 0; k < nz; ++k) {
+    const int kk = std::min(k, nz - k);
+    lamz[k] = 2.0 * (std::cos(((double)kk * 2.0 * pi) / nz) - 1.0) / (d->dz_fft * d->dz_fft);
+  }
   for (int j = 0; j < ny; ++j) {
     am[j] = 1.0 / (d->dyc[j] * d->dyf[j]);
     ap[j] = 1.0 / (d->dyc[j + 1] * d->dyf[j]);
@@ -507,13 +632,21 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
   h->mean_c = d->dx_fft * d->dz_fft / sVg;
   h->nxnz = (double)nx * (double)nz;
   h->scale = 1.0 / ((double)nx * (double)nz);
+  h->idx2 = 1.0 / (d->dx_fft * d->dx_fft);
+  h->idz2 = 1.0 / (d->dz_fft * d->dz_fft);
+  h->ctop_scale = 1.0 / (d->dyf[ny - 1] * (double)nx * (double)nz);
 
   if ((rc = upload(h, &h->d_lamx, lamx)) || (rc = upload(h, &h->d_lamz, lamz)) || (rc = upload(h, &h->d_am, am)) ||
       (rc = upload(h, &h->d_ap, ap)) || (rc = upload(h, &h->d_dyf, dyf)) || (rc = upload(h, &h->d_idyf, idyf)) ||
       (rc = upload(h, &h->d_idyc, idyc)) || (rc = upload(h, &h->d_idxf, idxf)) || (rc = upload(h, &h->d_idzf, idzf)) ||
-      (rc = upload(h, &h->d_twx, twiddles(nx))) || (rc = upload(h, &h->d_twz, twiddles(nz))))
+      (rc = upload(h, &h->d_twx, unit_twiddles(nx))) || (rc = upload(h, &h->d_tpx, pass_twiddles(nx / 2))) ||
+      (rc = upload(h, &h->d_tpz, pass_twiddles(nz))) || (rc = upload(h, &h->d_twx32, to_f32(unit_twiddles(nx)))) ||
+      (rc = upload(h, &h->d_tpx32, to_f32(pass_twiddles(nx / 2)))) ||
+      (rc = upload(h, &h->d_tpz32, to_f32(pass_twiddles(nz)))) ||
+      (rc = upload(h, &h->d_acc, std::vector<double>(64, 0.0))))
     return fail(rc);
   if ((rc = dev_alloc(h, &h->d_spec, (size_t)h->nkx * h->R)) || (rc = dev_alloc(h, &h->d_irho, h->n_rho)) ||
+      (rc = dev_alloc(h, &h->d_s, h->n_psi)) ||
       (rc = dev_alloc(h, &h->d_maxdiv, 1)))
     return fail(rc);
 
@@ -542,10 +675,24 @@ int tbfp_solve_fps_dev(tbfp_handle *h, const double *s, double *psi) {
   int rc = check_ptrs(h, {s, psi});
   if (rc) return rc;
   cudaSetDevice(h->device);
-  launch_fftx_fwd_from_s(s, h->Lpsi, h->g, h->plx, h->d_twx, h->d_spec, h->stream);
-  fps_spectral_solve(h);
-  launch_fftx_inv(h->d_spec, psi, h->Lpsi, h->hd_psi, h->g, h->plx, h->d_twx, h->scale, h->stream);
-  return finish(h, "tbfp_solve_fps");
+  TBFP_CK(h, cudaEventRecord(h->ev0, h->stream));
+  int iters = 1;
+  double rel = -1.0;
+  const int src = device_solve(h, s, psi, &iters, &rel);
+  if (src < 0) return src;
+  TBFP_CK(h, cudaEventRecord(h->ev1, h->stream));
+  h->last = tbfp_stats{};
+  h->last.iterations = iters;
+  h->last.rel_residual = rel;
+  h->last.max_div = -1.0;
+  h->last.cont_err = -1.0;
+  const int frc = finish(h, "tbfp_solve_fps");
+  if (frc) return frc;
+  if (!(h->flags & TBFP_FLAG_ASYNC)) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) h->last.ms_device = ms;
+  }
+  return src;
 }
 
 int tbfp_solve_fps(tbfp_handle *h, const double *s, double *psi) {
@@ -558,12 +705,12 @@ int tbfp_solve_fps(tbfp_handle *h, const double *s, double *psi) {
   if (h->hd_psi > 1 && (rc = h2d(h, h->h_psi, psi, h->n_psi))) return rc;
   const unsigned fl = h->flags;
   h->flags |= TBFP_FLAG_ASYNC;
-  rc = tbfp_solve_fps_dev(h, h->h_s, h->h_psi);
+  const int src = tbfp_solve_fps_dev(h, h->h_s, h->h_psi);
   h->flags = fl;
-  if (rc) return rc;
+  if (src < 0) return src;
   if ((rc = d2h(h, psi, h->h_psi, h->n_psi))) return rc;
   TBFP_CK(h, cudaStreamSynchronize(h->stream));
-  return TBFP_OK;
+  return src;
 }
 
 int tbfp_rhs_split_dev(tbfp_handle *h, const double *ux, const double *uy, const double *uz, const double *rho,
@@ -739,15 +886,76 @@ int tbfp_projection(tbfp_handle *h, double *ux, double *uy, double *uz, const do
   }
   const unsigned fl = h->flags;
   h->flags |= TBFP_FLAG_ASYNC;
-  rc = device_projection(h, h->h_ux, h->h_uy, h->h_uz, h->h_ux, h->h_uy, h->h_uz, h->h_rho, h->h_pn, h->h_pnm1,
-                         st ? dn : nullptr, st ? do_ : nullptr, dt, alpha, rho0, h->h_psi, stats);
+  const int prc = device_projection(h, h->h_ux, h->h_uy, h->h_uz, h->h_ux, h->h_uy, h->h_uz, h->h_rho, h->h_pn,
+                                    h->h_pnm1, st ? dn : nullptr, st ? do_ : nullptr, dt, alpha, rho0, h->h_psi, stats);
   h->flags = fl;
-  if (rc) return rc;
+  if (prc < 0) return prc;
   if ((rc = d2h(h, ux, h->h_ux, h->n_ux)) || (rc = d2h(h, uy, h->h_uy, h->n_uy)) ||
       (rc = d2h(h, uz, h->h_uz, h->n_uz)) || (rc = d2h(h, psi, h->h_psi, h->n_psi)))
     return rc;
   TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return prc;
+}
+
+// ---------------------------------------------------------------------------
+int tbfp_pcg_setup(tbfp_handle *h, const tbfp_mg_params *p) {
+  if (!h || !p) return TBFP_ENULL;
+  cudaSetDevice(h->device);
+  MgSolver *mg = new MgSolver();
+  std::string e;
+  const int rc = mg->init(*p, h->nx, h->ny, h->nz, h->mdxf.data(), h->mdxc.data(), h->mdyf.data(), h->mdyc.data(),
+                          h->mdzf.data(), h->mdzc.data(), &e);
+  if (rc != TBFP_OK) {
+    delete mg;
+    return set_err(h, rc, e);
+  }
+  delete h->mg;
+  h->mg = mg;
   return TBFP_OK;
+}
+
+int tbfp_pcg_solve_dev(tbfp_handle *h, double *psi, const double *beta, const double *q, tbfp_stats *stats) {
+  int rc = check_ptrs(h, {psi, beta, q});
+  if (rc) return rc;
+  if (!h->mg) return set_err(h, TBFP_EINVAL, "tbfp_pcg_solve: call tbfp_pcg_setup first");
+  cudaSetDevice(h->device);
+  TBFP_CK(h, cudaEventRecord(h->ev0, h->stream));
+  int iters = 0, cycles = 0;
+  double rel = -1.0;
+  std::string err;
+  const int src = h->mg->solve(psi, h->Lpsi, h->hd_psi, beta, h->Lrho, q, h->Lpsi, h->stream, &iters, &rel, &cycles,
+                               &err);
+  if (src < 0) return set_err(h, src, err);
+  TBFP_CK(h, cudaEventRecord(h->ev1, h->stream));
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->last = tbfp_stats{};
+  h->last.iterations = iters;
+  h->last.rel_residual = rel;
+  h->last.max_div = -1.0;
+  h->last.cont_err = -1.0;
+  h->last.ms_device = ms;
+  h->last.ms_stage[0] = cycles;  // V-cycles in total (informational)
+  if (stats) *stats = h->last;
+  return src;
+}
+
+int tbfp_pcg_solve(tbfp_handle *h, double *psi, const double *beta, const double *q, tbfp_stats *stats) {
+  int rc = check_ptrs(h, {psi, beta, q});
+  if (rc) return rc;
+  if (!h->mg) return set_err(h, TBFP_EINVAL, "tbfp_pcg_solve: call tbfp_pcg_setup first");
+  cudaSetDevice(h->device);
+  if ((rc = ensure_host_bufs(h, false))) return rc;
+  if (!h->h_beta && ((rc = dev_alloc(h, &h->h_beta, h->n_rho)) || (rc = dev_alloc(h, &h->h_q, h->n_psi)))) return rc;
+  if ((rc = h2d(h, h->h_psi, psi, h->n_psi)) || (rc = h2d(h, h->h_beta, beta, h->n_rho)) ||
+      (rc = h2d(h, h->h_q, q, h->n_psi)))
+    return rc;
+  const int src = tbfp_pcg_solve_dev(h, h->h_psi, h->h_beta, h->h_q, stats);
+  if (src < 0) return src;
+  if ((rc = d2h(h, psi, h->h_psi, h->n_psi))) return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return src;
 }
 
 }  // extern "C"

@@ -1,8 +1,9 @@
-// Device-side types shared by the projection kernels.
+// Device-side types, tile geometry and kernel launchers of the projection.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
 #include <string>
 
 #include "fft_smem.cuh"
@@ -53,34 +54,137 @@ struct CorrArgs {
   double invrho0;
 };
 
+// Source rows of the forward x transform.
+//   residual = false: s; with acc != nullptr also acc[0] += sum s*dyf(j) and
+//     acc[1] += sum s^2;
+//   residual = true: the refinement residual r = s - c [j == ny] - L psi of
+//     solveFPS's operator, with c = acc[0] * ctop_scale (the incompatible part
+//     of s, which the pinned (0,0) solve leaves on the top wall, so that the
+//     residual of the FP64 solution is zero), and acc_r[0] += sum r^2.
+struct XSrc {
+  const double *s;
+  Lay Ls;
+  const double *psi;
+  Lay Lp;
+  const double *am, *ap, *dyf;  // y operator coefficients and dyf(j), 0-based
+  double idx2, idz2;            // 1/dx^2, 1/dz^2 of the uniform x and z spacing
+  double ctop_scale;            // 1/(dyf(ny) nx nz)
+  double *acc, *acc_r;
+};
+
+// Transform lengths with a compiled kernel (nx/2 and nz): 2^a and 3*2^a, 4..512.
+#define TBFP_FFT_LENGTHS(X) \
+  X(4) X(6) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
+inline bool fft_length_supported(int n) {
+  switch (n) {
+#define TBFP_CASE(L) case L:
+    TBFP_FFT_LENGTHS(TBFP_CASE)
+#undef TBFP_CASE
+    return true;
+    default:
+      return false;
+  }
+}
+
+// --- tile geometry (shared by the host launchers and the kernels) -----------
+constexpr int kNT = 256;  // threads per CTA of the transform kernels (8 warps)
+constexpr int kNW = kNT / 32;
+constexpr int kWPB = 4;   // warps per CTA of the tridiagonal kernel
+
+// Each warp transforms its own sequences (rows of x, columns of z) with
+// __syncwarp only, 8 complex values per lane (16 for length 512).
+// Sequences per warp: the largest power of two keeping n*spw <= 256, or 1.
+__host__ __device__ constexpr int ct_lognb(int n) { return n >= 256 ? 0 : ct_log2(256 / n); }
+// Row stride of an x tile (complex slots): holds pad8(M)+1 slots; with nb rows
+// per warp interleaved in a phase of 8 lanes, rows must land on distinct
+// 16-byte bank groups: stride = (8/nb)*odd (mod 8) for nb < 8, odd for nb >= 8.
+__host__ __device__ constexpr int x_row_stride(int M) {
+  const int nb = 1 << ct_lognb(M);
+  int ld = pad8(M) + 1;
+  if (nb == 1) return ld;
+  const int want = nb >= 8 ? 1 : 8 / nb;  // required residue pattern
+  while (!((ld % 8) % want == 0 && ((ld % 8) / want) % 2 == 1)) ++ld;
+  return ld;
+}
+// Row stride of a z tile: the tile's 8*nb columns plus a skew for small nb.
+__host__ __device__ constexpr int z_row_stride(int nz) {
+  const int nb = 1 << ct_lognb(nz);
+  return 8 * nb + (nb <= 4 ? nb : 0);
+}
+__host__ __device__ constexpr int fftx_rows_per_cta(int M) { return kNW << ct_lognb(M); }
+__host__ __device__ constexpr int fftz_cols_per_cta(int nz) { return kNW << ct_lognb(nz); }
+// dynamic shared memory: tile + twiddle table, elements of esz bytes (16 for
+// double2, 8 for float2)
+__host__ __device__ constexpr size_t fftx_smem_bytes(int M, size_t esz = 16) {
+  return ((size_t)fftx_rows_per_cta(M) * x_row_stride(M) + M) * esz;
+}
+__host__ __device__ constexpr size_t fftz_smem_bytes(int nz, size_t esz = 16) {
+  return ((size_t)z_row_stride(nz) * (pad8(nz - 1) + 1) + nz) * esz;
+}
+// y systems: one lane owns T = ceil(ny/32) consecutive rows; a warp holds two
+// complex right-hand sides and two real coefficients per row
+inline int tri_rows_per_lane(int ny) { return (ny + 31) / 32; }
+inline size_t tridiag_smem_bytes(int ny) {
+  return (size_t)kWPB * 33 * tri_rows_per_lane(ny) * (2 * sizeof(double2) + 2 * sizeof(double));
+}
+
+// Pass-ordered twiddle table of a length-n transform (fft_smem.cuh), n
+// entries (the last R_0 unused), evaluated in extended precision.
+inline void fft_pass_twiddles(int n, double2 *out) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int e = 0; e < n; ++e) out[e] = make_double2(0.0, 0.0);
+  const int r0 = ct_rad(n, 0);
+  for (int p = 1; p < ct_nrad(n); ++p) {
+    const int R = ct_rad(n, p), NS = ct_ns(n, p);
+    for (int k0 = 0; k0 < NS; ++k0)
+      for (int r = 1; r < R; ++r) {
+        const long double a = 2.0L * pi * (long double)(k0 * r) / (long double)(NS * R);
+        out[NS - r0 + k0 * (R - 1) + (r - 1)] = make_double2((double)cosl(a), (double)(-sinl(a)));
+      }
+  }
+}
+// exp(-2*pi*i*m/n), m = 0..n-1 (the r2c/c2r post-processing factors for n = nx).
+inline void fft_unit_twiddles(int n, double2 *out) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int m = 0; m < n; ++m) {
+    const long double a = 2.0L * pi * (long double)m / (long double)n;
+    out[m] = make_double2((double)cosl(a), (double)(-sinl(a)));
+  }
+}
+
 // Error text returned by tbfp_last_error(NULL) (defined in tbfp_api.cu).
 void set_global_error(const std::string &msg);
 
-// Kernel launchers (defined in tbfp_kernels.cu).
+// Kernel launchers.  The x launchers take twx (fft_unit_twiddles(nx)) and tpx
+// (fft_pass_twiddles(nx/2)); the z launcher takes tpz (fft_pass_twiddles(nz)).
+cudaError_t prepare_kernels();  // raises the shared-memory limits; once per device
 void launch_recip(const double *rho, double *irho, long n, cudaStream_t st);
-cudaError_t prepare_kernels();
-int fft_max_length();
-int fftx_rows_per_cta(int M);
-int fftz_cols_per_cta(int nz);
-size_t fftx_smem_bytes(int M);
-size_t fftz_smem_bytes(int nz);
-size_t tridiag_smem_bytes(int ny);
-
-void launch_fftx_fwd_from_s(const double *s, Lay Ls, const GridK &g, const FftPlan &pl, const double2 *twx,
+void launch_fftx_fwd_from_s(const double *s, Lay Ls, const GridK &g, const double2 *twx, const double2 *tpx,
                             double2 *spec, cudaStream_t st);
-void launch_fftx_fwd_rhs(const RhsArgs &ra, bool has_st, const GridK &g, const FftPlan &pl, const double2 *twx,
-                         double2 *spec, cudaStream_t st);
 void launch_rhs(const RhsArgs &ra, bool has_st, const GridK &g, double *s, Lay Ls, cudaStream_t st);
-void launch_fftz(double2 *spec, const GridK &g, const FftPlan &pl, const double2 *twz, bool inverse,
-                 cudaStream_t st);
+void launch_fftz(double2 *spec, const GridK &g, const double2 *tpz, bool inverse, cudaStream_t st);
+void launch_fftz(float2 *spec, const GridK &g, const float2 *tpz, bool inverse, cudaStream_t st);
 void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st);
-void launch_fftx_inv(const double2 *spec, double *psi, Lay Lp, int hd, const GridK &g, const FftPlan &pl,
-                     const double2 *twx, double scale, cudaStream_t st);
+void launch_tridiag(float2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
+                    const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st);
+void launch_fftx_inv(const double2 *spec, double *psi, Lay Lp, int hd, const GridK &g, const double2 *twx,
+                     const double2 *tpx, double scale, cudaStream_t st);
+// mixed path: FP32 spectrum, psi = (accumulate ? psi : 0) + scale * c2r(spec)
+void launch_fftx_inv(const float2 *spec, double *psi, Lay Lp, int hd, const GridK &g, const float2 *twx,
+                     const float2 *tpx, double scale, bool accumulate, cudaStream_t st);
+void launch_fftx_fwd(const XSrc &src, bool residual, const GridK &g, const double2 *twx, const double2 *tpx,
+                     double2 *spec, cudaStream_t st);
+void launch_fftx_fwd(const XSrc &src, bool residual, const GridK &g, const float2 *twx, const float2 *tpx,
+                     float2 *spec, cudaStream_t st);
 void launch_correct_div(const CorrArgs &ca, bool has_st, const GridK &g, unsigned long long *maxdiv,
                         cudaStream_t st);
 void launch_correct_inplace(const CorrArgs &ca, bool has_st, const GridK &g, cudaStream_t st);
 void launch_div(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz, const GridK &g,
                 unsigned long long *maxdiv, cudaStream_t st);
+
+// per-file parts of prepare_kernels()
+cudaError_t prepare_xfft_kernels();
+cudaError_t prepare_yz_kernels();
 
 }  // namespace tbfp

@@ -52,9 +52,10 @@ constexpr long kOffIdyf = kOffDyf + rup(kNyMax);          // ny
 constexpr long kOffIdyc = kOffIdyf + rup(kNyMax);         // ny+1
 constexpr long kOffIdxf = kOffIdyc + rup(kNyMax + 1);     // nx
 constexpr long kOffIdzf = kOffIdxf + rup(kNxMax);         // nz
-constexpr long kOffTwx = kOffIdzf + rup(kNzMax);          // nx complex
-constexpr long kOffTwz = kOffTwx + rup(2 * kNxMax);       // nz complex
-constexpr long kTableEnd = kOffTwz + rup(2 * kNzMax);
+constexpr long kOffTwx = kOffIdzf + rup(kNzMax);          // nx complex: r2c/c2r factors
+constexpr long kOffTpx = kOffTwx + rup(2 * kNxMax);       // nx/2 complex: pass twiddles of nx/2
+constexpr long kOffTpz = kOffTpx + rup(kNxMax);           // nz complex: pass twiddles of nz
+constexpr long kTableEnd = kOffTpz + rup(2 * kNzMax);
 constexpr long kTableDoubles = kTableEnd - kOffLamx;
 
 // The scratch array: spectrum, then the set-up tables.  256-byte aligned so
@@ -89,21 +90,8 @@ extern "C" int tbfp_solve_fps_noalloc(const tbfp_desc *d, const double *s, doubl
     return fail(TBFP_EUNSUPPORTED,
                 "tbfp_solve_fps_noalloc: grid exceeds the static scratch ((nx/2+1)*ny*nz <= 4194304, "
                 "nx <= 4096, ny <= 2048, nz <= 2048); use tbfp_create/tbfp_solve_fps_dev");
-  FftPlan plx{}, plz{};
-  // same radix plans as tbfp_create: 8s, then 4, then 2, one 3 last
-  auto plan = [](int n, FftPlan *pl) {
-    std::memset(pl, 0, sizeof(*pl));
-    pl->n = n;
-    int m = n, k = 0;
-    while (m % 8 == 0 && m > 1 && k < 16) { pl->rad[k++] = 8; m /= 8; }
-    while (m % 4 == 0 && k < 16) { pl->rad[k++] = 4; m /= 4; }
-    while (m % 2 == 0 && k < 16) { pl->rad[k++] = 2; m /= 2; }
-    if (m % 3 == 0) { pl->rad[k++] = 3; m /= 3; }
-    pl->nrad = k;
-    return m == 1;
-  };
-  if (!plan(nx / 2, &plx) || !plan(nz, &plz) || nx / 2 > fft_max_length() || nz > fft_max_length())
-    return fail(TBFP_EUNSUPPORTED, "tbfp_solve_fps_noalloc: nx/2 and nz must be 2^a or 3*2^a within the tile length");
+  if (!fft_length_supported(nx / 2) || !fft_length_supported(nz))
+    return fail(TBFP_EUNSUPPORTED, "tbfp_solve_fps_noalloc: nx/2 and nz must be 2^a or 3*2^a between 4 and 512");
   if (tridiag_smem_bytes(ny) > 227 * 1024)
     return fail(TBFP_EUNSUPPORTED, "tbfp_solve_fps_noalloc: ny too large for the shared-memory tiles");
 
@@ -132,7 +120,10 @@ extern "C" int tbfp_solve_fps_noalloc(const tbfp_desc *d, const double *s, doubl
   auto T = [&](long off) { return t + (off - kOffLamx); };
   const double pi = 3.14159265358979323846;
   for (int i = 0; i < nkx; ++i) T(kOffLamx)[i] = 2.0 * (std::cos(((double)i * 2.0 * pi) / nx) - 1.0) / (d->dx_fft * d->dx_fft);
-  for (int k = 0; k < nz; ++k) T(kOffLamz)[k] = 2.0 * (std::cos(((double)k * 2.0 * pi) / nz) - 1.0) / (d->dz_fft * d->dz_fft);
+  for (int k = 0; k < nz; ++k) {  // even in k, as in tbfp_create
+    const int kk = k < nz - k ? k : nz - k;
+    T(kOffLamz)[k] = 2.0 * (std::cos(((double)kk * 2.0 * pi) / nz) - 1.0) / (d->dz_fft * d->dz_fft);
+  }
   for (int j = 0; j < ny; ++j) {
     T(kOffAm)[j] = 1.0 / (d->dyc[j] * d->dyf[j]);
     T(kOffAp)[j] = 1.0 / (d->dyc[j + 1] * d->dyf[j]);
@@ -144,17 +135,9 @@ extern "C" int tbfp_solve_fps_noalloc(const tbfp_desc *d, const double *s, doubl
   for (int j = 0; j <= ny; ++j) T(kOffIdyc)[j] = 1.0 / d->dyc[j];
   for (int i = 0; i < nx; ++i) T(kOffIdxf)[i] = 1.0 / d->dxf[i];
   for (int k = 0; k < nz; ++k) T(kOffIdzf)[k] = 1.0 / d->dzf[k];
-  const long double lpi = 3.141592653589793238462643383279502884L;
-  for (int m = 0; m < nx; ++m) {
-    const long double a = 2.0L * lpi * (long double)m / (long double)nx;
-    T(kOffTwx)[2 * m] = (double)cosl(a);
-    T(kOffTwx)[2 * m + 1] = (double)(-sinl(a));
-  }
-  for (int m = 0; m < nz; ++m) {
-    const long double a = 2.0L * lpi * (long double)m / (long double)nz;
-    T(kOffTwz)[2 * m] = (double)cosl(a);
-    T(kOffTwz)[2 * m + 1] = (double)(-sinl(a));
-  }
+  fft_unit_twiddles(nx, reinterpret_cast<double2 *>(T(kOffTwx)));
+  fft_pass_twiddles(nx / 2, reinterpret_cast<double2 *>(T(kOffTpx)));
+  fft_pass_twiddles(nz, reinterpret_cast<double2 *>(T(kOffTpz)));
   double sVg = d->s_Vg;
   if (!(sVg > 0.0)) {
     sVg = 0.0;
@@ -190,14 +173,15 @@ extern "C" int tbfp_solve_fps_noalloc(const tbfp_desc *d, const double *s, doubl
   Lp.sk = Lp.sj * (ny + 2 * d->hd_psi);
   double2 *spec = reinterpret_cast<double2 *>(base);
   const double2 *twx = reinterpret_cast<const double2 *>(base + kOffTwx);
-  const double2 *twz = reinterpret_cast<const double2 *>(base + kOffTwz);
+  const double2 *tpx = reinterpret_cast<const double2 *>(base + kOffTpx);
+  const double2 *tpz = reinterpret_cast<const double2 *>(base + kOffTpz);
 
-  launch_fftx_fwd_from_s(s, Lp, g, plx, twx, spec, st);
-  launch_fftz(spec, g, plz, twz, false, st);
+  launch_fftx_fwd_from_s(s, Lp, g, twx, tpx, spec, st);
+  launch_fftz(spec, g, tpz, false, st);
   launch_tridiag(spec, g, base + kOffLamx, base + kOffLamz, base + kOffAm, base + kOffAp, base + kOffDyf,
                  d->dx_fft * d->dz_fft / sVg, (double)nx * (double)nz, st);
-  launch_fftz(spec, g, plz, twz, true, st);
-  launch_fftx_inv(spec, psi, Lp, d->hd_psi, g, plx, twx, 1.0 / ((double)nx * (double)nz), st);
+  launch_fftz(spec, g, tpz, true, st);
+  launch_fftx_inv(spec, psi, Lp, d->hd_psi, g, twx, tpx, 1.0 / ((double)nx * (double)nz), st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(TBFP_ECUDA, std::string("tbfp_solve_fps_noalloc launch: ") + cudaGetErrorString(e));
   e = cudaStreamSynchronize(st);

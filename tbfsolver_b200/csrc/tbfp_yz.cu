@@ -1,0 +1,360 @@
+// FP64 z transforms and y (tridiagonal) solves of the split-pressure
+// projection (FAST_MODE of the reference), on the spectrum S[kx][row],
+// row = (k-1)*ny + (j-1):
+//   * the z transform of a fixed (kx, j) column strides by ny (a CTA stages a
+//     tile of consecutive j columns for all k in shared memory),
+//   * the y system of a fixed (kx, kz) is the contiguous run S[kx][kz*ny ...].
+#include <cuda_runtime.h>
+
+#include "tbfp_kernels.cuh"
+
+namespace tbfp {
+
+// ---------------------------------------------------------------------------
+// z transform (forward or backward) of a tile of TJZ consecutive j columns of
+// one kx plane, staged in shared memory (row k of the tile at pad8(k)*ES).
+// ---------------------------------------------------------------------------
+template <typename V, bool INV, int NZ>
+__global__ void __launch_bounds__(kNT, (NZ >= 384 ? 2 : 3)) k_fftz(V *__restrict__ spec, GridK g,
+                                                               const V *__restrict__ tpz) {
+  constexpr int LOGCPW = ct_lognb(NZ), LOGT = LOGCPW + 3, TJZ = 1 << LOGT;
+  constexpr int ES = z_row_stride(NZ), ROWS = pad8(NZ - 1) + 1;
+  constexpr int NL = (NZ << LOGT) / kNT;  // elements per thread (NZ*TJZ is a multiple of kNT)
+  static_assert((NZ << LOGT) % kNT == 0, "z tile must split evenly over the CTA");
+  extern __shared__ __align__(16) unsigned char smz[];
+  V *sm = reinterpret_cast<V *>(smz);
+  V *tw = sm + ES * ROWS;
+  for (int t = threadIdx.x; t < ct_twiddle_len(NZ); t += kNT) tw[t] = tpz[t];
+  const int kx = blockIdx.y;
+  const int j0 = blockIdx.x << LOGT;
+  const int nj = min(TJZ, g.ny - j0);
+  const int ny = g.ny;
+  V *base = spec + (long)kx * g.R + j0;
+#pragma unroll
+  for (int c = 0; c < NL; ++c) {
+    const int t = threadIdx.x + kNT * c;
+    const int k = t >> LOGT, jj = t & (TJZ - 1);
+    sm[pad8(k) * ES + jj] = (jj < nj) ? base[(long)k * ny + jj] : mk<V>(0, 0);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  fft_warp<V, NZ, LOGCPW, ES, 1, INV>(sm + (warp << LOGCPW), lane, tw);
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < NL; ++c) {
+    const int t = threadIdx.x + kNT * c;
+    const int k = t >> LOGT, jj = t & (TJZ - 1);
+    if (jj < nj) base[(long)k * ny + jj] = sm[pad8(k) * ES + jj];
+  }
+}
+
+template <typename V, int NZ>
+static void launch_fftz_n(V *spec, const GridK &g, const V *tpz, bool inverse, cudaStream_t st) {
+  constexpr int TJZ = fftz_cols_per_cta(NZ);
+  constexpr size_t smem = fftz_smem_bytes(NZ, sizeof(V));
+  dim3 grid((g.ny + TJZ - 1) / TJZ, g.nkx);
+  if (inverse) k_fftz<V, true, NZ><<<grid, kNT, smem, st>>>(spec, g, tpz);
+  else k_fftz<V, false, NZ><<<grid, kNT, smem, st>>>(spec, g, tpz);
+}
+
+template <typename V>
+static void launch_fftz_t(V *spec, const GridK &g, const V *tpz, bool inverse, cudaStream_t st) {
+  switch (g.nz) {
+#define TBFP_CASE(L) \
+  case L: launch_fftz_n<V, L>(spec, g, tpz, inverse, st); break;
+    TBFP_FFT_LENGTHS(TBFP_CASE)
+#undef TBFP_CASE
+    default: break;  // lengths are validated by tbfp_create
+  }
+}
+void launch_fftz(double2 *spec, const GridK &g, const double2 *tpz, bool inverse, cudaStream_t st) {
+  launch_fftz_t(spec, g, tpz, inverse, st);
+}
+void launch_fftz(float2 *spec, const GridK &g, const float2 *tpz, bool inverse, cudaStream_t st) {
+  launch_fftz_t(spec, g, tpz, inverse, st);
+}
+
+// ---------------------------------------------------------------------------
+// y systems (solveTriDiag, fastPoissonSolver.f90:280-333).  Row j (0-based) of
+// the reference, before its row scaling by r = 1/(lam - am - ap), is
+//     am_j x_{j-1} + (lam - am_j - ap_j) x_j + ap_j x_{j+1} = f_j,
+// lam = lamx(kx) + lamz(kz).  lamz is even in kz (the host table is built
+// symmetric), so the systems kz and nz-kz have the same matrix: one warp solves
+// both, computing the elimination coefficients once for two right-hand sides.
+// Lane l owns the T = ceil(ny/32) consecutive rows [l*T, l*T+len) (partition
+// method).  Forward within the block, with g_i = 1/(lam - am_i - ap_i - am_i ct_{i-1})
+// (ct, dt = 0 and at = -1 before the block):
+//   at_i x_{s-1} + x_i + ct_i x_{i+1} = dt_i,
+//   at_i = -am_i at_{i-1} g_i,  ct_i = ap_i g_i,  dt_i = (f_i - am_i dt_{i-1}) g_i,
+// which is the reference's scaled elimination (a = am r, c = ap r, d = f r)
+// with r cancelled.  A running backward pass gives
+//   x_s = hd - ha x_{s-1} - hc x_e,
+// so each lane contributes one reduced equation in y_l = x_{e_l}:
+//   at_e y_{l-1} + (1 - ct_e ha') y_l - ct_e hc' y_{l+1} = dt_e - ct_e hd'
+// (primes: the next lane's values), solved by parallel cyclic reduction over
+// the warp; then x_i = dt_i - at_i y_{l-1} - ct_i x_{i+1}.
+// The singular (0,0) system (Neumann walls) is gauged by pinning its last
+// unknown to zero and solved by one lane (Thomas: the cyclic reduction loses
+// digits on this only weakly diagonally dominant system); then its
+// volume-weighted mean is removed in spectral space:
+// sum_{i,k} p(i,j,k) = X(0,j,0), so zeroAveragePressure (:388-423) is
+// X(0,j,0) -= nx*nz * dx*dz*sum_j dyf(j) X(0,j,0) / s_Vg.
+// Shared memory per warp: row t of lane l at [t*33 + l] (conflict-free) for the
+// two right-hand sides and the two coefficient arrays.  The arithmetic is FP64
+// for both spectrum types (float2 spectra are widened on load).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+__device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+
+template <typename V>
+__global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, GridK g,
+                                                       const double *__restrict__ lamx,
+                                                       const double *__restrict__ lamz,
+                                                       const double *__restrict__ am, const double *__restrict__ ap,
+                                                       const double *__restrict__ dyf, double mean_c, double nxnz,
+                                                       int T, unsigned magicT) {
+  extern __shared__ unsigned char smraw[];
+  const int ny = g.ny, nz = g.nz;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int W = 33 * T;
+  double2 *d0 = reinterpret_cast<double2 *>(smraw) + warp * 2 * W;
+  double2 *d1 = d0 + W;
+  double *ca = reinterpret_cast<double *>(reinterpret_cast<double2 *>(smraw) + kWPB * 2 * W) + warp * 2 * W;
+  double *cc = ca + W;
+  const int nzh = nz / 2 + 1;  // kz = 0..nz/2 (nz is even)
+  const unsigned q = blockIdx.x * kWPB + warp;
+  if (q >= (unsigned)(g.nkx * nzh)) return;  // whole warp leaves; no block-level barrier follows
+  const int kx = (int)(q / (unsigned)nzh), kz = (int)(q - (unsigned)kx * nzh);
+  const int kz2 = (kz == 0) ? 0 : nz - kz;  // partner system (itself at kz = 0 and nz/2)
+  const bool two = kz2 != kz;
+  V *S0 = spec + (long)kx * g.R + (long)kz * ny;
+  V *S1 = spec + (long)kx * g.R + (long)kz2 * ny;
+  using VT = decltype(V::x);
+  auto ld = [](const V v) { return mk<double2>((double)v.x, (double)v.y); };
+  auto st = [](double2 v) { return mk<V>((VT)v.x, (VT)v.y); };
+
+  // slot of global row e: lane e/T (by the multiplier, exact for e < 2^16), row e mod T
+  auto slot = [&](int e) -> int {
+    const int l = (T == 1) ? e : (int)__umulhi((unsigned)e, magicT);
+    return (e - l * T) * 33 + l;
+  };
+  for (int e = lane; e < ny; e += 32) {
+    const int sl = slot(e);
+    d0[sl] = ld(S0[e]);
+    if (two) d1[sl] = ld(S1[e]);
+  }
+  __syncwarp();
+
+  const double lam = lamx[kx] + lamz[kz];
+  const bool pin = (kx == 0 && kz == 0);
+  if (pin) {
+    if (lane == 0) {
+      double ct_p = 0.0;
+      double2 dt_p = mk<double2>(0.0, 0.0);
+      for (int e = 0; e < ny; ++e) {
+        const int sl = slot(e);
+        double ct = 0.0;
+        double2 dt = mk<double2>(0.0, 0.0);
+        if (e < ny - 1) {
+          const double a = am[e], c = ap[e];
+          const double2 f = d0[sl];
+          const double gi = 1.0 / ((lam - a - c) - a * ct_p);
+          ct = c * gi;
+          dt = mk<double2>((f.x - a * dt_p.x) * gi, (f.y - a * dt_p.y) * gi);
+        }
+        cc[sl] = ct;
+        d0[sl] = dt;
+        ct_p = ct;
+        dt_p = dt;
+      }
+      double2 xn = d0[slot(ny - 1)];
+      for (int e = ny - 2; e >= 0; --e) {
+        const int sl = slot(e);
+        const double c = cc[sl];
+        xn = mk<double2>(d0[sl].x - c * xn.x, d0[sl].y - c * xn.y);
+        d0[sl] = xn;
+      }
+    }
+    __syncwarp();
+    double sx = 0.0, sy = 0.0;
+    for (int e = lane; e < ny; e += 32) {
+      const double2 v = d0[slot(e)];
+      sx += v.x * dyf[e];
+      sy += v.y * dyf[e];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sx += __shfl_xor_sync(0xffffffffu, sx, o);
+      sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    const double subx = sx * mean_c * nxnz, suby = sy * mean_c * nxnz;
+    for (int e = lane; e < ny; e += 32) {
+      const int sl = slot(e);
+      S0[e] = st(mk<double2>(d0[sl].x - subx, d0[sl].y - suby));
+    }
+    return;
+  }
+
+  const int NL = (ny + T - 1) / T;  // active lanes
+  const bool active = lane < NL;
+  const int s0 = lane * T;
+  const int len = active ? min(T, ny - s0) : 0;
+  // forward elimination within the lane's block
+  double at_e = 0.0, ct_e = 0.0;
+  double2 e0 = mk<double2>(0.0, 0.0), e1 = mk<double2>(0.0, 0.0);
+  if (active) {
+    double at_p = -1.0, ct_p = 0.0;
+    double2 p0 = mk<double2>(0.0, 0.0), p1 = mk<double2>(0.0, 0.0);
+    for (int t = 0; t < len; ++t) {
+      const int i = s0 + t;
+      const double a = am[i], c = ap[i];
+      const int sl = t * 33 + lane;
+      const double gi = 1.0 / ((lam - a - c) - a * ct_p);
+      const double at = -a * at_p * gi, ct = c * gi;
+      const double2 f0 = d0[sl], f1 = d1[sl];
+      p0 = mk<double2>((f0.x - a * p0.x) * gi, (f0.y - a * p0.y) * gi);
+      p1 = mk<double2>((f1.x - a * p1.x) * gi, (f1.y - a * p1.y) * gi);
+      ca[sl] = at;
+      cc[sl] = ct;
+      d0[sl] = p0;
+      d1[sl] = p1;
+      at_p = at;
+      ct_p = ct;
+    }
+    at_e = at_p;
+    ct_e = ct_p;
+    e0 = p0;
+    e1 = p1;
+  }
+  // running backward pass for x_s in terms of x_{s-1} and x_e
+  double ha = 0.0, hc = -1.0;
+  double2 h0 = mk<double2>(0.0, 0.0), h1 = mk<double2>(0.0, 0.0);
+  if (active && len >= 2) {
+    int sl = (len - 2) * 33 + lane;
+    h0 = d0[sl];
+    h1 = d1[sl];
+    ha = ca[sl];
+    hc = cc[sl];
+    for (int t = len - 3; t >= 0; --t) {
+      sl = t * 33 + lane;
+      const double ct = cc[sl];
+      const double2 v0 = d0[sl], v1 = d1[sl];
+      h0 = mk<double2>(v0.x - ct * h0.x, v0.y - ct * h0.y);
+      h1 = mk<double2>(v1.x - ct * h1.x, v1.y - ct * h1.y);
+      ha = ca[sl] - ct * ha;
+      hc = -ct * hc;
+    }
+  }
+  // reduced equation of this lane: A y_{l-1} + B y_l + C y_{l+1} = D
+  const double ha_n = shdn(ha, 1), hc_n = shdn(hc, 1);
+  const double h0x = shdn(h0.x, 1), h0y = shdn(h0.y, 1), h1x = shdn(h1.x, 1), h1y = shdn(h1.y, 1);
+  double A = 0.0, B = 1.0, C = 0.0;
+  double D[4] = {0.0, 0.0, 0.0, 0.0};
+  if (active) {
+    A = at_e;
+    D[0] = e0.x;
+    D[1] = e0.y;
+    D[2] = e1.x;
+    D[3] = e1.y;
+    if (lane + 1 < NL) {
+      B = 1.0 - ct_e * ha_n;
+      C = -ct_e * hc_n;
+      D[0] -= ct_e * h0x;
+      D[1] -= ct_e * h0y;
+      D[2] -= ct_e * h1x;
+      D[3] -= ct_e * h1y;
+    }
+  }
+  // parallel cyclic reduction over the 32 reduced equations
+#pragma unroll
+  for (int h = 1; h < 32; h <<= 1) {
+    double Am = shup(A, h), Bm = shup(B, h), Cm = shup(C, h);
+    double Ap = shdn(A, h), Bp = shdn(B, h), Cp = shdn(C, h);
+    double Dm[4], Dp[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      Dm[c] = shup(D[c], h);
+      Dp[c] = shdn(D[c], h);
+    }
+    const bool lo = lane < h, hi = lane + h >= 32;
+    if (lo) { Am = 0.0; Bm = 1.0; Cm = 0.0; }
+    if (hi) { Ap = 0.0; Bp = 1.0; Cp = 0.0; }
+    const double k1 = A / Bm, k2 = C / Bp;
+    const double nB = B - k1 * Cm - k2 * Ap;
+    A = -k1 * Am;
+    C = -k2 * Cp;
+    B = nB;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) D[c] = D[c] - (lo ? 0.0 : k1 * Dm[c]) - (hi ? 0.0 : k2 * Dp[c]);
+  }
+  const double iB = 1.0 / B;
+  double y[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) y[c] = D[c] * iB;
+  double ys[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double v = shup(y[c], 1);  // every lane takes part in the shuffle
+    ys[c] = (lane == 0) ? 0.0 : v;
+  }
+  if (active) {
+    double2 x0 = mk<double2>(y[0], y[1]), x1 = mk<double2>(y[2], y[3]);
+    d0[(len - 1) * 33 + lane] = x0;
+    d1[(len - 1) * 33 + lane] = x1;
+    for (int t = len - 2; t >= 0; --t) {
+      const int sl = t * 33 + lane;
+      const double a = ca[sl], c = cc[sl];
+      const double2 v0 = d0[sl], v1 = d1[sl];
+      x0 = mk<double2>(v0.x - a * ys[0] - c * x0.x, v0.y - a * ys[1] - c * x0.y);
+      x1 = mk<double2>(v1.x - a * ys[2] - c * x1.x, v1.y - a * ys[3] - c * x1.y);
+      d0[sl] = x0;
+      d1[sl] = x1;
+    }
+  }
+  __syncwarp();
+  for (int e = lane; e < ny; e += 32) {
+    const int sl = slot(e);
+    S0[e] = st(d0[sl]);
+    if (two) S1[e] = st(d1[sl]);
+  }
+}
+
+template <typename V>
+static void launch_tridiag_t(V *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
+                             const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st) {
+  const long nwarps = (long)g.nkx * (g.nz / 2 + 1);
+  const long nblk = (nwarps + kWPB - 1) / kWPB;
+  const int T = tri_rows_per_lane(g.ny);
+  // e/T == umulhi(e, floor(2^32/T) + 1) for every e < 2^16 (and T <= 2^16)
+  const unsigned magic = T > 1 ? (unsigned)((1ull << 32) / (unsigned long long)T + 1ull) : 0u;
+  k_tridiag<V><<<(unsigned)nblk, kWPB * 32, tridiag_smem_bytes(g.ny), st>>>(spec, g, lamx, lamz, am, ap, dyf,
+                                                                            mean_c, nxnz, T, magic);
+}
+void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
+                    const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st) {
+  launch_tridiag_t(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, st);
+}
+void launch_tridiag(float2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
+                    const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st) {
+  launch_tridiag_t(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, st);
+}
+
+cudaError_t prepare_yz_kernels() {
+  cudaError_t e = cudaSuccess;
+  auto set = [&](const void *fn, size_t bytes) {
+    const cudaError_t ee = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (ee != cudaSuccess) e = ee;
+  };
+#define TBFP_CASE(L)                                                             \
+  set((const void *)k_fftz<double2, false, L>, fftz_smem_bytes(L, 16));          \
+  set((const void *)k_fftz<double2, true, L>, fftz_smem_bytes(L, 16));           \
+  set((const void *)k_fftz<float2, false, L>, fftz_smem_bytes(L, 8));            \
+  set((const void *)k_fftz<float2, true, L>, fftz_smem_bytes(L, 8));
+  TBFP_FFT_LENGTHS(TBFP_CASE)
+#undef TBFP_CASE
+  set((const void *)k_tridiag<double2>, 227 * 1024);
+  set((const void *)k_tridiag<float2>, 227 * 1024);
+  return e;
+}
+
+}  // namespace tbfp

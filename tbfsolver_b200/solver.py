@@ -9,6 +9,9 @@ Names and argument meaning follow the Fortran modules they replace:
 * ``make_velocity_div_free`` -- momentumEqn.f90:999 (FAST_MODE).
 * ``compute_continuity_error`` -- auxiliaryRoutines.f90:42 (returns the value
   instead of printing it).
+* ``PCG``                -- pcgMod (src/pcg/pcg.f90) with its multigrid preconditioner
+  (multiGridMod, rbgsMod, poissMatMod): ``PCG(mesh, ...)`` is pcgCTOR (:62),
+  ``solve_pcg(psi, beta, q)`` is solvePCG (:103).
 
 The reference's old time levels ``psi%ptrf_`` and ``psi%ptrf_%ptrf_`` are
 passed explicitly as ``psi_n`` and ``psi_nm1``; the surface-tension old levels
@@ -24,8 +27,8 @@ import ctypes as C
 
 import numpy as np
 
-from ._native import (TBFP_EINVAL, TBFP_FLAG_ASYNC, TBFP_FLAG_TIMING, TBFP_FP64, TBFP_MIXED, TbfpDesc, TbfpError,
-                      TbfpStats, check, load)
+from ._native import (TBFP_EINVAL, TBFP_FLAG_ASYNC, TBFP_FLAG_RESIDUAL, TBFP_FLAG_TIMING, TBFP_FP64, TBFP_MIXED,
+                      TbfpDesc, TbfpError, TbfpMgParams, TbfpStats, check, load)
 from .fields import Field, VField
 from .grid import Grid
 
@@ -61,7 +64,8 @@ class FastPoissonSolver:
 
     def __init__(self, mesh: Grid, hd_psi: int = 1, hd_u: int = 2, hd_rho: int = 1, hd_st: int = 1,
                  precision: str = "fp64", tol: float = 1e-10, max_iter: int = 8, device: int = -1,
-                 stream: int | None = None, asynchronous: bool = False, timing: bool = False):
+                 stream: int | None = None, asynchronous: bool = False, timing: bool = False,
+                 residual: bool = False):
         self.lib = load()
         self.mesh = mesh
         self.hd_psi, self.hd_u, self.hd_rho, self.hd_st = hd_psi, hd_u, hd_rho, hd_st
@@ -78,7 +82,8 @@ class FastPoissonSolver:
                      dxf=_dptr(self._m["dxf"]), dxc=_dptr(self._m["dxc"]), dyf=_dptr(self._m["dyf"]),
                      dyc=_dptr(self._m["dyc"]), dzf=_dptr(self._m["dzf"]), dzc=_dptr(self._m["dzc"]),
                      s_Vg=mesh.s_Vg, precision=prec, tol=tol, max_iter=max_iter, device=device,
-                     stream=stream, flags=(TBFP_FLAG_ASYNC if asynchronous else 0) | (TBFP_FLAG_TIMING if timing else 0))
+                     stream=stream, flags=(TBFP_FLAG_ASYNC if asynchronous else 0) | (TBFP_FLAG_TIMING if timing else 0)
+                     | (TBFP_FLAG_RESIDUAL if residual else 0))
         h = C.c_void_p()
         check(self.lib.tbfp_create(C.byref(d), C.byref(h)), None)
         self.h = h
@@ -117,14 +122,21 @@ class FastPoissonSolver:
             if f.kind != "cl" or f.hd != self.hd_psi:
                 raise TbfpError(TBFP_EINVAL, f"expected a 'cl' field with halo {self.hd_psi}")
 
+    def last_stats(self) -> TbfpStats:
+        """Statistics of the last solve or projection (tbfp_get_stats)."""
+        st = TbfpStats()
+        check(self.lib.tbfp_get_stats(self.h, C.byref(st)), self.h)
+        return st
+
     # --- solveFPS ----------------------------------------------------------
-    def solve_fps(self, p: Field, s: Field) -> None:
+    def solve_fps(self, p: Field, s: Field) -> int:
         """solveFPS (fastPoissonSolver.f90:337-384): p <- L^{-1} s with zero volume-weighted
-        mean, ghosts updated."""
+        mean, ghosts updated.  Returns the status (0, or TBFP_ENOTCONVERGED when the
+        mixed path hit max_iter); iterations and residual are in last_stats()."""
         self._check_psi(p, s)
         dev = _placement([p, s])
         fn = self.lib.tbfp_solve_fps_dev if dev else self.lib.tbfp_solve_fps
-        check(fn(self.h, s.address(), p.address()), self.h)
+        return check(fn(self.h, s.address(), p.address()), self.h)
 
 
 class PoissonEqn:
@@ -221,3 +233,37 @@ def _zeros_like(a):
     import torch  # noqa: PLC0415
 
     return torch.zeros_like(a)
+
+
+class PCG:
+    """MG_MODE pressure solver (pcgCTOR, pcg.f90:62-99): FP64 conjugate gradients
+    preconditioned by FP32 red-black Gauss-Seidel multigrid V-cycles.  Defaults
+    are the reference's channel_18 settings (specs/pcg_solver)."""
+
+    def __init__(self, mesh: Grid, n_levels: int = 6, n_pre: int = 2, n_post: int = 2, tol_mg: float = 0.4,
+                 max_iter_mg: int = 100, tol_pcg: float = 1e-10, max_iter_pcg: int = 100, hd_psi: int = 1,
+                 hd_rho: int = 1, device: int = -1, stream: int | None = None):
+        self.solver = FastPoissonSolver(mesh, hd_psi=hd_psi, hd_rho=hd_rho, device=device, stream=stream)
+        self.lib, self.h, self.mesh = self.solver.lib, self.solver.h, mesh
+        self.params = TbfpMgParams(n_levels=n_levels, n_pre=n_pre, n_post=n_post, tol_mg=tol_mg,
+                                   max_iter_mg=max_iter_mg, tol_pcg=tol_pcg, max_iter_pcg=max_iter_pcg)
+        check(self.lib.tbfp_pcg_setup(self.h, C.byref(self.params)), self.h)
+
+    def close(self):
+        self.solver.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def solve_pcg(self, psi: Field, beta: Field, q: Field) -> TbfpStats:
+        """solvePCG (pcg.f90:103-140): psi (initial guess, result with ghosts)
+        solves L_beta psi = q.  Returns the statistics (iterations, ||r||/||q||);
+        an iteration cap is a soft condition (the stats say so)."""
+        dev = _placement([psi, beta, q])
+        st = TbfpStats()
+        fn = self.lib.tbfp_pcg_solve_dev if dev else self.lib.tbfp_pcg_solve
+        check(fn(self.h, psi.address(), beta.address(), q.address(), C.byref(st)), self.h)
+        return st

@@ -138,6 +138,38 @@ def test_solve_fps_random_rhs(dims, stretched):
     assert rel_linf(got, want.a) < TOL_P
 
 
+def test_solve_fps_two_layer_halo():
+    """hd_psi = 2: the same interior as hd_psi = 1, with both x and z ghost
+    layers periodic images and the first y ghost layer a copy of the wall cell
+    (updateBoundaries on one rank)."""
+    nx, ny, nz = 32, 24, 16
+    g = Grid(nx, ny, nz, 2 * np.pi, 2.0, np.pi, True, 1.5)
+    m = mesh_of(g)
+    rng = np.random.default_rng(11)
+    src = rng.standard_normal((nz, ny, nx))
+    src -= np.sum(src * m.volume()) / m.s_Vg
+    out = {}
+    for hd in (1, 2):
+        s = Field("cl", hd, nx, ny, nz)
+        s.interior()[...] = src
+        with FastPoissonSolver(g, hd_psi=hd) as fps:
+            p = _cuda(Field("cl", hd, nx, ny, nz))
+            fps.solve_fps(p, _cuda(s))
+            out[hd] = _np(p).a
+    a1, a2 = out[1], out[2]
+    assert np.array_equal(a2[2:-2, 2:-2, 2:-2], a1[1:-1, 1:-1, 1:-1])
+    # Fortran index f -> array index f + hd - 1 (hd = 2: f + 1)
+    ix = lambda f: f + 1  # noqa: E731
+    J, K = slice(ix(1), ix(ny) + 1), slice(ix(1), ix(nz) + 1)
+    for gh, src_i in ((-1, nx - 1), (0, nx), (nx + 1, 1), (nx + 2, 2)):
+        assert np.array_equal(a2[K, J, ix(gh)], a2[K, J, ix(src_i)]), gh
+    I = slice(ix(1), ix(nx) + 1)
+    for gh, src_k in ((-1, nz - 1), (0, nz), (nz + 1, 1), (nz + 2, 2)):
+        assert np.array_equal(a2[ix(gh), J, I], a2[ix(src_k), J, I]), gh
+    assert np.array_equal(a2[K, ix(0), I], a2[K, ix(1), I])
+    assert np.array_equal(a2[K, ix(ny + 1), I], a2[K, ix(ny), I])
+
+
 @pytest.mark.parametrize("stretched", [True, False])
 def test_incompatible_rhs_is_solved_with_the_defect_on_the_top_wall(stretched):
     """A source with a non-zero volume integral has no Neumann solution.  The
