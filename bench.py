@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
+    ap.add_argument("--mg", action="store_true", help="also time the MG_MODE projection (default for c5)")
     return ap.parse_args()
 
 
@@ -317,6 +318,33 @@ def main():
                  "max_div": mst.max_div, "vs_fp64": None}
         mx.close()
 
+    # MG_MODE leg (config 5: FP64 PCG + FP32 V-cycles, 6 levels, 2+2 sweeps,
+    # tolPCG 1e-10, tolMG 0.4) on the same input; psi starts from zero every step
+    mgres = None
+    if args.mg or args.config == "c5":
+        from tbfsolver_b200.solver import PCG
+        pcg = PCG(g, n_levels=6, n_pre=2, n_post=2, tol_mg=0.4, tol_pcg=1e-10, stream=stream.cuda_stream)
+        mpsi = new()
+        for _ in range(max(3, args.warmup)):
+            mpsi.a.zero_()
+            mst = pcg.projection(mpsi, inp.rho, u_in, dt, alpha, u_out=u_out)
+        stream.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nmg = max(1, min(args.steps, 5))
+        with torch.cuda.stream(stream):
+            g0.record(stream)
+            for _ in range(nmg):
+                mpsi.a.zero_()
+                mst = pcg.projection(mpsi, inp.rho, u_in, dt, alpha, u_out=u_out)
+            g1.record(stream)
+        stream.synchronize()
+        gms = g0.elapsed_time(g1) / nmg
+        mgres = {"value": g.ncells / (gms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": gms, "steps": nmg,
+                 "pcg_iterations": mst.iterations, "v_cycles": int(mst.ms_stage[0]), "rel_residual": mst.rel_residual,
+                 "max_div": mst.max_div, "fast_max_div": last.max_div,
+                 "note": "variable-coefficient PCG (MG_MODE) on the FAST leg's input; max_div of both paths"}
+        pcg.close()
+
     # end to end through the host entry point, pinned host buffers
     def pinned(f):
         h = torch.empty(f.a.shape, dtype=torch.float64, pin_memory=True)
@@ -386,6 +414,7 @@ def main():
         "solves_per_s": world * 1e3 / ms,
         "max_div": last.max_div, "cont_err": last.cont_err, "rel_residual": fp64_rel,
         "mixed": mixed,
+        "mg": mgres,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk, "unit": "GB/s",

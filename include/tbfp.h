@@ -219,6 +219,19 @@ int tbfp_pcg_setup(tbfp_handle *h, const tbfp_mg_params *p);
 int tbfp_pcg_solve(tbfp_handle *h, double *psi, const double *beta, const double *q, tbfp_stats *stats);
 int tbfp_pcg_solve_dev(tbfp_handle *h, double *psi, const double *beta, const double *q, tbfp_stats *stats);
 
+/* One MG_MODE projection (main.f90:197-212 with the MG branches):
+   q = div u* (computeSource, poissonEqn.f90:155-190), beta = dt*alpha/rho
+   (computeBeta, :311-342), tbfp_pcg_solve, addPressureGrad
+   (momentumEqn.f90:795-869) with the periodic equate, and max|div u| into
+   stats (computeContinuityError).  psi: initial guess in, pressure out.  The
+   _dev form reads u*_in and writes u*_out (may alias); the host form
+   corrects u in place. */
+int tbfp_projection_mg(tbfp_handle *h, double *ux, double *uy, double *uz, const double *rho, double dt,
+                       double alpha, double *psi, tbfp_stats *stats);
+int tbfp_projection_mg_dev(tbfp_handle *h, const double *ux_in, const double *uy_in, const double *uz_in,
+                           double *ux_out, double *uy_out, double *uz_out, const double *rho, double dt,
+                           double alpha, double *psi, tbfp_stats *stats);
+
 /* --- solveFPS without device allocation ------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
    memory (inside a CUDA graph capture, under a memory pool another runtime

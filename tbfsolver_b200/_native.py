@@ -86,6 +86,9 @@ PROTOTYPES = {
     "tbfp_pcg_setup": (C.c_int, [_H, C.POINTER(TbfpMgParams)]),
     "tbfp_pcg_solve": (C.c_int, [_H, _P, _P, _P, C.POINTER(TbfpStats)]),
     "tbfp_pcg_solve_dev": (C.c_int, [_H, _P, _P, _P, C.POINTER(TbfpStats)]),
+    "tbfp_projection_mg": (C.c_int, [_H, _P, _P, _P, _P, C.c_double, C.c_double, _P, C.POINTER(TbfpStats)]),
+    "tbfp_projection_mg_dev": (C.c_int, [_H, _P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double, _P,
+                                         C.POINTER(TbfpStats)]),
     "tbfp_solve_fps": (C.c_int, [_H, _P, _P]),
     "tbfp_solve_fps_dev": (C.c_int, [_H, _P, _P]),
     "tbfp_rhs_split": (C.c_int, [_H, _P, _P, _P, _P, _P, _P, _PP, _PP, _D, _D, _D, _P]),

@@ -52,6 +52,7 @@ struct tbfp_handle {
   // device tables
   double *d_lamx = nullptr, *d_lamz = nullptr, *d_am = nullptr, *d_ap = nullptr, *d_dyf = nullptr;
   double *d_idyf = nullptr, *d_idyc = nullptr, *d_idxf = nullptr, *d_idzf = nullptr;
+  double *d_idxc = nullptr, *d_idzc = nullptr;  // 1/dxc(1..nx+1), 1/dzc(1..nz+1) (MG_MODE correction)
   double2 *d_twx = nullptr;                     // exp(-2 pi i m/nx), the r2c/c2r factors
   double2 *d_tpx = nullptr, *d_tpz = nullptr;  // pass-ordered twiddles of lengths nx/2 and nz
   float2 *d_twx32 = nullptr, *d_tpx32 = nullptr, *d_tpz32 = nullptr;  // FP32 copies (TBFP_MIXED)
@@ -137,6 +138,11 @@ std::vector<double2> unit_twiddles(int n) {
 std::vector<double2> pass_twiddles(int n) {
   std::vector<double2> t(n);
   fft_pass_twiddles(n, t.data());
+  return t;
+}
+std::vector<double> inv_of(const double *a, int n) {
+  std::vector<double> t(n);
+  for (int i = 0; i < n; ++i) t[i] = 1.0 / a[i];
   return t;
 }
 std::vector<float2> to_f32(const std::vector<double2> &v) {
@@ -643,7 +649,8 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
       (rc = upload(h, &h->d_tpz, pass_twiddles(nz))) || (rc = upload(h, &h->d_twx32, to_f32(unit_twiddles(nx)))) ||
       (rc = upload(h, &h->d_tpx32, to_f32(pass_twiddles(nx / 2)))) ||
       (rc = upload(h, &h->d_tpz32, to_f32(pass_twiddles(nz)))) ||
-      (rc = upload(h, &h->d_acc, std::vector<double>(64, 0.0))))
+      (rc = upload(h, &h->d_acc, std::vector<double>(64, 0.0))) || (rc = upload(h, &h->d_idxc, inv_of(d->dxc, nx + 1))) ||
+      (rc = upload(h, &h->d_idzc, inv_of(d->dzc, nz + 1))))
     return fail(rc);
   if ((rc = dev_alloc(h, &h->d_spec, (size_t)h->nkx * h->R)) || (rc = dev_alloc(h, &h->d_irho, h->n_rho)) ||
       (rc = dev_alloc(h, &h->d_s, h->n_psi)) ||
@@ -939,6 +946,70 @@ int tbfp_pcg_solve_dev(tbfp_handle *h, double *psi, const double *beta, const do
   h->last.ms_stage[0] = cycles;  // V-cycles in total (informational)
   if (stats) *stats = h->last;
   return src;
+}
+
+int tbfp_projection_mg_dev(tbfp_handle *h, const double *ux_in, const double *uy_in, const double *uz_in,
+                           double *ux_out, double *uy_out, double *uz_out, const double *rho, double dt, double alpha,
+                           double *psi, tbfp_stats *stats) {
+  int rc = check_ptrs(h, {ux_in, uy_in, uz_in, ux_out, uy_out, uz_out, rho, psi});
+  if (rc) return rc;
+  if (!h->mg) return set_err(h, TBFP_EINVAL, "tbfp_projection_mg: call tbfp_pcg_setup first");
+  if (!(dt > 0.0) || !(alpha > 0.0)) return set_err(h, TBFP_EINVAL, "tbfp_projection_mg: dt and alpha must be positive");
+  cudaSetDevice(h->device);
+  cudaStream_t s = h->stream;
+  const double dta = dt * alpha;
+  TBFP_CK(h, cudaEventRecord(h->ev0, s));
+  // q = div u* into the s scratch, beta = dt alpha / rho into the 1/rho scratch
+  launch_mg_source_beta(ux_in, uy_in, uz_in, h->Lux, h->Luy, h->Luz, rho, h->Lrho, h->g, dta, h->d_s, h->Lpsi,
+                        h->d_irho, s);
+  int iters = 0, cycles = 0;
+  double rel = -1.0;
+  std::string err;
+  const int src = h->mg->solve(psi, h->Lpsi, h->hd_psi, h->d_irho, h->Lrho, h->d_s, h->Lpsi, s, &iters, &rel, &cycles,
+                               &err);
+  if (src < 0) return set_err(h, src, err);
+  launch_add_pressure_grad(ux_in, uy_in, uz_in, ux_out, uy_out, uz_out, h->Lux, h->Luy, h->Luz, psi, h->Lpsi, rho,
+                           h->Lrho, h->g, h->d_idxc, h->d_idzc, dta, s);
+  TBFP_CK(h, cudaMemsetAsync(h->d_maxdiv, 0, sizeof(unsigned long long), s));
+  launch_div(ux_out, uy_out, uz_out, h->Lux, h->Luy, h->Luz, h->g, h->d_maxdiv, s);
+  TBFP_CK(h, cudaEventRecord(h->ev1, s));
+  unsigned long long bits = 0;
+  TBFP_CK(h, cudaMemcpyAsync(&bits, h->d_maxdiv, sizeof(bits), cudaMemcpyDeviceToHost, s));
+  TBFP_CK(h, cudaStreamSynchronize(s));
+  double md;
+  std::memcpy(&md, &bits, sizeof(md));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->last = tbfp_stats{};
+  h->last.iterations = iters;
+  h->last.rel_residual = rel;
+  h->last.max_div = md;
+  h->last.cont_err = md * dt;
+  h->last.ms_device = ms;
+  h->last.ms_stage[0] = cycles;
+  if (stats) *stats = h->last;
+  const int frc = finish(h, "tbfp_projection_mg");
+  return frc ? frc : src;
+}
+
+int tbfp_projection_mg(tbfp_handle *h, double *ux, double *uy, double *uz, const double *rho, double dt, double alpha,
+                       double *psi, tbfp_stats *stats) {
+  int rc = check_ptrs(h, {ux, uy, uz, rho, psi});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  if ((rc = ensure_host_bufs(h, false))) return rc;
+  if ((rc = h2d(h, h->h_ux, ux, h->n_ux)) || (rc = h2d(h, h->h_uy, uy, h->n_uy)) ||
+      (rc = h2d(h, h->h_uz, uz, h->n_uz)) || (rc = h2d(h, h->h_rho, rho, h->n_rho)) ||
+      (rc = h2d(h, h->h_psi, psi, h->n_psi)))
+    return rc;
+  const int prc = tbfp_projection_mg_dev(h, h->h_ux, h->h_uy, h->h_uz, h->h_ux, h->h_uy, h->h_uz, h->h_rho, dt, alpha,
+                                         h->h_psi, stats);
+  if (prc < 0) return prc;
+  if ((rc = d2h(h, ux, h->h_ux, h->n_ux)) || (rc = d2h(h, uy, h->h_uy, h->n_uy)) ||
+      (rc = d2h(h, uz, h->h_uz, h->n_uz)) || (rc = d2h(h, psi, h->h_psi, h->n_psi)))
+    return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return prc;
 }
 
 int tbfp_pcg_solve(tbfp_handle *h, double *psi, const double *beta, const double *q, tbfp_stats *stats) {

@@ -243,3 +243,90 @@ cudaError_t prepare_kernels() {
 }
 
 }  // namespace tbfp
+
+namespace tbfp {
+
+// ---------------------------------------------------------------------------
+// MG_MODE source and coefficient: q = div u* (computeSource MG,
+// poissonEqn.f90:155-190, metrics per index) and beta = dt*alpha/rho
+// (computeBeta, :311-342) on the interior; beta is written with rho's layout.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_mg_source_beta(const double *__restrict__ ux, const double *__restrict__ uy,
+                                                       const double *__restrict__ uz, Lay Lux, Lay Luy, Lay Luz,
+                                                       const double *__restrict__ rho, Lay Lrho, GridK g, double dta,
+                                                       double *__restrict__ q, Lay Lq, double *__restrict__ beta) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  if (i > g.nx) return;
+  double d = (ux[at(Lux, i, j, k)] - ux[at(Lux, i - 1, j, k)]) * g.idxf[i - 1];
+  d = d + (uy[at(Luy, i, j, k)] - uy[at(Luy, i, j - 1, k)]) * g.idyf[j - 1];
+  d = d + (uz[at(Luz, i, j, k)] - uz[at(Luz, i, j, k - 1)]) * g.idzf[k - 1];
+  q[at(Lq, i, j, k)] = d;
+  const long r = at(Lrho, i, j, k);
+  beta[r] = dta / rho[r];
+}
+
+void launch_mg_source_beta(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz,
+                           const double *rho, Lay Lrho, const GridK &g, double dta, double *q, Lay Lq, double *beta,
+                           cudaStream_t st) {
+  dim3 grid((g.nx + 127) / 128, g.ny, g.nz);
+  k_mg_source_beta<<<grid, 128, 0, st>>>(ux, uy, uz, Lux, Luy, Luz, rho, Lrho, g, dta, q, Lq, beta);
+}
+
+// ---------------------------------------------------------------------------
+// makeVelocityDivFree MG = addPressureGrad (momentumEqn.f90:795-869, :980-993):
+//   u_d -= dt*alpha * (1/rho)_face * (p(+) - p) / dc_d
+// with (1/rho)_face = (1/rho(+) + 1/rho)/2, on the setEqnBounds ranges (wall
+// faces of uy copied through), then the periodic equate ux(0)=ux(nx),
+// uz(.,.,0)=uz(.,.,nz) (vfield.f90:124-189).  p and rho are read with their
+// ghosts (periodic images, wall copies).  Out of place or in place: a thread
+// reads and writes only its own cell's faces.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_add_pressure_grad(const double *__restrict__ uxi, const double *__restrict__ uyi,
+                                                          const double *__restrict__ uzi, double *__restrict__ uxo,
+                                                          double *__restrict__ uyo, double *__restrict__ uzo,
+                                                          Lay Lux, Lay Luy, Lay Luz, const double *__restrict__ p,
+                                                          Lay Lp, const double *__restrict__ rho, Lay Lrho, GridK g,
+                                                          const double *__restrict__ idxc, const double *__restrict__ idzc,
+                                                          double dta) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  if (i > g.nx) return;
+  const long pc = at(Lp, i, j, k), rc = at(Lrho, i, j, k);
+  const double irc = 1.0 / rho[rc];
+  {  // x face i+1/2: dxc(i+1)
+    const double ir = 0.5 * (1.0 / rho[rc + 1] + irc);
+    const long o = at(Lux, i, j, k);
+    const double v = uxi[o] - dta * ir * (p[pc + 1] - p[pc]) * idxc[i];
+    uxo[o] = v;
+    if (i == g.nx) uxo[at(Lux, 0, j, k)] = v;
+  }
+  {  // y face j+1/2: dyc(j+1); the wall faces j = 0 and j = ny keep their values
+    const long o = at(Luy, i, j, k);
+    if (j < g.ny) {
+      const double ir = 0.5 * (1.0 / rho[rc + Lrho.sj] + irc);
+      uyo[o] = uyi[o] - dta * ir * (p[pc + Lp.sj] - p[pc]) * g.idyc[j];
+    } else {
+      uyo[o] = uyi[o];
+    }
+    if (j == 1) uyo[at(Luy, i, 0, k)] = uyi[at(Luy, i, 0, k)];
+  }
+  {  // z face k+1/2: dzc(k+1)
+    const double ir = 0.5 * (1.0 / rho[rc + Lrho.sk] + irc);
+    const long o = at(Luz, i, j, k);
+    const double v = uzi[o] - dta * ir * (p[pc + Lp.sk] - p[pc]) * idzc[k];
+    uzo[o] = v;
+    if (k == g.nz) uzo[at(Luz, i, j, 0)] = v;
+  }
+}
+
+void launch_add_pressure_grad(const double *uxi, const double *uyi, const double *uzi, double *uxo, double *uyo,
+                              double *uzo, Lay Lux, Lay Luy, Lay Luz, const double *p, Lay Lp, const double *rho,
+                              Lay Lrho, const GridK &g, const double *idxc, const double *idzc, double dta,
+                              cudaStream_t st) {
+  dim3 grid((g.nx + 127) / 128, g.ny, g.nz);
+  k_add_pressure_grad<<<grid, 128, 0, st>>>(uxi, uyi, uzi, uxo, uyo, uzo, Lux, Luy, Luz, p, Lp, rho, Lrho, g, idxc,
+                                            idzc, dta);
+}
+
+}  // namespace tbfp

@@ -183,6 +183,16 @@ void launch_correct_inplace(const CorrArgs &ca, bool has_st, const GridK &g, cud
 void launch_div(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz, const GridK &g,
                 unsigned long long *maxdiv, cudaStream_t st);
 
+// MG_MODE source/beta (computeSource MG, computeBeta) and addPressureGrad.
+// idxc, idzc: 1/dxc(i), 1/dzc(k) for Fortran i = 1..nx+1 (0-based tables).
+void launch_mg_source_beta(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz,
+                           const double *rho, Lay Lrho, const GridK &g, double dta, double *q, Lay Lq, double *beta,
+                           cudaStream_t st);
+void launch_add_pressure_grad(const double *uxi, const double *uyi, const double *uzi, double *uxo, double *uyo,
+                              double *uzo, Lay Lux, Lay Luy, Lay Luz, const double *p, Lay Lp, const double *rho,
+                              Lay Lrho, const GridK &g, const double *idxc, const double *idzc, double dta,
+                              cudaStream_t st);
+
 // per-file parts of prepare_kernels()
 cudaError_t prepare_xfft_kernels();
 cudaError_t prepare_yz_kernels();

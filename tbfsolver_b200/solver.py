@@ -267,3 +267,23 @@ class PCG:
         fn = self.lib.tbfp_pcg_solve_dev if dev else self.lib.tbfp_pcg_solve
         check(fn(self.h, psi.address(), beta.address(), q.address(), C.byref(st)), self.h)
         return st
+
+    def projection(self, psi: Field, rho: Field, u: VField, dt: float, alpha: float,
+                   u_out: VField | None = None) -> TbfpStats:
+        """One MG_MODE projection (computeSource MG, computeBeta, solvePCG,
+        addPressureGrad, computeContinuityError): psi is the initial guess and
+        the pressure; u is corrected in place unless u_out is given (device
+        fields only)."""
+        dev = _placement([psi, rho, *u.components()])
+        st = TbfpStats()
+        if dev:
+            uo = u_out or u
+            check(self.lib.tbfp_projection_mg_dev(self.h, u.ux.address(), u.uy.address(), u.uz.address(),
+                                                  uo.ux.address(), uo.uy.address(), uo.uz.address(), rho.address(),
+                                                  dt, alpha, psi.address(), C.byref(st)), self.h)
+        else:
+            if u_out is not None:
+                raise TbfpError(TBFP_EINVAL, "u_out is only supported for device fields")
+            check(self.lib.tbfp_projection_mg(self.h, u.ux.address(), u.uy.address(), u.uz.address(),
+                                              rho.address(), dt, alpha, psi.address(), C.byref(st)), self.h)
+        return st

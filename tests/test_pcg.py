@@ -7,7 +7,7 @@ oracle's FP64 operator applied to the GPU result confirms that residual
 (1e-9, L-infinity relative to q); pressures agree with the oracle's after the
 gauge (the mean) is removed to 1e-6 relative, the level the 1e-10 residual
 allows for this operator's conditioning; the iteration count stays within a
-few of the oracle's (the preconditioner runs in FP32 here, FP64 there).
+few (or 30%) of the oracle's (the preconditioner runs in FP32 here, FP64 there).
 """
 import numpy as np
 import pytest
@@ -16,7 +16,7 @@ import torch
 from oracle import tbfp_oracle as O
 from tbfsolver_b200 import synth
 from tbfsolver_b200._native import TBFP_EINVAL, TbfpError
-from tbfsolver_b200.fields import Field
+from tbfsolver_b200.fields import Field, VField
 from tbfsolver_b200.grid import Grid
 from tbfsolver_b200.solver import PCG, FastPoissonSolver
 from tests._helpers import mesh_of, rel_linf, to_oracle
@@ -82,7 +82,8 @@ def test_pcg_on_a_stretched_six_level_grid():
     p_ref = O.FField("cl", 1, m.nx, m.ny, m.nz)
     it_ref, _ = mg.solve_pcg(p_ref, beta, q)
     st, psi = _gpu_pcg(g, q, beta, 6)
-    assert st.rel_residual <= 1e-10 and st.iterations <= it_ref + 10, (st.iterations, it_ref, st.rel_residual)
+    # FP32 smoothing in the preconditioner costs iterations against the FP64 oracle
+    assert st.rel_residual <= 1e-10 and st.iterations <= 1.3 * it_ref + 2, (st.iterations, it_ref, st.rel_residual)
     po = O.FField("cl", 1, m.nx, m.ny, m.nz, psi)
     assert rel_linf(O.apply_L(mg.levels[0], po, beta), q) < 1e-9
     a, b = po.interior(), p_ref.interior()
@@ -110,3 +111,36 @@ def test_pcg_errors():
     with pytest.raises(TbfpError) as e:
         PCG(g, n_levels=7)  # 16 is not divisible by 2^6
     assert e.value.code == TBFP_EINVAL
+
+
+def test_mg_projection_matches_the_oracle():
+    """One MG_MODE projection (computeSource MG, computeBeta, solvePCG,
+    addPressureGrad, computeContinuityError) against the oracle's chain on the
+    same input: pressures (gauge removed) and velocities agree to the PCG
+    tolerance, and max|div u| drops to the tolerance level."""
+    spec = synth.small_spec(32, 32, 16, nbubbles=2, radius=0.3, rhog=0.01)
+    inp = synth.make_inputs(spec, seed=4)
+    g = inp.grid
+    m = mesh_of(g)
+    ux, uy, uz, rho = [to_oracle(f, g) for f in (inp.u.ux, inp.u.uy, inp.u.uz, inp.rho)]
+    div0 = O.compute_continuity_error(m, ux, uy, uz)
+    q = O.compute_source_mg(m, ux, uy, uz)
+    beta = O.compute_beta(m, rho, inp.dt, inp.alpha)
+    mg = O.MGOracle(m, n_levels=3, n_pre=2, n_post=2, tol_mg=0.4, tol_pcg=1e-10)
+    p_ref = O.FField("cl", 1, m.nx, m.ny, m.nz)
+    mg.solve_pcg(p_ref, beta, q)
+    u_ref = [f.copy() for f in (ux, uy, uz)]
+    O.add_pressure_grad(m, *u_ref, p_ref, rho, inp.dt, inp.alpha)
+
+    dev = lambda f: Field.like(f, torch.from_numpy(np.ascontiguousarray(f.a)).to("cuda"))  # noqa: E731
+    u = VField(*[dev(f) for f in inp.u.components()])
+    psi = dev(Field("cl", 1, g.nx, g.ny, g.nz))
+    with PCG(g, n_levels=3) as pcg:
+        st = pcg.projection(psi, dev(inp.rho), u, inp.dt, inp.alpha)
+    assert st.rel_residual <= 1e-10 and st.max_div < 1e-8 * div0
+    a = psi.a.cpu().numpy()[1:-1, 1:-1, 1:-1]
+    b = p_ref.interior()
+    assert rel_linf(a - a.mean(), b - b.mean()) < 1e-6
+    for got, want in zip(u.components(), u_ref):
+        gi = Field.like(got, got.a.cpu().numpy()).interior()
+        assert rel_linf(gi, want.interior()) < 1e-9
