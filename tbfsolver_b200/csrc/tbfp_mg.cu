@@ -81,39 +81,43 @@ __device__ __forceinline__ void block_sum2(double a, double b, double *out_a, do
 // ---------------------------------------------------------------------------
 // One colour of iterateGS (rbgs.f90:215-250): cells with (i+j+k) mod 2 == colour
 // (1-based indices, red = 0) take p = (-q + sum a_nb p_nb) / sum a_nb.
+// With sum != nullptr (the last black sweep of a smoothing call) each thread
+// also adds its cell and the other cell of its x pair (2m, 2m+1: one of each
+// colour, nx even on every smoothed level) to *sum: the interior sum of p.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kMgThreads) k_rbgs_colour(MgLev L, float *__restrict__ p,
                                                            const float *__restrict__ q,
-                                                           const float *__restrict__ beta, int colour) {
+                                                           const float *__restrict__ beta, int colour,
+                                                           double *__restrict__ sum) {
   const int nxh = (L.nx + 1) / 2;
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long total = (long)nxh * L.ny * L.nz;
-  if (t >= total) return;
-  const int ih = (int)(t % nxh);
-  const long r = t / nxh;
-  const int j = (int)(r % L.ny), k = (int)(r / L.ny);
-  // colour of 1-based (i+1, j+1, k+1): (i + j + k + 3) mod 2, so the row's first
-  // 0-based index of this colour is (colour + j + k + 1) mod 2
-  const int ii = 2 * ih + ((colour + j + k + 1) & 1);
-  if (ii >= L.nx) return;
-  const int nx = L.nx, ny = L.ny, nz = L.nz;
-  auto at3 = [&](int a, int b, int c) { return ((long)c * ny + b) * nx + a; };
-  const Coef<float> c = coef<float>(L, beta, ii, j, k);
-  const float den = c.aR + c.aL + c.aT + c.aB + c.aF + c.aK;
-  const float pR = p[at3(wrap(ii + 1, nx), j, k)], pL = p[at3(wrap(ii - 1, nx), j, k)];
-  const float pT = p[at3(ii, clampi(j + 1, ny), k)], pB = p[at3(ii, clampi(j - 1, ny), k)];
-  const float pF = p[at3(ii, j, wrap(k + 1, nz))], pK = p[at3(ii, j, wrap(k - 1, nz))];
-  const float v = (-q[at3(ii, j, k)] + (c.aR * pR + c.aL * pL) + (c.aT * pT + c.aB * pB) + (c.aF * pF + c.aK * pK)) / den;
-  p[at3(ii, j, k)] = v;
+  double acc = 0.0;
+  if (t < total) {
+    const int ih = (int)(t % nxh);
+    const long r = t / nxh;
+    const int j = (int)(r % L.ny), k = (int)(r / L.ny);
+    // colour of 1-based (i+1, j+1, k+1): (i + j + k + 3) mod 2, so the row's first
+    // 0-based index of this colour is (colour + j + k + 1) mod 2
+    const int ii = 2 * ih + ((colour + j + k + 1) & 1);
+    if (ii < L.nx) {
+      const int nx = L.nx, ny = L.ny, nz = L.nz;
+      auto at3 = [&](int a, int b, int c) { return ((long)c * ny + b) * nx + a; };
+      const Coef<float> c = coef<float>(L, beta, ii, j, k);
+      const float den = c.aR + c.aL + c.aT + c.aB + c.aF + c.aK;
+      const float pR = p[at3(wrap(ii + 1, nx), j, k)], pL = p[at3(wrap(ii - 1, nx), j, k)];
+      const float pT = p[at3(ii, clampi(j + 1, ny), k)], pB = p[at3(ii, clampi(j - 1, ny), k)];
+      const float pF = p[at3(ii, j, wrap(k + 1, nz))], pK = p[at3(ii, j, wrap(k - 1, nz))];
+      const float v =
+          (-q[at3(ii, j, k)] + (c.aR * pR + c.aL * pL) + (c.aT * pT + c.aB * pB) + (c.aF * pF + c.aK * pK)) / den;
+      p[at3(ii, j, k)] = v;
+      if (sum) acc = (double)v + (double)((ii & 1) ? pL : pR);
+    }
+  }
+  if (sum) block_sum2(acc, 0.0, sum, nullptr);
 }
 
-// sum of p over the interior (correctFullNeumann's average, rbgs.f90:403-446)
-__global__ void __launch_bounds__(kMgThreads) k_sum(const float *__restrict__ p, long n, double *__restrict__ out) {
-  double s = 0.0;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) s += p[t];
-  block_sum2(s, 0.0, out, nullptr);
-}
-
+// p -= sum/n (correctFullNeumann, rbgs.f90:403-446)
 __global__ void __launch_bounds__(kMgThreads) k_sub_mean(float *__restrict__ p, long n,
                                                         const double *__restrict__ sum) {
   const float avg = (float)(*sum / (double)n);
@@ -555,6 +559,8 @@ struct MgSolver::Impl {
   int *fail = nullptr;
   std::vector<void *> allocs;
   size_t bytes = 0;
+  cudaGraphExec_t vgraph = nullptr;  // one V-cycle from the finest level
+  bool graph_failed = false;
 
   template <typename T>
   cudaError_t alloc(T **p, size_t count) {
@@ -567,6 +573,7 @@ struct MgSolver::Impl {
     return cudaSuccess;
   }
   ~Impl() {
+    if (vgraph) cudaGraphExecDestroy(vgraph);
     for (void *p : allocs) cudaFree(p);
   }
 };
@@ -745,17 +752,23 @@ struct Run {
   MgSolver::Impl &m;
   cudaStream_t st;
 
+  // iterateGS (rbgs.f90:186-272).  The reference removes the mean
+  // (correctFullNeumann) after every red+black iteration.  A sweep commutes
+  // with adding a constant to p (the update is an average of neighbours, q
+  // fixed), so removing the mean once after the last iteration gives the same
+  // p; the sum comes out of the last black sweep.
   void rbgs(int l, int n_iter, bool reset) {
     auto &L = m.lv[l];
     if (reset) k_fill<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, 0.0f);
+    if (n_iter == 0) return;
     const long half = (long)((L.nx + 1) / 2) * L.ny * L.nz;
+    cudaMemsetAsync(m.sc + 8, 0, sizeof(double), st);
     for (int it = 0; it < n_iter; ++it) {
-      k_rbgs_colour<<<nblk(half), kMgThreads, 0, st>>>(L.L, L.p, L.q, L.beta, 0);
-      k_rbgs_colour<<<nblk(half), kMgThreads, 0, st>>>(L.L, L.p, L.q, L.beta, 1);
-      cudaMemsetAsync(m.sc + 8, 0, sizeof(double), st);
-      k_sum<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, m.sc + 8);
-      k_sub_mean<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, m.sc + 8);
+      k_rbgs_colour<<<nblk(half), kMgThreads, 0, st>>>(L.L, L.p, L.q, L.beta, 0, nullptr);
+      k_rbgs_colour<<<nblk(half), kMgThreads, 0, st>>>(L.L, L.p, L.q, L.beta, 1,
+                                                        it == n_iter - 1 ? m.sc + 8 : nullptr);
     }
+    k_sub_mean<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, m.sc + 8);
   }
 
   void vcycle(int l) {
@@ -785,7 +798,9 @@ struct Run {
     return std::sqrt(v[0]) / (std::sqrt(v[1]) + 1e-300);
   }
 
-  // solveMG (multiGrid.f90:165-182): p starts at 0, V-cycles while res > tol_mg
+  // solveMG (multiGrid.f90:165-182): p starts at 0, V-cycles while res > tol_mg.
+  // Each V-cycle is one launch of a CUDA graph captured once per hierarchy
+  // (its buffers never move); without a graph the kernels are launched one by one.
   int solve_mg() {
     auto &L = m.lv[0];
     k_fill<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, 0.0f);
@@ -793,10 +808,32 @@ struct Run {
     int it = 0;
     while (it < m.prm.max_iter_mg && res > m.prm.tol_mg) {
       ++it;
-      vcycle(0);
+      if (m.vgraph) cudaGraphLaunch(m.vgraph, st);
+      else vcycle(0);
       res = fine_residual();
     }
     return it;
+  }
+
+  void capture() {
+    if (m.vgraph || m.graph_failed) return;
+    cudaStream_t cs = nullptr;
+    cudaGraph_t gr = nullptr;
+    bool ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess;
+    if (ok) ok = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      Run r{m, cs};
+      r.vcycle(0);
+      ok = cudaStreamEndCapture(cs, &gr) == cudaSuccess && gr != nullptr;
+    }
+    if (ok) ok = cudaGraphInstantiate(&m.vgraph, gr, 0) == cudaSuccess;
+    if (gr) cudaGraphDestroy(gr);
+    if (cs) cudaStreamDestroy(cs);
+    if (!ok) {
+      m.vgraph = nullptr;
+      m.graph_failed = true;
+      cudaGetLastError();  // clear a capture error; the eager path is used instead
+    }
   }
 };
 }  // namespace
@@ -817,6 +854,7 @@ int MgSolver::solve(double *psi, Lay Lp, int hd_psi, const double *beta, Lay Lb,
   F.beta = beta;
   F.Lb = Lb;
   Run run{m, st};
+  run.capture();
   *mg_cycles = 0;
   // beta on every level (restrictField, field.f90:1442-1470)
   k_beta32<<<nblk_grid(m.n), kMgThreads, 0, st>>>(F, m.lv[0].beta);
