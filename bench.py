@@ -217,11 +217,96 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_ensemble(args, world, rank, local):
+    """Config 4: 64 channels of the minimal box with seeded sizes, one
+    tbfp_ensemble call per step (all members forked over 8 streams, replayed as
+    one CUDA graph), against the same 64 projections made one after another
+    through the single-channel entry point."""
+    import torch
+    import torch.distributed as dist
+
+    from tbfsolver_b200 import synth
+    from tbfsolver_b200.fields import Field, VField
+    from tbfsolver_b200.solver import Ensemble, PoissonEqn
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    specs = synth.ensemble_specs(64, seed=args.seed + rank)
+    inps = [synth.make_inputs(sp, seed=args.seed + 1000 * rank + c, device="cuda") for c, sp in enumerate(specs)]
+    ncells = sum(sp.ncells for sp in specs)
+    dt, alpha, rho0 = inps[0].dt, inps[0].alpha, min(specs[0].rhol, specs[0].rhog)
+    seq = [PoissonEqn(i.grid, sp.rhol, sp.rhog) for i, sp in zip(inps, specs)]
+    members = []
+    for inp, eqn in zip(inps, seq):  # calls 1 and 2 of the chain build psi^n, psi^{n-1}
+        pn, pnm1 = inp.psi_n, inp.psi_nm1
+        uo = VField(*[Field.like(f, f.a.clone()) for f in inp.u.components()])
+        for _ in range(2):
+            psi = Field.like(pn, torch.zeros_like(pn.a))
+            eqn.projection(psi, pn, pnm1, inp.rho, inp.u, dt, alpha, u_out=uo, want_stats=False)
+            pnm1, pn = pn, psi
+        members.append((Field.like(pn, torch.zeros_like(pn.a)), pn, pnm1, inp.rho, inp.u, uo))
+    torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    ens = Ensemble([i.grid for i in inps], nstreams=8)
+    clk = ClockSampler(local)
+    clk.start()
+    ms = timed(lambda: ens.projection(members, dt, alpha, rho0, want_stats=False), args.steps)
+    clocks = clk.stop()
+    st = ens.projection(members, dt, alpha, rho0)
+
+    def sequential():
+        for (psi, pn, pnm1, rho, u, uo), eqn in zip(members, seq):
+            eqn.projection(psi, pn, pnm1, rho, u, dt, alpha, u_out=uo, want_stats=False)
+
+    ms_seq = timed(sequential, max(1, args.steps // 4))
+    ens.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": world * ncells / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"c4-ensemble-64ch-{ncells}cells", "channels": 64, "cells": ncells,
+                   "precision": "fp64", "parallelism": f"64 independent channels per GPU x{world}",
+                   "l2": "inputs larger than L2 (6 GB per step)", "timing": "events around synchronous calls"},
+        "max_div": max(x.max_div for x in st),
+        "sequential": {"value": world * ncells / (ms_seq * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms_seq,
+                       "note": "the same 64 projections one after another, single-channel entry point"},
+        "e2e": None, "gpu_launches": None, "clocks": clocks, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.config == "c4":
+        run_ensemble(args, world, rank, local)
         return
 
     import torch

@@ -232,6 +232,28 @@ int tbfp_projection_mg_dev(tbfp_handle *h, const double *ux_in, const double *uy
                            double *ux_out, double *uy_out, double *uz_out, const double *rho, double dt,
                            double alpha, double *psi, tbfp_stats *stats);
 
+/* --- ensemble: many independent channels per GPU ----------------------- */
+/* No counterpart in the reference, which runs one channel per job.  Each
+   member is a channel with its own descriptor (sizes may differ); its arrays
+   are device arrays laid out as for tbfp_projection_dev.  Members run on a
+   pool of nstreams streams; when every member is TBFP_FP64 the whole step is
+   captured once as a CUDA graph and replayed while the arrays and scalars
+   stay the same.  Calls are synchronous.  Surface tension is not supported in
+   an ensemble. */
+typedef struct tbfp_ensemble tbfp_ensemble;
+typedef struct {
+  const double *ux_in, *uy_in, *uz_in; /* u*: read */
+  double *ux_out, *uy_out, *uz_out;    /* projected u: written (may alias u*_in) */
+  const double *rho, *psi_n, *psi_nm1;
+  double *psi;                         /* pressure: written with ghosts */
+} tbfp_member_io;
+int tbfp_ensemble_create(int n, const tbfp_desc *descs, int nstreams, tbfp_ensemble **out);
+int tbfp_ensemble_destroy(tbfp_ensemble *e);
+int tbfp_ensemble_size(const tbfp_ensemble *e);
+/* One projection of every member; stats: NULL or n entries (max_div per member). */
+int tbfp_ensemble_projection_dev(tbfp_ensemble *e, const tbfp_member_io *io, double dt, double alpha,
+                                 double rho0, tbfp_stats *stats);
+
 /* --- solveFPS without device allocation ------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
    memory (inside a CUDA graph capture, under a memory pool another runtime

@@ -57,6 +57,11 @@ class TbfpMgParams(C.Structure):
                 ("max_iter_mg", C.c_int), ("tol_pcg", C.c_double), ("max_iter_pcg", C.c_int)]
 
 
+class TbfpMemberIO(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("ux_in", "uy_in", "uz_in", "ux_out", "uy_out", "uz_out", "rho", "psi_n",
+                                           "psi_nm1", "psi")]
+
+
 class TbfpStats(C.Structure):
     _fields_ = [
         ("iterations", C.c_int),
@@ -83,6 +88,11 @@ PROTOTYPES = {
     "tbfp_destroy": (C.c_int, [_H]),
     "tbfp_device_bytes": (C.c_size_t, [_H]),
     "tbfp_get_stats": (C.c_int, [_H, C.POINTER(TbfpStats)]),
+    "tbfp_ensemble_create": (C.c_int, [C.c_int, C.POINTER(TbfpDesc), C.c_int, C.POINTER(C.c_void_p)]),
+    "tbfp_ensemble_destroy": (C.c_int, [_H]),
+    "tbfp_ensemble_size": (C.c_int, [_H]),
+    "tbfp_ensemble_projection_dev": (C.c_int, [_H, C.POINTER(TbfpMemberIO), C.c_double, C.c_double, C.c_double,
+                                               C.POINTER(TbfpStats)]),
     "tbfp_pcg_setup": (C.c_int, [_H, C.POINTER(TbfpMgParams)]),
     "tbfp_pcg_solve": (C.c_int, [_H, _P, _P, _P, C.POINTER(TbfpStats)]),
     "tbfp_pcg_solve_dev": (C.c_int, [_H, _P, _P, _P, C.POINTER(TbfpStats)]),

@@ -1029,4 +1029,175 @@ int tbfp_pcg_solve(tbfp_handle *h, double *psi, const double *beta, const double
   return src;
 }
 
+// ---------------------------------------------------------------------------
+// Ensemble: many independent channels per GPU in one call.  Members run on a
+// pool of streams; with every member in plain FP64 the whole step (all
+// members' launches, forked over the pool) is captured once as a CUDA graph
+// and replayed while the arrays and scalars stay the same.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct tbfp_ensemble {
+  std::vector<tbfp_handle *> h;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> ev;  // [0] fork, [1..] joins
+  int device = 0;
+  bool graphable = true;
+  cudaGraphExec_t graph = nullptr;
+  std::vector<tbfp_member_io> key;
+  double kdt = 0.0, kalpha = 0.0, krho0 = 0.0;
+};
+
+namespace {
+bool same_io(const tbfp_member_io &a, const tbfp_member_io &b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
+
+int ensemble_launch_all(tbfp_ensemble *e, const tbfp_member_io *io, double dt, double alpha, double rho0) {
+  const int ns = (int)e->streams.size();
+  for (int s = 1; s < ns; ++s) cudaStreamWaitEvent(e->streams[s], e->ev[0], 0);
+  for (size_t i = 0; i < e->h.size(); ++i) {
+    const tbfp_member_io &m = io[i];
+    const int rc = device_projection(e->h[i], m.ux_in, m.uy_in, m.uz_in, m.ux_out, m.uy_out, m.uz_out, m.rho,
+                                     m.psi_n, m.psi_nm1, nullptr, nullptr, dt, alpha, rho0, m.psi, nullptr);
+    if (rc < 0) {
+      set_global_error(e->h[i]->err);
+      return rc;
+    }
+  }
+  for (int s = 1; s < ns; ++s) {
+    cudaEventRecord(e->ev[s], e->streams[s]);
+    cudaStreamWaitEvent(e->streams[0], e->ev[s], 0);
+  }
+  return TBFP_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int tbfp_ensemble_create(int n, const tbfp_desc *descs, int nstreams, tbfp_ensemble **out) {
+  set_global_error("");
+  if (!descs || !out) return TBFP_ENULL;
+  *out = nullptr;
+  if (n < 1 || nstreams < 1) return set_err(nullptr, TBFP_EINVAL, "tbfp_ensemble_create: need n >= 1 and nstreams >= 1");
+  tbfp_ensemble *e = new tbfp_ensemble();
+  e->device = descs[0].device;
+  if (e->device < 0) cudaGetDevice(&e->device);
+  cudaSetDevice(e->device);
+  const int ns = std::min(nstreams, n);
+  e->streams.resize(ns, nullptr);
+  e->ev.resize(ns, nullptr);
+  auto fail = [&](int rc) {
+    tbfp_ensemble_destroy(e);
+    return rc;
+  };
+  for (int s = 0; s < ns; ++s) {
+    if (cudaStreamCreateWithFlags(&e->streams[s], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev[s], cudaEventDisableTiming) != cudaSuccess)
+      return fail(set_err(nullptr, TBFP_ECUDA, "tbfp_ensemble_create: stream or event creation failed"));
+  }
+  for (int i = 0; i < n; ++i) {
+    tbfp_desc d = descs[i];
+    if (d.device >= 0 && d.device != e->device)
+      return fail(set_err(nullptr, TBFP_EINVAL, "tbfp_ensemble_create: members must share one device"));
+    d.device = e->device;
+    d.stream = e->streams[i % ns];
+    d.flags = (d.flags | TBFP_FLAG_ASYNC) & ~TBFP_FLAG_TIMING;
+    if (d.precision != TBFP_FP64 || (d.flags & TBFP_FLAG_RESIDUAL)) e->graphable = false;
+    tbfp_handle *h = nullptr;
+    const int rc = tbfp_create(&d, &h);
+    if (rc < 0) {
+      const std::string m = "tbfp_ensemble_create: member " + std::to_string(i) + ": " + g_create_error;
+      tbfp_ensemble_destroy(e);
+      return set_err(nullptr, rc, m);
+    }
+    e->h.push_back(h);
+  }
+  *out = e;
+  return TBFP_OK;
+}
+
+int tbfp_ensemble_destroy(tbfp_ensemble *e) {
+  if (!e) return TBFP_OK;
+  cudaSetDevice(e->device);
+  for (cudaStream_t s : e->streams)
+    if (s) cudaStreamSynchronize(s);
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  for (tbfp_handle *h : e->h) tbfp_destroy(h);
+  for (cudaEvent_t v : e->ev)
+    if (v) cudaEventDestroy(v);
+  for (cudaStream_t s : e->streams)
+    if (s) cudaStreamDestroy(s);
+  delete e;
+  return TBFP_OK;
+}
+
+int tbfp_ensemble_size(const tbfp_ensemble *e) { return e ? (int)e->h.size() : 0; }
+
+int tbfp_ensemble_projection_dev(tbfp_ensemble *e, const tbfp_member_io *io, double dt, double alpha, double rho0,
+                                 tbfp_stats *stats) {
+  set_global_error("");
+  if (!e || !io) return TBFP_ENULL;
+  const int n = (int)e->h.size();
+  for (int i = 0; i < n; ++i) {
+    const tbfp_member_io &m = io[i];
+    if (!m.ux_in || !m.uy_in || !m.uz_in || !m.ux_out || !m.uy_out || !m.uz_out || !m.rho || !m.psi_n ||
+        !m.psi_nm1 || !m.psi)
+      return set_err(nullptr, TBFP_ENULL, "tbfp_ensemble_projection: member " + std::to_string(i) + ": NULL array");
+  }
+  if (!(dt > 0.0) || !(alpha > 0.0) || !(rho0 > 0.0))
+    return set_err(nullptr, TBFP_EINVAL, "tbfp_ensemble_projection: dt, alpha and rho0 must be positive");
+  cudaSetDevice(e->device);
+  cudaStream_t s0 = e->streams[0];
+  int rc = TBFP_OK;
+  if (e->graphable) {
+    bool reuse = e->graph && e->kdt == dt && e->kalpha == alpha && e->krho0 == rho0 && (int)e->key.size() == n;
+    for (int i = 0; reuse && i < n; ++i) reuse = same_io(e->key[i], io[i]);
+    if (!reuse) {
+      if (e->graph) cudaGraphExecDestroy(e->graph);
+      e->graph = nullptr;
+      cudaGraph_t g = nullptr;
+      cudaError_t ce = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal);
+      if (ce == cudaSuccess) {
+        cudaEventRecord(e->ev[0], s0);
+        rc = ensemble_launch_all(e, io, dt, alpha, rho0);
+        ce = cudaStreamEndCapture(s0, &g);
+      }
+      if (rc < 0) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->graph, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (ce != cudaSuccess)
+        return set_err(nullptr, TBFP_ECUDA, std::string("tbfp_ensemble_projection: graph: ") + cudaGetErrorString(ce));
+      e->key.assign(io, io + n);
+      e->kdt = dt;
+      e->kalpha = alpha;
+      e->krho0 = rho0;
+    }
+    const cudaError_t ce = cudaGraphLaunch(e->graph, s0);
+    if (ce != cudaSuccess)
+      return set_err(nullptr, TBFP_ECUDA, std::string("tbfp_ensemble_projection: ") + cudaGetErrorString(ce));
+  } else {
+    cudaEventRecord(e->ev[0], s0);
+    rc = ensemble_launch_all(e, io, dt, alpha, rho0);
+    if (rc < 0) return rc;
+  }
+  const cudaError_t ce = cudaStreamSynchronize(s0);
+  if (ce != cudaSuccess)
+    return set_err(nullptr, TBFP_ECUDA, std::string("tbfp_ensemble_projection: ") + cudaGetErrorString(ce));
+  if (stats) {
+    for (int i = 0; i < n; ++i) {
+      unsigned long long bits = 0;
+      if (cudaMemcpy(&bits, e->h[i]->d_maxdiv, sizeof(bits), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return set_err(nullptr, TBFP_ECUDA, "tbfp_ensemble_projection: reading the continuity error");
+      double md;
+      std::memcpy(&md, &bits, sizeof(md));
+      stats[i] = e->h[i]->last;
+      stats[i].max_div = md;
+      stats[i].cont_err = md * dt;
+    }
+  }
+  return rc;
+}
+
 }  // extern "C"

@@ -30,6 +30,28 @@ constexpr int kMgThreads = 256;
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 __device__ __forceinline__ int clampi(int j, int n) { return j < 0 ? 0 : (j >= n ? n - 1 : j); }
 
+// Launch shape of the stencil kernels: grid (x tiles of kWalkX, y chunks of J
+// rows, z planes) with J = ceil(ny / gridDim.y); a thread owns column (i, k) of
+// a y chunk and walks it, so there is no integer division per cell.  Kernels
+// without a reduction are launched with J = 1 (one cell per thread, most
+// parallelism); reductions with J = kMgJ (one block sum per kMgJ rows).  Dense
+// level arrays: t = (k*ny + j)*nx + i (32-bit: every level holds fewer than
+// 2^31 cells, checked at set-up).
+constexpr int kMgJ = 16;
+constexpr int kWalkX = 128;  // threads per block of the column-walk kernels
+struct Walk {
+  int i, j0, j1, k;
+};
+__device__ __forceinline__ Walk walk(int ny) {
+  Walk w;
+  const int J = (ny + (int)gridDim.y - 1) / (int)gridDim.y;
+  w.i = blockIdx.x * blockDim.x + threadIdx.x;
+  w.k = blockIdx.z;
+  w.j0 = blockIdx.y * J;
+  w.j1 = min(w.j0 + J, ny);
+  return w;
+}
+
 // Face coefficients of cell (i, j, k) (0-based) from a dense beta.
 template <typename T>
 struct Coef {
@@ -81,40 +103,34 @@ __device__ __forceinline__ void block_sum2(double a, double b, double *out_a, do
 // ---------------------------------------------------------------------------
 // One colour of iterateGS (rbgs.f90:215-250): cells with (i+j+k) mod 2 == colour
 // (1-based indices, red = 0) take p = (-q + sum a_nb p_nb) / sum a_nb.
-// With sum != nullptr (the last black sweep of a smoothing call) each thread
-// also adds its cell and the other cell of its x pair (2m, 2m+1: one of each
-// colour, nx even on every smoothed level) to *sum: the interior sum of p.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kMgThreads) k_rbgs_colour(MgLev L, float *__restrict__ p,
-                                                           const float *__restrict__ q,
-                                                           const float *__restrict__ beta, int colour,
-                                                           double *__restrict__ sum) {
-  const int nxh = (L.nx + 1) / 2;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long total = (long)nxh * L.ny * L.nz;
-  double acc = 0.0;
-  if (t < total) {
-    const int ih = (int)(t % nxh);
-    const long r = t / nxh;
-    const int j = (int)(r % L.ny), k = (int)(r / L.ny);
-    // colour of 1-based (i+1, j+1, k+1): (i + j + k + 3) mod 2, so the row's first
-    // 0-based index of this colour is (colour + j + k + 1) mod 2
-    const int ii = 2 * ih + ((colour + j + k + 1) & 1);
-    if (ii < L.nx) {
-      const int nx = L.nx, ny = L.ny, nz = L.nz;
-      auto at3 = [&](int a, int b, int c) { return ((long)c * ny + b) * nx + a; };
-      const Coef<float> c = coef<float>(L, beta, ii, j, k);
-      const float den = c.aR + c.aL + c.aT + c.aB + c.aF + c.aK;
-      const float pR = p[at3(wrap(ii + 1, nx), j, k)], pL = p[at3(wrap(ii - 1, nx), j, k)];
-      const float pT = p[at3(ii, clampi(j + 1, ny), k)], pB = p[at3(ii, clampi(j - 1, ny), k)];
-      const float pF = p[at3(ii, j, wrap(k + 1, nz))], pK = p[at3(ii, j, wrap(k - 1, nz))];
-      const float v =
-          (-q[at3(ii, j, k)] + (c.aR * pR + c.aL * pL) + (c.aT * pT + c.aB * pB) + (c.aF * pF + c.aK * pK)) / den;
-      p[at3(ii, j, k)] = v;
-      if (sum) acc = (double)v + (double)((ii & 1) ? pL : pR);
-    }
+__global__ void __launch_bounds__(kWalkX) k_rbgs_colour(MgLev L, float *__restrict__ p,
+                                                       const float *__restrict__ q,
+                                                       const float *__restrict__ beta, int colour) {
+  const Walk w = walk(L.ny);
+  const int nx = L.nx, ny = L.ny, nz = L.nz, k = w.k;
+  if (w.i >= (nx + 1) / 2) return;  // no block-level barrier in this kernel
+  for (int j = w.j0; j < w.j1; ++j) {
+    // colour of 1-based (i+1, j+1, k+1) is (i + j + k + 3) mod 2, so the row's
+    // first 0-based index of this colour is (colour + j + k + 1) mod 2
+    const int ii = 2 * w.i + ((colour + j + k + 1) & 1);
+    if (ii >= nx) continue;
+    auto at3 = [&](int a, int b, int c) { return (c * ny + b) * nx + a; };
+    const Coef<float> c = coef<float>(L, beta, ii, j, k);
+    const float den = c.aR + c.aL + c.aT + c.aB + c.aF + c.aK;
+    const float pR = p[at3(wrap(ii + 1, nx), j, k)], pL = p[at3(wrap(ii - 1, nx), j, k)];
+    const float pT = p[at3(ii, clampi(j + 1, ny), k)], pB = p[at3(ii, clampi(j - 1, ny), k)];
+    const float pF = p[at3(ii, j, wrap(k + 1, nz))], pK = p[at3(ii, j, wrap(k - 1, nz))];
+    p[at3(ii, j, k)] =
+        (-q[at3(ii, j, k)] + (c.aR * pR + c.aL * pL) + (c.aT * pT + c.aB * pB) + (c.aF * pF + c.aK * pK)) / den;
   }
-  if (sum) block_sum2(acc, 0.0, sum, nullptr);
+}
+
+// interior sum of p (the average of correctFullNeumann, rbgs.f90:403-446)
+__global__ void __launch_bounds__(kMgThreads) k_sum(const float *__restrict__ p, long n, double *__restrict__ out) {
+  double s = 0.0;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) s += p[t];
+  block_sum2(s, 0.0, out, nullptr);
 }
 
 // p -= sum/n (correctFullNeumann, rbgs.f90:403-446)
@@ -129,24 +145,24 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_residual(MgLev L, const float
                                                            const float *__restrict__ q,
                                                            const float *__restrict__ beta, float *__restrict__ res,
                                                            double *__restrict__ nrm) {
-  const long n = (long)L.nx * L.ny * L.nz;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const Walk w = walk(L.ny);
+  const int nx = L.nx, ny = L.ny, nz = L.nz, i = w.i, k = w.k;
   double rr = 0.0, qq = 0.0;
-  if (t < n) {
-    const int nx = L.nx, ny = L.ny, nz = L.nz;
-    const int i = (int)(t % nx);
-    const long r = t / nx;
-    const int j = (int)(r % ny), k = (int)(r / ny);
-    auto at3 = [&](int a, int b, int c) { return ((long)c * ny + b) * nx + a; };
-    const Coef<float> c = coef<float>(L, beta, i, j, k);
-    const float pc = p[t];
-    const float Lp = c.aR * (p[at3(wrap(i + 1, nx), j, k)] - pc) - c.aL * (pc - p[at3(wrap(i - 1, nx), j, k)]) +
-                     c.aT * (p[at3(i, clampi(j + 1, ny), k)] - pc) - c.aB * (pc - p[at3(i, clampi(j - 1, ny), k)]) +
-                     c.aF * (p[at3(i, j, wrap(k + 1, nz))] - pc) - c.aK * (pc - p[at3(i, j, wrap(k - 1, nz))]);
-    const float v = q[t] - Lp;
-    res[t] = v;
-    rr = (double)v * v;
-    qq = (double)q[t] * q[t];
+  if (i < nx) {
+    auto at3 = [&](int a, int b, int c) { return (c * ny + b) * nx + a; };
+#pragma unroll 4
+    for (int j = w.j0; j < w.j1; ++j) {
+      const int t = at3(i, j, k);
+      const Coef<float> c = coef<float>(L, beta, i, j, k);
+      const float pc = p[t];
+      const float Lp = c.aR * (p[at3(wrap(i + 1, nx), j, k)] - pc) - c.aL * (pc - p[at3(wrap(i - 1, nx), j, k)]) +
+                       c.aT * (p[at3(i, clampi(j + 1, ny), k)] - pc) - c.aB * (pc - p[at3(i, clampi(j - 1, ny), k)]) +
+                       c.aF * (p[at3(i, j, wrap(k + 1, nz))] - pc) - c.aK * (pc - p[at3(i, j, wrap(k - 1, nz))]);
+      const float v = q[t] - Lp;
+      res[t] = v;
+      rr += (double)v * v;
+      qq += (double)q[t] * q[t];
+    }
   }
   if (nrm) block_sum2(rr, qq, nrm, nrm + 1);
 }
@@ -155,25 +171,24 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_residual(MgLev L, const float
 // separable trilinear weights w[I][a] (a = 0: child 2I-1, a = 1: child 2I, 1-based).
 __global__ void __launch_bounds__(kMgThreads) k_restrict(MgLev F, MgLev C, const float *__restrict__ fine,
                                                         float *__restrict__ coarse) {
-  const long n = (long)C.nx * C.ny * C.nz;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int I = (int)(t % C.nx);
-  const long r = t / C.nx;
-  const int J = (int)(r % C.ny), K = (int)(r / C.ny);
-  auto f = [&](int a, int b, int c) { return fine[((long)(2 * K + c) * F.ny + (2 * J + b)) * F.nx + (2 * I + a)]; };
+  const Walk w = walk(C.ny);
+  const int I = w.i, K = w.k;
+  if (I >= C.nx) return;  // no block-level barrier in this kernel
   const float x0 = C.rx[2 * I], x1 = C.rx[2 * I + 1];
-  const float y0 = C.ry[2 * J], y1 = C.ry[2 * J + 1];
   const float z0 = C.rz[2 * K], z1 = C.rz[2 * K + 1];
-  float s = (x0 * y0) * z0 * f(0, 0, 0);
-  s += (x1 * y0) * z0 * f(1, 0, 0);
-  s += (x0 * y1) * z0 * f(0, 1, 0);
-  s += (x1 * y1) * z0 * f(1, 1, 0);
-  s += (x0 * y0) * z1 * f(0, 0, 1);
-  s += (x1 * y0) * z1 * f(1, 0, 1);
-  s += (x0 * y1) * z1 * f(0, 1, 1);
-  s += (x1 * y1) * z1 * f(1, 1, 1);
-  coarse[t] = s;
+  for (int J = w.j0; J < w.j1; ++J) {
+    auto f = [&](int a, int b, int c) { return fine[((2 * K + c) * F.ny + (2 * J + b)) * F.nx + (2 * I + a)]; };
+    const float y0 = C.ry[2 * J], y1 = C.ry[2 * J + 1];
+    float s = (x0 * y0) * z0 * f(0, 0, 0);
+    s += (x1 * y0) * z0 * f(1, 0, 0);
+    s += (x0 * y1) * z0 * f(0, 1, 0);
+    s += (x1 * y1) * z0 * f(1, 1, 0);
+    s += (x0 * y0) * z1 * f(0, 0, 1);
+    s += (x1 * y0) * z1 * f(1, 0, 1);
+    s += (x0 * y1) * z1 * f(0, 1, 1);
+    s += (x1 * y1) * z1 * f(1, 1, 1);
+    coarse[(K * C.ny + J) * C.nx + I] = s;
+  }
 }
 
 // prolongationOp3D (interpolation.f90:129-181): fine += trilinear interpolation
@@ -181,30 +196,30 @@ __global__ void __launch_bounds__(kMgThreads) k_restrict(MgLev F, MgLev C, const
 // through wrapped / clamped indices).
 __global__ void __launch_bounds__(kMgThreads) k_prolong_add(MgLev F, MgLev C, const float *__restrict__ coarse,
                                                            float *__restrict__ fine) {
-  const long n = (long)F.nx * F.ny * F.nz;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int i = (int)(t % F.nx);
-  const long r = t / F.nx;
-  const int j = (int)(r % F.ny), k = (int)(r / F.ny);
+  const Walk w = walk(F.ny);
+  const int i = w.i, k = w.k;
+  if (i >= F.nx) return;  // no block-level barrier in this kernel
   // 1-based fine index i+1 -> ih = (i+1)/2, coarse 0-based ih-1 and ih
-  const int ih = (i + 1) / 2 - 1, jh = (j + 1) / 2 - 1, kh = (k + 1) / 2 - 1;
+  const int ih = (i + 1) / 2 - 1, kh = (k + 1) / 2 - 1;
   const int xa = wrap(ih, C.nx), xb = wrap(ih + 1, C.nx);
-  const int ya = clampi(jh, C.ny), yb = clampi(jh + 1, C.ny);
   const int za = wrap(kh, C.nz), zb = wrap(kh + 1, C.nz);
-  auto c = [&](int a, int b, int cc) { return coarse[((long)cc * C.ny + b) * C.nx + a]; };
   const float x0 = F.px[2 * i], x1 = F.px[2 * i + 1];
-  const float y0 = F.py[2 * j], y1 = F.py[2 * j + 1];
   const float z0 = F.pz[2 * k], z1 = F.pz[2 * k + 1];
-  float s = (x0 * y0) * z0 * c(xa, ya, za);
-  s += (x1 * y0) * z0 * c(xb, ya, za);
-  s += (x0 * y1) * z0 * c(xa, yb, za);
-  s += (x1 * y1) * z0 * c(xb, yb, za);
-  s += (x0 * y0) * z1 * c(xa, ya, zb);
-  s += (x1 * y0) * z1 * c(xb, ya, zb);
-  s += (x0 * y1) * z1 * c(xa, yb, zb);
-  s += (x1 * y1) * z1 * c(xb, yb, zb);
-  fine[t] += s;
+  auto c = [&](int a, int b, int cc) { return coarse[(cc * C.ny + b) * C.nx + a]; };
+  for (int j = w.j0; j < w.j1; ++j) {
+    const int jh = (j + 1) / 2 - 1;
+    const int ya = clampi(jh, C.ny), yb = clampi(jh + 1, C.ny);
+    const float y0 = F.py[2 * j], y1 = F.py[2 * j + 1];
+    float s = (x0 * y0) * z0 * c(xa, ya, za);
+    s += (x1 * y0) * z0 * c(xb, ya, za);
+    s += (x0 * y1) * z0 * c(xa, yb, za);
+    s += (x1 * y1) * z0 * c(xb, yb, za);
+    s += (x0 * y0) * z1 * c(xa, ya, zb);
+    s += (x1 * y0) * z1 * c(xb, ya, zb);
+    s += (x0 * y1) * z1 * c(xa, yb, zb);
+    s += (x1 * y1) * z1 * c(xb, yb, zb);
+    fine[(k * F.ny + j) * F.nx + i] += s;
+  }
 }
 
 __global__ void k_fill(float *__restrict__ p, long n, float v) {
@@ -251,7 +266,9 @@ __global__ void k_coarse_assemble(MgLev L, const float *__restrict__ beta, doubl
 
 __global__ void __launch_bounds__(1024) k_gauss_jordan(double *__restrict__ M, int n1, int *__restrict__ fail) {
   const int ld = 2 * n1;
-  extern __shared__ double fac[];  // n1 row factors
+  extern __shared__ double gj_smem[];
+  double *fac = gj_smem;        // n1 row factors of the current column
+  double *prow = gj_smem + n1;  // the scaled pivot row (2*n1)
   __shared__ double bestv[32];
   __shared__ int besti[32];
   __shared__ int piv;
@@ -302,12 +319,18 @@ __global__ void __launch_bounds__(1024) k_gauss_jordan(double *__restrict__ M, i
     __syncthreads();
     const double inv = 1.0 / M[(long)kcol * ld + kcol];
     for (int r = threadIdx.x; r < n1; r += blockDim.x) fac[r] = M[(long)r * ld + kcol];
+    for (int c = kcol + threadIdx.x; c < ld; c += blockDim.x) prow[c] = M[(long)kcol * ld + c] * inv;
     __syncthreads();
-    for (int c = kcol + threadIdx.x; c < ld; c += blockDim.x) M[(long)kcol * ld + c] *= inv;
-    __syncthreads();
-    for (long e = threadIdx.x; e < (long)n1 * (ld - kcol); e += blockDim.x) {
-      const int r = (int)(e / (ld - kcol)), c = kcol + (int)(e % (ld - kcol));
-      if (r != kcol) M[(long)r * ld + c] -= fac[r] * M[(long)kcol * ld + c];
+    for (int c = kcol + threadIdx.x; c < ld; c += blockDim.x) M[(long)kcol * ld + c] = prow[c];
+    // eliminate column kcol from the other rows: one warp per row, rows whose
+    // factor is zero (most of them early on: the matrix is a 7-point stencil) skipped
+    const int nw = (int)(blockDim.x >> 5);
+    for (int r = w; r < n1; r += nw) {
+      const double f = fac[r];
+      if (r == kcol || f == 0.0) continue;
+      double *row = M + (long)r * ld;
+#pragma unroll 8
+      for (int c = kcol + l; c < ld; c += 32) row[c] -= f * prow[c];
     }
     __syncthreads();
   }
@@ -365,21 +388,22 @@ __device__ __forceinline__ double apply_L64(const Fine &F, const Coef<double> &c
 __global__ void __launch_bounds__(kMgThreads) k_pcg_init(Fine F, const double *__restrict__ psi, Lay Lp,
                                                         const double *__restrict__ q, Lay Lq, double *__restrict__ r,
                                                         float *__restrict__ r32, double *__restrict__ acc) {
-  const long n = (long)F.nx * F.ny * F.nz;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const Walk w = walk(F.ny);
+  const int i = w.i, k = w.k;
   double qq = 0.0, rr = 0.0;
-  if (t < n) {
-    const int i = (int)(t % F.nx);
-    const long rw = t / F.nx;
-    const int j = (int)(rw % F.ny), k = (int)(rw / F.ny);
-    const Coef<double> c = coef64(F, i, j, k);
+  if (i < F.nx) {
     auto get = [&](int a, int b, int cc) { return psi[at(Lp, a + 1, b + 1, cc + 1)]; };
-    const double qv = q[at(Lq, i + 1, j + 1, k + 1)];
-    const double v = qv - apply_L64(F, c, get, i, j, k);
-    r[t] = v;
-    r32[t] = (float)v;
-    qq = qv * qv;
-    rr = v * v;
+#pragma unroll 4
+    for (int j = w.j0; j < w.j1; ++j) {
+      const int t = (k * F.ny + j) * F.nx + i;
+      const Coef<double> c = coef64(F, i, j, k);
+      const double qv = q[at(Lq, i + 1, j + 1, k + 1)];
+      const double v = qv - apply_L64(F, c, get, i, j, k);
+      r[t] = v;
+      r32[t] = (float)v;
+      qq += qv * qv;
+      rr += v * v;
+    }
   }
   block_sum2(qq, rr, acc, acc + 1);
 }
@@ -387,18 +411,19 @@ __global__ void __launch_bounds__(kMgThreads) k_pcg_init(Fine F, const double *_
 // qv = L d, sum d*qv -> *dq
 __global__ void __launch_bounds__(kMgThreads) k_pcg_qv(Fine F, const double *__restrict__ d, double *__restrict__ qv,
                                                       double *__restrict__ dq) {
-  const long n = (long)F.nx * F.ny * F.nz;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const Walk w = walk(F.ny);
+  const int i = w.i, k = w.k;
   double s = 0.0;
-  if (t < n) {
-    const int i = (int)(t % F.nx);
-    const long rw = t / F.nx;
-    const int j = (int)(rw % F.ny), k = (int)(rw / F.ny);
-    const Coef<double> c = coef64(F, i, j, k);
-    auto get = [&](int a, int b, int cc) { return d[((long)cc * F.ny + b) * F.nx + a]; };
-    const double v = apply_L64(F, c, get, i, j, k);
-    qv[t] = v;
-    s = d[t] * v;
+  if (i < F.nx) {
+    auto get = [&](int a, int b, int cc) { return d[(cc * F.ny + b) * F.nx + a]; };
+#pragma unroll 4
+    for (int j = w.j0; j < w.j1; ++j) {
+      const int t = (k * F.ny + j) * F.nx + i;
+      const Coef<double> c = coef64(F, i, j, k);
+      const double v = apply_L64(F, c, get, i, j, k);
+      qv[t] = v;
+      s += d[t] * v;
+    }
   }
   block_sum2(s, 0.0, dq, nullptr);
 }
@@ -408,19 +433,20 @@ __global__ void __launch_bounds__(kMgThreads) k_pcg_update(Fine F, double *__res
                                                           const double *__restrict__ d, const double *__restrict__ qv,
                                                           double *__restrict__ r, float *__restrict__ r32,
                                                           const double *__restrict__ sc, double *__restrict__ rr) {
-  const long n = (long)F.nx * F.ny * F.nz;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const Walk w = walk(F.ny);
+  const int i = w.i, k = w.k;
   const double alpha = sc[0] / sc[1];  // deltaN / (d . qv)
   double s = 0.0;
-  if (t < n) {
-    const int i = (int)(t % F.nx);
-    const long rw = t / F.nx;
-    const int j = (int)(rw % F.ny), k = (int)(rw / F.ny);
-    psi[at(Lp, i + 1, j + 1, k + 1)] += alpha * d[t];
-    const double v = r[t] - alpha * qv[t];
-    r[t] = v;
-    r32[t] = (float)v;
-    s = v * v;
+  if (i < F.nx) {
+#pragma unroll 4
+    for (int j = w.j0; j < w.j1; ++j) {
+      const int t = (k * F.ny + j) * F.nx + i;
+      psi[at(Lp, i + 1, j + 1, k + 1)] += alpha * d[t];
+      const double v = r[t] - alpha * qv[t];
+      r[t] = v;
+      r32[t] = (float)v;
+      s += v * v;
+    }
   }
   block_sum2(s, 0.0, rr, nullptr);
 }
@@ -444,13 +470,10 @@ __global__ void __launch_bounds__(kMgThreads) k_pcg_dir(const float *__restrict_
 
 // beta (caller layout, FP64) -> dense FP32 level-0 copy
 __global__ void k_beta32(Fine F, float *__restrict__ b32) {
-  const long n = (long)F.nx * F.ny * F.nz;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % F.nx);
-    const long rw = t / F.nx;
-    const int j = (int)(rw % F.ny), k = (int)(rw / F.ny);
-    b32[t] = (float)F.beta[at(F.Lb, i + 1, j + 1, k + 1)];
-  }
+  const Walk w = walk(F.ny);
+  const int i = w.i, k = w.k;
+  if (i >= F.nx) return;
+  for (int j = w.j0; j < w.j1; ++j) b32[(k * F.ny + j) * F.nx + i] = (float)F.beta[at(F.Lb, i + 1, j + 1, k + 1)];
 }
 
 // ghost images of psi (updateBoundaries on one rank): x, z periodic, first y
@@ -474,6 +497,9 @@ __global__ void k_psi_ghosts(double *__restrict__ psi, Lay Lp, int hd, int nx, i
 }
 
 unsigned nblk(long n) { return (unsigned)((n + kMgThreads - 1) / kMgThreads); }
+dim3 wgrid(int nxe, int ny, int nz, int J) {
+  return dim3((unsigned)((nxe + kWalkX - 1) / kWalkX), (unsigned)((ny + J - 1) / J), (unsigned)nz);
+}
 unsigned nblk_grid(long n) {
   long b = (n + kMgThreads - 1) / kMgThreads;
   return (unsigned)std::min<long>(b, 148L * 8);
@@ -607,6 +633,8 @@ int MgSolver::init(const tbfp_mg_params &prm, int nx, int ny, int nz, const doub
   if (ncoarse > 2048)
     return *err = "tbfp_pcg_setup: coarsest level has more than 2048 cells; use more levels", TBFP_EUNSUPPORTED;
   m.n1 = (int)ncoarse + 1;
+  if ((long)nx * ny * nz >= (1L << 31) || nz > 65535)
+    return *err = "tbfp_pcg_setup: grid too large (2^31 cells or nz > 65535)", TBFP_EUNSUPPORTED;
   cudaError_t e = cudaSuccess;
   auto ck = [&](cudaError_t x) {
     if (x != cudaSuccess && e == cudaSuccess) e = x;
@@ -737,6 +765,7 @@ int MgSolver::init(const tbfp_mg_params &prm, int nx, int ny, int nz, const doub
   ck(m.alloc(&m.r32, m.n));
   ck(m.alloc(&m.sc, 16));
   ck(m.alloc(&m.Minv, (size_t)m.n1 * 2 * m.n1));
+  ck(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * m.n1 * (int)sizeof(double)));
   ck(m.alloc(&m.fail, 1));
   if (e != cudaSuccess) {
     *err = std::string("tbfp_pcg_setup: ") + cudaGetErrorString(e);
@@ -756,18 +785,17 @@ struct Run {
   // (correctFullNeumann) after every red+black iteration.  A sweep commutes
   // with adding a constant to p (the update is an average of neighbours, q
   // fixed), so removing the mean once after the last iteration gives the same
-  // p; the sum comes out of the last black sweep.
+  // p.
   void rbgs(int l, int n_iter, bool reset) {
     auto &L = m.lv[l];
     if (reset) k_fill<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, 0.0f);
     if (n_iter == 0) return;
-    const long half = (long)((L.nx + 1) / 2) * L.ny * L.nz;
-    cudaMemsetAsync(m.sc + 8, 0, sizeof(double), st);
     for (int it = 0; it < n_iter; ++it) {
-      k_rbgs_colour<<<nblk(half), kMgThreads, 0, st>>>(L.L, L.p, L.q, L.beta, 0, nullptr);
-      k_rbgs_colour<<<nblk(half), kMgThreads, 0, st>>>(L.L, L.p, L.q, L.beta, 1,
-                                                        it == n_iter - 1 ? m.sc + 8 : nullptr);
+      k_rbgs_colour<<<wgrid((L.nx + 1) / 2, L.ny, L.nz, 1), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, 0);
+      k_rbgs_colour<<<wgrid((L.nx + 1) / 2, L.ny, L.nz, 1), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, 1);
     }
+    cudaMemsetAsync(m.sc + 8, 0, sizeof(double), st);
+    k_sum<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, m.sc + 8);
     k_sub_mean<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, m.sc + 8);
   }
 
@@ -779,11 +807,11 @@ struct Run {
       return;
     }
     rbgs(l, m.prm.n_pre, l != 0);
-    k_mg_residual<<<nblk(L.n), kMgThreads, 0, st>>>(L.L, L.p, L.q, L.beta, L.res, nullptr);
+    k_mg_residual<<<wgrid(L.nx, L.ny, L.nz, 1), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, L.res, nullptr);
     auto &C = m.lv[l + 1];
-    k_restrict<<<nblk(C.n), kMgThreads, 0, st>>>(L.L, C.L, L.res, C.q);
+    k_restrict<<<wgrid(C.nx, C.ny, C.nz, 1), kWalkX, 0, st>>>(L.L, C.L, L.res, C.q);
     vcycle(l + 1);
-    k_prolong_add<<<nblk(L.n), kMgThreads, 0, st>>>(L.L, C.L, C.p, L.p);
+    k_prolong_add<<<wgrid(L.nx, L.ny, L.nz, 1), kWalkX, 0, st>>>(L.L, C.L, C.p, L.p);
     rbgs(l, m.prm.n_post, false);
   }
 
@@ -791,7 +819,7 @@ struct Run {
   double fine_residual() {
     auto &L = m.lv[0];
     cudaMemsetAsync(m.sc + 6, 0, 2 * sizeof(double), st);
-    k_mg_residual<<<nblk(L.n), kMgThreads, 0, st>>>(L.L, L.p, L.q, L.beta, L.res, m.sc + 6);
+    k_mg_residual<<<wgrid(L.nx, L.ny, L.nz, kMgJ), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, L.res, m.sc + 6);
     double v[2] = {0.0, 0.0};
     cudaMemcpyAsync(v, m.sc + 6, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
@@ -857,17 +885,18 @@ int MgSolver::solve(double *psi, Lay Lp, int hd_psi, const double *beta, Lay Lb,
   run.capture();
   *mg_cycles = 0;
   // beta on every level (restrictField, field.f90:1442-1470)
-  k_beta32<<<nblk_grid(m.n), kMgThreads, 0, st>>>(F, m.lv[0].beta);
+  k_beta32<<<wgrid(m.nx, m.ny, m.nz, 1), kWalkX, 0, st>>>(F, m.lv[0].beta);
   for (size_t l = 1; l < m.lv.size(); ++l)
-    k_restrict<<<nblk(m.lv[l].n), kMgThreads, 0, st>>>(m.lv[l - 1].L, m.lv[l].L, m.lv[l - 1].beta, m.lv[l].beta);
+    k_restrict<<<wgrid(m.lv[l].nx, m.lv[l].ny, m.lv[l].nz, 1), kWalkX, 0, st>>>(m.lv[l - 1].L, m.lv[l].L,
+                                                                                 m.lv[l - 1].beta, m.lv[l].beta);
   // coarsest bordered system, inverted once for this beta
   auto &C = m.lv.back();
   cudaMemsetAsync(m.fail, 0, sizeof(int), st);
   k_coarse_assemble<<<1, 1024, 0, st>>>(C.L, C.beta, m.Minv, m.n1);
-  k_gauss_jordan<<<1, 1024, m.n1 * sizeof(double), st>>>(m.Minv, m.n1, m.fail);
+  k_gauss_jordan<<<1, 1024, 3 * m.n1 * sizeof(double), st>>>(m.Minv, m.n1, m.fail);
   // r = q - L psi (psi: the initial guess), z = MG(r), d = z
   cudaMemsetAsync(m.sc, 0, 16 * sizeof(double), st);
-  k_pcg_init<<<nblk(m.n), kMgThreads, 0, st>>>(F, psi, Lp, q, Lq, m.r, m.lv[0].q, m.sc + 4);
+  k_pcg_init<<<wgrid(m.nx, m.ny, m.nz, kMgJ), kWalkX, 0, st>>>(F, psi, Lp, q, Lq, m.r, m.lv[0].q, m.sc + 4);
   *mg_cycles += run.solve_mg();
   k_pcg_dot<<<nblk_grid(m.n), kMgThreads, 0, st>>>(m.r, m.lv[0].p, m.n, m.sc + 0);
   k_pcg_dir<<<nblk_grid(m.n), kMgThreads, 0, st>>>(m.lv[0].p, m.d, m.n, m.sc, 1);
@@ -893,9 +922,9 @@ int MgSolver::solve(double *psi, Lay Lp, int hd_psi, const double *beta, Lay Lb,
     if (it == m.prm.max_iter_pcg || !(res > m.prm.tol_pcg)) break;
     ++it;
     cudaMemsetAsync(m.sc + 1, 0, sizeof(double), st);
-    k_pcg_qv<<<nblk(m.n), kMgThreads, 0, st>>>(F, m.d, m.qv, m.sc + 1);
+    k_pcg_qv<<<wgrid(m.nx, m.ny, m.nz, kMgJ), kWalkX, 0, st>>>(F, m.d, m.qv, m.sc + 1);
     cudaMemsetAsync(m.sc + 5, 0, sizeof(double), st);
-    k_pcg_update<<<nblk(m.n), kMgThreads, 0, st>>>(F, psi, Lp, m.d, m.qv, m.r, m.lv[0].q, m.sc, m.sc + 5);
+    k_pcg_update<<<wgrid(m.nx, m.ny, m.nz, kMgJ), kWalkX, 0, st>>>(F, psi, Lp, m.d, m.qv, m.r, m.lv[0].q, m.sc, m.sc + 5);
     *mg_cycles += run.solve_mg();
     cudaMemcpyAsync(m.sc + 3, m.sc + 0, sizeof(double), cudaMemcpyDeviceToDevice, st);  // deltaN_old
     cudaMemsetAsync(m.sc + 2, 0, sizeof(double), st);

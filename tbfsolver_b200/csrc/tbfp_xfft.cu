@@ -34,7 +34,7 @@ void launch_recip(const double *rho, double *irho, long n, cudaStream_t st) {
 // rows.  V = double2 (FP64) or float2 (the FP32 spectrum of the mixed path).
 // ---------------------------------------------------------------------------
 template <typename V, int M, int MODE>
-__global__ void __launch_bounds__(kNT, 2) k_fftx_fwd(XSrc src, GridK g, const V *__restrict__ twx,
+__global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_fwd(XSrc src, GridK g, const V *__restrict__ twx,
                                                   const V *__restrict__ tpx, V *__restrict__ spec) {
   using T = decltype(V::x);
   constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kNT, 2) k_fftx_fwd(XSrc src, GridK g, const V 
   __syncthreads();
   // S[kx][r0 + row]: consecutive threads take consecutive rows of one kx
   constexpr int NST = ((M + 1) << LOGTJ);
-#pragma unroll 4
+#pragma unroll
   for (int t = threadIdx.x; t < NST; t += kNT) {
     const int kx = t >> LOGTJ, row = t & (TJ - 1);
     if (row < nrows) spec[(long)kx * g.R + r0 + row] = sm[row * LD + pad8(kx)];
@@ -306,7 +306,7 @@ void launch_rhs(const RhsArgs &ra, bool has_st, const GridK &g, double *s, Lay L
 constexpr int kNoGhost = -(1 << 30);  // no ghost image of this index
 
 template <typename V, int M, bool ACC>
-__global__ void __launch_bounds__(kNT, 2) k_fftx_inv(const V *__restrict__ spec, double *__restrict__ psi, Lay Lp,
+__global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_inv(const V *__restrict__ spec, double *__restrict__ psi, Lay Lp,
                                                   int hd, GridK g, const V *__restrict__ twx,
                                                   const V *__restrict__ tpx, double scale) {
   using T = decltype(V::x);
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(kNT, 2) k_fftx_inv(const V *__restrict__ spec,
   const int r0 = blockIdx.x << LOGTJ;
   const int nrows = min(TJ, (int)g.R - r0);
   constexpr int NLD = ((M + 1) << LOGTJ);
-#pragma unroll 4
+#pragma unroll
   for (int t = threadIdx.x; t < NLD; t += kNT) {
     const int kx = t >> LOGTJ, row = t & (TJ - 1);
     sm[row * LD + pad8(kx)] = (row < nrows) ? spec[(long)kx * g.R + r0 + row] : mk<V>(T(0), T(0));

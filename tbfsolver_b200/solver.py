@@ -9,6 +9,8 @@ Names and argument meaning follow the Fortran modules they replace:
 * ``make_velocity_div_free`` -- momentumEqn.f90:999 (FAST_MODE).
 * ``compute_continuity_error`` -- auxiliaryRoutines.f90:42 (returns the value
   instead of printing it).
+* ``Ensemble``           -- many independent channels per GPU in one call (no
+  counterpart in the reference, which runs one channel per job).
 * ``PCG``                -- pcgMod (src/pcg/pcg.f90) with its multigrid preconditioner
   (multiGridMod, rbgsMod, poissMatMod): ``PCG(mesh, ...)`` is pcgCTOR (:62),
   ``solve_pcg(psi, beta, q)`` is solvePCG (:103).
@@ -28,7 +30,7 @@ import ctypes as C
 import numpy as np
 
 from ._native import (TBFP_EINVAL, TBFP_FLAG_ASYNC, TBFP_FLAG_RESIDUAL, TBFP_FLAG_TIMING, TBFP_FP64, TBFP_MIXED,
-                      TbfpDesc, TbfpError, TbfpMgParams, TbfpStats, check, load)
+                      TbfpDesc, TbfpError, TbfpMemberIO, TbfpMgParams, TbfpStats, check, load)
 from .fields import Field, VField
 from .grid import Grid
 
@@ -59,6 +61,24 @@ class _PtrTriple:
             self.addr = C.cast(self.arr, C.c_void_p).value
 
 
+def _metrics(mesh: Grid) -> dict:
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    return {
+        "dxf": np.ascontiguousarray(mesh.dxf.r(1, nx)), "dxc": np.ascontiguousarray(mesh.dxc.r(1, nx + 1)),
+        "dyf": np.ascontiguousarray(mesh.dyf.r(1, ny)), "dyc": np.ascontiguousarray(mesh.dyc.r(1, ny + 1)),
+        "dzf": np.ascontiguousarray(mesh.dzf.r(1, nz)), "dzc": np.ascontiguousarray(mesh.dzc.r(1, nz + 1)),
+    }
+
+
+def _desc(mesh: Grid, m: dict, hd_psi, hd_u, hd_rho, hd_st, precision, tol, max_iter, device, stream, flags):
+    prec = {"fp64": TBFP_FP64, "mixed": TBFP_MIXED}[precision]
+    return TbfpDesc(nx=mesh.nx, ny=mesh.ny, nz=mesh.nz, hd_psi=hd_psi, hd_u=hd_u, hd_rho=hd_rho, hd_st=hd_st,
+                    dx_fft=mesh.dx_fft, dz_fft=mesh.dz_fft, dxf=_dptr(m["dxf"]), dxc=_dptr(m["dxc"]),
+                    dyf=_dptr(m["dyf"]), dyc=_dptr(m["dyc"]), dzf=_dptr(m["dzf"]), dzc=_dptr(m["dzc"]),
+                    s_Vg=mesh.s_Vg, precision=prec, tol=tol, max_iter=max_iter, device=device, stream=stream,
+                    flags=flags)
+
+
 class FastPoissonSolver:
     """The split-constant-coefficient direct Poisson solver on one GPU."""
 
@@ -69,21 +89,11 @@ class FastPoissonSolver:
         self.lib = load()
         self.mesh = mesh
         self.hd_psi, self.hd_u, self.hd_rho, self.hd_st = hd_psi, hd_u, hd_rho, hd_st
-        nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
         # keep the metric arrays alive while the descriptor is read
-        self._m = {
-            "dxf": np.ascontiguousarray(mesh.dxf.r(1, nx)), "dxc": np.ascontiguousarray(mesh.dxc.r(1, nx + 1)),
-            "dyf": np.ascontiguousarray(mesh.dyf.r(1, ny)), "dyc": np.ascontiguousarray(mesh.dyc.r(1, ny + 1)),
-            "dzf": np.ascontiguousarray(mesh.dzf.r(1, nz)), "dzc": np.ascontiguousarray(mesh.dzc.r(1, nz + 1)),
-        }
-        prec = {"fp64": TBFP_FP64, "mixed": TBFP_MIXED}[precision]
-        d = TbfpDesc(nx=nx, ny=ny, nz=nz, hd_psi=hd_psi, hd_u=hd_u, hd_rho=hd_rho, hd_st=hd_st,
-                     dx_fft=mesh.dx_fft, dz_fft=mesh.dz_fft,
-                     dxf=_dptr(self._m["dxf"]), dxc=_dptr(self._m["dxc"]), dyf=_dptr(self._m["dyf"]),
-                     dyc=_dptr(self._m["dyc"]), dzf=_dptr(self._m["dzf"]), dzc=_dptr(self._m["dzc"]),
-                     s_Vg=mesh.s_Vg, precision=prec, tol=tol, max_iter=max_iter, device=device,
-                     stream=stream, flags=(TBFP_FLAG_ASYNC if asynchronous else 0) | (TBFP_FLAG_TIMING if timing else 0)
-                     | (TBFP_FLAG_RESIDUAL if residual else 0))
+        self._m = _metrics(mesh)
+        d = _desc(mesh, self._m, hd_psi, hd_u, hd_rho, hd_st, precision, tol, max_iter, device, stream,
+                  (TBFP_FLAG_ASYNC if asynchronous else 0) | (TBFP_FLAG_TIMING if timing else 0)
+                  | (TBFP_FLAG_RESIDUAL if residual else 0))
         h = C.c_void_p()
         check(self.lib.tbfp_create(C.byref(d), C.byref(h)), None)
         self.h = h
@@ -287,3 +297,53 @@ class PCG:
             check(self.lib.tbfp_projection_mg(self.h, u.ux.address(), u.uy.address(), u.uz.address(),
                                               rho.address(), dt, alpha, psi.address(), C.byref(st)), self.h)
         return st
+
+
+class Ensemble:
+    """Many independent channels on one GPU (tbfp_ensemble_*): each member has
+    its own grid; one call projects every member.  Plain FP64 members are run
+    as one replayed CUDA graph."""
+
+    def __init__(self, meshes, nstreams: int = 8, precision: str = "fp64", tol: float = 1e-10, max_iter: int = 8,
+                 device: int = -1):
+        self.lib = load()
+        self.meshes = list(meshes)
+        self._m = [_metrics(g) for g in self.meshes]
+        descs = (TbfpDesc * len(self.meshes))(*[_desc(g, m, 1, 2, 1, 1, precision, tol, max_iter, device, None, 0)
+                                                for g, m in zip(self.meshes, self._m)])
+        h = C.c_void_p()
+        check(self.lib.tbfp_ensemble_create(len(self.meshes), descs, nstreams, C.byref(h)), None)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.tbfp_ensemble_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover - interpreter shutdown
+            pass
+
+    def projection(self, members, dt: float, alpha: float, rho0: float, want_stats: bool = True):
+        """members: one (psi, psi_n, psi_nm1, rho, u, u_out) tuple of device fields per
+        channel (u_out may be u).  Returns the per-member statistics or None."""
+        n = len(self.meshes)
+        if len(members) != n:
+            raise TbfpError(TBFP_EINVAL, f"expected {n} members")
+        io = (TbfpMemberIO * n)()
+        for k, (psi, pn, pnm1, rho, u, uo) in enumerate(members):
+            if not _placement([psi, pn, pnm1, rho, *u.components(), *uo.components()]):
+                raise TbfpError(TBFP_EINVAL, "ensemble members must be device fields")
+            io[k] = TbfpMemberIO(u.ux.address(), u.uy.address(), u.uz.address(), uo.ux.address(), uo.uy.address(),
+                                 uo.uz.address(), rho.address(), pn.address(), pnm1.address(), psi.address())
+        st = (TbfpStats * n)() if want_stats else None
+        check(self.lib.tbfp_ensemble_projection_dev(self.h, io, dt, alpha, rho0, st), None)
+        return list(st) if want_stats else None

@@ -73,6 +73,25 @@ CONFIGS = {
 }
 
 
+
+def ensemble_specs(n: int = 64, seed: int = 4) -> list:
+    """The ensemble workload: n channels of the reference's minimal channel box
+    (pi x 2 x pi/2, channel_18/specs/mesh:20-22), each with a seeded grid
+    nx in {64, 96, 128}, ny in {96, 128, 192}, nz in {32, 48, 64} (tanh
+    gamma 1.5), 4-24 bubbles of radius R in [0.2, 0.3], rho_l/rho_g = 1/0.05."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(n):
+        nx = int(rng.choice([64, 96, 128]))
+        ny = int(rng.choice([96, 128, 192]))
+        nz = int(rng.choice([32, 48, 64]))
+        nb = int(rng.integers(4, 25))
+        r = float(rng.uniform(0.2, 0.3))
+        out.append(ChannelSpec(f"c4-{c:02d}-{nx}x{ny}x{nz}", nx, ny, nz, Lx=math.pi, Ly=2.0, Lz=0.5 * math.pi,
+                               y_stretched=True, gamma=1.5, nbubbles=nb, radius=r, rhol=1.0, rhog=0.05))
+    return out
+
+
 # ---------------------------------------------------------------------------
 # counter-based noise
 # ---------------------------------------------------------------------------
