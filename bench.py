@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--mg", action="store_true", help="also time the MG_MODE projection (default for c5)")
+    ap.add_argument("--no-mg", action="store_true", help="skip the MG_MODE leg")
     return ap.parse_args()
 
 
@@ -406,7 +407,7 @@ def main():
     # MG_MODE leg (config 5: FP64 PCG + FP32 V-cycles, 6 levels, 2+2 sweeps,
     # tolPCG 1e-10, tolMG 0.4) on the same input; psi starts from zero every step
     mgres = None
-    if args.mg or args.config == "c5":
+    if (args.mg or args.config == "c5") and not args.no_mg:
         from tbfsolver_b200.solver import PCG
         pcg = PCG(g, n_levels=6, n_pre=2, n_post=2, tol_mg=0.4, tol_pcg=1e-10, stream=stream.cuda_stream)
         mpsi = new()

@@ -88,7 +88,7 @@ __device__ __forceinline__ double face_update(double u, double r, double ir0, do
 }
 
 template <bool ST>
-__global__ void __launch_bounds__(128, 6) k_correct_div(CorrArgs a, GridK g, unsigned long long *__restrict__ maxdiv) {
+__global__ void __launch_bounds__(128, 8) k_correct_div(CorrArgs a, GridK g, unsigned long long *__restrict__ maxdiv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int k = blockIdx.z + 1;
   const int j0 = blockIdx.y * kJC + 1, j1 = min(j0 + kJC - 1, g.ny);
