@@ -232,6 +232,24 @@ int tbfp_projection_mg_dev(tbfp_handle *h, const double *ux_in, const double *uy
                            double *ux_out, double *uy_out, double *uz_out, const double *rho, double dt,
                            double alpha, double *psi, tbfp_stats *stats);
 
+/* --- slab form: one channel split over several GPUs --------------------- */
+/* One rank's share of a channel split over P ranks (the reference's pencil
+   decomposition with py = 1, pencilDec.f90:359-562): in physical space the z
+   planes k0 .. k0+d->nz-1 of nz_total (d describes the local slab: d->nz and
+   dzf/dzc are local, d->s_Vg is the whole channel's and must be given), in
+   spectral space the wavenumbers kx0 .. kx0+nkx_loc-1.  solveFPS becomes
+     tbfp_slab_forward_x(s -> S_z[nx/2+1][nz_loc][ny]),  all-to-all to
+     S_x[nkx_loc][nz_total][ny],  tbfp_slab_spectral(S_x),  all-to-all back,
+     tbfp_slab_inverse_x(S_z -> psi),  z ghost planes of psi exchanged,
+   with the exchanges done by the caller (tbfsolver_b200.dist).  tbfp_rhs_split
+   and tbfp_correct on a slab handle read the z neighbours of the end planes
+   from the ghost planes (exchanged by the caller) instead of wrapping.
+   Spectra are complex FP64, interleaved. */
+int tbfp_slab_create(const tbfp_desc *d, int nz_total, int k0, int kx0, int nkx_loc, tbfp_handle **out);
+int tbfp_slab_forward_x(tbfp_handle *h, const double *s, double *spec_z);
+int tbfp_slab_spectral(tbfp_handle *h, double *spec_x);
+int tbfp_slab_inverse_x(tbfp_handle *h, const double *spec_z, double *psi);
+
 /* --- ensemble: many independent channels per GPU ----------------------- */
 /* No counterpart in the reference, which runs one channel per job.  Each
    member is a channel with its own descriptor (sizes may differ); its arrays

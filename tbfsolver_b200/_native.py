@@ -88,6 +88,10 @@ PROTOTYPES = {
     "tbfp_destroy": (C.c_int, [_H]),
     "tbfp_device_bytes": (C.c_size_t, [_H]),
     "tbfp_get_stats": (C.c_int, [_H, C.POINTER(TbfpStats)]),
+    "tbfp_slab_create": (C.c_int, [C.POINTER(TbfpDesc), C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "tbfp_slab_forward_x": (C.c_int, [_H, _P, _P]),
+    "tbfp_slab_spectral": (C.c_int, [_H, _P]),
+    "tbfp_slab_inverse_x": (C.c_int, [_H, _P, _P]),
     "tbfp_ensemble_create": (C.c_int, [C.c_int, C.POINTER(TbfpDesc), C.c_int, C.POINTER(C.c_void_p)]),
     "tbfp_ensemble_destroy": (C.c_int, [_H]),
     "tbfp_ensemble_size": (C.c_int, [_H]),

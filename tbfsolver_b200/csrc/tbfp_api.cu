@@ -59,6 +59,9 @@ struct tbfp_handle {
   double *d_acc = nullptr;  // reductions of the residual passes: [0] sum s dyf, [1] sum s^2, [2..] sum r^2
   double idx2 = 0.0, idz2 = 0.0, ctop_scale = 0.0;
   tbfp_stats last{};        // statistics of the last solve or projection
+  bool slab = false;        // one rank's slab of a channel (tbfp_slab_create)
+  GridK gs{};               // slab form: the spectral stage's grid (local kx, all kz)
+  int nz_total = 0;
   MgSolver *mg = nullptr;   // MG_MODE hierarchy (tbfp_pcg_setup)
   std::vector<double> mdxf, mdxc, mdyf, mdyc, mdzf, mdzc;  // caller's metrics, kept for tbfp_pcg_setup
   double *h_beta = nullptr, *h_q = nullptr;                // device copies for tbfp_pcg_solve
@@ -486,12 +489,29 @@ int tbfp_destroy(tbfp_handle *h) {
   return TBFP_OK;
 }
 
-int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
+}  // extern "C"
+
+namespace {
+// Geometry of a slab handle: this rank holds the planes k0 .. k0+nz-1 of a
+// channel of nz_total planes (physical space) and the kx0 .. kx0+nkx_loc-1
+// wavenumbers (spectral space).
+struct SlabSpec {
+  int nz_total, k0, kx0, nkx_loc;
+};
+
+int create_impl(const tbfp_desc *d, const SlabSpec *sl, tbfp_handle **out) {
   g_create_error.clear();
   if (!d || !out) return set_err(nullptr, TBFP_ENULL, "tbfp_create: NULL descriptor or output");
   *out = nullptr;
-  if (d->nx < 4 || d->ny < 4 || d->nz < 2 || (d->nx % 2) != 0)
+  if (d->nx < 4 || d->ny < 4 || d->nz < (sl ? 1 : 2) || (d->nx % 2) != 0)
     return set_err(nullptr, TBFP_EINVAL, "tbfp_create: need nx even >= 4, ny >= 4, nz >= 2");
+  if (sl) {
+    if (sl->nz_total < d->nz || sl->k0 < 0 || sl->k0 + d->nz > sl->nz_total || sl->kx0 < 0 || sl->nkx_loc < 1 ||
+        sl->kx0 + sl->nkx_loc > d->nx / 2 + 1 || d->nz < d->hd_psi)
+      return set_err(nullptr, TBFP_EINVAL, "tbfp_slab_create: inconsistent slab geometry");
+    if (!(d->s_Vg > 0.0) || d->precision != TBFP_FP64)
+      return set_err(nullptr, TBFP_EINVAL, "tbfp_slab_create: needs the channel's s_Vg and TBFP_FP64");
+  }
   if (d->hd_psi < 1 || d->hd_rho < 1 || d->hd_u < 0 || d->hd_st < 0)
     return set_err(nullptr, TBFP_EINVAL, "tbfp_create: halo widths must be hd_psi>=1, hd_rho>=1, hd_u>=0, hd_st>=0");
   if (!d->dxf || !d->dxc || !d->dyf || !d->dyc || !d->dzf || !d->dzc)
@@ -513,7 +533,7 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
   if (!(d->dxc[0] > 0.0) || !(d->dzc[0] > 0.0))
     return set_err(nullptr, TBFP_EINVAL, "tbfp_create: dxc(1), dzc(1) must be positive");
 
-  if (!fft_length_supported(d->nx / 2) || !fft_length_supported(d->nz))
+  if (!fft_length_supported(d->nx / 2) || !fft_length_supported(sl ? sl->nz_total : d->nz))
     return set_err(nullptr, TBFP_EUNSUPPORTED,
                    "tbfp_create: nx/2 and nz must be 2^a or 3*2^a between 4 and 512");
   if (tridiag_smem_bytes(d->ny) > 227 * 1024)
@@ -546,6 +566,9 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
     return set_err(nullptr, TBFP_ENODEVICE, "tbfp_create: cannot select the CUDA device");
   }
   const int nx = h->nx, ny = h->ny, nz = h->nz;
+  const int nzt = sl ? sl->nz_total : nz;  // planes of the whole channel (z transform length)
+  h->slab = sl != nullptr;
+  h->nz_total = nzt;
   h->Lpsi = make_lay(1, 1, 1, nx, ny, h->hd_psi, &h->n_psi, nz);
   h->Lrho = make_lay(1, 1, 1, nx, ny, h->hd_rho, &h->n_rho, nz);
   h->Lux = make_lay(0, 1, 1, nx + 1, ny, h->hd_u, &h->n_ux, nz);
@@ -607,14 +630,14 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
   h->mdzf.assign(d->dzf, d->dzf + nz);
   h->mdzc.assign(d->dzc, d->dzc + nz + 1);
   h->dz_fft = d->dz_fft;
-  std::vector<double> lamx(h->nkx), lamz(nz), am(ny), ap(ny), dyf(ny), idyf(ny), idyc(ny + 1), idxf(nx), idzf(nz);
+  std::vector<double> lamx(h->nkx), lamz(nzt), am(ny), ap(ny), dyf(ny), idyf(ny), idyc(ny + 1), idxf(nx), idzf(nz);
   for (int i = 0; i < h->nkx; ++i)
     lamx[i] = 2.0 * (std::cos(((double)i * 2.0 * pi) / nx) - 1.0) / (d->dx_fft * d->dx_fft);
   // lamz(k) of fastPoissonSolver.f90:215-251, evaluated at min(k, nz-k) so the
   // table is exactly even in k (the y solve pairs kz with nz-kz)
-  for (int k = 0; k < nz; ++k) {
-    const int kk = std::min(k, nz - k);
-    lamz[k] = 2.0 * (std::cos(((double)kk * 2.0 * pi) / nz) - 1.0) / (d->dz_fft * d->dz_fft);
+  for (int k = 0; k < nzt; ++k) {
+    const int kk = std::min(k, nzt - k);
+    lamz[k] = 2.0 * (std::cos(((double)kk * 2.0 * pi) / nzt) - 1.0) / (d->dz_fft * d->dz_fft);
   }
   for (int j = 0; j < ny; ++j) {
     am[j] = 1.0 / (d->dyc[j] * d->dyf[j]);
@@ -636,19 +659,19 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
   }
   h->s_Vg = sVg;
   h->mean_c = d->dx_fft * d->dz_fft / sVg;
-  h->nxnz = (double)nx * (double)nz;
-  h->scale = 1.0 / ((double)nx * (double)nz);
+  h->nxnz = (double)nx * (double)nzt;
+  h->scale = 1.0 / ((double)nx * (double)nzt);
   h->idx2 = 1.0 / (d->dx_fft * d->dx_fft);
   h->idz2 = 1.0 / (d->dz_fft * d->dz_fft);
-  h->ctop_scale = 1.0 / (d->dyf[ny - 1] * (double)nx * (double)nz);
+  h->ctop_scale = 1.0 / (d->dyf[ny - 1] * (double)nx * (double)nzt);
 
   if ((rc = upload(h, &h->d_lamx, lamx)) || (rc = upload(h, &h->d_lamz, lamz)) || (rc = upload(h, &h->d_am, am)) ||
       (rc = upload(h, &h->d_ap, ap)) || (rc = upload(h, &h->d_dyf, dyf)) || (rc = upload(h, &h->d_idyf, idyf)) ||
       (rc = upload(h, &h->d_idyc, idyc)) || (rc = upload(h, &h->d_idxf, idxf)) || (rc = upload(h, &h->d_idzf, idzf)) ||
       (rc = upload(h, &h->d_twx, unit_twiddles(nx))) || (rc = upload(h, &h->d_tpx, pass_twiddles(nx / 2))) ||
-      (rc = upload(h, &h->d_tpz, pass_twiddles(nz))) || (rc = upload(h, &h->d_twx32, to_f32(unit_twiddles(nx)))) ||
+      (rc = upload(h, &h->d_tpz, pass_twiddles(nzt))) || (rc = upload(h, &h->d_twx32, to_f32(unit_twiddles(nx)))) ||
       (rc = upload(h, &h->d_tpx32, to_f32(pass_twiddles(nx / 2)))) ||
-      (rc = upload(h, &h->d_tpz32, to_f32(pass_twiddles(nz)))) ||
+      (rc = upload(h, &h->d_tpz32, to_f32(pass_twiddles(nzt)))) ||
       (rc = upload(h, &h->d_acc, std::vector<double>(64, 0.0))) || (rc = upload(h, &h->d_idxc, inv_of(d->dxc, nx + 1))) ||
       (rc = upload(h, &h->d_idzc, inv_of(d->dzc, nz + 1))))
     return fail(rc);
@@ -665,22 +688,75 @@ int tbfp_create(const tbfp_desc *d, tbfp_handle **out) {
   g.M = nx / 2;
   g.R = h->R;
   g.idxf1 = 1.0 / d->dxf[0];
-  g.idzf1 = 1.0 / d->dzf[0];
   g.idxc1 = 1.0 / d->dxc[0];
-  g.idzc1 = 1.0 / d->dzc[0];
+  // z is uniform (the FFT direction): its metric is the channel's dz_fft, the
+  // same number on every rank of a split channel, so a slab's stencils round
+  // exactly as the whole channel's (dzf(k), dzc(k) differ from it by rounding)
+  g.idzf1 = 1.0 / d->dz_fft;
+  g.idzc1 = 1.0 / d->dz_fft;
   g.idyf = h->d_idyf;
   g.idyc = h->d_idyc;
   g.idxf = h->d_idxf;
   g.idzf = h->d_idzf;
+  if (sl) {
+    g.slab = 1;
+    h->gs = g;
+    h->gs.nz = nzt;
+    h->gs.nkx = sl->nkx_loc;
+    h->gs.R = (long)ny * nzt;
+    h->gs.kx0 = sl->kx0;
+  }
   cudaSetDevice(dev_prev);
   *out = h;
   return TBFP_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int tbfp_create(const tbfp_desc *d, tbfp_handle **out) { return create_impl(d, nullptr, out); }
+
+int tbfp_slab_create(const tbfp_desc *d, int nz_total, int k0, int kx0, int nkx_loc, tbfp_handle **out) {
+  const SlabSpec sl{nz_total, k0, kx0, nkx_loc};
+  return create_impl(d, &sl, out);
+}
+
+int tbfp_slab_forward_x(tbfp_handle *h, const double *s, double *spec_z) {
+  int rc = check_ptrs(h, {s, spec_z});
+  if (rc) return rc;
+  if (!h->slab) return set_err(h, TBFP_EINVAL, "tbfp_slab_forward_x: not a slab handle");
+  cudaSetDevice(h->device);
+  launch_fftx_fwd_from_s(s, h->Lpsi, h->g, h->d_twx, h->d_tpx, reinterpret_cast<double2 *>(spec_z), h->stream);
+  return finish(h, "tbfp_slab_forward_x");
+}
+
+int tbfp_slab_spectral(tbfp_handle *h, double *spec_x) {
+  int rc = check_ptrs(h, {spec_x});
+  if (rc) return rc;
+  if (!h->slab) return set_err(h, TBFP_EINVAL, "tbfp_slab_spectral: not a slab handle");
+  cudaSetDevice(h->device);
+  double2 *sp = reinterpret_cast<double2 *>(spec_x);
+  launch_fftz(sp, h->gs, h->d_tpz, false, h->stream);
+  launch_tridiag(sp, h->gs, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, h->stream);
+  launch_fftz(sp, h->gs, h->d_tpz, true, h->stream);
+  return finish(h, "tbfp_slab_spectral");
+}
+
+int tbfp_slab_inverse_x(tbfp_handle *h, const double *spec_z, double *psi) {
+  int rc = check_ptrs(h, {spec_z, psi});
+  if (rc) return rc;
+  if (!h->slab) return set_err(h, TBFP_EINVAL, "tbfp_slab_inverse_x: not a slab handle");
+  cudaSetDevice(h->device);
+  launch_fftx_inv(reinterpret_cast<const double2 *>(spec_z), psi, h->Lpsi, h->hd_psi, h->g, h->d_twx, h->d_tpx,
+                  h->scale, h->stream);
+  return finish(h, "tbfp_slab_inverse_x");
 }
 
 // ---------------------------------------------------------------------------
 int tbfp_solve_fps_dev(tbfp_handle *h, const double *s, double *psi) {
   int rc = check_ptrs(h, {s, psi});
   if (rc) return rc;
+  if (h->slab) return set_err(h, TBFP_EINVAL, "tbfp_solve_fps: a slab handle solves with tbfp_slab_*");
   cudaSetDevice(h->device);
   TBFP_CK(h, cudaEventRecord(h->ev0, h->stream));
   int iters = 1;
@@ -856,6 +932,7 @@ int tbfp_projection_dev(tbfp_handle *h, const double *ux_in, const double *uy_in
   int rc = check_ptrs(h, {ux_in, uy_in, uz_in, ux_out, uy_out, uz_out, rho, psi_n, psi_nm1, psi});
   if (rc) return rc;
   if ((rc = check_st(h, st_n, st_nm1))) return rc;
+  if (h->slab) return set_err(h, TBFP_EINVAL, "tbfp_projection: a slab handle solves with tbfp_slab_*");
   if (!(dt > 0.0) || !(alpha > 0.0) || !(rho0 > 0.0))
     return set_err(h, TBFP_EINVAL, "tbfp_projection: dt, alpha and rho0 must be positive");
   cudaSetDevice(h->device);

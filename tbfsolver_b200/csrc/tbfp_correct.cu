@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(128, 8) k_correct_div(CorrArgs a, GridK g, uns
   const int j0 = blockIdx.y * kJC + 1, j1 = min(j0 + kJC - 1, g.ny);
   const bool valid = i <= g.nx;
   const int ic = valid ? i : g.nx;  // clamped index keeps every load in bounds
-  const int km = (k == 1) ? g.nz : k - 1;
+  const int km = (k == 1 && !g.slab) ? g.nz : k - 1;
   // 32-bit element offsets (tbfp_create checks every array has < 2^31 elements)
   const int pjs = (int)a.Lpsi.sj, rjs = (int)a.Lrho.sj;
   const int xjs = (int)a.Lux.sj, yjs = (int)a.Luy.sj, zjs = (int)a.Luz.sj;
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(128, 8) k_correct_div(CorrArgs a, GridK g, uns
       if (i == g.nx) uxo[ox - ic] = uxp;  // ux(0, j, k)
       uyo[oy] = uyp;
       uzo[oz] = uzp;
-      if (k == g.nz) uzo[oz - k * (int)a.Luz.sk] = uzp;  // uz(i, j, 0)
+      if (k == g.nz && !g.slab) uzo[oz - k * (int)a.Luz.sk] = uzp;  // uz(i, j, 0)
       double dv = (uxp - uxm) * idx;
       dv = dv + (uyp - uym) * g.idyf[j - 1];
       dv = dv + (uzp - uzq) * idz;
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(128) k_correct_inplace(CorrArgs a, GridK g) {
   a.uxo[at(a.Lux, i, j, k)] = uxp;
   if (i == g.nx) a.uxo[at(a.Lux, 0, j, k)] = uxp;
   a.uzo[at(a.Luz, i, j, k)] = uzp;
-  if (k == g.nz) a.uzo[at(a.Luz, i, j, 0)] = uzp;
+  if (k == g.nz && !g.slab) a.uzo[at(a.Luz, i, j, 0)] = uzp;
 }
 
 void launch_correct_inplace(const CorrArgs &ca, bool has_st, const GridK &g, cudaStream_t st) {

@@ -24,12 +24,17 @@ __host__ __device__ __forceinline__ long at(const Lay &L, int i, int j, int k) {
 struct GridK {
   int nx, ny, nz, nkx, M;  // M = nx/2 (length of the half-length complex x transform)
   long R;                  // ny*nz: number of x rows
-  double idxf1, idzf1;     // 1/dxf(1), 1/dzf(1)
-  double idxc1, idzc1;     // 1/dxc(1), 1/dzc(1)
+  double idxf1, idzf1;     // 1/dxf(1), 1/dz_fft
+  double idxc1, idzc1;     // 1/dxc(1), 1/dz_fft
   const double *idyf;      // 1/dyf(j), j=1..ny
   const double *idyc;      // 1/dyc(j), j=1..ny+1
   const double *idxf;      // 1/dxf(i), i=1..nx
   const double *idzf;      // 1/dzf(k), k=1..nz
+  // slab form (one rank of a channel split over ranks): 0 for a whole channel.
+  // With slab = 1 the z neighbours of the first and last plane are the ghost
+  // planes the caller exchanged (no periodic wrap, no z ghost images written),
+  // and kx0 is the global index of the first local kx (spectral stage).
+  int slab, kx0;
 };
 
 // Inputs of the split right-hand side (poissonEqn.f90:193-305).

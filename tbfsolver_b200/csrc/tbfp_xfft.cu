@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_inv(const V *_
     const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
     // ghost images of the row: first y ghost layer (wall copy), periodic z
     const int jg = (j == 1) ? 0 : (j == g.ny ? g.ny + 1 : -1);
-    const int kg = (k <= hd) ? k + g.nz : (k > g.nz - hd ? k - g.nz : kNoGhost);
+    const int kg = g.slab ? kNoGhost : ((k <= hd) ? k + g.nz : (k > g.nz - hd ? k - g.nz : kNoGhost));
     double *p00 = psi + at(Lp, 0, j, k);
     double *p10 = (jg >= 0) ? psi + at(Lp, 0, jg, k) : nullptr;
     double *p01 = (kg != kNoGhost) ? psi + at(Lp, 0, j, kg) : nullptr;

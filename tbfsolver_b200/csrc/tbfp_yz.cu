@@ -145,8 +145,8 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
   }
   __syncwarp();
 
-  const double lam = lamx[kx] + lamz[kz];
-  const bool pin = (kx == 0 && kz == 0);
+  const double lam = lamx[kx + g.kx0] + lamz[kz];
+  const bool pin = (kx + g.kx0 == 0 && kz == 0);
   if (pin) {
     if (lane == 0) {
       double ct_p = 0.0;

@@ -65,47 +65,62 @@ def _real(t: torch.Tensor) -> torch.Tensor:
     return torch.view_as_real(t) if t.is_complex() else t
 
 
+def kx_send_chunks(sz: torch.Tensor, s: Slabs) -> list:
+    """S_z[nkx, nz_loc, ny] cut into the flat chunks for every destination rank
+    (destination q gets its kx range, all local k)."""
+    assert sz.shape[0] == s.nkx and sz.shape[1] == s.nz_loc
+    xr = _real(sz.contiguous())
+    return [xr[s.kxslab(q)[0]:s.kxslab(q)[0] + s.kxslab(q)[1]].reshape(-1) for q in range(s.world)]
+
+
+def kx_assemble(chunks: list, s: Slabs, ny: int, cplx: bool) -> torch.Tensor:
+    """S_x[nkx_loc, nz, ny] from the chunks received from every source rank."""
+    tail = (2,) if cplx else ()
+    out = torch.empty((s.nkx_loc, s.nz, ny) + tail, dtype=chunks[0].dtype, device=chunks[0].device)
+    for p, c in enumerate(chunks):
+        k0, nzp = s.zslab(p)
+        out[:, k0:k0 + nzp] = c.reshape((s.nkx_loc, nzp, ny) + tail)
+    return torch.view_as_complex(out) if cplx else out
+
+
+def z_send_chunks(sx: torch.Tensor, s: Slabs) -> list:
+    """S_x[nkx_loc, nz, ny] cut for every destination (its k range, local kx)."""
+    assert sx.shape[0] == s.nkx_loc and sx.shape[1] == s.nz
+    xr = _real(sx)
+    return [xr[:, s.zslab(q)[0]:s.zslab(q)[0] + s.zslab(q)[1]].reshape(-1) for q in range(s.world)]
+
+
+def z_assemble(chunks: list, s: Slabs, ny: int, cplx: bool) -> torch.Tensor:
+    """S_z[nkx, nz_loc, ny] from the chunks of every source (kx ranges in order)."""
+    out = torch.cat(chunks).reshape((s.nkx, s.nz_loc, ny) + ((2,) if cplx else ()))
+    return torch.view_as_complex(out) if cplx else out
+
+
+def _all_to_all(chunks: list, sizes_in: list, group) -> list:
+    send = torch.cat(chunks)
+    recv = torch.empty(sum(sizes_in), dtype=send.dtype, device=send.device)
+    dist.all_to_all_single(recv, send, sizes_in, [c.numel() for c in chunks], group=group)
+    return list(torch.split(recv, sizes_in))
+
+
 def to_kx_slabs(sz: torch.Tensor, s: Slabs, group=None) -> torch.Tensor:
     """S_z[nkx, nz_loc, ny] -> S_x[nkx_loc, nz, ny] (the first all-to-all of a solve)."""
-    assert sz.shape[0] == s.nkx and sz.shape[1] == s.nz_loc
     ny = sz.shape[2]
-    send = _real(sz.contiguous()).reshape(-1)
-    per_entry = send.numel() // (s.nkx * s.nz_loc * ny)  # 2 for complex
-    in_splits = [s.kxslab(q)[1] * s.nz_loc * ny * per_entry for q in range(s.world)]
-    out_splits = [s.nkx_loc * s.zslab(p)[1] * ny * per_entry for p in range(s.world)]
-    recv = torch.empty(sum(out_splits), dtype=send.dtype, device=send.device)
-    if s.world == 1:
-        recv.copy_(send)
-    else:
-        dist.all_to_all_single(recv, send, out_splits, in_splits, group=group)
-    out = torch.empty((s.nkx_loc, s.nz, ny) + ((2,) if sz.is_complex() else ()), dtype=send.dtype,
-                      device=send.device)
-    off = 0
-    for p in range(s.world):
-        k0, nzp = s.zslab(p)
-        blk = recv[off:off + out_splits[p]].reshape((s.nkx_loc, nzp, ny) + out.shape[3:])
-        out[:, k0:k0 + nzp] = blk
-        off += out_splits[p]
-    return torch.view_as_complex(out) if sz.is_complex() else out
+    chunks = kx_send_chunks(sz, s)
+    if s.world > 1:
+        per = 2 if sz.is_complex() else 1
+        chunks = _all_to_all(chunks, [s.nkx_loc * s.zslab(p)[1] * ny * per for p in range(s.world)], group)
+    return kx_assemble(chunks, s, ny, sz.is_complex())
 
 
 def to_z_slabs(sx: torch.Tensor, s: Slabs, group=None) -> torch.Tensor:
     """S_x[nkx_loc, nz, ny] -> S_z[nkx, nz_loc, ny] (the second all-to-all)."""
-    assert sx.shape[0] == s.nkx_loc and sx.shape[1] == s.nz
     ny = sx.shape[2]
-    xr = _real(sx)
-    per_entry = 2 if sx.is_complex() else 1
-    # pack for each destination q its k range, kx-major
-    send = torch.cat([xr[:, s.zslab(q)[0]:s.zslab(q)[0] + s.zslab(q)[1]].reshape(-1) for q in range(s.world)])
-    in_splits = [s.nkx_loc * s.zslab(q)[1] * ny * per_entry for q in range(s.world)]
-    out_splits = [s.kxslab(p)[1] * s.nz_loc * ny * per_entry for p in range(s.world)]
-    recv = torch.empty(sum(out_splits), dtype=send.dtype, device=send.device)
-    if s.world == 1:
-        recv.copy_(send)
-    else:
-        dist.all_to_all_single(recv, send, out_splits, in_splits, group=group)
-    out = recv.reshape((s.nkx, s.nz_loc, ny) + ((2,) if sx.is_complex() else ()))
-    return torch.view_as_complex(out) if sx.is_complex() else out
+    chunks = z_send_chunks(sx, s)
+    if s.world > 1:
+        per = 2 if sx.is_complex() else 1
+        chunks = _all_to_all(chunks, [s.kxslab(p)[1] * s.nz_loc * ny * per for p in range(s.world)], group)
+    return z_assemble(chunks, s, ny, sx.is_complex())
 
 
 def exchange_z_ghosts(f: torch.Tensor, s: Slabs, hd: int, group=None) -> None:
@@ -147,3 +162,85 @@ def max_over_ranks(x: float, device="cpu", group=None) -> float:
 def rank_seed(seed: int, rank: int) -> int:
     """Seed of a rank's own channel (replicas): independent inputs per GPU."""
     return seed + rank
+
+
+def exchange_z_ghosts_local(fields: list, slabs: list, hd: int) -> None:
+    """The ghost exchange of exchange_z_ghosts for several ranks held by one
+    process (fields[r] is rank r's slab): the same planes move, by copies."""
+    P = len(fields)
+    lows = [f[hd:2 * hd].clone() for f in fields]
+    highs = [f[s.nz_loc:s.nz_loc + hd].clone() for f, s in zip(fields, slabs)]
+    for r, (f, s) in enumerate(zip(fields, slabs)):
+        f[0:hd] = highs[(r - 1) % P]
+        f[s.nz_loc + hd:s.nz_loc + 2 * hd] = lows[(r + 1) % P]
+
+
+def all_to_all_local(sends: list) -> list:
+    """sends[p][q] -> recv[q][p] for several ranks held by one process."""
+    P = len(sends)
+    return [[sends[p][q] for p in range(P)] for q in range(P)]
+
+
+class SlabChannel:
+    """One rank's share of a channel split over ranks (tbfp_slab_*): solveFPS on
+    z slabs / kx slabs with the two all-to-alls and the ghost exchange of this
+    module.  The local arrays use the single-channel layout of the slab
+    (nz_loc planes plus halos)."""
+
+    def __init__(self, mesh, world: int, rank: int, hd_psi: int = 1, hd_u: int = 2, hd_rho: int = 1,
+                 device: int = -1):
+        import ctypes as C
+
+        import numpy as np
+
+        from ._native import TbfpDesc, check, load
+        from .solver import _dptr
+
+        self.lib = load()
+        self.mesh, self.world, self.rank = mesh, world, rank
+        self.s = s = Slabs(mesh.nx, mesh.ny, mesh.nz, world, rank)
+        self.hd_psi, self.hd_u, self.hd_rho = hd_psi, hd_u, hd_rho
+        nx, ny = mesh.nx, mesh.ny
+        k0, nzl = s.k0, s.nz_loc
+        self._m = {
+            "dxf": np.ascontiguousarray(mesh.dxf.r(1, nx)), "dxc": np.ascontiguousarray(mesh.dxc.r(1, nx + 1)),
+            "dyf": np.ascontiguousarray(mesh.dyf.r(1, ny)), "dyc": np.ascontiguousarray(mesh.dyc.r(1, ny + 1)),
+            "dzf": np.ascontiguousarray(mesh.dzf.r(k0 + 1, k0 + nzl)),
+            "dzc": np.ascontiguousarray(mesh.dzc.r(k0 + 1, k0 + nzl + 1)),
+        }
+        m = self._m
+        d = TbfpDesc(nx=nx, ny=ny, nz=nzl, hd_psi=hd_psi, hd_u=hd_u, hd_rho=hd_rho, hd_st=1, dx_fft=mesh.dx_fft,
+                     dz_fft=mesh.dz_fft, dxf=_dptr(m["dxf"]), dxc=_dptr(m["dxc"]), dyf=_dptr(m["dyf"]),
+                     dyc=_dptr(m["dyc"]), dzf=_dptr(m["dzf"]), dzc=_dptr(m["dzc"]), s_Vg=mesh.s_Vg, precision=0,
+                     tol=1e-10, max_iter=1, device=device, stream=None, flags=0)
+        h = C.c_void_p()
+        check(self.lib.tbfp_slab_create(C.byref(d), mesh.nz, k0, s.kx0, s.nkx_loc, C.byref(h)), None)
+        self.h = h
+        dev = torch.device("cuda", torch.cuda.current_device() if device < 0 else device)
+        self.spec_z = torch.empty((s.nkx, nzl, ny), dtype=torch.complex128, device=dev)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.tbfp_destroy(self.h)
+            self.h = None
+
+    def forward_x(self, s_field) -> torch.Tensor:
+        from ._native import check
+        check(self.lib.tbfp_slab_forward_x(self.h, s_field.address(), self.spec_z.data_ptr()), self.h)
+        return self.spec_z
+
+    def spectral(self, spec_x: torch.Tensor) -> None:
+        from ._native import check
+        check(self.lib.tbfp_slab_spectral(self.h, spec_x.data_ptr()), self.h)
+
+    def inverse_x(self, spec_z: torch.Tensor, psi) -> None:
+        from ._native import check
+        check(self.lib.tbfp_slab_inverse_x(self.h, spec_z.contiguous().data_ptr(), psi.address()), self.h)
+
+    def solve_fps(self, psi, s_field, group=None) -> None:
+        """solveFPS on this rank's slab (a collective: every rank calls it)."""
+        sz = self.forward_x(s_field)
+        sx = to_kx_slabs(sz, self.s, group).contiguous()
+        self.spectral(sx)
+        self.inverse_x(to_z_slabs(sx, self.s, group), psi)
+        exchange_z_ghosts(psi.a, self.s, self.hd_psi, group)
