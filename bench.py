@@ -509,7 +509,7 @@ def main():
         "step_roofline": {"b_alg_bytes": ab["b_alg"], "achieved": ab["b_alg"] / (ms * 1e-3) / 1e9,
                           "frac": ab["b_alg"] / (ms * 1e-3) / 1e9 / pk},
         "stages": stages,
-        "gpu_launches": 7 * args.steps,
+        "gpu_launches": 8 * args.steps,  # recip, rhs, x fwd, z fwd, y solve, z inv, x inv, correct
         "clocks": clocks,
         "cpu_baseline": cpu,
     }

@@ -92,6 +92,14 @@ inline bool fft_length_supported(int n) {
 }
 
 // --- tile geometry (shared by the host launchers and the kernels) -----------
+// Asynchronous 16-byte copy global -> shared (cp.async, no register staging):
+// a thread issues all its copies back to back and waits once.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 constexpr int kNT = 256;  // threads per CTA of the transform kernels (8 warps)
 constexpr int kNW = kNT / 32;
 constexpr int kWPB = 4;   // warps per CTA of the tridiagonal kernel

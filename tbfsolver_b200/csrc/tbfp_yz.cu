@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
                                                        const double *__restrict__ am, const double *__restrict__ ap,
                                                        const double *__restrict__ dyf, double mean_c, double nxnz,
                                                        int T, unsigned magicT) {
-  extern __shared__ unsigned char smraw[];
+  extern __shared__ __align__(16) unsigned char smraw[];
   const int ny = g.ny, nz = g.nz;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int W = 33 * T;
@@ -138,10 +138,21 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
     const int l = (T == 1) ? e : (int)__umulhi((unsigned)e, magicT);
     return (e - l * T) * 33 + l;
   };
-  for (int e = lane; e < ny; e += 32) {
-    const int sl = slot(e);
-    d0[sl] = ld(S0[e]);
-    if (two) d1[sl] = ld(S1[e]);
+  if constexpr (sizeof(V) == sizeof(double2)) {
+    // all of the lane's rows in flight at once
+    for (int e = lane; e < ny; e += 32) {
+      const int sl = slot(e);
+      cp_async16(d0 + sl, S0 + e);
+      if (two) cp_async16(d1 + sl, S1 + e);
+    }
+    cp_async_wait_all();
+  } else {
+#pragma unroll 4
+    for (int e = lane; e < ny; e += 32) {
+      const int sl = slot(e);
+      d0[sl] = ld(S0[e]);
+      if (two) d1[sl] = ld(S1[e]);
+    }
   }
   __syncwarp();
 
