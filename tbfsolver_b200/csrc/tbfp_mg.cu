@@ -104,33 +104,36 @@ __device__ __forceinline__ void block_sum2(double a, double b, double *out_a, do
 // One colour of iterateGS (rbgs.f90:215-250): cells with (i+j+k) mod 2 == colour
 // (1-based indices, red = 0) take p = (-q + sum a_nb p_nb) / sum a_nb.
 // ---------------------------------------------------------------------------
+// sum: when not NULL, the sum of the updated cells is added to *sum (the last
+// red and black sweeps of a smoothing call give sum(p) for correctFullNeumann
+// without another pass).  A wall cell's clamped y neighbour is the cell
+// itself, so a sweep also reads cells of its own colour there.
 __global__ void __launch_bounds__(kWalkX) k_rbgs_colour(MgLev L, float *__restrict__ p,
                                                        const float *__restrict__ q,
-                                                       const float *__restrict__ beta, int colour) {
+                                                       const float *__restrict__ beta, int colour,
+                                                       double *__restrict__ sum) {
   const Walk w = walk(L.ny);
   const int nx = L.nx, ny = L.ny, nz = L.nz, k = w.k;
-  if (w.i >= (nx + 1) / 2) return;  // no block-level barrier in this kernel
-  for (int j = w.j0; j < w.j1; ++j) {
-    // colour of 1-based (i+1, j+1, k+1) is (i + j + k + 3) mod 2, so the row's
-    // first 0-based index of this colour is (colour + j + k + 1) mod 2
-    const int ii = 2 * w.i + ((colour + j + k + 1) & 1);
-    if (ii >= nx) continue;
-    auto at3 = [&](int a, int b, int c) { return (c * ny + b) * nx + a; };
-    const Coef<float> c = coef<float>(L, beta, ii, j, k);
-    const float den = c.aR + c.aL + c.aT + c.aB + c.aF + c.aK;
-    const float pR = p[at3(wrap(ii + 1, nx), j, k)], pL = p[at3(wrap(ii - 1, nx), j, k)];
-    const float pT = p[at3(ii, clampi(j + 1, ny), k)], pB = p[at3(ii, clampi(j - 1, ny), k)];
-    const float pF = p[at3(ii, j, wrap(k + 1, nz))], pK = p[at3(ii, j, wrap(k - 1, nz))];
-    p[at3(ii, j, k)] =
-        (-q[at3(ii, j, k)] + (c.aR * pR + c.aL * pL) + (c.aT * pT + c.aB * pB) + (c.aF * pF + c.aK * pK)) / den;
+  double acc = 0.0;
+  if (w.i < (nx + 1) / 2) {
+    for (int j = w.j0; j < w.j1; ++j) {
+      // colour of 1-based (i+1, j+1, k+1) is (i + j + k + 3) mod 2, so the row's
+      // first 0-based index of this colour is (colour + j + k + 1) mod 2
+      const int ii = 2 * w.i + ((colour + j + k + 1) & 1);
+      if (ii >= nx) continue;
+      auto at3 = [&](int a, int b, int c) { return (c * ny + b) * nx + a; };
+      const Coef<float> c = coef<float>(L, beta, ii, j, k);
+      const float den = c.aR + c.aL + c.aT + c.aB + c.aF + c.aK;
+      const float pR = p[at3(wrap(ii + 1, nx), j, k)], pL = p[at3(wrap(ii - 1, nx), j, k)];
+      const float pT = p[at3(ii, clampi(j + 1, ny), k)], pB = p[at3(ii, clampi(j - 1, ny), k)];
+      const float pF = p[at3(ii, j, wrap(k + 1, nz))], pK = p[at3(ii, j, wrap(k - 1, nz))];
+      const float v =
+          (-q[at3(ii, j, k)] + (c.aR * pR + c.aL * pL) + (c.aT * pT + c.aB * pB) + (c.aF * pF + c.aK * pK)) / den;
+      p[at3(ii, j, k)] = v;
+      acc += v;
+    }
   }
-}
-
-// interior sum of p (the average of correctFullNeumann, rbgs.f90:403-446)
-__global__ void __launch_bounds__(kMgThreads) k_sum(const float *__restrict__ p, long n, double *__restrict__ out) {
-  double s = 0.0;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) s += p[t];
-  block_sum2(s, 0.0, out, nullptr);
+  if (sum) block_sum2(acc, 0.0, sum, nullptr);  // sum is uniform over the grid
 }
 
 // p -= sum/n (correctFullNeumann, rbgs.f90:403-446)
@@ -194,11 +197,18 @@ __global__ void __launch_bounds__(kMgThreads) k_restrict(MgLev F, MgLev C, const
 // prolongationOp3D (interpolation.f90:129-181): fine += trilinear interpolation
 // between coarse centroids ih = i/2 and ih+1 (1-based, the coarse ghosts read
 // through wrapped / clamped indices).
+// The means left by the smoothing calls (correctFullNeumann) are removed here:
+// fsum/finv the fine level's pre-smoothing sum and 1/cells, csum/cinv the
+// coarse level's post-smoothing sum (NULL: nothing pending); the weights sum
+// to 1, so interpolating p - mean subtracts the mean.
 __global__ void __launch_bounds__(kMgThreads) k_prolong_add(MgLev F, MgLev C, const float *__restrict__ coarse,
-                                                           float *__restrict__ fine) {
+                                                           float *__restrict__ fine, const double *__restrict__ fsum,
+                                                           double finv, const double *__restrict__ csum,
+                                                           double cinv) {
   const Walk w = walk(F.ny);
   const int i = w.i, k = w.k;
   if (i >= F.nx) return;  // no block-level barrier in this kernel
+  const float mf = fsum ? (float)(*fsum * finv) : 0.0f, mc = csum ? (float)(*csum * cinv) : 0.0f;
   // 1-based fine index i+1 -> ih = (i+1)/2, coarse 0-based ih-1 and ih
   const int ih = (i + 1) / 2 - 1, kh = (k + 1) / 2 - 1;
   const int xa = wrap(ih, C.nx), xb = wrap(ih + 1, C.nx);
@@ -218,7 +228,8 @@ __global__ void __launch_bounds__(kMgThreads) k_prolong_add(MgLev F, MgLev C, co
     s += (x1 * y0) * z1 * c(xb, ya, zb);
     s += (x0 * y1) * z1 * c(xa, yb, zb);
     s += (x1 * y1) * z1 * c(xb, yb, zb);
-    fine[(k * F.ny + j) * F.nx + i] += s;
+    const int t = (k * F.ny + j) * F.nx + i;
+    fine[t] = (fine[t] - mf) + (s - mc);
   }
 }
 
@@ -230,21 +241,33 @@ __global__ void k_fill(float *__restrict__ p, long n, float v) {
 // Coarsest level (solveMat, poissMat.f90:289-312): the system V*(-L) p = -V*s
 // with Neumann walls, bordered by the Lagrange row sum(p) = 0, in FP64.  The
 // bordered matrix depends only on beta, so it is inverted once per PCG solve
-// (Gauss-Jordan with partial pivoting, one CTA) and every V-cycle applies the
-// inverse (the reference refactorises with MUMPS on every call; the result is
-// the same linear solve).
+// and every V-cycle applies the inverse (the reference refactorises with MUMPS
+// on every call; the result is the same linear solve).
+//
+// Inversion: blocked Gauss-Jordan on [K | I] without pivoting, in the order
+// cells 0..n-2, border, cell n-1 (unknowns n-1 and n swapped).  K's cell block
+// A = V*(-L) is an irreducible singular M-matrix, so its proper leading
+// submatrices are nonsingular M-matrices, the bordered leading block
+// [A_11 1; 1^T 0] is nonsingular (1^T A_11^-1 1 > 0) and so is K: every
+// leading minor of the reordered matrix is nonzero and elimination needs no
+// row exchanges.  Panels of kGB columns: one CTA inverts the panel's diagonal
+// block and scales the panel rows by it; the other rows take the rank-kGB
+// update from many CTAs.
 // ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ int coarse_perm(int x, int n) { return x == n - 1 ? n : (x == n ? n - 1 : x); }
+
 __global__ void k_coarse_assemble(MgLev L, const float *__restrict__ beta, double *__restrict__ M, int n1) {
   const int n = n1 - 1;
   const int ld = 2 * n1;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < (long)n1 * ld; e += (long)gridDim.x * blockDim.x)
     M[e] = 0.0;
   __syncthreads();  // one CTA
-  for (int r = threadIdx.x; r < n; r += blockDim.x) {
-    const int i = r % L.nx, j = (r / L.nx) % L.ny, k = r / (L.nx * L.ny);
+  for (int r0 = threadIdx.x; r0 < n; r0 += blockDim.x) {
+    const int r = coarse_perm(r0, n);
+    const int i = r0 % L.nx, j = (r0 / L.nx) % L.ny, k = r0 / (L.nx * L.ny);
     const Coef<double> c = coef<double>(L, beta, i, j, k);
     const double V = (double)L.vx[i] * (double)L.vy[j] * (double)L.vz[k];
-    auto idx = [&](int a, int b, int cc) { return (cc * L.ny + b) * L.nx + a; };
+    auto idx = [&](int a, int b, int cc) { return coarse_perm((cc * L.ny + b) * L.nx + a, n); };
     double diag = 0.0;
     auto term = [&](double a, int col) {
       M[(long)r * ld + col] -= V * a;
@@ -257,96 +280,110 @@ __global__ void k_coarse_assemble(MgLev L, const float *__restrict__ beta, doubl
     if (j < L.ny - 1) term(c.aT, idx(i, j + 1, k));
     if (j > 0) term(c.aB, idx(i, j - 1, k));
     M[(long)r * ld + r] += diag;
-    M[(long)r * ld + n] = 1.0;
-    M[(long)n * ld + r] = 1.0;
+    const int bdr = coarse_perm(n, n);
+    M[(long)r * ld + bdr] = 1.0;
+    M[(long)bdr * ld + r] = 1.0;
   }
   __syncthreads();
-  for (int r = threadIdx.x; r < n1; r += blockDim.x) M[(long)r * ld + n1 + r] = 1.0;  // [A | I]
+  for (int r = threadIdx.x; r < n1; r += blockDim.x) M[(long)r * ld + n1 + r] = 1.0;  // [K | I]
 }
 
-__global__ void __launch_bounds__(1024) k_gauss_jordan(double *__restrict__ M, int n1, int *__restrict__ fail) {
-  const int ld = 2 * n1;
-  extern __shared__ double gj_smem[];
-  double *fac = gj_smem;        // n1 row factors of the current column
-  double *prow = gj_smem + n1;  // the scaled pivot row (2*n1)
-  __shared__ double bestv[32];
-  __shared__ int besti[32];
-  __shared__ int piv;
-  for (int kcol = 0; kcol < n1; ++kcol) {
-    // pivot: max |M[r][kcol]|, r >= kcol
-    double bv = -1.0;
-    int bi = kcol;
-    for (int r = kcol + threadIdx.x; r < n1; r += blockDim.x) {
-      const double v = fabs(M[(long)r * ld + kcol]);
-      if (v > bv) {
-        bv = v;
-        bi = r;
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ov > bv || (ov == bv && oi < bi)) {
-        bv = ov;
-        bi = oi;
-      }
-    }
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-      bestv[w] = bv;
-      besti[w] = bi;
-    }
+constexpr int kGB = 32;     // panel width
+constexpr int kGPT = 256;   // threads of the panel kernel
+// Rows p0 .. p0+pb-1 of [K | I]: D = K[p0.., p0..] is inverted in shared memory
+// (Gauss-Jordan, no exchanges), the panel rows become D^-1 times themselves
+// (columns p0.. on; the columns before p0 are already unit vectors), and the
+// panel's column block of every row is saved in Cb (the update's multipliers).
+__global__ void __launch_bounds__(kGPT) k_gj_panel(double *__restrict__ M, int n1, int p0, double *__restrict__ Cb,
+                                                  int *__restrict__ fail) {
+  const int ld = 2 * n1, pb = min(kGB, n1 - p0), tid = threadIdx.x;
+  __shared__ double A[kGB][2 * kGB + 1];
+  for (int e = tid; e < kGB * 2 * kGB; e += kGPT) {
+    const int r = e / (2 * kGB), c = e % (2 * kGB);
+    double v = 0.0;
+    if (r < pb && c < pb) v = M[(long)(p0 + r) * ld + p0 + c];
+    else if (c >= kGB) v = (c - kGB == r) ? 1.0 : 0.0;
+    else if (r >= pb && c == r) v = 1.0;  // unused rows of a short last panel
+    A[r][c] = v;
+  }
+  for (long e = tid; e < (long)n1 * pb; e += kGPT) {
+    const int r = (int)(e / pb), t = (int)(e % pb);
+    Cb[(long)r * kGB + t] = M[(long)r * ld + p0 + t];
+  }
+  __shared__ double fcol[kGB];
+  __syncthreads();
+  for (int k = 0; k < kGB; ++k) {
+    const double piv = A[k][k];
+    __syncthreads();  // every thread has read the pivot before row k is scaled
+    if (tid == 0 && !(fabs(piv) > 0.0 && fabs(piv) < 1e300)) *fail = 1;
+    const double ip = 1.0 / piv;
+    for (int c = tid; c < 2 * kGB; c += kGPT) A[k][c] *= ip;
+    for (int r = tid; r < kGB; r += kGPT) fcol[r] = A[r][k];  // row k's own entry is not used
     __syncthreads();
-    if (threadIdx.x == 0) {
-      double v = -1.0;
-      int b = kcol;
-      for (int q = 0; q < (int)(blockDim.x >> 5); ++q)
-        if (bestv[q] > v) {
-          v = bestv[q];
-          b = besti[q];
-        }
-      piv = b;
-      if (!(v > 0.0)) *fail = 1;
-    }
-    __syncthreads();
-    const int p = piv;
-    if (p != kcol)
-      for (int c = kcol + threadIdx.x; c < ld; c += blockDim.x) {
-        const double a = M[(long)kcol * ld + c];
-        M[(long)kcol * ld + c] = M[(long)p * ld + c];
-        M[(long)p * ld + c] = a;
-      }
-    __syncthreads();
-    const double inv = 1.0 / M[(long)kcol * ld + kcol];
-    for (int r = threadIdx.x; r < n1; r += blockDim.x) fac[r] = M[(long)r * ld + kcol];
-    for (int c = kcol + threadIdx.x; c < ld; c += blockDim.x) prow[c] = M[(long)kcol * ld + c] * inv;
-    __syncthreads();
-    for (int c = kcol + threadIdx.x; c < ld; c += blockDim.x) M[(long)kcol * ld + c] = prow[c];
-    // eliminate column kcol from the other rows: one warp per row, rows whose
-    // factor is zero (most of them early on: the matrix is a 7-point stencil) skipped
-    const int nw = (int)(blockDim.x >> 5);
-    for (int r = w; r < n1; r += nw) {
-      const double f = fac[r];
-      if (r == kcol || f == 0.0) continue;
-      double *row = M + (long)r * ld;
-#pragma unroll 8
-      for (int c = kcol + l; c < ld; c += 32) row[c] -= f * prow[c];
+    for (int e = tid; e < kGB * 2 * kGB; e += kGPT) {
+      const int r = e / (2 * kGB), c = e % (2 * kGB);
+      if (r != k) A[r][c] -= fcol[r] * A[k][c];
     }
     __syncthreads();
   }
+  // panel rows, column by column (each thread owns columns): R = D^-1 * rows
+  for (int c = p0 + tid; c < ld; c += kGPT) {
+    double x[kGB];
+#pragma unroll
+    for (int s = 0; s < kGB; ++s) x[s] = s < pb ? M[(long)(p0 + s) * ld + c] : 0.0;
+    for (int t = 0; t < pb; ++t) {
+      double y = 0.0;
+#pragma unroll
+      for (int s = 0; s < kGB; ++s) y += A[t][kGB + s] * x[s];
+      M[(long)(p0 + t) * ld + c] = y;
+    }
+  }
 }
 
-// p = A^-1 (-V s) on the coarsest level (the Lagrange row's right-hand side is 0)
+// Rows outside the panel: M[r][c] -= sum_t Cb[r][t] * M[p0+t][c], c >= p0.
+// CTA tile: 32 rows x 128 columns; thread = one column, 16 rows.
+__global__ void __launch_bounds__(256) k_gj_update(double *__restrict__ M, int n1, int p0,
+                                                   const double *__restrict__ Cb) {
+  const int ld = 2 * n1, pb = min(kGB, n1 - p0);
+  const int r0 = blockIdx.y * 32, c0 = p0 + blockIdx.x * 128;
+  __shared__ double Ct[32][kGB + 1];
+  __shared__ double Rt[kGB][128];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < 32 * kGB; e += 256) {
+    const int r = e / kGB, t = e % kGB;
+    Ct[r][t] = (r0 + r < n1 && t < pb) ? Cb[(long)(r0 + r) * kGB + t] : 0.0;
+  }
+  for (int e = tid; e < kGB * 128; e += 256) {
+    const int t = e / 128, c = e % 128;
+    Rt[t][c] = (t < pb && c0 + c < ld) ? M[(long)(p0 + t) * ld + c0 + c] : 0.0;
+  }
+  __syncthreads();
+  const int c = tid & 127, rh = (tid >> 7) * 16;
+  if (c0 + c >= ld) return;  // no barrier follows
+#pragma unroll 1
+  for (int rr = 0; rr < 16; ++rr) {
+    const int r = r0 + rh + rr;
+    if (r >= n1 || (r >= p0 && r < p0 + pb)) continue;
+    double acc = 0.0;
+#pragma unroll
+    for (int t = 0; t < kGB; ++t) acc += Ct[rh + rr][t] * Rt[t][c];
+    M[(long)r * ld + c0 + c] -= acc;
+  }
+}
+
+// p = K^-1 (-V s) on the coarsest level (the Lagrange row's right-hand side is
+// 0); the inverse is stored in the reordered basis.
 __global__ void k_coarse_apply(MgLev L, const double *__restrict__ M, int n1, const float *__restrict__ s,
                                float *__restrict__ p) {
   const int n = n1 - 1, ld = 2 * n1;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= n) return;
+  const long row = (long)coarse_perm(warp, n) * ld + n1;
   double acc = 0.0;
   for (int c = lane; c < n; c += 32) {
     const int i = c % L.nx, j = (c / L.nx) % L.ny, k = c / (L.nx * L.ny);
     const double V = (double)L.vx[i] * (double)L.vy[j] * (double)L.vz[k];
-    acc += M[(long)warp * ld + n1 + c] * (-V * (double)s[c]);
+    acc += M[row + coarse_perm(c, n)] * (-V * (double)s[c]);
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if (lane == 0) p[warp] = (float)acc;
@@ -496,7 +533,6 @@ __global__ void k_psi_ghosts(double *__restrict__ psi, Lay Lp, int hd, int nx, i
   }
 }
 
-unsigned nblk(long n) { return (unsigned)((n + kMgThreads - 1) / kMgThreads); }
 dim3 wgrid(int nxe, int ny, int nz, int J) {
   return dim3((unsigned)((nxe + kWalkX - 1) / kWalkX), (unsigned)((ny + J - 1) / J), (unsigned)nz);
 }
@@ -581,6 +617,8 @@ struct MgSolver::Impl {
   double *r = nullptr, *d = nullptr, *qv = nullptr, *sc = nullptr;  // sc: scalars and norms
   float *r32 = nullptr;
   double *Minv = nullptr;
+  double *Cb = nullptr;  // multipliers of one Gauss-Jordan panel (n1 x kGB)
+  double *msum = nullptr;  // per level: pending sums of p after pre- and post-smoothing
   int n1 = 0;
   int *fail = nullptr;
   std::vector<void *> allocs;
@@ -765,7 +803,8 @@ int MgSolver::init(const tbfp_mg_params &prm, int nx, int ny, int nz, const doub
   ck(m.alloc(&m.r32, m.n));
   ck(m.alloc(&m.sc, 16));
   ck(m.alloc(&m.Minv, (size_t)m.n1 * 2 * m.n1));
-  ck(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * m.n1 * (int)sizeof(double)));
+  ck(m.alloc(&m.Cb, (size_t)m.n1 * kGB));
+  ck(m.alloc(&m.msum, 2 * m.lv.size()));
   ck(m.alloc(&m.fail, 1));
   if (e != cudaSuccess) {
     *err = std::string("tbfp_pcg_setup: ") + cudaGetErrorString(e);
@@ -775,7 +814,7 @@ int MgSolver::init(const tbfp_mg_params &prm, int nx, int ny, int nz, const doub
 }
 
 // sc layout: [0] deltaN, [1] d.qv, [2] deltaN_new, [3] deltaN_old, [4] sum q^2, [5] sum r^2,
-//            [6] MG residual sum res^2, [7] MG sum q^2, [8] mean sum
+//            [6] MG residual sum res^2, [7] MG sum q^2
 namespace {
 struct Run {
   MgSolver::Impl &m;
@@ -786,33 +825,45 @@ struct Run {
   // with adding a constant to p (the update is an average of neighbours, q
   // fixed), so removing the mean once after the last iteration gives the same
   // p.
-  void rbgs(int l, int n_iter, bool reset) {
+  // The mean of p is not removed in a separate pass: the last red and black
+  // sweeps of a smoothing call add sum(p) into `slot`, and the kernel that
+  // next combines p with another level (k_prolong_add) subtracts it; the
+  // residual in between does not need it (L p ignores constants).  Returns
+  // whether a sum is pending in `slot`.  With reset, p starts from 0.
+  bool rbgs(int l, int n_iter, bool reset, double *slot) {
     auto &L = m.lv[l];
     if (reset) k_fill<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, 0.0f);
-    if (n_iter == 0) return;
+    if (n_iter == 0) return false;
     for (int it = 0; it < n_iter; ++it) {
-      k_rbgs_colour<<<wgrid((L.nx + 1) / 2, L.ny, L.nz, 1), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, 0);
-      k_rbgs_colour<<<wgrid((L.nx + 1) / 2, L.ny, L.nz, 1), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, 1);
+      const bool last = it == n_iter - 1;
+      const int J = last ? kMgJ : 1;
+      double *sum = last ? slot : nullptr;
+      k_rbgs_colour<<<wgrid((L.nx + 1) / 2, L.ny, L.nz, J), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, 0, sum);
+      k_rbgs_colour<<<wgrid((L.nx + 1) / 2, L.ny, L.nz, J), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, 1, sum);
     }
-    cudaMemsetAsync(m.sc + 8, 0, sizeof(double), st);
-    k_sum<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, m.sc + 8);
-    k_sub_mean<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, m.sc + 8);
+    return true;
   }
 
   void vcycle(int l) {
     const int last = (int)m.lv.size() - 1;
     auto &L = m.lv[l];
+    if (l == 0) cudaMemsetAsync(m.msum, 0, 2 * m.lv.size() * sizeof(double), st);
     if (l == last) {
       k_coarse_apply<<<(unsigned)((L.n * 32 + 255) / 256), 256, 0, st>>>(L.L, m.Minv, m.n1, L.q, L.p);
-      return;
+      return;  // the bordered solve gives sum(p) = 0: nothing pending
     }
-    rbgs(l, m.prm.n_pre, l != 0);
+    double *pre = m.msum + 2 * l, *post = m.msum + 2 * l + 1;
+    const bool hpre = rbgs(l, m.prm.n_pre, l != 0, pre);
     k_mg_residual<<<wgrid(L.nx, L.ny, L.nz, 1), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, L.res, nullptr);
     auto &C = m.lv[l + 1];
     k_restrict<<<wgrid(C.nx, C.ny, C.nz, 1), kWalkX, 0, st>>>(L.L, C.L, L.res, C.q);
     vcycle(l + 1);
-    k_prolong_add<<<wgrid(L.nx, L.ny, L.nz, 1), kWalkX, 0, st>>>(L.L, C.L, C.p, L.p);
-    rbgs(l, m.prm.n_post, false);
+    const bool hcpost = l + 1 < last && m.prm.n_post > 0;
+    k_prolong_add<<<wgrid(L.nx, L.ny, L.nz, 1), kWalkX, 0, st>>>(
+        L.L, C.L, C.p, L.p, hpre ? pre : nullptr, 1.0 / (double)L.n, hcpost ? m.msum + 2 * (l + 1) + 1 : nullptr,
+        1.0 / (double)C.n);
+    const bool hpost = rbgs(l, m.prm.n_post, false, post);
+    if (l == 0 && hpost) k_sub_mean<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, post);
   }
 
   // ||q - L p|| / ||q|| at the finest level (computeResiduals' res)
@@ -893,7 +944,11 @@ int MgSolver::solve(double *psi, Lay Lp, int hd_psi, const double *beta, Lay Lb,
   auto &C = m.lv.back();
   cudaMemsetAsync(m.fail, 0, sizeof(int), st);
   k_coarse_assemble<<<1, 1024, 0, st>>>(C.L, C.beta, m.Minv, m.n1);
-  k_gauss_jordan<<<1, 1024, 3 * m.n1 * sizeof(double), st>>>(m.Minv, m.n1, m.fail);
+  for (int p0 = 0; p0 < m.n1; p0 += kGB) {
+    k_gj_panel<<<1, kGPT, 0, st>>>(m.Minv, m.n1, p0, m.Cb, m.fail);
+    const dim3 ug((unsigned)((2 * m.n1 - p0 + 127) / 128), (unsigned)((m.n1 + 31) / 32));
+    k_gj_update<<<ug, 256, 0, st>>>(m.Minv, m.n1, p0, m.Cb);
+  }
   // r = q - L psi (psi: the initial guess), z = MG(r), d = z
   cudaMemsetAsync(m.sc, 0, 16 * sizeof(double), st);
   k_pcg_init<<<wgrid(m.nx, m.ny, m.nz, kMgJ), kWalkX, 0, st>>>(F, psi, Lp, q, Lq, m.r, m.lv[0].q, m.sc + 4);
