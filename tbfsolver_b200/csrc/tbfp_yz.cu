@@ -106,7 +106,11 @@ void launch_fftz(float2 *spec, const GridK &g, const float2 *tpz, bool inverse, 
 __device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 
-template <typename V>
+// TM > 0: every lane holds at most TM rows and keeps their elimination
+// coefficients at_i, ct_i in registers (shared memory holds only the two
+// right-hand sides, so more warps fit per SM); TM = 0: any T, coefficients in
+// shared memory.
+template <typename V, int TM>
 __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, GridK g,
                                                        const double *__restrict__ lamx,
                                                        const double *__restrict__ lamz,
@@ -119,8 +123,11 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
   const int W = 33 * T;
   double2 *d0 = reinterpret_cast<double2 *>(smraw) + warp * 2 * W;
   double2 *d1 = d0 + W;
-  double *ca = reinterpret_cast<double *>(reinterpret_cast<double2 *>(smraw) + kWPB * 2 * W) + warp * 2 * W;
-  double *cc = ca + W;
+  double *ca = nullptr, *cc = nullptr;
+  if constexpr (TM == 0) {
+    ca = reinterpret_cast<double *>(reinterpret_cast<double2 *>(smraw) + kWPB * 2 * W) + warp * 2 * W;
+    cc = ca + W;
+  }
   const int nzh = nz / 2 + 1;  // kz = 0..nz/2 (nz is even)
   const unsigned q = blockIdx.x * kWPB + warp;
   if (q >= (unsigned)(g.nkx * nzh)) return;  // whole warp leaves; no block-level barrier follows
@@ -159,6 +166,8 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
   const double lam = lamx[kx + g.kx0] + lamz[kz];
   const bool pin = (kx + g.kx0 == 0 && kz == 0);
   if (pin) {
+    // single system: its factors c_j go where the partner's right-hand side would be
+    double *cpin = (TM == 0) ? cc : reinterpret_cast<double *>(d1);
     if (lane == 0) {
       double ct_p = 0.0;
       double2 dt_p = mk<double2>(0.0, 0.0);
@@ -173,7 +182,7 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
           ct = c * gi;
           dt = mk<double2>((f.x - a * dt_p.x) * gi, (f.y - a * dt_p.y) * gi);
         }
-        cc[sl] = ct;
+        cpin[sl] = ct;
         d0[sl] = dt;
         ct_p = ct;
         dt_p = dt;
@@ -181,7 +190,7 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
       double2 xn = d0[slot(ny - 1)];
       for (int e = ny - 2; e >= 0; --e) {
         const int sl = slot(e);
-        const double c = cc[sl];
+        const double c = cpin[sl];
         xn = mk<double2>(d0[sl].x - c * xn.x, d0[sl].y - c * xn.y);
         d0[sl] = xn;
       }
@@ -210,13 +219,15 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
   const bool active = lane < NL;
   const int s0 = lane * T;
   const int len = active ? min(T, ny - s0) : 0;
+  constexpr int TR = TM > 0 ? TM : 1;
+  double at_r[TR], ct_r[TR];
   // forward elimination within the lane's block
   double at_e = 0.0, ct_e = 0.0;
   double2 e0 = mk<double2>(0.0, 0.0), e1 = mk<double2>(0.0, 0.0);
   if (active) {
     double at_p = -1.0, ct_p = 0.0;
     double2 p0 = mk<double2>(0.0, 0.0), p1 = mk<double2>(0.0, 0.0);
-    for (int t = 0; t < len; ++t) {
+    auto row = [&](int t) {
       const int i = s0 + t;
       const double a = am[i], c = ap[i];
       const int sl = t * 33 + lane;
@@ -225,12 +236,25 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
       const double2 f0 = d0[sl], f1 = d1[sl];
       p0 = mk<double2>((f0.x - a * p0.x) * gi, (f0.y - a * p0.y) * gi);
       p1 = mk<double2>((f1.x - a * p1.x) * gi, (f1.y - a * p1.y) * gi);
-      ca[sl] = at;
-      cc[sl] = ct;
       d0[sl] = p0;
       d1[sl] = p1;
       at_p = at;
       ct_p = ct;
+    };
+    if constexpr (TM > 0) {
+#pragma unroll
+      for (int t = 0; t < TM; ++t)
+        if (t < len) {
+          row(t);
+          at_r[t] = at_p;
+          ct_r[t] = ct_p;
+        }
+    } else {
+      for (int t = 0; t < len; ++t) {
+        row(t);
+        ca[t * 33 + lane] = at_p;
+        cc[t * 33 + lane] = ct_p;
+      }
     }
     at_e = at_p;
     ct_e = ct_p;
@@ -240,21 +264,27 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
   // running backward pass for x_s in terms of x_{s-1} and x_e
   double ha = 0.0, hc = -1.0;
   double2 h0 = mk<double2>(0.0, 0.0), h1 = mk<double2>(0.0, 0.0);
-  if (active && len >= 2) {
-    int sl = (len - 2) * 33 + lane;
-    h0 = d0[sl];
-    h1 = d1[sl];
-    ha = ca[sl];
-    hc = cc[sl];
-    for (int t = len - 3; t >= 0; --t) {
-      sl = t * 33 + lane;
-      const double ct = cc[sl];
-      const double2 v0 = d0[sl], v1 = d1[sl];
+  auto back_run = [&](int t, double at, double ct) {
+    const int sl = t * 33 + lane;
+    const double2 v0 = d0[sl], v1 = d1[sl];
+    if (t == len - 2) {
+      h0 = v0;
+      h1 = v1;
+      ha = at;
+      hc = ct;
+    } else {
       h0 = mk<double2>(v0.x - ct * h0.x, v0.y - ct * h0.y);
       h1 = mk<double2>(v1.x - ct * h1.x, v1.y - ct * h1.y);
-      ha = ca[sl] - ct * ha;
+      ha = at - ct * ha;
       hc = -ct * hc;
     }
+  };
+  if constexpr (TM > 0) {
+#pragma unroll
+    for (int t = TM - 2; t >= 0; --t)
+      if (t <= len - 2) back_run(t, at_r[t], ct_r[t]);
+  } else {
+    for (int t = len - 2; t >= 0; --t) back_run(t, ca[t * 33 + lane], cc[t * 33 + lane]);
   }
   // reduced equation of this lane: A y_{l-1} + B y_l + C y_{l+1} = D
   const double ha_n = shdn(ha, 1), hc_n = shdn(hc, 1);
@@ -312,14 +342,20 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
     double2 x0 = mk<double2>(y[0], y[1]), x1 = mk<double2>(y[2], y[3]);
     d0[(len - 1) * 33 + lane] = x0;
     d1[(len - 1) * 33 + lane] = x1;
-    for (int t = len - 2; t >= 0; --t) {
+    auto back_sub = [&](int t, double a, double c) {
       const int sl = t * 33 + lane;
-      const double a = ca[sl], c = cc[sl];
       const double2 v0 = d0[sl], v1 = d1[sl];
       x0 = mk<double2>(v0.x - a * ys[0] - c * x0.x, v0.y - a * ys[1] - c * x0.y);
       x1 = mk<double2>(v1.x - a * ys[2] - c * x1.x, v1.y - a * ys[3] - c * x1.y);
       d0[sl] = x0;
       d1[sl] = x1;
+    };
+    if constexpr (TM > 0) {
+#pragma unroll
+      for (int t = TM - 2; t >= 0; --t)
+        if (t <= len - 2) back_sub(t, at_r[t], ct_r[t]);
+    } else {
+      for (int t = len - 2; t >= 0; --t) back_sub(t, ca[t * 33 + lane], cc[t * 33 + lane]);
     }
   }
   __syncwarp();
@@ -330,16 +366,26 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
   }
 }
 
+// shared memory of a k_tridiag<V, TM> block: the two right-hand sides per warp,
+// plus the coefficient arrays when TM == 0
+static size_t tridiag_block_smem(int T, int TM) {
+  return (size_t)kWPB * 33 * T * (2 * sizeof(double2) + (TM == 0 ? 2 * sizeof(double) : 0));
+}
+
 template <typename V>
 static void launch_tridiag_t(V *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                              const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st) {
   const long nwarps = (long)g.nkx * (g.nz / 2 + 1);
-  const long nblk = (nwarps + kWPB - 1) / kWPB;
+  const unsigned nblk = (unsigned)((nwarps + kWPB - 1) / kWPB);
   const int T = tri_rows_per_lane(g.ny);
   // e/T == umulhi(e, floor(2^32/T) + 1) for every e < 2^16 (and T <= 2^16)
   const unsigned magic = T > 1 ? (unsigned)((1ull << 32) / (unsigned long long)T + 1ull) : 0u;
-  k_tridiag<V><<<(unsigned)nblk, kWPB * 32, tridiag_smem_bytes(g.ny), st>>>(spec, g, lamx, lamz, am, ap, dyf,
-                                                                            mean_c, nxnz, T, magic);
+  const dim3 blk(kWPB * 32);
+  if (T <= 4) k_tridiag<V, 4><<<nblk, blk, tridiag_block_smem(T, 4), st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, T, magic);
+  else if (T <= 8) k_tridiag<V, 8><<<nblk, blk, tridiag_block_smem(T, 8), st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, T, magic);
+  else if (T <= 12) k_tridiag<V, 12><<<nblk, blk, tridiag_block_smem(T, 12), st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, T, magic);
+  else if (T <= 16) k_tridiag<V, 16><<<nblk, blk, tridiag_block_smem(T, 16), st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, T, magic);
+  else k_tridiag<V, 0><<<nblk, blk, tridiag_block_smem(T, 0), st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, T, magic);
 }
 void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st) {
@@ -363,8 +409,11 @@ cudaError_t prepare_yz_kernels() {
   set((const void *)k_fftz<float2, true, L>, fftz_smem_bytes(L, 8));
   TBFP_FFT_LENGTHS(TBFP_CASE)
 #undef TBFP_CASE
-  set((const void *)k_tridiag<double2>, 227 * 1024);
-  set((const void *)k_tridiag<float2>, 227 * 1024);
+#define TBFP_TRI(TM)                                          \
+  set((const void *)k_tridiag<double2, TM>, 227 * 1024);      \
+  set((const void *)k_tridiag<float2, TM>, 227 * 1024);
+  TBFP_TRI(0) TBFP_TRI(4) TBFP_TRI(8) TBFP_TRI(12) TBFP_TRI(16)
+#undef TBFP_TRI
   return e;
 }
 
