@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--mg", action="store_true", help="also time the MG_MODE projection (default for c5)")
     ap.add_argument("--no-mg", action="store_true", help="skip the MG_MODE leg")
+    ap.add_argument("--no-vof", action="store_true", help="skip the material-properties leg")
     return ap.parse_args()
 
 
@@ -431,6 +432,34 @@ def main():
                  "note": "variable-coefficient PCG (MG_MODE) on the FAST leg's input; max_div of both paths"}
         pcg.close()
 
+    # material properties (updateMaterialProps + smoothVF) producing rho for the
+    # projection, on the same channel; compulsory bytes: read c, write cs, rho, mu
+    vofres = None
+    if not args.no_vof:
+        from tbfsolver_b200.solver import VOF
+        vof = VOF(eqn.solver, rhol=spec.rhol, rhog=spec.rhog, mul=1e-3, mug=1e-3 * spec.rhog)
+        vc = Field.like(inp.rho, inp.cs.a.clone())
+        vcs, vrho, vmu = (Field.like(inp.rho, torch.empty_like(inp.rho.a)) for _ in range(3))
+        for _ in range(max(3, args.warmup)):
+            vof.update_material_props(vc, vcs, vrho, vmu)
+        stream.synchronize()
+        v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            v0.record(stream)
+            for _ in range(args.steps):
+                vof.update_material_props(vc, vcs, vrho, vmu)
+            v1.record(stream)
+        stream.synchronize()
+        vms = v0.elapsed_time(v1) / args.steps
+        vbytes = 32.0 * inp.rho.a.numel()
+        pk0, _ = peaks()
+        vofres = {"value": g.ncells / (vms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": vms,
+                  "alg_bytes": vbytes, "alg_GBps": vbytes / (vms * 1e-3) / 1e9,
+                  "frac": vbytes / (vms * 1e-3) / 1e9 / pk0, "launches_per_step": 11,
+                  "note": "cs, rho, mu from the volume fraction (two cell-vertex-cell passes); bytes: read c, "
+                          "write cs, rho, mu"}
+        del vc, vcs, vrho, vmu
+
     # end to end through the host entry point, pinned host buffers
     def pinned(f):
         h = torch.empty(f.a.shape, dtype=torch.float64, pin_memory=True)
@@ -501,6 +530,7 @@ def main():
         "max_div": last.max_div, "cont_err": last.cont_err, "rel_residual": fp64_rel,
         "mixed": mixed,
         "mg": mgres,
+        "material_props": vofres,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk, "unit": "GB/s",

@@ -232,6 +232,27 @@ int tbfp_projection_mg_dev(tbfp_handle *h, const double *ux_in, const double *uy
                            double *ux_out, double *uy_out, double *uz_out, const double *rho, double dt,
                            double alpha, double *psi, tbfp_stats *stats);
 
+/* --- material properties from the volume fraction ---------------------- */
+/* updateMaterialProps (VOF.f90:197-233) with smoothVF (VOF.f90:235-262), the
+   step that produces rho for the projection: cs = two cell -> vertex -> cell
+   passes of c (cellToVertex / vertexToCell, interpolation.f90:188-276), each
+   followed by the boundary update of a cell field; then, over the whole
+   arrays (halos included), rho = rhog*cs + (1-cs)*rhol and
+   mu = mug*cs + (1-cs)*mul.  c, cs, rho, mu are cell fields with rho's layout
+   (halo hd_rho); c's ghosts must be current (the reference updates them).
+   tbfp_vof_setup takes the grid coordinates (grid.f90:633-688: centroids
+   xc(0:nx+1), yc(0:ny+1), zc(0:nz+1) and faces xf(0:nx), yf(0:ny), zf(0:nz))
+   and the phase properties (VOFCTOR), once per handle; a whole-channel
+   handle only. */
+typedef struct {
+  const double *xc, *yc, *zc; /* centroids, Fortran indices 0..n+1 */
+  const double *xf, *yf, *zf; /* faces, Fortran indices 0..n */
+  double rhol, rhog, mul, mug;
+} tbfp_vof_desc;
+int tbfp_vof_setup(tbfp_handle *h, const tbfp_vof_desc *v);
+int tbfp_material_props(tbfp_handle *h, const double *c, double *cs, double *rho, double *mu);
+int tbfp_material_props_dev(tbfp_handle *h, const double *c, double *cs, double *rho, double *mu);
+
 /* --- slab form: one channel split over several GPUs --------------------- */
 /* One rank's share of a channel split over P ranks (the reference's pencil
    decomposition with py = 1, pencilDec.f90:359-562): in physical space the z

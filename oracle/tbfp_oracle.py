@@ -851,3 +851,75 @@ def add_pressure_grad(mesh: Mesh, ux: FField, uy: FField, uz: FField, p: FField,
     upd(uy, 1, nx, 1, ny - 1, 1, nz, 0, 1, 0, mesh.dyc.r(2, ny)[None, :, None])
     upd(uz, 1, nx, 1, ny, 0, nz, 0, 0, 1, mesh.dzc.r(1, nz + 1)[:, None, None])
     equate_periodic_bc(ux, uz)
+
+
+# ---------------------------------------------------------------------------
+# Material properties: updateMaterialProps (VOF.f90:197-233) with smoothVF
+# (VOF.f90:235-262), cellToVertex / vertexToCell (interpolation.f90:188-276)
+# ---------------------------------------------------------------------------
+def cell_to_vertex(mesh: Mesh, q: FField) -> np.ndarray:
+    """cellToVertex (interpolation.f90:188-229) onto the vertex array s_cv(0:nx, 0:ny, 0:nz)
+    (VOF.f90:156): the trilinear value at vertex (i, j, k) from cells i..i+1,
+    j..j+1, k..k+1, weights w1..w8 and volume V as written there, summed in
+    the same order.  Returns shape (nz+1, ny+1, nx+1)."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    x, y, z = mesh.xc.r(0, nx + 1), mesh.yc.r(0, ny + 1), mesh.zc.r(0, nz + 1)
+    xv, yv, zv = mesh.xf.r(0, nx), mesh.yf.r(0, ny), mesh.zf.r(0, nz)
+    X1, X2 = (x[1:] - xv)[None, None, :], (xv - x[:-1])[None, None, :]   # x(i+1)-xv(i), xv(i)-x(i)
+    Y1, Y2 = (yv - y[:-1])[None, :, None], (y[1:] - yv)[None, :, None]   # yv(j)-y(j), y(j+1)-yv(j)
+    Z1, Z2 = (z[1:] - zv)[:, None, None], (zv - z[:-1])[:, None, None]   # z(k+1)-zv(k), zv(k)-z(k)
+    V = ((x[1:] - x[:-1])[None, None, :] * (y[1:] - y[:-1])[None, :, None]) * (z[1:] - z[:-1])[:, None, None]
+    Q = lambda di, dj, dk: q.v(di, nx + di, dj, ny + dj, dk, nz + dk)  # noqa: E731  q(i+di, j+dj, k+dk)
+    s = (X1 * Y1) * Z1 * Q(0, 1, 0)
+    s = s + (X2 * Y1) * Z1 * Q(1, 1, 0)
+    s = s + (X1 * Y1) * Z2 * Q(0, 1, 1)
+    s = s + (X2 * Y1) * Z2 * Q(1, 1, 1)
+    s = s + (X1 * Y2) * Z1 * Q(0, 0, 0)
+    s = s + (X2 * Y2) * Z1 * Q(1, 0, 0)
+    s = s + (X1 * Y2) * Z2 * Q(0, 0, 1)
+    s = s + (X2 * Y2) * Z2 * Q(1, 0, 1)
+    return s / V
+
+
+def vertex_to_cell(mesh: Mesh, qv: np.ndarray, q: FField) -> None:
+    """vertexToCell (interpolation.f90:234-276): the interior cells of q from
+    their 8 vertices (qv as returned by cell_to_vertex)."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    x, y, z = mesh.xc.r(1, nx), mesh.yc.r(1, ny), mesh.zc.r(1, nz)
+    xv, yv, zv = mesh.xf.r(0, nx), mesh.yf.r(0, ny), mesh.zf.r(0, nz)
+    X1, X2 = (xv[1:] - x)[None, None, :], (x - xv[:-1])[None, None, :]   # xv(i)-x(i), x(i)-xv(i-1)
+    Y1, Y2 = (y - yv[:-1])[None, :, None], (yv[1:] - y)[None, :, None]   # y(j)-yv(j-1), yv(j)-y(j)
+    Z1, Z2 = (zv[1:] - z)[:, None, None], (z - zv[:-1])[:, None, None]   # zv(k)-z(k), z(k)-zv(k-1)
+    V = ((xv[1:] - xv[:-1])[None, None, :] * (yv[1:] - yv[:-1])[None, :, None]) * (zv[1:] - zv[:-1])[:, None, None]
+    P = lambda di, dj, dk: qv[dk:dk + nz, dj:dj + ny, di:di + nx]  # noqa: E731  qv(i-1+di, j-1+dj, k-1+dk)
+    s = (X1 * Y1) * Z1 * P(0, 1, 0)
+    s = s + (X2 * Y1) * Z1 * P(1, 1, 0)
+    s = s + (X1 * Y1) * Z2 * P(0, 1, 1)
+    s = s + (X2 * Y1) * Z2 * P(1, 1, 1)
+    s = s + (X1 * Y2) * Z1 * P(0, 0, 0)
+    s = s + (X2 * Y2) * Z1 * P(1, 0, 0)
+    s = s + (X1 * Y2) * Z2 * P(0, 0, 1)
+    s = s + (X2 * Y2) * Z2 * P(1, 0, 1)
+    q.interior()[...] = s / V
+
+
+def smooth_vf(mesh: Mesh, c: FField) -> FField:
+    """smoothVF (VOF.f90:235-262), smooth_level = 1: cell -> vertex -> cell from c,
+    boundary update, once more from cs, boundary update.  c's ghosts must be
+    current; cs has c's halo."""
+    cs = FField("cl", c.hd, c.nx, c.ny, c.nz)
+    vertex_to_cell(mesh, cell_to_vertex(mesh, c), cs)
+    update_boundaries_cl_channel(cs)
+    vertex_to_cell(mesh, cell_to_vertex(mesh, cs), cs)
+    update_boundaries_cl_channel(cs)
+    return cs
+
+
+def update_material_props(mesh: Mesh, c: FField, rhol: float, rhog: float, mul: float, mug: float):
+    """updateMaterialProps (VOF.f90:197-233): cs = smoothVF(c), then over the
+    whole arrays (halos included) mu = mug*cs + (1-cs)*mul, rho = rhog*cs + (1-cs)*rhol.
+    Returns (cs, rho, mu)."""
+    cs = smooth_vf(mesh, c)
+    rho = FField("cl", c.hd, c.nx, c.ny, c.nz, rhog * cs.a + (1.0 - cs.a) * rhol)
+    mu = FField("cl", c.hd, c.nx, c.ny, c.nz, mug * cs.a + (1.0 - cs.a) * mul)
+    return cs, rho, mu

@@ -57,6 +57,12 @@ class TbfpMgParams(C.Structure):
                 ("max_iter_mg", C.c_int), ("tol_pcg", C.c_double), ("max_iter_pcg", C.c_int)]
 
 
+class TbfpVofDesc(C.Structure):
+    _fields_ = [("xc", C.c_void_p), ("yc", C.c_void_p), ("zc", C.c_void_p), ("xf", C.c_void_p), ("yf", C.c_void_p),
+                ("zf", C.c_void_p), ("rhol", C.c_double), ("rhog", C.c_double), ("mul", C.c_double),
+                ("mug", C.c_double)]
+
+
 class TbfpMemberIO(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("ux_in", "uy_in", "uz_in", "ux_out", "uy_out", "uz_out", "rho", "psi_n",
                                            "psi_nm1", "psi")]
@@ -98,6 +104,9 @@ PROTOTYPES = {
     "tbfp_ensemble_projection_dev": (C.c_int, [_H, C.POINTER(TbfpMemberIO), C.c_double, C.c_double, C.c_double,
                                                C.POINTER(TbfpStats)]),
     "tbfp_pcg_setup": (C.c_int, [_H, C.POINTER(TbfpMgParams)]),
+    "tbfp_vof_setup": (C.c_int, [_H, C.POINTER(TbfpVofDesc)]),
+    "tbfp_material_props": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tbfp_material_props_dev": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tbfp_pcg_solve": (C.c_int, [_H, _P, _P, _P, C.POINTER(TbfpStats)]),
     "tbfp_pcg_solve_dev": (C.c_int, [_H, _P, _P, _P, C.POINTER(TbfpStats)]),
     "tbfp_projection_mg": (C.c_int, [_H, _P, _P, _P, _P, C.c_double, C.c_double, _P, C.POINTER(TbfpStats)]),

@@ -62,6 +62,13 @@ struct tbfp_handle {
   bool slab = false;        // one rank's slab of a channel (tbfp_slab_create)
   GridK gs{};               // slab form: the spectral stage's grid (local kx, all kz)
   int nz_total = 0;
+  // material properties (tbfp_vof_setup)
+  bool vof = false;
+  VofTab vt{};
+  VofSep vsep{};
+  double *d_qv = nullptr;                     // vertex scratch, (nx+1)(ny+1)(nz+1)
+  double rhol = 0.0, rhog = 0.0, mul = 0.0, mug = 0.0;
+  double *h_vof[4] = {nullptr, nullptr, nullptr, nullptr};  // c, cs, rho, mu for tbfp_material_props
   MgSolver *mg = nullptr;   // MG_MODE hierarchy (tbfp_pcg_setup)
   std::vector<double> mdxf, mdxc, mdyf, mdyc, mdzf, mdzc;  // caller's metrics, kept for tbfp_pcg_setup
   double *h_beta = nullptr, *h_q = nullptr;                // device copies for tbfp_pcg_solve
@@ -982,6 +989,144 @@ int tbfp_projection(tbfp_handle *h, double *ux, double *uy, double *uz, const do
 }
 
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// updateMaterialProps (VOF.f90:197-233) with smoothVF (:235-262)
+// ---------------------------------------------------------------------------
+void run_material_props(tbfp_handle *h, const double *c, double *cs, double *rho, double *mu) {
+  if (h->hd_rho == 1)
+    launch_material_props_fused(h->vsep, c, cs, rho, mu, h->d_qv, h->Lrho, h->nx, h->ny, h->nz, h->rhol, h->rhog, h->mul,
+                                h->mug, h->stream);
+  else
+    launch_material_props(h->vt, c, cs, rho, mu, h->d_qv, h->Lrho, (long)h->n_rho, h->nx, h->ny, h->nz, h->hd_rho,
+                          h->rhol, h->rhog, h->mul, h->mug, h->stream);
+}
+
+int tbfp_vof_setup(tbfp_handle *h, const tbfp_vof_desc *v) {
+  if (!h || !v) return TBFP_ENULL;
+  if (!v->xc || !v->yc || !v->zc || !v->xf || !v->yf || !v->zf)
+    return set_err(h, TBFP_ENULL, "tbfp_vof_setup: a coordinate array is NULL");
+  if (h->slab) return set_err(h, TBFP_EINVAL, "tbfp_vof_setup: needs a whole-channel handle");
+  if (h->vof) return set_err(h, TBFP_EINVAL, "tbfp_vof_setup: already set up for this handle");
+  const int nx = h->nx, ny = h->ny, nz = h->nz;
+  // distance tables of cellToVertex / vertexToCell (interpolation.f90:188-276)
+  auto c2v = [](const double *c, const double *f, int n, int dir, std::vector<double> &a1, std::vector<double> &a2,
+                std::vector<double> &hh) {
+    a1.resize(n + 1);
+    a2.resize(n + 1);
+    hh.resize(n + 1);
+    for (int i = 0; i <= n; ++i) {
+      if (dir == 1) {  // y: yv(j)-y(j), y(j+1)-yv(j)
+        a1[i] = f[i] - c[i];
+        a2[i] = c[i + 1] - f[i];
+      } else {  // x, z: x(i+1)-xv(i), xv(i)-x(i)
+        a1[i] = c[i + 1] - f[i];
+        a2[i] = f[i] - c[i];
+      }
+      hh[i] = c[i + 1] - c[i];
+    }
+  };
+  auto v2c = [](const double *c, const double *f, int n, int dir, std::vector<double> &a1, std::vector<double> &a2,
+                std::vector<double> &vv) {
+    a1.resize(n);
+    a2.resize(n);
+    vv.resize(n);
+    for (int i = 1; i <= n; ++i) {
+      if (dir == 1) {  // y: y(j)-yv(j-1), yv(j)-y(j)
+        a1[i - 1] = c[i] - f[i - 1];
+        a2[i - 1] = f[i] - c[i];
+      } else {  // x, z: xv(i)-x(i), x(i)-xv(i-1)
+        a1[i - 1] = f[i] - c[i];
+        a2[i - 1] = c[i] - f[i - 1];
+      }
+      vv[i - 1] = f[i] - f[i - 1];
+    }
+  };
+  std::vector<double> t[18];
+  c2v(v->xc, v->xf, nx, 0, t[0], t[1], t[2]);
+  c2v(v->yc, v->yf, ny, 1, t[3], t[4], t[5]);
+  c2v(v->zc, v->zf, nz, 2, t[6], t[7], t[8]);
+  v2c(v->xc, v->xf, nx, 0, t[9], t[10], t[11]);
+  v2c(v->yc, v->yf, ny, 1, t[12], t[13], t[14]);
+  v2c(v->zc, v->zf, nz, 2, t[15], t[16], t[17]);
+  for (int i = 0; i <= nx; ++i)
+    if (!(t[2][i] > 0.0)) return set_err(h, TBFP_EINVAL, "tbfp_vof_setup: xc must increase");
+  for (int j = 0; j <= ny; ++j)
+    if (!(t[5][j] > 0.0)) return set_err(h, TBFP_EINVAL, "tbfp_vof_setup: yc must increase");
+  for (int k = 0; k <= nz; ++k)
+    if (!(t[8][k] > 0.0)) return set_err(h, TBFP_EINVAL, "tbfp_vof_setup: zc must increase");
+  cudaSetDevice(h->device);
+  double *d[18];
+  int rc;
+  for (int e = 0; e < 18; ++e)
+    if ((rc = upload(h, &d[e], t[e]))) return rc;
+  // halo 1 (the reference's): two fused passes through a field-shaped scratch;
+  // otherwise the vertex array of the reference's s_cv
+  const size_t nscr = h->hd_rho == 1 ? h->n_rho : (size_t)(nx + 1) * (ny + 1) * (nz + 1);
+  if ((rc = dev_alloc(h, &h->d_qv, nscr))) return rc;
+  h->vt = VofTab{d[0], d[1], d[2], d[3], d[4], d[5], d[6], d[7], d[8],
+                 d[9], d[10], d[11], d[12], d[13], d[14], d[15], d[16], d[17]};
+  // separable pass per direction: cell i takes vertices i-1 (weight a) and i
+  // (weight b) of vertexToCell, vertex v takes cells v (weight e) and v+1
+  // (weight f) of cellToVertex; in y the tables hold the weights in the other
+  // order (interpolation.f90:206-224, 252-271).
+  auto sep = [](const std::vector<double> &c1, const std::vector<double> &c2, const std::vector<double> &hh,
+                const std::vector<double> &v1, const std::vector<double> &v2, const std::vector<double> &VV, int n,
+                bool ydir, std::vector<double> &m, std::vector<double> &z, std::vector<double> &p) {
+    m.resize(n);
+    z.resize(n);
+    p.resize(n);
+    for (int i = 1; i <= n; ++i) {
+      const double a = (ydir ? v2[i - 1] : v1[i - 1]) / VV[i - 1], b = (ydir ? v1[i - 1] : v2[i - 1]) / VV[i - 1];
+      const double e0 = (ydir ? c2[i - 1] : c1[i - 1]) / hh[i - 1], f0 = (ydir ? c1[i - 1] : c2[i - 1]) / hh[i - 1];
+      const double e1 = (ydir ? c2[i] : c1[i]) / hh[i], f1 = (ydir ? c1[i] : c2[i]) / hh[i];
+      m[i - 1] = a * e0;
+      z[i - 1] = a * f0 + b * e1;
+      p[i - 1] = b * f1;
+    }
+  };
+  std::vector<double> sw[9];
+  sep(t[0], t[1], t[2], t[9], t[10], t[11], nx, false, sw[0], sw[1], sw[2]);
+  sep(t[3], t[4], t[5], t[12], t[13], t[14], ny, true, sw[3], sw[4], sw[5]);
+  sep(t[6], t[7], t[8], t[15], t[16], t[17], nz, false, sw[6], sw[7], sw[8]);
+  double *ds[9];
+  for (int e = 0; e < 9; ++e)
+    if ((rc = upload(h, &ds[e], sw[e]))) return rc;
+  h->vsep = VofSep{ds[0], ds[1], ds[2], ds[3], ds[4], ds[5], ds[6], ds[7], ds[8]};
+  h->rhol = v->rhol;
+  h->rhog = v->rhog;
+  h->mul = v->mul;
+  h->mug = v->mug;
+  h->vof = true;
+  return TBFP_OK;
+}
+
+int tbfp_material_props_dev(tbfp_handle *h, const double *c, double *cs, double *rho, double *mu) {
+  int rc = check_ptrs(h, {c, cs, rho, mu});
+  if (rc) return rc;
+  if (!h->vof) return set_err(h, TBFP_EINVAL, "tbfp_material_props: call tbfp_vof_setup first");
+  if (aliased(c, cs) || aliased(c, rho) || aliased(c, mu) || aliased(cs, rho) || aliased(cs, mu) || aliased(rho, mu))
+    return set_err(h, TBFP_EINVAL, "tbfp_material_props: c, cs, rho and mu must be distinct arrays");
+  cudaSetDevice(h->device);
+  run_material_props(h, c, cs, rho, mu);
+  return finish(h, "tbfp_material_props");
+}
+
+int tbfp_material_props(tbfp_handle *h, const double *c, double *cs, double *rho, double *mu) {
+  int rc = check_ptrs(h, {c, cs, rho, mu});
+  if (rc) return rc;
+  if (!h->vof) return set_err(h, TBFP_EINVAL, "tbfp_material_props: call tbfp_vof_setup first");
+  cudaSetDevice(h->device);
+  for (double *&b : h->h_vof)
+    if (!b && (rc = dev_alloc(h, &b, h->n_rho))) return rc;
+  const size_t n = h->n_rho;
+  if ((rc = h2d(h, h->h_vof[0], c, n))) return rc;
+  run_material_props(h, h->h_vof[0], h->h_vof[1], h->h_vof[2], h->h_vof[3]);
+  if ((rc = d2h(h, cs, h->h_vof[1], n)) || (rc = d2h(h, rho, h->h_vof[2], n)) || (rc = d2h(h, mu, h->h_vof[3], n)))
+    return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return finish(h, "tbfp_material_props");
+}
+
 int tbfp_pcg_setup(tbfp_handle *h, const tbfp_mg_params *p) {
   if (!h || !p) return TBFP_ENULL;
   cudaSetDevice(h->device);

@@ -196,6 +196,30 @@ void launch_correct_inplace(const CorrArgs &ca, bool has_st, const GridK &g, cud
 void launch_div(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz, const GridK &g,
                 unsigned long long *maxdiv, cudaStream_t st);
 
+// Material properties (updateMaterialProps + smoothVF, tbfp_vof.cu).  Distance
+// tables of the two interpolations (interpolation.f90:188-276), per direction:
+// cellToVertex at vertex i = 0..n: c*1 = x(i+1)-xv(i) (x) / yv(j)-y(j) (y) /
+// z(k+1)-zv(k) (z), c*2 = xv(i)-x(i) / y(j+1)-yv(j) / zv(k)-z(k), h* = x(i+1)-x(i);
+// vertexToCell at cell i = 1..n (table index i-1): v*1 = xv(i)-x(i) / y(j)-yv(j-1) /
+// zv(k)-z(k), v*2 = x(i)-xv(i-1) / yv(j)-y(j) / z(k)-zv(k-1), V* = xv(i)-xv(i-1).
+struct VofTab {
+  const double *cx1, *cx2, *hx, *cy1, *cy2, *hy, *cz1, *cz2, *hz;
+  const double *vx1, *vx2, *Vx, *vy1, *vy2, *Vy, *vz1, *vz2, *Vz;
+};
+// qv: (nx+1)(ny+1)(nz+1) scratch; c, cs, rho, mu laid out by L (n elements, halo hd)
+void launch_material_props(const VofTab &t, const double *c, double *cs, double *rho, double *mu, double *qv, Lay L,
+                           long n, int nx, int ny, int nz, int hd, double rhol, double rhog, double mul, double mug,
+                           cudaStream_t st);
+// Separable form of one cell -> vertex -> cell pass, per direction and cell
+// i = 1..n (table index i-1): out(i) = m(i) in(i-1) + z(i) in(i) + p(i) in(i+1).
+struct VofSep {
+  const double *xm, *x0, *xp, *ym, *y0, *yp, *zm, *z0, *zp;
+};
+// the same for halo 1 in two fused launches; tmp: a scratch field laid out by L
+void launch_material_props_fused(const VofSep &w, const double *c, double *cs, double *rho, double *mu, double *tmp,
+                                 Lay L, int nx, int ny, int nz, double rhol, double rhog, double mul, double mug,
+                                 cudaStream_t st);
+
 // MG_MODE source/beta (computeSource MG, computeBeta) and addPressureGrad.
 // idxc, idzc: 1/dxc(i), 1/dzc(k) for Fortran i = 1..nx+1 (0-based tables).
 void launch_mg_source_beta(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz,

@@ -1,0 +1,213 @@
+// Material properties from the volume fraction: updateMaterialProps
+// (VOF.f90:197-233) with smoothVF (VOF.f90:235-262).  cs is c after two
+// cell -> vertex -> cell passes (cellToVertex / vertexToCell,
+// interpolation.f90:188-276), each followed by the boundary update of a cell
+// field (zero normal gradient at the y walls, periodic halos in x then z);
+// then rho = rhog*cs + (1-cs)*rhol and mu = mug*cs + (1-cs)*mul over the whole
+// arrays, halos included.  FP64; the weights of both interpolations are
+// products of per-direction distances, tabulated on the host.
+#include <cuda_runtime.h>
+
+#include "tbfp_kernels.cuh"
+
+namespace tbfp {
+
+namespace {
+
+constexpr int kVT = 128;
+
+// vertex (i, j, k), 0 <= i <= nx: from cells i..i+1 (and j, k likewise)
+__global__ void __launch_bounds__(kVT) k_cell_to_vertex(VofTab t, const double *__restrict__ q, Lay L,
+                                                        double *__restrict__ qv, int nx, int ny, int nz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i > nx) return;
+  const int o = (int)at(L, i, j, k), sj = (int)L.sj, sk = (int)L.sk;
+  const double X1 = t.cx1[i], X2 = t.cx2[i], Y1 = t.cy1[j], Y2 = t.cy2[j], Z1 = t.cz1[k], Z2 = t.cz2[k];
+  // weights and sum in the order of interpolation.f90:206-224
+  const double w1 = (X1 * Y1) * Z1, w2 = (X2 * Y1) * Z1, w3 = (X1 * Y1) * Z2, w4 = (X2 * Y1) * Z2;
+  const double w5 = (X1 * Y2) * Z1, w6 = (X2 * Y2) * Z1, w7 = (X1 * Y2) * Z2, w8 = (X2 * Y2) * Z2;
+  const double V = (t.hx[i] * t.hy[j]) * t.hz[k];
+  double s = w1 * q[o + sj];
+  s = s + w2 * q[o + 1 + sj];
+  s = s + w3 * q[o + sj + sk];
+  s = s + w4 * q[o + 1 + sj + sk];
+  s = s + w5 * q[o];
+  s = s + w6 * q[o + 1];
+  s = s + w7 * q[o + sk];
+  s = s + w8 * q[o + 1 + sk];
+  qv[((long)k * (ny + 1) + j) * (nx + 1) + i] = s / V;
+}
+
+// interior cell (i, j, k), 1 <= i <= nx: from vertices i-1..i
+__global__ void __launch_bounds__(kVT) k_vertex_to_cell(VofTab t, const double *__restrict__ qv,
+                                                        double *__restrict__ q, Lay L, int nx, int ny) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
+  if (i > nx) return;
+  const long vj = nx + 1, vk = (long)(ny + 1) * (nx + 1);
+  const long v = (long)(k - 1) * vk + (long)(j - 1) * vj + (i - 1);  // qv(i-1, j-1, k-1)
+  const double X1 = t.vx1[i - 1], X2 = t.vx2[i - 1], Y1 = t.vy1[j - 1], Y2 = t.vy2[j - 1];
+  const double Z1 = t.vz1[k - 1], Z2 = t.vz2[k - 1];
+  // weights and sum in the order of interpolation.f90:252-271
+  const double w1 = (X1 * Y1) * Z1, w2 = (X2 * Y1) * Z1, w3 = (X1 * Y1) * Z2, w4 = (X2 * Y1) * Z2;
+  const double w5 = (X1 * Y2) * Z1, w6 = (X2 * Y2) * Z1, w7 = (X1 * Y2) * Z2, w8 = (X2 * Y2) * Z2;
+  const double V = (t.Vx[i - 1] * t.Vy[j - 1]) * t.Vz[k - 1];
+  double s = w1 * qv[v + vj];
+  s = s + w2 * qv[v + 1 + vj];
+  s = s + w3 * qv[v + vj + vk];
+  s = s + w4 * qv[v + 1 + vj + vk];
+  s = s + w5 * qv[v];
+  s = s + w6 * qv[v + 1];
+  s = s + w7 * qv[v + vk];
+  s = s + w8 * qv[v + 1 + vk];
+  q[at(L, i, j, k)] = s / V;
+}
+
+// updateBoundaries of a cell field of the channel (field.f90:950-974):
+// phase 0, zero normal gradient at the y walls on the interior i, k range
+// (one ghost layer, boundaryField_S.f90:694-727); phase 1, periodic x halos
+// over all j, k; phase 2, periodic z halos over all i, j.
+__global__ void k_bc_cell(double *__restrict__ f, Lay L, int nx, int ny, int nz, int hd, int phase) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+  if (phase == 0) {
+    const int i = a + 1, k = b + 1;
+    if (i > nx) return;
+    f[at(L, i, 0, k)] = f[at(L, i, 1, k)];
+    f[at(L, i, ny + 1, k)] = f[at(L, i, ny, k)];
+  } else if (phase == 1) {
+    const int j = a + 1 - hd, k = b + 1 - hd;  // j, k over the extended ranges
+    if (j > ny + hd) return;
+    for (int g = 0; g < hd; ++g) {
+      f[at(L, nx + 1 + g, j, k)] = f[at(L, 1 + g, j, k)];
+      f[at(L, 1 - hd + g, j, k)] = f[at(L, nx - hd + 1 + g, j, k)];
+    }
+  } else {
+    const int i = a + 1 - hd, j = b + 1 - hd;  // i, j over the extended ranges
+    if (i > nx + hd) return;
+    for (int g = 0; g < hd; ++g) {
+      f[at(L, i, j, nz + 1 + g)] = f[at(L, i, j, 1 + g)];
+      f[at(L, i, j, 1 - hd + g)] = f[at(L, i, j, nz - hd + 1 + g)];
+    }
+  }
+}
+
+// rho and mu over the whole arrays (VOF.f90:220-221)
+__global__ void k_props(const double *__restrict__ cs, double *__restrict__ rho, double *__restrict__ mu, long n,
+                        double rhol, double rhog, double mul, double mug) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const double c = cs[e];
+    mu[e] = mug * c + (1.0 - c) * mul;
+    rho[e] = rhog * c + (1.0 - c) * rhol;
+  }
+}
+
+void bc_cell(double *f, Lay L, int nx, int ny, int nz, int hd, cudaStream_t st) {
+  k_bc_cell<<<dim3((nx + kVT - 1) / kVT, nz), kVT, 0, st>>>(f, L, nx, ny, nz, hd, 0);
+  k_bc_cell<<<dim3((ny + 2 * hd + kVT - 1) / kVT, nz + 2 * hd), kVT, 0, st>>>(f, L, nx, ny, nz, hd, 1);
+  k_bc_cell<<<dim3((nx + 2 * hd + kVT - 1) / kVT, ny + 2 * hd), kVT, 0, st>>>(f, L, nx, ny, nz, hd, 2);
+}
+
+// One smoothing pass (cellToVertex then vertexToCell) for halo 1, in
+// separable form.  Both interpolations are products of 1-D linear weights
+// (w = X*Y*Z / (hx*hy*hz)), so a pass is, per direction, the 3-point stencil
+//   out(i) = m(i) in(i-1) + z(i) in(i) + p(i) in(i+1)
+// with m, z, p from the distance tables (VofSep, built on the host), applied
+// in z, then y, then x through a shared-memory tile: 9 FMAs per cell instead
+// of the 16 products and 2 divisions per vertex and cell of the direct form
+// (same operator; rounding differs in the last bits).  A CTA owns cells
+// [i0, i0+kSX) x [j0, j0+kSY) x [k0, k0+kSZ) (1-based) and stages their input
+// ring.  The boundary update that follows a pass in the reference (y walls,
+// then x, then z halos over the extended ranges) leaves each ghost cell equal
+// to the interior cell reached by mapping every coordinate independently (x:
+// 0 -> nx, nx+1 -> 1; y: 0 -> 1, ny+1 -> ny; z: 0 -> nz, nz+1 -> 1), so each
+// cell also writes the ghost cells that copy it.  PROPS: the final pass, which
+// also writes rho and mu (VOF.f90:220-221) at the cell and its ghost images.
+constexpr int kSX = 32, kSY = 8, kSZ = 4, kST = 256;
+
+template <bool PROPS>
+__global__ void __launch_bounds__(kST) k_smooth_pass(VofSep w, const double *__restrict__ in, double *__restrict__ out,
+                                                     double *__restrict__ rho, double *__restrict__ mu, Lay L,
+                                                     int nx, int ny, int nz, double rhol, double rhog, double mul,
+                                                     double mug) {
+  constexpr int CX = kSX + 2, CY = kSY + 2, CZ = kSZ + 2;
+  __shared__ double buf0[CZ * CY * CX];  // input ring, then the tile after y
+  __shared__ double c1[kSZ][CY][CX];     // after z
+  auto c0 = reinterpret_cast<double(*)[CY][CX]>(buf0);
+  auto c2 = reinterpret_cast<double(*)[kSY][CX]>(buf0);
+  const int i0 = blockIdx.x * kSX + 1, j0 = blockIdx.y * kSY + 1, k0 = blockIdx.z * kSZ + 1;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < CX * CY * CZ; e += kST) {
+    const int cx = e % CX, cy = (e / CX) % CY, cz = e / (CX * CY);
+    const int gi = i0 - 1 + cx, gj = j0 - 1 + cy, gk = k0 - 1 + cz;
+    double v = 0.0;
+    if (gi <= nx + 1 && gj <= ny + 1 && gk <= nz + 1) v = in[at(L, gi, gj, gk)];
+    c0[cz][cy][cx] = v;
+  }
+  __syncthreads();
+  for (int e = tid; e < CX * CY * kSZ; e += kST) {
+    const int cx = e % CX, cy = (e / CX) % CY, oz = e / (CX * CY);
+    const int k = min(k0 + oz, nz) - 1;
+    c1[oz][cy][cx] = w.zm[k] * c0[oz][cy][cx] + w.z0[k] * c0[oz + 1][cy][cx] + w.zp[k] * c0[oz + 2][cy][cx];
+  }
+  __syncthreads();
+  for (int e = tid; e < CX * kSY * kSZ; e += kST) {
+    const int cx = e % CX, oy = (e / CX) % kSY, oz = e / (CX * kSY);
+    const int j = min(j0 + oy, ny) - 1;
+    c2[oz][oy][cx] = w.ym[j] * c1[oz][oy][cx] + w.y0[j] * c1[oz][oy + 1][cx] + w.yp[j] * c1[oz][oy + 2][cx];
+  }
+  __syncthreads();
+  for (int e = tid; e < kSX * kSY * kSZ; e += kST) {
+    const int ox = e % kSX, oy = (e / kSX) % kSY, oz = e / (kSX * kSY);
+    const int i = i0 + ox, j = j0 + oy, k = k0 + oz;
+    if (i > nx || j > ny || k > nz) continue;
+    const double c = w.xm[i - 1] * c2[oz][oy][ox] + w.x0[i - 1] * c2[oz][oy][ox + 1] + w.xp[i - 1] * c2[oz][oy][ox + 2];
+    const double m = mug * c + (1.0 - c) * mul, r = rhog * c + (1.0 - c) * rhol;
+    // the cell and the ghost cells equal to it
+    const int xs[2] = {i, i == nx ? 0 : (i == 1 ? nx + 1 : -1)};
+    const int ys[2] = {j, j == 1 ? 0 : (j == ny ? ny + 1 : -1)};
+    const int zs[2] = {k, k == nz ? 0 : (k == 1 ? nz + 1 : -1)};
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int d = 0; d < 2; ++d) {
+          if (xs[a] < 0 || ys[b] < 0 || zs[d] < 0) continue;
+          const long o = at(L, xs[a], ys[b], zs[d]);
+          out[o] = c;
+          if constexpr (PROPS) {
+            mu[o] = m;
+            rho[o] = r;
+          }
+        }
+  }
+}
+
+}  // namespace
+
+// Halo-1 fields (the reference's c, cs, rho, mu): two fused passes, the first
+// into the scratch tmp (laid out like the fields), the second into cs with
+// rho and mu.
+void launch_material_props_fused(const VofSep &w, const double *c, double *cs, double *rho, double *mu, double *tmp,
+                                 Lay L, int nx, int ny, int nz, double rhol, double rhog, double mul, double mug,
+                                 cudaStream_t st) {
+  const dim3 grid((nx + kSX - 1) / kSX, (ny + kSY - 1) / kSY, (nz + kSZ - 1) / kSZ);
+  k_smooth_pass<false><<<grid, kST, 0, st>>>(w, c, tmp, nullptr, nullptr, L, nx, ny, nz, 0.0, 0.0, 0.0, 0.0);
+  k_smooth_pass<true><<<grid, kST, 0, st>>>(w, tmp, cs, rho, mu, L, nx, ny, nz, rhol, rhog, mul, mug);
+}
+
+void launch_material_props(const VofTab &t, const double *c, double *cs, double *rho, double *mu, double *qv, Lay L,
+                           long n, int nx, int ny, int nz, int hd, double rhol, double rhog, double mul, double mug,
+                           cudaStream_t st) {
+  const dim3 gv((nx + 1 + kVT - 1) / kVT, ny + 1, nz + 1), gc((nx + kVT - 1) / kVT, ny, nz);
+  k_cell_to_vertex<<<gv, kVT, 0, st>>>(t, c, L, qv, nx, ny, nz);
+  k_vertex_to_cell<<<gc, kVT, 0, st>>>(t, qv, cs, L, nx, ny);
+  bc_cell(cs, L, nx, ny, nz, hd, st);
+  k_cell_to_vertex<<<gv, kVT, 0, st>>>(t, cs, L, qv, nx, ny, nz);
+  k_vertex_to_cell<<<gc, kVT, 0, st>>>(t, qv, cs, L, nx, ny);
+  bc_cell(cs, L, nx, ny, nz, hd, st);
+  long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_props<<<(unsigned)blocks, 256, 0, st>>>(cs, rho, mu, n, rhol, rhog, mul, mug);
+}
+
+}  // namespace tbfp

@@ -30,7 +30,8 @@ import ctypes as C
 import numpy as np
 
 from ._native import (TBFP_EINVAL, TBFP_FLAG_ASYNC, TBFP_FLAG_RESIDUAL, TBFP_FLAG_TIMING, TBFP_FP64, TBFP_MIXED,
-                      TbfpDesc, TbfpError, TbfpMemberIO, TbfpMgParams, TbfpStats, check, load)
+                      TbfpDesc, TbfpError, TbfpMemberIO, TbfpMgParams, TbfpStats,
+                      TbfpVofDesc, check, load)
 from .fields import Field, VField
 from .grid import Grid
 
@@ -243,6 +244,34 @@ def _zeros_like(a):
     import torch  # noqa: PLC0415
 
     return torch.zeros_like(a)
+
+
+class VOF:
+    """Material properties of the two-phase mixture (the VOF type's
+    updateMaterialProps, VOF.f90:197-233, with smoothVF, :235-262) on a solver's
+    handle: cs = smoothed volume fraction, rho and mu from cs.  The fields c, cs,
+    rho, mu are cell fields with the solver's rho halo."""
+
+    def __init__(self, solver: FastPoissonSolver, rhol: float, rhog: float, mul: float, mug: float):
+        m = solver.mesh
+        nx, ny, nz = m.nx, m.ny, m.nz
+        self.solver = solver
+        self.rhol, self.rhog, self.mul, self.mug = rhol, rhog, mul, mug
+        self._c = {
+            "xc": np.ascontiguousarray(m.xc.r(0, nx + 1)), "yc": np.ascontiguousarray(m.yc.r(0, ny + 1)),
+            "zc": np.ascontiguousarray(m.zc.r(0, nz + 1)), "xf": np.ascontiguousarray(m.xf.r(0, nx)),
+            "yf": np.ascontiguousarray(m.yf.r(0, ny)), "zf": np.ascontiguousarray(m.zf.r(0, nz)),
+        }
+        v = TbfpVofDesc(rhol=rhol, rhog=rhog, mul=mul, mug=mug,
+                        **{k: a.ctypes.data_as(C.c_void_p) for k, a in self._c.items()})
+        check(solver.lib.tbfp_vof_setup(solver.h, C.byref(v)), solver.h)
+
+    def update_material_props(self, c: Field, cs: Field, rho: Field, mu: Field) -> None:
+        """updateMaterialProps (VOF.f90:197-233): cs, rho and mu from c (c's ghosts current)."""
+        sv = self.solver
+        dev = _placement([c, cs, rho, mu])
+        fn = sv.lib.tbfp_material_props_dev if dev else sv.lib.tbfp_material_props
+        check(fn(sv.h, c.address(), cs.address(), rho.address(), mu.address()), sv.h)
 
 
 class PCG:
