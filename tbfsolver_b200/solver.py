@@ -277,7 +277,20 @@ class VOF:
 class PCG:
     """MG_MODE pressure solver (pcgCTOR, pcg.f90:62-99): FP64 conjugate gradients
     preconditioned by FP32 red-black Gauss-Seidel multigrid V-cycles.  Defaults
-    are the reference's channel_18 settings (specs/pcg_solver)."""
+    are those of the 256x256x128 MG workload (6 levels, 2 + 2 sweeps); a case's
+    own settings come from its specs/pcg_solver file through from_specs."""
+
+    @classmethod
+    def from_specs(cls, mesh: Grid, specs_dir: str, **kw) -> "PCG":
+        """pcgCTOR / multiGridCTOR reading specs/pcg_solver (pcg.f90:82-85,
+        multiGrid.f90:81-86): nLevels, nPreSweep, nPostSweep, tolMG, maxIterMG,
+        tolPCG, maxIterPCG."""
+        from .io import ParFile  # noqa: PLC0415
+
+        p = ParFile("pcg_solver", specs_dir)
+        return cls(mesh, n_levels=p.read_int("nLevels"), n_pre=p.read_int("nPreSweep"),
+                   n_post=p.read_int("nPostSweep"), tol_mg=p.read_real("tolMG"), max_iter_mg=p.read_int("maxIterMG"),
+                   tol_pcg=p.read_real("tolPCG"), max_iter_pcg=p.read_int("maxIterPCG"), **kw)
 
     def __init__(self, mesh: Grid, n_levels: int = 6, n_pre: int = 2, n_post: int = 2, tol_mg: float = 0.4,
                  max_iter_mg: int = 100, tol_pcg: float = 1e-10, max_iter_pcg: int = 100, hd_psi: int = 1,
