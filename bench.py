@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--mg", action="store_true", help="also time the MG_MODE projection (default for c5)")
     ap.add_argument("--no-mg", action="store_true", help="skip the MG_MODE leg")
     ap.add_argument("--no-vof", action="store_true", help="skip the material-properties leg")
+    ap.add_argument("--no-momentum", action="store_true", help="skip the momentum-predictor leg")
     return ap.parse_args()
 
 
@@ -460,6 +461,35 @@ def main():
                           "write cs, rho, mu"}
         del vc, vcs, vrho, vmu
 
+    # momentum predictor (solveMomentumEqn FAST, QUICK, AB2) on the same channel;
+    # compulsory bytes of the in-place step: read u, c, mu, rho and the flux
+    # history, write u and the new fluxes (15 FP64 values per cell)
+    momres = None
+    if not args.no_momentum:
+        from tbfsolver_b200.solver import MomentumEqn
+        mom = MomentumEqn(eqn.solver, scheme=2, gch=0.0, g=0.0)
+        mu_ = Field.like(inp.rho, 1e-3 * (1.0 - inp.cs.a) + 1e-3 * spec.rhog * inp.cs.a)
+        mu_u = VField(*[Field.like(f, f.a.clone()) for f in u_in.components()])
+        for _ in range(max(3, args.warmup)):
+            mom.predictor(mu_u, inp.cs, mu_, inp.rho, dt=dt, alpha=alpha, gamma=1.5, xi=-0.5, rho0=inp.rho0)
+        stream.synchronize()
+        t0m, t1m = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            t0m.record(stream)
+            for _ in range(args.steps):
+                mom.predictor(mu_u, inp.cs, mu_, inp.rho, dt=dt, alpha=alpha, gamma=1.5, xi=-0.5, rho0=inp.rho0)
+            t1m.record(stream)
+        stream.synchronize()
+        mms_ = t0m.elapsed_time(t1m) / args.steps
+        mbytes = 15 * 8.0 * g.ncells
+        pk0, _ = peaks()
+        momres = {"value": g.ncells / (mms_ * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": mms_,
+                  "alg_bytes": mbytes, "alg_GBps": mbytes / (mms_ * 1e-3) / 1e9,
+                  "frac": mbytes / (mms_ * 1e-3) / 1e9 / pk0, "launches_per_step": 2, "scheme": "QUICK",
+                  "note": "convection + diffusion fluxes and the AB2 update of u in place; bytes: read u, c, mu, "
+                          "rho, flux history, write u, fluxes"}
+        del mu_, mu_u
+
     # end to end through the host entry point, pinned host buffers
     def pinned(f):
         h = torch.empty(f.a.shape, dtype=torch.float64, pin_memory=True)
@@ -531,6 +561,7 @@ def main():
         "mixed": mixed,
         "mg": mgres,
         "material_props": vofres,
+        "momentum": momres,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk, "unit": "GB/s",

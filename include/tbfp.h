@@ -253,6 +253,41 @@ int tbfp_vof_setup(tbfp_handle *h, const tbfp_vof_desc *v);
 int tbfp_material_props(tbfp_handle *h, const double *c, double *cs, double *rho, double *mu);
 int tbfp_material_props_dev(tbfp_handle *h, const double *c, double *cs, double *rho, double *mu);
 
+/* --- momentum predictor ------------------------------------------------ */
+/* solveMomentumEqn FAST (momentumEqn.f90:161-194) without its closing
+   updateBoundariesV, which stays with the caller as for the projection: the
+   convection (flux-limited) and diffusion (variable viscosity) fluxes of
+   updateConveDiff from the current u, u += dt*(gamma*phi + xi*phi_prev)
+   (addConvDiff), then the sources of addSource: ux += dt*alpha*(st_x/rho0 +
+   fs/rho_x + gCH), uy += dt*alpha*(st_y/rho0 + g), uz += dt*alpha*st_z/rho0,
+   on the equation boxes (ux faces 0..nx, uy faces 1..ny-1, uz faces 0..nz,
+   setEqnBounds :1134-1190).  u is updated in place; c, mu and rho are cell
+   fields with rho's layout; st is NULL or the three surface-tension
+   components (hd_st).  u needs its two-layer halo current (the limiters read
+   u at +-2).  The library keeps the flux history (phi of the last call);
+   tbfp_momentum_setup starts it at zero (initFluxes), tbfp_momentum_fluxes
+   loads or reads it (initOldTimeFlux / printOldTimeFlux) as host arrays over
+   the equation boxes in Fortran order: phi_x (0:nx,1:ny,1:nz),
+   phi_y (1:nx,1:ny-1,1:nz), phi_z (1:nx,1:ny,0:nz).  The spacings are the
+   mesh's own metrics (grid.f90:334-399) including the ghost entries the
+   stencils reach: dxf(0:nx+1), dxc(0:nx+1), dyf(0:ny+1), dyc(0:ny+1),
+   dzf(0:nz+1), dzc(0:nz+1), n+2 values each. */
+typedef struct {
+  int scheme; /* specs/schemes convection_scheme: 0 central, 1 upwind, 2 QUICK, 3 van Leer,
+                 4 superbee, 5 superbee where the volume fraction varies, central elsewhere */
+  double gch; /* specs/parameters gCH: streamwise driving added to ux */
+  double g;   /* specs/parameters g: body force added to uy */
+  const double *dxf, *dxc, *dyf, *dyc, *dzf, *dzc;
+} tbfp_momentum_desc;
+int tbfp_momentum_setup(tbfp_handle *h, const tbfp_momentum_desc *m);
+int tbfp_momentum_fluxes(tbfp_handle *h, double *phi_x, double *phi_y, double *phi_z, int set);
+int tbfp_momentum_predictor(tbfp_handle *h, double *ux, double *uy, double *uz, const double *c, const double *mu,
+                            const double *rho, const double *const *st, double dt, double alpha, double gamma,
+                            double xi, double rho0, double fs);
+int tbfp_momentum_predictor_dev(tbfp_handle *h, double *ux, double *uy, double *uz, const double *c,
+                                const double *mu, const double *rho, const double *const *st, double dt,
+                                double alpha, double gamma, double xi, double rho0, double fs);
+
 /* --- slab form: one channel split over several GPUs --------------------- */
 /* One rank's share of a channel split over P ranks (the reference's pencil
    decomposition with py = 1, pencilDec.f90:359-562): in physical space the z

@@ -923,3 +923,197 @@ def update_material_props(mesh: Mesh, c: FField, rhol: float, rhog: float, mul: 
     rho = FField("cl", c.hd, c.nx, c.ny, c.nz, rhog * cs.a + (1.0 - cs.a) * rhol)
     mu = FField("cl", c.hd, c.nx, c.ny, c.nz, mug * cs.a + (1.0 - cs.a) * mul)
     return cs, rho, mu
+
+
+# ---------------------------------------------------------------------------
+# Momentum predictor: solveMomentumEqn FAST (momentumEqn.f90:161-194) without
+# its closing updateBoundariesV: copyOldFluxes / resetFluxes, updateConveDiff
+# (:198-607), addConvDiff (:738-791), addSource (:874-973)
+# ---------------------------------------------------------------------------
+def approx_zero(d: np.ndarray) -> np.ndarray:
+    """approx_zero (auxiliaryRoutines.f90:553-565)."""
+    return np.where(d == 0.0, 1e-50, d)
+
+
+def compute_limiters(vc, vm, vp, vpp, vmm, cxp, cxm, cyp, cym, czp, czm, scheme: int):
+    """compute_limiters (momentumEqn.f90:611-663) with the limiters of :667-734:
+    0 central, 1 upwind, 2 QUICK, 3 van Leer, 4 superbee, 5 superbee where the
+    volume fraction varies (dc > epsilon in any direction), central elsewhere."""
+    if scheme == 0:
+        one = np.ones_like(vc)
+        return one, one, one, one
+    if scheme == 1:
+        z = np.zeros_like(vc)
+        return z, z, z, z
+    rs = [(vc - vm) / approx_zero(vp - vc), (vpp - vp) / approx_zero(vp - vc),
+          (vm - vmm) / approx_zero(vc - vm), (vp - vc) / approx_zero(vc - vm)]
+
+    def quick(r):
+        return (r + 3.0) / 4.0
+
+    def vanleer(r):
+        r = np.maximum(0.0, r)
+        return (r + np.abs(r)) / (1.0 + np.abs(r))
+
+    def superbee(r):
+        r = np.maximum(0.0, r)
+        return np.maximum(np.maximum(0.0, np.minimum(2.0 * r, 1.0)), np.minimum(r, 2.0))
+
+    if scheme == 2:
+        return tuple(quick(r) for r in rs)
+    if scheme == 3:
+        return tuple(vanleer(r) for r in rs)
+    if scheme == 4:
+        return tuple(superbee(r) for r in rs)
+    if scheme == 5:
+        small = EPS64
+        sharp = ((cxp - cxm) > small) | ((cyp - cym) > small) | ((czp - czm) > small)
+        return tuple(np.where(sharp, superbee(r), 1.0) for r in rs)
+    raise ValueError(f"unknown convection scheme {scheme}")
+
+
+def _flux(q, a, b, psi_up, psi_um):
+    """F = max(q,0)*A + min(q,0)*B with A = a + psi_up/2 (b - a), B = b + psi_um/2 (a - b)."""
+    A = a + 0.5 * psi_up * (b - a)
+    B = b + 0.5 * psi_um * (a - b)
+    return np.maximum(q, 0.0) * A + np.minimum(q, 0.0) * B
+
+
+def momentum_fluxes(mesh: Mesh, ux: FField, uy: FField, uz: FField, c: FField, mu: FField, rho: FField,
+                    scheme: int):
+    """updateConveDiff (momentumEqn.f90:198-607): the convection + diffusion
+    fluxes phiX, phiY, phiZ on the equation bounds of setEqnBounds (:1134-1190)
+    for the channel: ux i=0..nx, uy j=1..ny-1 (fixed walls), uz k=0..nz.
+    Returns dense (k, j, i) arrays."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    out = []
+    for comp, (i0, i1, j0, j1, k0, k1) in enumerate([(0, nx, 1, ny, 1, nz), (1, nx, 1, ny - 1, 1, nz),
+                                                     (1, nx, 1, ny, 0, nz)]):
+        S = lambda f, di=0, dj=0, dk=0: f.v(i0 + di, i1 + di, j0 + dj, j1 + dj, k0 + dk, k1 + dk)  # noqa: E731
+        X = lambda a, d=0: a.r(i0 + d, i1 + d)[None, None, :]  # noqa: E731
+        Y = lambda a, d=0: a.r(j0 + d, j1 + d)[None, :, None]  # noqa: E731
+        Z = lambda a, d=0: a.r(k0 + d, k1 + d)[:, None, None]  # noqa: E731
+        if comp == 0:
+            u = ux
+            cl = (S(c, 1), S(c), S(c, 0, 1), S(c, 0, -1), S(c, 0, 0, 1), S(c, 0, 0, -1))
+        elif comp == 1:
+            u = uy
+            cl = (S(c, 1), S(c, -1), S(c, 0, 1), S(c), S(c, 0, 0, 1), S(c, 0, 0, -1))
+        else:
+            u = uz
+            cl = (S(c, 1), S(c, -1), S(c, 0, 1), S(c, 0, -1), S(c, 0, 0, 1), S(c))
+        U = lambda di=0, dj=0, dk=0: S(u, di, dj, dk)  # noqa: E731
+
+        def lim(d):
+            e = [(1 if d == n else 0) for n in range(3)]
+            p = lambda s: U(*[s * x for x in e])  # noqa: E731
+            return compute_limiters(U(), p(-1), p(1), p(2), p(-2), *cl, scheme)
+
+        phi = np.zeros_like(U())
+        # --- convection
+        if comp == 0:
+            l = lim(0)
+            qp, qm = 0.5 * (U() + U(1)), 0.5 * (U() + U(-1))
+            phi = phi - (_flux(qp, U(), U(1), l[0], l[1]) - _flux(qm, U(-1), U(), l[2], l[3])) / X(mesh.dxc, 1)
+            l = lim(1)
+            qp, qm = 0.5 * (S(uy, 1) + S(uy)), 0.5 * (S(uy, 1, -1) + S(uy, 0, -1))
+            phi = phi - (_flux(qp, U(), U(0, 1), l[0], l[1]) - _flux(qm, U(0, -1), U(), l[2], l[3])) / Y(mesh.dyf)
+            l = lim(2)
+            qp, qm = 0.5 * (S(uz) + S(uz, 1)), 0.5 * (S(uz, 0, 0, -1) + S(uz, 1, 0, -1))
+            phi = phi - (_flux(qp, U(), U(0, 0, 1), l[0], l[1]) - _flux(qm, U(0, 0, -1), U(), l[2], l[3])) / Z(mesh.dzf)
+        elif comp == 1:
+            l = lim(0)
+            qp = 0.5 * (S(ux, 0, 1) * Y(mesh.dyf, 1) + S(ux) * Y(mesh.dyf)) / Y(mesh.dyc, 1)
+            qm = 0.5 * (S(ux, -1, 1) * Y(mesh.dyf, 1) + S(ux, -1) * Y(mesh.dyf)) / Y(mesh.dyc, 1)
+            phi = phi - (_flux(qp, U(), U(1), l[0], l[1]) - _flux(qm, U(-1), U(), l[2], l[3])) / X(mesh.dxf)
+            l = lim(1)
+            qp, qm = 0.5 * (U() + U(0, 1)), 0.5 * (U() + U(0, -1))
+            phi = phi - (_flux(qp, U(), U(0, 1), l[0], l[1]) - _flux(qm, U(0, -1), U(), l[2], l[3])) / Y(mesh.dyc, 1)
+            l = lim(2)
+            qp = 0.5 * (S(uz, 0, 1) * Y(mesh.dyf, 1) + S(uz) * Y(mesh.dyf)) / Y(mesh.dyc, 1)
+            qm = 0.5 * (S(uz, 0, 1, -1) * Y(mesh.dyf, 1) + S(uz, 0, 0, -1) * Y(mesh.dyf)) / Y(mesh.dyc, 1)
+            phi = phi - (_flux(qp, U(), U(0, 0, 1), l[0], l[1]) - _flux(qm, U(0, 0, -1), U(), l[2], l[3])) / Z(mesh.dzf)
+        else:
+            l = lim(0)
+            qp, qm = 0.5 * (S(ux) + S(ux, 0, 0, 1)), 0.5 * (S(ux, -1) + S(ux, -1, 0, 1))
+            phi = phi - (_flux(qp, U(), U(1), l[0], l[1]) - _flux(qm, U(-1), U(), l[2], l[3])) / X(mesh.dxf)
+            l = lim(1)
+            qp, qm = 0.5 * (S(uy) + S(uy, 0, 0, 1)), 0.5 * (S(uy, 0, -1) + S(uy, 0, -1, 1))
+            phi = phi - (_flux(qp, U(), U(0, 1), l[0], l[1]) - _flux(qm, U(0, -1), U(), l[2], l[3])) / Y(mesh.dyf)
+            l = lim(2)
+            qp, qm = 0.5 * (U() + U(0, 0, 1)), 0.5 * (U() + U(0, 0, -1))
+            phi = phi - (_flux(qp, U(), U(0, 0, 1), l[0], l[1]) - _flux(qm, U(0, 0, -1), U(), l[2], l[3])) / Z(mesh.dzc, 1)
+        # --- diffusion
+        M = lambda di=0, dj=0, dk=0: S(mu, di, dj, dk)  # noqa: E731
+        if comp == 0:
+            mur, mul = M(1), M()
+            dxx = (mur * (U(1) - U()) / X(mesh.dxf, 1) - mul * (U() - U(-1)) / X(mesh.dxf)) / X(mesh.dxc, 1)
+            dxxt = dxx
+            mur = 0.25 * (M(1) + M() + M(1, 1) + M(0, 1))
+            mul = 0.25 * (M(1) + M() + M(1, -1) + M(0, -1))
+            dyy = (mur * (U(0, 1) - U()) / Y(mesh.dyc, 1) - mul * (U() - U(0, -1)) / Y(mesh.dyc)) / Y(mesh.dyf)
+            dyyt = (mur * (S(uy, 1) - S(uy)) / X(mesh.dxc, 1) - mul * (S(uy, 1, -1) - S(uy, 0, -1)) / X(mesh.dxc, 1)) / Y(mesh.dyf)
+            mur = 0.25 * (M(1) + M() + M(1, 0, 1) + M(0, 0, 1))
+            mul = 0.25 * (M(1) + M() + M(1, 0, -1) + M(0, 0, -1))
+            dzz = (mur * (U(0, 0, 1) - U()) / Z(mesh.dzc, 1) - mul * (U() - U(0, 0, -1)) / Z(mesh.dzc)) / Z(mesh.dzf)
+            dzzt = (mur * (S(uz, 1) - S(uz)) / X(mesh.dxc, 1) - mul * (S(uz, 1, 0, -1) - S(uz, 0, 0, -1)) / X(mesh.dxc, 1)) / Z(mesh.dzf)
+            invrho = 0.5 * (1.0 / S(rho, 1) + 1.0 / S(rho))
+        elif comp == 1:
+            mur = 0.25 * (M() + M(1) + M(0, 1) + M(1, 1))
+            mul = 0.25 * (M() + M(-1) + M(0, 1) + M(-1, 1))
+            dxx = (mur * (U(1) - U()) / X(mesh.dxc, 1) - mul * (U() - U(-1)) / X(mesh.dxc)) / X(mesh.dxf)
+            dxxt = (mur * (S(ux, 0, 1) - S(ux)) / Y(mesh.dyc, 1) - mul * (S(ux, -1, 1) - S(ux, -1)) / Y(mesh.dyc, 1)) / X(mesh.dxf)
+            mur, mul = M(0, 1), M()
+            dyy = (mur * (U(0, 1) - U()) / Y(mesh.dyf, 1) - mul * (U() - U(0, -1)) / Y(mesh.dyf)) / Y(mesh.dyc, 1)
+            dyyt = dyy
+            mur = 0.25 * (M() + M(0, 0, 1) + M(0, 1) + M(0, 1, 1))
+            mul = 0.25 * (M() + M(0, 0, -1) + M(0, 1) + M(0, 1, -1))
+            dzz = (mur * (U(0, 0, 1) - U()) / Z(mesh.dzc, 1) - mul * (U() - U(0, 0, -1)) / Z(mesh.dzc)) / Z(mesh.dzf)
+            dzzt = (mur * (S(uz, 0, 1) - S(uz)) / Y(mesh.dyc, 1) - mul * (S(uz, 0, 1, -1) - S(uz, 0, 0, -1)) / Y(mesh.dyc, 1)) / Z(mesh.dzf)
+            invrho = 0.5 * (1.0 / S(rho, 0, 1) + 1.0 / S(rho))
+        else:
+            mur = 0.25 * (M() + M(0, 0, 1) + M(1) + M(1, 0, 1))
+            mul = 0.25 * (M() + M(0, 0, 1) + M(-1) + M(-1, 0, 1))
+            dxx = (mur * (U(1) - U()) / X(mesh.dxc, 1) - mul * (U() - U(-1)) / X(mesh.dxc)) / X(mesh.dxf)
+            dxxt = (mur * (S(ux, 0, 0, 1) - S(ux)) / Z(mesh.dzc, 1) - mul * (S(ux, -1, 0, 1) - S(ux, -1)) / Z(mesh.dzc, 1)) / X(mesh.dxf)
+            mur = 0.25 * (M() + M(0, 0, 1) + M(0, 1) + M(0, 1, 1))
+            mul = 0.25 * (M() + M(0, 0, 1) + M(0, -1) + M(0, -1, 1))
+            dyy = (mur * (U(0, 1) - U()) / Y(mesh.dyc, 1) - mul * (U() - U(0, -1)) / Y(mesh.dyc)) / Y(mesh.dyf)
+            dyyt = (mur * (S(uy, 0, 0, 1) - S(uy)) / Z(mesh.dzc, 1) - mul * (S(uy, 0, -1, 1) - S(uy, 0, -1)) / Z(mesh.dzc, 1)) / Y(mesh.dyf)
+            mur, mul = M(0, 0, 1), M()
+            dzz = (mur * (U(0, 0, 1) - U()) / Z(mesh.dzf, 1) - mul * (U() - U(0, 0, -1)) / Z(mesh.dzf)) / Z(mesh.dzc, 1)
+            dzzt = dzz
+            invrho = 0.5 * (1.0 / S(rho, 0, 0, 1) + 1.0 / S(rho))
+        phi = phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho
+        out.append(phi)
+    return tuple(out)
+
+
+def momentum_predictor(mesh: Mesh, ux: FField, uy: FField, uz: FField, c: FField, mu: FField, rho: FField,
+                       phi_prev, dt: float, alpha: float, gamma: float, xi: float, rho0: float,
+                       gch: float = 0.0, g: float = 0.0, fs: float = 0.0, st=None, scheme: int = 2):
+    """solveMomentumEqn FAST (momentumEqn.f90:161-194) without the closing
+    updateBoundariesV: the new fluxes from u, then u += dt*(gamma*phi + xi*phi_prev)
+    (addConvDiff :738-791) and the sources of addSource (:874-973):
+    ux += r/rho0 st_x + invrho_x r fs + r gCH, uy += r/rho0 st_y + r g,
+    uz += r/rho0 st_z, r = dt*alpha.  Updates u in place; returns the new fluxes
+    (the next call's phi_prev)."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    phi = momentum_fluxes(mesh, ux, uy, uz, c, mu, rho, scheme)
+    boxes = [(0, nx, 1, ny, 1, nz), (1, nx, 1, ny - 1, 1, nz), (1, nx, 1, ny, 0, nz)]
+    r = dt * alpha
+    invrho0 = 1.0 / rho0
+    for d, (u, (i0, i1, j0, j1, k0, k1)) in enumerate(zip((ux, uy, uz), boxes)):
+        t = u.v(i0, i1, j0, j1, k0, k1)
+        t[...] = t + dt * (gamma * phi[d] + xi * phi_prev[d])
+    for d, (u, (i0, i1, j0, j1, k0, k1)) in enumerate(zip((ux, uy, uz), boxes)):
+        t = u.v(i0, i1, j0, j1, k0, k1)
+        s = st[d].v(i0, i1, j0, j1, k0, k1) if st is not None else 0.0
+        if d == 0:
+            invrho = 0.5 * (1.0 / rho.v(i0 + 1, i1 + 1, j0, j1, k0, k1) + 1.0 / rho.v(i0, i1, j0, j1, k0, k1))
+            t[...] = t + invrho0 * r * s + invrho * r * fs + r * gch
+        elif d == 1:
+            t[...] = t + invrho0 * r * s + r * g
+        else:
+            t[...] = t + invrho0 * r * s
+    return phi

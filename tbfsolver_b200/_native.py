@@ -63,6 +63,11 @@ class TbfpVofDesc(C.Structure):
                 ("mug", C.c_double)]
 
 
+class TbfpMomentumDesc(C.Structure):
+    _fields_ = [("scheme", C.c_int), ("gch", C.c_double), ("g", C.c_double)] + [
+        (n, C.c_void_p) for n in ("dxf", "dxc", "dyf", "dyc", "dzf", "dzc")]
+
+
 class TbfpMemberIO(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("ux_in", "uy_in", "uz_in", "ux_out", "uy_out", "uz_out", "rho", "psi_n",
                                            "psi_nm1", "psi")]
@@ -105,6 +110,10 @@ PROTOTYPES = {
                                                C.POINTER(TbfpStats)]),
     "tbfp_pcg_setup": (C.c_int, [_H, C.POINTER(TbfpMgParams)]),
     "tbfp_vof_setup": (C.c_int, [_H, C.POINTER(TbfpVofDesc)]),
+    "tbfp_momentum_setup": (C.c_int, [_H, C.POINTER(TbfpMomentumDesc)]),
+    "tbfp_momentum_fluxes": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "tbfp_momentum_predictor": (C.c_int, [_H] + [C.c_void_p] * 7 + [C.c_double] * 6),
+    "tbfp_momentum_predictor_dev": (C.c_int, [_H] + [C.c_void_p] * 7 + [C.c_double] * 6),
     "tbfp_material_props": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tbfp_material_props_dev": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tbfp_pcg_solve": (C.c_int, [_H, _P, _P, _P, C.POINTER(TbfpStats)]),

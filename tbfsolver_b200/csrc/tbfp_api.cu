@@ -69,6 +69,15 @@ struct tbfp_handle {
   double *d_qv = nullptr;                     // vertex scratch, (nx+1)(ny+1)(nz+1)
   double rhol = 0.0, rhog = 0.0, mul = 0.0, mug = 0.0;
   double *h_vof[4] = {nullptr, nullptr, nullptr, nullptr};  // c, cs, rho, mu for tbfp_material_props
+  // momentum predictor (tbfp_momentum_setup)
+  bool mom = false;
+  int mom_scheme = 2;
+  double mom_gch = 0.0, mom_g = 0.0;
+  MomentumTabs mt{};
+  double *d_phi[2][3] = {};  // flux history: [cur][component], swapped per call
+  int phi_cur = 0;
+  size_t n_phi[3] = {0, 0, 0};
+  double *h_mom[2] = {nullptr, nullptr};  // c, mu copies for tbfp_momentum_predictor
   MgSolver *mg = nullptr;   // MG_MODE hierarchy (tbfp_pcg_setup)
   std::vector<double> mdxf, mdxc, mdyf, mdyc, mdzf, mdzc;  // caller's metrics, kept for tbfp_pcg_setup
   double *h_beta = nullptr, *h_q = nullptr;                // device copies for tbfp_pcg_solve
@@ -1125,6 +1134,119 @@ int tbfp_material_props(tbfp_handle *h, const double *c, double *cs, double *rho
     return rc;
   TBFP_CK(h, cudaStreamSynchronize(h->stream));
   return finish(h, "tbfp_material_props");
+}
+
+// ---------------------------------------------------------------------------
+// solveMomentumEqn FAST (momentumEqn.f90:161-194)
+// ---------------------------------------------------------------------------
+int tbfp_momentum_setup(tbfp_handle *h, const tbfp_momentum_desc *m) {
+  if (!h || !m) return TBFP_ENULL;
+  if (h->slab) return set_err(h, TBFP_EINVAL, "tbfp_momentum_setup: needs a whole-channel handle");
+  if (h->mom) return set_err(h, TBFP_EINVAL, "tbfp_momentum_setup: already set up for this handle");
+  if (m->scheme < 0 || m->scheme > 5) return set_err(h, TBFP_EINVAL, "tbfp_momentum_setup: scheme must be 0..5");
+  if (h->hd_u < 2 || h->hd_rho < 1)
+    return set_err(h, TBFP_EINVAL, "tbfp_momentum_setup: needs hd_u >= 2 and hd_rho >= 1");
+  if (!m->dxf || !m->dxc || !m->dyf || !m->dyc || !m->dzf || !m->dzc)
+    return set_err(h, TBFP_ENULL, "tbfp_momentum_setup: a spacing table is NULL");
+  const int nx = h->nx, ny = h->ny, nz = h->nz;
+  // spacings by Fortran index 0..n+1, as the mesh holds them
+  std::vector<double> dxf(m->dxf, m->dxf + nx + 2), dxc(m->dxc, m->dxc + nx + 2);
+  std::vector<double> dyf(m->dyf, m->dyf + ny + 2), dyc(m->dyc, m->dyc + ny + 2);
+  std::vector<double> dzf(m->dzf, m->dzf + nz + 2), dzc(m->dzc, m->dzc + nz + 2);
+  cudaSetDevice(h->device);
+  double *d[6];
+  int rc;
+  const std::vector<double> *tabs[6] = {&dxf, &dxc, &dyf, &dyc, &dzf, &dzc};
+  for (int e = 0; e < 6; ++e)
+    if ((rc = upload(h, &d[e], *tabs[e]))) return rc;
+  h->mt = MomentumTabs{d[0], d[1], d[2], d[3], d[4], d[5]};
+  h->n_phi[0] = (size_t)(nx + 1) * ny * nz;
+  h->n_phi[1] = (size_t)nx * (ny - 1) * nz;
+  h->n_phi[2] = (size_t)nx * ny * (nz + 1);
+  for (int b = 0; b < 2; ++b)
+    for (int c = 0; c < 3; ++c) {
+      if ((rc = dev_alloc(h, &h->d_phi[b][c], h->n_phi[c]))) return rc;
+      TBFP_CK(h, cudaMemset(h->d_phi[b][c], 0, h->n_phi[c] * sizeof(double)));  // initFluxes
+    }
+  h->mom_scheme = m->scheme;
+  h->mom_gch = m->gch;
+  h->mom_g = m->g;
+  h->phi_cur = 0;
+  h->mom = true;
+  return TBFP_OK;
+}
+
+int tbfp_momentum_fluxes(tbfp_handle *h, double *phi_x, double *phi_y, double *phi_z, int set) {
+  int rc = check_ptrs(h, {phi_x, phi_y, phi_z});
+  if (rc) return rc;
+  if (!h->mom) return set_err(h, TBFP_EINVAL, "tbfp_momentum_fluxes: call tbfp_momentum_setup first");
+  cudaSetDevice(h->device);
+  double *host[3] = {phi_x, phi_y, phi_z};
+  for (int c = 0; c < 3; ++c) {
+    if (set) rc = h2d(h, h->d_phi[h->phi_cur][c], host[c], h->n_phi[c]);
+    else rc = d2h(h, host[c], h->d_phi[h->phi_cur][c], h->n_phi[c]);
+    if (rc) return rc;
+  }
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return TBFP_OK;
+}
+
+int tbfp_momentum_predictor_dev(tbfp_handle *h, double *ux, double *uy, double *uz, const double *c,
+                                const double *mu, const double *rho, const double *const *st, double dt,
+                                double alpha, double gamma, double xi, double rho0, double fs) {
+  int rc = check_ptrs(h, {ux, uy, uz, c, mu, rho});
+  if (rc) return rc;
+  if (!h->mom) return set_err(h, TBFP_EINVAL, "tbfp_momentum_predictor: call tbfp_momentum_setup first");
+  if (st && (!st[0] || !st[1] || !st[2]))
+    return set_err(h, TBFP_ENULL, "tbfp_momentum_predictor: a surface-tension component pointer is NULL");
+  if (!(dt > 0.0) || !(rho0 > 0.0))
+    return set_err(h, TBFP_EINVAL, "tbfp_momentum_predictor: dt and rho0 must be positive");
+  cudaSetDevice(h->device);
+  // copyOldFluxes + resetFluxes: the previous fluxes stay where they are and
+  // the new ones go to the other buffer
+  const int prev = h->phi_cur, cur = 1 - h->phi_cur;
+  double *const phi[3] = {h->d_phi[cur][0], h->d_phi[cur][1], h->d_phi[cur][2]};
+  const double *const pp[3] = {h->d_phi[prev][0], h->d_phi[prev][1], h->d_phi[prev][2]};
+  launch_momentum(h->mt, ux, uy, uz, c, mu, rho, st, h->Lux, h->Luy, h->Luz, h->Lrho, h->Lst, phi, pp, h->nx, h->ny,
+                  h->nz, h->mom_scheme, dt, alpha, gamma, xi, rho0, fs, h->mom_gch, h->mom_g, h->stream);
+  h->phi_cur = cur;
+  return finish(h, "tbfp_momentum_predictor");
+}
+
+int tbfp_momentum_predictor(tbfp_handle *h, double *ux, double *uy, double *uz, const double *c, const double *mu,
+                            const double *rho, const double *const *st, double dt, double alpha, double gamma,
+                            double xi, double rho0, double fs) {
+  int rc = check_ptrs(h, {ux, uy, uz, c, mu, rho});
+  if (rc) return rc;
+  if (!h->mom) return set_err(h, TBFP_EINVAL, "tbfp_momentum_predictor: call tbfp_momentum_setup first");
+  if (st && (!st[0] || !st[1] || !st[2]))
+    return set_err(h, TBFP_ENULL, "tbfp_momentum_predictor: a surface-tension component pointer is NULL");
+  cudaSetDevice(h->device);
+  const bool has_st = st != nullptr;
+  if ((rc = ensure_host_bufs(h, has_st))) return rc;
+  for (double *&b : h->h_mom)
+    if (!b && (rc = dev_alloc(h, &b, h->n_rho))) return rc;
+  if ((rc = h2d(h, h->h_ux, ux, h->n_ux)) || (rc = h2d(h, h->h_uy, uy, h->n_uy)) ||
+      (rc = h2d(h, h->h_uz, uz, h->n_uz)) || (rc = h2d(h, h->h_rho, rho, h->n_rho)) ||
+      (rc = h2d(h, h->h_mom[0], c, h->n_rho)) || (rc = h2d(h, h->h_mom[1], mu, h->n_rho)))
+    return rc;
+  const double *dst[3] = {nullptr, nullptr, nullptr};
+  if (has_st) {
+    for (int e = 0; e < 3; ++e) {
+      if ((rc = h2d(h, h->h_st[e], st[e], h->n_st[e]))) return rc;
+      dst[e] = h->h_st[e];
+    }
+  }
+  const int flags = h->flags;
+  h->flags |= TBFP_FLAG_ASYNC;
+  rc = tbfp_momentum_predictor_dev(h, h->h_ux, h->h_uy, h->h_uz, h->h_mom[0], h->h_mom[1], h->h_rho,
+                                   has_st ? dst : nullptr, dt, alpha, gamma, xi, rho0, fs);
+  h->flags = flags;
+  if (rc) return rc;
+  if ((rc = d2h(h, ux, h->h_ux, h->n_ux)) || (rc = d2h(h, uy, h->h_uy, h->n_uy)) || (rc = d2h(h, uz, h->h_uz, h->n_uz)))
+    return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return finish(h, "tbfp_momentum_predictor");
 }
 
 int tbfp_pcg_setup(tbfp_handle *h, const tbfp_mg_params *p) {

@@ -220,6 +220,20 @@ void launch_material_props_fused(const VofSep &w, const double *c, double *cs, d
                                  Lay L, int nx, int ny, int nz, double rhol, double rhog, double mul, double mug,
                                  cudaStream_t st);
 
+// Momentum predictor (tbfp_momentum.cu).  Spacings indexed by the Fortran
+// index: dxf, dxc, dzf, dzc over 0..n+1 (x and z periodic), dyf over 1..ny and
+// dyc over 1..ny+1 (tables of ny+2 entries).
+struct MomentumTabs {
+  const double *dxf, *dxc, *dyf, *dyc, *dzf, *dzc;
+};
+// phi: the new fluxes (written), prev: the previous call's; dense over the
+// equation boxes ux (0:nx,1:ny,1:nz), uy (1:nx,1:ny-1,1:nz), uz (1:nx,1:ny,0:nz)
+void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, const double *c, const double *mu,
+                     const double *rho, const double *const *st, Lay Lux, Lay Luy, Lay Luz, Lay Lc, const Lay *Lst,
+                     double *const phi[3], const double *const prev[3], int nx, int ny, int nz, int scheme, double dt,
+                     double alpha, double gamma, double xi, double rho0, double fs, double gch, double g,
+                     cudaStream_t st_);
+
 // MG_MODE source/beta (computeSource MG, computeBeta) and addPressureGrad.
 // idxc, idzc: 1/dxc(i), 1/dzc(k) for Fortran i = 1..nx+1 (0-based tables).
 void launch_mg_source_beta(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz,

@@ -31,7 +31,7 @@ import numpy as np
 
 from ._native import (TBFP_EINVAL, TBFP_FLAG_ASYNC, TBFP_FLAG_RESIDUAL, TBFP_FLAG_TIMING, TBFP_FP64, TBFP_MIXED,
                       TbfpDesc, TbfpError, TbfpMemberIO, TbfpMgParams, TbfpStats,
-                      TbfpVofDesc, check, load)
+                      TbfpMomentumDesc, TbfpVofDesc, check, load)
 from .fields import Field, VField
 from .grid import Grid
 
@@ -272,6 +272,64 @@ class VOF:
         dev = _placement([c, cs, rho, mu])
         fn = sv.lib.tbfp_material_props_dev if dev else sv.lib.tbfp_material_props
         check(fn(sv.h, c.address(), cs.address(), rho.address(), mu.address()), sv.h)
+
+
+class MomentumEqn:
+    """The momentum predictor of FAST_MODE (momentumEqnCTOR, momentumEqn.f90:98-157;
+    solveMomentumEqn :161-194 without its closing updateBoundariesV) on a
+    solver's handle.  The flux history (phi of the last step, for AB2) lives in
+    the library; fluxes() / set_fluxes() read and load it (printOldTimeFlux /
+    initOldTimeFlux)."""
+
+    def __init__(self, solver: FastPoissonSolver, scheme: int = 2, gch: float = 0.0, g: float = 0.0):
+        self.solver = solver
+        g_ = solver.mesh
+        self._t = {n: np.ascontiguousarray(getattr(g_, n).r(0, nn + 1))
+                   for n, nn in (("dxf", g_.nx), ("dxc", g_.nx), ("dyf", g_.ny), ("dyc", g_.ny), ("dzf", g_.nz),
+                                 ("dzc", g_.nz))}
+        m = TbfpMomentumDesc(scheme=scheme, gch=gch, g=g, **{n: a.ctypes.data_as(C.c_void_p).value
+                                                             for n, a in self._t.items()})
+        check(solver.lib.tbfp_momentum_setup(solver.h, C.byref(m)), solver.h)
+
+    @classmethod
+    def from_specs(cls, solver: FastPoissonSolver, specs_dir: str) -> "MomentumEqn":
+        """Settings read as momentumEqnCTOR reads them: convection_scheme from
+        specs/schemes, g and gCH from specs/parameters."""
+        from .io import ParFile  # noqa: PLC0415
+
+        par = ParFile("parameters", specs_dir)
+        return cls(solver, scheme=ParFile("schemes", specs_dir).read_int("convection_scheme"),
+                   gch=par.read_real("gCH"), g=par.read_real("g"))
+
+    def _shapes(self):
+        m = self.solver.mesh
+        return [(m.nz, m.ny, m.nx + 1), (m.nz, m.ny - 1, m.nx), (m.nz + 1, m.ny, m.nx)]
+
+    def fluxes(self):
+        """The fluxes of the last step (phi_x, phi_y, phi_z) over the equation boxes."""
+        out = [np.zeros(s) for s in self._shapes()]
+        sv = self.solver
+        check(sv.lib.tbfp_momentum_fluxes(sv.h, *[a.ctypes.data_as(C.c_void_p) for a in out], 0), sv.h)
+        return tuple(out)
+
+    def set_fluxes(self, phi) -> None:
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in phi]
+        for a, s in zip(arrs, self._shapes()):
+            if a.shape != s:
+                raise TbfpError(TBFP_EINVAL, f"flux array of shape {a.shape}, expected {s}")
+        sv = self.solver
+        check(sv.lib.tbfp_momentum_fluxes(sv.h, *[a.ctypes.data_as(C.c_void_p) for a in arrs], 1), sv.h)
+
+    def predictor(self, u: VField, c: Field, mu: Field, rho: Field, dt: float, alpha: float, gamma: float,
+                  xi: float, rho0: float, fs: float = 0.0, st=None) -> None:
+        """solveMomentumEqn FAST: u (in place) <- u + dt*(gamma*phi + xi*phi_prev) + sources."""
+        sv = self.solver
+        fields = [*u.components(), c, mu, rho] + list(st or [])
+        dev = _placement(fields)
+        s = _PtrTriple(st)
+        fn = sv.lib.tbfp_momentum_predictor_dev if dev else sv.lib.tbfp_momentum_predictor
+        check(fn(sv.h, u.ux.address(), u.uy.address(), u.uz.address(), c.address(), mu.address(), rho.address(),
+                 s.addr, dt, alpha, gamma, xi, rho0, fs), sv.h)
 
 
 class PCG:
