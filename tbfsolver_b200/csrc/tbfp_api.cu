@@ -1154,12 +1154,18 @@ int tbfp_momentum_setup(tbfp_handle *h, const tbfp_momentum_desc *m) {
   std::vector<double> dyf(m->dyf, m->dyf + ny + 2), dyc(m->dyc, m->dyc + ny + 2);
   std::vector<double> dzf(m->dzf, m->dzf + nz + 2), dzc(m->dzc, m->dzc + nz + 2);
   cudaSetDevice(h->device);
-  double *d[6];
+  // the kernel multiplies by reciprocals, each the correctly rounded 1/d
+  auto recip = [](const std::vector<double> &v) {
+    std::vector<double> r(v.size());
+    for (size_t e = 0; e < v.size(); ++e) r[e] = 1.0 / v[e];
+    return r;
+  };
+  const std::vector<double> tabs[7] = {dyf, recip(dxf), recip(dxc), recip(dyf), recip(dyc), recip(dzf), recip(dzc)};
+  double *d[7];
   int rc;
-  const std::vector<double> *tabs[6] = {&dxf, &dxc, &dyf, &dyc, &dzf, &dzc};
-  for (int e = 0; e < 6; ++e)
-    if ((rc = upload(h, &d[e], *tabs[e]))) return rc;
-  h->mt = MomentumTabs{d[0], d[1], d[2], d[3], d[4], d[5]};
+  for (int e = 0; e < 7; ++e)
+    if ((rc = upload(h, &d[e], tabs[e]))) return rc;
+  h->mt = MomentumTabs{d[0], d[1], d[2], d[3], d[4], d[5], d[6]};
   h->n_phi[0] = (size_t)(nx + 1) * ny * nz;
   h->n_phi[1] = (size_t)nx * (ny - 1) * nz;
   h->n_phi[2] = (size_t)nx * ny * (nz + 1);

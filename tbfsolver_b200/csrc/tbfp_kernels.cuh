@@ -223,8 +223,9 @@ void launch_material_props_fused(const VofSep &w, const double *c, double *cs, d
 // Momentum predictor (tbfp_momentum.cu).  Spacings indexed by the Fortran
 // index: dxf, dxc, dzf, dzc over 0..n+1 (x and z periodic), dyf over 1..ny and
 // dyc over 1..ny+1 (tables of ny+2 entries).
+// dyf and the reciprocals of every spacing, Fortran index 0..n+1 -> [index]
 struct MomentumTabs {
-  const double *dxf, *dxc, *dyf, *dyc, *dzf, *dzc;
+  const double *dyf, *rdxf, *rdxc, *rdyf, *rdyc, *rdzf, *rdzc;
 };
 // phi: the new fluxes (written), prev: the previous call's; dense over the
 // equation boxes ux (0:nx,1:ny,1:nz), uy (1:nx,1:ny-1,1:nz), uz (1:nx,1:ny,0:nz)
