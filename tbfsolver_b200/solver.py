@@ -320,6 +320,40 @@ class MomentumEqn:
         sv = self.solver
         check(sv.lib.tbfp_momentum_fluxes(sv.h, *[a.ctypes.data_as(C.c_void_p) for a in arrs], 1), sv.h)
 
+    def _boxes(self):
+        m = self.solver.mesh
+        return [(0, m.nx, 1, m.ny, 1, m.nz), (1, m.nx, 1, m.ny - 1, 1, m.nz), (1, m.nx, 1, m.ny, 0, m.nz)]
+
+    def write_old_time_flux(self, case_dir: str, n: int) -> None:
+        """printOldTimeFlux (momentumEqn.f90:1279-1290): the flux history as the
+        vector field phi0 of time folder n (files phi0x, phi0y, phi0z in the
+        field format), the equation boxes filled and the uy wall faces zero (phi0
+        is created zeroed, initOpt=-1)."""
+        from . import io  # noqa: PLC0415
+
+        m = self.solver.mesh
+        for comp, kind, phi, b in zip("xyz", ("sx", "sy", "sz"), self.fluxes(), self._boxes()):
+            f = Field(kind, 1, m.nx, m.ny, m.nz)
+            f.v(*b)[...] = phi
+            io.write_field(case_dir, n, "phi0" + comp, f)
+
+    def read_old_time_flux(self, case_dir: str, n: int) -> None:
+        """initOldTimeFlux (momentumEqn.f90:1254-1275): phi0 of time folder n
+        into the flux history; a component file that is absent reads as zero
+        (readField_if_present, field.f90:308-326)."""
+        import os  # noqa: PLC0415
+
+        from . import io  # noqa: PLC0415
+
+        m = self.solver.mesh
+        hist = []
+        for comp, kind, b in zip("xyz", ("sx", "sy", "sz"), self._boxes()):
+            f = Field(kind, 1, m.nx, m.ny, m.nz)
+            if os.path.exists(io.field_path(case_dir, n, "phi0" + comp)):
+                io.read_field(case_dir, n, "phi0" + comp, f)
+            hist.append(np.ascontiguousarray(f.v(*b)))
+        self.set_fluxes(hist)
+
     def predictor(self, u: VField, c: Field, mu: Field, rho: Field, dt: float, alpha: float, gamma: float,
                   xi: float, rho0: float, fs: float = 0.0, st=None) -> None:
         """solveMomentumEqn FAST: u (in place) <- u + dt*(gamma*phi + xi*phi_prev) + sources."""

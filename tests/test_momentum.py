@@ -192,3 +192,30 @@ def test_flux_history_is_loaded_and_read_back():
         for f, f0, h, b in zip(du.components(), u, hist, boxes):
             got = Field(f.kind, f.hd, nx, ny, nz, _host(f)).v(*b)
             assert np.max(np.abs(got - (f0.v(*b) + dt * h))) <= 2.3e-16 * np.max(np.abs(got))
+
+
+@pytest.mark.gpu
+def test_flux_history_round_trips_through_phi0_files(tmp_path):
+    """printOldTimeFlux writes phi0x/y/z of the output folder in the field
+    format; initOldTimeFlux reads them back (an absent component as zero)."""
+    from tbfsolver_b200 import io
+
+    nx, ny, nz = 16, 12, 8
+    g = _grid(nx, ny, nz, True)
+    rng = np.random.default_rng(11)
+    with FastPoissonSolver(g) as fps:
+        mom = MomentumEqn(fps, scheme=2)
+        hist = [rng.standard_normal(s) for s in mom._shapes()]
+        mom.set_fluxes(hist)
+        mom.write_old_time_flux(str(tmp_path), 7)
+    fy = Field("sy", 1, nx, ny, nz)
+    io.read_field(str(tmp_path), 7, "phi0y", fy)
+    assert np.array_equal(fy.v(1, nx, 1, ny - 1, 1, nz), hist[1])
+    assert not fy.v(1, nx, 0, 0, 1, nz).any() and not fy.v(1, nx, ny, ny, 1, nz).any()
+    (tmp_path / "7" / "phi0z").unlink()
+    with FastPoissonSolver(g) as fps:
+        mom = MomentumEqn(fps, scheme=2)
+        mom.read_old_time_flux(str(tmp_path), 7)
+        got = mom.fluxes()
+    assert np.array_equal(got[0], hist[0]) and np.array_equal(got[1], hist[1])
+    assert not got[2].any()
