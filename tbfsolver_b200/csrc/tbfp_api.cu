@@ -1214,7 +1214,8 @@ int tbfp_momentum_predictor_dev(tbfp_handle *h, double *ux, double *uy, double *
   double *const phi[3] = {h->d_phi[cur][0], h->d_phi[cur][1], h->d_phi[cur][2]};
   const double *const pp[3] = {h->d_phi[prev][0], h->d_phi[prev][1], h->d_phi[prev][2]};
   launch_momentum(h->mt, ux, uy, uz, c, mu, rho, st, h->Lux, h->Luy, h->Luz, h->Lrho, h->Lst, phi, pp, h->nx, h->ny,
-                  h->nz, h->mom_scheme, dt, alpha, gamma, xi, rho0, fs, h->mom_gch, h->mom_g, h->stream);
+                  h->nz, h->mom_scheme, dt, alpha, gamma, xi, rho0, fs, h->mom_gch, h->mom_g, h->hd_u, h->hd_rho,
+                  h->stream);
   h->phi_cur = cur;
   return finish(h, "tbfp_momentum_predictor");
 }

@@ -98,6 +98,10 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 constexpr int kNT = 256;  // threads per CTA of the transform kernels (8 warps)
@@ -232,8 +236,8 @@ struct MomentumTabs {
 void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, const double *c, const double *mu,
                      const double *rho, const double *const *st, Lay Lux, Lay Luy, Lay Luz, Lay Lc, const Lay *Lst,
                      double *const phi[3], const double *const prev[3], int nx, int ny, int nz, int scheme, double dt,
-                     double alpha, double gamma, double xi, double rho0, double fs, double gch, double g,
-                     cudaStream_t st_);
+                     double alpha, double gamma, double xi, double rho0, double fs, double gch, double g, int hdu,
+                     int hdc, cudaStream_t st_);
 
 // MG_MODE source/beta (computeSource MG, computeBeta) and addPressureGrad.
 // idxc, idzc: 1/dxc(i), 1/dzc(k) for Fortran i = 1..nx+1 (0-based tables).

@@ -71,6 +71,29 @@ __device__ __forceinline__ double flux(double q, double a, double b, double pu, 
   return fmax(q, 0.0) * A + fmin(q, 0.0) * B;
 }
 
+// Fp - Fm of one direction: the limited flux through the upper face (between
+// vc and vp) minus the one through the lower face (between vm and vc)
+// (momentumEqn.f90:240-256 and the like).  QUICK's limiter is psi = (r+3)/4
+// with r a ratio whose denominator is the face's own difference d, so the
+// flux's psi*d/2 is ((numerator) + 3d)/8 without the division; d == 0 keeps
+// the reference's value (approx_zero makes psi*d exactly 0 there).
+template <int S>
+__device__ __forceinline__ double conv_diff(double qp, double qm, double vmm, double vm, double vc, double vp,
+                                            double vpp, bool sh) {
+  if constexpr (S == 2) {
+    const double d = vp - vc, e = vc - vm;
+    const double Ap = d == 0.0 ? vc : vc + 0.125 * (e + 3.0 * d);
+    const double Bp = d == 0.0 ? vp : vp - 0.125 * ((vpp - vp) + 3.0 * d);
+    const double Am = e == 0.0 ? vm : vm + 0.125 * ((vm - vmm) + 3.0 * e);
+    const double Bm = e == 0.0 ? vc : vc - 0.125 * (d + 3.0 * e);
+    return (fmax(qp, 0.0) * Ap + fmin(qp, 0.0) * Bp) - (fmax(qm, 0.0) * Am + fmin(qm, 0.0) * Bm);
+  } else {
+    double ps[4];
+    limiters<S>(vc, vm, vp, vpp, vmm, sh, ps);
+    return flux(qp, vc, vp, ps[0], ps[1]) - flux(qm, vm, vc, ps[2], ps[3]);
+  }
+}
+
 struct MomArgs {
   const double *ux, *uy, *uz, *c, *mu, *rho;
   Lay Lux, Luy, Luz, Lc;  // c, mu, rho share Lc
@@ -78,6 +101,7 @@ struct MomArgs {
   const double *dyf, *rdxf, *rdxc, *rdyf, *rdyc, *rdzf, *rdzc;
   double *phx, *phy, *phz;  // fluxes, dense over the equation boxes
   int nx, ny, nz;
+  int hdu, hdc;  // halos of the velocity and cell arrays
 };
 
 __device__ __forceinline__ long box_x(const MomArgs &a, int i, int j, int k) {
@@ -90,50 +114,82 @@ __device__ __forceinline__ long box_z(const MomArgs &a, int i, int j, int k) {
   return ((long)k * a.ny + (j - 1)) * a.nx + (i - 1);
 }
 
-// Each field is read through a pointer to the thread's own element and 32-bit
-// strides: a neighbour costs one address computation per distinct (dj, dk)
-// and a load with an immediate i offset.  c, mu and rho share one layout.
-#define TBFP_MOM_ACCESSORS                                                                    \
-  const double *__restrict__ pU = a.ux + at(a.Lux, i, j, k);                                  \
-  const double *__restrict__ pV = a.uy + at(a.Luy, i, j, k);                                  \
-  const double *__restrict__ pW = a.uz + at(a.Luz, i, j, k);                                  \
-  const long oc = at(a.Lc, i, j, k);                                                          \
-  const double *__restrict__ pC = a.c + oc;                                                   \
-  const double *__restrict__ pM = a.mu + oc;                                                  \
-  const double *__restrict__ pR = a.rho + oc;                                                 \
-  const int uj = (int)a.Lux.sj, uk = (int)a.Lux.sk, vj = (int)a.Luy.sj, vk = (int)a.Luy.sk;   \
-  const int wj = (int)a.Luz.sj, wk = (int)a.Luz.sk, cj = (int)a.Lc.sj, ck = (int)a.Lc.sk;     \
-  auto u = [&](int di, int dj, int dk) { return __ldg(pU + (di + dj * uj + dk * uk)); };       \
-  auto v = [&](int di, int dj, int dk) { return __ldg(pV + (di + dj * vj + dk * vk)); };       \
-  auto w = [&](int di, int dj, int dk) { return __ldg(pW + (di + dj * wj + dk * wk)); };       \
-  auto c = [&](int di, int dj, int dk) { return __ldg(pC + (di + dj * cj + dk * ck)); };       \
-  auto m = [&](int di, int dj, int dk) { return __ldg(pM + (di + dj * cj + dk * ck)); };       \
-  auto rho = [&](int di, int dj, int dk) { return __ldg(pR + (di + dj * cj + dk * ck)); };     \
+// Two ways to reach a field's neighbours.  GAcc reads global memory through
+// a pointer to the thread's own element and 32-bit strides (one address per
+// distinct (dj, dk), an immediate i offset).  SAcc reads the shared-memory
+// plane rings of the tiled kernel: the thread's own element of ring slot 0
+// plus the offset of the slot holding plane k + dk.  c, mu and rho share one
+// layout.
+struct GAcc {
+  const double *__restrict__ pU;
+  const double *__restrict__ pV;
+  const double *__restrict__ pW;
+  const double *__restrict__ pC;
+  const double *__restrict__ pM;
+  const double *__restrict__ pR;
+  int uj, uk, vj, vk, wj, wk, cj, ck;
+  __device__ GAcc(const MomArgs &a, int i, int j, int k)
+      : pU(a.ux + at(a.Lux, i, j, k)), pV(a.uy + at(a.Luy, i, j, k)), pW(a.uz + at(a.Luz, i, j, k)),
+        pC(a.c + at(a.Lc, i, j, k)), pM(a.mu + at(a.Lc, i, j, k)), pR(a.rho + at(a.Lc, i, j, k)),
+        uj((int)a.Lux.sj), uk((int)a.Lux.sk), vj((int)a.Luy.sj), vk((int)a.Luy.sk), wj((int)a.Luz.sj),
+        wk((int)a.Luz.sk), cj((int)a.Lc.sj), ck((int)a.Lc.sk) {}
+  __device__ double u(int di, int dj, int dk) const { return __ldg(pU + (di + dj * uj + dk * uk)); }
+  __device__ double v(int di, int dj, int dk) const { return __ldg(pV + (di + dj * vj + dk * vk)); }
+  __device__ double w(int di, int dj, int dk) const { return __ldg(pW + (di + dj * wj + dk * wk)); }
+  __device__ double c(int di, int dj, int dk) const { return __ldg(pC + (di + dj * cj + dk * ck)); }
+  __device__ double m(int di, int dj, int dk) const { return __ldg(pM + (di + dj * cj + dk * ck)); }
+  __device__ double r(int di, int dj, int dk) const { return __ldg(pR + (di + dj * cj + dk * ck)); }
+};
+
+// tiled kernel geometry: a 32 x 8 tile of (i, j) columns marches up in k; the
+// velocity planes k-2..k+2 (in-plane halo 2) and the cell planes k-1..k+1
+// (halo 1) sit in rings of shared memory, the next plane loading meanwhile
+constexpr int kTX = 32, kTY = 8, kKC = 64;
+constexpr int kHV = 2, kHC = 1;
+constexpr int kPV = kTX + 2 * kHV, kPC = kTX + 2 * kHC;  // row pitches
+constexpr int kNV = kPV * (kTY + 2 * kHV), kNC = kPC * (kTY + 2 * kHC);  // doubles per plane
+constexpr int kRV = 6, kRC = 4;  // ring depths: 5 + 1 and 3 + 1 planes
+
+struct SAcc {
+  const double *sU, *sV, *sW, *sC, *sM, *sR;
+  int ov[5], oc[3];  // slot offsets of planes k-2..k+2 (velocity), k-1..k+1 (cell)
+  __device__ double u(int di, int dj, int dk) const { return sU[ov[dk + 2] + dj * kPV + di]; }
+  __device__ double v(int di, int dj, int dk) const { return sV[ov[dk + 2] + dj * kPV + di]; }
+  __device__ double w(int di, int dj, int dk) const { return sW[ov[dk + 2] + dj * kPV + di]; }
+  __device__ double c(int di, int dj, int dk) const { return sC[oc[dk + 1] + dj * kPC + di]; }
+  __device__ double m(int di, int dj, int dk) const { return sM[oc[dk + 1] + dj * kPC + di]; }
+  __device__ double r(int di, int dj, int dk) const { return sR[oc[dk + 1] + dj * kPC + di]; }
+};
+
+#define TBFP_MOM_ACCESSORS                                                       \
+  auto u = [&](int di, int dj, int dk) { return A.u(di, dj, dk); };              \
+  auto v = [&](int di, int dj, int dk) { return A.v(di, dj, dk); };              \
+  auto w = [&](int di, int dj, int dk) { return A.w(di, dj, dk); };              \
+  auto c = [&](int di, int dj, int dk) { return A.c(di, dj, dk); };              \
+  auto m = [&](int di, int dj, int dk) { return A.m(di, dj, dk); };              \
+  auto rho = [&](int di, int dj, int dk) { return A.r(di, dj, dk); };            \
   (void)c
 
 // updateConveDiff, x component at face (i, j, k) (momentumEqn.f90:228-341)
-template <int S>
-__device__ double phi_x(const MomArgs &a, int i, int j, int k) {
+template <int S, class Acc>
+__device__ __forceinline__ double phi_x(const Acc &A, const MomArgs &a, int i, int j, int k, double irc) {
   TBFP_MOM_ACCESSORS;
   const bool sh = sharp_cell<S>(c(1, 0, 0), c(0, 0, 0), c(0, 1, 0), c(0, -1, 0), c(0, 0, 1), c(0, 0, -1));
   const double uc = u(0, 0, 0);
   const double rxc = a.rdxc[i + 1], ryf = a.rdyf[j], rzf = a.rdzf[k];
-  double phi = 0.0, ps[4], qp, qm;
+  double phi = 0.0, qp, qm;
   // d(uu)/dx
-  limiters<S>(uc, u(-1, 0, 0), u(1, 0, 0), u(2, 0, 0), u(-2, 0, 0), sh, ps);
   qp = 0.5 * (uc + u(1, 0, 0));
   qm = 0.5 * (uc + u(-1, 0, 0));
-  phi = phi - (flux(qp, uc, u(1, 0, 0), ps[0], ps[1]) - flux(qm, u(-1, 0, 0), uc, ps[2], ps[3])) * rxc;
+  phi = phi - conv_diff<S>(qp, qm, u(-2, 0, 0), u(-1, 0, 0), uc, u(1, 0, 0), u(2, 0, 0), sh) * rxc;
   // d(vu)/dy
-  limiters<S>(uc, u(0, -1, 0), u(0, 1, 0), u(0, 2, 0), u(0, -2, 0), sh, ps);
   qp = 0.5 * (v(1, 0, 0) + v(0, 0, 0));
   qm = 0.5 * (v(1, -1, 0) + v(0, -1, 0));
-  phi = phi - (flux(qp, uc, u(0, 1, 0), ps[0], ps[1]) - flux(qm, u(0, -1, 0), uc, ps[2], ps[3])) * ryf;
+  phi = phi - conv_diff<S>(qp, qm, u(0, -2, 0), u(0, -1, 0), uc, u(0, 1, 0), u(0, 2, 0), sh) * ryf;
   // d(wu)/dz
-  limiters<S>(uc, u(0, 0, -1), u(0, 0, 1), u(0, 0, 2), u(0, 0, -2), sh, ps);
   qp = 0.5 * (w(0, 0, 0) + w(1, 0, 0));
   qm = 0.5 * (w(0, 0, -1) + w(1, 0, -1));
-  phi = phi - (flux(qp, uc, u(0, 0, 1), ps[0], ps[1]) - flux(qm, u(0, 0, -1), uc, ps[2], ps[3])) * rzf;
+  phi = phi - conv_diff<S>(qp, qm, u(0, 0, -2), u(0, 0, -1), uc, u(0, 0, 1), u(0, 0, 2), sh) * rzf;
   // diffusion
   double mur = m(1, 0, 0), mul = m(0, 0, 0);
   const double dxx = (mur * (u(1, 0, 0) - uc) * a.rdxf[i + 1] - mul * (uc - u(-1, 0, 0)) * a.rdxf[i]) * rxc;
@@ -146,34 +202,31 @@ __device__ double phi_x(const MomArgs &a, int i, int j, int k) {
   mul = 0.25 * (m(1, 0, 0) + m(0, 0, 0) + m(1, 0, -1) + m(0, 0, -1));
   const double dzz = (mur * (u(0, 0, 1) - uc) * a.rdzc[k + 1] - mul * (uc - u(0, 0, -1)) * a.rdzc[k]) * rzf;
   const double dzzt = (mur * (w(1, 0, 0) - w(0, 0, 0)) * rxc - mul * (w(1, 0, -1) - w(0, 0, -1)) * rxc) * rzf;
-  const double invrho = 0.5 * (1.0 / rho(1, 0, 0) + 1.0 / rho(0, 0, 0));
+  const double invrho = 0.5 * (1.0 / rho(1, 0, 0) + irc);
   return phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho;
 }
 
 // y component at face (i, j, k) (momentumEqn.f90:344-467)
-template <int S>
-__device__ double phi_y(const MomArgs &a, int i, int j, int k) {
+template <int S, class Acc>
+__device__ __forceinline__ double phi_y(const Acc &A, const MomArgs &a, int i, int j, int k, double irc) {
   TBFP_MOM_ACCESSORS;
   const bool sh = sharp_cell<S>(c(1, 0, 0), c(-1, 0, 0), c(0, 1, 0), c(0, 0, 0), c(0, 0, 1), c(0, 0, -1));
   const double vc = v(0, 0, 0);
   const double dyfj = a.dyf[j], dyfp = a.dyf[j + 1], rycp = a.rdyc[j + 1];
   const double rxf = a.rdxf[i], rzf = a.rdzf[k];
-  double phi = 0.0, ps[4], qp, qm;
+  double phi = 0.0, qp, qm;
   // d(uv)/dx
-  limiters<S>(vc, v(-1, 0, 0), v(1, 0, 0), v(2, 0, 0), v(-2, 0, 0), sh, ps);
   qp = 0.5 * (u(0, 1, 0) * dyfp + u(0, 0, 0) * dyfj) * rycp;
   qm = 0.5 * (u(-1, 1, 0) * dyfp + u(-1, 0, 0) * dyfj) * rycp;
-  phi = phi - (flux(qp, vc, v(1, 0, 0), ps[0], ps[1]) - flux(qm, v(-1, 0, 0), vc, ps[2], ps[3])) * rxf;
+  phi = phi - conv_diff<S>(qp, qm, v(-2, 0, 0), v(-1, 0, 0), vc, v(1, 0, 0), v(2, 0, 0), sh) * rxf;
   // d(vv)/dy
-  limiters<S>(vc, v(0, -1, 0), v(0, 1, 0), v(0, 2, 0), v(0, -2, 0), sh, ps);
   qp = 0.5 * (vc + v(0, 1, 0));
   qm = 0.5 * (vc + v(0, -1, 0));
-  phi = phi - (flux(qp, vc, v(0, 1, 0), ps[0], ps[1]) - flux(qm, v(0, -1, 0), vc, ps[2], ps[3])) * rycp;
+  phi = phi - conv_diff<S>(qp, qm, v(0, -2, 0), v(0, -1, 0), vc, v(0, 1, 0), v(0, 2, 0), sh) * rycp;
   // d(wv)/dz
-  limiters<S>(vc, v(0, 0, -1), v(0, 0, 1), v(0, 0, 2), v(0, 0, -2), sh, ps);
   qp = 0.5 * (w(0, 1, 0) * dyfp + w(0, 0, 0) * dyfj) * rycp;
   qm = 0.5 * (w(0, 1, -1) * dyfp + w(0, 0, -1) * dyfj) * rycp;
-  phi = phi - (flux(qp, vc, v(0, 0, 1), ps[0], ps[1]) - flux(qm, v(0, 0, -1), vc, ps[2], ps[3])) * rzf;
+  phi = phi - conv_diff<S>(qp, qm, v(0, 0, -2), v(0, 0, -1), vc, v(0, 0, 1), v(0, 0, 2), sh) * rzf;
   // diffusion
   double mur = 0.25 * (m(0, 0, 0) + m(1, 0, 0) + m(0, 1, 0) + m(1, 1, 0));
   double mul = 0.25 * (m(0, 0, 0) + m(-1, 0, 0) + m(0, 1, 0) + m(-1, 1, 0));
@@ -187,33 +240,30 @@ __device__ double phi_y(const MomArgs &a, int i, int j, int k) {
   mul = 0.25 * (m(0, 0, 0) + m(0, 0, -1) + m(0, 1, 0) + m(0, 1, -1));
   const double dzz = (mur * (v(0, 0, 1) - vc) * a.rdzc[k + 1] - mul * (vc - v(0, 0, -1)) * a.rdzc[k]) * rzf;
   const double dzzt = (mur * (w(0, 1, 0) - w(0, 0, 0)) * rycp - mul * (w(0, 1, -1) - w(0, 0, -1)) * rycp) * rzf;
-  const double invrho = 0.5 * (1.0 / rho(0, 1, 0) + 1.0 / rho(0, 0, 0));
+  const double invrho = 0.5 * (1.0 / rho(0, 1, 0) + irc);
   return phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho;
 }
 
 // z component at face (i, j, k) (momentumEqn.f90:470-603)
-template <int S>
-__device__ double phi_z(const MomArgs &a, int i, int j, int k) {
+template <int S, class Acc>
+__device__ __forceinline__ double phi_z(const Acc &A, const MomArgs &a, int i, int j, int k, double irc) {
   TBFP_MOM_ACCESSORS;
   const bool sh = sharp_cell<S>(c(1, 0, 0), c(-1, 0, 0), c(0, 1, 0), c(0, -1, 0), c(0, 0, 1), c(0, 0, 0));
   const double wc = w(0, 0, 0);
   const double rxf = a.rdxf[i], ryf = a.rdyf[j], rzcp = a.rdzc[k + 1];
-  double phi = 0.0, ps[4], qp, qm;
+  double phi = 0.0, qp, qm;
   // d(uw)/dx
-  limiters<S>(wc, w(-1, 0, 0), w(1, 0, 0), w(2, 0, 0), w(-2, 0, 0), sh, ps);
   qp = 0.5 * (u(0, 0, 0) + u(0, 0, 1));
   qm = 0.5 * (u(-1, 0, 0) + u(-1, 0, 1));
-  phi = phi - (flux(qp, wc, w(1, 0, 0), ps[0], ps[1]) - flux(qm, w(-1, 0, 0), wc, ps[2], ps[3])) * rxf;
+  phi = phi - conv_diff<S>(qp, qm, w(-2, 0, 0), w(-1, 0, 0), wc, w(1, 0, 0), w(2, 0, 0), sh) * rxf;
   // d(vw)/dy
-  limiters<S>(wc, w(0, -1, 0), w(0, 1, 0), w(0, 2, 0), w(0, -2, 0), sh, ps);
   qp = 0.5 * (v(0, 0, 0) + v(0, 0, 1));
   qm = 0.5 * (v(0, -1, 0) + v(0, -1, 1));
-  phi = phi - (flux(qp, wc, w(0, 1, 0), ps[0], ps[1]) - flux(qm, w(0, -1, 0), wc, ps[2], ps[3])) * ryf;
+  phi = phi - conv_diff<S>(qp, qm, w(0, -2, 0), w(0, -1, 0), wc, w(0, 1, 0), w(0, 2, 0), sh) * ryf;
   // d(ww)/dz
-  limiters<S>(wc, w(0, 0, -1), w(0, 0, 1), w(0, 0, 2), w(0, 0, -2), sh, ps);
   qp = 0.5 * (wc + w(0, 0, 1));
   qm = 0.5 * (wc + w(0, 0, -1));
-  phi = phi - (flux(qp, wc, w(0, 0, 1), ps[0], ps[1]) - flux(qm, w(0, 0, -1), wc, ps[2], ps[3])) * rzcp;
+  phi = phi - conv_diff<S>(qp, qm, w(0, 0, -2), w(0, 0, -1), wc, w(0, 0, 1), w(0, 0, 2), sh) * rzcp;
   // diffusion
   double mur = 0.25 * (m(0, 0, 0) + m(0, 0, 1) + m(1, 0, 0) + m(1, 0, 1));
   double mul = 0.25 * (m(0, 0, 0) + m(0, 0, 1) + m(-1, 0, 0) + m(-1, 0, 1));
@@ -227,23 +277,119 @@ __device__ double phi_z(const MomArgs &a, int i, int j, int k) {
   mul = m(0, 0, 0);
   const double dzz = (mur * (w(0, 0, 1) - wc) * a.rdzf[k + 1] - mul * (wc - w(0, 0, -1)) * a.rdzf[k]) * rzcp;
   const double dzzt = dzz;
-  const double invrho = 0.5 * (1.0 / rho(0, 0, 1) + 1.0 / rho(0, 0, 0));
+  const double invrho = 0.5 * (1.0 / rho(0, 0, 1) + irc);
   return phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho;
 }
 #undef TBFP_MOM_ACCESSORS
 
-// grid over i = 1..nx, j = 1..ny, k = 0..nz; each thread the components whose
-// box holds it, and the thread at i = nx also the x component's face i = 0
+// Tiled form: block (32, 8) over a tile of (i, j) columns, i = 1..nx,
+// j = 1..ny, marching k over a chunk of kKC planes of 0..nz; each thread the
+// components whose box holds its (i, j, k).  A plane outside a field's array
+// is not loaded: no stencil of a computed component reaches it.
 template <int S>
-__global__ void __launch_bounds__(kMT) k_momentum_fluxes(MomArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y + 1, k = blockIdx.z;
-  if (i > a.nx) return;
-  if (k >= 1) {
-    a.phx[box_x(a, i, j, k)] = phi_x<S>(a, i, j, k);
-    if (i == a.nx) a.phx[box_x(a, 0, j, k)] = phi_x<S>(a, 0, j, k);
-    if (j <= a.ny - 1) a.phy[box_y(a, i, j, k)] = phi_y<S>(a, i, j, k);
+__global__ void __launch_bounds__(kTX * kTY, 2) k_momentum_fluxes(MomArgs a) {
+  extern __shared__ double sm[];
+  double *rU = sm, *rV = rU + kRV * kNV, *rW = rV + kRV * kNV;
+  double *rM = rW + kRV * kNV, *rR = rM + kRC * kNC, *rC = rR + kRC * kNC;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+  const int i0 = blockIdx.x * kTX + 1, j0 = blockIdx.y * kTY + 1;
+  const int kb = blockIdx.z * kKC, ke = min(kb + kKC - 1, a.nz);
+  const int i = i0 + tx, j = j0 + ty;
+  const bool in = i <= a.nx && j <= a.ny;
+  const int vhi = a.hdu, chi = a.hdc;  // upper bound of every array: n + halo
+
+  auto load_v = [&](double *ring, const double *f, const Lay &L, int kp) {
+    if (kp < L.klo || kp > a.nz + vhi) return;
+    double *dst = ring + ((kp + 3 * kRV) % kRV) * kNV;
+    for (int e = tid; e < kNV; e += kTX * kTY) {
+      const int rr = e / kPV, cc = e - rr * kPV;
+      const int gi = i0 - kHV + cc, gj = j0 - kHV + rr;
+      if (gi >= L.ilo && gi <= a.nx + vhi && gj >= L.jlo && gj <= a.ny + vhi) cp_async8(dst + e, f + at(L, gi, gj, kp));
+    }
+  };
+  auto load_c = [&](double *ring, const double *f, int kp) {
+    const Lay &L = a.Lc;
+    if (kp < L.klo || kp > a.nz + chi) return;
+    double *dst = ring + ((kp + 3 * kRC) % kRC) * kNC;
+    for (int e = tid; e < kNC; e += kTX * kTY) {
+      const int rr = e / kPC, cc = e - rr * kPC;
+      const int gi = i0 - kHC + cc, gj = j0 - kHC + rr;
+      if (gi >= L.ilo && gi <= a.nx + chi && gj >= L.jlo && gj <= a.ny + chi) cp_async8(dst + e, f + at(L, gi, gj, kp));
+    }
+  };
+  auto load_planes = [&](int kv, int kcl) {
+    load_v(rU, a.ux, a.Lux, kv);
+    load_v(rV, a.uy, a.Luy, kv);
+    load_v(rW, a.uz, a.Luz, kv);
+    load_c(rM, a.mu, kcl);
+    load_c(rR, a.rho, kcl);
+    if (S == 5) load_c(rC, a.c, kcl);
+  };
+  for (int d = -2; d <= 2; ++d) {
+    load_v(rU, a.ux, a.Lux, kb + d);
+    load_v(rV, a.uy, a.Luy, kb + d);
+    load_v(rW, a.uz, a.Luz, kb + d);
   }
-  a.phz[box_z(a, i, j, k)] = phi_z<S>(a, i, j, k);
+  for (int d = -1; d <= 1; ++d) {
+    load_c(rM, a.mu, kb + d);
+    load_c(rR, a.rho, kb + d);
+    if (S == 5) load_c(rC, a.c, kb + d);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  SAcc A;
+  A.sU = rU + (ty + kHV) * kPV + tx + kHV;
+  A.sV = rV + (ty + kHV) * kPV + tx + kHV;
+  A.sW = rW + (ty + kHV) * kPV + tx + kHV;
+  A.sM = rM + (ty + kHC) * kPC + tx + kHC;
+  A.sR = rR + (ty + kHC) * kPC + tx + kHC;
+  A.sC = rC + (ty + kHC) * kPC + tx + kHC;
+  for (int k = kb; k <= ke; ++k) {
+    // planes k+3 (velocity) and k+2 (cell) into the slots of k-3 and k-2, read by the previous step only
+    if (k < ke) load_planes(k + 3, k + 2);
+#pragma unroll
+    for (int d = 0; d < 5; ++d) A.ov[d] = ((k + d - 2 + 3 * kRV) % kRV) * kNV;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) A.oc[d] = ((k + d - 1 + 3 * kRC) % kRC) * kNC;
+    if (in) {
+      const double irc = 1.0 / A.r(0, 0, 0);  // 1/rho of the own cell, shared by the three components
+      if (k >= 1) {
+        a.phx[box_x(a, i, j, k)] = phi_x<S>(A, a, i, j, k, irc);
+        if (j <= a.ny - 1) a.phy[box_y(a, i, j, k)] = phi_y<S>(A, a, i, j, k, irc);
+      }
+      a.phz[box_z(a, i, j, k)] = phi_z<S>(A, a, i, j, k, irc);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
+}
+
+constexpr size_t tiled_smem_bytes(int S) {
+  return sizeof(double) * (3 * kRV * kNV + (S == 5 ? 3 : 2) * kRC * kNC);
+}
+
+// the x component's face i = 0 (the periodic duplicate of i = nx, computed
+// from its own stencil), one thread per (j, k)
+template <int S>
+__global__ void __launch_bounds__(kMT) k_momentum_fluxes_i0(MomArgs a) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y + 1;
+  if (j > a.ny) return;
+  const GAcc A(a, 0, j, k);
+  a.phx[box_x(a, 0, j, k)] = phi_x<S>(A, a, 0, j, k, 1.0 / A.r(0, 0, 0));
+}
+
+template <int S>
+void launch_fluxes(const MomArgs &a, cudaStream_t st) {
+  static bool attr[64] = {};  // per device: the attribute belongs to the device's context
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 64 || !attr[dev]) {
+    cudaFuncSetAttribute(k_momentum_fluxes<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tiled_smem_bytes(S));
+    if (dev < 64) attr[dev] = true;
+  }
+  const dim3 blk(kTX, kTY), grid((a.nx + kTX - 1) / kTX, (a.ny + kTY - 1) / kTY, (a.nz + 1 + kKC - 1) / kKC);
+  k_momentum_fluxes<S><<<grid, blk, tiled_smem_bytes(S), st>>>(a);
+  k_momentum_fluxes_i0<S><<<dim3((a.ny + kMT - 1) / kMT, a.nz), kMT, 0, st>>>(a);
 }
 
 struct MomUpd {
@@ -292,8 +438,8 @@ __global__ void __launch_bounds__(kMT) k_momentum_update(MomUpd a) {
 void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, const double *c, const double *mu,
                      const double *rho, const double *const *st, Lay Lux, Lay Luy, Lay Luz, Lay Lc, const Lay *Lst,
                      double *const phi[3], const double *const prev[3], int nx, int ny, int nz, int scheme, double dt,
-                     double alpha, double gamma, double xi, double rho0, double fs, double gch, double g,
-                     cudaStream_t st_) {
+                     double alpha, double gamma, double xi, double rho0, double fs, double gch, double g, int hdu,
+                     int hdc, cudaStream_t st_) {
   MomArgs a{};
   a.ux = ux;
   a.uy = uy;
@@ -318,15 +464,17 @@ void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, 
   a.nx = nx;
   a.ny = ny;
   a.nz = nz;
-  const dim3 grid((nx + kMT - 1) / kMT, ny, nz + 1);
+  a.hdu = hdu;
+  a.hdc = hdc;
   switch (scheme) {
-    case 0: k_momentum_fluxes<0><<<grid, kMT, 0, st_>>>(a); break;
-    case 1: k_momentum_fluxes<1><<<grid, kMT, 0, st_>>>(a); break;
-    case 2: k_momentum_fluxes<2><<<grid, kMT, 0, st_>>>(a); break;
-    case 3: k_momentum_fluxes<3><<<grid, kMT, 0, st_>>>(a); break;
-    case 4: k_momentum_fluxes<4><<<grid, kMT, 0, st_>>>(a); break;
-    default: k_momentum_fluxes<5><<<grid, kMT, 0, st_>>>(a); break;
+    case 0: launch_fluxes<0>(a, st_); break;
+    case 1: launch_fluxes<1>(a, st_); break;
+    case 2: launch_fluxes<2>(a, st_); break;
+    case 3: launch_fluxes<3>(a, st_); break;
+    case 4: launch_fluxes<4>(a, st_); break;
+    default: launch_fluxes<5>(a, st_); break;
   }
+  const dim3 grid((nx + kMT - 1) / kMT, ny, nz + 1);
   MomUpd b{};
   b.ux = ux;
   b.uy = uy;
