@@ -161,6 +161,17 @@ struct SAcc {
   __device__ double r(int di, int dj, int dk) const { return sR[oc[dk + 1] + dj * kPC + di]; }
 };
 
+// the spacings one cell's stencils use (reciprocals, and dyf at j, j+1),
+// loaded once per cell through the read-only path
+struct Met {
+  double rxf0, rxf1, rxc0, rxc1, ryf0, ryf1, ryc0, ryc1, dyf0, dyf1, rzf0, rzf1, rzc0, rzc1;
+  __device__ Met(const MomArgs &a, int i, int j, int k)
+      : rxf0(__ldg(a.rdxf + i)), rxf1(__ldg(a.rdxf + i + 1)), rxc0(__ldg(a.rdxc + i)), rxc1(__ldg(a.rdxc + i + 1)),
+        ryf0(__ldg(a.rdyf + j)), ryf1(__ldg(a.rdyf + j + 1)), ryc0(__ldg(a.rdyc + j)), ryc1(__ldg(a.rdyc + j + 1)),
+        dyf0(__ldg(a.dyf + j)), dyf1(__ldg(a.dyf + j + 1)), rzf0(__ldg(a.rdzf + k)), rzf1(__ldg(a.rdzf + k + 1)),
+        rzc0(__ldg(a.rdzc + k)), rzc1(__ldg(a.rdzc + k + 1)) {}
+};
+
 #define TBFP_MOM_ACCESSORS                                                       \
   auto u = [&](int di, int dj, int dk) { return A.u(di, dj, dk); };              \
   auto v = [&](int di, int dj, int dk) { return A.v(di, dj, dk); };              \
@@ -172,11 +183,11 @@ struct SAcc {
 
 // updateConveDiff, x component at face (i, j, k) (momentumEqn.f90:228-341)
 template <int S, class Acc>
-__device__ __forceinline__ double phi_x(const Acc &A, const MomArgs &a, int i, int j, int k, double irc) {
+__device__ __forceinline__ double phi_x(const Acc &A, const Met &g, double irc) {
   TBFP_MOM_ACCESSORS;
   const bool sh = sharp_cell<S>(c(1, 0, 0), c(0, 0, 0), c(0, 1, 0), c(0, -1, 0), c(0, 0, 1), c(0, 0, -1));
   const double uc = u(0, 0, 0);
-  const double rxc = a.rdxc[i + 1], ryf = a.rdyf[j], rzf = a.rdzf[k];
+  const double rxc = g.rxc1, ryf = g.ryf0, rzf = g.rzf0;
   double phi = 0.0, qp, qm;
   // d(uu)/dx
   qp = 0.5 * (uc + u(1, 0, 0));
@@ -192,15 +203,15 @@ __device__ __forceinline__ double phi_x(const Acc &A, const MomArgs &a, int i, i
   phi = phi - conv_diff<S>(qp, qm, u(0, 0, -2), u(0, 0, -1), uc, u(0, 0, 1), u(0, 0, 2), sh) * rzf;
   // diffusion
   double mur = m(1, 0, 0), mul = m(0, 0, 0);
-  const double dxx = (mur * (u(1, 0, 0) - uc) * a.rdxf[i + 1] - mul * (uc - u(-1, 0, 0)) * a.rdxf[i]) * rxc;
+  const double dxx = (mur * (u(1, 0, 0) - uc) * g.rxf1 - mul * (uc - u(-1, 0, 0)) * g.rxf0) * rxc;
   const double dxxt = dxx;
   mur = 0.25 * (m(1, 0, 0) + m(0, 0, 0) + m(1, 1, 0) + m(0, 1, 0));
   mul = 0.25 * (m(1, 0, 0) + m(0, 0, 0) + m(1, -1, 0) + m(0, -1, 0));
-  const double dyy = (mur * (u(0, 1, 0) - uc) * a.rdyc[j + 1] - mul * (uc - u(0, -1, 0)) * a.rdyc[j]) * ryf;
+  const double dyy = (mur * (u(0, 1, 0) - uc) * g.ryc1 - mul * (uc - u(0, -1, 0)) * g.ryc0) * ryf;
   const double dyyt = (mur * (v(1, 0, 0) - v(0, 0, 0)) * rxc - mul * (v(1, -1, 0) - v(0, -1, 0)) * rxc) * ryf;
   mur = 0.25 * (m(1, 0, 0) + m(0, 0, 0) + m(1, 0, 1) + m(0, 0, 1));
   mul = 0.25 * (m(1, 0, 0) + m(0, 0, 0) + m(1, 0, -1) + m(0, 0, -1));
-  const double dzz = (mur * (u(0, 0, 1) - uc) * a.rdzc[k + 1] - mul * (uc - u(0, 0, -1)) * a.rdzc[k]) * rzf;
+  const double dzz = (mur * (u(0, 0, 1) - uc) * g.rzc1 - mul * (uc - u(0, 0, -1)) * g.rzc0) * rzf;
   const double dzzt = (mur * (w(1, 0, 0) - w(0, 0, 0)) * rxc - mul * (w(1, 0, -1) - w(0, 0, -1)) * rxc) * rzf;
   const double invrho = 0.5 * (1.0 / rho(1, 0, 0) + irc);
   return phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho;
@@ -208,12 +219,12 @@ __device__ __forceinline__ double phi_x(const Acc &A, const MomArgs &a, int i, i
 
 // y component at face (i, j, k) (momentumEqn.f90:344-467)
 template <int S, class Acc>
-__device__ __forceinline__ double phi_y(const Acc &A, const MomArgs &a, int i, int j, int k, double irc) {
+__device__ __forceinline__ double phi_y(const Acc &A, const Met &g, double irc) {
   TBFP_MOM_ACCESSORS;
   const bool sh = sharp_cell<S>(c(1, 0, 0), c(-1, 0, 0), c(0, 1, 0), c(0, 0, 0), c(0, 0, 1), c(0, 0, -1));
   const double vc = v(0, 0, 0);
-  const double dyfj = a.dyf[j], dyfp = a.dyf[j + 1], rycp = a.rdyc[j + 1];
-  const double rxf = a.rdxf[i], rzf = a.rdzf[k];
+  const double dyfj = g.dyf0, dyfp = g.dyf1, rycp = g.ryc1;
+  const double rxf = g.rxf0, rzf = g.rzf0;
   double phi = 0.0, qp, qm;
   // d(uv)/dx
   qp = 0.5 * (u(0, 1, 0) * dyfp + u(0, 0, 0) * dyfj) * rycp;
@@ -230,15 +241,15 @@ __device__ __forceinline__ double phi_y(const Acc &A, const MomArgs &a, int i, i
   // diffusion
   double mur = 0.25 * (m(0, 0, 0) + m(1, 0, 0) + m(0, 1, 0) + m(1, 1, 0));
   double mul = 0.25 * (m(0, 0, 0) + m(-1, 0, 0) + m(0, 1, 0) + m(-1, 1, 0));
-  const double dxx = (mur * (v(1, 0, 0) - vc) * a.rdxc[i + 1] - mul * (vc - v(-1, 0, 0)) * a.rdxc[i]) * rxf;
+  const double dxx = (mur * (v(1, 0, 0) - vc) * g.rxc1 - mul * (vc - v(-1, 0, 0)) * g.rxc0) * rxf;
   const double dxxt = (mur * (u(0, 1, 0) - u(0, 0, 0)) * rycp - mul * (u(-1, 1, 0) - u(-1, 0, 0)) * rycp) * rxf;
   mur = m(0, 1, 0);
   mul = m(0, 0, 0);
-  const double dyy = (mur * (v(0, 1, 0) - vc) * a.rdyf[j + 1] - mul * (vc - v(0, -1, 0)) * a.rdyf[j]) * rycp;
+  const double dyy = (mur * (v(0, 1, 0) - vc) * g.ryf1 - mul * (vc - v(0, -1, 0)) * g.ryf0) * rycp;
   const double dyyt = dyy;
   mur = 0.25 * (m(0, 0, 0) + m(0, 0, 1) + m(0, 1, 0) + m(0, 1, 1));
   mul = 0.25 * (m(0, 0, 0) + m(0, 0, -1) + m(0, 1, 0) + m(0, 1, -1));
-  const double dzz = (mur * (v(0, 0, 1) - vc) * a.rdzc[k + 1] - mul * (vc - v(0, 0, -1)) * a.rdzc[k]) * rzf;
+  const double dzz = (mur * (v(0, 0, 1) - vc) * g.rzc1 - mul * (vc - v(0, 0, -1)) * g.rzc0) * rzf;
   const double dzzt = (mur * (w(0, 1, 0) - w(0, 0, 0)) * rycp - mul * (w(0, 1, -1) - w(0, 0, -1)) * rycp) * rzf;
   const double invrho = 0.5 * (1.0 / rho(0, 1, 0) + irc);
   return phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho;
@@ -246,11 +257,11 @@ __device__ __forceinline__ double phi_y(const Acc &A, const MomArgs &a, int i, i
 
 // z component at face (i, j, k) (momentumEqn.f90:470-603)
 template <int S, class Acc>
-__device__ __forceinline__ double phi_z(const Acc &A, const MomArgs &a, int i, int j, int k, double irc) {
+__device__ __forceinline__ double phi_z(const Acc &A, const Met &g, double irc) {
   TBFP_MOM_ACCESSORS;
   const bool sh = sharp_cell<S>(c(1, 0, 0), c(-1, 0, 0), c(0, 1, 0), c(0, -1, 0), c(0, 0, 1), c(0, 0, 0));
   const double wc = w(0, 0, 0);
-  const double rxf = a.rdxf[i], ryf = a.rdyf[j], rzcp = a.rdzc[k + 1];
+  const double rxf = g.rxf0, ryf = g.ryf0, rzcp = g.rzc1;
   double phi = 0.0, qp, qm;
   // d(uw)/dx
   qp = 0.5 * (u(0, 0, 0) + u(0, 0, 1));
@@ -267,15 +278,15 @@ __device__ __forceinline__ double phi_z(const Acc &A, const MomArgs &a, int i, i
   // diffusion
   double mur = 0.25 * (m(0, 0, 0) + m(0, 0, 1) + m(1, 0, 0) + m(1, 0, 1));
   double mul = 0.25 * (m(0, 0, 0) + m(0, 0, 1) + m(-1, 0, 0) + m(-1, 0, 1));
-  const double dxx = (mur * (w(1, 0, 0) - wc) * a.rdxc[i + 1] - mul * (wc - w(-1, 0, 0)) * a.rdxc[i]) * rxf;
+  const double dxx = (mur * (w(1, 0, 0) - wc) * g.rxc1 - mul * (wc - w(-1, 0, 0)) * g.rxc0) * rxf;
   const double dxxt = (mur * (u(0, 0, 1) - u(0, 0, 0)) * rzcp - mul * (u(-1, 0, 1) - u(-1, 0, 0)) * rzcp) * rxf;
   mur = 0.25 * (m(0, 0, 0) + m(0, 0, 1) + m(0, 1, 0) + m(0, 1, 1));
   mul = 0.25 * (m(0, 0, 0) + m(0, 0, 1) + m(0, -1, 0) + m(0, -1, 1));
-  const double dyy = (mur * (w(0, 1, 0) - wc) * a.rdyc[j + 1] - mul * (wc - w(0, -1, 0)) * a.rdyc[j]) * ryf;
+  const double dyy = (mur * (w(0, 1, 0) - wc) * g.ryc1 - mul * (wc - w(0, -1, 0)) * g.ryc0) * ryf;
   const double dyyt = (mur * (v(0, 0, 1) - v(0, 0, 0)) * rzcp - mul * (v(0, -1, 1) - v(0, -1, 0)) * rzcp) * ryf;
   mur = m(0, 0, 1);
   mul = m(0, 0, 0);
-  const double dzz = (mur * (w(0, 0, 1) - wc) * a.rdzf[k + 1] - mul * (wc - w(0, 0, -1)) * a.rdzf[k]) * rzcp;
+  const double dzz = (mur * (w(0, 0, 1) - wc) * g.rzf1 - mul * (wc - w(0, 0, -1)) * g.rzf0) * rzcp;
   const double dzzt = dzz;
   const double invrho = 0.5 * (1.0 / rho(0, 0, 1) + irc);
   return phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho;
@@ -353,11 +364,12 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_momentum_fluxes(MomArgs a) {
     for (int d = 0; d < 3; ++d) A.oc[d] = ((k + d - 1 + 3 * kRC) % kRC) * kNC;
     if (in) {
       const double irc = 1.0 / A.r(0, 0, 0);  // 1/rho of the own cell, shared by the three components
+      const Met g(a, i, j, k);
       if (k >= 1) {
-        a.phx[box_x(a, i, j, k)] = phi_x<S>(A, a, i, j, k, irc);
-        if (j <= a.ny - 1) a.phy[box_y(a, i, j, k)] = phi_y<S>(A, a, i, j, k, irc);
+        a.phx[box_x(a, i, j, k)] = phi_x<S>(A, g, irc);
+        if (j <= a.ny - 1) a.phy[box_y(a, i, j, k)] = phi_y<S>(A, g, irc);
       }
-      a.phz[box_z(a, i, j, k)] = phi_z<S>(A, a, i, j, k, irc);
+      a.phz[box_z(a, i, j, k)] = phi_z<S>(A, g, irc);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -375,7 +387,7 @@ __global__ void __launch_bounds__(kMT) k_momentum_fluxes_i0(MomArgs a) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y + 1;
   if (j > a.ny) return;
   const GAcc A(a, 0, j, k);
-  a.phx[box_x(a, 0, j, k)] = phi_x<S>(A, a, 0, j, k, 1.0 / A.r(0, 0, 0));
+  a.phx[box_x(a, 0, j, k)] = phi_x<S>(A, Met(a, 0, j, k), 1.0 / A.r(0, 0, 0));
 }
 
 template <int S>
