@@ -94,6 +94,38 @@ __device__ __forceinline__ double conv_diff(double qp, double qm, double vmm, do
   }
 }
 
+// the limiter of one ratio (momentumEqn.f90:667-734) for schemes 3 and 4
+template <int S>
+__device__ __forceinline__ double lim(double x) {
+  if constexpr (S == 3) {
+    const double y = fmax(0.0, x);
+    return (y + fabs(y)) / (1.0 + fabs(y));
+  } else {
+    return superbee(x);
+  }
+}
+
+// The limited flux through the face between vc and vp (vm and vpp the next
+// values outward), for schemes 0-4, whose limiters depend on the face alone:
+// the upper face of one cell is then the lower face of the next bit for bit
+// (the lower face's ratios have the same numerators and denominator), so a
+// face is computed once.
+template <int S>
+__device__ __forceinline__ double face_flux(double q, double vm, double vc, double vp, double vpp) {
+  if constexpr (S == 2) {
+    const double d = vp - vc;
+    const double A = d == 0.0 ? vc : vc + 0.125 * ((vc - vm) + 3.0 * d);
+    const double B = d == 0.0 ? vp : vp - 0.125 * ((vpp - vp) + 3.0 * d);
+    return fmax(q, 0.0) * A + fmin(q, 0.0) * B;
+  } else if constexpr (S == 0 || S == 1) {
+    const double p = S == 0 ? 1.0 : 0.0;
+    return flux(q, vc, vp, p, p);
+  } else {
+    const double ip = 1.0 / approx_zero(vp - vc);
+    return flux(q, vc, vp, lim<S>((vc - vm) * ip), lim<S>((vpp - vp) * ip));
+  }
+}
+
 struct MomArgs {
   const double *ux, *uy, *uz, *c, *mu, *rho;
   Lay Lux, Luy, Luz, Lc;  // c, mu, rho share Lc
@@ -159,6 +191,26 @@ struct SAcc {
   __device__ double c(int di, int dj, int dk) const { return sC[oc[dk + 1] + dj * kPC + di]; }
   __device__ double m(int di, int dj, int dk) const { return sM[oc[dk + 1] + dj * kPC + di]; }
   __device__ double r(int di, int dj, int dk) const { return sR[oc[dk + 1] + dj * kPC + di]; }
+  // the accessor of the cell (di, dj) columns away in the same plane
+  __device__ SAcc shifted(int di, int dj) const {
+    SAcc b = *this;
+    b.sU += di + dj * kPV;
+    b.sV += di + dj * kPV;
+    b.sW += di + dj * kPV;
+    b.sC += di + dj * kPC;
+    b.sM += di + dj * kPC;
+    b.sR += di + dj * kPC;
+    return b;
+  }
+  // the accessor of the cell one plane down (reaches planes k-2..k+1 only)
+  __device__ SAcc down() const {
+    SAcc b = *this;
+#pragma unroll
+    for (int d = 4; d > 0; --d) b.ov[d] = ov[d - 1];
+#pragma unroll
+    for (int d = 2; d > 0; --d) b.oc[d] = oc[d - 1];
+    return b;
+  }
 };
 
 // the spacings one cell's stencils use (reciprocals, and dyf at j, j+1),
@@ -181,27 +233,70 @@ struct Met {
   auto rho = [&](int di, int dj, int dk) { return A.r(di, dj, dk); };            \
   (void)c
 
-// updateConveDiff, x component at face (i, j, k) (momentumEqn.f90:228-341)
+// The upper-face fluxes of the nine (component, direction) pairs at the
+// accessor's cell (updateConveDiff, momentumEqn.f90:228-603): ux faces
 template <int S, class Acc>
-__device__ __forceinline__ double phi_x(const Acc &A, const Met &g, double irc) {
+__device__ __forceinline__ double F_xx(const Acc &A) {
   TBFP_MOM_ACCESSORS;
-  const bool sh = sharp_cell<S>(c(1, 0, 0), c(0, 0, 0), c(0, 1, 0), c(0, -1, 0), c(0, 0, 1), c(0, 0, -1));
+  return face_flux<S>(0.5 * (u(0, 0, 0) + u(1, 0, 0)), u(-1, 0, 0), u(0, 0, 0), u(1, 0, 0), u(2, 0, 0));
+}
+template <int S, class Acc>
+__device__ __forceinline__ double F_xy(const Acc &A) {
+  TBFP_MOM_ACCESSORS;
+  return face_flux<S>(0.5 * (v(1, 0, 0) + v(0, 0, 0)), u(0, -1, 0), u(0, 0, 0), u(0, 1, 0), u(0, 2, 0));
+}
+template <int S, class Acc>
+__device__ __forceinline__ double F_xz(const Acc &A) {
+  TBFP_MOM_ACCESSORS;
+  return face_flux<S>(0.5 * (w(0, 0, 0) + w(1, 0, 0)), u(0, 0, -1), u(0, 0, 0), u(0, 0, 1), u(0, 0, 2));
+}
+// uy faces
+template <int S, class Acc>
+__device__ __forceinline__ double F_yx(const Acc &A, const Met &g) {
+  TBFP_MOM_ACCESSORS;
+  return face_flux<S>(0.5 * (u(0, 1, 0) * g.dyf1 + u(0, 0, 0) * g.dyf0) * g.ryc1, v(-1, 0, 0), v(0, 0, 0), v(1, 0, 0),
+                      v(2, 0, 0));
+}
+template <int S, class Acc>
+__device__ __forceinline__ double F_yy(const Acc &A) {
+  TBFP_MOM_ACCESSORS;
+  return face_flux<S>(0.5 * (v(0, 0, 0) + v(0, 1, 0)), v(0, -1, 0), v(0, 0, 0), v(0, 1, 0), v(0, 2, 0));
+}
+template <int S, class Acc>
+__device__ __forceinline__ double F_yz(const Acc &A, const Met &g) {
+  TBFP_MOM_ACCESSORS;
+  return face_flux<S>(0.5 * (w(0, 1, 0) * g.dyf1 + w(0, 0, 0) * g.dyf0) * g.ryc1, v(0, 0, -1), v(0, 0, 0), v(0, 0, 1),
+                      v(0, 0, 2));
+}
+// uz faces
+template <int S, class Acc>
+__device__ __forceinline__ double F_zx(const Acc &A) {
+  TBFP_MOM_ACCESSORS;
+  return face_flux<S>(0.5 * (u(0, 0, 0) + u(0, 0, 1)), w(-1, 0, 0), w(0, 0, 0), w(1, 0, 0), w(2, 0, 0));
+}
+template <int S, class Acc>
+__device__ __forceinline__ double F_zy(const Acc &A) {
+  TBFP_MOM_ACCESSORS;
+  return face_flux<S>(0.5 * (v(0, 0, 0) + v(0, 0, 1)), w(0, -1, 0), w(0, 0, 0), w(0, 1, 0), w(0, 2, 0));
+}
+template <int S, class Acc>
+__device__ __forceinline__ double F_zz(const Acc &A) {
+  TBFP_MOM_ACCESSORS;
+  return face_flux<S>(0.5 * (w(0, 0, 0) + w(0, 0, 1)), w(0, 0, -1), w(0, 0, 0), w(0, 0, 1), w(0, 0, 2));
+}
+
+// x component at face (i, j, k) (momentumEqn.f90:228-341) from the convective
+// flux differences (upper minus lower face) of its three directions, plus the
+// diffusion with its transposed terms
+template <class Acc>
+__device__ __forceinline__ double tail_x(const Acc &A, const Met &g, double irc, double cx, double cy, double cz) {
+  TBFP_MOM_ACCESSORS;
   const double uc = u(0, 0, 0);
   const double rxc = g.rxc1, ryf = g.ryf0, rzf = g.rzf0;
-  double phi = 0.0, qp, qm;
-  // d(uu)/dx
-  qp = 0.5 * (uc + u(1, 0, 0));
-  qm = 0.5 * (uc + u(-1, 0, 0));
-  phi = phi - conv_diff<S>(qp, qm, u(-2, 0, 0), u(-1, 0, 0), uc, u(1, 0, 0), u(2, 0, 0), sh) * rxc;
-  // d(vu)/dy
-  qp = 0.5 * (v(1, 0, 0) + v(0, 0, 0));
-  qm = 0.5 * (v(1, -1, 0) + v(0, -1, 0));
-  phi = phi - conv_diff<S>(qp, qm, u(0, -2, 0), u(0, -1, 0), uc, u(0, 1, 0), u(0, 2, 0), sh) * ryf;
-  // d(wu)/dz
-  qp = 0.5 * (w(0, 0, 0) + w(1, 0, 0));
-  qm = 0.5 * (w(0, 0, -1) + w(1, 0, -1));
-  phi = phi - conv_diff<S>(qp, qm, u(0, 0, -2), u(0, 0, -1), uc, u(0, 0, 1), u(0, 0, 2), sh) * rzf;
-  // diffusion
+  double phi = 0.0;
+  phi = phi - cx * rxc;  // d(uu)/dx
+  phi = phi - cy * ryf;  // d(vu)/dy
+  phi = phi - cz * rzf;  // d(wu)/dz
   double mur = m(1, 0, 0), mul = m(0, 0, 0);
   const double dxx = (mur * (u(1, 0, 0) - uc) * g.rxf1 - mul * (uc - u(-1, 0, 0)) * g.rxf0) * rxc;
   const double dxxt = dxx;
@@ -218,27 +313,15 @@ __device__ __forceinline__ double phi_x(const Acc &A, const Met &g, double irc) 
 }
 
 // y component at face (i, j, k) (momentumEqn.f90:344-467)
-template <int S, class Acc>
-__device__ __forceinline__ double phi_y(const Acc &A, const Met &g, double irc) {
+template <class Acc>
+__device__ __forceinline__ double tail_y(const Acc &A, const Met &g, double irc, double cx, double cy, double cz) {
   TBFP_MOM_ACCESSORS;
-  const bool sh = sharp_cell<S>(c(1, 0, 0), c(-1, 0, 0), c(0, 1, 0), c(0, 0, 0), c(0, 0, 1), c(0, 0, -1));
   const double vc = v(0, 0, 0);
-  const double dyfj = g.dyf0, dyfp = g.dyf1, rycp = g.ryc1;
-  const double rxf = g.rxf0, rzf = g.rzf0;
-  double phi = 0.0, qp, qm;
-  // d(uv)/dx
-  qp = 0.5 * (u(0, 1, 0) * dyfp + u(0, 0, 0) * dyfj) * rycp;
-  qm = 0.5 * (u(-1, 1, 0) * dyfp + u(-1, 0, 0) * dyfj) * rycp;
-  phi = phi - conv_diff<S>(qp, qm, v(-2, 0, 0), v(-1, 0, 0), vc, v(1, 0, 0), v(2, 0, 0), sh) * rxf;
-  // d(vv)/dy
-  qp = 0.5 * (vc + v(0, 1, 0));
-  qm = 0.5 * (vc + v(0, -1, 0));
-  phi = phi - conv_diff<S>(qp, qm, v(0, -2, 0), v(0, -1, 0), vc, v(0, 1, 0), v(0, 2, 0), sh) * rycp;
-  // d(wv)/dz
-  qp = 0.5 * (w(0, 1, 0) * dyfp + w(0, 0, 0) * dyfj) * rycp;
-  qm = 0.5 * (w(0, 1, -1) * dyfp + w(0, 0, -1) * dyfj) * rycp;
-  phi = phi - conv_diff<S>(qp, qm, v(0, 0, -2), v(0, 0, -1), vc, v(0, 0, 1), v(0, 0, 2), sh) * rzf;
-  // diffusion
+  const double rycp = g.ryc1, rxf = g.rxf0, rzf = g.rzf0;
+  double phi = 0.0;
+  phi = phi - cx * rxf;   // d(uv)/dx
+  phi = phi - cy * rycp;  // d(vv)/dy
+  phi = phi - cz * rzf;   // d(wv)/dz
   double mur = 0.25 * (m(0, 0, 0) + m(1, 0, 0) + m(0, 1, 0) + m(1, 1, 0));
   double mul = 0.25 * (m(0, 0, 0) + m(-1, 0, 0) + m(0, 1, 0) + m(-1, 1, 0));
   const double dxx = (mur * (v(1, 0, 0) - vc) * g.rxc1 - mul * (vc - v(-1, 0, 0)) * g.rxc0) * rxf;
@@ -256,26 +339,15 @@ __device__ __forceinline__ double phi_y(const Acc &A, const Met &g, double irc) 
 }
 
 // z component at face (i, j, k) (momentumEqn.f90:470-603)
-template <int S, class Acc>
-__device__ __forceinline__ double phi_z(const Acc &A, const Met &g, double irc) {
+template <class Acc>
+__device__ __forceinline__ double tail_z(const Acc &A, const Met &g, double irc, double cx, double cy, double cz) {
   TBFP_MOM_ACCESSORS;
-  const bool sh = sharp_cell<S>(c(1, 0, 0), c(-1, 0, 0), c(0, 1, 0), c(0, -1, 0), c(0, 0, 1), c(0, 0, 0));
   const double wc = w(0, 0, 0);
   const double rxf = g.rxf0, ryf = g.ryf0, rzcp = g.rzc1;
-  double phi = 0.0, qp, qm;
-  // d(uw)/dx
-  qp = 0.5 * (u(0, 0, 0) + u(0, 0, 1));
-  qm = 0.5 * (u(-1, 0, 0) + u(-1, 0, 1));
-  phi = phi - conv_diff<S>(qp, qm, w(-2, 0, 0), w(-1, 0, 0), wc, w(1, 0, 0), w(2, 0, 0), sh) * rxf;
-  // d(vw)/dy
-  qp = 0.5 * (v(0, 0, 0) + v(0, 0, 1));
-  qm = 0.5 * (v(0, -1, 0) + v(0, -1, 1));
-  phi = phi - conv_diff<S>(qp, qm, w(0, -2, 0), w(0, -1, 0), wc, w(0, 1, 0), w(0, 2, 0), sh) * ryf;
-  // d(ww)/dz
-  qp = 0.5 * (wc + w(0, 0, 1));
-  qm = 0.5 * (wc + w(0, 0, -1));
-  phi = phi - conv_diff<S>(qp, qm, w(0, 0, -2), w(0, 0, -1), wc, w(0, 0, 1), w(0, 0, 2), sh) * rzcp;
-  // diffusion
+  double phi = 0.0;
+  phi = phi - cx * rxf;   // d(uw)/dx
+  phi = phi - cy * ryf;   // d(vw)/dy
+  phi = phi - cz * rzcp;  // d(ww)/dz
   double mur = 0.25 * (m(0, 0, 0) + m(0, 0, 1) + m(1, 0, 0) + m(1, 0, 1));
   double mul = 0.25 * (m(0, 0, 0) + m(0, 0, 1) + m(-1, 0, 0) + m(-1, 0, 1));
   const double dxx = (mur * (w(1, 0, 0) - wc) * g.rxc1 - mul * (wc - w(-1, 0, 0)) * g.rxc0) * rxf;
@@ -291,7 +363,61 @@ __device__ __forceinline__ double phi_z(const Acc &A, const Met &g, double irc) 
   const double invrho = 0.5 * (1.0 / rho(0, 0, 1) + irc);
   return phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho;
 }
+
+// The per-cell forms (every scheme; scheme 5's limiters depend on the cell):
+// both faces of each direction at the cell itself
+template <int S, class Acc>
+__device__ __forceinline__ double phi_x(const Acc &A, const Met &g, double irc) {
+  TBFP_MOM_ACCESSORS;
+  const bool sh = sharp_cell<S>(c(1, 0, 0), c(0, 0, 0), c(0, 1, 0), c(0, -1, 0), c(0, 0, 1), c(0, 0, -1));
+  const double uc = u(0, 0, 0);
+  const double cx = conv_diff<S>(0.5 * (uc + u(1, 0, 0)), 0.5 * (uc + u(-1, 0, 0)), u(-2, 0, 0), u(-1, 0, 0), uc,
+                                 u(1, 0, 0), u(2, 0, 0), sh);
+  const double cy = conv_diff<S>(0.5 * (v(1, 0, 0) + v(0, 0, 0)), 0.5 * (v(1, -1, 0) + v(0, -1, 0)), u(0, -2, 0),
+                                 u(0, -1, 0), uc, u(0, 1, 0), u(0, 2, 0), sh);
+  const double cz = conv_diff<S>(0.5 * (w(0, 0, 0) + w(1, 0, 0)), 0.5 * (w(0, 0, -1) + w(1, 0, -1)), u(0, 0, -2),
+                                 u(0, 0, -1), uc, u(0, 0, 1), u(0, 0, 2), sh);
+  return tail_x(A, g, irc, cx, cy, cz);
+}
+
+template <int S, class Acc>
+__device__ __forceinline__ double phi_y(const Acc &A, const Met &g, double irc) {
+  TBFP_MOM_ACCESSORS;
+  const bool sh = sharp_cell<S>(c(1, 0, 0), c(-1, 0, 0), c(0, 1, 0), c(0, 0, 0), c(0, 0, 1), c(0, 0, -1));
+  const double vc = v(0, 0, 0);
+  const double dyfj = g.dyf0, dyfp = g.dyf1, rycp = g.ryc1;
+  const double cx = conv_diff<S>(0.5 * (u(0, 1, 0) * dyfp + u(0, 0, 0) * dyfj) * rycp,
+                                 0.5 * (u(-1, 1, 0) * dyfp + u(-1, 0, 0) * dyfj) * rycp, v(-2, 0, 0), v(-1, 0, 0), vc,
+                                 v(1, 0, 0), v(2, 0, 0), sh);
+  const double cy = conv_diff<S>(0.5 * (vc + v(0, 1, 0)), 0.5 * (vc + v(0, -1, 0)), v(0, -2, 0), v(0, -1, 0), vc,
+                                 v(0, 1, 0), v(0, 2, 0), sh);
+  const double cz = conv_diff<S>(0.5 * (w(0, 1, 0) * dyfp + w(0, 0, 0) * dyfj) * rycp,
+                                 0.5 * (w(0, 1, -1) * dyfp + w(0, 0, -1) * dyfj) * rycp, v(0, 0, -2), v(0, 0, -1), vc,
+                                 v(0, 0, 1), v(0, 0, 2), sh);
+  return tail_y(A, g, irc, cx, cy, cz);
+}
+
+template <int S, class Acc>
+__device__ __forceinline__ double phi_z(const Acc &A, const Met &g, double irc) {
+  TBFP_MOM_ACCESSORS;
+  const bool sh = sharp_cell<S>(c(1, 0, 0), c(-1, 0, 0), c(0, 1, 0), c(0, -1, 0), c(0, 0, 1), c(0, 0, 0));
+  const double wc = w(0, 0, 0);
+  const double cx = conv_diff<S>(0.5 * (u(0, 0, 0) + u(0, 0, 1)), 0.5 * (u(-1, 0, 0) + u(-1, 0, 1)), w(-2, 0, 0),
+                                 w(-1, 0, 0), wc, w(1, 0, 0), w(2, 0, 0), sh);
+  const double cy = conv_diff<S>(0.5 * (v(0, 0, 0) + v(0, 0, 1)), 0.5 * (v(0, -1, 0) + v(0, -1, 1)), w(0, -2, 0),
+                                 w(0, -1, 0), wc, w(0, 1, 0), w(0, 2, 0), sh);
+  const double cz = conv_diff<S>(0.5 * (wc + w(0, 0, 1)), 0.5 * (wc + w(0, 0, -1)), w(0, 0, -2), w(0, 0, -1), wc,
+                                 w(0, 0, 1), w(0, 0, 2), sh);
+  return tail_z(A, g, irc, cx, cy, cz);
+}
 #undef TBFP_MOM_ACCESSORS
+
+// Computing each face once (schemes 0-4) costs a barrier, shared-memory
+// traffic and the edge faces; it pays where the limiter is expensive (van
+// Leer's and superbee's divisions and branches: 27 % and 22 % faster on
+// 512x384x256) and loses where it is cheap (central, upwind, QUICK: 8-10 %
+// slower), so those keep both faces per cell, as scheme 5 must.
+__host__ __device__ constexpr bool share_faces(int S) { return S == 3 || S == 4; }
 
 // Tiled form: block (32, 8) over a tile of (i, j) columns, i = 1..nx,
 // j = 1..ny, marching k over a chunk of kKC planes of 0..nz; each thread the
@@ -302,6 +428,9 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_momentum_fluxes(MomArgs a) {
   extern __shared__ double sm[];
   double *rU = sm, *rV = rU + kRV * kNV, *rW = rV + kRV * kNV;
   double *rM = rW + kRV * kNV, *rR = rM + kRC * kNC, *rC = rR + kRC * kNC;
+  // face fluxes of one plane (schemes 0-4): x faces [3][kTY][kTX+1], y faces [3][kTY+1][kTX]
+  double *fx = rC, *fy = fx + 3 * kTY * (kTX + 1);
+  double fzl0 = 0.0, fzl1 = 0.0, fzl2 = 0.0;  // lower z faces of the current plane
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
   const int i0 = blockIdx.x * kTX + 1, j0 = blockIdx.y * kTY + 1;
   const int kb = blockIdx.z * kKC, ke = min(kb + kKC - 1, a.nz);
@@ -362,22 +491,77 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_momentum_fluxes(MomArgs a) {
     for (int d = 0; d < 5; ++d) A.ov[d] = ((k + d - 2 + 3 * kRV) % kRV) * kNV;
 #pragma unroll
     for (int d = 0; d < 3; ++d) A.oc[d] = ((k + d - 1 + 3 * kRC) % kRC) * kNC;
-    if (in) {
-      const double irc = 1.0 / A.r(0, 0, 0);  // 1/rho of the own cell, shared by the three components
-      const Met g(a, i, j, k);
-      if (k >= 1) {
-        a.phx[box_x(a, i, j, k)] = phi_x<S>(A, g, irc);
-        if (j <= a.ny - 1) a.phy[box_y(a, i, j, k)] = phi_y<S>(A, g, irc);
+    if constexpr (!share_faces(S)) {
+      if (in) {
+        const double irc = 1.0 / A.r(0, 0, 0);  // 1/rho of the own cell, shared by the three components
+        const Met g(a, i, j, k);
+        if (k >= 1) {
+          a.phx[box_x(a, i, j, k)] = phi_x<S>(A, g, irc);
+          if (j <= a.ny - 1) a.phy[box_y(a, i, j, k)] = phi_y<S>(A, g, irc);
+        }
+        a.phz[box_z(a, i, j, k)] = phi_z<S>(A, g, irc);
       }
-      a.phz[box_z(a, i, j, k)] = phi_z<S>(A, g, irc);
+    } else {
+      // each face once: the cell's upper x, y faces into shared memory, its
+      // upper z faces in registers (the next plane's lower ones); the tile's
+      // lower edge faces by warp 0 (x, 8 rows) and warp 1 (y, 32 columns)
+      double fzn0 = 0.0, fzn1 = 0.0, fzn2 = 0.0;
+      if (in) {
+        const Met g(a, i, j, k);
+        fx[(0 * kTY + ty) * (kTX + 1) + tx + 1] = F_xx<S>(A);
+        fx[(1 * kTY + ty) * (kTX + 1) + tx + 1] = F_yx<S>(A, g);
+        fx[(2 * kTY + ty) * (kTX + 1) + tx + 1] = F_zx<S>(A);
+        fy[(0 * (kTY + 1) + ty + 1) * kTX + tx] = F_xy<S>(A);
+        fy[(1 * (kTY + 1) + ty + 1) * kTX + tx] = F_yy<S>(A);
+        fy[(2 * (kTY + 1) + ty + 1) * kTX + tx] = F_zy<S>(A);
+        fzn0 = F_xz<S>(A);
+        fzn1 = F_yz<S>(A, g);
+        fzn2 = F_zz<S>(A);
+        if (k == kb) {  // the chunk's first lower z faces (ux, uy need none at k = 0)
+          const SAcc B = A.down();
+          if (kb > 0) {
+            fzl0 = F_xz<S>(B);
+            fzl1 = F_yz<S>(B, g);
+          }
+          fzl2 = F_zz<S>(B);
+        }
+      }
+      if (ty == 0 && tx < kTY && j0 + tx <= a.ny) {
+        const SAcc E = A.shifted(-1 - tx, tx);
+        const Met ge(a, i0 - 1, j0 + tx, k);
+        fx[(0 * kTY + tx) * (kTX + 1)] = F_xx<S>(E);
+        fx[(1 * kTY + tx) * (kTX + 1)] = F_yx<S>(E, ge);
+        fx[(2 * kTY + tx) * (kTX + 1)] = F_zx<S>(E);
+      } else if (ty == 1 && i0 + tx <= a.nx) {
+        const SAcc E = A.shifted(0, -2);
+        fy[(0 * (kTY + 1)) * kTX + tx] = F_xy<S>(E);
+        fy[(1 * (kTY + 1)) * kTX + tx] = F_yy<S>(E);
+        fy[(2 * (kTY + 1)) * kTX + tx] = F_zy<S>(E);
+      }
+      __syncthreads();
+      if (in) {
+        const Met g(a, i, j, k);
+        const double irc = 1.0 / A.r(0, 0, 0);
+        auto cxd = [&](int c) { return fx[(c * kTY + ty) * (kTX + 1) + tx + 1] - fx[(c * kTY + ty) * (kTX + 1) + tx]; };
+        auto cyd = [&](int c) { return fy[(c * (kTY + 1) + ty + 1) * kTX + tx] - fy[(c * (kTY + 1) + ty) * kTX + tx]; };
+        if (k >= 1) {
+          a.phx[box_x(a, i, j, k)] = tail_x(A, g, irc, cxd(0), cyd(0), fzn0 - fzl0);
+          if (j <= a.ny - 1) a.phy[box_y(a, i, j, k)] = tail_y(A, g, irc, cxd(1), cyd(1), fzn1 - fzl1);
+        }
+        a.phz[box_z(a, i, j, k)] = tail_z(A, g, irc, cxd(2), cyd(2), fzn2 - fzl2);
+      }
+      fzl0 = fzn0;
+      fzl1 = fzn1;
+      fzl2 = fzn2;
     }
     cp_async_wait_all();
     __syncthreads();
   }
 }
 
-constexpr size_t tiled_smem_bytes(int S) {
-  return sizeof(double) * (3 * kRV * kNV + (S == 5 ? 3 : 2) * kRC * kNC);
+__host__ __device__ constexpr size_t tiled_smem_bytes(int S) {
+  return sizeof(double) * (3 * kRV * kNV + 2 * kRC * kNC + (S == 5 ? kRC * kNC : 0) +
+                           (share_faces(S) ? 3 * kTY * (kTX + 1) + 3 * (kTY + 1) * kTX : 0));
 }
 
 // the x component's face i = 0 (the periodic duplicate of i = nx, computed
