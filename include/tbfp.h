@@ -271,13 +271,16 @@ int tbfp_material_props_dev(tbfp_handle *h, const double *c, double *cs, double 
    phi_y (1:nx,1:ny-1,1:nz), phi_z (1:nx,1:ny,0:nz).  The spacings are the
    mesh's own metrics (grid.f90:334-399) including the ghost entries the
    stencils reach: dxf(0:nx+1), dxc(0:nx+1), dyf(0:ny+1), dyc(0:ny+1),
-   dzf(0:nz+1), dzc(0:nz+1), n+2 values each. */
+   dzf(0:nz+1), dzc(0:nz+1), n+2 values each.  yc(0:ny+1), yf(0:ny) and the
+   wall values serve tbfp_update_boundaries_v. */
 typedef struct {
   int scheme; /* specs/schemes convection_scheme: 0 central, 1 upwind, 2 QUICK, 3 van Leer,
                  4 superbee, 5 superbee where the volume fraction varies, central elsewhere */
   double gch; /* specs/parameters gCH: streamwise driving added to ux */
   double g;   /* specs/parameters g: body force added to uy */
   const double *dxf, *dxc, *dyf, *dyc, *dzf, *dzc;
+  const double *yc, *yf;       /* y centroids (0:ny+1) and faces (0:ny) */
+  double ubot[3], utop[3];     /* fixedValue of ux, uy, uz at the bottom and top walls (bvx3, bvx4, ...) */
 } tbfp_momentum_desc;
 int tbfp_momentum_setup(tbfp_handle *h, const tbfp_momentum_desc *m);
 int tbfp_momentum_fluxes(tbfp_handle *h, double *phi_x, double *phi_y, double *phi_z, int set);
@@ -287,6 +290,16 @@ int tbfp_momentum_predictor(tbfp_handle *h, double *ux, double *uy, double *uz, 
 int tbfp_momentum_predictor_dev(tbfp_handle *h, double *ux, double *uy, double *uz, const double *c,
                                 const double *mu, const double *rho, const double *const *st, double dt,
                                 double alpha, double gamma, double xi, double rho0, double fs);
+/* updateBoundariesV (vfield.f90:111-189) for the channel, in place on u: the
+   fixedValue walls in y (one ghost layer, boundaryField_S.f90:593-690, with
+   the spacings of setMetrics :138-214), the periodic halos in x and z
+   (updateHalo, field.f90:708-946, the rank being its own neighbour) and the
+   periodic duplicates ux(0,:,:) = ux(nx,:,:), uz(:,:,0) = uz(:,:,nz).  Other
+   y-ghost layers are only copied periodically, as in the reference.
+   solveMomentumEqn is tbfp_momentum_predictor followed by this call.  Needs
+   tbfp_momentum_setup. */
+int tbfp_update_boundaries_v(tbfp_handle *h, double *ux, double *uy, double *uz);
+int tbfp_update_boundaries_v_dev(tbfp_handle *h, double *ux, double *uy, double *uz);
 
 /* --- slab form: one channel split over several GPUs --------------------- */
 /* One rank's share of a channel split over P ranks (the reference's pencil

@@ -217,6 +217,54 @@ def equate_periodic_bc(ux: FField, uz: FField) -> None:
     uz.v(uz.lb[0], uz.ub[0], uz.lb[1], uz.ub[1], 0, 0)[...] = uz.v(uz.lb[0], uz.ub[0], uz.lb[1], uz.ub[1], uz.nz, uz.nz)
 
 
+def wall_metrics(mesh: Mesh, kind: str):
+    """setMetrics (boundaryField_S.f90:138-214) at the y walls:
+    ((dhb, dhi) of the bottom, (dhb, dhi) of the top) for a field of type kind."""
+    ny = mesh.ny
+    if kind == "sy":
+        return ((mesh.dyf[0], mesh.dyf[0] + mesh.dyf[1]), (mesh.dyf[ny + 1], mesh.dyf[ny] + mesh.dyf[ny + 1]))
+    return ((mesh.yf[0] - mesh.yc[0], mesh.dyc[1]), (mesh.yc[ny + 1] - mesh.yf[ny], mesh.dyc[ny + 1]))
+
+
+def update_boundaries_v_channel(mesh: Mesh, ux: FField, uy: FField, uz: FField, ubot=(0.0, 0.0, 0.0),
+                                utop=(0.0, 0.0, 0.0)) -> None:
+    """updateBoundariesV (vfield.f90:111-119) for the channel on one rank.  Per
+    component, updateBoundaries (field.f90:950-974): the fixedValue walls in y
+    (updateFixedValueBoundary, boundaryField_S.f90:593-690: one ghost layer over
+    the interior i, k range, from the first interior layer -- the second for a
+    'sy' field, whose walls are the faces j = 0 and ny -- with setMetrics'
+    spacings), then the periodic halo exchanges in x and then z over the full
+    extended ranges (updateHalo, field.f90:708-946; the rank is its own x and z
+    neighbour, y has none); then equatePeriodicBC (vfield.f90:124-189).  ubot,
+    utop: the wall values of ux, uy, uz (bvx3/bvx4 ... of the case's u file)."""
+    for f, bb, bt in zip((ux, uy, uz), ubot, utop):
+        nx, ny, nz, hd = f.nx, f.ny, f.nz, f.hd
+        is_, js, ks = _KIND_LO[f.kind]
+        ie, je, ke = nx, ny, nz
+        (hb, hi), (tb, ti) = wall_metrics(mesh, f.kind)
+        jb = js + 1 if f.kind == "sy" else js
+        jt = je - 1 if f.kind == "sy" else je
+        f.v(is_, ie, js - 1, js - 1, ks, ke)[...] = (f.v(is_, ie, jb, jb, ks, ke) * hb - bb * hi) / (hb - hi)
+        f.v(is_, ie, je + 1, je + 1, ks, ke)[...] = (f.v(is_, ie, jt, jt, ks, ke) * tb - bt * ti) / (tb - ti)
+        il, ih, jl, jh, kl, kh = is_ - hd, ie + hd, js - hd, je + hd, ks - hd, ke + hd
+        # x: receive from the right into ie+1.. what it sends to the left, and
+        # from the left into is-hd.. what it sends to the right
+        if f.kind == "sx":
+            f.v(ie + 1, ie + hd, jl, jh, kl, kh)[...] = f.v(is_ + 1, is_ + hd, jl, jh, kl, kh)
+            f.v(is_ - hd, is_ - 1, jl, jh, kl, kh)[...] = f.v(ie - hd, ie - 1, jl, jh, kl, kh)
+        else:
+            f.v(ie + 1, ie + hd, jl, jh, kl, kh)[...] = f.v(is_, is_ + hd - 1, jl, jh, kl, kh)
+            f.v(is_ - hd, is_ - 1, jl, jh, kl, kh)[...] = f.v(ie - hd + 1, ie, jl, jh, kl, kh)
+        # z over all i, j
+        if f.kind == "sz":
+            f.v(il, ih, jl, jh, ke + 1, ke + hd)[...] = f.v(il, ih, jl, jh, ks + 1, ks + hd)
+            f.v(il, ih, jl, jh, ks - hd, ks - 1)[...] = f.v(il, ih, jl, jh, ke - hd, ke - 1)
+        else:
+            f.v(il, ih, jl, jh, ke + 1, ke + hd)[...] = f.v(il, ih, jl, jh, ks, ks + hd - 1)
+            f.v(il, ih, jl, jh, ks - hd, ks - 1)[...] = f.v(il, ih, jl, jh, ke - hd + 1, ke)
+    equate_periodic_bc(ux, uz)
+
+
 # ---------------------------------------------------------------------------
 # poissonEqn.f90 (FAST_MODE): split right-hand side
 # ---------------------------------------------------------------------------

@@ -65,7 +65,8 @@ class TbfpVofDesc(C.Structure):
 
 class TbfpMomentumDesc(C.Structure):
     _fields_ = [("scheme", C.c_int), ("gch", C.c_double), ("g", C.c_double)] + [
-        (n, C.c_void_p) for n in ("dxf", "dxc", "dyf", "dyc", "dzf", "dzc")]
+        (n, C.c_void_p) for n in ("dxf", "dxc", "dyf", "dyc", "dzf", "dzc", "yc", "yf")] + [
+        ("ubot", C.c_double * 3), ("utop", C.c_double * 3)]
 
 
 class TbfpMemberIO(C.Structure):
@@ -114,6 +115,8 @@ PROTOTYPES = {
     "tbfp_momentum_fluxes": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "tbfp_momentum_predictor": (C.c_int, [_H] + [C.c_void_p] * 7 + [C.c_double] * 6),
     "tbfp_momentum_predictor_dev": (C.c_int, [_H] + [C.c_void_p] * 7 + [C.c_double] * 6),
+    "tbfp_update_boundaries_v": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tbfp_update_boundaries_v_dev": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tbfp_material_props": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tbfp_material_props_dev": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tbfp_pcg_solve": (C.c_int, [_H, _P, _P, _P, C.POINTER(TbfpStats)]),

@@ -78,6 +78,7 @@ struct tbfp_handle {
   int phi_cur = 0;
   size_t n_phi[3] = {0, 0, 0};
   double *h_mom[2] = {nullptr, nullptr};  // c, mu copies for tbfp_momentum_predictor
+  WallTabs wt{};                           // updateBoundariesV wall spacings and values
   MgSolver *mg = nullptr;   // MG_MODE hierarchy (tbfp_pcg_setup)
   std::vector<double> mdxf, mdxc, mdyf, mdyc, mdzf, mdzc;  // caller's metrics, kept for tbfp_pcg_setup
   double *h_beta = nullptr, *h_q = nullptr;                // device copies for tbfp_pcg_solve
@@ -1146,8 +1147,8 @@ int tbfp_momentum_setup(tbfp_handle *h, const tbfp_momentum_desc *m) {
   if (m->scheme < 0 || m->scheme > 5) return set_err(h, TBFP_EINVAL, "tbfp_momentum_setup: scheme must be 0..5");
   if (h->hd_u < 2 || h->hd_rho < 1)
     return set_err(h, TBFP_EINVAL, "tbfp_momentum_setup: needs hd_u >= 2 and hd_rho >= 1");
-  if (!m->dxf || !m->dxc || !m->dyf || !m->dyc || !m->dzf || !m->dzc)
-    return set_err(h, TBFP_ENULL, "tbfp_momentum_setup: a spacing table is NULL");
+  if (!m->dxf || !m->dxc || !m->dyf || !m->dyc || !m->dzf || !m->dzc || !m->yc || !m->yf)
+    return set_err(h, TBFP_ENULL, "tbfp_momentum_setup: a spacing or coordinate table is NULL");
   const int nx = h->nx, ny = h->ny, nz = h->nz;
   // spacings by Fortran index 0..n+1, as the mesh holds them
   std::vector<double> dxf(m->dxf, m->dxf + nx + 2), dxc(m->dxc, m->dxc + nx + 2);
@@ -1174,6 +1175,22 @@ int tbfp_momentum_setup(tbfp_handle *h, const tbfp_momentum_desc *m) {
       if ((rc = dev_alloc(h, &h->d_phi[b][c], h->n_phi[c]))) return rc;
       TBFP_CK(h, cudaMemset(h->d_phi[b][c], 0, h->n_phi[c] * sizeof(double)));  // initFluxes
     }
+  // setMetrics at the y walls: 'cl'-type spacings for ux and uz, face spacings for uy
+  for (int e = 0; e < 3; ++e) {
+    if (e == 1) {
+      h->wt.hb[e] = m->dyf[0];
+      h->wt.hi[e] = m->dyf[0] + m->dyf[1];
+      h->wt.tb[e] = m->dyf[ny + 1];
+      h->wt.ti[e] = m->dyf[ny] + m->dyf[ny + 1];
+    } else {
+      h->wt.hb[e] = m->yf[0] - m->yc[0];
+      h->wt.hi[e] = m->dyc[1];
+      h->wt.tb[e] = m->yc[ny + 1] - m->yf[ny];
+      h->wt.ti[e] = m->dyc[ny + 1];
+    }
+    h->wt.bb[e] = m->ubot[e];
+    h->wt.bt[e] = m->utop[e];
+  }
   h->mom_scheme = m->scheme;
   h->mom_gch = m->gch;
   h->mom_g = m->g;
@@ -1218,6 +1235,31 @@ int tbfp_momentum_predictor_dev(tbfp_handle *h, double *ux, double *uy, double *
                   h->stream);
   h->phi_cur = cur;
   return finish(h, "tbfp_momentum_predictor");
+}
+
+int tbfp_update_boundaries_v_dev(tbfp_handle *h, double *ux, double *uy, double *uz) {
+  int rc = check_ptrs(h, {ux, uy, uz});
+  if (rc) return rc;
+  if (!h->mom) return set_err(h, TBFP_EINVAL, "tbfp_update_boundaries_v: call tbfp_momentum_setup first");
+  cudaSetDevice(h->device);
+  launch_boundaries_v(h->wt, ux, uy, uz, h->Lux, h->Luy, h->Luz, h->nx, h->ny, h->nz, h->hd_u, h->stream);
+  return finish(h, "tbfp_update_boundaries_v");
+}
+
+int tbfp_update_boundaries_v(tbfp_handle *h, double *ux, double *uy, double *uz) {
+  int rc = check_ptrs(h, {ux, uy, uz});
+  if (rc) return rc;
+  if (!h->mom) return set_err(h, TBFP_EINVAL, "tbfp_update_boundaries_v: call tbfp_momentum_setup first");
+  cudaSetDevice(h->device);
+  if ((rc = ensure_host_bufs(h, false))) return rc;
+  if ((rc = h2d(h, h->h_ux, ux, h->n_ux)) || (rc = h2d(h, h->h_uy, uy, h->n_uy)) || (rc = h2d(h, h->h_uz, uz, h->n_uz)))
+    return rc;
+  launch_boundaries_v(h->wt, h->h_ux, h->h_uy, h->h_uz, h->Lux, h->Luy, h->Luz, h->nx, h->ny, h->nz, h->hd_u,
+                      h->stream);
+  if ((rc = d2h(h, ux, h->h_ux, h->n_ux)) || (rc = d2h(h, uy, h->h_uy, h->n_uy)) || (rc = d2h(h, uz, h->h_uz, h->n_uz)))
+    return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return finish(h, "tbfp_update_boundaries_v");
 }
 
 int tbfp_momentum_predictor(tbfp_handle *h, double *ux, double *uy, double *uz, const double *c, const double *mu,

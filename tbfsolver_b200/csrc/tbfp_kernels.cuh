@@ -239,6 +239,14 @@ void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, 
                      double alpha, double gamma, double xi, double rho0, double fs, double gch, double g, int hdu,
                      int hdc, cudaStream_t st_);
 
+// updateBoundariesV for the channel: the y-wall spacings of setMetrics (dhb,
+// dhi at the bottom and top) and the wall values, per component ux, uy, uz
+struct WallTabs {
+  double hb[3], hi[3], tb[3], ti[3], bb[3], bt[3];
+};
+void launch_boundaries_v(const WallTabs &w, double *ux, double *uy, double *uz, Lay Lux, Lay Luy, Lay Luz, int nx,
+                         int ny, int nz, int hd, cudaStream_t st);
+
 // MG_MODE source/beta (computeSource MG, computeBeta) and addPressureGrad.
 // idxc, idzc: 1/dxc(i), 1/dzc(k) for Fortran i = 1..nx+1 (0-based tables).
 void launch_mg_source_beta(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz,

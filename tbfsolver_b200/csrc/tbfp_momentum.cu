@@ -629,6 +629,75 @@ __global__ void __launch_bounds__(kMT) k_momentum_update(MomUpd a) {
   a.uz[o] = u + a.invrho0 * a.r * st;
 }
 
+// updateBoundariesV for the channel (vfield.f90:111-189): fixedValue walls in
+// y, periodic halos in x and z, the periodic duplicates ux(0) = ux(nx),
+// uz(0) = uz(nz).  The reference's sequence (wall ghost layer on the interior
+// i, k range; x exchange over all j, k; z exchange over whole planes; equate)
+// leaves every written element equal to a function of elements it never
+// writes: with mx(i) = i + nx for i < 1, i - nx for i > nx (the equate is
+// mx(0) = nx), likewise mz, the element (i, j, k) becomes
+//   j = js-1 or je+1 (the wall ghosts): the wall formula of (mx(i), jb/jt, mz(k)),
+//   any other j:                        the element (mx(i), j, mz(k)),
+// so one gather pass in place is race-free.  It visits the halo planes
+// k < 1 and k > nz (all i, j) and, for k = 1..nz, the wall ghost rows (all i)
+// and the x halo columns (and ux's i = 0) of the other rows.
+struct BcComp {
+  double *f;
+  Lay L;
+  int ilo, ihi, jlo, jhi, klo, khi;  // allocated extents
+  int js, je, jb, jt;                // interior j range, the wall formulas' source rows
+  double hb, hi, tb, ti, bb, bt;     // dhb, dhi and wall value: bottom, top
+  long n_planes, n_total;            // elements visited in the halo planes; in all
+};
+struct BcArgs {
+  BcComp c[3];
+  int nx, nz;
+};
+
+__device__ __forceinline__ double wall(double v, double dhb, double dhi, double bf) {
+  // (f*dhb - bf*dhi)/(dhb - dhi), rounded as written
+  return __ddiv_rn(__dsub_rn(__dmul_rn(v, dhb), __dmul_rn(bf, dhi)), __dsub_rn(dhb, dhi));
+}
+
+__global__ void __launch_bounds__(256) k_boundaries_v(BcArgs a) {
+  const BcComp &c = a.c[blockIdx.y];
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= c.n_total) return;
+  const int NI = c.ihi - c.ilo + 1, NJ = c.jhi - c.jlo + 1;
+  int i, j, k;
+  if (t < c.n_planes) {
+    const long pl = NI * (long)NJ;
+    const int p = (int)(t / pl), r = (int)(t - p * pl);
+    const int nlow = 1 - c.klo;  // planes klo..0
+    k = p < nlow ? c.klo + p : a.nz + 1 + (p - nlow);
+    j = c.jlo + r / NI;
+    i = c.ilo + r % NI;
+  } else {
+    const long u = t - c.n_planes;
+    const int nxh = (1 - c.ilo) + (c.ihi - a.nx);  // x halo columns (ux: with i = 0)
+    const long per_k = 2L * NI + (long)(NJ - 2) * nxh;
+    k = 1 + (int)(u / per_k);
+    const int r = (int)(u - (k - 1) * per_k);
+    if (r < 2 * NI) {
+      j = r < NI ? c.js - 1 : c.je + 1;
+      i = c.ilo + r % NI;
+    } else {
+      const int q = r - 2 * NI, jj = q / nxh, ii = q - jj * nxh;
+      j = c.jlo + jj;
+      if (j >= c.js - 1) ++j;
+      if (j >= c.je + 1) ++j;
+      i = ii < 1 - c.ilo ? c.ilo + ii : a.nx + 1 + (ii - (1 - c.ilo));
+    }
+  }
+  const int mi = i < 1 ? i + a.nx : (i > a.nx ? i - a.nx : i);
+  const int mk = k < 1 ? k + a.nz : (k > a.nz ? k - a.nz : k);
+  double v;
+  if (j == c.js - 1) v = wall(c.f[at(c.L, mi, c.jb, mk)], c.hb, c.hi, c.bb);
+  else if (j == c.je + 1) v = wall(c.f[at(c.L, mi, c.jt, mk)], c.tb, c.ti, c.bt);
+  else v = c.f[at(c.L, mi, j, mk)];
+  c.f[at(c.L, i, j, k)] = v;
+}
+
 }  // namespace
 
 void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, const double *c, const double *mu,
@@ -706,6 +775,44 @@ void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, 
   b.ny = ny;
   b.nz = nz;
   k_momentum_update<<<grid, kMT, 0, st_>>>(b);
+}
+
+void launch_boundaries_v(const WallTabs &w, double *ux, double *uy, double *uz, Lay Lux, Lay Luy, Lay Luz, int nx,
+                         int ny, int nz, int hd, cudaStream_t st) {
+  BcArgs a{};
+  a.nx = nx;
+  a.nz = nz;
+  double *f[3] = {ux, uy, uz};
+  const Lay L[3] = {Lux, Luy, Luz};
+  long most = 0;
+  for (int e = 0; e < 3; ++e) {
+    BcComp &c = a.c[e];
+    const int is = e == 0 ? 0 : 1, js = e == 1 ? 0 : 1, ks = e == 2 ? 0 : 1;
+    c.f = f[e];
+    c.L = L[e];
+    c.ilo = is - hd;
+    c.ihi = nx + hd;
+    c.jlo = js - hd;
+    c.jhi = ny + hd;
+    c.klo = ks - hd;
+    c.khi = nz + hd;
+    c.js = js;
+    c.je = ny;
+    c.jb = e == 1 ? js + 1 : js;
+    c.jt = e == 1 ? ny - 1 : ny;
+    c.hb = w.hb[e];
+    c.hi = w.hi[e];
+    c.tb = w.tb[e];
+    c.ti = w.ti[e];
+    c.bb = w.bb[e];
+    c.bt = w.bt[e];
+    const long NI = c.ihi - c.ilo + 1, NJ = c.jhi - c.jlo + 1;
+    const long nplanes = (1 - c.klo) + hd, nxh = (1 - c.ilo) + hd;
+    c.n_planes = nplanes * NI * NJ;
+    c.n_total = c.n_planes + (long)nz * (2 * NI + (NJ - 2) * nxh);
+    most = c.n_total > most ? c.n_total : most;
+  }
+  k_boundaries_v<<<dim3((unsigned)((most + 255) / 256), 3), 256, 0, st>>>(a);
 }
 
 }  // namespace tbfp

@@ -202,3 +202,23 @@ class ParFile:
 
     def read_string(self, name: str) -> str:
         return self._value(name).rstrip(" ")
+
+
+def velocity_walls(specs_dir: str):
+    """The y-wall values of u from the case's boundary file specs/fstart_bc/u
+    (read by vfieldCTOR / boundaryFieldCTOR through parFile: bx1..bx6 the types
+    of the six patches, bvx1..bvx6 their values; likewise y, z).  The library
+    runs the channel: periodic (type 3) in x and z, fixedValue (type 1) at the
+    bottom (patch 3) and top (patch 4); anything else is an error.  Returns
+    ((ux, uy, uz) at the bottom, (ux, uy, uz) at the top); no file gives the
+    no-slip zeros."""
+    path = os.path.join(specs_dir, "fstart_bc", "u")
+    if not os.path.exists(path):
+        return (0.0, 0.0, 0.0), (0.0, 0.0, 0.0)
+    bc = ParFile("u", os.path.dirname(path))
+    for comp in "xyz":
+        types = [bc.read_int(f"b{comp}{n}") for n in range(1, 7)]
+        if types != [3, 3, 1, 1, 3, 3]:
+            raise ValueError(f"velocity boundaries of u{comp}: patch types {types}; the channel (periodic x "
+                             "and z, fixedValue walls in y) is supported")
+    return (tuple(bc.read_real(f"bv{c}3") for c in "xyz"), tuple(bc.read_real(f"bv{c}4") for c in "xyz"))

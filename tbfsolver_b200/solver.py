@@ -281,25 +281,32 @@ class MomentumEqn:
     the library; fluxes() / set_fluxes() read and load it (printOldTimeFlux /
     initOldTimeFlux)."""
 
-    def __init__(self, solver: FastPoissonSolver, scheme: int = 2, gch: float = 0.0, g: float = 0.0):
+    def __init__(self, solver: FastPoissonSolver, scheme: int = 2, gch: float = 0.0, g: float = 0.0,
+                 ubot=(0.0, 0.0, 0.0), utop=(0.0, 0.0, 0.0)):
         self.solver = solver
         g_ = solver.mesh
         self._t = {n: np.ascontiguousarray(getattr(g_, n).r(0, nn + 1))
                    for n, nn in (("dxf", g_.nx), ("dxc", g_.nx), ("dyf", g_.ny), ("dyc", g_.ny), ("dzf", g_.nz),
-                                 ("dzc", g_.nz))}
-        m = TbfpMomentumDesc(scheme=scheme, gch=gch, g=g, **{n: a.ctypes.data_as(C.c_void_p).value
-                                                             for n, a in self._t.items()})
+                                 ("dzc", g_.nz), ("yc", g_.ny))}
+        self._t["yf"] = np.ascontiguousarray(g_.yf.r(0, g_.ny))
+        m = TbfpMomentumDesc(scheme=scheme, gch=gch, g=g, ubot=(C.c_double * 3)(*ubot),
+                             utop=(C.c_double * 3)(*utop),
+                             **{n: a.ctypes.data_as(C.c_void_p).value for n, a in self._t.items()})
         check(solver.lib.tbfp_momentum_setup(solver.h, C.byref(m)), solver.h)
 
     @classmethod
     def from_specs(cls, solver: FastPoissonSolver, specs_dir: str) -> "MomentumEqn":
         """Settings read as momentumEqnCTOR reads them: convection_scheme from
-        specs/schemes, g and gCH from specs/parameters."""
+        specs/schemes, g and gCH from specs/parameters; the wall values from
+        specs/fstart_bc/u when present."""
         from .io import ParFile  # noqa: PLC0415
 
+        from .io import velocity_walls  # noqa: PLC0415
+
         par = ParFile("parameters", specs_dir)
+        ubot, utop = velocity_walls(specs_dir)
         return cls(solver, scheme=ParFile("schemes", specs_dir).read_int("convection_scheme"),
-                   gch=par.read_real("gCH"), g=par.read_real("g"))
+                   gch=par.read_real("gCH"), g=par.read_real("g"), ubot=ubot, utop=utop)
 
     def _shapes(self):
         m = self.solver.mesh
@@ -353,6 +360,21 @@ class MomentumEqn:
                 io.read_field(case_dir, n, "phi0" + comp, f)
             hist.append(np.ascontiguousarray(f.v(*b)))
         self.set_fluxes(hist)
+
+    def update_boundaries_v(self, u: VField) -> None:
+        """updateBoundariesV (vfield.f90:111-189): wall ghosts, periodic halos and
+        duplicates of u, in place."""
+        sv = self.solver
+        dev = _placement(list(u.components()))
+        fn = sv.lib.tbfp_update_boundaries_v_dev if dev else sv.lib.tbfp_update_boundaries_v
+        check(fn(sv.h, u.ux.address(), u.uy.address(), u.uz.address()), sv.h)
+
+    def solve(self, u: VField, c: Field, mu: Field, rho: Field, dt: float, alpha: float, gamma: float, xi: float,
+              rho0: float, fs: float = 0.0, st=None) -> None:
+        """solveMomentumEqn (momentumEqn.f90:161-194): the predictor, then
+        updateBoundariesV, so u comes out ready for the next step's stencils."""
+        self.predictor(u, c, mu, rho, dt, alpha, gamma, xi, rho0, fs, st)
+        self.update_boundaries_v(u)
 
     def predictor(self, u: VField, c: Field, mu: Field, rho: Field, dt: float, alpha: float, gamma: float,
                   xi: float, rho0: float, fs: float = 0.0, st=None) -> None:

@@ -98,3 +98,22 @@ def test_reads_the_reference_case_specs():
     assert pcg.read_real("tolMG") == 0.4 and pcg.read_real("tolPCG") == 1e-10
     par = io.ParFile("parameters", SPECS)
     assert par.read_real("rhog") == 0.1 and par.read_real("mul") == 3.33333333333333e-4
+
+
+def test_velocity_walls_from_the_boundary_file(tmp_path):
+    """specs/fstart_bc/u in the case's format: periodic x, z and fixedValue walls
+    give the wall values; another patch type is refused; no file is no-slip."""
+    from tbfsolver_b200.io import velocity_walls
+
+    assert velocity_walls(str(tmp_path)) == ((0.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+    d = tmp_path / "fstart_bc"
+    d.mkdir()
+    lines = ["! header", "gridx_type sx", "init_opt 2"]
+    for c, top in zip("xyz", ("1.5d0", "0.d0", "-2.5d-1")):
+        lines += [f"b{c}{n} {t}" for n, t in zip(range(1, 7), (3, 3, 1, 1, 3, 3))]
+        lines += [f"bv{c}1 0.d0", f"bv{c}2 0.d0", f"bv{c}3 0.d0", f"bv{c}4 {top}", f"bv{c}5 0.d0", f"bv{c}6 0.d0"]
+    (d / "u").write_text("\n".join(lines) + "\n")
+    assert velocity_walls(str(tmp_path)) == ((0.0, 0.0, 0.0), (1.5, 0.0, -0.25))
+    (d / "u").write_text("\n".join(lines).replace("by3 1", "by3 2") + "\n")
+    with pytest.raises(ValueError):
+        velocity_walls(str(tmp_path))

@@ -219,3 +219,75 @@ def test_flux_history_round_trips_through_phi0_files(tmp_path):
         got = mom.fluxes()
     assert np.array_equal(got[0], hist[0]) and np.array_equal(got[1], hist[1])
     assert not got[2].any()
+
+
+# --- updateBoundariesV --------------------------------------------------------
+def test_wall_ghosts_mirror_the_first_layer_on_a_uniform_grid():
+    """No-slip walls on a uniform grid: the wall sits halfway between the ghost
+    and the first cell centre (ux, uz), or the ghost face mirrors face 1 about
+    the wall face (uy), so the ghost is minus the first value (to the rounding
+    of the coordinate differences in setMetrics); the x and z halos and the
+    periodic duplicates are copies."""
+    nx, ny, nz = 8, 6, 4
+    g = _grid(nx, ny, nz, False)
+    m = mesh_of(g)
+    u = _velocity(g, 21)
+    O.update_boundaries_v_channel(m, *u)
+    ux, uy, uz = u
+    assert np.allclose(ux.v(0, nx, 0, 0, 1, nz), -ux.v(0, nx, 1, 1, 1, nz), rtol=1e-13, atol=0)
+    assert np.allclose(ux.v(0, nx, ny + 1, ny + 1, 1, nz), -ux.v(0, nx, ny, ny, 1, nz), rtol=1e-13, atol=0)
+    assert np.allclose(uy.v(1, nx, -1, -1, 1, nz), -uy.v(1, nx, 1, 1, 1, nz), rtol=1e-13, atol=0)
+    assert np.allclose(uz.v(1, nx, 0, 0, 0, nz), -uz.v(1, nx, 1, 1, 0, nz), rtol=1e-13, atol=0)
+    full = (-HD_U + 1, ny + HD_U, -HD_U + 1, nz + HD_U)
+    assert np.array_equal(ux.v(-2, -1, *full), ux.v(nx - 2, nx - 1, *full))
+    assert np.array_equal(ux.v(0, 0, *full), ux.v(nx, nx, *full))
+    assert np.array_equal(uz.v(-1, nx + 2, -1, ny + 2, 0, 0), uz.v(-1, nx + 2, -1, ny + 2, nz, nz))
+    assert np.array_equal(uy.v(-1, nx + 2, -2, ny + 2, nz + 1, nz + 2), uy.v(-1, nx + 2, -2, ny + 2, 1, 2))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("hd,where", [(2, "device"), (2, "host"), (3, "device")])
+def test_boundaries_match_the_oracle_bit_for_bit(hd, where):
+    """tbfp_update_boundaries_v against the oracle's literal sequence (walls,
+    x exchange, z exchange, equate) on random arrays, moving walls included."""
+    from tbfsolver_b200.fields import field_shape as fsh
+
+    nx, ny, nz = 24, 20, 12
+    g = _grid(nx, ny, nz, True)
+    rng = np.random.default_rng(hd)
+    u = [O.FField(k, hd, nx, ny, nz, rng.standard_normal(fsh(k, hd, nx, ny, nz))) for k in ("sx", "sy", "sz")]
+    ub, ut = (0.25, 0.0, -0.5), (1.0, 0.0, 0.125)
+    with FastPoissonSolver(g, hd_u=hd) as fps:
+        mom = MomentumEqn(fps, scheme=2, ubot=ub, utop=ut)
+        du = VField(*[_to_dev(f, where) for f in u])
+        mom.update_boundaries_v(du)
+        got = [_host(f) for f in du.components()]
+    O.update_boundaries_v_channel(mesh_of(g), *u, ub, ut)
+    for a, b in zip(got, u):
+        assert np.array_equal(a, b.a)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scheme", [2, 4])
+def test_two_momentum_steps_with_boundaries_match_the_oracle(scheme):
+    """solveMomentumEqn twice (predictor + updateBoundariesV, AB2 on the second
+    step): the second step's stencils read the halos the first one refreshed."""
+    nx, ny, nz = 32, 24, 16
+    g = _grid(nx, ny, nz, True)
+    m = mesh_of(g)
+    u = _velocity(g, 5)
+    c, mu, rho = _props(g, 6)
+    O.update_boundaries_v_channel(m, *u)
+    kw = dict(dt=2e-3, alpha=1.0, rho0=0.02)
+    with FastPoissonSolver(g, hd_u=HD_U, hd_rho=HD_RHO) as fps:
+        mom = MomentumEqn(fps, scheme=scheme, gch=0.4)
+        du = VField(*[_to_dev(f, "device") for f in u])
+        dc, dmu, drho = (_to_dev(f, "device") for f in (c, mu, rho))
+        prev = [np.zeros(s) for s in mom._shapes()]
+        for gamma, xi in ((1.0, 0.0), (1.5, -0.5)):
+            mom.solve(du, dc, dmu, drho, gamma=gamma, xi=xi, **kw)
+            prev = O.momentum_predictor(m, *u, c, mu, rho, prev, kw["dt"], kw["alpha"], gamma, xi, kw["rho0"],
+                                        gch=0.4, scheme=scheme)
+            O.update_boundaries_v_channel(m, *u)
+            for got, want in zip(du.components(), u):
+                assert rel_linf(_host(got), want.a) < 1e-13
