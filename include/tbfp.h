@@ -169,8 +169,8 @@ int tbfp_rhs_split_dev(tbfp_handle *h, const double *ux, const double *uy, const
 /* --- makeVelocityDivFree, FAST_MODE (momentumEqn.f90:999-1127) --------- */
 /* In place on ux, uy, uz: faces of setEqnBounds (momentumEqn.f90:1134-1190)
    are corrected and the periodic duplicate faces are equated
-   (vfield.f90:124-189).  The remaining ghost/halo refresh of u is left to the
-   caller's updateBoundariesV, as in the reference. */
+   (vfield.f90:124-189).  The rest of the routine's closing updateBoundariesV
+   (momentumEqn.f90:1088: wall ghosts and halos) is tbfp_update_boundaries_v. */
 int tbfp_correct(tbfp_handle *h, double *ux, double *uy, double *uz, const double *psi,
                  const double *psi_n, const double *psi_nm1, const double *rho,
                  const double *const *st_n, const double *const *st_nm1,
@@ -300,6 +300,22 @@ int tbfp_momentum_predictor_dev(tbfp_handle *h, double *ux, double *uy, double *
    tbfp_momentum_setup. */
 int tbfp_update_boundaries_v(tbfp_handle *h, double *ux, double *uy, double *uz);
 int tbfp_update_boundaries_v_dev(tbfp_handle *h, double *ux, double *uy, double *uz);
+
+/* --- flow control (auxiliaryRoutines.f90:336-540) ----------------------- */
+/* Volume sums over the ux faces i = 0..nx-1, j = 1..ny, k = 1..nz with the
+   staggered volume Vsx = dxc(i+1)*dyf(j)*dzf(k) (grid.f90:812-838):
+   tbfp_rho_face_sum: sum of 0.5*(rho(i+1)+rho(i))*Vsx, setPressGrad's rho_sum
+   (its mean density is the sum over s_Vg; fs follows on the host);
+   tbfp_flow_rate: sum of ux*Vsx, computeFlowRate's Q.  On a slab handle the
+   sums cover the local planes and the caller adds them over the ranks (the
+   reference's Mpi_Allreduce).  tbfp_add_ux: ux(0:nx,1:ny,1:nz) += uf,
+   setFlowRate's shift (updateBoundariesV follows). */
+int tbfp_rho_face_sum(tbfp_handle *h, const double *rho, double *sum);
+int tbfp_rho_face_sum_dev(tbfp_handle *h, const double *rho, double *sum);
+int tbfp_flow_rate(tbfp_handle *h, const double *ux, double *q);
+int tbfp_flow_rate_dev(tbfp_handle *h, const double *ux, double *q);
+int tbfp_add_ux(tbfp_handle *h, double *ux, double uf);
+int tbfp_add_ux_dev(tbfp_handle *h, double *ux, double uf);
 
 /* --- slab form: one channel split over several GPUs --------------------- */
 /* One rank's share of a channel split over P ranks (the reference's pencil

@@ -265,6 +265,52 @@ def update_boundaries_v_channel(mesh: Mesh, ux: FField, uy: FField, uz: FField, 
     equate_periodic_bc(ux, uz)
 
 
+def _seq_sum(v: np.ndarray) -> float:
+    """A sum in element order (loop order), one rounding per addition."""
+    return float(np.cumsum(np.concatenate(([0.0], np.ravel(v))))[-1])
+
+
+def staggered_x_volume(mesh: Mesh) -> np.ndarray:
+    """Vsx(i,j,k) = dxc(i+1)*dyf(j)*dzf(k), i = 0..nx (grid.f90:812-838), as (nz, ny, nx+1)."""
+    dx = mesh.dxc.r(1, mesh.nx + 1)[None, None, :]
+    return (dx * mesh.dyf.r(1, mesh.ny)[None, :, None]) * mesh.dzf.r(1, mesh.nz)[:, None, None]
+
+
+def set_press_grad(mesh: Mesh, rho: FField, flow_ctrl: int, ret: float, rhol: float, mul: float, g: float) -> float:
+    """setPressGrad (auxiliaryRoutines.f90:336-393): fs from the mean density at
+    the ux faces i = 0..nx-1 (the reference's OpenMP reduction has no fixed
+    order; the restatement sums in loop order)."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    x = 0.5 * (rho.v(1, nx, 1, ny, 1, nz) + rho.v(0, nx - 1, 1, ny, 1, nz))
+    rho_av = _seq_sum(x * staggered_x_volume(mesh)[:, :, :nx]) / mesh.s_Vg
+    if flow_ctrl == 1:
+        nul = mul / rhol
+        re = 1.0 / nul
+        tauw = (ret / re) * (ret / re)
+        return tauw - rho_av * g
+    if flow_ctrl in (2, 3):
+        return -rho_av * g
+    return 0.0
+
+
+def compute_flow_rate(mesh: Mesh, ux: FField) -> float:
+    """computeFlowRate (auxiliaryRoutines.f90:517-546): sum of ux*Vsx over i = 0..nx-1."""
+    nx = mesh.nx
+    return _seq_sum(ux.v(0, nx - 1, 1, mesh.ny, 1, mesh.nz) * staggered_x_volume(mesh)[:, :, :nx])
+
+
+def set_flow_rate(mesh: Mesh, ux: FField, uy: FField, uz: FField, q0: float, flow_ctrl: int, ubot=(0.0, 0.0, 0.0),
+                  utop=(0.0, 0.0, 0.0)) -> None:
+    """setFlowRate (auxiliaryRoutines.f90:467-513): for flow_ctrl 2, ux += (Q0 - Q)/s_Vg
+    over ux(0:nx,1:ny,1:nz), then updateBoundariesV."""
+    if flow_ctrl != 2:
+        return
+    uf = (q0 - compute_flow_rate(mesh, ux)) / mesh.s_Vg
+    t = ux.v(0, mesh.nx, 1, mesh.ny, 1, mesh.nz)
+    t[...] = t + uf
+    update_boundaries_v_channel(mesh, ux, uy, uz, ubot, utop)
+
+
 # ---------------------------------------------------------------------------
 # poissonEqn.f90 (FAST_MODE): split right-hand side
 # ---------------------------------------------------------------------------

@@ -116,6 +116,12 @@ PROTOTYPES = {
     "tbfp_momentum_predictor": (C.c_int, [_H] + [C.c_void_p] * 7 + [C.c_double] * 6),
     "tbfp_momentum_predictor_dev": (C.c_int, [_H] + [C.c_void_p] * 7 + [C.c_double] * 6),
     "tbfp_update_boundaries_v": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tbfp_rho_face_sum": (C.c_int, [_H, C.c_void_p, C.POINTER(C.c_double)]),
+    "tbfp_rho_face_sum_dev": (C.c_int, [_H, C.c_void_p, C.POINTER(C.c_double)]),
+    "tbfp_flow_rate": (C.c_int, [_H, C.c_void_p, C.POINTER(C.c_double)]),
+    "tbfp_flow_rate_dev": (C.c_int, [_H, C.c_void_p, C.POINTER(C.c_double)]),
+    "tbfp_add_ux": (C.c_int, [_H, C.c_void_p, C.c_double]),
+    "tbfp_add_ux_dev": (C.c_int, [_H, C.c_void_p, C.c_double]),
     "tbfp_update_boundaries_v_dev": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tbfp_material_props": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tbfp_material_props_dev": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -79,6 +79,8 @@ struct tbfp_handle {
   size_t n_phi[3] = {0, 0, 0};
   double *h_mom[2] = {nullptr, nullptr};  // c, mu copies for tbfp_momentum_predictor
   WallTabs wt{};                           // updateBoundariesV wall spacings and values
+  // flow control: dxc(1..nx), dyf(1..ny), dzf(1..nz) on the device, ny*nz row partials + the sum
+  double *d_fdxc = nullptr, *d_fdyf = nullptr, *d_fdzf = nullptr, *d_fpart = nullptr;
   MgSolver *mg = nullptr;   // MG_MODE hierarchy (tbfp_pcg_setup)
   std::vector<double> mdxf, mdxc, mdyf, mdyc, mdzf, mdzc;  // caller's metrics, kept for tbfp_pcg_setup
   double *h_beta = nullptr, *h_q = nullptr;                // device copies for tbfp_pcg_solve
@@ -1296,6 +1298,79 @@ int tbfp_momentum_predictor(tbfp_handle *h, double *ux, double *uy, double *uz, 
     return rc;
   TBFP_CK(h, cudaStreamSynchronize(h->stream));
   return finish(h, "tbfp_momentum_predictor");
+}
+
+// ---------------------------------------------------------------------------
+// flow control (auxiliaryRoutines.f90:336-540)
+// ---------------------------------------------------------------------------
+namespace {
+int face_sum(tbfp_handle *h, int mode, const double *f, Lay L, double *out) {
+  int rc;
+  if (!h->d_fpart) {
+    const std::vector<double> dxc(h->mdxc.begin(), h->mdxc.begin() + h->nx);
+    if ((rc = upload(h, &h->d_fdxc, dxc)) || (rc = upload(h, &h->d_fdyf, h->mdyf)) ||
+        (rc = upload(h, &h->d_fdzf, h->mdzf)) || (rc = dev_alloc(h, &h->d_fpart, (size_t)h->ny * h->nz + 1)))
+      return rc;
+  }
+  double *sum = h->d_fpart + (size_t)h->ny * h->nz;
+  launch_face_sum(mode, f, L, h->d_fdxc, h->d_fdyf, h->d_fdzf, h->nx, h->ny, h->nz, h->d_fpart, sum, h->stream);
+  TBFP_CK(h, cudaMemcpyAsync(out, sum, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return TBFP_OK;
+}
+}  // namespace
+
+int tbfp_rho_face_sum_dev(tbfp_handle *h, const double *rho, double *sum) {
+  int rc = check_ptrs(h, {rho, sum});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  if ((rc = face_sum(h, 0, rho, h->Lrho, sum))) return rc;
+  return finish(h, "tbfp_rho_face_sum");
+}
+
+int tbfp_rho_face_sum(tbfp_handle *h, const double *rho, double *sum) {
+  int rc = check_ptrs(h, {rho, sum});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  if ((rc = ensure_host_bufs(h, false)) || (rc = h2d(h, h->h_rho, rho, h->n_rho))) return rc;
+  if ((rc = face_sum(h, 0, h->h_rho, h->Lrho, sum))) return rc;
+  return finish(h, "tbfp_rho_face_sum");
+}
+
+int tbfp_flow_rate_dev(tbfp_handle *h, const double *ux, double *q) {
+  int rc = check_ptrs(h, {ux, q});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  if ((rc = face_sum(h, 1, ux, h->Lux, q))) return rc;
+  return finish(h, "tbfp_flow_rate");
+}
+
+int tbfp_flow_rate(tbfp_handle *h, const double *ux, double *q) {
+  int rc = check_ptrs(h, {ux, q});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  if ((rc = ensure_host_bufs(h, false)) || (rc = h2d(h, h->h_ux, ux, h->n_ux))) return rc;
+  if ((rc = face_sum(h, 1, h->h_ux, h->Lux, q))) return rc;
+  return finish(h, "tbfp_flow_rate");
+}
+
+int tbfp_add_ux_dev(tbfp_handle *h, double *ux, double uf) {
+  int rc = check_ptrs(h, {ux});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  launch_add_ux(ux, h->Lux, h->nx, h->ny, h->nz, uf, h->stream);
+  return finish(h, "tbfp_add_ux");
+}
+
+int tbfp_add_ux(tbfp_handle *h, double *ux, double uf) {
+  int rc = check_ptrs(h, {ux});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  if ((rc = ensure_host_bufs(h, false)) || (rc = h2d(h, h->h_ux, ux, h->n_ux))) return rc;
+  launch_add_ux(h->h_ux, h->Lux, h->nx, h->ny, h->nz, uf, h->stream);
+  if ((rc = d2h(h, ux, h->h_ux, h->n_ux))) return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return finish(h, "tbfp_add_ux");
 }
 
 int tbfp_pcg_setup(tbfp_handle *h, const tbfp_mg_params *p) {

@@ -247,6 +247,13 @@ struct WallTabs {
 void launch_boundaries_v(const WallTabs &w, double *ux, double *uy, double *uz, Lay Lux, Lay Luy, Lay Luz, int nx,
                          int ny, int nz, int hd, cudaStream_t st);
 
+// Flow control: mode 0 sums 0.5*(rho(i+1)+rho(i))*Vsx, mode 1 sums ux*Vsx over
+// i = 0..nx-1, j = 1..ny, k = 1..nz into *out (device); part holds ny*nz
+// partials.  dxc, dyf, dzf: device tables of dxc(1..nx), dyf(1..ny), dzf(1..nz).
+void launch_face_sum(int mode, const double *f, Lay L, const double *dxc, const double *dyf, const double *dzf, int nx,
+                     int ny, int nz, double *part, double *out, cudaStream_t st);
+void launch_add_ux(double *ux, Lay L, int nx, int ny, int nz, double uf, cudaStream_t st);
+
 // MG_MODE source/beta (computeSource MG, computeBeta) and addPressureGrad.
 // idxc, idzc: 1/dxc(i), 1/dzc(k) for Fortran i = 1..nx+1 (0-based tables).
 void launch_mg_source_beta(const double *ux, const double *uy, const double *uz, Lay Lux, Lay Luy, Lay Luz,

@@ -284,6 +284,7 @@ class MomentumEqn:
     def __init__(self, solver: FastPoissonSolver, scheme: int = 2, gch: float = 0.0, g: float = 0.0,
                  ubot=(0.0, 0.0, 0.0), utop=(0.0, 0.0, 0.0)):
         self.solver = solver
+        self.scheme, self.gch, self.g = int(scheme), float(gch), float(g)
         g_ = solver.mesh
         self._t = {n: np.ascontiguousarray(getattr(g_, n).r(0, nn + 1))
                    for n, nn in (("dxf", g_.nx), ("dxc", g_.nx), ("dyf", g_.ny), ("dyc", g_.ny), ("dzf", g_.nz),
@@ -386,6 +387,100 @@ class MomentumEqn:
         fn = sv.lib.tbfp_momentum_predictor_dev if dev else sv.lib.tbfp_momentum_predictor
         check(fn(sv.h, u.ux.address(), u.uy.address(), u.uz.address(), c.address(), mu.address(), rho.address(),
                  s.addr, dt, alpha, gamma, xi, rho0, fs), sv.h)
+
+
+class FlowControl:
+    """The channel's flow control (momentumEqnCTOR, momentumEqn.f90:109-146, and
+    auxiliaryRoutines.f90:336-546): flow_ctrl 1 drives ux with the pressure
+    gradient of the friction Reynolds number ret, 2 holds the flow rate at q0,
+    3 only balances gravity, anything else does nothing.  The volume sums run
+    on the GPU (tbfp_rho_face_sum, tbfp_flow_rate); the scalar formulas are
+    the reference's."""
+
+    def __init__(self, solver: FastPoissonSolver, flow_ctrl: int, ret: float = 0.0, q0: float = 0.0):
+        self.solver = solver
+        self.flow_ctrl, self.ret, self.q0 = int(flow_ctrl), float(ret), float(q0)
+
+    @classmethod
+    def from_specs(cls, solver: FastPoissonSolver, specs_dir: str, u: VField | None = None) -> "FlowControl":
+        """As momentumEqnCTOR reads specs/flowControl: flowCtrl; Ret for 1; for 2
+        flow_rate (times Lx*Lz) when read_flow_rate is true, else the flow rate
+        of the initial u."""
+        from .io import ParFile  # noqa: PLC0415
+
+        pf = ParFile("flowControl", specs_dir)
+        ctrl = pf.read_int("flowCtrl")
+        fc = cls(solver, ctrl)
+        if ctrl == 1:
+            fc.ret = pf.read_real("Ret")
+        if ctrl == 2:
+            if pf.read_bool("read_flow_rate"):
+                m = solver.mesh
+                fc.q0 = pf.read_real("flow_rate") * m.Lx * m.Lz
+            else:
+                if u is None:
+                    raise TbfpError(TBFP_EINVAL, "flowCtrl 2 without read_flow_rate needs the initial velocity")
+                fc.q0 = fc.flow_rate(u)
+        return fc
+
+    def rho_face_sum(self, rho: Field) -> float:
+        sv = self.solver
+        out = C.c_double(0.0)
+        fn = sv.lib.tbfp_rho_face_sum_dev if _placement([rho]) else sv.lib.tbfp_rho_face_sum
+        check(fn(sv.h, rho.address(), C.byref(out)), sv.h)
+        return out.value
+
+    def flow_rate(self, u: VField) -> float:
+        """computeFlowRate: the sum of ux*Vsx over the faces i = 0..nx-1."""
+        sv = self.solver
+        out = C.c_double(0.0)
+        fn = sv.lib.tbfp_flow_rate_dev if _placement([u.ux]) else sv.lib.tbfp_flow_rate
+        check(fn(sv.h, u.ux.address(), C.byref(out)), sv.h)
+        return out.value
+
+    def set_press_grad(self, rho: Field, rhol: float, mul: float, g: float) -> float:
+        """setPressGrad (auxiliaryRoutines.f90:336-393): the forcing fs of the
+        momentum predictor; g is the momentum equation's gCH."""
+        rho_av = self.rho_face_sum(rho) / self.solver.mesh.s_Vg
+        if self.flow_ctrl == 1:
+            nul = mul / rhol
+            re = 1.0 / nul
+            tauw = (self.ret / re) * (self.ret / re)
+            return tauw - rho_av * g
+        if self.flow_ctrl in (2, 3):
+            return -rho_av * g
+        return 0.0
+
+    def set_flow_rate(self, mom: "MomentumEqn", u: VField) -> None:
+        """setFlowRate (auxiliaryRoutines.f90:467-513): for flowCtrl 2, ux += (Q0 - Q)/s_Vg
+        over ux(0:nx,1:ny,1:nz), then updateBoundariesV."""
+        if self.flow_ctrl != 2:
+            return
+        uf = (self.q0 - self.flow_rate(u)) / self.solver.mesh.s_Vg
+        sv = self.solver
+        fn = sv.lib.tbfp_add_ux_dev if _placement([u.ux]) else sv.lib.tbfp_add_ux
+        check(fn(sv.h, u.ux.address(), uf), sv.h)
+        mom.update_boundaries_v(u)
+
+
+def fast_substep(eqn: PoissonEqn, vof: VOF, mom: MomentumEqn, flow: FlowControl, c: Field, cs: Field, rho: Field,
+                 mu: Field, u: VField, psi: Field, psi_n: Field, psi_nm1: Field, dt: float, alpha: float,
+                 gamma: float, xi: float, st_n=None, st_nm1=None, want_stats: bool = True):
+    """One Runge-Kutta substep of tph_flow_solver (main.f90:177-209) from
+    updateMaterialProps on, all on the GPU when the fields are device fields:
+    updateMaterialProps, setPressGrad, solveMomentumEqn (predictor +
+    updateBoundariesV), solvePoissonEqn + makeVelocityDivFree (with its closing
+    updateBoundariesV) + computeContinuityError, setFlowRate.  The VOF
+    advection and the surface tension before it, and updatePressure's level
+    rotation after it (PoissonEqn.update_pressure), stay with the caller.  vof,
+    mom and flow must live on eqn's handle.  Returns the projection's stats."""
+    vof.update_material_props(c, cs, rho, mu)
+    fs = flow.set_press_grad(rho, vof.rhol, vof.mul, mom.gch)
+    mom.solve(u, c, mu, rho, dt, alpha, gamma, xi, eqn.rho0, fs=fs, st=st_n)
+    stats = eqn.projection(psi, psi_n, psi_nm1, rho, u, dt, alpha, st_n, st_nm1, want_stats=want_stats)
+    mom.update_boundaries_v(u)
+    flow.set_flow_rate(mom, u)
+    return stats
 
 
 class PCG:
