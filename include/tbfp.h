@@ -290,6 +290,15 @@ int tbfp_momentum_predictor(tbfp_handle *h, double *ux, double *uy, double *uz, 
 int tbfp_momentum_predictor_dev(tbfp_handle *h, double *ux, double *uy, double *uz, const double *c,
                                 const double *mu, const double *rho, const double *const *st, double dt,
                                 double alpha, double gamma, double xi, double rho0, double fs);
+/* The same step out of place, device pointers only: u is read, u_out (no
+   alias of u) receives the updated boxes and u's values everywhere else; the
+   update runs inside the flux kernel (no separate pass over u), which suits a
+   pipeline that keeps u and u* in two buffers (the projection's _dev form
+   reads u* and writes u). */
+int tbfp_momentum_predictor_out_dev(tbfp_handle *h, const double *ux, const double *uy, const double *uz,
+                                    double *ux_out, double *uy_out, double *uz_out, const double *c, const double *mu,
+                                    const double *rho, const double *const *st, double dt, double alpha, double gamma,
+                                    double xi, double rho0, double fs);
 /* updateBoundariesV (vfield.f90:111-189) for the channel, in place on u: the
    fixedValue walls in y (one ghost layer, boundaryField_S.f90:593-690, with
    the spacings of setMetrics :138-214), the periodic halos in x and z

@@ -1234,9 +1234,37 @@ int tbfp_momentum_predictor_dev(tbfp_handle *h, double *ux, double *uy, double *
   const double *const pp[3] = {h->d_phi[prev][0], h->d_phi[prev][1], h->d_phi[prev][2]};
   launch_momentum(h->mt, ux, uy, uz, c, mu, rho, st, h->Lux, h->Luy, h->Luz, h->Lrho, h->Lst, phi, pp, h->nx, h->ny,
                   h->nz, h->mom_scheme, dt, alpha, gamma, xi, rho0, fs, h->mom_gch, h->mom_g, h->hd_u, h->hd_rho,
-                  h->stream);
+                  nullptr, h->stream);
   h->phi_cur = cur;
   return finish(h, "tbfp_momentum_predictor");
+}
+
+int tbfp_momentum_predictor_out_dev(tbfp_handle *h, const double *ux, const double *uy, const double *uz,
+                                    double *ux_out, double *uy_out, double *uz_out, const double *c, const double *mu,
+                                    const double *rho, const double *const *st, double dt, double alpha, double gamma,
+                                    double xi, double rho0, double fs) {
+  int rc = check_ptrs(h, {ux, uy, uz, ux_out, uy_out, uz_out, c, mu, rho});
+  if (rc) return rc;
+  if (!h->mom) return set_err(h, TBFP_EINVAL, "tbfp_momentum_predictor_out: call tbfp_momentum_setup first");
+  if (st && (!st[0] || !st[1] || !st[2]))
+    return set_err(h, TBFP_ENULL, "tbfp_momentum_predictor_out: a surface-tension component pointer is NULL");
+  if (!(dt > 0.0) || !(rho0 > 0.0))
+    return set_err(h, TBFP_EINVAL, "tbfp_momentum_predictor_out: dt and rho0 must be positive");
+  const double *ins[3] = {ux, uy, uz};
+  const double *outs[3] = {ux_out, uy_out, uz_out};
+  for (const double *o : outs)
+    for (const double *i : ins)
+      if (o == i) return set_err(h, TBFP_EINVAL, "tbfp_momentum_predictor_out: u_out must not alias u");
+  cudaSetDevice(h->device);
+  const int prev = h->phi_cur, cur = 1 - h->phi_cur;
+  double *const phi[3] = {h->d_phi[cur][0], h->d_phi[cur][1], h->d_phi[cur][2]};
+  const double *const pp[3] = {h->d_phi[prev][0], h->d_phi[prev][1], h->d_phi[prev][2]};
+  double *const uo[3] = {ux_out, uy_out, uz_out};
+  launch_momentum(h->mt, const_cast<double *>(ux), const_cast<double *>(uy), const_cast<double *>(uz), c, mu, rho, st,
+                  h->Lux, h->Luy, h->Luz, h->Lrho, h->Lst, phi, pp, h->nx, h->ny, h->nz, h->mom_scheme, dt, alpha,
+                  gamma, xi, rho0, fs, h->mom_gch, h->mom_g, h->hd_u, h->hd_rho, uo, h->stream);
+  h->phi_cur = cur;
+  return finish(h, "tbfp_momentum_predictor_out");
 }
 
 int tbfp_update_boundaries_v_dev(tbfp_handle *h, double *ux, double *uy, double *uz) {

@@ -232,12 +232,14 @@ struct MomentumTabs {
   const double *dyf, *rdxf, *rdxc, *rdyf, *rdyc, *rdzf, *rdzc;
 };
 // phi: the new fluxes (written), prev: the previous call's; dense over the
-// equation boxes ux (0:nx,1:ny,1:nz), uy (1:nx,1:ny-1,1:nz), uz (1:nx,1:ny,0:nz)
+// equation boxes ux (0:nx,1:ny,1:nz), uy (1:nx,1:ny-1,1:nz), uz (1:nx,1:ny,0:nz).
+// u_out NULL: u is updated in place; else u is read only and u_out (no alias
+// of u) receives the update on the boxes and u's values elsewhere.
 void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, const double *c, const double *mu,
                      const double *rho, const double *const *st, Lay Lux, Lay Luy, Lay Luz, Lay Lc, const Lay *Lst,
                      double *const phi[3], const double *const prev[3], int nx, int ny, int nz, int scheme, double dt,
                      double alpha, double gamma, double xi, double rho0, double fs, double gch, double g, int hdu,
-                     int hdc, cudaStream_t st_);
+                     int hdc, double *const *u_out, cudaStream_t st_);
 
 // updateBoundariesV for the channel: the y-wall spacings of setMetrics (dhb,
 // dhi at the bottom and top) and the wall values, per component ux, uy, uz

@@ -134,7 +134,22 @@ struct MomArgs {
   double *phx, *phy, *phz;  // fluxes, dense over the equation boxes
   int nx, ny, nz;
   int hdu, hdc;  // halos of the velocity and cell arrays
+  // the out-of-place form's update (addConvDiff + addSource) into uxo, uyo, uzo
+  double *uxo, *uyo, *uzo;
+  const double *ppx, *ppy, *ppz, *stx, *sty, *stz;
+  Lay Lsx, Lsy, Lsz;
+  double dt, gamma, xi, r, invrho0, fs, gch, g;
 };
+
+// one component's flux into its buffer and, in the out-of-place form, its
+// addConvDiff + addSource update from the thread's own u (the expressions of
+// k_momentum_update, so both forms give the same values)
+template <bool OUT>
+__device__ __forceinline__ void emit_x(const MomArgs &a, int i, int j, int k, double phi, double uc, double invrho);
+template <bool OUT>
+__device__ __forceinline__ void emit_y(const MomArgs &a, int i, int j, int k, double phi, double uc);
+template <bool OUT>
+__device__ __forceinline__ void emit_z(const MomArgs &a, int i, int j, int k, double phi, double uc);
 
 __device__ __forceinline__ long box_x(const MomArgs &a, int i, int j, int k) {
   return ((long)(k - 1) * a.ny + (j - 1)) * (a.nx + 1) + i;
@@ -144,6 +159,37 @@ __device__ __forceinline__ long box_y(const MomArgs &a, int i, int j, int k) {
 }
 __device__ __forceinline__ long box_z(const MomArgs &a, int i, int j, int k) {
   return ((long)k * a.ny + (j - 1)) * a.nx + (i - 1);
+}
+
+template <bool OUT>
+__device__ __forceinline__ void emit_x(const MomArgs &a, int i, int j, int k, double phi, double uc, double invrho) {
+  const long q = box_x(a, i, j, k);
+  a.phx[q] = phi;
+  if constexpr (OUT) {
+    const double u = uc + a.dt * (a.gamma * phi + a.xi * __ldg(a.ppx + q));
+    const double st = a.stx ? __ldg(a.stx + at(a.Lsx, i, j, k)) : 0.0;
+    a.uxo[at(a.Lux, i, j, k)] = u + a.invrho0 * a.r * st + invrho * a.r * a.fs + a.r * a.gch;
+  }
+}
+template <bool OUT>
+__device__ __forceinline__ void emit_y(const MomArgs &a, int i, int j, int k, double phi, double uc) {
+  const long q = box_y(a, i, j, k);
+  a.phy[q] = phi;
+  if constexpr (OUT) {
+    const double u = uc + a.dt * (a.gamma * phi + a.xi * __ldg(a.ppy + q));
+    const double st = a.sty ? __ldg(a.sty + at(a.Lsy, i, j, k)) : 0.0;
+    a.uyo[at(a.Luy, i, j, k)] = u + a.invrho0 * a.r * st + a.r * a.g;
+  }
+}
+template <bool OUT>
+__device__ __forceinline__ void emit_z(const MomArgs &a, int i, int j, int k, double phi, double uc) {
+  const long q = box_z(a, i, j, k);
+  a.phz[q] = phi;
+  if constexpr (OUT) {
+    const double u = uc + a.dt * (a.gamma * phi + a.xi * __ldg(a.ppz + q));
+    const double st = a.stz ? __ldg(a.stz + at(a.Lsz, i, j, k)) : 0.0;
+    a.uzo[at(a.Luz, i, j, k)] = u + a.invrho0 * a.r * st;
+  }
 }
 
 // Two ways to reach a field's neighbours.  GAcc reads global memory through
@@ -289,7 +335,7 @@ __device__ __forceinline__ double F_zz(const Acc &A) {
 // flux differences (upper minus lower face) of its three directions, plus the
 // diffusion with its transposed terms
 template <class Acc>
-__device__ __forceinline__ double tail_x(const Acc &A, const Met &g, double irc, double cx, double cy, double cz) {
+__device__ __forceinline__ double tail_x(const Acc &A, const Met &g, double invrho, double cx, double cy, double cz) {
   TBFP_MOM_ACCESSORS;
   const double uc = u(0, 0, 0);
   const double rxc = g.rxc1, ryf = g.ryf0, rzf = g.rzf0;
@@ -308,13 +354,12 @@ __device__ __forceinline__ double tail_x(const Acc &A, const Met &g, double irc,
   mul = 0.25 * (m(1, 0, 0) + m(0, 0, 0) + m(1, 0, -1) + m(0, 0, -1));
   const double dzz = (mur * (u(0, 0, 1) - uc) * g.rzc1 - mul * (uc - u(0, 0, -1)) * g.rzc0) * rzf;
   const double dzzt = (mur * (w(1, 0, 0) - w(0, 0, 0)) * rxc - mul * (w(1, 0, -1) - w(0, 0, -1)) * rxc) * rzf;
-  const double invrho = 0.5 * (1.0 / rho(1, 0, 0) + irc);
   return phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho;
 }
 
 // y component at face (i, j, k) (momentumEqn.f90:344-467)
 template <class Acc>
-__device__ __forceinline__ double tail_y(const Acc &A, const Met &g, double irc, double cx, double cy, double cz) {
+__device__ __forceinline__ double tail_y(const Acc &A, const Met &g, double invrho, double cx, double cy, double cz) {
   TBFP_MOM_ACCESSORS;
   const double vc = v(0, 0, 0);
   const double rycp = g.ryc1, rxf = g.rxf0, rzf = g.rzf0;
@@ -334,13 +379,12 @@ __device__ __forceinline__ double tail_y(const Acc &A, const Met &g, double irc,
   mul = 0.25 * (m(0, 0, 0) + m(0, 0, -1) + m(0, 1, 0) + m(0, 1, -1));
   const double dzz = (mur * (v(0, 0, 1) - vc) * g.rzc1 - mul * (vc - v(0, 0, -1)) * g.rzc0) * rzf;
   const double dzzt = (mur * (w(0, 1, 0) - w(0, 0, 0)) * rycp - mul * (w(0, 1, -1) - w(0, 0, -1)) * rycp) * rzf;
-  const double invrho = 0.5 * (1.0 / rho(0, 1, 0) + irc);
   return phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho;
 }
 
 // z component at face (i, j, k) (momentumEqn.f90:470-603)
 template <class Acc>
-__device__ __forceinline__ double tail_z(const Acc &A, const Met &g, double irc, double cx, double cy, double cz) {
+__device__ __forceinline__ double tail_z(const Acc &A, const Met &g, double invrho, double cx, double cy, double cz) {
   TBFP_MOM_ACCESSORS;
   const double wc = w(0, 0, 0);
   const double rxf = g.rxf0, ryf = g.ryf0, rzcp = g.rzc1;
@@ -360,14 +404,13 @@ __device__ __forceinline__ double tail_z(const Acc &A, const Met &g, double irc,
   mul = m(0, 0, 0);
   const double dzz = (mur * (w(0, 0, 1) - wc) * g.rzf1 - mul * (wc - w(0, 0, -1)) * g.rzf0) * rzcp;
   const double dzzt = dzz;
-  const double invrho = 0.5 * (1.0 / rho(0, 0, 1) + irc);
   return phi + (dxx + dyy + dzz + dxxt + dyyt + dzzt) * invrho;
 }
 
 // The per-cell forms (every scheme; scheme 5's limiters depend on the cell):
 // both faces of each direction at the cell itself
 template <int S, class Acc>
-__device__ __forceinline__ double phi_x(const Acc &A, const Met &g, double irc) {
+__device__ __forceinline__ double phi_x(const Acc &A, const Met &g, double invrho) {
   TBFP_MOM_ACCESSORS;
   const bool sh = sharp_cell<S>(c(1, 0, 0), c(0, 0, 0), c(0, 1, 0), c(0, -1, 0), c(0, 0, 1), c(0, 0, -1));
   const double uc = u(0, 0, 0);
@@ -377,11 +420,11 @@ __device__ __forceinline__ double phi_x(const Acc &A, const Met &g, double irc) 
                                  u(0, -1, 0), uc, u(0, 1, 0), u(0, 2, 0), sh);
   const double cz = conv_diff<S>(0.5 * (w(0, 0, 0) + w(1, 0, 0)), 0.5 * (w(0, 0, -1) + w(1, 0, -1)), u(0, 0, -2),
                                  u(0, 0, -1), uc, u(0, 0, 1), u(0, 0, 2), sh);
-  return tail_x(A, g, irc, cx, cy, cz);
+  return tail_x(A, g, invrho, cx, cy, cz);
 }
 
 template <int S, class Acc>
-__device__ __forceinline__ double phi_y(const Acc &A, const Met &g, double irc) {
+__device__ __forceinline__ double phi_y(const Acc &A, const Met &g, double invrho) {
   TBFP_MOM_ACCESSORS;
   const bool sh = sharp_cell<S>(c(1, 0, 0), c(-1, 0, 0), c(0, 1, 0), c(0, 0, 0), c(0, 0, 1), c(0, 0, -1));
   const double vc = v(0, 0, 0);
@@ -394,11 +437,11 @@ __device__ __forceinline__ double phi_y(const Acc &A, const Met &g, double irc) 
   const double cz = conv_diff<S>(0.5 * (w(0, 1, 0) * dyfp + w(0, 0, 0) * dyfj) * rycp,
                                  0.5 * (w(0, 1, -1) * dyfp + w(0, 0, -1) * dyfj) * rycp, v(0, 0, -2), v(0, 0, -1), vc,
                                  v(0, 0, 1), v(0, 0, 2), sh);
-  return tail_y(A, g, irc, cx, cy, cz);
+  return tail_y(A, g, invrho, cx, cy, cz);
 }
 
 template <int S, class Acc>
-__device__ __forceinline__ double phi_z(const Acc &A, const Met &g, double irc) {
+__device__ __forceinline__ double phi_z(const Acc &A, const Met &g, double invrho) {
   TBFP_MOM_ACCESSORS;
   const bool sh = sharp_cell<S>(c(1, 0, 0), c(-1, 0, 0), c(0, 1, 0), c(0, -1, 0), c(0, 0, 1), c(0, 0, 0));
   const double wc = w(0, 0, 0);
@@ -408,7 +451,7 @@ __device__ __forceinline__ double phi_z(const Acc &A, const Met &g, double irc) 
                                  w(0, -1, 0), wc, w(0, 1, 0), w(0, 2, 0), sh);
   const double cz = conv_diff<S>(0.5 * (wc + w(0, 0, 1)), 0.5 * (wc + w(0, 0, -1)), w(0, 0, -2), w(0, 0, -1), wc,
                                  w(0, 0, 1), w(0, 0, 2), sh);
-  return tail_z(A, g, irc, cx, cy, cz);
+  return tail_z(A, g, invrho, cx, cy, cz);
 }
 #undef TBFP_MOM_ACCESSORS
 
@@ -423,7 +466,7 @@ __host__ __device__ constexpr bool share_faces(int S) { return S == 3 || S == 4;
 // j = 1..ny, marching k over a chunk of kKC planes of 0..nz; each thread the
 // components whose box holds its (i, j, k).  A plane outside a field's array
 // is not loaded: no stencil of a computed component reaches it.
-template <int S>
+template <int S, bool OUT>
 __global__ void __launch_bounds__(kTX * kTY, 2) k_momentum_fluxes(MomArgs a) {
   extern __shared__ double sm[];
   double *rU = sm, *rV = rU + kRV * kNV, *rW = rV + kRV * kNV;
@@ -496,10 +539,11 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_momentum_fluxes(MomArgs a) {
         const double irc = 1.0 / A.r(0, 0, 0);  // 1/rho of the own cell, shared by the three components
         const Met g(a, i, j, k);
         if (k >= 1) {
-          a.phx[box_x(a, i, j, k)] = phi_x<S>(A, g, irc);
-          if (j <= a.ny - 1) a.phy[box_y(a, i, j, k)] = phi_y<S>(A, g, irc);
+          const double ivx = 0.5 * (1.0 / A.r(1, 0, 0) + irc);
+          emit_x<OUT>(a, i, j, k, phi_x<S>(A, g, ivx), A.u(0, 0, 0), ivx);
+          if (j <= a.ny - 1) emit_y<OUT>(a, i, j, k, phi_y<S>(A, g, 0.5 * (1.0 / A.r(0, 1, 0) + irc)), A.v(0, 0, 0));
         }
-        a.phz[box_z(a, i, j, k)] = phi_z<S>(A, g, irc);
+        emit_z<OUT>(a, i, j, k, phi_z<S>(A, g, 0.5 * (1.0 / A.r(0, 0, 1) + irc)), A.w(0, 0, 0));
       }
     } else {
       // each face once: the cell's upper x, y faces into shared memory, its
@@ -545,10 +589,14 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_momentum_fluxes(MomArgs a) {
         auto cxd = [&](int c) { return fx[(c * kTY + ty) * (kTX + 1) + tx + 1] - fx[(c * kTY + ty) * (kTX + 1) + tx]; };
         auto cyd = [&](int c) { return fy[(c * (kTY + 1) + ty + 1) * kTX + tx] - fy[(c * (kTY + 1) + ty) * kTX + tx]; };
         if (k >= 1) {
-          a.phx[box_x(a, i, j, k)] = tail_x(A, g, irc, cxd(0), cyd(0), fzn0 - fzl0);
-          if (j <= a.ny - 1) a.phy[box_y(a, i, j, k)] = tail_y(A, g, irc, cxd(1), cyd(1), fzn1 - fzl1);
+          const double ivx = 0.5 * (1.0 / A.r(1, 0, 0) + irc);
+          emit_x<OUT>(a, i, j, k, tail_x(A, g, ivx, cxd(0), cyd(0), fzn0 - fzl0), A.u(0, 0, 0), ivx);
+          if (j <= a.ny - 1)
+            emit_y<OUT>(a, i, j, k, tail_y(A, g, 0.5 * (1.0 / A.r(0, 1, 0) + irc), cxd(1), cyd(1), fzn1 - fzl1),
+                        A.v(0, 0, 0));
         }
-        a.phz[box_z(a, i, j, k)] = tail_z(A, g, irc, cxd(2), cyd(2), fzn2 - fzl2);
+        emit_z<OUT>(a, i, j, k, tail_z(A, g, 0.5 * (1.0 / A.r(0, 0, 1) + irc), cxd(2), cyd(2), fzn2 - fzl2),
+                    A.w(0, 0, 0));
       }
       fzl0 = fzn0;
       fzl1 = fzn1;
@@ -566,26 +614,89 @@ __host__ __device__ constexpr size_t tiled_smem_bytes(int S) {
 
 // the x component's face i = 0 (the periodic duplicate of i = nx, computed
 // from its own stencil), one thread per (j, k)
-template <int S>
+template <int S, bool OUT>
 __global__ void __launch_bounds__(kMT) k_momentum_fluxes_i0(MomArgs a) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y + 1;
   if (j > a.ny) return;
   const GAcc A(a, 0, j, k);
-  a.phx[box_x(a, 0, j, k)] = phi_x<S>(A, Met(a, 0, j, k), 1.0 / A.r(0, 0, 0));
+  const double ivx = 0.5 * (1.0 / A.r(1, 0, 0) + 1.0 / A.r(0, 0, 0));
+  emit_x<OUT>(a, 0, j, k, phi_x<S>(A, Met(a, 0, j, k), ivx), A.u(0, 0, 0), ivx);
 }
 
-template <int S>
+// The out-of-place form leaves the elements outside the equation boxes to
+// this copy from u_in: uy's wall faces, every ghost and halo layer (the
+// boundary update that follows rewrites the ones the reference rewrites).
+// It visits, per component, the planes outside the box's k range, the rows
+// outside its j range and the columns outside its i range.
+struct Cmp {
+  const double *in;
+  double *out;
+  Lay L;
+  int ilo, ihi, jlo, jhi, klo, khi;  // array
+  int bi0, bi1, bj0, bj1, bk0, bk1;  // equation box
+  long n_planes, n_total;
+};
+struct CmpArgs {
+  Cmp c[3];
+};
+
+__global__ void __launch_bounds__(256) k_copy_outside_box(CmpArgs a) {
+  const Cmp &c = a.c[blockIdx.y];
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= c.n_total) return;
+  const int NI = c.ihi - c.ilo + 1, NJ = c.jhi - c.jlo + 1;
+  const int nkl = c.bk0 - c.klo, njl = c.bj0 - c.jlo, njh = c.jhi - c.bj1, nil = c.bi0 - c.ilo, nih = c.ihi - c.bi1;
+  int i, j, k;
+  if (t < c.n_planes) {
+    const long pl = (long)NI * NJ;
+    const int p = (int)(t / pl), r = (int)(t - p * pl);
+    k = p < nkl ? c.klo + p : c.bk1 + 1 + (p - nkl);
+    j = c.jlo + r / NI;
+    i = c.ilo + r % NI;
+  } else {
+    const long u = t - c.n_planes;
+    const long per_k = (long)(njl + njh) * NI + (long)(c.bj1 - c.bj0 + 1) * (nil + nih);
+    k = c.bk0 + (int)(u / per_k);
+    const int r = (int)(u - (k - c.bk0) * per_k);
+    if (r < (njl + njh) * NI) {
+      const int rr = r / NI;
+      j = rr < njl ? c.jlo + rr : c.bj1 + 1 + (rr - njl);
+      i = c.ilo + r % NI;
+    } else {
+      const int q = r - (njl + njh) * NI, jj = q / (nil + nih), ii = q - jj * (nil + nih);
+      j = c.bj0 + jj;
+      i = ii < nil ? c.ilo + ii : c.bi1 + 1 + (ii - nil);
+    }
+  }
+  const long o = at(c.L, i, j, k);
+  c.out[o] = c.in[o];
+}
+
+template <int S, bool OUT>
 void launch_fluxes(const MomArgs &a, cudaStream_t st) {
   static bool attr[64] = {};  // per device: the attribute belongs to the device's context
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !attr[dev]) {
-    cudaFuncSetAttribute(k_momentum_fluxes<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tiled_smem_bytes(S));
+    cudaFuncSetAttribute(k_momentum_fluxes<S, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)tiled_smem_bytes(S));
     if (dev < 64) attr[dev] = true;
   }
   const dim3 blk(kTX, kTY), grid((a.nx + kTX - 1) / kTX, (a.ny + kTY - 1) / kTY, (a.nz + 1 + kKC - 1) / kKC);
-  k_momentum_fluxes<S><<<grid, blk, tiled_smem_bytes(S), st>>>(a);
-  k_momentum_fluxes_i0<S><<<dim3((a.ny + kMT - 1) / kMT, a.nz), kMT, 0, st>>>(a);
+  k_momentum_fluxes<S, OUT><<<grid, blk, tiled_smem_bytes(S), st>>>(a);
+  k_momentum_fluxes_i0<S, OUT><<<dim3((a.ny + kMT - 1) / kMT, a.nz), kMT, 0, st>>>(a);
+}
+
+template <bool OUT>
+void launch_fluxes_scheme(int scheme, const MomArgs &a, cudaStream_t st) {
+  switch (scheme) {
+    case 0: launch_fluxes<0, OUT>(a, st); break;
+    case 1: launch_fluxes<1, OUT>(a, st); break;
+    case 2: launch_fluxes<2, OUT>(a, st); break;
+    case 3: launch_fluxes<3, OUT>(a, st); break;
+    case 4: launch_fluxes<4, OUT>(a, st); break;
+    default: launch_fluxes<5, OUT>(a, st); break;
+  }
 }
 
 struct MomUpd {
@@ -704,7 +815,7 @@ void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, 
                      const double *rho, const double *const *st, Lay Lux, Lay Luy, Lay Luz, Lay Lc, const Lay *Lst,
                      double *const phi[3], const double *const prev[3], int nx, int ny, int nz, int scheme, double dt,
                      double alpha, double gamma, double xi, double rho0, double fs, double gch, double g, int hdu,
-                     int hdc, cudaStream_t st_) {
+                     int hdc, double *const *u_out, cudaStream_t st_) {
   MomArgs a{};
   a.ux = ux;
   a.uy = uy;
@@ -731,14 +842,65 @@ void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, 
   a.nz = nz;
   a.hdu = hdu;
   a.hdc = hdc;
-  switch (scheme) {
-    case 0: launch_fluxes<0>(a, st_); break;
-    case 1: launch_fluxes<1>(a, st_); break;
-    case 2: launch_fluxes<2>(a, st_); break;
-    case 3: launch_fluxes<3>(a, st_); break;
-    case 4: launch_fluxes<4>(a, st_); break;
-    default: launch_fluxes<5>(a, st_); break;
+  if (u_out) {
+    // fused: the flux kernel also writes u_out on the boxes; the rest of u_out is copied from u
+    a.uxo = u_out[0];
+    a.uyo = u_out[1];
+    a.uzo = u_out[2];
+    a.ppx = prev[0];
+    a.ppy = prev[1];
+    a.ppz = prev[2];
+    a.stx = st ? st[0] : nullptr;
+    a.sty = st ? st[1] : nullptr;
+    a.stz = st ? st[2] : nullptr;
+    if (st) {
+      a.Lsx = Lst[0];
+      a.Lsy = Lst[1];
+      a.Lsz = Lst[2];
+    }
+    a.dt = dt;
+    a.gamma = gamma;
+    a.xi = xi;
+    a.r = dt * alpha;
+    a.invrho0 = 1.0 / rho0;
+    a.fs = fs;
+    a.gch = gch;
+    a.g = g;
+    launch_fluxes_scheme<true>(scheme, a, st_);
+    CmpArgs ca{};
+    const double *in[3] = {ux, uy, uz};
+    const Lay L[3] = {Lux, Luy, Luz};
+    long most = 0;
+    for (int e = 0; e < 3; ++e) {
+      Cmp &c = ca.c[e];
+      const int is = e == 0 ? 0 : 1, js = e == 1 ? 0 : 1, ks = e == 2 ? 0 : 1;
+      c.in = in[e];
+      c.out = u_out[e];
+      c.L = L[e];
+      c.ilo = is - hdu;
+      c.ihi = nx + hdu;
+      c.jlo = js - hdu;
+      c.jhi = ny + hdu;
+      c.klo = ks - hdu;
+      c.khi = nz + hdu;
+      // equation boxes: ux (0:nx,1:ny,1:nz), uy (1:nx,1:ny-1,1:nz), uz (1:nx,1:ny,0:nz)
+      c.bi0 = e == 0 ? 0 : 1;
+      c.bi1 = nx;
+      c.bj0 = 1;
+      c.bj1 = e == 1 ? ny - 1 : ny;
+      c.bk0 = e == 2 ? 0 : 1;
+      c.bk1 = nz;
+      const long NI = c.ihi - c.ilo + 1, NJ = c.jhi - c.jlo + 1;
+      const long nk_out = (c.bk0 - c.klo) + (c.khi - c.bk1), nj_out = (c.bj0 - c.jlo) + (c.jhi - c.bj1);
+      const long ni_out = (c.bi0 - c.ilo) + (c.ihi - c.bi1);
+      c.n_planes = nk_out * NI * NJ;
+      c.n_total = c.n_planes + (long)(c.bk1 - c.bk0 + 1) * (nj_out * NI + (long)(c.bj1 - c.bj0 + 1) * ni_out);
+      most = c.n_total > most ? c.n_total : most;
+    }
+    k_copy_outside_box<<<dim3((unsigned)((most + 255) / 256), 3), 256, 0, st_>>>(ca);
+    return;
   }
+  launch_fluxes_scheme<false>(scheme, a, st_);
   const dim3 grid((nx + kMT - 1) / kMT, ny, nz + 1);
   MomUpd b{};
   b.ux = ux;

@@ -14,6 +14,15 @@ Names and argument meaning follow the Fortran modules they replace:
 * ``PCG``                -- pcgMod (src/pcg/pcg.f90) with its multigrid preconditioner
   (multiGridMod, rbgsMod, poissMatMod): ``PCG(mesh, ...)`` is pcgCTOR (:62),
   ``solve_pcg(psi, beta, q)`` is solvePCG (:103).
+* ``VOF``                -- the VOF type's material properties (src/VOF/VOF.f90:197-262).
+* ``MomentumEqn``        -- momentumEqnMod in FAST_MODE (src/momentumEqn/momentumEqn.f90):
+  ``solve`` is solveMomentumEqn (:161) with updateBoundariesV (vfield.f90:111),
+  ``write_old_time_flux`` / ``read_old_time_flux`` are printOldTimeFlux /
+  initOldTimeFlux (:1254-1290).
+* ``FlowControl``        -- setPressGrad, computeFlowRate, setFlowRate
+  (src/auxiliaryRoutines/auxiliaryRoutines.f90:336-546).
+* ``fast_substep``       -- one Runge-Kutta substep of tph_flow_solver (src/main.f90:177-209)
+  after the VOF advection.
 
 The reference's old time levels ``psi%ptrf_`` and ``psi%ptrf_%ptrf_`` are
 passed explicitly as ``psi_n`` and ``psi_nm1``; the surface-tension old levels
@@ -371,19 +380,30 @@ class MomentumEqn:
         check(fn(sv.h, u.ux.address(), u.uy.address(), u.uz.address()), sv.h)
 
     def solve(self, u: VField, c: Field, mu: Field, rho: Field, dt: float, alpha: float, gamma: float, xi: float,
-              rho0: float, fs: float = 0.0, st=None) -> None:
+              rho0: float, fs: float = 0.0, st=None, u_out: VField | None = None) -> None:
         """solveMomentumEqn (momentumEqn.f90:161-194): the predictor, then
-        updateBoundariesV, so u comes out ready for the next step's stencils."""
-        self.predictor(u, c, mu, rho, dt, alpha, gamma, xi, rho0, fs, st)
-        self.update_boundaries_v(u)
+        updateBoundariesV, so the result comes out ready for the next stencils;
+        in u, or in u_out (device fields) with u left as it was."""
+        self.predictor(u, c, mu, rho, dt, alpha, gamma, xi, rho0, fs, st, u_out=u_out)
+        self.update_boundaries_v(u_out if u_out is not None else u)
 
     def predictor(self, u: VField, c: Field, mu: Field, rho: Field, dt: float, alpha: float, gamma: float,
-                  xi: float, rho0: float, fs: float = 0.0, st=None) -> None:
-        """solveMomentumEqn FAST: u (in place) <- u + dt*(gamma*phi + xi*phi_prev) + sources."""
+                  xi: float, rho0: float, fs: float = 0.0, st=None, u_out: VField | None = None) -> None:
+        """solveMomentumEqn FAST without its boundary update: u <- u + dt*(gamma*phi +
+        xi*phi_prev) + sources, in place, or into u_out (device fields; the update
+        then runs inside the flux kernel and u is only read)."""
         sv = self.solver
         fields = [*u.components(), c, mu, rho] + list(st or [])
-        dev = _placement(fields)
+        dev = _placement(fields + (list(u_out.components()) if u_out is not None else []))
         s = _PtrTriple(st)
+        if u_out is not None:
+            if not dev:
+                raise TbfpError(TBFP_EINVAL, "u_out is only supported for device fields")
+            check(sv.lib.tbfp_momentum_predictor_out_dev(
+                sv.h, u.ux.address(), u.uy.address(), u.uz.address(), u_out.ux.address(), u_out.uy.address(),
+                u_out.uz.address(), c.address(), mu.address(), rho.address(), s.addr, dt, alpha, gamma, xi, rho0,
+                fs), sv.h)
+            return
         fn = sv.lib.tbfp_momentum_predictor_dev if dev else sv.lib.tbfp_momentum_predictor
         check(fn(sv.h, u.ux.address(), u.uy.address(), u.uz.address(), c.address(), mu.address(), rho.address(),
                  s.addr, dt, alpha, gamma, xi, rho0, fs), sv.h)
@@ -465,7 +485,8 @@ class FlowControl:
 
 def fast_substep(eqn: PoissonEqn, vof: VOF, mom: MomentumEqn, flow: FlowControl, c: Field, cs: Field, rho: Field,
                  mu: Field, u: VField, psi: Field, psi_n: Field, psi_nm1: Field, dt: float, alpha: float,
-                 gamma: float, xi: float, st_n=None, st_nm1=None, want_stats: bool = True):
+                 gamma: float, xi: float, st_n=None, st_nm1=None, want_stats: bool = True,
+                 u_star: VField | None = None):
     """One Runge-Kutta substep of tph_flow_solver (main.f90:177-209) from
     updateMaterialProps on, all on the GPU when the fields are device fields:
     updateMaterialProps, setPressGrad, solveMomentumEqn (predictor +
@@ -473,11 +494,19 @@ def fast_substep(eqn: PoissonEqn, vof: VOF, mom: MomentumEqn, flow: FlowControl,
     updateBoundariesV) + computeContinuityError, setFlowRate.  The VOF
     advection and the surface tension before it, and updatePressure's level
     rotation after it (PoissonEqn.update_pressure), stay with the caller.  vof,
-    mom and flow must live on eqn's handle.  Returns the projection's stats."""
+    mom and flow must live on eqn's handle.  With a scratch u_star (device
+    fields) the predictor writes u* there and the projection writes the result
+    back into u, so the predictor's update needs no pass of its own.  Returns
+    the projection's stats."""
     vof.update_material_props(c, cs, rho, mu)
     fs = flow.set_press_grad(rho, vof.rhol, vof.mul, mom.gch)
-    mom.solve(u, c, mu, rho, dt, alpha, gamma, xi, eqn.rho0, fs=fs, st=st_n)
-    stats = eqn.projection(psi, psi_n, psi_nm1, rho, u, dt, alpha, st_n, st_nm1, want_stats=want_stats)
+    if u_star is not None:
+        mom.solve(u, c, mu, rho, dt, alpha, gamma, xi, eqn.rho0, fs=fs, st=st_n, u_out=u_star)
+        stats = eqn.projection(psi, psi_n, psi_nm1, rho, u_star, dt, alpha, st_n, st_nm1, u_out=u,
+                               want_stats=want_stats)
+    else:
+        mom.solve(u, c, mu, rho, dt, alpha, gamma, xi, eqn.rho0, fs=fs, st=st_n)
+        stats = eqn.projection(psi, psi_n, psi_nm1, rho, u, dt, alpha, st_n, st_nm1, want_stats=want_stats)
     mom.update_boundaries_v(u)
     flow.set_flow_rate(mom, u)
     return stats

@@ -137,3 +137,42 @@ def test_two_fast_substeps_on_the_gpu_match_the_oracle_chain():
         assert rel_linf(dpn.a.cpu().numpy()[1:-1, 1:-1, 1:-1], pn.a[1:-1, 1:-1, 1:-1]) < 1e-10
     finally:
         eqn.close()
+
+
+@pytest.mark.gpu
+def test_double_buffered_substep_matches_the_in_place_one():
+    """fast_substep with a u_star scratch (out-of-place predictor, projection
+    from u_star back into u) gives the in-place chain's velocity and pressure."""
+    from tbfsolver_b200.solver import VOF, PoissonEqn, fast_substep
+
+    nx, ny, nz = 32, 24, 16
+    g = _grid(nx, ny, nz, True)
+    m = mesh_of(g)
+    props = dict(rhol=1.0, rhog=0.1, mul=3.3e-4, mug=3.3e-4)
+    spec = synth.small_spec(nx, ny, nz, stretched=True, nbubbles=3, radius=0.35)
+    c0 = synth.vof_field(spec, synth.bubble_centres(spec, 8), hd=1).numpy().copy()
+    u0 = _velocity(g, 9)
+    O.update_boundaries_v_channel(m, *u0)
+    dev = lambda a, kind="cl", hd=1: Field(kind, hd, nx, ny, nz, torch.from_numpy(a.copy()).cuda())  # noqa: E731
+    out = []
+    for star in (False, True):
+        eqn = PoissonEqn(g, props["rhol"], props["rhog"])
+        try:
+            vof = VOF(eqn.solver, **props)
+            mom = MomentumEqn(eqn.solver, scheme=2, gch=0.1)
+            flow = FlowControl(eqn.solver, 1, ret=127.3)
+            du = VField(*[dev(f.a, f.kind, f.hd) for f in u0])
+            us = VField(*[dev(np.zeros_like(f.a), f.kind, f.hd) for f in u0]) if star else None
+            z = np.zeros(field_shape("cl", 1, nx, ny, nz))
+            dc, dcs, drho, dmu, dpsi, dpn, dpm = (dev(a) for a in (c0, z, z, z, z, z, z))
+            for gamma, xi in ((1.0, 0.0), (1.5, -0.5)):
+                fast_substep(eqn, vof, mom, flow, dc, dcs, drho, dmu, du, dpsi, dpn, dpm, 2e-3, 1.0, gamma, xi,
+                             u_star=us)
+                dpn, dpm, dpsi = PoissonEqn.update_pressure(dpsi, dpn, dpm)
+            out.append(([f.a.cpu().numpy() for f in du.components()], dpn.a.cpu().numpy()))
+        finally:
+            eqn.close()
+    (ua, pa), (ub, pb) = out
+    for a, b in zip(ua, ub):
+        assert rel_linf(b, a) < 1e-13
+    assert rel_linf(pb, pa) < 1e-12
