@@ -111,75 +111,140 @@ void bc_cell(double *f, Lay L, int nx, int ny, int nz, int hd, cudaStream_t st) 
 // (w = X*Y*Z / (hx*hy*hz)), so a pass is, per direction, the 3-point stencil
 //   out(i) = m(i) in(i-1) + z(i) in(i) + p(i) in(i+1)
 // with m, z, p from the distance tables (VofSep, built on the host), applied
-// in z, then y, then x through a shared-memory tile: 9 FMAs per cell instead
-// of the 16 products and 2 divisions per vertex and cell of the direct form
-// (same operator; rounding differs in the last bits).  A CTA owns cells
-// [i0, i0+kSX) x [j0, j0+kSY) x [k0, k0+kSZ) (1-based) and stages their input
-// ring.  The boundary update that follows a pass in the reference (y walls,
-// then x, then z halos over the extended ranges) leaves each ghost cell equal
-// to the interior cell reached by mapping every coordinate independently (x:
-// 0 -> nx, nx+1 -> 1; y: 0 -> 1, ny+1 -> ny; z: 0 -> nz, nz+1 -> 1), so each
-// cell also writes the ghost cells that copy it.  PROPS: the final pass, which
-// also writes rho and mu (VOF.f90:220-221) at the cell and its ghost images.
-constexpr int kSX = 32, kSY = 8, kSZ = 4, kST = 256;
+// in z, then y, then x: 9 FMAs per cell instead of the 16 products and 2
+// divisions per vertex and cell of the direct form (same operator; rounding
+// differs in the last bits).  A CTA owns a kMX x kMY tile of (i, j) columns
+// and marches up a chunk of kMKC planes: the input planes k-1, k, k+1 (with
+// their in-plane halo) sit in a ring of eight shared-memory slots, planes
+// k+2..k+4 in flight by cp.async (one commit group per plane, three planes
+// of prefetch cover the DRAM latency of the short per-plane steps) while plane
+// k is combined in z, then y, then x.  Each input plane is read once per chunk
+// (the halo rows and columns add a third).
+// The boundary update that follows a pass in the reference (y walls, then x,
+// then z halos over the extended ranges) leaves each ghost cell equal to the
+// interior cell reached by mapping every coordinate independently (x: 0 -> nx,
+// nx+1 -> 1; y: 0 -> 1, ny+1 -> ny; z: 0 -> nz, nz+1 -> 1), so each cell also
+// writes the ghost cells that copy it.  PROPS: the final pass, which also
+// writes rho and mu (VOF.f90:220-221) at the cell and its ghost images.
+constexpr int kMX = 32, kMY = 8, kMKC = 32, kMT2 = kMX * kMY;
 
 template <bool PROPS>
-__global__ void __launch_bounds__(kST) k_smooth_pass(VofSep w, const double *__restrict__ in, double *__restrict__ out,
-                                                     double *__restrict__ rho, double *__restrict__ mu, Lay L,
-                                                     int nx, int ny, int nz, double rhol, double rhog, double mul,
-                                                     double mug) {
-  constexpr int CX = kSX + 2, CY = kSY + 2, CZ = kSZ + 2;
-  __shared__ double buf0[CZ * CY * CX];  // input ring, then the tile after y
-  __shared__ double c1[kSZ][CY][CX];     // after z
-  auto c0 = reinterpret_cast<double(*)[CY][CX]>(buf0);
-  auto c2 = reinterpret_cast<double(*)[kSY][CX]>(buf0);
-  const int i0 = blockIdx.x * kSX + 1, j0 = blockIdx.y * kSY + 1, k0 = blockIdx.z * kSZ + 1;
-  const int tid = threadIdx.x;
-  for (int e = tid; e < CX * CY * CZ; e += kST) {
-    const int cx = e % CX, cy = (e / CX) % CY, cz = e / (CX * CY);
-    const int gi = i0 - 1 + cx, gj = j0 - 1 + cy, gk = k0 - 1 + cz;
-    double v = 0.0;
-    if (gi <= nx + 1 && gj <= ny + 1 && gk <= nz + 1) v = in[at(L, gi, gj, gk)];
-    c0[cz][cy][cx] = v;
-  }
-  __syncthreads();
-  for (int e = tid; e < CX * CY * kSZ; e += kST) {
-    const int cx = e % CX, cy = (e / CX) % CY, oz = e / (CX * CY);
-    const int k = min(k0 + oz, nz) - 1;
-    c1[oz][cy][cx] = w.zm[k] * c0[oz][cy][cx] + w.z0[k] * c0[oz + 1][cy][cx] + w.zp[k] * c0[oz + 2][cy][cx];
-  }
-  __syncthreads();
-  for (int e = tid; e < CX * kSY * kSZ; e += kST) {
-    const int cx = e % CX, oy = (e / CX) % kSY, oz = e / (CX * kSY);
-    const int j = min(j0 + oy, ny) - 1;
-    c2[oz][oy][cx] = w.ym[j] * c1[oz][oy][cx] + w.y0[j] * c1[oz][oy + 1][cx] + w.yp[j] * c1[oz][oy + 2][cx];
-  }
-  __syncthreads();
-  for (int e = tid; e < kSX * kSY * kSZ; e += kST) {
-    const int ox = e % kSX, oy = (e / kSX) % kSY, oz = e / (kSX * kSY);
-    const int i = i0 + ox, j = j0 + oy, k = k0 + oz;
-    if (i > nx || j > ny || k > nz) continue;
-    const double c = w.xm[i - 1] * c2[oz][oy][ox] + w.x0[i - 1] * c2[oz][oy][ox + 1] + w.xp[i - 1] * c2[oz][oy][ox + 2];
-    const double m = mug * c + (1.0 - c) * mul, r = rhog * c + (1.0 - c) * rhol;
-    // the cell and the ghost cells equal to it
-    const int xs[2] = {i, i == nx ? 0 : (i == 1 ? nx + 1 : -1)};
-    const int ys[2] = {j, j == 1 ? 0 : (j == ny ? ny + 1 : -1)};
-    const int zs[2] = {k, k == nz ? 0 : (k == 1 ? nz + 1 : -1)};
+__global__ void __launch_bounds__(kMT2, 4) k_smooth_march(VofSep w, const double *__restrict__ in,
+                                                       double *__restrict__ out, double *__restrict__ rho,
+                                                       double *__restrict__ mu, Lay L, int nx, int ny, int nz,
+                                                       double rhol, double rhog, double mul, double mug) {
+  constexpr int CX = kMX + 2, CY = kMY + 2, NP = CX * CY, NY = kMY * CX;
+  static_assert(NP <= 2 * kMT2 && NY <= 2 * kMT2, "two elements per thread");
+  __shared__ double ring[8][NP];     // input planes, slot = plane & 7
+  __shared__ double c1[NP];          // after z
+  __shared__ double c2[kMY][CX];     // after y
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kMX + tx;
+  const int i0 = blockIdx.x * kMX + 1, j0 = blockIdx.y * kMY + 1;
+  const int kb = blockIdx.z * kMKC + 1, ke = min(kb + kMKC - 1, nz);
+  // everything that does not change up the march, once: the thread's (up to)
+  // two tile elements with their plane-0 offsets, its y-pass elements with
+  // their weights, its x weights and output offset
+  long src[2];
+  bool ld[2];
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+  for (int q = 0; q < 2; ++q) {
+    const int e = tid + q * kMT2, cx = e % CX, cy = e / CX;
+    const int gi = i0 - 1 + cx, gj = j0 - 1 + cy;
+    ld[q] = e < NP && gi <= nx + 1 && gj <= ny + 1;
+    src[q] = ld[q] ? at(L, gi, gj, 0) : 0;
+  }
+  int ye[2];
+  double ywm[2], yw0[2], ywp[2];
 #pragma unroll
-      for (int b = 0; b < 2; ++b)
+  for (int q = 0; q < 2; ++q) {
+    const int e = tid + q * kMT2, cx = e % CX, oy = e / CX;
+    ye[q] = e < NY ? oy * CX + cx : -1;
+    const int jj = min(j0 + min(oy, kMY - 1), ny) - 1;
+    ywm[q] = w.ym[jj];
+    yw0[q] = w.y0[jj];
+    ywp[q] = w.yp[jj];
+  }
+  const int i = i0 + tx, j = j0 + ty;
+  const bool in_tile = i <= nx && j <= ny;
+  const int ic = min(i, nx) - 1;
+  const double xwm = w.xm[ic], xw0 = w.x0[ic], xwp = w.xp[ic];
+  const long oij = at(L, min(i, nx), min(j, ny), 0);
+  const int xs1 = i == nx ? 0 : (i == 1 ? nx + 1 : -1), ys1 = j == 1 ? 0 : (j == ny ? ny + 1 : -1);
+  auto load = [&](int kp) {  // plane kp of 0..nz+1
+    double *dst = ring[kp & 7];
+    const long ko = (long)kp * L.sk;
 #pragma unroll
-        for (int d = 0; d < 2; ++d) {
-          if (xs[a] < 0 || ys[b] < 0 || zs[d] < 0) continue;
-          const long o = at(L, xs[a], ys[b], zs[d]);
-          out[o] = c;
-          if constexpr (PROPS) {
-            mu[o] = m;
-            rho[o] = r;
-          }
+    for (int q = 0; q < 2; ++q) {
+      const int e = tid + q * kMT2;
+      if (ld[q]) cp_async8(dst + e, in + src[q] + ko);
+      else if (e < NP) dst[e] = 0.0;
+    }
+  };
+  // groups: {kb-1, kb, kb+1}, {kb+2}, {kb+3}; then one per step (possibly empty)
+  load(kb - 1);
+  load(kb);
+  load(kb + 1);
+  cp_async_commit();
+  if (kb + 2 <= ke + 1) load(kb + 2);
+  cp_async_commit();
+  if (kb + 3 <= ke + 1) load(kb + 3);
+  cp_async_commit();
+  cp_async_wait_group<2>();
+  __syncthreads();
+  for (int k = kb; k <= ke; ++k) {
+    // plane k+4 into the slot of plane k-4, read four steps ago
+    if (k + 4 <= ke + 1) load(k + 4);
+    cp_async_commit();
+    {
+      const double zm = w.zm[k - 1], z0 = w.z0[k - 1], zp = w.zp[k - 1];
+      const double *pm = ring[(k - 1) & 7], *p0 = ring[k & 7], *pp = ring[(k + 1) & 7];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int e = tid + q * kMT2;
+        if (e < NP) c1[e] = zm * pm[e] + z0 * p0[e] + zp * pp[e];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int e = ye[q];
+      if (e >= 0) (&c2[0][0])[e] = ywm[q] * c1[e] + yw0[q] * c1[e + CX] + ywp[q] * c1[e + 2 * CX];
+    }
+    __syncthreads();
+    if (in_tile) {
+      const double c = xwm * c2[ty][tx] + xw0 * c2[ty][tx + 1] + xwp * c2[ty][tx + 2];
+      const double m = mug * c + (1.0 - c) * mul, r = rhog * c + (1.0 - c) * rhol;
+      const int zs1 = k == nz ? 0 : (k == 1 ? nz + 1 : -1);
+      if (xs1 < 0 && ys1 < 0 && zs1 < 0) {
+        const long o = oij + (long)k * L.sk;
+        out[o] = c;
+        if constexpr (PROPS) {
+          mu[o] = m;
+          rho[o] = r;
         }
+      } else {
+        // the cell and the ghost cells equal to it
+        const int xs[2] = {i, xs1}, ys[2] = {j, ys1}, zs[2] = {k, zs1};
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int d = 0; d < 2; ++d) {
+              if (xs[a] < 0 || ys[b] < 0 || zs[d] < 0) continue;
+              const long o = at(L, xs[a], ys[b], zs[d]);
+              out[o] = c;
+              if constexpr (PROPS) {
+                mu[o] = m;
+                rho[o] = r;
+              }
+            }
+      }
+    }
+    cp_async_wait_group<2>();  // plane k+2 has landed (k+3, k+4 may be in flight)
+    __syncthreads();
   }
+  cp_async_wait_all();
 }
 
 }  // namespace
@@ -190,9 +255,9 @@ __global__ void __launch_bounds__(kST) k_smooth_pass(VofSep w, const double *__r
 void launch_material_props_fused(const VofSep &w, const double *c, double *cs, double *rho, double *mu, double *tmp,
                                  Lay L, int nx, int ny, int nz, double rhol, double rhog, double mul, double mug,
                                  cudaStream_t st) {
-  const dim3 grid((nx + kSX - 1) / kSX, (ny + kSY - 1) / kSY, (nz + kSZ - 1) / kSZ);
-  k_smooth_pass<false><<<grid, kST, 0, st>>>(w, c, tmp, nullptr, nullptr, L, nx, ny, nz, 0.0, 0.0, 0.0, 0.0);
-  k_smooth_pass<true><<<grid, kST, 0, st>>>(w, tmp, cs, rho, mu, L, nx, ny, nz, rhol, rhog, mul, mug);
+  const dim3 grid((nx + kMX - 1) / kMX, (ny + kMY - 1) / kMY, (nz + kMKC - 1) / kMKC), blk(kMX, kMY);
+  k_smooth_march<false><<<grid, blk, 0, st>>>(w, c, tmp, nullptr, nullptr, L, nx, ny, nz, 0.0, 0.0, 0.0, 0.0);
+  k_smooth_march<true><<<grid, blk, 0, st>>>(w, tmp, cs, rho, mu, L, nx, ny, nz, rhol, rhog, mul, mug);
 }
 
 void launch_material_props(const VofTab &t, const double *c, double *cs, double *rho, double *mu, double *qv, Lay L,
