@@ -456,7 +456,7 @@ def main():
         pk0, _ = peaks()
         vofres = {"value": g.ncells / (vms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": vms,
                   "alg_bytes": vbytes, "alg_GBps": vbytes / (vms * 1e-3) / 1e9,
-                  "frac": vbytes / (vms * 1e-3) / 1e9 / pk0, "launches_per_step": 11,
+                  "frac": vbytes / (vms * 1e-3) / 1e9 / pk0, "launches_per_step": 2,
                   "note": "cs, rho, mu from the volume fraction (two cell-vertex-cell passes); bytes: read c, "
                           "write cs, rho, mu"}
         del vc, vcs, vrho, vmu
