@@ -1144,7 +1144,6 @@ int tbfp_material_props(tbfp_handle *h, const double *c, double *cs, double *rho
 // ---------------------------------------------------------------------------
 int tbfp_momentum_setup(tbfp_handle *h, const tbfp_momentum_desc *m) {
   if (!h || !m) return TBFP_ENULL;
-  if (h->slab) return set_err(h, TBFP_EINVAL, "tbfp_momentum_setup: needs a whole-channel handle");
   if (h->mom) return set_err(h, TBFP_EINVAL, "tbfp_momentum_setup: already set up for this handle");
   if (m->scheme < 0 || m->scheme > 5) return set_err(h, TBFP_EINVAL, "tbfp_momentum_setup: scheme must be 0..5");
   if (h->hd_u < 2 || h->hd_rho < 1)
@@ -1272,7 +1271,8 @@ int tbfp_update_boundaries_v_dev(tbfp_handle *h, double *ux, double *uy, double 
   if (rc) return rc;
   if (!h->mom) return set_err(h, TBFP_EINVAL, "tbfp_update_boundaries_v: call tbfp_momentum_setup first");
   cudaSetDevice(h->device);
-  launch_boundaries_v(h->wt, ux, uy, uz, h->Lux, h->Luy, h->Luz, h->nx, h->ny, h->nz, h->hd_u, h->stream);
+  launch_boundaries_v(h->wt, ux, uy, uz, h->Lux, h->Luy, h->Luz, h->nx, h->ny, h->nz, h->hd_u, h->slab != 0,
+                      h->stream);
   return finish(h, "tbfp_update_boundaries_v");
 }
 
@@ -1285,7 +1285,7 @@ int tbfp_update_boundaries_v(tbfp_handle *h, double *ux, double *uy, double *uz)
   if ((rc = h2d(h, h->h_ux, ux, h->n_ux)) || (rc = h2d(h, h->h_uy, uy, h->n_uy)) || (rc = h2d(h, h->h_uz, uz, h->n_uz)))
     return rc;
   launch_boundaries_v(h->wt, h->h_ux, h->h_uy, h->h_uz, h->Lux, h->Luy, h->Luz, h->nx, h->ny, h->nz, h->hd_u,
-                      h->stream);
+                      h->slab != 0, h->stream);
   if ((rc = d2h(h, ux, h->h_ux, h->n_ux)) || (rc = d2h(h, uy, h->h_uy, h->n_uy)) || (rc = d2h(h, uz, h->h_uz, h->n_uz)))
     return rc;
   TBFP_CK(h, cudaStreamSynchronize(h->stream));

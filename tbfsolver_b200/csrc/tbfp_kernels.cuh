@@ -252,8 +252,11 @@ void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, 
 struct WallTabs {
   double hb[3], hi[3], tb[3], ti[3], bb[3], bt[3];
 };
+// slab: a rank of a z-split channel; its z ghost planes and uz's plane k = 0
+// come from the neighbours (the caller's exchange), so only the wall ghosts
+// and the x halos of the planes ks..nz are written here.
 void launch_boundaries_v(const WallTabs &w, double *ux, double *uy, double *uz, Lay Lux, Lay Luy, Lay Luz, int nx,
-                         int ny, int nz, int hd, cudaStream_t st);
+                         int ny, int nz, int hd, bool slab, cudaStream_t st);
 
 // Flow control: mode 0 sums 0.5*(rho(i+1)+rho(i))*Vsx, mode 1 sums ux*Vsx over
 // i = 0..nx-1, j = 1..ny, k = 1..nz into *out (device); part holds ny*nz

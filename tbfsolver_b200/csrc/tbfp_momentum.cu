@@ -751,18 +751,22 @@ __global__ void __launch_bounds__(kMT) k_momentum_update(MomUpd a) {
 //   any other j:                        the element (mx(i), j, mz(k)),
 // so one gather pass in place is race-free.  It visits the halo planes
 // k < 1 and k > nz (all i, j) and, for k = 1..nz, the wall ghost rows (all i)
-// and the x halo columns (and ux's i = 0) of the other rows.
+// and the x halo columns (and ux's i = 0) of the other rows.  On a slab of a
+// z-split channel the z ghost planes and uz's plane 0 belong to the
+// neighbours' exchange: the pass covers the planes ks..nz without z wrap.
 struct BcComp {
   double *f;
   Lay L;
   int ilo, ihi, jlo, jhi, klo, khi;  // allocated extents
   int js, je, jb, jt;                // interior j range, the wall formulas' source rows
   double hb, hi, tb, ti, bb, bt;     // dhb, dhi and wall value: bottom, top
+  int kin0;                          // first plane of the row/column part (1; ks on a slab)
   long n_planes, n_total;            // elements visited in the halo planes; in all
 };
 struct BcArgs {
   BcComp c[3];
   int nx, nz;
+  int slab;  // 1: no z wrap (planes ks..nz only, mz = identity)
 };
 
 __device__ __forceinline__ double wall(double v, double dhb, double dhi, double bf) {
@@ -787,8 +791,8 @@ __global__ void __launch_bounds__(256) k_boundaries_v(BcArgs a) {
     const long u = t - c.n_planes;
     const int nxh = (1 - c.ilo) + (c.ihi - a.nx);  // x halo columns (ux: with i = 0)
     const long per_k = 2L * NI + (long)(NJ - 2) * nxh;
-    k = 1 + (int)(u / per_k);
-    const int r = (int)(u - (k - 1) * per_k);
+    k = c.kin0 + (int)(u / per_k);
+    const int r = (int)(u - (k - c.kin0) * per_k);
     if (r < 2 * NI) {
       j = r < NI ? c.js - 1 : c.je + 1;
       i = c.ilo + r % NI;
@@ -801,7 +805,7 @@ __global__ void __launch_bounds__(256) k_boundaries_v(BcArgs a) {
     }
   }
   const int mi = i < 1 ? i + a.nx : (i > a.nx ? i - a.nx : i);
-  const int mk = k < 1 ? k + a.nz : (k > a.nz ? k - a.nz : k);
+  const int mk = a.slab ? k : (k < 1 ? k + a.nz : (k > a.nz ? k - a.nz : k));
   double v;
   if (j == c.js - 1) v = wall(c.f[at(c.L, mi, c.jb, mk)], c.hb, c.hi, c.bb);
   else if (j == c.je + 1) v = wall(c.f[at(c.L, mi, c.jt, mk)], c.tb, c.ti, c.bt);
@@ -940,10 +944,11 @@ void launch_momentum(const MomentumTabs &t, double *ux, double *uy, double *uz, 
 }
 
 void launch_boundaries_v(const WallTabs &w, double *ux, double *uy, double *uz, Lay Lux, Lay Luy, Lay Luz, int nx,
-                         int ny, int nz, int hd, cudaStream_t st) {
+                         int ny, int nz, int hd, bool slab, cudaStream_t st) {
   BcArgs a{};
   a.nx = nx;
   a.nz = nz;
+  a.slab = slab ? 1 : 0;
   double *f[3] = {ux, uy, uz};
   const Lay L[3] = {Lux, Luy, Luz};
   long most = 0;
@@ -970,8 +975,11 @@ void launch_boundaries_v(const WallTabs &w, double *ux, double *uy, double *uz, 
     c.bt = w.bt[e];
     const long NI = c.ihi - c.ilo + 1, NJ = c.jhi - c.jlo + 1;
     const long nplanes = (1 - c.klo) + hd, nxh = (1 - c.ilo) + hd;
-    c.n_planes = nplanes * NI * NJ;
-    c.n_total = c.n_planes + (long)nz * (2 * NI + (NJ - 2) * nxh);
+    // a slab leaves its z ghost planes (and uz's plane 0) to the exchange and
+    // does the walls and x halos of its planes ks..nz
+    c.kin0 = slab ? ks : 1;
+    c.n_planes = slab ? 0 : nplanes * NI * NJ;
+    c.n_total = c.n_planes + (long)(nz - c.kin0 + 1) * (2 * NI + (NJ - 2) * nxh);
     most = c.n_total > most ? c.n_total : most;
   }
   k_boundaries_v<<<dim3((unsigned)((most + 255) / 256), 3), 256, 0, st>>>(a);

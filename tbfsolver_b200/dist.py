@@ -150,6 +150,53 @@ def exchange_z_ghosts(f: torch.Tensor, s: Slabs, hd: int, group=None) -> None:
     f[s.nz_loc + hd:s.nz_loc + 2 * hd] = recv_hi
 
 
+def exchange_z_ghosts_sz(f: torch.Tensor, s: Slabs, hd: int, group=None) -> None:
+    """The z exchange of a z-staggered field (uz, planes -hd..nz_loc+hd) on a
+    slab: the hd ghost planes on each side and the periodic duplicate
+    uz(:,:,0) = the rank below's uz(:,:,nz_loc) (updateHalo's 'sz' case,
+    field.f90:910-930, and equatePeriodicBC, vfield.f90:124-189): the planes
+    nz_loc-hd..nz_loc of the rank below land in -hd..0, the planes 1..hd of
+    the rank above in nz_loc+1..nz_loc+hd."""
+    n = s.nz_loc
+    if n < hd + 1:
+        raise ValueError("a slab must hold more than hd planes")
+    up = f[n:n + hd + 1]              # k = nz_loc-hd..nz_loc -> rank above's -hd..0
+    down = f[hd + 1:2 * hd + 1]       # k = 1..hd -> rank below's nz_loc+1..nz_loc+hd
+    if s.world == 1:
+        f[0:hd + 1] = up.clone()
+        f[n + hd + 1:n + 2 * hd + 1] = down.clone()
+        return
+    below, above = (s.rank - 1) % s.world, (s.rank + 1) % s.world
+    recv_lo = torch.empty_like(up)
+    recv_hi = torch.empty_like(down)
+    ops = [dist.P2POp(dist.isend, up.contiguous(), above, group, 3),
+           dist.P2POp(dist.irecv, recv_lo, below, group, 3),
+           dist.P2POp(dist.isend, down.contiguous(), below, group, 4),
+           dist.P2POp(dist.irecv, recv_hi, above, group, 4)]
+    for w in dist.batch_isend_irecv(ops):
+        w.wait()
+    f[0:hd + 1] = recv_lo
+    f[n + hd + 1:n + 2 * hd + 1] = recv_hi
+
+
+def exchange_v_ghosts(u, s: Slabs, hd: int, group=None) -> None:
+    """The z part of updateBoundariesV on a slab (after tbfp_update_boundaries_v
+    did the walls and x halos): ux and uy as cell-like fields, uz with its
+    periodic duplicate."""
+    exchange_z_ghosts(u.ux.a, s, hd, group)
+    exchange_z_ghosts(u.uy.a, s, hd, group)
+    exchange_z_ghosts_sz(u.uz.a, s, hd, group)
+
+
+def sum_over_ranks(x: float, device="cpu", group=None) -> float:
+    """A volume sum over the ranks of a split channel (the reference's Mpi_Allreduce)."""
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return float(x)
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return float(t.item())
+
+
 def max_over_ranks(x: float, device="cpu", group=None) -> float:
     """The maximum of a per-rank value (device times are reported this way)."""
     if not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:
@@ -173,6 +220,16 @@ def exchange_z_ghosts_local(fields: list, slabs: list, hd: int) -> None:
     for r, (f, s) in enumerate(zip(fields, slabs)):
         f[0:hd] = highs[(r - 1) % P]
         f[s.nz_loc + hd:s.nz_loc + 2 * hd] = lows[(r + 1) % P]
+
+
+def exchange_z_ghosts_sz_local(fields: list, slabs: list, hd: int) -> None:
+    """exchange_z_ghosts_sz for several ranks held by one process, by copies."""
+    P = len(fields)
+    ups = [f[s.nz_loc:s.nz_loc + hd + 1].clone() for f, s in zip(fields, slabs)]
+    downs = [f[hd + 1:2 * hd + 1].clone() for f in fields]
+    for r, (f, s) in enumerate(zip(fields, slabs)):
+        f[0:hd + 1] = ups[(r - 1) % P]
+        f[s.nz_loc + hd + 1:s.nz_loc + 2 * hd + 1] = downs[(r + 1) % P]
 
 
 def all_to_all_local(sends: list) -> list:

@@ -295,9 +295,14 @@ class MomentumEqn:
         self.solver = solver
         self.scheme, self.gch, self.g = int(scheme), float(gch), float(g)
         g_ = solver.mesh
+        # a rank of a z-split channel (dist.SlabChannel) holds planes k0+1..k0+nz
+        slab = getattr(solver, "s", None)
+        self._k0, self._nz = (slab.k0, slab.nz_loc) if slab is not None else (0, g_.nz)
+        k0, nzl = self._k0, self._nz
         self._t = {n: np.ascontiguousarray(getattr(g_, n).r(0, nn + 1))
-                   for n, nn in (("dxf", g_.nx), ("dxc", g_.nx), ("dyf", g_.ny), ("dyc", g_.ny), ("dzf", g_.nz),
-                                 ("dzc", g_.nz), ("yc", g_.ny))}
+                   for n, nn in (("dxf", g_.nx), ("dxc", g_.nx), ("dyf", g_.ny), ("dyc", g_.ny), ("yc", g_.ny))}
+        for n in ("dzf", "dzc"):
+            self._t[n] = np.ascontiguousarray(getattr(g_, n).r(k0, k0 + nzl + 1))
         self._t["yf"] = np.ascontiguousarray(g_.yf.r(0, g_.ny))
         m = TbfpMomentumDesc(scheme=scheme, gch=gch, g=g, ubot=(C.c_double * 3)(*ubot),
                              utop=(C.c_double * 3)(*utop),
@@ -319,8 +324,8 @@ class MomentumEqn:
                    gch=par.read_real("gCH"), g=par.read_real("g"), ubot=ubot, utop=utop)
 
     def _shapes(self):
-        m = self.solver.mesh
-        return [(m.nz, m.ny, m.nx + 1), (m.nz, m.ny - 1, m.nx), (m.nz + 1, m.ny, m.nx)]
+        m, nz = self.solver.mesh, self._nz
+        return [(nz, m.ny, m.nx + 1), (nz, m.ny - 1, m.nx), (nz + 1, m.ny, m.nx)]
 
     def fluxes(self):
         """The fluxes of the last step (phi_x, phi_y, phi_z) over the equation boxes."""
@@ -338,6 +343,8 @@ class MomentumEqn:
         check(sv.lib.tbfp_momentum_fluxes(sv.h, *[a.ctypes.data_as(C.c_void_p) for a in arrs], 1), sv.h)
 
     def _boxes(self):
+        if self._nz != self.solver.mesh.nz:
+            raise TbfpError(TBFP_EINVAL, "the phi0 files hold the whole channel: gather the slabs' fluxes first")
         m = self.solver.mesh
         return [(0, m.nx, 1, m.ny, 1, m.nz), (1, m.nx, 1, m.ny - 1, 1, m.nz), (1, m.nx, 1, m.ny, 0, m.nz)]
 
@@ -417,9 +424,19 @@ class FlowControl:
     on the GPU (tbfp_rho_face_sum, tbfp_flow_rate); the scalar formulas are
     the reference's."""
 
-    def __init__(self, solver: FastPoissonSolver, flow_ctrl: int, ret: float = 0.0, q0: float = 0.0):
+    def __init__(self, solver: FastPoissonSolver, flow_ctrl: int, ret: float = 0.0, q0: float = 0.0, group=None):
         self.solver = solver
         self.flow_ctrl, self.ret, self.q0 = int(flow_ctrl), float(ret), float(q0)
+        # on a rank of a z-split channel the volume sums add over the ranks (Mpi_Allreduce)
+        self._slab = getattr(solver, "s", None) is not None
+        self.group = group
+
+    def _global(self, x: float) -> float:
+        if not self._slab:
+            return x
+        from .dist import sum_over_ranks  # noqa: PLC0415
+
+        return sum_over_ranks(x, group=self.group)
 
     @classmethod
     def from_specs(cls, solver: FastPoissonSolver, specs_dir: str, u: VField | None = None) -> "FlowControl":
@@ -448,7 +465,7 @@ class FlowControl:
         out = C.c_double(0.0)
         fn = sv.lib.tbfp_rho_face_sum_dev if _placement([rho]) else sv.lib.tbfp_rho_face_sum
         check(fn(sv.h, rho.address(), C.byref(out)), sv.h)
-        return out.value
+        return self._global(out.value)
 
     def flow_rate(self, u: VField) -> float:
         """computeFlowRate: the sum of ux*Vsx over the faces i = 0..nx-1."""
@@ -456,7 +473,7 @@ class FlowControl:
         out = C.c_double(0.0)
         fn = sv.lib.tbfp_flow_rate_dev if _placement([u.ux]) else sv.lib.tbfp_flow_rate
         check(fn(sv.h, u.ux.address(), C.byref(out)), sv.h)
-        return out.value
+        return self._global(out.value)
 
     def set_press_grad(self, rho: Field, rhol: float, mul: float, g: float) -> float:
         """setPressGrad (auxiliaryRoutines.f90:336-393): the forcing fs of the

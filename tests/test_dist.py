@@ -11,7 +11,8 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from tbfsolver_b200.dist import Slabs, exchange_z_ghosts, max_over_ranks, split, to_kx_slabs, to_z_slabs
+from tbfsolver_b200.dist import (Slabs, exchange_z_ghosts, exchange_z_ghosts_sz, exchange_z_ghosts_sz_local,
+                                 max_over_ranks, split, sum_over_ranks, to_kx_slabs, to_z_slabs)
 
 
 def _free_port():
@@ -43,6 +44,16 @@ def _worker(rank, world, port, nx, ny, nz, errq):
             exchange_z_ghosts(loc, s, hd)
             idx = [(s.k0 - hd + m) % nz for m in range(s.nz_loc + 2 * hd)]
             assert torch.equal(loc, f[idx])
+        # uz-like arrays (planes -hd..nz_loc+hd): ghosts and the periodic duplicate
+        # plane 0 = the rank below's nz_loc; global faces 0..nz with face 0 == face nz
+        for hd in (1, 2):
+            faces = torch.from_numpy(rng.standard_normal((nz, 3, 5)))  # faces 1..nz at index 0..nz-1
+            loc = torch.full((s.nz_loc + 1 + 2 * hd, 3, 5), float("nan"), dtype=torch.float64)
+            loc[hd + 1:hd + 1 + s.nz_loc] = faces[s.k0:s.k0 + s.nz_loc]
+            exchange_z_ghosts_sz(loc, s, hd)
+            idx = [(s.k0 - hd + m - 1) % nz for m in range(s.nz_loc + 1 + 2 * hd)]
+            assert torch.equal(loc, faces[idx])
+        assert sum_over_ranks(float(rank + 1)) == float(world * (world + 1) // 2)
         assert max_over_ranks(float(rank + 1)) == float(world)
         dist.barrier()
         dist.destroy_process_group()
@@ -70,3 +81,20 @@ def test_partition():
     s1 = Slabs(16, 4, 12, 1, 0)
     exchange_z_ghosts(loc, s1, 1)
     assert torch.equal(loc[0], f[11]) and torch.equal(loc[13], f[0])
+
+
+def test_sz_exchange_one_process_matches_the_periodic_faces():
+    """exchange_z_ghosts_sz_local over three slabs held by one process: every
+    slab's planes -hd..nz_loc+hd hold the periodic faces k0-hd..k0+nz_loc+hd."""
+    nz, hd = 10, 2
+    slabs = [Slabs(8, 4, nz, 3, r) for r in range(3)]
+    faces = torch.arange(float(nz)).reshape(nz, 1)  # faces 1..nz at index 0..nz-1
+    locs = []
+    for s in slabs:
+        loc = torch.full((s.nz_loc + 1 + 2 * hd, 1), float("nan"))
+        loc[hd + 1:hd + 1 + s.nz_loc] = faces[s.k0:s.k0 + s.nz_loc]
+        locs.append(loc)
+    exchange_z_ghosts_sz_local(locs, slabs, hd)
+    for s, loc in zip(slabs, locs):
+        idx = [(s.k0 - hd + m - 1) % nz for m in range(s.nz_loc + 1 + 2 * hd)]
+        assert torch.equal(loc, faces[idx])
