@@ -242,8 +242,8 @@ int tbfp_projection_mg_dev(tbfp_handle *h, const double *ux_in, const double *uy
    (halo hd_rho); c's ghosts must be current (the reference updates them).
    tbfp_vof_setup takes the grid coordinates (grid.f90:633-688: centroids
    xc(0:nx+1), yc(0:ny+1), zc(0:nz+1) and faces xf(0:nx), yf(0:ny), zf(0:nz))
-   and the phase properties (VOFCTOR), once per handle; a whole-channel
-   handle only. */
+   and the phase properties (VOFCTOR), once per handle (on a slab handle:
+   the local planes' z coordinates zc(k0:k0+nz+1), zf(k0:k0+nz), hd_rho = 1). */
 typedef struct {
   const double *xc, *yc, *zc; /* centroids, Fortran indices 0..n+1 */
   const double *xf, *yf, *zf; /* faces, Fortran indices 0..n */
@@ -252,6 +252,14 @@ typedef struct {
 int tbfp_vof_setup(tbfp_handle *h, const tbfp_vof_desc *v);
 int tbfp_material_props(tbfp_handle *h, const double *c, double *cs, double *rho, double *mu);
 int tbfp_material_props_dev(tbfp_handle *h, const double *c, double *cs, double *rho, double *mu);
+/* One of the two smoothing passes (hd_rho = 1, device pointers): out = the
+   cell -> vertex -> cell pass of in with its ghost images; with rho and mu
+   (the second pass) also the properties.  On a slab handle (a z-split
+   channel) the pass writes no z ghost images: the caller exchanges the z ghost
+   planes of out (and rho, mu) with the neighbours after each pass, as the
+   reference's updateBoundaries does.  tbfp_material_props is
+   pass(c -> scratch), pass(scratch -> cs, rho, mu) on a whole channel. */
+int tbfp_material_props_pass_dev(tbfp_handle *h, const double *in, double *out, double *rho, double *mu);
 
 /* --- momentum predictor ------------------------------------------------ */
 /* solveMomentumEqn FAST (momentumEqn.f90:161-194) without its closing

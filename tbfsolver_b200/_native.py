@@ -116,6 +116,7 @@ PROTOTYPES = {
     "tbfp_momentum_predictor": (C.c_int, [_H] + [C.c_void_p] * 7 + [C.c_double] * 6),
     "tbfp_momentum_predictor_dev": (C.c_int, [_H] + [C.c_void_p] * 7 + [C.c_double] * 6),
     "tbfp_momentum_predictor_out_dev": (C.c_int, [_H] + [C.c_void_p] * 10 + [C.c_double] * 6),
+    "tbfp_material_props_pass_dev": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tbfp_update_boundaries_v": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tbfp_rho_face_sum": (C.c_int, [_H, C.c_void_p, C.POINTER(C.c_double)]),
     "tbfp_rho_face_sum_dev": (C.c_int, [_H, C.c_void_p, C.POINTER(C.c_double)]),

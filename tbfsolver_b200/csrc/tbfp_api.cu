@@ -1017,7 +1017,8 @@ int tbfp_vof_setup(tbfp_handle *h, const tbfp_vof_desc *v) {
   if (!h || !v) return TBFP_ENULL;
   if (!v->xc || !v->yc || !v->zc || !v->xf || !v->yf || !v->zf)
     return set_err(h, TBFP_ENULL, "tbfp_vof_setup: a coordinate array is NULL");
-  if (h->slab) return set_err(h, TBFP_EINVAL, "tbfp_vof_setup: needs a whole-channel handle");
+  if (h->slab && h->hd_rho != 1)
+    return set_err(h, TBFP_EUNSUPPORTED, "tbfp_vof_setup: a slab handle needs hd_rho = 1 (the fused passes)");
   if (h->vof) return set_err(h, TBFP_EINVAL, "tbfp_vof_setup: already set up for this handle");
   const int nx = h->nx, ny = h->ny, nz = h->nz;
   // distance tables of cellToVertex / vertexToCell (interpolation.f90:188-276)
@@ -1112,10 +1113,29 @@ int tbfp_vof_setup(tbfp_handle *h, const tbfp_vof_desc *v) {
   return TBFP_OK;
 }
 
+int tbfp_material_props_pass_dev(tbfp_handle *h, const double *in, double *out, double *rho, double *mu) {
+  int rc = check_ptrs(h, {in, out});
+  if (rc) return rc;
+  if (!h->vof) return set_err(h, TBFP_EINVAL, "tbfp_material_props_pass: call tbfp_vof_setup first");
+  if (h->hd_rho != 1) return set_err(h, TBFP_EUNSUPPORTED, "tbfp_material_props_pass: needs hd_rho = 1");
+  if ((rho == nullptr) != (mu == nullptr))
+    return set_err(h, TBFP_EINVAL, "tbfp_material_props_pass: rho and mu are both given or both NULL");
+  if (aliased(in, out) || (rho && (aliased(in, rho) || aliased(in, mu) || aliased(out, rho) || aliased(out, mu) ||
+                                   aliased(rho, mu))))
+    return set_err(h, TBFP_EINVAL, "tbfp_material_props_pass: the arrays must be distinct");
+  cudaSetDevice(h->device);
+  launch_smooth_pass(h->vsep, in, out, rho, mu, h->Lrho, h->nx, h->ny, h->nz, h->rhol, h->rhog, h->mul, h->mug,
+                     !h->slab, h->stream);
+  return finish(h, "tbfp_material_props_pass");
+}
+
 int tbfp_material_props_dev(tbfp_handle *h, const double *c, double *cs, double *rho, double *mu) {
   int rc = check_ptrs(h, {c, cs, rho, mu});
   if (rc) return rc;
   if (!h->vof) return set_err(h, TBFP_EINVAL, "tbfp_material_props: call tbfp_vof_setup first");
+  if (h->slab)
+    return set_err(h, TBFP_EINVAL, "tbfp_material_props: on a slab handle run the two passes "
+                                   "(tbfp_material_props_pass_dev) with the z ghost exchange between them");
   if (aliased(c, cs) || aliased(c, rho) || aliased(c, mu) || aliased(cs, rho) || aliased(cs, mu) || aliased(rho, mu))
     return set_err(h, TBFP_EINVAL, "tbfp_material_props: c, cs, rho and mu must be distinct arrays");
   cudaSetDevice(h->device);
@@ -1127,6 +1147,9 @@ int tbfp_material_props(tbfp_handle *h, const double *c, double *cs, double *rho
   int rc = check_ptrs(h, {c, cs, rho, mu});
   if (rc) return rc;
   if (!h->vof) return set_err(h, TBFP_EINVAL, "tbfp_material_props: call tbfp_vof_setup first");
+  if (h->slab)
+    return set_err(h, TBFP_EINVAL, "tbfp_material_props: on a slab handle run the two passes "
+                                   "(tbfp_material_props_pass_dev) with the z ghost exchange between them");
   cudaSetDevice(h->device);
   for (double *&b : h->h_vof)
     if (!b && (rc = dev_alloc(h, &b, h->n_rho))) return rc;

@@ -229,6 +229,10 @@ struct VofSep {
 void launch_material_props_fused(const VofSep &w, const double *c, double *cs, double *rho, double *mu, double *tmp,
                                  Lay L, int nx, int ny, int nz, double rhol, double rhog, double mul, double mug,
                                  cudaStream_t st);
+// One fused smoothing pass (halo 1); rho, mu non-NULL: the final pass with the
+// properties.  zimg = false on a slab: no periodic z ghost images.
+void launch_smooth_pass(const VofSep &w, const double *in, double *out, double *rho, double *mu, Lay L, int nx, int ny,
+                        int nz, double rhol, double rhog, double mul, double mug, bool zimg, cudaStream_t st);
 
 // Momentum predictor (tbfp_momentum.cu).  Spacings indexed by the Fortran
 // index: dxf, dxc, dzf, dzc over 0..n+1 (x and z periodic), dyf over 1..ny and

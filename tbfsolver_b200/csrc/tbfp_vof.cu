@@ -126,13 +126,15 @@ void bc_cell(double *f, Lay L, int nx, int ny, int nz, int hd, cudaStream_t st) 
 // nx+1 -> 1; y: 0 -> 1, ny+1 -> ny; z: 0 -> nz, nz+1 -> 1), so each cell also
 // writes the ghost cells that copy it.  PROPS: the final pass, which also
 // writes rho and mu (VOF.f90:220-221) at the cell and its ghost images.
+// zimg = 0 (a slab of a z-split channel): no z ghost images, the neighbours'
+// planes arrive by the caller's exchange between the passes.
 constexpr int kMX = 32, kMY = 8, kMKC = 32, kMT2 = kMX * kMY;
 
 template <bool PROPS>
 __global__ void __launch_bounds__(kMT2, 4) k_smooth_march(VofSep w, const double *__restrict__ in,
                                                        double *__restrict__ out, double *__restrict__ rho,
                                                        double *__restrict__ mu, Lay L, int nx, int ny, int nz,
-                                                       double rhol, double rhog, double mul, double mug) {
+                                                       double rhol, double rhog, double mul, double mug, int zimg) {
   constexpr int CX = kMX + 2, CY = kMY + 2, NP = CX * CY, NY = kMY * CX;
   static_assert(NP <= 2 * kMT2 && NY <= 2 * kMT2, "two elements per thread");
   __shared__ double ring[8][NP];     // input planes, slot = plane & 7
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(kMT2, 4) k_smooth_march(VofSep w, const double
     if (in_tile) {
       const double c = xwm * c2[ty][tx] + xw0 * c2[ty][tx + 1] + xwp * c2[ty][tx + 2];
       const double m = mug * c + (1.0 - c) * mul, r = rhog * c + (1.0 - c) * rhol;
-      const int zs1 = k == nz ? 0 : (k == 1 ? nz + 1 : -1);
+      const int zs1 = !zimg ? -1 : (k == nz ? 0 : (k == 1 ? nz + 1 : -1));
       if (xs1 < 0 && ys1 < 0 && zs1 < 0) {
         const long o = oij + (long)k * L.sk;
         out[o] = c;
@@ -256,8 +258,17 @@ void launch_material_props_fused(const VofSep &w, const double *c, double *cs, d
                                  Lay L, int nx, int ny, int nz, double rhol, double rhog, double mul, double mug,
                                  cudaStream_t st) {
   const dim3 grid((nx + kMX - 1) / kMX, (ny + kMY - 1) / kMY, (nz + kMKC - 1) / kMKC), blk(kMX, kMY);
-  k_smooth_march<false><<<grid, blk, 0, st>>>(w, c, tmp, nullptr, nullptr, L, nx, ny, nz, 0.0, 0.0, 0.0, 0.0);
-  k_smooth_march<true><<<grid, blk, 0, st>>>(w, tmp, cs, rho, mu, L, nx, ny, nz, rhol, rhog, mul, mug);
+  k_smooth_march<false><<<grid, blk, 0, st>>>(w, c, tmp, nullptr, nullptr, L, nx, ny, nz, 0.0, 0.0, 0.0, 0.0, 1);
+  k_smooth_march<true><<<grid, blk, 0, st>>>(w, tmp, cs, rho, mu, L, nx, ny, nz, rhol, rhog, mul, mug, 1);
+}
+
+void launch_smooth_pass(const VofSep &w, const double *in, double *out, double *rho, double *mu, Lay L, int nx, int ny,
+                        int nz, double rhol, double rhog, double mul, double mug, bool zimg, cudaStream_t st) {
+  const dim3 grid((nx + kMX - 1) / kMX, (ny + kMY - 1) / kMY, (nz + kMKC - 1) / kMKC), blk(kMX, kMY);
+  if (rho)
+    k_smooth_march<true><<<grid, blk, 0, st>>>(w, in, out, rho, mu, L, nx, ny, nz, rhol, rhog, mul, mug, zimg);
+  else
+    k_smooth_march<false><<<grid, blk, 0, st>>>(w, in, out, nullptr, nullptr, L, nx, ny, nz, 0.0, 0.0, 0.0, 0.0, zimg);
 }
 
 void launch_material_props(const VofTab &t, const double *c, double *cs, double *rho, double *mu, double *qv, Lay L,

@@ -188,6 +188,20 @@ def exchange_v_ghosts(u, s: Slabs, hd: int, group=None) -> None:
     exchange_z_ghosts_sz(u.uz.a, s, hd, group)
 
 
+def slab_material_props(vof, c, cs, rho, mu, tmp, s: Slabs, group=None, exchange=None) -> None:
+    """updateMaterialProps on a slab: the two smoothing passes, each followed by
+    the z ghost exchange of what it wrote (the reference's updateBoundaries of
+    cs between the passes; rho and mu are computed over the whole arrays
+    there, so their ghost planes are the neighbours' values too).  exchange
+    (fields) replaces the collective exchange, e.g. by copies between slabs
+    held in one process; by default exchange_z_ghosts on each field."""
+    ex = exchange or (lambda fs: [exchange_z_ghosts(f.a, s, 1, group) for f in fs])
+    vof.smooth_pass(c, tmp)
+    ex([tmp])
+    vof.smooth_pass(tmp, cs, rho, mu)
+    ex([cs, rho, mu])
+
+
 def sum_over_ranks(x: float, device="cpu", group=None) -> float:
     """A volume sum over the ranks of a split channel (the reference's Mpi_Allreduce)."""
     if not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:

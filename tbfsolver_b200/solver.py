@@ -263,13 +263,16 @@ class VOF:
 
     def __init__(self, solver: FastPoissonSolver, rhol: float, rhog: float, mul: float, mug: float):
         m = solver.mesh
-        nx, ny, nz = m.nx, m.ny, m.nz
+        nx, ny = m.nx, m.ny
+        # a rank of a z-split channel (dist.SlabChannel) holds planes k0+1..k0+nz
+        slab = getattr(solver, "s", None)
+        k0, nz = (slab.k0, slab.nz_loc) if slab is not None else (0, m.nz)
         self.solver = solver
         self.rhol, self.rhog, self.mul, self.mug = rhol, rhog, mul, mug
         self._c = {
             "xc": np.ascontiguousarray(m.xc.r(0, nx + 1)), "yc": np.ascontiguousarray(m.yc.r(0, ny + 1)),
-            "zc": np.ascontiguousarray(m.zc.r(0, nz + 1)), "xf": np.ascontiguousarray(m.xf.r(0, nx)),
-            "yf": np.ascontiguousarray(m.yf.r(0, ny)), "zf": np.ascontiguousarray(m.zf.r(0, nz)),
+            "zc": np.ascontiguousarray(m.zc.r(k0, k0 + nz + 1)), "xf": np.ascontiguousarray(m.xf.r(0, nx)),
+            "yf": np.ascontiguousarray(m.yf.r(0, ny)), "zf": np.ascontiguousarray(m.zf.r(k0, k0 + nz)),
         }
         v = TbfpVofDesc(rhol=rhol, rhog=rhog, mul=mul, mug=mug,
                         **{k: a.ctypes.data_as(C.c_void_p) for k, a in self._c.items()})
@@ -281,6 +284,16 @@ class VOF:
         dev = _placement([c, cs, rho, mu])
         fn = sv.lib.tbfp_material_props_dev if dev else sv.lib.tbfp_material_props
         check(fn(sv.h, c.address(), cs.address(), rho.address(), mu.address()), sv.h)
+
+    def smooth_pass(self, inp: Field, out: Field, rho: Field | None = None, mu: Field | None = None) -> None:
+        """One smoothing pass (device fields, halo 1); with rho and mu the second
+        pass with the properties.  On a slab the caller exchanges the z ghost
+        planes of out (rho, mu) after it (dist.slab_material_props)."""
+        sv = self.solver
+        _placement([inp, out, rho, mu])
+        check(sv.lib.tbfp_material_props_pass_dev(sv.h, inp.address(), out.address(),
+                                                  rho.address() if rho is not None else None,
+                                                  mu.address() if mu is not None else None), sv.h)
 
 
 class MomentumEqn:

@@ -1,9 +1,10 @@
-"""The momentum step (predictor + updateBoundariesV) on the slabs of a z-split
-channel, the ranks held by one process on one GPU and their exchanges done by
-copies (the planes dist.exchange_v_ghosts moves between GPUs): every rank
-runs the whole-channel kernels on its planes with its ghost planes from the
-neighbours, so the assembled velocity and fluxes equal the whole-channel
-step bit for bit."""
+"""The momentum step (predictor + updateBoundariesV) and the material
+properties on the slabs of a z-split channel, the ranks held by one process on
+one GPU and their exchanges done by copies (the planes dist.exchange_v_ghosts
+and dist.slab_material_props move between GPUs): every rank runs the
+whole-channel kernels on its planes with its ghost planes from the
+neighbours, so the assembled fields and fluxes equal the whole channel's bit
+for bit."""
 import numpy as np
 import pytest
 import torch
@@ -67,6 +68,46 @@ def test_slab_momentum_step_is_the_whole_channel_step(P, dims, scheme):
                 assert torch.equal(got.a, _zslice(want, k0, nzl).a), ch.rank
             for got, want, kz in zip(mo.fluxes(), whole_phi, (0, 0, 1)):
                 assert np.array_equal(got, want[k0:k0 + nzl + kz]), ch.rank
+    finally:
+        for ch in chans:
+            ch.close()
+
+
+@pytest.mark.parametrize("P,dims", [(2, (32, 24, 16)), (3, (48, 40, 24))])
+def test_slab_material_props_are_the_whole_channel_props(P, dims):
+    """updateMaterialProps on slabs: pass, z ghost exchange, pass, exchange
+    (dist.slab_material_props, here with the exchanges done by copies between
+    slabs held in one process) gives the whole channel's cs, rho, mu bit for
+    bit, ghost planes included."""
+    from tbfsolver_b200.solver import VOF
+
+    nx, ny, nz = dims
+    g = Grid(nx, ny, nz, 2 * np.pi, 2.0, np.pi, True, 1.5)
+    props = dict(rhol=1.0, rhog=0.05, mul=1e-3, mug=5e-5)
+    spec = synth.small_spec(nx, ny, nz, stretched=True, nbubbles=3, radius=0.35)
+    c = Field("cl", 1, nx, ny, nz, synth.vof_field(spec, synth.bubble_centres(spec, P), hd=1).cuda())
+    zeros = lambda f: Field.like(f, torch.zeros_like(f.a))  # noqa: E731
+    with FastPoissonSolver(g) as fps:
+        vof = VOF(fps, **props)
+        w = [zeros(c) for _ in range(3)]
+        vof.update_material_props(c, *w)
+    chans = [SlabChannel(g, P, r) for r in range(P)]
+    try:
+        vofs = [VOF(ch, **props) for ch in chans]
+        sc = [_zslice(c, ch.s.k0, ch.s.nz_loc) for ch in chans]
+        tmp = [zeros(x) for x in sc]
+        outs = [[zeros(x) for _ in range(3)] for x in sc]
+        slabs = [ch.s for ch in chans]
+        for v, x, t in zip(vofs, sc, tmp):
+            v.smooth_pass(x, t)
+        exchange_z_ghosts_local([t.a for t in tmp], slabs, 1)
+        for v, t, (cs, rho, mu) in zip(vofs, tmp, outs):
+            v.smooth_pass(t, cs, rho, mu)
+        for q in range(3):
+            exchange_z_ghosts_local([o[q].a for o in outs], slabs, 1)
+        for ch, o in zip(chans, outs):
+            for got, want in zip(o, w):
+                assert torch.equal(got.a, _zslice(want, ch.s.k0, ch.s.nz_loc).a), ch.rank
     finally:
         for ch in chans:
             ch.close()
