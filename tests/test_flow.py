@@ -176,3 +176,45 @@ def test_double_buffered_substep_matches_the_in_place_one():
     for a, b in zip(ua, ub):
         assert rel_linf(b, a) < 1e-13
     assert rel_linf(pb, pa) < 1e-12
+
+
+@pytest.mark.gpu
+def test_new_entry_points_refuse_bad_calls():
+    """The momentum, boundary, flow and property entry points fail loudly
+    (TbfpError with the library's message) instead of computing garbage."""
+    from tbfsolver_b200._native import TBFP_EINVAL, TBFP_ENULL, TbfpError, load
+    from tbfsolver_b200.dist import SlabChannel
+    from tbfsolver_b200.solver import VOF
+
+    g = _grid(16, 12, 8, True)
+    lib = load()
+    with FastPoissonSolver(g) as fps:
+        mom = MomentumEqn.__new__(MomentumEqn)  # a wrapper without setup
+        mom.solver = fps
+        u = VField(*[Field(k, 2, 16, 12, 8, torch.zeros(field_shape(k, 2, 16, 12, 8), dtype=torch.float64,
+                                                      device="cuda")) for k in ("sx", "sy", "sz")])
+        with pytest.raises(TbfpError) as e:
+            mom.update_boundaries_v(u)
+        assert e.value.code == TBFP_EINVAL and "tbfp_momentum_setup" in str(e.value)
+        assert lib.tbfp_update_boundaries_v_dev(fps.h, None, None, None) == TBFP_ENULL
+        mom = MomentumEqn(fps, scheme=2)
+        cl = lambda: Field("cl", 1, 16, 12, 8, torch.ones(field_shape("cl", 1, 16, 12, 8), dtype=torch.float64,  # noqa: E731
+                                                            device="cuda"))
+        with pytest.raises(TbfpError) as e:  # u_out aliasing u
+            mom.predictor(u, cl(), cl(), cl(), dt=1e-3, alpha=1.0, gamma=1.0, xi=0.0, rho0=1.0, u_out=u)
+        assert e.value.code == TBFP_EINVAL
+        with pytest.raises(TbfpError):  # dt must be positive
+            mom.predictor(u, cl(), cl(), cl(), dt=0.0, alpha=1.0, gamma=1.0, xi=0.0, rho0=1.0)
+        with pytest.raises(TbfpError):  # a second setup on the handle
+            MomentumEqn(fps, scheme=2)
+    chan = SlabChannel(g, 2, 0)
+    try:
+        vof = VOF(chan, rhol=1.0, rhog=0.1, mul=1e-3, mug=1e-4)
+        c = Field("cl", 1, 16, 12, chan.s.nz_loc,
+                  torch.zeros(field_shape("cl", 1, 16, 12, chan.s.nz_loc), dtype=torch.float64, device="cuda"))
+        outs = [Field.like(c, torch.zeros_like(c.a)) for _ in range(3)]
+        with pytest.raises(TbfpError) as e:  # a slab needs the two passes with exchanges
+            vof.update_material_props(c, *outs)
+        assert "tbfp_material_props_pass_dev" in str(e.value)
+    finally:
+        chan.close()
