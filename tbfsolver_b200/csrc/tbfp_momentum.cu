@@ -1,19 +1,23 @@
-// Momentum predictor: solveMomentumEqn FAST (momentumEqn.f90:161-194) without
-// its closing updateBoundariesV (the caller's halo refresh, as for the
-// projection).  Kernel 1, updateConveDiff (:198-607): the convection (flux
-// limited, compute_limiters :611-734) and diffusion (variable viscosity, with
-// the transposed stress terms) of each velocity component on its equation
-// box (setEqnBounds :1134-1190: ux i = 0..nx, uy j = 1..ny-1, uz k = 0..nz),
-// into the flux arrays.  Kernel 2, addConvDiff (:738-791) and addSource
-// (:874-973): u += dt*(gamma*phi + xi*phi_prev), then the surface-tension,
-// forcing and body-force sources.  Every expression follows the reference's
-// operand order, with one substitution: a quotient by a grid spacing is a
-// product with the spacing's reciprocal (tables built once on the host, each
-// the correctly rounded 1/d), and the four limiter ratios of one direction
-// share the reciprocals of their two denominators.  Each such term then
-// differs from the reference's quotient by at most an ulp or two, and FP64
-// divisions -- 96 per cell in the literal form, the kernel's whole cost --
-// drop to 24 reciprocals.  The kernel is specialised per convection scheme.
+// Momentum predictor: solveMomentumEqn FAST (momentumEqn.f90:161-194), and
+// its closing updateBoundariesV (vfield.f90:111-189) as a launch of its own.
+// The flux kernel, updateConveDiff (:198-607): the convection (flux limited,
+// compute_limiters :611-734) and diffusion (variable viscosity, with the
+// transposed stress terms) of each velocity component on its equation box
+// (setEqnBounds :1134-1190: ux i = 0..nx, uy j = 1..ny-1, uz k = 0..nz), into
+// the flux arrays; a tiled kernel that marches up z with the stencil planes in
+// shared memory, plus a small launch for the ux faces i = 0.  The update,
+// addConvDiff (:738-791) and addSource (:874-973): u += dt*(gamma*phi +
+// xi*phi_prev), then the surface-tension, forcing and body-force sources --
+// a separate pass over u in place, or inside the flux kernel when u* goes to
+// a second buffer.  Every expression follows the reference's operand order,
+// with these substitutions: a quotient by a grid spacing is a product with the
+// spacing's reciprocal (tables built once on the host, each the correctly
+// rounded 1/d); the four limiter ratios of one direction share the
+// reciprocals of their two denominators; QUICK's ratio cancels against the
+// face difference it multiplies (exact zero differences kept).  Each such term
+// differs from the reference's by an ulp or two, and the 96 FP64 divisions per
+// cell of the literal form drop to at most 22 reciprocals (4 for QUICK).  The
+// kernels are specialised per convection scheme.
 #include <cuda_runtime.h>
 
 #include "tbfp_kernels.cuh"
