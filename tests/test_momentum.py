@@ -330,3 +330,29 @@ def test_out_of_place_predictor_equals_the_in_place_one(scheme):
         assert rel_linf(b, a) < 1e-15
     for a, b in zip(pa, pb):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("hd_u,hd_rho", [(3, 1), (2, 2), (3, 2)])
+def test_predictor_with_wider_halos_matches_the_oracle(hd_u, hd_rho):
+    """The kernels address every array through its layout: wider velocity or
+    cell halos than the reference's 2 and 1 give the same step."""
+    nx, ny, nz = 24, 20, 12
+    g = _grid(nx, ny, nz, True)
+    m = mesh_of(g)
+    rng = np.random.default_rng(hd_u * 10 + hd_rho)
+    u = [O.FField(k, hd_u, nx, ny, nz, rng.uniform(-0.5, 0.5, field_shape(k, hd_u, nx, ny, nz))) for k in ("sx", "sy", "sz")]
+    cl = lambda lo, hi: O.FField("cl", hd_rho, nx, ny, nz, rng.uniform(lo, hi, field_shape("cl", hd_rho, nx, ny, nz)))  # noqa: E731
+    c, mu, rho = cl(0.0, 1.0), cl(1e-4, 1e-3), cl(0.1, 1.0)
+    kw = dict(dt=2e-3, alpha=1.0, gamma=1.0, xi=0.0, rho0=0.1, fs=0.2)
+    with FastPoissonSolver(g, hd_u=hd_u, hd_rho=hd_rho) as fps:
+        mom = MomentumEqn(fps, scheme=5, gch=0.3)
+        du = VField(*[_to_dev(f, "device") for f in u])
+        dc, dmu, drho = (_to_dev(f, "device") for f in (c, mu, rho))
+        mom.predictor(du, dc, dmu, drho, **kw)
+        got = [_host(f) for f in du.components()]
+    prev = [np.zeros(s) for s in ((nz, ny, nx + 1), (nz, ny - 1, nx), (nz + 1, ny, nx))]
+    O.momentum_predictor(m, *u, c, mu, rho, prev, kw["dt"], kw["alpha"], kw["gamma"], kw["xi"], kw["rho0"],
+                         gch=0.3, fs=kw["fs"], scheme=5)
+    for a, b in zip(got, u):
+        assert rel_linf(a, b.a) < 1e-13
