@@ -536,6 +536,15 @@ __global__ void k_psi_ghosts(double *__restrict__ psi, Lay Lp, int hd, int nx, i
 dim3 wgrid(int nxe, int ny, int nz, int J) {
   return dim3((unsigned)((nxe + kWalkX - 1) / kWalkX), (unsigned)((ny + J - 1) / J), (unsigned)nz);
 }
+// Rows per block of a summing sweep: up to kMgJ (fewer atomics on the sum),
+// but never so many that the grid drops below ~8 blocks per SM -- a walk of J
+// rows is a serial chain, and on the coarse levels (a few thousand rows) J =
+// kMgJ left a few dozen blocks walking 16 rows each (15 us per sweep where
+// one row per block takes 3-5 us).
+int sum_rows(int nxe, int ny, int nz) {
+  const long rows = (long)((nxe + kWalkX - 1) / kWalkX) * ny * nz;
+  return (int)std::max<long>(1, std::min<long>(kMgJ, rows / (148L * 8)));
+}
 unsigned nblk_grid(long n) {
   long b = (n + kMgThreads - 1) / kMgThreads;
   return (unsigned)std::min<long>(b, 148L * 8);
@@ -836,7 +845,7 @@ struct Run {
     if (n_iter == 0) return false;
     for (int it = 0; it < n_iter; ++it) {
       const bool last = it == n_iter - 1;
-      const int J = last ? kMgJ : 1;
+      const int J = last ? sum_rows((L.nx + 1) / 2, L.ny, L.nz) : 1;
       double *sum = last ? slot : nullptr;
       k_rbgs_colour<<<wgrid((L.nx + 1) / 2, L.ny, L.nz, J), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, 0, sum);
       k_rbgs_colour<<<wgrid((L.nx + 1) / 2, L.ny, L.nz, J), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, 1, sum);
