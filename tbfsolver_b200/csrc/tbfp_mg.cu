@@ -536,6 +536,15 @@ __global__ void k_psi_ghosts(double *__restrict__ psi, Lay Lp, int hd, int nx, i
 dim3 wgrid(int nxe, int ny, int nz, int J) {
   return dim3((unsigned)((nxe + kWalkX - 1) / kWalkX), (unsigned)((ny + J - 1) / J), (unsigned)nz);
 }
+// Rows per block of the level kernels without a reduction: a walk of up to
+// jmax rows where the grid stays above rows/div blocks.  One row per block on
+// every level made the finest level's kernels launch-rate bound (65,536
+// blocks of one row for a residual on 256x256x128): walking up to 4 rows
+// (sweeps up to 16) was 7 % faster over a PCG solve.
+int rows_j(int nxe, int ny, int nz, long div, int jmax) {
+  const long rows = (long)((nxe + kWalkX - 1) / kWalkX) * ny * nz;
+  return (int)std::max<long>(1, std::min<long>(jmax, rows / div));
+}
 // Rows per block of a summing sweep: up to kMgJ (fewer atomics on the sum),
 // but never so many that the grid drops below ~8 blocks per SM -- a walk of J
 // rows is a serial chain, and on the coarse levels (a few thousand rows) J =
@@ -845,7 +854,7 @@ struct Run {
     if (n_iter == 0) return false;
     for (int it = 0; it < n_iter; ++it) {
       const bool last = it == n_iter - 1;
-      const int J = last ? sum_rows((L.nx + 1) / 2, L.ny, L.nz) : 1;
+      const int J = last ? sum_rows((L.nx + 1) / 2, L.ny, L.nz) : rows_j((L.nx + 1) / 2, L.ny, L.nz, 4096, kMgJ);
       double *sum = last ? slot : nullptr;
       k_rbgs_colour<<<wgrid((L.nx + 1) / 2, L.ny, L.nz, J), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, 0, sum);
       k_rbgs_colour<<<wgrid((L.nx + 1) / 2, L.ny, L.nz, J), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, 1, sum);
@@ -863,12 +872,12 @@ struct Run {
     }
     double *pre = m.msum + 2 * l, *post = m.msum + 2 * l + 1;
     const bool hpre = rbgs(l, m.prm.n_pre, l != 0, pre);
-    k_mg_residual<<<wgrid(L.nx, L.ny, L.nz, 1), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, L.res, nullptr);
+    k_mg_residual<<<wgrid(L.nx, L.ny, L.nz, rows_j(L.nx, L.ny, L.nz, 4096, 4)), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, L.res, nullptr);
     auto &C = m.lv[l + 1];
-    k_restrict<<<wgrid(C.nx, C.ny, C.nz, 1), kWalkX, 0, st>>>(L.L, C.L, L.res, C.q);
+    k_restrict<<<wgrid(C.nx, C.ny, C.nz, rows_j(C.nx, C.ny, C.nz, 4096, 4)), kWalkX, 0, st>>>(L.L, C.L, L.res, C.q);
     vcycle(l + 1);
     const bool hcpost = l + 1 < last && m.prm.n_post > 0;
-    k_prolong_add<<<wgrid(L.nx, L.ny, L.nz, 1), kWalkX, 0, st>>>(
+    k_prolong_add<<<wgrid(L.nx, L.ny, L.nz, rows_j(L.nx, L.ny, L.nz, 4096, 4)), kWalkX, 0, st>>>(
         L.L, C.L, C.p, L.p, hpre ? pre : nullptr, 1.0 / (double)L.n, hcpost ? m.msum + 2 * (l + 1) + 1 : nullptr,
         1.0 / (double)C.n);
     const bool hpost = rbgs(l, m.prm.n_post, false, post);
