@@ -141,16 +141,31 @@ __global__ void __launch_bounds__(128, 8) k_correct_div(CorrArgs a, GridK g, uns
     // every load of this step, issued together
     const int ow = op + xo, qw = oq + xo;
     const double psx = ps[op + 1], pnx = pn[op + 1], pox = po[op + 1], irx = ir[oq + 1];
-    const double psw = ps[ow], pnw = pn[ow], pow_ = po[ow], irw = ir[qw];
-    const double psw1 = ps[ow + 1], pnw1 = pn[ow + 1], pow1 = po[ow + 1], irw1 = ir[qw + 1];
+    // the lower x face is the upper face of lane - 1; lane 0 computes it
+    const bool lead = (threadIdx.x & 31) == 0;
+    double psw = 0.0, pnw = 0.0, pow_ = 0.0, irw = 0.0, psw1 = 0.0, pnw1 = 0.0, pow1 = 0.0, irw1 = 0.0, ux_w = 0.0;
+    if (lead) {
+      psw = ps[ow];
+      pnw = pn[ow];
+      pow_ = po[ow];
+      irw = ir[qw];
+      psw1 = ps[ow + 1];
+      pnw1 = pn[ow + 1];
+      pow1 = po[ow + 1];
+      irw1 = ir[qw + 1];
+      ux_w = uxi[ox + xo];
+    }
     const double psy = ps[op + pjs], pny = pn[op + pjs], poy = po[op + pjs], iry = ir[oq + rjs];
     const double psz = ps[op + pz], pnz = pn[op + pz], poz = po[op + pz], irz = ir[oq + qz];
     const double psm = ps[op + pm], pnm = pn[op + pm], pom = po[op + pm], irm = ir[oq + qm];
-    const double ux_c = uxi[ox], ux_w = uxi[ox + xo], uy_c = uyi[oy], uz_c = uzi[oz], uz_m = uzi[oz + zm];
+    const double ux_c = uxi[ox], uy_c = uyi[oy], uz_c = uzi[oz], uz_m = uzi[oz + zm];
 
     const double uxp = face_update(ux_c, r, ir0, irx, irc, idxc, psx, psc, pnx, pnc, pox, poc, stf(0, ic, j, k));
-    const double uxm = face_update(ux_w, r, ir0, irw1, irw, idxc, psw1, psw, pnw1, pnw, pow1, pow_,
-                                   stf(0, ic + xo, j, k));
+    const double uxl = lead ? face_update(ux_w, r, ir0, irw1, irw, idxc, psw1, psw, pnw1, pnw, pow1, pow_,
+                                          stf(0, ic + xo, j, k))
+                            : 0.0;
+    const double uxs = __shfl_up_sync(0xffffffffu, uxp, 1);
+    const double uxm = lead ? uxl : uxs;
     const double uyp = (j < g.ny) ? face_update(uy_c, r, ir0, iry, irc, g.idyc[j], psy, psc, pny, pnc, poy, poc,
                                                 stf(1, ic, j, k))
                                   : uy_c;
