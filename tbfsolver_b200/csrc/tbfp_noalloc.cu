@@ -1,14 +1,13 @@
 // tbfp_solve_fps_noalloc: the solveFPS path for callers that cannot allocate
 // device memory.
 //
-// Some callers cannot call cudaMalloc: codes that run inside a CUDA graph
-// capture, inside a memory pool that another runtime owns, or under a
-// framework that forbids allocation on its solver path (a Fortran driver that
-// hands over device arrays it allocated itself is the typical case).  This
-// entry point takes the grid descriptor and the caller's device arrays and
-// allocates nothing: its work spectrum and its set-up tables live in one
-// file-scope __device__ array of fixed size that every GPU loading the library
-// holds until the process exits.
+// Some callers cannot call cudaMalloc: a code whose device memory belongs to
+// a pool that another runtime owns, or a framework that forbids allocation on
+// its solver path (a Fortran driver that hands over device arrays it allocated
+// itself is the typical case).  This entry point takes the grid descriptor and
+// the caller's device arrays and allocates nothing: its work spectrum and its
+// set-up tables live in one file-scope __device__ array of fixed size that
+// every GPU loading the library holds until the process exits.
 //
 // * Limits: (nx/2+1)*ny*nz <= TBFP_NOALLOC_MAX_SPECTRUM complex entries
 //   (64 MiB), nx <= 4096, ny <= 2048, nz <= 2048; larger sizes are rejected
@@ -23,6 +22,7 @@
 //   or on two streams -- race on the array and must be serialised by the caller.
 //   (Within one process the host side of this function holds a lock and
 //   synchronises its stream before returning, which serialises its own calls.)
+// * The caller's current device is the same after the call as before it.
 // * Errors: the status code, with the message in tbfp_last_error(NULL).
 #include <cuda_runtime.h>
 
@@ -73,9 +73,25 @@ int fail(int code, const std::string &msg) {
   return code;
 }
 
+int solve_fps_noalloc(const tbfp_desc *d, const double *s, double *psi);
+
 }  // namespace
 
+// The caller's current device is restored on every return path.
 extern "C" int tbfp_solve_fps_noalloc(const tbfp_desc *d, const double *s, double *psi) {
+  int prev = -1;
+  const bool have_prev = cudaGetDevice(&prev) == cudaSuccess;
+  const int rc = solve_fps_noalloc(d, s, psi);
+  if (have_prev) {
+    int now = -1;
+    if (cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+  }
+  return rc;
+}
+
+namespace {
+
+int solve_fps_noalloc(const tbfp_desc *d, const double *s, double *psi) {
   set_global_error("");
   if (!d || !s || !psi) return fail(TBFP_ENULL, "tbfp_solve_fps_noalloc: NULL argument");
   if (d->nx < 4 || d->ny < 4 || d->nz < 2 || (d->nx % 2) != 0 || d->hd_psi < 1)
@@ -85,6 +101,16 @@ extern "C" int tbfp_solve_fps_noalloc(const tbfp_desc *d, const double *s, doubl
   if (!(d->dx_fft > 0.0) || !(d->dz_fft > 0.0))
     return fail(TBFP_EINVAL, "tbfp_solve_fps_noalloc: dx_fft and dz_fft must be positive");
   const int nx = d->nx, ny = d->ny, nz = d->nz, nkx = nx / 2 + 1;
+  if (nx <= kNxMax && ny <= kNyMax && nz <= kNzMax) {  // the same metric checks as tbfp_create
+    for (int i = 0; i < nx; ++i)
+      if (!(d->dxf[i] > 0.0)) return fail(TBFP_EINVAL, "tbfp_solve_fps_noalloc: dxf must be positive");
+    for (int j = 0; j < ny; ++j)
+      if (!(d->dyf[j] > 0.0)) return fail(TBFP_EINVAL, "tbfp_solve_fps_noalloc: dyf must be positive");
+    for (int j = 0; j <= ny; ++j)
+      if (!(d->dyc[j] > 0.0)) return fail(TBFP_EINVAL, "tbfp_solve_fps_noalloc: dyc must be positive");
+    for (int k = 0; k < nz; ++k)
+      if (!(d->dzf[k] > 0.0)) return fail(TBFP_EINVAL, "tbfp_solve_fps_noalloc: dzf must be positive");
+  }
   const long R = (long)ny * nz;
   if (nx > kNxMax || ny > kNyMax || nz > kNzMax || (long)nkx * R > kSpecMax)
     return fail(TBFP_EUNSUPPORTED,
@@ -188,3 +214,5 @@ extern "C" int tbfp_solve_fps_noalloc(const tbfp_desc *d, const double *s, doubl
   if (e != cudaSuccess) return fail(TBFP_ECUDA, std::string("tbfp_solve_fps_noalloc: ") + cudaGetErrorString(e));
   return TBFP_OK;
 }
+
+}  // namespace
