@@ -53,14 +53,22 @@ extern "C" {
 #define TBFP_ENOMEM (-4)     /* device allocation failed */
 #define TBFP_EUNSUPPORTED (-5) /* size or feature not supported */
 #define TBFP_ENODEVICE (-6)  /* no usable CUDA device */
+#define TBFP_ENONFINITE (-7) /* a NaN or Inf reached a residual, the pressure or max|div u|: a
+                                non-finite input, or a breakdown (the reference aborts) */
+#define TBFP_ESINGULAR (-8)  /* MG_MODE: the coarsest-level system is singular (beta not positive) */
 
 /* precision modes */
 #define TBFP_FP64 0  /* plain FP64: the drop-in for solveFPS */
 #define TBFP_MIXED 1 /* FP32 transforms + FP64 defect correction: psi = solve32(s), then
-                        psi += solve32(s - L psi) until ||s - L psi||_2/||s||_2 <= tol.
-                        The residual is that of the system the FP64 path solves (the
-                        incompatible part of s, sum s V != 0, sits on the top wall).
-                        Synchronises the stream once per correction sweep. */
+                        psi += solve32(s - L psi) until ||s - L psi||_2/||s||_2 <= tol and,
+                        in a projection, also max|div u| <= tol (div u of the corrected
+                        velocity is alpha*dt/rho0 * (s - L psi) cell by cell).  The
+                        residual is that of the system the FP64 path solves (the
+                        incompatible part of s, sum s V != 0, sits on the top wall).  The
+                        loop runs on the device (a CUDA graph with a conditional WHILE
+                        node, also inside a caller's stream capture): no host round trip
+                        per sweep.  A synchronous call reads the outcome back; with
+                        TBFP_FLAG_ASYNC and no stats the sweep count is reported as -1. */
 
 /* create-time flags */
 #define TBFP_FLAG_ASYNC 1u  /* do not synchronise the stream before returning */
@@ -356,9 +364,9 @@ int tbfp_slab_inverse_x(tbfp_handle *h, const double *spec_z, double *psi);
 /* No counterpart in the reference, which runs one channel per job.  Each
    member is a channel with its own descriptor (sizes may differ); its arrays
    are device arrays laid out as for tbfp_projection_dev.  Members run on a
-   pool of nstreams streams; when every member is TBFP_FP64 the whole step is
-   captured once as a CUDA graph and replayed while the arrays and scalars
-   stay the same.  Calls are synchronous.  Surface tension is not supported in
+   pool of nstreams streams; the whole step (TBFP_MIXED members with their
+   device-side refinement loops included) is captured once as a CUDA graph and
+   replayed while the arrays and scalars stay the same.  Calls are synchronous.  Surface tension is not supported in
    an ensemble. */
 typedef struct tbfp_ensemble tbfp_ensemble;
 typedef struct {
@@ -376,8 +384,8 @@ int tbfp_ensemble_projection_dev(tbfp_ensemble *e, const tbfp_member_io *io, dou
 
 /* --- solveFPS without device allocation ------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device
-   memory (inside a CUDA graph capture, under a memory pool another runtime
-   owns, or a driver that only hands over arrays it allocated itself): the same
+   memory (code under a memory pool another runtime owns, or a driver that
+   only hands over arrays it allocated itself): the same
    solve as tbfp_solve_fps_dev, on the caller's device arrays s and psi, with no
    handle.  Work spectrum and set-up tables live in one static device array that
    every GPU loading the library holds until exit, which limits the grid to
@@ -385,7 +393,8 @@ int tbfp_ensemble_projection_dev(tbfp_ensemble *e, const tbfp_member_io *io, dou
    nx <= 4096, ny <= 2048, nz <= 2048 (else TBFP_EUNSUPPORTED).  The first call
    on a device looks up the array's address; make it before any stream capture.
    All calls share the array: calls that overlap on the GPU race.  Runs on
-   d->stream (NULL: the legacy default stream), synchronous; error text via
+   d->stream (NULL: the legacy default stream), synchronous; the caller's
+   current device is restored before returning; error text via
    tbfp_last_error(NULL).  Only the fields nx, ny, nz, hd_psi, dx_fft, dz_fft,
    dxf, dyf, dyc, dzf, s_Vg, device and stream of d are read. */
 #define TBFP_NOALLOC_MAX_SPECTRUM 4194304

@@ -21,6 +21,8 @@ TBFP_ECUDA = -3
 TBFP_ENOMEM = -4
 TBFP_EUNSUPPORTED = -5
 TBFP_ENODEVICE = -6
+TBFP_ENONFINITE = -7
+TBFP_ESINGULAR = -8
 
 TBFP_FP64 = 0
 TBFP_MIXED = 1

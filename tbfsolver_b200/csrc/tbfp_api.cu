@@ -32,6 +32,14 @@ namespace tbfp {
 void set_global_error(const std::string &msg) { g_create_error = msg; }
 }  // namespace tbfp
 
+// An executable graph of the mixed refinement for one (s, psi) pair of arrays.
+struct MixedGraph {
+  const double *s = nullptr;
+  double *psi = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long used = 0;
+};
+
 struct tbfp_handle {
   int nx = 0, ny = 0, nz = 0, nkx = 0;
   long R = 0;
@@ -56,7 +64,13 @@ struct tbfp_handle {
   double2 *d_twx = nullptr;                     // exp(-2 pi i m/nx), the r2c/c2r factors
   double2 *d_tpx = nullptr, *d_tpz = nullptr;  // pass-ordered twiddles of lengths nx/2 and nz
   float2 *d_twx32 = nullptr, *d_tpx32 = nullptr, *d_tpz32 = nullptr;  // FP32 copies (TBFP_MIXED)
-  double *d_acc = nullptr;  // reductions of the residual passes: [0] sum s dyf, [1] sum s^2, [2..] sum r^2
+  double *d_acc = nullptr;  // reductions of the residual passes: [0] sum s dyf, [1] sum s^2, [2] sum r^2,
+                            // [3] max|s - L psi| (bits)
+  MixedCtl *d_ctl = nullptr;  // device-side control of the mixed refinement loop
+  cudaStream_t cap = nullptr, cap_body = nullptr;  // capture streams of the mixed-refinement graphs
+  MixedGraph mgr[4];          // executable refinement graphs, least recently used evicted
+  unsigned long long mgr_tick = 0;
+  bool mgr_off = false;       // the runtime refused the conditional graph: host-driven loop
   double idx2 = 0.0, idz2 = 0.0, ctop_scale = 0.0;
   tbfp_stats last{};        // statistics of the last solve or projection
   bool slab = false;        // one rank's slab of a channel (tbfp_slab_create)
@@ -303,58 +317,211 @@ int read_rel_residual(tbfp_handle *h, int slot, double *rel) {
   TBFP_CK(h, cudaMemcpyAsync(&v[1], h->d_acc + slot, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   TBFP_CK(h, cudaStreamSynchronize(h->stream));
   *rel = v[0] > 0.0 ? std::sqrt(v[1] / v[0]) : std::sqrt(v[1]);
+  if (!std::isfinite(*rel)) return set_err(h, TBFP_ENONFINITE, "tbfp_solve_fps: non-finite residual (NaN or Inf in s)");
   return TBFP_OK;
+}
+
+// --- mixed precision: FP32 spectral solves, FP64 residuals, device-side loop ---
+// Sums: acc[0] = sum s dyf, acc[1] = sum s^2 (first pass); acc[2] = sum r^2 and
+// acc[3] = max|s - L psi| of the latest residual pass (cleared by each decision).
+XSrc mixed_x(tbfp_handle *h, const double *s, const double *psi) {
+  XSrc x = xsrc(h, s, psi);
+  x.acc = h->d_acc;
+  x.acc_r = h->d_acc + 2;
+  return x;
+}
+
+void mixed_spectral32(tbfp_handle *h, float2 *sp, cudaStream_t st) {
+  launch_fftz(sp, h->g, h->d_tpz32, false, st);
+  launch_tridiag(sp, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, st);
+  launch_fftz(sp, h->g, h->d_tpz32, true, st);
+}
+
+// psi = solve32(s), then the first residual pass (r transformed into the
+// spectrum for the next sweep) and its decision.
+void mixed_head(tbfp_handle *h, const double *s, double *psi, cudaStream_t st, cudaGraphConditionalHandle cond,
+                bool use_cond) {
+  float2 *sp = reinterpret_cast<float2 *>(h->d_spec);
+  const XSrc x = mixed_x(h, s, psi);
+  launch_fftx_fwd(x, false, h->g, h->d_twx32, h->d_tpx32, sp, st);
+  mixed_spectral32(h, sp, st);
+  launch_fftx_inv(sp, psi, h->Lpsi, h->hd_psi, h->g, h->d_twx32, h->d_tpx32, h->scale, false, st);
+  launch_fftx_fwd(x, true, h->g, h->d_twx32, h->d_tpx32, sp, st);
+  launch_mixed_decide(h->d_ctl, h->d_acc, h->d_acc + 2, cond, use_cond, st);
+}
+
+// One refinement sweep psi += solve32(r), then the residual pass and decision.
+void mixed_body(tbfp_handle *h, const double *s, double *psi, cudaStream_t st, cudaGraphConditionalHandle cond,
+                bool use_cond) {
+  float2 *sp = reinterpret_cast<float2 *>(h->d_spec);
+  const XSrc x = mixed_x(h, s, psi);
+  mixed_spectral32(h, sp, st);
+  launch_fftx_inv(sp, psi, h->Lpsi, h->hd_psi, h->g, h->d_twx32, h->d_tpx32, h->scale, true, st);
+  launch_fftx_fwd(x, true, h->g, h->d_twx32, h->d_tpx32, sp, st);
+  launch_mixed_decide(h->d_ctl, h->d_acc, h->d_acc + 2, cond, use_cond, st);
+}
+
+// Emit the whole refinement into the capture that st belongs to: the head,
+// then a WHILE conditional node whose body (captured on the handle's second
+// capture stream) is one sweep; the decision kernels set the condition, so the
+// loop runs on the device with no host round trip.  Returns false if the
+// runtime refused a step (the capture is then invalid).
+bool emit_mixed_loop(tbfp_handle *h, const double *s, double *psi, cudaStream_t st) {
+  cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  if (cudaStreamGetCaptureInfo(st, &cst, nullptr, &g, nullptr, nullptr) != cudaSuccess ||
+      cst != cudaStreamCaptureStatusActive || !g)
+    return false;
+  if (!h->cap_body && cudaStreamCreateWithFlags(&h->cap_body, cudaStreamNonBlocking) != cudaSuccess) return false;
+  cudaGraphConditionalHandle hc{};
+  if (cudaGraphConditionalHandleCreate(&hc, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
+  mixed_head(h, s, psi, st, hc, true);
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  if (cudaStreamGetCaptureInfo(st, &cst, nullptr, &g, &deps, &nd) != cudaSuccess) return false;
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = hc;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cn = nullptr;
+  if (cudaGraphAddNode(&cn, g, deps, nd, &cp) != cudaSuccess) return false;
+  if (cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) return false;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if (cudaStreamBeginCaptureToGraph(h->cap_body, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+      cudaSuccess)
+    return false;
+  mixed_body(h, s, psi, h->cap_body, hc, true);
+  cudaGraph_t bout = nullptr;
+  return cudaStreamEndCapture(h->cap_body, &bout) == cudaSuccess;
+}
+
+// An executable graph of the whole refinement for the arrays (s, psi).
+cudaGraphExec_t build_mixed_graph(tbfp_handle *h, const double *s, double *psi) {
+  if (!h->cap && cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
+  if (ok) ok = cudaStreamBeginCaptureToGraph(h->cap, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+               cudaSuccess;
+  if (ok) {
+    ok = emit_mixed_loop(h, s, psi, h->cap);
+    cudaGraph_t gout = nullptr;
+    ok = (cudaStreamEndCapture(h->cap, &gout) == cudaSuccess) && ok;
+  }
+  if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  if (!ok) {
+    if (ex) cudaGraphExecDestroy(ex);
+    ex = nullptr;
+    cudaGetLastError();  // clear the refusal; the host-driven loop is used instead
+  }
+  return ex;
+}
+
+// The refinement of s into psi on stream st: device-side loop (a cached graph
+// per (s, psi), or emitted into the caller's capture), else a host-driven loop
+// that reads the decision after every pass.  dscale > 0 adds the divergence
+// bar of the projection (MixedCtl).  The outcome is in h->d_ctl.
+int mixed_solve(tbfp_handle *h, const double *s, double *psi, double dscale, cudaStream_t st) {
+  launch_mixed_params(h->d_ctl, h->d_acc, h->tol, h->tol, dscale, h->max_iter, st);
+  cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+  TBFP_CK(h, cudaStreamIsCapturing(st, &cst));
+  if (cst == cudaStreamCaptureStatusActive) {  // e.g. an ensemble being captured
+    if (!emit_mixed_loop(h, s, psi, st))
+      return set_err(h, TBFP_ECUDA, "mixed refinement: cannot add the device-side loop to the capture");
+    return TBFP_OK;
+  }
+  cudaGraphExec_t ex = nullptr;
+  if (!h->mgr_off) {
+    MixedGraph *hit = nullptr, *lru = &h->mgr[0];
+    for (MixedGraph &m : h->mgr) {
+      if (m.exec && m.s == s && m.psi == psi) hit = &m;
+      if (m.used < lru->used) lru = &m;
+    }
+    if (!hit) {
+      cudaGraphExec_t fresh = build_mixed_graph(h, s, psi);
+      if (!fresh) {
+        h->mgr_off = true;
+      } else {
+        if (lru->exec) {  // evicted: let a launch still in flight finish first
+          TBFP_CK(h, cudaStreamSynchronize(st));
+          cudaGraphExecDestroy(lru->exec);
+        }
+        *lru = MixedGraph{s, psi, fresh, 0};
+        hit = lru;
+      }
+    }
+    if (hit) {
+      hit->used = ++h->mgr_tick;
+      ex = hit->exec;
+    }
+  }
+  if (ex) {
+    TBFP_CK(h, cudaGraphLaunch(ex, st));
+    return TBFP_OK;
+  }
+  const cudaGraphConditionalHandle none{};
+  mixed_head(h, s, psi, st, none, false);
+  for (;;) {
+    MixedCtl c{};
+    TBFP_CK(h, cudaMemcpyAsync(&c, h->d_ctl, sizeof(c), cudaMemcpyDeviceToHost, st));
+    TBFP_CK(h, cudaStreamSynchronize(st));
+    if (c.done) break;
+    mixed_body(h, s, psi, st, none, false);
+  }
+  return TBFP_OK;
+}
+
+// The refinement's outcome (one read of the control block): status TBFP_OK,
+// TBFP_ENOTCONVERGED or TBFP_ENONFINITE (with its message).
+int read_mixed(tbfp_handle *h, int *iters, double *rel, double *div) {
+  MixedCtl c{};
+  TBFP_CK(h, cudaMemcpyAsync(&c, h->d_ctl, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  *iters = c.iters;
+  *rel = c.rel;
+  if (div) *div = c.div;
+  if (c.status == TBFP_ENONFINITE)
+    return set_err(h, TBFP_ENONFINITE, "mixed refinement: non-finite residual (NaN or Inf in the inputs)");
+  return c.status;
 }
 
 // solveFPS (fastPoissonSolver.f90:337-384) on device arrays, including the
 // zero-mean gauge and the ghost update of psi.
 //   TBFP_FP64: one FP64 direct solve; with TBFP_FLAG_RESIDUAL one more pass
-//     computes ||s - L psi||/||s||.
+//     computes ||s - L psi||/||s|| (and reads it back).
 //   TBFP_MIXED: direct solves with an FP32 spectrum (FP64 tridiagonal
-//     arithmetic) and FP64 defect correction: psi = solve32(s), then while
-//     ||r||/||s|| > tol: psi += solve32(r), r = s - L psi recomputed in FP64 by
-//     the forward x pass.  The host reads the residual norm after each pass.
-int device_solve(tbfp_handle *h, const double *s, double *psi, int *iters, double *rel) {
+//     arithmetic) and FP64 defect correction, psi = solve32(s), then
+//     psi += solve32(r) with r = s - L psi recomputed in FP64 by the forward x
+//     pass, until the device-side decision stops the loop (MixedCtl; dscale as
+//     there).  With read the outcome is read back: iterations, residual, status.
+int device_solve(tbfp_handle *h, const double *s, double *psi, double dscale, bool read, int *iters, double *rel) {
   cudaStream_t st = h->stream;
   *iters = 1;
   *rel = -1.0;
-  const bool want_res = h->precision == TBFP_MIXED || (h->flags & TBFP_FLAG_RESIDUAL);
-  if (want_res) TBFP_CK(h, cudaMemsetAsync(h->d_acc, 0, 64 * sizeof(double), st));
-  XSrc x = xsrc(h, s, psi);
-  if (!want_res) x.acc = nullptr;
   if (h->precision == TBFP_FP64) {
+    const bool want_res = (h->flags & TBFP_FLAG_RESIDUAL) != 0;
+    if (want_res) TBFP_CK(h, cudaMemsetAsync(h->d_acc, 0, 4 * sizeof(double), st));
+    XSrc x = xsrc(h, s, psi);
+    if (!want_res) x.acc = nullptr;
     launch_fftx_fwd(x, false, h->g, h->d_twx, h->d_tpx, h->d_spec, st);
     fps_spectral_solve(h);
     launch_fftx_inv(h->d_spec, psi, h->Lpsi, h->hd_psi, h->g, h->d_twx, h->d_tpx, h->scale, st);
     if (want_res) {
       x.acc_r = h->d_acc + 2;
       launch_fftx_fwd(x, true, h->g, h->d_twx, h->d_tpx, h->d_spec, st);  // residual (spectrum is scratch)
-      int rc = read_rel_residual(h, 2, rel);
-      if (rc) return rc;
+      return read_rel_residual(h, 2, rel);
     }
     return TBFP_OK;
   }
-  float2 *sp = reinterpret_cast<float2 *>(h->d_spec);
-  auto spectral32 = [&]() {
-    launch_fftz(sp, h->g, h->d_tpz32, false, st);
-    launch_tridiag(sp, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, st);
-    launch_fftz(sp, h->g, h->d_tpz32, true, st);
-  };
-  launch_fftx_fwd(x, false, h->g, h->d_twx32, h->d_tpx32, sp, st);
-  spectral32();
-  launch_fftx_inv(sp, psi, h->Lpsi, h->hd_psi, h->g, h->d_twx32, h->d_tpx32, h->scale, false, st);
-  for (int it = 0;; ++it) {
-    const int slot = 2 + (it < 60 ? it : 61);
-    x.acc_r = h->d_acc + slot;
-    launch_fftx_fwd(x, true, h->g, h->d_twx32, h->d_tpx32, sp, st);  // r of the current psi, transformed
-    int rc = read_rel_residual(h, slot, rel);
-    if (rc) return rc;
-    if (*rel <= h->tol) return TBFP_OK;
-    if (*iters >= h->max_iter) return TBFP_ENOTCONVERGED;
-    spectral32();
-    launch_fftx_inv(sp, psi, h->Lpsi, h->hd_psi, h->g, h->d_twx32, h->d_tpx32, h->scale, true, st);
-    ++*iters;
+  int rc = mixed_solve(h, s, psi, dscale, st);
+  if (rc) return rc;
+  if (!read) {
+    *iters = -1;  // not read back (asynchronous call)
+    return TBFP_OK;
   }
+  return read_mixed(h, iters, rel, nullptr);
 }
 
 bool aliased(const void *a, const void *b) { return a == b; }
@@ -394,6 +561,7 @@ int device_projection(tbfp_handle *h, const double *uxi, const double *uyi, cons
   launch_rhs(ra, st, h->g, h->d_s, h->Lpsi, s);
   int iters = 1, solve_rc = TBFP_OK;
   double rel = -1.0;
+  const bool read = stats != nullptr || !(h->flags & TBFP_FLAG_ASYNC);
   if (h->precision == TBFP_FP64 && !(h->flags & TBFP_FLAG_RESIDUAL)) {
     launch_fftx_fwd_from_s(h->d_s, h->Lpsi, h->g, h->d_twx, h->d_tpx, h->d_spec, s);
     mark(2);
@@ -408,7 +576,8 @@ int device_projection(tbfp_handle *h, const double *uxi, const double *uyi, cons
   } else {  // iterative or checked solve: its passes are timed as one stage (TRIDIAG)
     mark(2);
     mark(3);
-    solve_rc = device_solve(h, h->d_s, psi, &iters, &rel);
+    // the mixed loop also stops on max|div u| = alpha*dt/rho0 * max|s - L psi| <= tol
+    solve_rc = device_solve(h, h->d_s, psi, alpha * dt / rho0, false, &iters, &rel);
     if (solve_rc < 0) return solve_rc;
     mark(4);
     mark(5);
@@ -427,36 +596,82 @@ int device_projection(tbfp_handle *h, const double *uxi, const double *uyi, cons
     mark(8);
   }
   TBFP_CK(h, cudaEventRecord(h->ev1, s));
-  if (stats) {
+  tbfp_stats out{};
+  out.iterations = iters;
+  out.rel_residual = rel;
+  out.max_div = -1.0;
+  out.cont_err = -1.0;
+  if (read) {  // one read-back: max|div u| (NaN-propagating) and the mixed loop's outcome
     unsigned long long bits = 0;
-    TBFP_CK(h, cudaMemcpyAsync(&bits, h->d_maxdiv, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
-    TBFP_CK(h, cudaStreamSynchronize(h->stream));
+    MixedCtl c{};
+    TBFP_CK(h, cudaMemcpyAsync(&bits, h->d_maxdiv, sizeof(bits), cudaMemcpyDeviceToHost, s));
+    if (h->precision == TBFP_MIXED) TBFP_CK(h, cudaMemcpyAsync(&c, h->d_ctl, sizeof(c), cudaMemcpyDeviceToHost, s));
+    TBFP_CK(h, cudaStreamSynchronize(s));
     double md;
     std::memcpy(&md, &bits, sizeof(md));
+    out.max_div = md;
+    out.cont_err = md * dt;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-    stats->iterations = iters;
-    stats->rel_residual = rel;
-    stats->max_div = md;
-    stats->cont_err = md * dt;
-    stats->ms_device = ms;
+    out.ms_device = ms;
     for (int i = 0; i < TBFP_NSTAGES; ++i) {
       float m = 0.f;
       if (timing) cudaEventElapsedTime(&m, h->evs[i], h->evs[i + 1]);
-      stats->ms_stage[i] = m;
+      out.ms_stage[i] = m;
     }
+    if (h->precision == TBFP_MIXED) {
+      out.iterations = c.iters;
+      out.rel_residual = c.rel;
+      solve_rc = c.status;
+    }
+    if (!std::isfinite(md) || solve_rc == TBFP_ENONFINITE) {
+      h->last = out;
+      if (stats) *stats = out;
+      return set_err(h, TBFP_ENONFINITE,
+                     "tbfp_projection: non-finite max|div u| or residual (NaN or Inf in u*, rho, psi^n or psi^n-1)");
+    }
+  } else if (h->precision == TBFP_MIXED) {
+    out.iterations = -1;  // the loop's outcome is on the device; not read back
   }
-  if (stats) {
-    h->last = *stats;
-  } else {
-    h->last = tbfp_stats{};
-    h->last.iterations = iters;
-    h->last.rel_residual = rel;
-    h->last.max_div = -1.0;
-    h->last.cont_err = -1.0;
-  }
+  h->last = out;
+  if (stats) *stats = out;
   const int frc = finish(h, "tbfp_projection");
   return frc ? frc : solve_rc;
+}
+
+// solveFPS body of tbfp_solve_fps[_dev]; with read the call waits for the
+// device and reads back the outcome: the mixed loop's status, or for the FP64
+// path one pressure value, which a NaN or Inf anywhere in s reaches (every
+// transform output depends on every input, and every unknown of a tridiagonal
+// system on every right-hand side entry).
+int solve_fps_core(tbfp_handle *h, const double *s, double *psi, bool read) {
+  int rc = check_ptrs(h, {s, psi});
+  if (rc) return rc;
+  if (h->slab) return set_err(h, TBFP_EINVAL, "tbfp_solve_fps: a slab handle solves with tbfp_slab_*");
+  cudaSetDevice(h->device);
+  TBFP_CK(h, cudaEventRecord(h->ev0, h->stream));
+  int iters = 1;
+  double rel = -1.0;
+  const int src = device_solve(h, s, psi, 0.0, read, &iters, &rel);
+  if (src < 0) return src;
+  TBFP_CK(h, cudaEventRecord(h->ev1, h->stream));
+  h->last = tbfp_stats{};
+  h->last.iterations = iters;
+  h->last.rel_residual = rel;
+  h->last.max_div = -1.0;
+  h->last.cont_err = -1.0;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_err(h, e, "tbfp_solve_fps");
+  if (read) {
+    double p111 = 0.0;
+    TBFP_CK(h, cudaMemcpyAsync(&p111, psi + at(h->Lpsi, 1, 1, 1), sizeof(double), cudaMemcpyDeviceToHost,
+                               h->stream));
+    TBFP_CK(h, cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) h->last.ms_device = ms;
+    if (!std::isfinite(p111)) return set_err(h, TBFP_ENONFINITE, "tbfp_solve_fps: non-finite pressure (NaN or Inf in s)");
+  }
+  return src;
 }
 
 }  // namespace
@@ -475,6 +690,8 @@ const char *tbfp_strerror(int status) {
     case TBFP_ENOMEM: return "device memory allocation failed";
     case TBFP_EUNSUPPORTED: return "size or feature not supported";
     case TBFP_ENODEVICE: return "no usable CUDA device";
+    case TBFP_ENONFINITE: return "non-finite value (NaN or Inf) in a residual or a result";
+    case TBFP_ESINGULAR: return "singular coarsest-level system";
     default: return "unknown status";
   }
 }
@@ -497,6 +714,10 @@ int tbfp_destroy(tbfp_handle *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   delete h->mg;
   h->mg = nullptr;
+  for (MixedGraph &m : h->mgr)
+    if (m.exec) cudaGraphExecDestroy(m.exec);
+  if (h->cap) cudaStreamDestroy(h->cap);
+  if (h->cap_body) cudaStreamDestroy(h->cap_body);
   for (void *p : h->allocs) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -696,7 +917,7 @@ int create_impl(const tbfp_desc *d, const SlabSpec *sl, tbfp_handle **out) {
     return fail(rc);
   if ((rc = dev_alloc(h, &h->d_spec, (size_t)h->nkx * h->R)) || (rc = dev_alloc(h, &h->d_irho, h->n_rho)) ||
       (rc = dev_alloc(h, &h->d_s, h->n_psi)) ||
-      (rc = dev_alloc(h, &h->d_maxdiv, 1)))
+      (rc = dev_alloc(h, &h->d_maxdiv, 1)) || (rc = dev_alloc(h, &h->d_ctl, 1)))
     return fail(rc);
 
   GridK &g = h->g;
@@ -773,28 +994,7 @@ int tbfp_slab_inverse_x(tbfp_handle *h, const double *spec_z, double *psi) {
 
 // ---------------------------------------------------------------------------
 int tbfp_solve_fps_dev(tbfp_handle *h, const double *s, double *psi) {
-  int rc = check_ptrs(h, {s, psi});
-  if (rc) return rc;
-  if (h->slab) return set_err(h, TBFP_EINVAL, "tbfp_solve_fps: a slab handle solves with tbfp_slab_*");
-  cudaSetDevice(h->device);
-  TBFP_CK(h, cudaEventRecord(h->ev0, h->stream));
-  int iters = 1;
-  double rel = -1.0;
-  const int src = device_solve(h, s, psi, &iters, &rel);
-  if (src < 0) return src;
-  TBFP_CK(h, cudaEventRecord(h->ev1, h->stream));
-  h->last = tbfp_stats{};
-  h->last.iterations = iters;
-  h->last.rel_residual = rel;
-  h->last.max_div = -1.0;
-  h->last.cont_err = -1.0;
-  const int frc = finish(h, "tbfp_solve_fps");
-  if (frc) return frc;
-  if (!(h->flags & TBFP_FLAG_ASYNC)) {
-    float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) h->last.ms_device = ms;
-  }
-  return src;
+  return solve_fps_core(h, s, psi, !(h && (h->flags & TBFP_FLAG_ASYNC)));
 }
 
 int tbfp_solve_fps(tbfp_handle *h, const double *s, double *psi) {
@@ -805,10 +1005,7 @@ int tbfp_solve_fps(tbfp_handle *h, const double *s, double *psi) {
   if ((rc = h2d(h, h->h_s, s, h->n_psi))) return rc;
   // keep the caller's untouched entries (deep y ghost layers) as they are
   if (h->hd_psi > 1 && (rc = h2d(h, h->h_psi, psi, h->n_psi))) return rc;
-  const unsigned fl = h->flags;
-  h->flags |= TBFP_FLAG_ASYNC;
-  const int src = tbfp_solve_fps_dev(h, h->h_s, h->h_psi);
-  h->flags = fl;
+  const int src = solve_fps_core(h, h->h_s, h->h_psi, true);
   if (src < 0) return src;
   if ((rc = d2h(h, psi, h->h_psi, h->n_psi))) return rc;
   TBFP_CK(h, cudaStreamSynchronize(h->stream));
@@ -1620,7 +1817,7 @@ int tbfp_ensemble_create(int n, const tbfp_desc *descs, int nstreams, tbfp_ensem
     d.device = e->device;
     d.stream = e->streams[i % ns];
     d.flags = (d.flags | TBFP_FLAG_ASYNC) & ~TBFP_FLAG_TIMING;
-    if (d.precision != TBFP_FP64 || (d.flags & TBFP_FLAG_RESIDUAL)) e->graphable = false;
+    if (d.flags & TBFP_FLAG_RESIDUAL) e->graphable = false;  // reads its residual back on the host
     tbfp_handle *h = nullptr;
     const int rc = tbfp_create(&d, &h);
     if (rc < 0) {
@@ -1714,6 +1911,15 @@ int tbfp_ensemble_projection_dev(tbfp_ensemble *e, const tbfp_member_io *io, dou
       stats[i] = e->h[i]->last;
       stats[i].max_div = md;
       stats[i].cont_err = md * dt;
+      if (e->h[i]->precision == TBFP_MIXED) {
+        const int mrc = read_mixed(e->h[i], &stats[i].iterations, &stats[i].rel_residual, nullptr);
+        if (mrc < 0) return set_err(nullptr, mrc, "tbfp_ensemble_projection: member " + std::to_string(i) + ": " +
+                                                       e->h[i]->err);
+        if (mrc > rc) rc = mrc;
+      }
+      if (!std::isfinite(md))
+        return set_err(nullptr, TBFP_ENONFINITE,
+                       "tbfp_ensemble_projection: member " + std::to_string(i) + ": non-finite max|div u|");
     }
   }
   return rc;

@@ -53,13 +53,13 @@ __device__ __forceinline__ double corr_z(const CorrArgs &a, const GridK &g, int 
 
 __device__ __forceinline__ void block_max_atomic(double v, unsigned long long *out) {
   __shared__ double red[32];
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = nanmax_nonneg(v, __shfl_xor_sync(0xffffffffu, v, o));
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   if (l == 0) red[w] = v;
   __syncthreads();
   if (w == 0) {
     v = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = nanmax_nonneg(v, __shfl_xor_sync(0xffffffffu, v, o));
     if (l == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
   }
 }
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(128, 8) k_correct_div(CorrArgs a, GridK g, uns
       double dv = (uxp - uxm) * idx;
       dv = dv + (uyp - uym) * g.idyf[j - 1];
       dv = dv + (uzp - uzq) * idz;
-      vmax = fmax(vmax, fabs(dv));
+      vmax = nanmax_nonneg(vmax, dv);
     }
     uym = uyp;
     psc = psy;
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(128) k_div(const double *__restrict__ ux, cons
       double dv = (ux[at(Lux, i, j, k)] - ux[at(Lux, i - 1, j, k)]) * idx;
       dv = dv + (uy[at(Luy, i, j, k)] - uy[at(Luy, i, j - 1, k)]) * g.idyf[j - 1];
       dv = dv + (uz[at(Luz, i, j, k)] - uz[at(Luz, i, j, k - 1)]) * idz;
-      vmax = fmax(vmax, fabs(dv));
+      vmax = nanmax_nonneg(vmax, dv);
     }
   }
   block_max_atomic(vmax, maxdiv);

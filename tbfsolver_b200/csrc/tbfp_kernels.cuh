@@ -66,6 +66,9 @@ struct CorrArgs {
 //     solveFPS's operator, with c = acc[0] * ctop_scale (the incompatible part
 //     of s, which the pinned (0,0) solve leaves on the top wall, so that the
 //     residual of the FP64 solution is zero), and acc_r[0] += sum r^2.
+//   With acc_r, the residual pass also folds max|s - L psi| (= max|r + c [j == ny]|,
+//   the quantity that bounds the divergence the correction leaves) into acc_r[1]
+//   as the bits of a non-negative double (a NaN wins).
 struct XSrc {
   const double *s;
   Lay Ls;
@@ -75,6 +78,24 @@ struct XSrc {
   double idx2, idz2;            // 1/dx^2, 1/dz^2 of the uniform x and z spacing
   double ctop_scale;            // 1/(dyf(ny) nx nz)
   double *acc, *acc_r;
+};
+
+// Device-side control of the mixed-precision refinement loop.  Per call the
+// host sets tol, dtol, dscale and max_iter (launch_mixed_params, which also
+// clears the sums); after every residual pass launch_mixed_decide evaluates
+//   rel = ||r||_2/||s||_2 from acc[1] and acc_r[0],  div = dscale * max|s - L psi|
+// and stops the loop (done = 1) when rel <= tol and, with dscale > 0, div <= dtol
+// (status TBFP_OK); when the sweeps reach max_iter (status TBFP_ENOTCONVERGED);
+// or when rel or div is not finite (status TBFP_ENONFINITE).  For the
+// projection dscale = alpha*dt/rho0, because the corrected velocity has
+// div u = alpha*dt/rho0 * (s - L psi) cell by cell, so div is max|div u|.
+struct MixedCtl {
+  double tol, dtol, dscale;  // set per call
+  double rel, div;           // of the last residual pass
+  int max_iter;              // set per call
+  int iters;                 // FP32 solves so far
+  int status;                // TBFP_OK, TBFP_ENOTCONVERGED or TBFP_ENONFINITE once done
+  int done;
 };
 
 // Transform lengths with a compiled kernel (nx/2 and nz): 2^a and 3*2^a, 4..512.
@@ -108,6 +129,19 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait_group() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Maximum of two non-negative values that lets a NaN win (fmax would drop it,
+// and a NaN must reach the host): the bit patterns of non-negative doubles
+// order like their values, and a NaN with its sign cleared lies above +Inf.
+// The sign is cleared on the bits, not by fabs: a NaN that the device makes
+// (Inf - Inf, 0 * Inf) can keep its sign bit through fabs, and a negative
+// pattern would lose to every finite value.
+__device__ __forceinline__ double abs_bits(double v) {
+  return __longlong_as_double(__double_as_longlong(v) & 0x7fffffffffffffffLL);
+}
+__device__ __forceinline__ double nanmax_nonneg(double a, double b) {
+  return __longlong_as_double(max(__double_as_longlong(abs_bits(a)), __double_as_longlong(abs_bits(b))));
 }
 
 constexpr int kNT = 256;  // threads per CTA of the transform kernels (8 warps)
@@ -200,6 +234,14 @@ void launch_fftx_fwd(const XSrc &src, bool residual, const GridK &g, const doubl
                      double2 *spec, cudaStream_t st);
 void launch_fftx_fwd(const XSrc &src, bool residual, const GridK &g, const float2 *twx, const float2 *tpx,
                      float2 *spec, cudaStream_t st);
+// Mixed-precision loop control (MixedCtl): params clears acc[0..3] and starts
+// the count at one solve; decide reads acc[1] (sum s^2) and acc_r[0..1], writes
+// ctl and clears acc_r for the next pass; with cond it also sets the WHILE
+// condition of the graph it runs in (1: run another sweep).
+void launch_mixed_params(MixedCtl *ctl, double *acc, double tol, double dtol, double dscale, int max_iter,
+                         cudaStream_t st);
+void launch_mixed_decide(MixedCtl *ctl, const double *acc, double *acc_r, cudaGraphConditionalHandle cond,
+                         bool use_cond, cudaStream_t st);
 void launch_correct_div(const CorrArgs &ca, bool has_st, const GridK &g, unsigned long long *maxdiv,
                         cudaStream_t st);
 void launch_correct_inplace(const CorrArgs &ca, bool has_st, const GridK &g, cudaStream_t st);

@@ -884,32 +884,47 @@ struct Run {
     if (l == 0 && hpost) k_sub_mean<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, post);
   }
 
-  // ||q - L p|| / ||q|| at the finest level (computeResiduals' res)
-  double fine_residual() {
+  // ||q - L p|| / ||q|| at the finest level (computeResiduals' res) into *res;
+  // a CUDA error returns TBFP_ECUDA with its text in *err.
+  int fine_residual(double *res, std::string *err) {
     auto &L = m.lv[0];
     cudaMemsetAsync(m.sc + 6, 0, 2 * sizeof(double), st);
     k_mg_residual<<<wgrid(L.nx, L.ny, L.nz, kMgJ), kWalkX, 0, st>>>(L.L, L.p, L.q, L.beta, L.res, m.sc + 6);
     double v[2] = {0.0, 0.0};
     cudaMemcpyAsync(v, m.sc + 6, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
-    return std::sqrt(v[0]) / (std::sqrt(v[1]) + 1e-300);
+    const cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      *err = std::string("tbfp_pcg_solve (multigrid residual): ") + cudaGetErrorString(e);
+      return TBFP_ECUDA;
+    }
+    *res = std::sqrt(v[0]) / (std::sqrt(v[1]) + 1e-300);
+    return TBFP_OK;
   }
 
   // solveMG (multiGrid.f90:165-182): p starts at 0, V-cycles while res > tol_mg.
   // Each V-cycle is one launch of a CUDA graph captured once per hierarchy
   // (its buffers never move); without a graph the kernels are launched one by one.
-  int solve_mg() {
+  // Adds the V-cycles to *cycles.  A non-finite residual (the FP32 hierarchy
+  // overflowed, or a NaN reached it) is a hard error.
+  int solve_mg(int *cycles, std::string *err) {
     auto &L = m.lv[0];
     k_fill<<<nblk_grid(L.n), kMgThreads, 0, st>>>(L.p, L.n, 0.0f);
-    double res = fine_residual();
+    double res = 0.0;
+    int rc = fine_residual(&res, err);
     int it = 0;
-    while (it < m.prm.max_iter_mg && res > m.prm.tol_mg) {
+    while (rc == TBFP_OK && std::isfinite(res) && it < m.prm.max_iter_mg && res > m.prm.tol_mg) {
       ++it;
       if (m.vgraph) cudaGraphLaunch(m.vgraph, st);
       else vcycle(0);
-      res = fine_residual();
+      rc = fine_residual(&res, err);
     }
-    return it;
+    *cycles += it;
+    if (rc) return rc;
+    if (!std::isfinite(res)) {
+      *err = "tbfp_pcg_solve: non-finite multigrid residual (NaN or Inf in q, beta or the iterate)";
+      return TBFP_ENONFINITE;
+    }
+    return TBFP_OK;
   }
 
   void capture() {
@@ -970,7 +985,8 @@ int MgSolver::solve(double *psi, Lay Lp, int hd_psi, const double *beta, Lay Lb,
   // r = q - L psi (psi: the initial guess), z = MG(r), d = z
   cudaMemsetAsync(m.sc, 0, 16 * sizeof(double), st);
   k_pcg_init<<<wgrid(m.nx, m.ny, m.nz, kMgJ), kWalkX, 0, st>>>(F, psi, Lp, q, Lq, m.r, m.lv[0].q, m.sc + 4);
-  *mg_cycles += run.solve_mg();
+  int rc = run.solve_mg(mg_cycles, err);
+  if (rc) return rc;
   k_pcg_dot<<<nblk_grid(m.n), kMgThreads, 0, st>>>(m.r, m.lv[0].p, m.n, m.sc + 0);
   k_pcg_dir<<<nblk_grid(m.n), kMgThreads, 0, st>>>(m.lv[0].p, m.d, m.n, m.sc, 1);
   double nrm[2];
@@ -984,7 +1000,7 @@ int MgSolver::solve(double *psi, Lay Lp, int hd_psi, const double *beta, Lay Lb,
   }
   if (fail) {
     *err = "tbfp_pcg_solve: singular coarsest-level system";
-    return TBFP_ECUDA;
+    return TBFP_ESINGULAR;
   }
   const double qn = std::sqrt(nrm[0] + 1e-300);
   double rr = nrm[1];
@@ -992,13 +1008,18 @@ int MgSolver::solve(double *psi, Lay Lp, int hd_psi, const double *beta, Lay Lb,
   double res = std::sqrt(rr) / qn;
   while (true) {
     res = std::sqrt(rr) / qn;
+    if (!std::isfinite(res)) {  // a NaN would otherwise fail every comparison and read as converged
+      *err = "tbfp_pcg_solve: non-finite PCG residual (NaN or Inf in q, beta or the initial guess)";
+      return TBFP_ENONFINITE;
+    }
     if (it == m.prm.max_iter_pcg || !(res > m.prm.tol_pcg)) break;
     ++it;
     cudaMemsetAsync(m.sc + 1, 0, sizeof(double), st);
     k_pcg_qv<<<wgrid(m.nx, m.ny, m.nz, kMgJ), kWalkX, 0, st>>>(F, m.d, m.qv, m.sc + 1);
     cudaMemsetAsync(m.sc + 5, 0, sizeof(double), st);
     k_pcg_update<<<wgrid(m.nx, m.ny, m.nz, kMgJ), kWalkX, 0, st>>>(F, psi, Lp, m.d, m.qv, m.r, m.lv[0].q, m.sc, m.sc + 5);
-    *mg_cycles += run.solve_mg();
+    rc = run.solve_mg(mg_cycles, err);
+    if (rc) return rc;
     cudaMemcpyAsync(m.sc + 3, m.sc + 0, sizeof(double), cudaMemcpyDeviceToDevice, st);  // deltaN_old
     cudaMemsetAsync(m.sc + 2, 0, sizeof(double), st);
     k_pcg_dot<<<nblk_grid(m.n), kMgThreads, 0, st>>>(m.r, m.lv[0].p, m.n, m.sc + 2);

@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_fwd(XSrc src, 
   extern __shared__ __align__(16) unsigned char smx[];
   V *sm = reinterpret_cast<V *>(smx);
   V *tw = sm + TJ * LD;
-  __shared__ double red[kNW][2];
+  __shared__ double red[kNW][3];
   for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = tpx[t];
   const int r0 = blockIdx.x << LOGTJ;
   const int nrows = min(TJ, (int)g.R - r0);
@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_fwd(XSrc src, 
   T *wsr = reinterpret_cast<T *>(wsm);
   const bool sums = (MODE == 0) ? src.acc != nullptr : true;
   const double ctop = (MODE == 1) ? src.acc[0] * src.ctop_scale : 0.0;
-  double sum0 = 0.0, sum1 = 0.0;
+  double sum0 = 0.0, sum1 = 0.0, vmax = 0.0;
 
 #pragma unroll
   for (int rl = 0; rl < RPW; ++rl) {
@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_fwd(XSrc src, 
                                apj * (p[i + sj] - p0) + (p[i + sk] + p[i - sk] - 2.0 * p0) * src.idz2;
             const double v = (srow[i] - cj) - lap;
             sum1 += v * v;
+            vmax = nanmax_nonneg(vmax, v + cj);
             dst[2 * pad8(ii >> 1) + (ii & 1)] = (T)v;
           }
         }
@@ -106,24 +107,28 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_fwd(XSrc src, 
     for (int o = 16; o > 0; o >>= 1) {
       sum0 += __shfl_xor_sync(0xffffffffu, sum0, o);
       sum1 += __shfl_xor_sync(0xffffffffu, sum1, o);
+      if constexpr (MODE == 1) vmax = nanmax_nonneg(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
     }
     if (lane == 0) {
       red[warp][0] = sum0;
       red[warp][1] = sum1;
+      red[warp][2] = vmax;
     }
   }
   __syncthreads();  // twiddle table, rows and partial sums in place
   if (sums && threadIdx.x == 0) {
-    double a0 = 0.0, a1 = 0.0;
+    double a0 = 0.0, a1 = 0.0, m = 0.0;
     for (int w = 0; w < kNW; ++w) {
       a0 += red[w][0];
       a1 += red[w][1];
+      m = nanmax_nonneg(m, red[w][2]);
     }
     if constexpr (MODE == 0) {
       atomicAdd(src.acc, a0);
       atomicAdd(src.acc + 1, a1);
     } else {
       atomicAdd(src.acc_r, a1);
+      atomicMax(reinterpret_cast<unsigned long long *>(src.acc_r + 1), (unsigned long long)__double_as_longlong(m));
     }
   }
   fft_warp<V, M, LOGRPW, 1, LD, false>(wsm, lane, tw);
@@ -203,6 +208,55 @@ void launch_fftx_fwd(const XSrc &src, bool residual, const GridK &g, const float
                      float2 *spec, cudaStream_t st) {
   if (residual) launch_x_fwd_t<float2, 1>(src, g, twx, tpx, spec, st);
   else launch_x_fwd_t<float2, 0>(src, g, twx, tpx, spec, st);
+}
+
+// ---------------------------------------------------------------------------
+// Device-side control of the mixed-precision refinement (MixedCtl).
+// ---------------------------------------------------------------------------
+__global__ void k_mixed_params(MixedCtl *ctl, double *acc, double tol, double dtol, double dscale, int max_iter) {
+  acc[0] = 0.0;
+  acc[1] = 0.0;
+  acc[2] = 0.0;
+  acc[3] = 0.0;
+  ctl->tol = tol;
+  ctl->dtol = dtol;
+  ctl->dscale = dscale;
+  ctl->max_iter = max_iter;
+  ctl->iters = 1;
+  ctl->rel = -1.0;
+  ctl->div = -1.0;
+  ctl->status = 0;
+  ctl->done = 0;
+}
+
+__global__ void k_mixed_decide(MixedCtl *ctl, const double *acc, double *acc_r, cudaGraphConditionalHandle cond,
+                               int use_cond) {
+  const double ss = acc[1], rr = acc_r[0];
+  const double rel = ss > 0.0 ? sqrt(rr / ss) : sqrt(rr);
+  const double div = ctl->dscale > 0.0 ? ctl->dscale * acc_r[1] : 0.0;
+  acc_r[0] = 0.0;  // the next residual pass accumulates afresh
+  acc_r[1] = 0.0;
+  ctl->rel = rel;
+  ctl->div = ctl->dscale > 0.0 ? div : -1.0;
+  int done = 1;
+  if (!isfinite(rel) || !isfinite(div)) ctl->status = -7;  // TBFP_ENONFINITE
+  else if (rel <= ctl->tol && div <= ctl->dtol) ctl->status = 0;
+  else if (ctl->iters >= ctl->max_iter) ctl->status = 1;  // TBFP_ENOTCONVERGED
+  else {
+    done = 0;
+    ctl->iters += 1;  // the sweep that follows
+  }
+  ctl->done = done;
+  if (use_cond) cudaGraphSetConditional(cond, done ? 0u : 1u);
+}
+
+void launch_mixed_params(MixedCtl *ctl, double *acc, double tol, double dtol, double dscale, int max_iter,
+                         cudaStream_t st) {
+  k_mixed_params<<<1, 1, 0, st>>>(ctl, acc, tol, dtol, dscale, max_iter);
+}
+void launch_mixed_decide(MixedCtl *ctl, const double *acc, double *acc_r, cudaGraphConditionalHandle cond,
+                         bool use_cond, cudaStream_t st) {
+  k_mixed_decide<<<1, 1, 0, st>>>(ctl, acc, acc_r, cond, use_cond ? 1 : 0);
 }
 
 // Split RHS into s on the interior (tbfp_rhs_split and the projection).  Grid

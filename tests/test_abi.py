@@ -42,8 +42,8 @@ def test_library_exports_every_declared_symbol(lib):
 
 def test_version_and_strerror(lib):
     assert lib.tbfp_abi_version() == 1
-    for code in (0, 1, -1, -2, -3, -4, -5, -6):
-        assert lib.tbfp_strerror(code)
+    for code in (0, 1, -1, -2, -3, -4, -5, -6, -7, -8):
+        assert lib.tbfp_strerror(code) != b"unknown status"
     assert lib.tbfp_strerror(12345) == b"unknown status"
 
 

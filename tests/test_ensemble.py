@@ -2,8 +2,13 @@
 sizes projected in one call, through the C ABI, against one projection per
 channel with the single-channel entry point.  The kernels are the same, so
 the FP64 results must agree bit for bit, on the first call (graph capture),
-on a replay, and after the arrays change (re-capture); a mixed-precision
-ensemble (run without a graph) must reach its residual target."""
+on a replay, and after the arrays change (re-capture).  A mixed-precision
+ensemble runs inside the same captured graph, each member's refinement loop a
+conditional node on the device; it must reach its residual and divergence
+targets on the first call and on replays, and agree with single-channel mixed
+calls to 1e-11, well inside the mixed path's own 1e-8 bar against FP64.  They
+do not agree bit for bit: the residual passes sum with atomics in no fixed
+order, and the sum of s dyf sets the top-wall term of the residual.)"""
 import numpy as np
 import pytest
 import torch
@@ -62,14 +67,30 @@ def test_ensemble_matches_single_channel_projections():
                 assert st.max_div == want_st.max_div and st.max_div < 1e-9
 
 
+def _reference_mixed(inp, rho0):
+    eqn = PoissonEqn(inp.grid, inp.spec.rhol, inp.spec.rhog, precision="mixed", tol=1e-10, max_iter=8)
+    psi, pn, pnm1, rho, u, uo = _io(inp)
+    st = eqn.projection(psi, pn, pnm1, rho, u, inp.dt, inp.alpha, u_out=uo)
+    eqn.close()
+    return st, psi, uo
+
+
 def test_mixed_ensemble_reaches_tolerance():
-    specs = [synth.small_spec(64, 48, 32, nbubbles=2, rhog=0.05), synth.small_spec(48, 40, 24, nbubbles=1, rhog=0.05)]
+    specs = [synth.small_spec(64, 48, 32, nbubbles=2, rhog=0.05), synth.small_spec(48, 40, 24, nbubbles=1, rhog=0.05),
+             synth.small_spec(96, 64, 48, nbubbles=3, rhog=0.05)]
     inps = _members(specs, 5)
     with Ensemble([i.grid for i in inps], nstreams=2, precision="mixed", tol=1e-10) as ens:
         members = [_io(i) for i in inps]
-        stats = ens.projection(members, inps[0].dt, inps[0].alpha, 0.05)
-    for inp, m, st in zip(inps, members, stats):
-        assert st.rel_residual <= 1e-10 and st.iterations >= 2
-        _, want_psi, _ = _reference(inp, 0.05)
-        a, b = m[0].a.cpu().numpy(), want_psi.a.cpu().numpy()
-        assert np.max(np.abs(a - b)) / np.max(np.abs(b)) < 1e-8
+        for rep in range(3):  # capture, then replays of the graph with its conditional loops
+            for m in members:
+                m[0].a.zero_()
+            stats = ens.projection(members, inps[0].dt, inps[0].alpha, 0.05)
+            for inp, m, st in zip(inps, members, stats):
+                assert st.rel_residual <= 1e-10 and st.iterations >= 2 and st.max_div <= 1e-10, (rep, st.iterations)
+                want_st, want_psi, want_u = _reference_mixed(inp, 0.05)
+                assert st.iterations == want_st.iterations
+                a, b = m[0].a.cpu().numpy(), want_psi.a.cpu().numpy()
+                assert np.max(np.abs(a - b)) / np.max(np.abs(b)) < 1e-11
+                _, p64, _ = _reference(inp, 0.05)
+                c = p64.a.cpu().numpy()
+                assert np.max(np.abs(a - c)) / np.max(np.abs(c)) < 1e-8

@@ -9,7 +9,13 @@ import pytest
 from tbfsolver_b200 import io
 from tbfsolver_b200.fields import Field, VField
 
-SPECS = "/root/reference/channel_18/specs"
+# The reference's own example case (channel_18/specs), where a checkout of the
+# reference is available: TBFP_REFERENCE_DIR names its root.  Tests that read it
+# are skipped without it.
+_REF = os.environ.get("TBFP_REFERENCE_DIR", "")
+SPECS = os.path.join(_REF, "channel_18", "specs") if _REF else ""
+needs_specs = pytest.mark.skipif(not (SPECS and os.path.isdir(SPECS)),
+                                 reason="set TBFP_REFERENCE_DIR to a checkout of the reference")
 
 
 @pytest.mark.parametrize("kind", ["cl", "sx", "sy", "sz"])
@@ -88,7 +94,7 @@ def test_parameter_file_reader(tmp_path):
         p.read_int("ny")
 
 
-@pytest.mark.skipif(not os.path.isdir(SPECS), reason="reference case not present")
+@needs_specs
 def test_reads_the_reference_case_specs():
     mesh = io.ParFile("mesh", SPECS)
     assert (mesh.read_int("nx"), mesh.read_int("ny"), mesh.read_int("nz")) == (192, 160, 96)
