@@ -366,6 +366,244 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same solve with the rows per lane T a compile-time constant (T <= 16).
+// The system is padded to 32*T rows: a row i >= ny is the decoupled equation
+// x_i = 0 (its off-diagonals are zero and its diagonal is one), so every lane
+// eliminates exactly T rows and the loops unroll with no per-lane guard; the
+// off-diagonals of the lane's rows are loaded before the elimination starts.
+// The reciprocals on the elimination's dependent chain are Newton-Raphson
+// iterations (y <- y + y(1 - x y), twice) from the PTX rcp.approx.ftz.f64
+// seed: fewer dependent instructions than a division, within an ulp of 1/x
+// (the arguments are bounded away from zero: |lam - am - ap| >= am + ap and the
+// reduced diagonals stay near one).  The off-diagonals are read inside the
+// unrolled elimination (L1-resident tables), so only the elimination
+// coefficients of the lane's rows stay in registers.  The cyclic reduction takes one reciprocal
+// per lane and level (1/B, exchanged with the neighbours) in place of two
+// divisions.  The singular (0,0) system keeps the serial pinned path.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+template <int T>
+__host__ __device__ constexpr int tri_min_blocks() {
+  return T <= 6 ? 6 : (T <= 8 ? 4 : 3);
+}
+
+template <typename V, int T>
+__global__ void __launch_bounds__(kWPB * 32, tri_min_blocks<T>()) k_tridiag_t(
+    V *__restrict__ spec, GridK g, const double *__restrict__ lamx, const double *__restrict__ lamz,
+    const double *__restrict__ am, const double *__restrict__ ap, const double *__restrict__ dyf, double mean_c,
+    double nxnz) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int W = 33 * T;
+  const int ny = g.ny, nz = g.nz;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *d0 = reinterpret_cast<double2 *>(smraw) + warp * 2 * W;
+  double2 *d1 = d0 + W;
+  const int nzh = nz / 2 + 1;
+  const unsigned q = blockIdx.x * kWPB + warp;
+  if (q >= (unsigned)(g.nkx * nzh)) return;  // whole warp leaves; no block-level barrier follows
+  const int kx = (int)(q / (unsigned)nzh), kz = (int)(q - (unsigned)kx * nzh);
+  const int kz2 = (kz == 0) ? 0 : nz - kz;
+  const bool two = kz2 != kz;
+  V *S0 = spec + (long)kx * g.R + (long)kz * ny;
+  V *S1 = spec + (long)kx * g.R + (long)kz2 * ny;
+  using VT = decltype(V::x);
+  auto st = [](double2 v) { return mk<V>((VT)v.x, (VT)v.y); };
+  // row e lives in lane e / T at slot (e mod T)*33 + lane; padding rows are zero
+#pragma unroll
+  for (int c = 0; c < T; ++c) {
+    const int e = lane + 32 * c;
+    const int l = e / T, sl = (e - l * T) * 33 + l;
+    if (e < ny) {
+      if constexpr (sizeof(V) == sizeof(double2)) {
+        cp_async16(d0 + sl, S0 + e);
+        if (two) cp_async16(d1 + sl, S1 + e);
+      } else {
+        const V v0 = S0[e];
+        d0[sl] = mk<double2>((double)v0.x, (double)v0.y);
+        if (two) {
+          const V v1 = S1[e];
+          d1[sl] = mk<double2>((double)v1.x, (double)v1.y);
+        }
+      }
+    } else {
+      d0[sl] = mk<double2>(0.0, 0.0);
+      d1[sl] = mk<double2>(0.0, 0.0);
+    }
+  }
+  const double lam = lamx[kx + g.kx0] + lamz[kz];
+  const bool pin = (kx + g.kx0 == 0 && kz == 0);
+  const int s0 = lane * T;
+  if constexpr (sizeof(V) == sizeof(double2)) cp_async_wait_all();
+  __syncwarp();
+
+  if (pin) {  // single system: pinned serial Thomas (as k_tridiag), factors in d1
+    double *cpin = reinterpret_cast<double *>(d1);
+    auto slot = [&](int e) { return (e % T) * 33 + e / T; };
+    if (lane == 0) {
+      double ct_p = 0.0;
+      double2 dt_p = mk<double2>(0.0, 0.0);
+      for (int e = 0; e < ny; ++e) {
+        const int sl = slot(e);
+        double ct = 0.0;
+        double2 dt = mk<double2>(0.0, 0.0);
+        if (e < ny - 1) {
+          const double a = am[e], c = ap[e];
+          const double2 f = d0[sl];
+          const double gi = 1.0 / ((lam - a - c) - a * ct_p);
+          ct = c * gi;
+          dt = mk<double2>((f.x - a * dt_p.x) * gi, (f.y - a * dt_p.y) * gi);
+        }
+        cpin[sl] = ct;
+        d0[sl] = dt;
+        ct_p = ct;
+        dt_p = dt;
+      }
+      double2 xn = d0[slot(ny - 1)];
+      for (int e = ny - 2; e >= 0; --e) {
+        const int sl = slot(e);
+        const double c = cpin[sl];
+        xn = mk<double2>(d0[sl].x - c * xn.x, d0[sl].y - c * xn.y);
+        d0[sl] = xn;
+      }
+    }
+    __syncwarp();
+    double sx = 0.0, sy = 0.0;
+    for (int e = lane; e < ny; e += 32) {
+      const double2 v = d0[slot(e)];
+      sx += v.x * dyf[e];
+      sy += v.y * dyf[e];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sx += __shfl_xor_sync(0xffffffffu, sx, o);
+      sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    const double subx = sx * mean_c * nxnz, suby = sy * mean_c * nxnz;
+    for (int e = lane; e < ny; e += 32) {
+      const int sl = slot(e);
+      S0[e] = st(mk<double2>(d0[sl].x - subx, d0[sl].y - suby));
+    }
+    return;
+  }
+
+  // forward elimination within the lane's block (padding rows: diagonal one)
+  double at_r[T], ct_r[T];
+  double at_p = -1.0, ct_p = 0.0;
+  double2 p0 = mk<double2>(0.0, 0.0), p1 = mk<double2>(0.0, 0.0);
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    const bool real = s0 + t < ny;  // off-diagonals zero, diagonal one on padding rows
+    const double a = real ? am[s0 + t] : 0.0, c = real ? ap[s0 + t] : 0.0;
+    const double dg = real ? lam : 1.0;
+    const int sl = t * 33 + lane;
+    const double gi = rcp_nr((dg - a - c) - a * ct_p);
+    const double2 f0 = d0[sl], f1 = d1[sl];
+    p0 = mk<double2>((f0.x - a * p0.x) * gi, (f0.y - a * p0.y) * gi);
+    p1 = mk<double2>((f1.x - a * p1.x) * gi, (f1.y - a * p1.y) * gi);
+    d0[sl] = p0;
+    d1[sl] = p1;
+    at_p = -a * at_p * gi;
+    ct_p = c * gi;
+    at_r[t] = at_p;
+    ct_r[t] = ct_p;
+  }
+  // running backward pass: x_s = hd - ha x_{s-1} - hc x_e
+  double ha = 0.0, hc = -1.0;
+  double2 h0 = mk<double2>(0.0, 0.0), h1 = mk<double2>(0.0, 0.0);
+  if constexpr (T >= 2) {
+    h0 = d0[(T - 2) * 33 + lane];
+    h1 = d1[(T - 2) * 33 + lane];
+    ha = at_r[T - 2];
+    hc = ct_r[T - 2];
+#pragma unroll
+    for (int t = T - 3; t >= 0; --t) {
+      const double2 v0 = d0[t * 33 + lane], v1 = d1[t * 33 + lane];
+      const double ct = ct_r[t];
+      h0 = mk<double2>(v0.x - ct * h0.x, v0.y - ct * h0.y);
+      h1 = mk<double2>(v1.x - ct * h1.x, v1.y - ct * h1.y);
+      ha = at_r[t] - ct * ha;
+      hc = -ct * hc;
+    }
+  }
+  // reduced equation of this lane: A y_{l-1} + B y_l + C y_{l+1} = D
+  const double ha_n = shdn(ha, 1), hc_n = shdn(hc, 1);
+  const double h0x = shdn(h0.x, 1), h0y = shdn(h0.y, 1), h1x = shdn(h1.x, 1), h1y = shdn(h1.y, 1);
+  const double at_e = at_r[T - 1], ct_e = ct_r[T - 1];
+  double A = at_e, B = 1.0, C = 0.0;
+  double D[4] = {p0.x, p0.y, p1.x, p1.y};
+  if (lane < 31) {
+    B = 1.0 - ct_e * ha_n;
+    C = -ct_e * hc_n;
+    D[0] -= ct_e * h0x;
+    D[1] -= ct_e * h0y;
+    D[2] -= ct_e * h1x;
+    D[3] -= ct_e * h1y;
+  }
+  // parallel cyclic reduction over the 32 reduced equations
+#pragma unroll
+  for (int h = 1; h < 32; h <<= 1) {
+    const double iB = rcp_nr(B);
+    double Am = shup(A, h), iBm = shup(iB, h), Cm = shup(C, h);
+    double Ap = shdn(A, h), iBp = shdn(iB, h), Cp = shdn(C, h);
+    double Dm[4], Dp[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      Dm[c] = shup(D[c], h);
+      Dp[c] = shdn(D[c], h);
+    }
+    const bool lo = lane < h, hi = lane + h >= 32;
+    const double k1 = lo ? 0.0 : A * iBm, k2 = hi ? 0.0 : C * iBp;
+    if (lo) Am = Cm = 0.0;
+    if (hi) Ap = Cp = 0.0;
+    B = B - k1 * Cm - k2 * Ap;
+    A = -k1 * Am;
+    C = -k2 * Cp;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) D[c] = D[c] - k1 * Dm[c] - k2 * Dp[c];
+  }
+  const double iBf = rcp_nr(B);
+  double y[4], ys[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) y[c] = D[c] * iBf;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double v = shup(y[c], 1);  // every lane takes part in the shuffle
+    ys[c] = (lane == 0) ? 0.0 : v;
+  }
+  double2 x0 = mk<double2>(y[0], y[1]), x1 = mk<double2>(y[2], y[3]);
+  d0[(T - 1) * 33 + lane] = x0;
+  d1[(T - 1) * 33 + lane] = x1;
+#pragma unroll
+  for (int t = T - 2; t >= 0; --t) {
+    const int sl = t * 33 + lane;
+    const double a = at_r[t], c = ct_r[t];
+    const double2 v0 = d0[sl], v1 = d1[sl];
+    x0 = mk<double2>(v0.x - a * ys[0] - c * x0.x, v0.y - a * ys[1] - c * x0.y);
+    x1 = mk<double2>(v1.x - a * ys[2] - c * x1.x, v1.y - a * ys[3] - c * x1.y);
+    d0[sl] = x0;
+    d1[sl] = x1;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < T; ++c) {
+    const int e = lane + 32 * c;
+    if (e < ny) {
+      const int l = e / T, sl = (e - l * T) * 33 + l;
+      S0[e] = st(d0[sl]);
+      if (two) S1[e] = st(d1[sl]);
+    }
+  }
+}
+
 // shared memory of a k_tridiag<V, TM> block: the two right-hand sides per warp,
 // plus the coefficient arrays when TM == 0
 static size_t tridiag_block_smem(int T, int TM) {
@@ -381,6 +619,16 @@ static void launch_tridiag_t(V *spec, const GridK &g, const double *lamx, const 
   // e/T == umulhi(e, floor(2^32/T) + 1) for every e < 2^16 (and T <= 2^16)
   const unsigned magic = T > 1 ? (unsigned)((1ull << 32) / (unsigned long long)T + 1ull) : 0u;
   const dim3 blk(kWPB * 32);
+  const size_t sm2 = (size_t)kWPB * 2 * 33 * T * sizeof(double2);
+  switch (T) {
+#define TBFP_TRI_T(TT) \
+  case TT: k_tridiag_t<V, TT><<<nblk, blk, sm2, st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz); return;
+    TBFP_TRI_T(1) TBFP_TRI_T(2) TBFP_TRI_T(3) TBFP_TRI_T(4) TBFP_TRI_T(5) TBFP_TRI_T(6) TBFP_TRI_T(7)
+    TBFP_TRI_T(8) TBFP_TRI_T(9) TBFP_TRI_T(10) TBFP_TRI_T(11) TBFP_TRI_T(12) TBFP_TRI_T(13) TBFP_TRI_T(14)
+    TBFP_TRI_T(15) TBFP_TRI_T(16)
+#undef TBFP_TRI_T
+    default: break;
+  }
   if (T <= 4) k_tridiag<V, 4><<<nblk, blk, tridiag_block_smem(T, 4), st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, T, magic);
   else if (T <= 8) k_tridiag<V, 8><<<nblk, blk, tridiag_block_smem(T, 8), st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, T, magic);
   else if (T <= 12) k_tridiag<V, 12><<<nblk, blk, tridiag_block_smem(T, 12), st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, T, magic);
@@ -414,6 +662,13 @@ cudaError_t prepare_yz_kernels() {
   set((const void *)k_tridiag<float2, TM>, 227 * 1024);
   TBFP_TRI(0) TBFP_TRI(4) TBFP_TRI(8) TBFP_TRI(12) TBFP_TRI(16)
 #undef TBFP_TRI
+#define TBFP_TRI_T(TT)                                        \
+  set((const void *)k_tridiag_t<double2, TT>, 227 * 1024);    \
+  set((const void *)k_tridiag_t<float2, TT>, 227 * 1024);
+  TBFP_TRI_T(1) TBFP_TRI_T(2) TBFP_TRI_T(3) TBFP_TRI_T(4) TBFP_TRI_T(5) TBFP_TRI_T(6) TBFP_TRI_T(7)
+  TBFP_TRI_T(8) TBFP_TRI_T(9) TBFP_TRI_T(10) TBFP_TRI_T(11) TBFP_TRI_T(12) TBFP_TRI_T(13) TBFP_TRI_T(14)
+  TBFP_TRI_T(15) TBFP_TRI_T(16)
+#undef TBFP_TRI_T
   return e;
 }
 
