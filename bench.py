@@ -233,9 +233,10 @@ def run_reference(args, world, rank):
 
 def ensemble_measure(args, world, rank, local, precisions=("fp64",)):
     """Config 4: 64 channels of the minimal box with seeded sizes, one
-    tbfp_ensemble call per step (all members forked over 8 streams, replayed as
-    one CUDA graph; mixed members keep their refinement loops on the device),
-    against the same 64 projections made one after another through the
+    tbfp_ensemble call per step -- in the form the autotuner picks, and in each
+    form forced: the multi-stream CUDA graph and the one persistent launch
+    (mixed members run in the graph with their refinement loops on the device)
+    -- against the same 64 projections made one after another through the
     single-channel FP64 entry point.  Returns a dict on rank 0, else None."""
     import torch
     import torch.distributed as dist
@@ -284,18 +285,26 @@ def ensemble_measure(args, world, rank, local, precisions=("fp64",)):
 
     res = {}
     clocks = None
-    for prec in precisions:
-        ens = Ensemble([i.grid for i in inps], nstreams=8, precision=prec, tol=1e-10, max_iter=8)
+    # FP64: the form the autotuner picks (measured on the first call), then each form forced;
+    # mixed members run in the graph form (device-side refinement loops)
+    runs = [("fp64", "fp64", "auto"), ("fp64_graph", "fp64", "graph"), ("fp64_persistent", "fp64", "persistent")]
+    runs = [r for r in runs if r[1] in precisions] + [("mixed", "mixed", "auto")] * ("mixed" in precisions)
+    for key, prec, mode in runs:
+        ens = Ensemble([i.grid for i in inps], nstreams=8, precision=prec, tol=1e-10, max_iter=8, mode=mode)
         clk = ClockSampler(local)
         clk.start()
         ms = timed(lambda: ens.projection(members, dt, alpha, rho0, want_stats=False), args.steps)
         c = clk.stop()
         clocks = clocks or c
         st = ens.projection(members, dt, alpha, rho0)
+        form, param, tuned = ens.mode()
         ens.close()
-        res[prec] = {"value": world * ncells / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms,
-                     "solves_per_s": world * 64e3 / ms, "max_div": max(x.max_div for x in st),
-                     "max_sweeps": max(x.iterations for x in st)}
+        res[key] = {"value": world * ncells / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms,
+                    "solves_per_s": world * 64e3 / ms, "max_div": max(x.max_div for x in st),
+                    "max_sweeps": max(x.iterations for x in st), "form": form, "form_param": param}
+        if mode == "auto" and prec == "fp64":
+            res[key]["tuned_ms"] = {"graph": tuned[0], "persistent_1_block_per_sm": tuned[1],
+                                    "persistent_2_blocks_per_sm": tuned[2]}
 
     def sequential():
         for (psi, pn, pnm1, rho, u, uo), eqn in zip(members, seq):
@@ -330,7 +339,9 @@ def run_ensemble(args, world, rank, local):
         "config": {"workload": r["workload"], "channels": 64, "cells": r["cells"],
                    "precision": "fp64", "parallelism": f"64 independent channels per GPU x{world}",
                    "l2": "inputs larger than L2 (6 GB per step)", "timing": "events around synchronous calls"},
-        "max_div": f["max_div"], "mixed": r["mixed"], "sequential": r["sequential"],
+        "max_div": f["max_div"], "form": f["form"], "form_param": f["form_param"],
+        "tuned_ms": f.get("tuned_ms"), "fp64_graph": r.get("fp64_graph"),
+        "fp64_persistent": r.get("fp64_persistent"), "mixed": r["mixed"], "sequential": r["sequential"],
         "e2e": None, "gpu_launches": None, "clocks": r["clocks"], "cpu_baseline": None,
     }
     print(json.dumps(line), flush=True)

@@ -56,6 +56,7 @@ extern "C" {
 #define TBFP_ENONFINITE (-7) /* a NaN or Inf reached a residual, the pressure or max|div u|: a
                                 non-finite input, or a breakdown (the reference aborts) */
 #define TBFP_ESINGULAR (-8)  /* MG_MODE: the coarsest-level system is singular (beta not positive) */
+#define TBFP_ETIMEOUT (-9)   /* a bounded device-side wait ran out (persistent ensemble kernel) */
 
 /* precision modes */
 #define TBFP_FP64 0  /* plain FP64: the drop-in for solveFPS */
@@ -375,9 +376,29 @@ typedef struct {
   const double *rho, *psi_n, *psi_nm1;
   double *psi;                         /* pressure: written with ghosts */
 } tbfp_member_io;
+/* Execution forms of an ensemble. */
+#define TBFP_ENS_AUTO 0       /* choose by measurement on the first call, cached per device and sizes */
+#define TBFP_ENS_GRAPH 1      /* each member's kernels on a pool of streams, one replayed CUDA graph */
+#define TBFP_ENS_PERSISTENT 2 /* one persistent launch of every stage of every member (a device work
+                                 queue of (member, stage, tile) items with per-member stage counters),
+                                 replayed as a CUDA graph; FP64 members with out-of-place velocity,
+                                 nx/2 <= 128, nz <= 128, ny <= 256 */
 int tbfp_ensemble_create(int n, const tbfp_desc *descs, int nstreams, tbfp_ensemble **out);
 int tbfp_ensemble_destroy(tbfp_ensemble *e);
 int tbfp_ensemble_size(const tbfp_ensemble *e);
+/* Request a form (TBFP_ENS_*); param: blocks per SM of the persistent form (0: as many as fit).
+   TBFP_ENS_AUTO, the default, times the graph and the persistent kernel at one and two blocks per
+   SM on the first call for a set of arrays (when every member is out of place), keeps the fastest,
+   and appends the choice to the tuning cache file: $TBFP_TUNE_CACHE, else
+   $XDG_CACHE_HOME/tbfp_tune.txt, else $HOME/.cache/tbfp_tune.txt (one line per decision:
+   key, form, param, ms).  An ensemble of the same sizes on the same device reads it back. */
+int tbfp_ensemble_set_mode(tbfp_ensemble *e, int mode, int param);
+/* The form in use (0 before the first call) and its param; tuned_ms (NULL or 3 entries): the
+   measured ms of the graph and of the persistent form at 1 and 2 blocks per SM (-1: not measured). */
+int tbfp_ensemble_get_mode(const tbfp_ensemble *e, int *mode, int *param, float *tuned_ms);
+/* Bound on each dependency wait of the persistent kernel, in polls of about 0.1 us (default 1e7,
+   about a second).  A wait that runs out stops the launch: the call returns TBFP_ETIMEOUT. */
+int tbfp_ensemble_set_wait_limit(tbfp_ensemble *e, long long polls);
 /* One projection of every member; stats: NULL or n entries (max_div per member). */
 int tbfp_ensemble_projection_dev(tbfp_ensemble *e, const tbfp_member_io *io, double dt, double alpha,
                                  double rho0, tbfp_stats *stats);

@@ -23,6 +23,10 @@ TBFP_EUNSUPPORTED = -5
 TBFP_ENODEVICE = -6
 TBFP_ENONFINITE = -7
 TBFP_ESINGULAR = -8
+TBFP_ETIMEOUT = -9
+TBFP_ENS_AUTO = 0
+TBFP_ENS_GRAPH = 1
+TBFP_ENS_PERSISTENT = 2
 
 TBFP_FP64 = 0
 TBFP_MIXED = 1
@@ -109,6 +113,9 @@ PROTOTYPES = {
     "tbfp_ensemble_create": (C.c_int, [C.c_int, C.POINTER(TbfpDesc), C.c_int, C.POINTER(C.c_void_p)]),
     "tbfp_ensemble_destroy": (C.c_int, [_H]),
     "tbfp_ensemble_size": (C.c_int, [_H]),
+    "tbfp_ensemble_set_mode": (C.c_int, [_H, C.c_int, C.c_int]),
+    "tbfp_ensemble_get_mode": (C.c_int, [_H, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+    "tbfp_ensemble_set_wait_limit": (C.c_int, [_H, C.c_longlong]),
     "tbfp_ensemble_projection_dev": (C.c_int, [_H, C.POINTER(TbfpMemberIO), C.c_double, C.c_double, C.c_double,
                                                C.POINTER(TbfpStats)]),
     "tbfp_pcg_setup": (C.c_int, [_H, C.POINTER(TbfpMgParams)]),

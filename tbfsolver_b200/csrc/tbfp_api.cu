@@ -1,12 +1,14 @@
 // C ABI of the projection library: handle lifecycle, set-up tables and the
 // orchestration of the kernels in tbfp_kernels.cu.  See include/tbfp.h.
 #include <cuda_runtime.h>
+#include <sys/stat.h>
 
 #include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -692,6 +694,7 @@ const char *tbfp_strerror(int status) {
     case TBFP_ENODEVICE: return "no usable CUDA device";
     case TBFP_ENONFINITE: return "non-finite value (NaN or Inf) in a residual or a result";
     case TBFP_ESINGULAR: return "singular coarsest-level system";
+    case TBFP_ETIMEOUT: return "a bounded device-side wait ran out";
     default: return "unknown status";
   }
 }
@@ -1746,10 +1749,21 @@ int tbfp_pcg_solve(tbfp_handle *h, double *psi, const double *beta, const double
 }
 
 // ---------------------------------------------------------------------------
-// Ensemble: many independent channels per GPU in one call.  Members run on a
-// pool of streams; with every member in plain FP64 the whole step (all
-// members' launches, forked over the pool) is captured once as a CUDA graph
-// and replayed while the arrays and scalars stay the same.
+// Ensemble: many independent channels per GPU in one call, in one of two forms:
+//   graph:      each member's kernels on a pool of streams, captured once as a
+//               CUDA graph and replayed while the arrays and scalars stay the
+//               same (TBFP_MIXED members keep their device-side refinement
+//               loops inside the graph);
+//   persistent: every stage of every member in ONE launch of resident blocks
+//               that take (member, stage, tile) items from a device work queue
+//               (tbfp_ensemble.cu), that launch captured in a graph with the
+//               reset of the queue.  FP64 out-of-place members whose lengths
+//               the persistent kernel is compiled for (nx/2, nz <= 128,
+//               ceil(ny/32) <= 8).
+// TBFP_ENS_AUTO times the candidates (the graph, the persistent kernel at one
+// and two blocks per SM) on the first call for a set of arrays, keeps the
+// fastest and records it in the tuning cache file, keyed by the device and
+// the members' sizes; later ensembles of the same sizes read the choice back.
 // ---------------------------------------------------------------------------
 }  // extern "C"
 
@@ -1758,10 +1772,29 @@ struct tbfp_ensemble {
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> ev;  // [0] fork, [1..] joins
   int device = 0;
-  bool graphable = true;
+  bool graphable = true;        // the multi-stream form may be captured
+  bool persistent_ok = true;    // every member fits the persistent kernel
+  int mode = TBFP_ENS_AUTO;     // requested form
+  int param = 0;                // requested blocks per SM of the persistent form (0: occupancy)
+  int use_mode = 0, use_param = 0;  // form in use once chosen
+  long long spin_limit = 10000000;  // polls of a dependency wait (~0.1 us each)
+  std::string sizes_key;
+  // graph form
   cudaGraphExec_t graph = nullptr;
   std::vector<tbfp_member_io> key;
   double kdt = 0.0, kalpha = 0.0, krho0 = 0.0;
+  // persistent form
+  size_t smem = 0;
+  EnsMember *d_mem = nullptr;
+  int *d_qstart = nullptr;
+  EnsCtl *d_ctl = nullptr;
+  size_t ctl_bytes = 0;
+  int total_items = 0;
+  cudaGraphExec_t pgraph = nullptr;
+  int pgraph_blocks = 0;
+  std::vector<tbfp_member_io> pkey;
+  double pdt = 0.0, palpha = 0.0, prho0 = 0.0;
+  float tuned_ms[3] = {-1.f, -1.f, -1.f};  // graph, persistent x1, persistent x2
 };
 
 namespace {
@@ -1783,6 +1816,266 @@ int ensemble_launch_all(tbfp_ensemble *e, const tbfp_member_io *io, double dt, d
     cudaEventRecord(e->ev[s], e->streams[s]);
     cudaStreamWaitEvent(e->streams[0], e->ev[s], 0);
   }
+  return TBFP_OK;
+}
+
+// The graph form: capture (when the arrays or scalars changed) and launch.
+int ensemble_run_graph(tbfp_ensemble *e, const tbfp_member_io *io, double dt, double alpha, double rho0) {
+  const int n = (int)e->h.size();
+  cudaStream_t s0 = e->streams[0];
+  if (!e->graphable) {
+    cudaEventRecord(e->ev[0], s0);
+    return ensemble_launch_all(e, io, dt, alpha, rho0);
+  }
+  bool reuse = e->graph && e->kdt == dt && e->kalpha == alpha && e->krho0 == rho0 && (int)e->key.size() == n;
+  for (int i = 0; reuse && i < n; ++i) reuse = same_io(e->key[i], io[i]);
+  if (!reuse) {
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+    cudaGraph_t g = nullptr;
+    int rc = TBFP_OK;
+    cudaError_t ce = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+      cudaEventRecord(e->ev[0], s0);
+      rc = ensemble_launch_all(e, io, dt, alpha, rho0);
+      ce = cudaStreamEndCapture(s0, &g);
+    }
+    if (rc < 0) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (ce != cudaSuccess)
+      return set_err(nullptr, TBFP_ECUDA, std::string("tbfp_ensemble_projection: graph: ") + cudaGetErrorString(ce));
+    e->key.assign(io, io + n);
+    e->kdt = dt;
+    e->kalpha = alpha;
+    e->krho0 = rho0;
+  }
+  const cudaError_t ce = cudaGraphLaunch(e->graph, s0);
+  if (ce != cudaSuccess)
+    return set_err(nullptr, TBFP_ECUDA, std::string("tbfp_ensemble_projection: ") + cudaGetErrorString(ce));
+  return TBFP_OK;
+}
+
+// A member as the persistent kernel sees it.
+EnsMember ens_member(tbfp_handle *h, const tbfp_member_io &m, double dt, double alpha, double rho0) {
+  EnsMember em{};
+  em.g = h->g;
+  em.ra = rhs_args(h, m.ux_in, m.uy_in, m.uz_in, m.psi_n, m.psi_nm1, nullptr, nullptr, dt, alpha, rho0);
+  em.ca = corr_args(h, m.ux_in, m.uy_in, m.uz_in, m.ux_out, m.uy_out, m.uz_out, m.psi, m.psi_n, m.psi_nm1, nullptr,
+                    nullptr, dt, alpha, rho0);
+  em.xs = XSrc{};
+  em.xs.s = h->d_s;
+  em.xs.Ls = h->Lpsi;
+  em.rho = m.rho;
+  em.irho = h->d_irho;
+  em.s = h->d_s;
+  em.n_rho = (long)h->n_rho;
+  em.spec = h->d_spec;
+  em.psi = m.psi;
+  em.Lpsi = h->Lpsi;
+  em.hd_psi = h->hd_psi;
+  em.twx = h->d_twx;
+  em.tpx = h->d_tpx;
+  em.tpz = h->d_tpz;
+  em.lamx = h->d_lamx;
+  em.lamz = h->d_lamz;
+  em.am = h->d_am;
+  em.ap = h->d_ap;
+  em.dyf = h->d_dyf;
+  em.mean_c = h->mean_c;
+  em.nxnz = h->nxnz;
+  em.scale = h->scale;
+  em.maxdiv = h->d_maxdiv;
+  em.T = tri_rows_per_lane(h->ny);
+  ens_items(h->g, (long)h->n_rho, em.T, em.items);
+  return em;
+}
+
+bool all_out_of_place(const tbfp_member_io *io, int n) {
+  for (int i = 0; i < n; ++i)
+    if (aliased(io[i].ux_in, io[i].ux_out) || aliased(io[i].uy_in, io[i].uy_out) ||
+        aliased(io[i].uz_in, io[i].uz_out))
+      return false;
+  return true;
+}
+
+// The persistent form: upload the member table (when the arrays or scalars
+// changed), capture [reset of the queue, one launch] as a graph, launch it.
+int ensemble_run_persistent(tbfp_ensemble *e, const tbfp_member_io *io, double dt, double alpha, double rho0,
+                            int blocks_per_sm) {
+  const int n = (int)e->h.size();
+  cudaStream_t s0 = e->streams[0];
+  int dev_sms = 0;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, e->device);
+  const int occ = ensemble_blocks_per_sm(e->smem);
+  if (occ < 1) return set_err(nullptr, TBFP_EUNSUPPORTED, "tbfp_ensemble_projection: persistent kernel does not fit");
+  const int bps = (blocks_per_sm > 0 && blocks_per_sm < occ) ? blocks_per_sm : occ;
+  const int blocks = bps * dev_sms;
+  bool same = e->pgraph && e->pgraph_blocks == blocks && e->pdt == dt && e->palpha == alpha && e->prho0 == rho0 &&
+              (int)e->pkey.size() == n;
+  for (int i = 0; same && i < n; ++i) same = same_io(e->pkey[i], io[i]);
+  if (!same) {
+    bool table_same = (int)e->pkey.size() == n && e->pdt == dt && e->palpha == alpha && e->prho0 == rho0;
+    for (int i = 0; table_same && i < n; ++i) table_same = same_io(e->pkey[i], io[i]);
+    if (!table_same) {
+      std::vector<EnsMember> mem(n);
+      std::vector<int> qs(kEnsStages * n + 1, 0);
+      for (int i = 0; i < n; ++i) mem[i] = ens_member(e->h[i], io[i], dt, alpha, rho0);
+      int run = 0;
+      for (int st = 0; st < kEnsStages; ++st)
+        for (int i = 0; i < n; ++i) {
+          qs[st * n + i] = run;
+          run += mem[i].items[st];
+        }
+      qs[kEnsStages * n] = run;
+      e->total_items = run;
+      cudaStreamSynchronize(s0);  // the previous launch may still read the table
+      if (cudaMemcpy(e->d_mem, mem.data(), sizeof(EnsMember) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+          cudaMemcpy(e->d_qstart, qs.data(), sizeof(int) * qs.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return set_err(nullptr, TBFP_ECUDA, "tbfp_ensemble_projection: uploading the member table");
+    }
+    if (e->pgraph) cudaGraphExecDestroy(e->pgraph);
+    e->pgraph = nullptr;
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+      cudaMemsetAsync(e->d_ctl, 0, e->ctl_bytes, s0);
+      launch_ensemble_persistent(e->d_mem, n, e->d_qstart, e->d_ctl, e->spin_limit, blocks, e->smem, s0);
+      ce = cudaStreamEndCapture(s0, &g);
+    }
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->pgraph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (ce != cudaSuccess)
+      return set_err(nullptr, TBFP_ECUDA, std::string("tbfp_ensemble_projection: persistent graph: ") +
+                                              cudaGetErrorString(ce));
+    e->pgraph_blocks = blocks;
+    e->pkey.assign(io, io + n);
+    e->pdt = dt;
+    e->palpha = alpha;
+    e->prho0 = rho0;
+  }
+  const cudaError_t ce = cudaGraphLaunch(e->pgraph, s0);
+  if (ce != cudaSuccess)
+    return set_err(nullptr, TBFP_ECUDA, std::string("tbfp_ensemble_projection: ") + cudaGetErrorString(ce));
+  return TBFP_OK;
+}
+
+// --- the tuning cache: one line per decision, "<key> <mode> <param> <ms>" ---
+std::string tune_cache_path() {
+  if (const char *p = std::getenv("TBFP_TUNE_CACHE")) return p;
+  if (const char *x = std::getenv("XDG_CACHE_HOME")) return std::string(x) + "/tbfp_tune.txt";
+  if (const char *hm = std::getenv("HOME")) return std::string(hm) + "/.cache/tbfp_tune.txt";
+  return "";
+}
+
+bool tune_lookup(const std::string &key, int *mode, int *param) {
+  const std::string path = tune_cache_path();
+  if (path.empty()) return false;
+  FILE *f = std::fopen(path.c_str(), "r");
+  if (!f) return false;
+  char k[512];
+  int m = 0, p = 0;
+  float ms = 0.f;
+  bool found = false;
+  while (std::fscanf(f, "%511s %d %d %f", k, &m, &p, &ms) == 4)
+    if (key == k) {  // the last line for a key wins
+      *mode = m;
+      *param = p;
+      found = true;
+    }
+  std::fclose(f);
+  return found;
+}
+
+void tune_record(const std::string &key, int mode, int param, float ms) {
+  const std::string path = tune_cache_path();
+  if (path.empty()) return;
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos && slash > 0) mkdir(path.substr(0, slash).c_str(), 0755);  // one level, if missing
+  FILE *f = std::fopen(path.c_str(), "a");
+  if (!f) return;  // an unwritable cache only costs a new tuning next time
+  std::fprintf(f, "%s %d %d %.4f\n", key.c_str(), mode, param, ms);
+  std::fclose(f);
+}
+
+// Device time of one call of a form (after one untimed call).
+int time_form(tbfp_ensemble *e, const tbfp_member_io *io, double dt, double alpha, double rho0, int mode, int param,
+              float *ms) {
+  cudaStream_t s0 = e->streams[0];
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  int rc = TBFP_OK;
+  for (int rep = 0; rep < 4 && rc == TBFP_OK; ++rep) {
+    if (rep == 1) cudaEventRecord(a, s0);
+    rc = (mode == TBFP_ENS_GRAPH) ? ensemble_run_graph(e, io, dt, alpha, rho0)
+                                  : ensemble_run_persistent(e, io, dt, alpha, rho0, param);
+  }
+  cudaEventRecord(b, s0);
+  cudaError_t ce = cudaEventSynchronize(b);
+  float t = 0.f;
+  if (rc == TBFP_OK && ce == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc) return rc;
+  if (ce != cudaSuccess) return set_err(nullptr, TBFP_ECUDA, std::string("ensemble tuning: ") + cudaGetErrorString(ce));
+  *ms = t / 3.f;
+  return TBFP_OK;
+}
+
+// Choose the form: the requested one, the cached choice, or a measurement.
+int ensemble_choose(tbfp_ensemble *e, const tbfp_member_io *io, double dt, double alpha, double rho0) {
+  const int n = (int)e->h.size();
+  const bool pers = e->persistent_ok && all_out_of_place(io, n);
+  if (e->mode == TBFP_ENS_GRAPH || (e->mode == TBFP_ENS_PERSISTENT && !pers)) {
+    if (e->mode == TBFP_ENS_PERSISTENT)
+      return set_err(nullptr, TBFP_EUNSUPPORTED,
+                     "tbfp_ensemble_projection: the persistent form needs FP64 out-of-place members with "
+                     "nx/2, nz <= 128 and ny <= 256");
+    e->use_mode = TBFP_ENS_GRAPH;
+    e->use_param = (int)e->streams.size();
+    return TBFP_OK;
+  }
+  if (e->mode == TBFP_ENS_PERSISTENT) {
+    e->use_mode = TBFP_ENS_PERSISTENT;
+    e->use_param = e->param;
+    return TBFP_OK;
+  }
+  if (!pers) {  // nothing to choose between
+    e->use_mode = TBFP_ENS_GRAPH;
+    e->use_param = (int)e->streams.size();
+    return TBFP_OK;
+  }
+  int m = 0, p = 0;
+  if (tune_lookup(e->sizes_key, &m, &p) && (m == TBFP_ENS_GRAPH || m == TBFP_ENS_PERSISTENT)) {
+    e->use_mode = m;
+    e->use_param = p;
+    return TBFP_OK;
+  }
+  // measure: the graph, then the persistent kernel at 1 and 2 blocks per SM
+  float best = 0.f;
+  int bm = TBFP_ENS_GRAPH, bp = (int)e->streams.size();
+  const int occ = ensemble_blocks_per_sm(e->smem);
+  for (int c = 0; c < 3; ++c) {
+    const int mode = c == 0 ? TBFP_ENS_GRAPH : TBFP_ENS_PERSISTENT;
+    const int param = c == 0 ? (int)e->streams.size() : c;
+    if (c > 0 && c > occ) continue;
+    float ms = 0.f;
+    const int rc = time_form(e, io, dt, alpha, rho0, mode, param, &ms);
+    if (rc) return rc;
+    e->tuned_ms[c] = ms;
+    if (c == 0 || ms < best) {
+      best = ms;
+      bm = mode;
+      bp = param;
+    }
+  }
+  e->use_mode = bm;
+  e->use_param = bp;
+  tune_record(e->sizes_key, bm, bp, best);
   return TBFP_OK;
 }
 }  // namespace
@@ -1810,6 +2103,9 @@ int tbfp_ensemble_create(int n, const tbfp_desc *descs, int nstreams, tbfp_ensem
         cudaEventCreateWithFlags(&e->ev[s], cudaEventDisableTiming) != cudaSuccess)
       return fail(set_err(nullptr, TBFP_ECUDA, "tbfp_ensemble_create: stream or event creation failed"));
   }
+  cudaDeviceProp prop{};
+  cudaGetDeviceProperties(&prop, e->device);
+  std::string sig;
   for (int i = 0; i < n; ++i) {
     tbfp_desc d = descs[i];
     if (d.device >= 0 && d.device != e->device)
@@ -1826,6 +2122,27 @@ int tbfp_ensemble_create(int n, const tbfp_desc *descs, int nstreams, tbfp_ensem
       return set_err(nullptr, rc, m);
     }
     e->h.push_back(h);
+    const int T = tri_rows_per_lane(d.ny);
+    if (d.precision != TBFP_FP64 || (d.flags & TBFP_FLAG_RESIDUAL) || !ens_supported(d.nx / 2, d.nz, T))
+      e->persistent_ok = false;
+    else e->smem = std::max(e->smem, ens_smem_bytes(d.nx / 2, d.nz, T));
+    sig += std::to_string(d.nx) + "x" + std::to_string(d.ny) + "x" + std::to_string(d.nz) + ";";
+  }
+  // tuning-cache key: the device and the members' sizes (FNV-1a of the list)
+  unsigned long long hsh = 1469598103934665603ull;
+  for (char c : sig) hsh = (hsh ^ (unsigned char)c) * 1099511628211ull;
+  std::string dev = prop.name;
+  for (char &c : dev)
+    if (c == ' ') c = '_';
+  char kb[64];
+  std::snprintf(kb, sizeof(kb), "%d-%016llx", n, hsh);
+  e->sizes_key = "ensemble|" + dev + "|" + kb;
+  if (e->persistent_ok) {
+    e->ctl_bytes = sizeof(EnsCtl) + sizeof(int) * (size_t)n * kEnsStages;
+    if (prepare_ensemble_kernel(e->smem) != cudaSuccess || cudaMalloc(&e->d_mem, sizeof(EnsMember) * n) != cudaSuccess ||
+        cudaMalloc(&e->d_qstart, sizeof(int) * ((size_t)kEnsStages * n + 1)) != cudaSuccess ||
+        cudaMalloc(&e->d_ctl, e->ctl_bytes) != cudaSuccess)
+      return fail(set_err(nullptr, TBFP_ENOMEM, "tbfp_ensemble_create: persistent-form buffers"));
   }
   *out = e;
   return TBFP_OK;
@@ -1837,16 +2154,53 @@ int tbfp_ensemble_destroy(tbfp_ensemble *e) {
   for (cudaStream_t s : e->streams)
     if (s) cudaStreamSynchronize(s);
   if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->pgraph) cudaGraphExecDestroy(e->pgraph);
   for (tbfp_handle *h : e->h) tbfp_destroy(h);
   for (cudaEvent_t v : e->ev)
     if (v) cudaEventDestroy(v);
   for (cudaStream_t s : e->streams)
     if (s) cudaStreamDestroy(s);
+  if (e->d_mem) cudaFree(e->d_mem);
+  if (e->d_qstart) cudaFree(e->d_qstart);
+  if (e->d_ctl) cudaFree(e->d_ctl);
   delete e;
   return TBFP_OK;
 }
 
 int tbfp_ensemble_size(const tbfp_ensemble *e) { return e ? (int)e->h.size() : 0; }
+
+int tbfp_ensemble_set_mode(tbfp_ensemble *e, int mode, int param) {
+  set_global_error("");
+  if (!e) return TBFP_ENULL;
+  if (mode != TBFP_ENS_AUTO && mode != TBFP_ENS_GRAPH && mode != TBFP_ENS_PERSISTENT)
+    return set_err(nullptr, TBFP_EINVAL, "tbfp_ensemble_set_mode: unknown mode");
+  if (mode == TBFP_ENS_PERSISTENT && !e->persistent_ok)
+    return set_err(nullptr, TBFP_EUNSUPPORTED,
+                   "tbfp_ensemble_set_mode: the persistent form needs FP64 members with nx/2, nz <= 128 and "
+                   "ny <= 256");
+  e->mode = mode;
+  e->param = param;
+  e->use_mode = 0;  // choose again on the next call
+  return TBFP_OK;
+}
+
+int tbfp_ensemble_get_mode(const tbfp_ensemble *e, int *mode, int *param, float *tuned_ms) {
+  if (!e) return TBFP_ENULL;
+  if (mode) *mode = e->use_mode;
+  if (param) *param = e->use_param;
+  if (tuned_ms)
+    for (int c = 0; c < 3; ++c) tuned_ms[c] = e->tuned_ms[c];
+  return TBFP_OK;
+}
+
+int tbfp_ensemble_set_wait_limit(tbfp_ensemble *e, long long polls) {
+  if (!e) return TBFP_ENULL;
+  if (polls < 0) return set_err(nullptr, TBFP_EINVAL, "tbfp_ensemble_set_wait_limit: negative limit");
+  e->spin_limit = polls;
+  if (e->pgraph) cudaGraphExecDestroy(e->pgraph);  // the limit is a launch argument: capture again
+  e->pgraph = nullptr;
+  return TBFP_OK;
+}
 
 int tbfp_ensemble_projection_dev(tbfp_ensemble *e, const tbfp_member_io *io, double dt, double alpha, double rho0,
                                  tbfp_stats *stats) {
@@ -1864,43 +2218,25 @@ int tbfp_ensemble_projection_dev(tbfp_ensemble *e, const tbfp_member_io *io, dou
   cudaSetDevice(e->device);
   cudaStream_t s0 = e->streams[0];
   int rc = TBFP_OK;
-  if (e->graphable) {
-    bool reuse = e->graph && e->kdt == dt && e->kalpha == alpha && e->krho0 == rho0 && (int)e->key.size() == n;
-    for (int i = 0; reuse && i < n; ++i) reuse = same_io(e->key[i], io[i]);
-    if (!reuse) {
-      if (e->graph) cudaGraphExecDestroy(e->graph);
-      e->graph = nullptr;
-      cudaGraph_t g = nullptr;
-      cudaError_t ce = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal);
-      if (ce == cudaSuccess) {
-        cudaEventRecord(e->ev[0], s0);
-        rc = ensemble_launch_all(e, io, dt, alpha, rho0);
-        ce = cudaStreamEndCapture(s0, &g);
-      }
-      if (rc < 0) {
-        if (g) cudaGraphDestroy(g);
-        return rc;
-      }
-      if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->graph, g, 0);
-      if (g) cudaGraphDestroy(g);
-      if (ce != cudaSuccess)
-        return set_err(nullptr, TBFP_ECUDA, std::string("tbfp_ensemble_projection: graph: ") + cudaGetErrorString(ce));
-      e->key.assign(io, io + n);
-      e->kdt = dt;
-      e->kalpha = alpha;
-      e->krho0 = rho0;
-    }
-    const cudaError_t ce = cudaGraphLaunch(e->graph, s0);
-    if (ce != cudaSuccess)
-      return set_err(nullptr, TBFP_ECUDA, std::string("tbfp_ensemble_projection: ") + cudaGetErrorString(ce));
-  } else {
-    cudaEventRecord(e->ev[0], s0);
-    rc = ensemble_launch_all(e, io, dt, alpha, rho0);
-    if (rc < 0) return rc;
+  if (e->use_mode == 0 || (e->use_mode == TBFP_ENS_PERSISTENT && !all_out_of_place(io, n))) {
+    if (e->use_mode == TBFP_ENS_PERSISTENT) e->use_mode = 0;
+    if ((rc = ensemble_choose(e, io, dt, alpha, rho0))) return rc;
   }
+  rc = (e->use_mode == TBFP_ENS_PERSISTENT) ? ensemble_run_persistent(e, io, dt, alpha, rho0, e->use_param)
+                                            : ensemble_run_graph(e, io, dt, alpha, rho0);
+  if (rc < 0) return rc;
   const cudaError_t ce = cudaStreamSynchronize(s0);
   if (ce != cudaSuccess)
     return set_err(nullptr, TBFP_ECUDA, std::string("tbfp_ensemble_projection: ") + cudaGetErrorString(ce));
+  if (e->use_mode == TBFP_ENS_PERSISTENT) {  // a dependency wait that ran out of polls stops the launch
+    int abort_word = 0;
+    if (cudaMemcpy(&abort_word, &e->d_ctl->abort, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return set_err(nullptr, TBFP_ECUDA, "tbfp_ensemble_projection: reading the work-queue state");
+    if (abort_word)
+      return set_err(nullptr, TBFP_ETIMEOUT,
+                     "tbfp_ensemble_projection: a dependency wait of the persistent kernel ran out of polls");
+  }
+  rc = TBFP_OK;
   if (stats) {
     for (int i = 0; i < n; ++i) {
       unsigned long long bits = 0;
@@ -1908,7 +2244,9 @@ int tbfp_ensemble_projection_dev(tbfp_ensemble *e, const tbfp_member_io *io, dou
         return set_err(nullptr, TBFP_ECUDA, "tbfp_ensemble_projection: reading the continuity error");
       double md;
       std::memcpy(&md, &bits, sizeof(md));
-      stats[i] = e->h[i]->last;
+      stats[i] = tbfp_stats{};
+      stats[i].iterations = 1;
+      stats[i].rel_residual = -1.0;
       stats[i].max_div = md;
       stats[i].cont_err = md * dt;
       if (e->h[i]->precision == TBFP_MIXED) {

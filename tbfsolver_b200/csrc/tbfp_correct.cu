@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "tbfp_kernels.cuh"
+#include "tbfp_stages.cuh"
 
 namespace tbfp {
 
@@ -51,149 +52,9 @@ __device__ __forceinline__ double corr_z(const CorrArgs &a, const GridK &g, int 
   return a.uzi[at(a.Luz, i, j, k)] - a.r * (a.invrho0 * dpr + (invrho - a.invrho0) * dpr0);
 }
 
-__device__ __forceinline__ void block_max_atomic(double v, unsigned long long *out) {
-  __shared__ double red[32];
-  for (int o = 16; o > 0; o >>= 1) v = nanmax_nonneg(v, __shfl_xor_sync(0xffffffffu, v, o));
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  if (w == 0) {
-    v = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v = nanmax_nonneg(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if (l == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
-  }
-}
-
-// Out-of-place correction fused with the continuity check.  Grid (x tiles of
-// 128, y chunks of kJC rows, nz); a thread owns column (i, k) of a y chunk and
-// walks it in j with one pointer per array and neighbour, so the lower y face
-// of a cell is the upper face computed one step before.  Every thread computes
-// both of its x faces (the lower one is the upper face of cell i-1, or of cell
-// nx at i = 1: the periodic image), which keeps the warp free of divergent
-// recomputation.  The periodic duplicates ux(0)=ux(nx), uz(.,.,0)=uz(.,.,nz) are
-// the equated values of vfield.f90:124-189 and the uy wall faces are copied
-// through.  |div u| (auxiliaryRoutines.f90:71-75) is reduced per block and
-// folded into *maxdiv with one atomic.
-constexpr int kJC = 32;
-
-// Face update of makeVelocityDivFree FAST for one face: u - r*(invrho0*dpr + (invrho-invrho0)*dpr0),
-// dpr = (psi+ - psi)*idc, dpr0 = (2(pn+ - pn) - (po+ - po))*idc [- 2 st^n + st^{n-1}].
-__device__ __forceinline__ double face_update(double u, double r, double ir0, double irp, double irc, double idc,
-                                              double ps_p, double ps_c, double pn_p, double pn_c, double po_p,
-                                              double po_c, double st) {
-  const double invrho = 0.5 * (irp + irc);
-  const double dpr = (ps_p - ps_c) * idc;
-  const double dpr0 = (2.0 * (pn_p - pn_c) - (po_p - po_c)) * idc - st;
-  return u - r * (ir0 * dpr + (invrho - ir0) * dpr0);
-}
-
 template <bool ST>
 __global__ void __launch_bounds__(128, 8) k_correct_div(CorrArgs a, GridK g, unsigned long long *__restrict__ maxdiv) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int k = blockIdx.z + 1;
-  const int j0 = blockIdx.y * kJC + 1, j1 = min(j0 + kJC - 1, g.ny);
-  const bool valid = i <= g.nx;
-  const int ic = valid ? i : g.nx;  // clamped index keeps every load in bounds
-  const int km = (k == 1 && !g.slab) ? g.nz : k - 1;
-  // 32-bit element offsets (tbfp_create checks every array has < 2^31 elements)
-  const int pjs = (int)a.Lpsi.sj, rjs = (int)a.Lrho.sj;
-  const int xjs = (int)a.Lux.sj, yjs = (int)a.Luy.sj, zjs = (int)a.Luz.sj;
-  // offset of the lower x neighbour's centre: cell i-1, or cell nx at i = 1
-  const int xo = (ic == 1) ? g.nx - 1 : -1;
-  int op = (int)at(a.Lpsi, ic, j0, k), oq = (int)at(a.Lrho, ic, j0, k);
-  const int pz = (int)a.Lpsi.sk, pm = (km - k) * (int)a.Lpsi.sk;
-  const int qz = (int)a.Lrho.sk, qm = (km - k) * (int)a.Lrho.sk;
-  int ox = (int)at(a.Lux, ic, j0, k), oy = (int)at(a.Luy, ic, j0, k), oz = (int)at(a.Luz, ic, j0, k);
-  const int zm = (km - k) * (int)a.Luz.sk;
-  const double *__restrict__ ps = a.psi;
-  const double *__restrict__ pn = a.pn;
-  const double *__restrict__ po = a.pnm1;
-  const double *__restrict__ ir = a.irho;
-  const double *__restrict__ uxi = a.uxi;
-  const double *__restrict__ uyi = a.uyi;
-  const double *__restrict__ uzi = a.uzi;
-  double *__restrict__ uxo = a.uxo;
-  double *__restrict__ uyo = a.uyo;
-  double *__restrict__ uzo = a.uzo;
-  const double r = a.r, ir0 = a.invrho0;
-  const double idxc = g.idxc1, idzc = g.idzc1;
-  const double idx = g.idxf[ic - 1], idz = g.idzf[k - 1];
-  // surface-tension terms of one face (zero without surface tension)
-  auto stf = [&](int c, int ii, int jj, int kk) -> double {
-    if constexpr (ST) {
-      const long q = at(a.Lst[c], ii, jj, kk);
-      return 2.0 * a.stn[c][q] - a.sto[c][q];
-    } else return 0.0;
-  };
-
-  // centre values of the current cell, carried along j
-  double psc = ps[op], pnc = pn[op], poc = po[op], irc = ir[oq];
-  double uym;
-  if (j0 > 1) {
-    uym = face_update(uyi[oy - yjs], r, ir0, irc, ir[oq - rjs], g.idyc[j0 - 1], psc, ps[op - pjs], pnc,
-                      pn[op - pjs], poc, po[op - pjs], stf(1, ic, j0 - 1, k));
-  } else {
-    uym = uyi[oy - yjs];
-    if (valid) uyo[oy - yjs] = uym;
-  }
-  double vmax = 0.0;
-  for (int j = j0; j <= j1; ++j) {
-    // every load of this step, issued together
-    const int ow = op + xo, qw = oq + xo;
-    const double psx = ps[op + 1], pnx = pn[op + 1], pox = po[op + 1], irx = ir[oq + 1];
-    // the lower x face is the upper face of lane - 1; lane 0 computes it
-    const bool lead = (threadIdx.x & 31) == 0;
-    double psw = 0.0, pnw = 0.0, pow_ = 0.0, irw = 0.0, psw1 = 0.0, pnw1 = 0.0, pow1 = 0.0, irw1 = 0.0, ux_w = 0.0;
-    if (lead) {
-      psw = ps[ow];
-      pnw = pn[ow];
-      pow_ = po[ow];
-      irw = ir[qw];
-      psw1 = ps[ow + 1];
-      pnw1 = pn[ow + 1];
-      pow1 = po[ow + 1];
-      irw1 = ir[qw + 1];
-      ux_w = uxi[ox + xo];
-    }
-    const double psy = ps[op + pjs], pny = pn[op + pjs], poy = po[op + pjs], iry = ir[oq + rjs];
-    const double psz = ps[op + pz], pnz = pn[op + pz], poz = po[op + pz], irz = ir[oq + qz];
-    const double psm = ps[op + pm], pnm = pn[op + pm], pom = po[op + pm], irm = ir[oq + qm];
-    const double ux_c = uxi[ox], uy_c = uyi[oy], uz_c = uzi[oz], uz_m = uzi[oz + zm];
-
-    const double uxp = face_update(ux_c, r, ir0, irx, irc, idxc, psx, psc, pnx, pnc, pox, poc, stf(0, ic, j, k));
-    const double uxl = lead ? face_update(ux_w, r, ir0, irw1, irw, idxc, psw1, psw, pnw1, pnw, pow1, pow_,
-                                          stf(0, ic + xo, j, k))
-                            : 0.0;
-    const double uxs = __shfl_up_sync(0xffffffffu, uxp, 1);
-    const double uxm = lead ? uxl : uxs;
-    const double uyp = (j < g.ny) ? face_update(uy_c, r, ir0, iry, irc, g.idyc[j], psy, psc, pny, pnc, poy, poc,
-                                                stf(1, ic, j, k))
-                                  : uy_c;
-    const double uzp = face_update(uz_c, r, ir0, irz, irc, idzc, psz, psc, pnz, pnc, poz, poc, stf(2, ic, j, k));
-    const double uzq = face_update(uz_m, r, ir0, irc, irm, idzc, psc, psm, pnc, pnm, poc, pom, stf(2, ic, j, km));
-    if (valid) {
-      uxo[ox] = uxp;
-      if (i == g.nx) uxo[ox - ic] = uxp;  // ux(0, j, k)
-      uyo[oy] = uyp;
-      uzo[oz] = uzp;
-      if (k == g.nz && !g.slab) uzo[oz - k * (int)a.Luz.sk] = uzp;  // uz(i, j, 0)
-      double dv = (uxp - uxm) * idx;
-      dv = dv + (uyp - uym) * g.idyf[j - 1];
-      dv = dv + (uzp - uzq) * idz;
-      vmax = nanmax_nonneg(vmax, dv);
-    }
-    uym = uyp;
-    psc = psy;
-    pnc = pny;
-    poc = poy;
-    irc = iry;
-    op += pjs;
-    oq += rjs;
-    ox += xjs;
-    oy += yjs;
-    oz += zjs;
-  }
-  block_max_atomic(vmax, maxdiv);
+  correct_div_body<ST>(a, g, maxdiv, blockIdx.x, blockIdx.y, blockIdx.z, threadIdx.x);
 }
 
 void launch_correct_div(const CorrArgs &ca, bool has_st, const GridK &g, unsigned long long *maxdiv,

@@ -98,6 +98,58 @@ struct MixedCtl {
   int done;
 };
 
+// One member of an ensemble as the persistent kernel sees it (tbfp_ensemble.cu):
+// its grid, the arguments of each stage and its tile counts.  Built on the host
+// from the member's handle and arrays, copied to the device once per set of
+// arrays.  Stages: 0 1/rho, 1 split RHS, 2 forward x, 3 forward z, 4 y systems,
+// 5 backward z, 6 backward x, 7 correction with the continuity check.
+constexpr int kEnsStages = 8;
+struct EnsMember {
+  GridK g;
+  RhsArgs ra;
+  CorrArgs ca;
+  XSrc xs;                        // s -> forward x (acc = nullptr)
+  const double *rho;
+  double *irho, *s;
+  long n_rho;
+  double2 *spec;
+  double *psi;
+  Lay Lpsi;
+  int hd_psi;
+  const double2 *twx, *tpx, *tpz;
+  const double *lamx, *lamz, *am, *ap, *dyf;
+  double mean_c, nxnz, scale;
+  unsigned long long *maxdiv;
+  int T;                          // rows per lane of the y systems
+  int items[kEnsStages];          // work items of each stage (256-thread tiles)
+};
+// Work-queue state of one persistent launch (zeroed before the launch):
+// next item, items finished per (member, stage), and the abort word (1 = a
+// dependency wait ran out of its spin budget).
+struct EnsCtl {
+  int next;
+  int abort;
+  int pad[2];
+  int done[1];  // [members * kEnsStages], allocated with the block
+};
+// Lengths the persistent kernel is compiled for: nx/2 and nz up to 128, rows
+// per lane (ceil(ny/32)) up to 8.  Larger members use the graph form.
+constexpr int kEnsMaxLen = 128, kEnsMaxT = 8;
+inline bool ens_supported(int M, int nz, int T) {
+  return M <= kEnsMaxLen && nz <= kEnsMaxLen && T <= kEnsMaxT;
+}
+// Work items of each stage of a member, and the dynamic shared memory the
+// persistent kernel needs for it.
+void ens_items(const GridK &g, long n_rho, int T, int *items);
+size_t ens_smem_bytes(int M, int nz, int T);
+// One persistent launch over every member: grid = blocks_per_sm x SMs;
+// spin_limit bounds each dependency wait (iterations of ~0.1 us).  qstart
+// holds the prefix sums of the items, stage-major: qstart[s*n + m].
+cudaError_t launch_ensemble_persistent(const EnsMember *mem, int n, const int *qstart, EnsCtl *ctl,
+                                       long long spin_limit, int blocks, size_t smem, cudaStream_t st);
+cudaError_t prepare_ensemble_kernel(size_t smem);
+int ensemble_blocks_per_sm(size_t smem);
+
 // Transform lengths with a compiled kernel (nx/2 and nz): 2^a and 3*2^a, 4..512.
 #define TBFP_FFT_LENGTHS(X) \
   X(4) X(6) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)

@@ -1,0 +1,764 @@
+// Tile bodies of the FP64/FP32 projection kernels as device functions.
+//
+// Each kernel of the projection (tbfp_xfft.cu, tbfp_yz.cu, tbfp_correct.cu) is
+// a thin __global__ wrapper that calls one of these bodies with its block
+// coordinates; the persistent ensemble kernel (tbfp_ensemble.cu) calls the
+// same bodies for the tiles it takes from its work queue.  COH = true reads
+// the buffers that are written during the same launch (1/rho, s, the spectrum,
+// psi) through L2 (ld.global.cg): a persistent kernel consumes data that other
+// blocks of the same launch produced, which the read-only and L1 paths of a
+// plain load do not guarantee to see.  The standalone kernels use COH = false.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "tbfp_kernels.cuh"
+
+namespace tbfp {
+
+template <bool COH, typename X>
+__device__ __forceinline__ X ldc(const X *p) {
+  if constexpr (COH) return __ldcg(p);
+  else return *p;
+}
+
+constexpr int kRJ = 32;                // y rows walked by one thread of the RHS kernel
+constexpr int kNoGhost = -(1 << 30);  // no ghost image of this index
+
+// 1/rho over elements [t0, t1) of the (halo-inclusive) density array.
+__device__ __forceinline__ void recip_body(const double *__restrict__ rho, double *__restrict__ irho, long t0,
+                                           long t1, int tid, int nthreads) {
+  for (long t = t0 + tid; t < t1; t += nthreads) irho[t] = 1.0 / rho[t];
+}
+
+__device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+__device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+
+// ---------------------------------------------------------------------------
+// Forward x transform (see k_fftx_fwd in tbfp_xfft.cu)
+// ---------------------------------------------------------------------------
+template <typename V, int M, int MODE, bool COH = false>
+__device__ __forceinline__ void fftx_fwd_body(XSrc src, GridK g, const V *__restrict__ twx,
+                                              const V *__restrict__ tpx, V *__restrict__ spec, int bx,
+                                              unsigned char *smx) {
+  using T = decltype(V::x);
+  constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
+  constexpr int LD = x_row_stride(M), NX = 2 * M, NXC = (NX + 31) / 32;
+  V *sm = reinterpret_cast<V *>(smx);
+  V *tw = sm + TJ * LD;
+  __shared__ double red[kNW][3];
+  for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = tpx[t];
+  const int r0 = bx << LOGTJ;
+  const int nrows = min(TJ, (int)g.R - r0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  V *wsm = sm + warp * RPW * LD;  // this warp's rows
+  T *wsr = reinterpret_cast<T *>(wsm);
+  const bool sums = (MODE == 0) ? src.acc != nullptr : true;
+  const double ctop = (MODE == 1) ? src.acc[0] * src.ctop_scale : 0.0;
+  double sum0 = 0.0, sum1 = 0.0, vmax = 0.0;
+
+#pragma unroll
+  for (int rl = 0; rl < RPW; ++rl) {
+    const int row = warp * RPW + rl;
+    T *dst = wsr + rl * 2 * LD;
+    if (row < nrows) {
+      const unsigned rr = (unsigned)(r0 + row);
+      const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
+      const double *srow = src.s + at(src.Ls, 0, j, k);
+      if constexpr (MODE == 0) {
+        const double wy = sums ? src.dyf[j - 1] : 0.0;
+#pragma unroll
+        for (int c = 0; c < NXC; ++c) {
+          const int ii = lane + 32 * c;
+          if (NX % 32 == 0 || ii < NX) {
+            const double v = ldc<COH>(srow + ii + 1);
+            sum0 += v * wy;
+            sum1 += v * v;
+            dst[2 * pad8(ii >> 1) + (ii & 1)] = (T)v;
+          }
+        }
+      } else {
+        // r = s - c [j == ny] - L psi (the operator whose eigenvectors the solve uses)
+        const double *p = src.psi + at(src.Lp, 0, j, k);
+        const long sj = src.Lp.sj, sk = src.Lp.sk;
+        const double amj = src.am[j - 1], apj = src.ap[j - 1];
+        const double cj = (j == g.ny) ? ctop : 0.0;
+#pragma unroll
+        for (int c = 0; c < NXC; ++c) {
+          const int ii = lane + 32 * c;
+          if (NX % 32 == 0 || ii < NX) {
+            const int i = ii + 1;
+            const double p0 = p[i];
+            const double lap = (p[i + 1] + p[i - 1] - 2.0 * p0) * src.idx2 + amj * (p[i - sj] - p0) +
+                               apj * (p[i + sj] - p0) + (p[i + sk] + p[i - sk] - 2.0 * p0) * src.idz2;
+            const double v = (srow[i] - cj) - lap;
+            sum1 += v * v;
+            vmax = nanmax_nonneg(vmax, v + cj);
+            dst[2 * pad8(ii >> 1) + (ii & 1)] = (T)v;
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < NXC; ++c) {
+        const int ii = lane + 32 * c;
+        if (NX % 32 == 0 || ii < NX) dst[2 * pad8(ii >> 1) + (ii & 1)] = T(0);
+      }
+    }
+  }
+  if (sums) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sum0 += __shfl_xor_sync(0xffffffffu, sum0, o);
+      sum1 += __shfl_xor_sync(0xffffffffu, sum1, o);
+      if constexpr (MODE == 1) vmax = nanmax_nonneg(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    }
+    if (lane == 0) {
+      red[warp][0] = sum0;
+      red[warp][1] = sum1;
+      red[warp][2] = vmax;
+    }
+  }
+  __syncthreads();  // twiddle table, rows and partial sums in place
+  if (sums && threadIdx.x == 0) {
+    double a0 = 0.0, a1 = 0.0, m = 0.0;
+    for (int w = 0; w < kNW; ++w) {
+      a0 += red[w][0];
+      a1 += red[w][1];
+      m = nanmax_nonneg(m, red[w][2]);
+    }
+    if constexpr (MODE == 0) {
+      atomicAdd(src.acc, a0);
+      atomicAdd(src.acc + 1, a1);
+    } else {
+      atomicAdd(src.acc_r, a1);
+      atomicMax(reinterpret_cast<unsigned long long *>(src.acc_r + 1), (unsigned long long)__double_as_longlong(m));
+    }
+  }
+  fft_warp<V, M, LOGRPW, 1, LD, false>(wsm, lane, tw);
+
+  // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx)
+  constexpr int NPAIR = M / 2 + 1, NPC = (NPAIR + 31) / 32;
+  const T half = T(0.5);
+#pragma unroll
+  for (int rl = 0; rl < RPW; ++rl) {
+    V *Z = wsm + rl * LD;
+#pragma unroll
+    for (int c = 0; c < NPC; ++c) {
+      const int kk = lane + 32 * c;
+      if (kk >= NPAIR) break;
+      if (kk == 0) {
+        const V z0 = Z[0];
+        Z[0] = mk<V>(z0.x + z0.y, T(0));
+        Z[pad8(M)] = mk<V>(z0.x - z0.y, T(0));
+      } else {
+        const int km = M - kk;
+        const V a = Z[pad8(kk)], b = Z[pad8(km)];
+        const V wa = twx[kk], wb = twx[km];
+        V ep = mk<V>(a.x + b.x, a.y - b.y);  // Z_k + conj Z_{M-k}
+        V em = mk<V>(a.x - b.x, a.y + b.y);  // Z_k - conj Z_{M-k}
+        V t1 = cmul(wa, em);                  // W^k * em
+        Z[pad8(kk)] = mk<V>(half * (ep.x + t1.y), half * (ep.y - t1.x));  // (ep - i t1)/2
+        if (km != kk) {
+          V fp = mk<V>(b.x + a.x, b.y - a.y);
+          V fm = mk<V>(b.x - a.x, b.y + a.y);
+          V t2 = cmul(wb, fm);
+          Z[pad8(km)] = mk<V>(half * (fp.x + t2.y), half * (fp.y - t2.x));
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // S[kx][r0 + row]: consecutive threads take consecutive rows of one kx
+  constexpr int NST = ((M + 1) << LOGTJ);
+#pragma unroll
+  for (int t = threadIdx.x; t < NST; t += kNT) {
+    const int kx = t >> LOGTJ, row = t & (TJ - 1);
+    if (row < nrows) spec[(long)kx * g.R + r0 + row] = sm[row * LD + pad8(kx)];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Split right-hand side (see k_rhs in tbfp_xfft.cu)
+// ---------------------------------------------------------------------------
+template <bool ST, bool COH = false>
+__device__ __forceinline__ void rhs_body(RhsArgs a, GridK g, double *__restrict__ s, Lay Ls, int bx, int by, int bz,
+                                         int tx) {
+  const int i = bx * 128 + tx + 1;
+  const int k = bz + 1;
+  const int j0 = by * kRJ + 1, j1 = min(j0 + kRJ - 1, g.ny);
+  if (i > g.nx) return;  // no block-level barrier in this kernel
+  const int pjs = (int)a.Lpsi.sj, pks = (int)a.Lpsi.sk, rjs = (int)a.Lrho.sj, rks = (int)a.Lrho.sk;
+  const int xjs = (int)a.Lux.sj, yjs = (int)a.Luy.sj, zjs = (int)a.Luz.sj, zks = (int)a.Luz.sk;
+  const int sjs = (int)Ls.sj;
+  int op = (int)at(a.Lpsi, i, j0, k), oq = (int)at(a.Lrho, i, j0, k);
+  int ox = (int)at(a.Lux, i, j0, k), oy = (int)at(a.Luy, i, j0, k), oz = (int)at(a.Luz, i, j0, k);
+  int os = (int)at(Ls, i, j0, k);
+  const double *__restrict__ ux = a.ux;
+  const double *__restrict__ uy = a.uy;
+  const double *__restrict__ uz = a.uz;
+  const double *__restrict__ ir = a.irho;
+  const double *__restrict__ pn = a.pn;
+  const double *__restrict__ po = a.pnm1;
+  const double h = a.rho0 * 0.5;
+  const double idxf = g.idxf1, idzf = g.idzf1, idxc = g.idxc1, idzc = g.idzc1;
+  // carried along j: centre values and the lower y face
+  double irc = ldc<COH>(ir + (oq)), pc = pn[op], oc = po[op];
+  double irm = ldc<COH>(ir + (oq - rjs)), pm = pn[op - pjs], om = po[op - pjs];
+  double uym = uy[oy - yjs];
+  for (int j = j0; j <= j1; ++j) {
+    const double uxc = ux[ox], uxm = ux[ox - 1], uyc = uy[oy], uzc = uz[oz], uzm = uz[oz - zks];
+    const double irxp = ldc<COH>(ir + (oq + 1)), irxm = ldc<COH>(ir + (oq - 1)), iryp = ldc<COH>(ir + (oq + rjs)), irzp = ldc<COH>(ir + (oq + rks)), irzm = ldc<COH>(ir + (oq - rks));
+    const double pxp = pn[op + 1], pxm = pn[op - 1], pyp = pn[op + pjs], pzp = pn[op + pks], pzm = pn[op - pks];
+    const double oxp = po[op + 1], oxm = po[op - 1], oyp = po[op + pjs], ozp = po[op + pks], ozm = po[op - pks];
+    const double idyf = g.idyf[j - 1], idycp = g.idyc[j], idycm = g.idyc[j - 1];
+
+    const double ddx = (uxc - uxm) * idxf;
+    const double ddy = (uyc - uym) * idyf;
+    const double ddz = (uzc - uzm) * idzf;
+    double r = ((ddx + ddy) + ddz) * a.r * a.rho0;
+    const double apx = 1.0 - h * (irxp + irc);
+    const double amx = 1.0 - h * (irxm + irc);
+    const double apy = 1.0 - h * (iryp + irc);
+    const double amy = 1.0 - h * (irm + irc);
+    const double apz = 1.0 - h * (irzp + irc);
+    const double amz = 1.0 - h * (irzm + irc);
+    double dpxp = (2.0 * (pxp - pc) - (oxp - oc)) * idxc;
+    double dpxm = (2.0 * (pc - pxm) - (oc - oxm)) * idxc;
+    double dpyp = (2.0 * (pyp - pc) - (oyp - oc)) * idycp;
+    double dpym = (2.0 * (pc - pm) - (oc - om)) * idycm;
+    double dpzp = (2.0 * (pzp - pc) - (ozp - oc)) * idzc;
+    double dpzm = (2.0 * (pc - pzm) - (oc - ozm)) * idzc;
+    if constexpr (ST) {
+      const long x0 = at(a.Lst[0], i, j, k), y0 = at(a.Lst[1], i, j, k), z0 = at(a.Lst[2], i, j, k);
+      dpxp = dpxp - 2.0 * a.stn[0][x0] + a.sto[0][x0];
+      dpxm = dpxm - 2.0 * a.stn[0][x0 - 1] + a.sto[0][x0 - 1];
+      dpyp = dpyp - 2.0 * a.stn[1][y0] + a.sto[1][y0];
+      dpym = dpym - 2.0 * a.stn[1][y0 - a.Lst[1].sj] + a.sto[1][y0 - a.Lst[1].sj];
+      dpzp = dpzp - 2.0 * a.stn[2][z0] + a.sto[2][z0];
+      dpzm = dpzm - 2.0 * a.stn[2][z0 - a.Lst[2].sk] + a.sto[2][z0 - a.Lst[2].sk];
+    }
+    r = r + (apx * dpxp - amx * dpxm) * idxf;
+    r = r + (apy * dpyp - amy * dpym) * idyf;
+    r = r + (apz * dpzp - amz * dpzm) * idzf;
+    s[os] = r;
+    irm = irc;
+    pm = pc;
+    om = oc;
+    irc = iryp;
+    pc = pyp;
+    oc = oyp;
+    uym = uyc;
+    op += pjs;
+    oq += rjs;
+    ox += xjs;
+    oy += yjs;
+    oz += zjs;
+    os += sjs;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Inverse x transform (see k_fftx_inv in tbfp_xfft.cu)
+// ---------------------------------------------------------------------------
+template <typename V, int M, bool ACC, bool COH = false>
+__device__ __forceinline__ void fftx_inv_body(const V *__restrict__ spec, double *__restrict__ psi, Lay Lp, int hd,
+                                              GridK g, const V *__restrict__ twx, const V *__restrict__ tpx,
+                                              double scale, int bx, unsigned char *smx) {
+  using T = decltype(V::x);
+  constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
+  constexpr int LD = x_row_stride(M), NX = 2 * M, NXC = (NX + 31) / 32;
+  V *sm = reinterpret_cast<V *>(smx);
+  V *tw = sm + TJ * LD;
+  for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = tpx[t];
+  const int r0 = bx << LOGTJ;
+  const int nrows = min(TJ, (int)g.R - r0);
+  constexpr int NLD = ((M + 1) << LOGTJ);
+#pragma unroll
+  for (int t = threadIdx.x; t < NLD; t += kNT) {
+    const int kx = t >> LOGTJ, row = t & (TJ - 1);
+    sm[row * LD + pad8(kx)] = (row < nrows) ? ldc<COH>(spec + ((long)kx * g.R + r0 + row)) : mk<V>(T(0), T(0));
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  V *wsm = sm + warp * RPW * LD;
+  // Z[k] = (X_k + conj X_{M-k}) + i conj(W^k) (X_k - conj X_{M-k}),  k = 0..M-1
+  constexpr int NPAIR = M / 2 + 1, NPC = (NPAIR + 31) / 32;
+#pragma unroll
+  for (int rl = 0; rl < RPW; ++rl) {
+    V *X = wsm + rl * LD;
+#pragma unroll
+    for (int c = 0; c < NPC; ++c) {
+      const int kk = lane + 32 * c;
+      if (kk >= NPAIR) break;
+      if (kk == 0) {
+        const T a = X[0].x, b = X[pad8(M)].x;
+        X[0] = mk<V>(a + b, a - b);
+      } else {
+        const int km = M - kk;
+        const V a = X[pad8(kk)], b = X[pad8(km)];
+        const V wa = cconj(twx[kk]), wb = cconj(twx[km]);
+        V ep = mk<V>(a.x + b.x, a.y - b.y);
+        V em = mk<V>(a.x - b.x, a.y + b.y);
+        V t1 = cmul(wa, em);
+        X[pad8(kk)] = mk<V>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
+        if (km != kk) {
+          V fp = mk<V>(b.x + a.x, b.y - a.y);
+          V fm = mk<V>(b.x - a.x, b.y + a.y);
+          V t2 = cmul(wb, fm);
+          X[pad8(km)] = mk<V>(fp.x - t2.y, fp.y + t2.x);
+        }
+      }
+    }
+  }
+  __syncwarp();
+  fft_warp<V, M, LOGRPW, 1, LD, true>(wsm, lane, tw);
+  const T *wsr = reinterpret_cast<const T *>(wsm);
+#pragma unroll
+  for (int rl = 0; rl < RPW; ++rl) {
+    const int row = warp * RPW + rl;
+    if (row >= nrows) break;
+    const unsigned rr = (unsigned)(r0 + row);
+    const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
+    // ghost images of the row: first y ghost layer (wall copy), periodic z
+    const int jg = (j == 1) ? 0 : (j == g.ny ? g.ny + 1 : -1);
+    const int kg = g.slab ? kNoGhost : ((k <= hd) ? k + g.nz : (k > g.nz - hd ? k - g.nz : kNoGhost));
+    double *p00 = psi + at(Lp, 0, j, k);
+    double *p10 = (jg >= 0) ? psi + at(Lp, 0, jg, k) : nullptr;
+    double *p01 = (kg != kNoGhost) ? psi + at(Lp, 0, j, kg) : nullptr;
+    double *p11 = (p10 && p01) ? psi + at(Lp, 0, jg, kg) : nullptr;
+    const T *src = wsr + rl * 2 * LD;
+#pragma unroll
+    for (int c = 0; c < NXC; ++c) {
+      const int ii = lane + 32 * c;
+      if (NX % 32 != 0 && ii >= NX) break;
+      const int i = ii + 1;
+      double v = (double)src[2 * pad8(ii >> 1) + (ii & 1)] * scale;
+      if constexpr (ACC) v += p00[i];  // refinement: psi += correction
+      const int ig = (i <= hd) ? i + NX : (i > NX - hd ? i - NX : kNoGhost);
+      p00[i] = v;
+      if (ig != kNoGhost) p00[ig] = v;
+      if (p10) {
+        p10[i] = v;
+        if (ig != kNoGhost) p10[ig] = v;
+      }
+      if (p01) {
+        p01[i] = v;
+        if (ig != kNoGhost) p01[ig] = v;
+      }
+      if (p11) {
+        p11[i] = v;
+        if (ig != kNoGhost) p11[ig] = v;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z transform and y systems (see k_fftz and k_tridiag_t in tbfp_yz.cu)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+template <int T>
+__host__ __device__ constexpr int tri_min_blocks() {
+  return T <= 6 ? 6 : (T <= 8 ? 4 : 3);
+}
+
+
+template <typename V, bool INV, int NZ, bool COH = false>
+__device__ __forceinline__ void fftz_body(V *__restrict__ spec, GridK g, const V *__restrict__ tpz, int bx, int by,
+                                          unsigned char *smz) {
+  constexpr int LOGCPW = ct_lognb(NZ), LOGT = LOGCPW + 3, TJZ = 1 << LOGT;
+  constexpr int ES = z_row_stride(NZ), ROWS = pad8(NZ - 1) + 1;
+  constexpr int NL = (NZ << LOGT) / kNT;  // elements per thread (NZ*TJZ is a multiple of kNT)
+  static_assert((NZ << LOGT) % kNT == 0, "z tile must split evenly over the CTA");
+  V *sm = reinterpret_cast<V *>(smz);
+  V *tw = sm + ES * ROWS;
+  for (int t = threadIdx.x; t < ct_twiddle_len(NZ); t += kNT) tw[t] = tpz[t];
+  const int kx = by;
+  const int j0 = bx << LOGT;
+  const int nj = min(TJZ, g.ny - j0);
+  const int ny = g.ny;
+  V *base = spec + (long)kx * g.R + j0;
+#pragma unroll
+  for (int c = 0; c < NL; ++c) {
+    const int t = threadIdx.x + kNT * c;
+    const int k = t >> LOGT, jj = t & (TJZ - 1);
+    sm[pad8(k) * ES + jj] = (jj < nj) ? ldc<COH>(base + ((long)k * ny + jj)) : mk<V>(0, 0);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  fft_warp<V, NZ, LOGCPW, ES, 1, INV>(sm + (warp << LOGCPW), lane, tw);
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < NL; ++c) {
+    const int t = threadIdx.x + kNT * c;
+    const int k = t >> LOGT, jj = t & (TJZ - 1);
+    if (jj < nj) base[(long)k * ny + jj] = sm[pad8(k) * ES + jj];
+  }
+}
+
+template <typename V, int T>
+__device__ __forceinline__ void tridiag_t_body(V *__restrict__ spec, GridK g, const double *__restrict__ lamx,
+                                               const double *__restrict__ lamz, const double *__restrict__ am,
+                                               const double *__restrict__ ap, const double *__restrict__ dyf,
+                                               double mean_c, double nxnz, unsigned q, int warp,
+                                               unsigned char *smraw) {
+  constexpr int W = 33 * T;
+  const int ny = g.ny, nz = g.nz;
+  const int lane = threadIdx.x & 31;
+  double2 *d0 = reinterpret_cast<double2 *>(smraw) + warp * 2 * W;
+  double2 *d1 = d0 + W;
+  const int nzh = nz / 2 + 1;
+  if (q >= (unsigned)(g.nkx * nzh)) return;  // whole warp leaves; no block-level barrier follows
+  const int kx = (int)(q / (unsigned)nzh), kz = (int)(q - (unsigned)kx * nzh);
+  const int kz2 = (kz == 0) ? 0 : nz - kz;
+  const bool two = kz2 != kz;
+  V *S0 = spec + (long)kx * g.R + (long)kz * ny;
+  V *S1 = spec + (long)kx * g.R + (long)kz2 * ny;
+  using VT = decltype(V::x);
+  auto st = [](double2 v) { return mk<V>((VT)v.x, (VT)v.y); };
+  // row e lives in lane e / T at slot (e mod T)*33 + lane; padding rows are zero
+#pragma unroll
+  for (int c = 0; c < T; ++c) {
+    const int e = lane + 32 * c;
+    const int l = e / T, sl = (e - l * T) * 33 + l;
+    if (e < ny) {
+      if constexpr (sizeof(V) == sizeof(double2)) {
+        cp_async16(d0 + sl, S0 + e);
+        if (two) cp_async16(d1 + sl, S1 + e);
+      } else {
+        const V v0 = S0[e];
+        d0[sl] = mk<double2>((double)v0.x, (double)v0.y);
+        if (two) {
+          const V v1 = S1[e];
+          d1[sl] = mk<double2>((double)v1.x, (double)v1.y);
+        }
+      }
+    } else {
+      d0[sl] = mk<double2>(0.0, 0.0);
+      d1[sl] = mk<double2>(0.0, 0.0);
+    }
+  }
+  const double lam = lamx[kx + g.kx0] + lamz[kz];
+  const bool pin = (kx + g.kx0 == 0 && kz == 0);
+  const int s0 = lane * T;
+  if constexpr (sizeof(V) == sizeof(double2)) cp_async_wait_all();
+  __syncwarp();
+
+  if (pin) {  // single system: pinned serial Thomas (as k_tridiag), factors in d1
+    double *cpin = reinterpret_cast<double *>(d1);
+    auto slot = [&](int e) { return (e % T) * 33 + e / T; };
+    if (lane == 0) {
+      double ct_p = 0.0;
+      double2 dt_p = mk<double2>(0.0, 0.0);
+      for (int e = 0; e < ny; ++e) {
+        const int sl = slot(e);
+        double ct = 0.0;
+        double2 dt = mk<double2>(0.0, 0.0);
+        if (e < ny - 1) {
+          const double a = am[e], c = ap[e];
+          const double2 f = d0[sl];
+          const double gi = 1.0 / ((lam - a - c) - a * ct_p);
+          ct = c * gi;
+          dt = mk<double2>((f.x - a * dt_p.x) * gi, (f.y - a * dt_p.y) * gi);
+        }
+        cpin[sl] = ct;
+        d0[sl] = dt;
+        ct_p = ct;
+        dt_p = dt;
+      }
+      double2 xn = d0[slot(ny - 1)];
+      for (int e = ny - 2; e >= 0; --e) {
+        const int sl = slot(e);
+        const double c = cpin[sl];
+        xn = mk<double2>(d0[sl].x - c * xn.x, d0[sl].y - c * xn.y);
+        d0[sl] = xn;
+      }
+    }
+    __syncwarp();
+    double sx = 0.0, sy = 0.0;
+    for (int e = lane; e < ny; e += 32) {
+      const double2 v = d0[slot(e)];
+      sx += v.x * dyf[e];
+      sy += v.y * dyf[e];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sx += __shfl_xor_sync(0xffffffffu, sx, o);
+      sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    const double subx = sx * mean_c * nxnz, suby = sy * mean_c * nxnz;
+    for (int e = lane; e < ny; e += 32) {
+      const int sl = slot(e);
+      S0[e] = st(mk<double2>(d0[sl].x - subx, d0[sl].y - suby));
+    }
+    return;
+  }
+
+  // forward elimination within the lane's block (padding rows: diagonal one)
+  double at_r[T], ct_r[T];
+  double at_p = -1.0, ct_p = 0.0;
+  double2 p0 = mk<double2>(0.0, 0.0), p1 = mk<double2>(0.0, 0.0);
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    const bool real = s0 + t < ny;  // off-diagonals zero, diagonal one on padding rows
+    const double a = real ? am[s0 + t] : 0.0, c = real ? ap[s0 + t] : 0.0;
+    const double dg = real ? lam : 1.0;
+    const int sl = t * 33 + lane;
+    const double gi = rcp_nr((dg - a - c) - a * ct_p);
+    const double2 f0 = d0[sl], f1 = d1[sl];
+    p0 = mk<double2>((f0.x - a * p0.x) * gi, (f0.y - a * p0.y) * gi);
+    p1 = mk<double2>((f1.x - a * p1.x) * gi, (f1.y - a * p1.y) * gi);
+    d0[sl] = p0;
+    d1[sl] = p1;
+    at_p = -a * at_p * gi;
+    ct_p = c * gi;
+    at_r[t] = at_p;
+    ct_r[t] = ct_p;
+  }
+  // running backward pass: x_s = hd - ha x_{s-1} - hc x_e
+  double ha = 0.0, hc = -1.0;
+  double2 h0 = mk<double2>(0.0, 0.0), h1 = mk<double2>(0.0, 0.0);
+  if constexpr (T >= 2) {
+    h0 = d0[(T - 2) * 33 + lane];
+    h1 = d1[(T - 2) * 33 + lane];
+    ha = at_r[T - 2];
+    hc = ct_r[T - 2];
+#pragma unroll
+    for (int t = T - 3; t >= 0; --t) {
+      const double2 v0 = d0[t * 33 + lane], v1 = d1[t * 33 + lane];
+      const double ct = ct_r[t];
+      h0 = mk<double2>(v0.x - ct * h0.x, v0.y - ct * h0.y);
+      h1 = mk<double2>(v1.x - ct * h1.x, v1.y - ct * h1.y);
+      ha = at_r[t] - ct * ha;
+      hc = -ct * hc;
+    }
+  }
+  // reduced equation of this lane: A y_{l-1} + B y_l + C y_{l+1} = D
+  const double ha_n = shdn(ha, 1), hc_n = shdn(hc, 1);
+  const double h0x = shdn(h0.x, 1), h0y = shdn(h0.y, 1), h1x = shdn(h1.x, 1), h1y = shdn(h1.y, 1);
+  const double at_e = at_r[T - 1], ct_e = ct_r[T - 1];
+  double A = at_e, B = 1.0, C = 0.0;
+  double D[4] = {p0.x, p0.y, p1.x, p1.y};
+  if (lane < 31) {
+    B = 1.0 - ct_e * ha_n;
+    C = -ct_e * hc_n;
+    D[0] -= ct_e * h0x;
+    D[1] -= ct_e * h0y;
+    D[2] -= ct_e * h1x;
+    D[3] -= ct_e * h1y;
+  }
+  // parallel cyclic reduction over the 32 reduced equations
+#pragma unroll
+  for (int h = 1; h < 32; h <<= 1) {
+    const double iB = rcp_nr(B);
+    double Am = shup(A, h), iBm = shup(iB, h), Cm = shup(C, h);
+    double Ap = shdn(A, h), iBp = shdn(iB, h), Cp = shdn(C, h);
+    double Dm[4], Dp[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      Dm[c] = shup(D[c], h);
+      Dp[c] = shdn(D[c], h);
+    }
+    const bool lo = lane < h, hi = lane + h >= 32;
+    const double k1 = lo ? 0.0 : A * iBm, k2 = hi ? 0.0 : C * iBp;
+    if (lo) Am = Cm = 0.0;
+    if (hi) Ap = Cp = 0.0;
+    B = B - k1 * Cm - k2 * Ap;
+    A = -k1 * Am;
+    C = -k2 * Cp;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) D[c] = D[c] - k1 * Dm[c] - k2 * Dp[c];
+  }
+  const double iBf = rcp_nr(B);
+  double y[4], ys[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) y[c] = D[c] * iBf;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double v = shup(y[c], 1);  // every lane takes part in the shuffle
+    ys[c] = (lane == 0) ? 0.0 : v;
+  }
+  double2 x0 = mk<double2>(y[0], y[1]), x1 = mk<double2>(y[2], y[3]);
+  d0[(T - 1) * 33 + lane] = x0;
+  d1[(T - 1) * 33 + lane] = x1;
+#pragma unroll
+  for (int t = T - 2; t >= 0; --t) {
+    const int sl = t * 33 + lane;
+    const double a = at_r[t], c = ct_r[t];
+    const double2 v0 = d0[sl], v1 = d1[sl];
+    x0 = mk<double2>(v0.x - a * ys[0] - c * x0.x, v0.y - a * ys[1] - c * x0.y);
+    x1 = mk<double2>(v1.x - a * ys[2] - c * x1.x, v1.y - a * ys[3] - c * x1.y);
+    d0[sl] = x0;
+    d1[sl] = x1;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < T; ++c) {
+    const int e = lane + 32 * c;
+    if (e < ny) {
+      const int l = e / T, sl = (e - l * T) * 33 + l;
+      S0[e] = st(d0[sl]);
+      if (two) S1[e] = st(d1[sl]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Velocity correction with the continuity check (see k_correct_div in tbfp_correct.cu)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void block_max_atomic(double v, unsigned long long *out) {
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) v = nanmax_nonneg(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = nanmax_nonneg(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (l == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// Out-of-place correction fused with the continuity check.  Grid (x tiles of
+// 128, y chunks of kJC rows, nz); a thread owns column (i, k) of a y chunk and
+// walks it in j with one pointer per array and neighbour, so the lower y face
+// of a cell is the upper face computed one step before.  Every thread computes
+// both of its x faces (the lower one is the upper face of cell i-1, or of cell
+// nx at i = 1: the periodic image), which keeps the warp free of divergent
+// recomputation.  The periodic duplicates ux(0)=ux(nx), uz(.,.,0)=uz(.,.,nz) are
+// the equated values of vfield.f90:124-189 and the uy wall faces are copied
+// through.  |div u| (auxiliaryRoutines.f90:71-75) is reduced per block and
+// folded into *maxdiv with one atomic.
+constexpr int kJC = 32;
+
+// Face update of makeVelocityDivFree FAST for one face: u - r*(invrho0*dpr + (invrho-invrho0)*dpr0),
+// dpr = (psi+ - psi)*idc, dpr0 = (2(pn+ - pn) - (po+ - po))*idc [- 2 st^n + st^{n-1}].
+__device__ __forceinline__ double face_update(double u, double r, double ir0, double irp, double irc, double idc,
+                                              double ps_p, double ps_c, double pn_p, double pn_c, double po_p,
+                                              double po_c, double st) {
+  const double invrho = 0.5 * (irp + irc);
+  const double dpr = (ps_p - ps_c) * idc;
+  const double dpr0 = (2.0 * (pn_p - pn_c) - (po_p - po_c)) * idc - st;
+  return u - r * (ir0 * dpr + (invrho - ir0) * dpr0);
+}
+
+
+template <bool ST, bool COH = false>
+__device__ __forceinline__ void correct_div_body(CorrArgs a, GridK g, unsigned long long *__restrict__ maxdiv, int bx,
+                                                 int by, int bz, int tx) {
+  const int i = bx * 128 + tx + 1;
+  const int k = bz + 1;
+  const int j0 = by * kJC + 1, j1 = min(j0 + kJC - 1, g.ny);
+  const bool valid = i <= g.nx;
+  const int ic = valid ? i : g.nx;  // clamped index keeps every load in bounds
+  const int km = (k == 1 && !g.slab) ? g.nz : k - 1;
+  // 32-bit element offsets (tbfp_create checks every array has < 2^31 elements)
+  const int pjs = (int)a.Lpsi.sj, rjs = (int)a.Lrho.sj;
+  const int xjs = (int)a.Lux.sj, yjs = (int)a.Luy.sj, zjs = (int)a.Luz.sj;
+  // offset of the lower x neighbour's centre: cell i-1, or cell nx at i = 1
+  const int xo = (ic == 1) ? g.nx - 1 : -1;
+  int op = (int)at(a.Lpsi, ic, j0, k), oq = (int)at(a.Lrho, ic, j0, k);
+  const int pz = (int)a.Lpsi.sk, pm = (km - k) * (int)a.Lpsi.sk;
+  const int qz = (int)a.Lrho.sk, qm = (km - k) * (int)a.Lrho.sk;
+  int ox = (int)at(a.Lux, ic, j0, k), oy = (int)at(a.Luy, ic, j0, k), oz = (int)at(a.Luz, ic, j0, k);
+  const int zm = (km - k) * (int)a.Luz.sk;
+  const double *__restrict__ ps = a.psi;
+  const double *__restrict__ pn = a.pn;
+  const double *__restrict__ po = a.pnm1;
+  const double *__restrict__ ir = a.irho;
+  const double *__restrict__ uxi = a.uxi;
+  const double *__restrict__ uyi = a.uyi;
+  const double *__restrict__ uzi = a.uzi;
+  double *__restrict__ uxo = a.uxo;
+  double *__restrict__ uyo = a.uyo;
+  double *__restrict__ uzo = a.uzo;
+  const double r = a.r, ir0 = a.invrho0;
+  const double idxc = g.idxc1, idzc = g.idzc1;
+  const double idx = g.idxf[ic - 1], idz = g.idzf[k - 1];
+  // surface-tension terms of one face (zero without surface tension)
+  auto stf = [&](int c, int ii, int jj, int kk) -> double {
+    if constexpr (ST) {
+      const long q = at(a.Lst[c], ii, jj, kk);
+      return 2.0 * a.stn[c][q] - a.sto[c][q];
+    } else return 0.0;
+  };
+
+  // centre values of the current cell, carried along j
+  double psc = ldc<COH>(ps + (op)), pnc = pn[op], poc = po[op], irc = ldc<COH>(ir + (oq));
+  double uym;
+  if (j0 > 1) {
+    uym = face_update(uyi[oy - yjs], r, ir0, irc, ldc<COH>(ir + (oq - rjs)), g.idyc[j0 - 1], psc, ldc<COH>(ps + (op - pjs)), pnc,
+                      pn[op - pjs], poc, po[op - pjs], stf(1, ic, j0 - 1, k));
+  } else {
+    uym = uyi[oy - yjs];
+    if (valid) uyo[oy - yjs] = uym;
+  }
+  double vmax = 0.0;
+  for (int j = j0; j <= j1; ++j) {
+    // every load of this step, issued together
+    const int ow = op + xo, qw = oq + xo;
+    const double psx = ldc<COH>(ps + (op + 1)), pnx = pn[op + 1], pox = po[op + 1], irx = ldc<COH>(ir + (oq + 1));
+    // the lower x face is the upper face of lane - 1; lane 0 computes it
+    const bool lead = (threadIdx.x & 31) == 0;
+    double psw = 0.0, pnw = 0.0, pow_ = 0.0, irw = 0.0, psw1 = 0.0, pnw1 = 0.0, pow1 = 0.0, irw1 = 0.0, ux_w = 0.0;
+    if (lead) {
+      psw = ldc<COH>(ps + (ow));
+      pnw = pn[ow];
+      pow_ = po[ow];
+      irw = ldc<COH>(ir + (qw));
+      psw1 = ldc<COH>(ps + (ow + 1));
+      pnw1 = pn[ow + 1];
+      pow1 = po[ow + 1];
+      irw1 = ldc<COH>(ir + (qw + 1));
+      ux_w = uxi[ox + xo];
+    }
+    const double psy = ldc<COH>(ps + (op + pjs)), pny = pn[op + pjs], poy = po[op + pjs], iry = ldc<COH>(ir + (oq + rjs));
+    const double psz = ldc<COH>(ps + (op + pz)), pnz = pn[op + pz], poz = po[op + pz], irz = ldc<COH>(ir + (oq + qz));
+    const double psm = ldc<COH>(ps + (op + pm)), pnm = pn[op + pm], pom = po[op + pm], irm = ldc<COH>(ir + (oq + qm));
+    const double ux_c = uxi[ox], uy_c = uyi[oy], uz_c = uzi[oz], uz_m = uzi[oz + zm];
+
+    const double uxp = face_update(ux_c, r, ir0, irx, irc, idxc, psx, psc, pnx, pnc, pox, poc, stf(0, ic, j, k));
+    const double uxl = lead ? face_update(ux_w, r, ir0, irw1, irw, idxc, psw1, psw, pnw1, pnw, pow1, pow_,
+                                          stf(0, ic + xo, j, k))
+                            : 0.0;
+    const double uxs = __shfl_up_sync(0xffffffffu, uxp, 1);
+    const double uxm = lead ? uxl : uxs;
+    const double uyp = (j < g.ny) ? face_update(uy_c, r, ir0, iry, irc, g.idyc[j], psy, psc, pny, pnc, poy, poc,
+                                                stf(1, ic, j, k))
+                                  : uy_c;
+    const double uzp = face_update(uz_c, r, ir0, irz, irc, idzc, psz, psc, pnz, pnc, poz, poc, stf(2, ic, j, k));
+    const double uzq = face_update(uz_m, r, ir0, irc, irm, idzc, psc, psm, pnc, pnm, poc, pom, stf(2, ic, j, km));
+    if (valid) {
+      uxo[ox] = uxp;
+      if (i == g.nx) uxo[ox - ic] = uxp;  // ux(0, j, k)
+      uyo[oy] = uyp;
+      uzo[oz] = uzp;
+      if (k == g.nz && !g.slab) uzo[oz - k * (int)a.Luz.sk] = uzp;  // uz(i, j, 0)
+      double dv = (uxp - uxm) * idx;
+      dv = dv + (uyp - uym) * g.idyf[j - 1];
+      dv = dv + (uzp - uzq) * idz;
+      vmax = nanmax_nonneg(vmax, dv);
+    }
+    uym = uyp;
+    psc = psy;
+    pnc = pny;
+    poc = poy;
+    irc = iry;
+    op += pjs;
+    oq += rjs;
+    ox += xjs;
+    oy += yjs;
+    oz += zjs;
+  }
+  block_max_atomic(vmax, maxdiv);
+}
+
+}  // namespace tbfp

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "tbfp_kernels.cuh"
+#include "tbfp_stages.cuh"
 
 namespace tbfp {
 
@@ -17,35 +18,8 @@ namespace tbfp {
 template <typename V, bool INV, int NZ>
 __global__ void __launch_bounds__(kNT, (NZ >= 384 ? 2 : 3)) k_fftz(V *__restrict__ spec, GridK g,
                                                                const V *__restrict__ tpz) {
-  constexpr int LOGCPW = ct_lognb(NZ), LOGT = LOGCPW + 3, TJZ = 1 << LOGT;
-  constexpr int ES = z_row_stride(NZ), ROWS = pad8(NZ - 1) + 1;
-  constexpr int NL = (NZ << LOGT) / kNT;  // elements per thread (NZ*TJZ is a multiple of kNT)
-  static_assert((NZ << LOGT) % kNT == 0, "z tile must split evenly over the CTA");
   extern __shared__ __align__(16) unsigned char smz[];
-  V *sm = reinterpret_cast<V *>(smz);
-  V *tw = sm + ES * ROWS;
-  for (int t = threadIdx.x; t < ct_twiddle_len(NZ); t += kNT) tw[t] = tpz[t];
-  const int kx = blockIdx.y;
-  const int j0 = blockIdx.x << LOGT;
-  const int nj = min(TJZ, g.ny - j0);
-  const int ny = g.ny;
-  V *base = spec + (long)kx * g.R + j0;
-#pragma unroll
-  for (int c = 0; c < NL; ++c) {
-    const int t = threadIdx.x + kNT * c;
-    const int k = t >> LOGT, jj = t & (TJZ - 1);
-    sm[pad8(k) * ES + jj] = (jj < nj) ? base[(long)k * ny + jj] : mk<V>(0, 0);
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  fft_warp<V, NZ, LOGCPW, ES, 1, INV>(sm + (warp << LOGCPW), lane, tw);
-  __syncthreads();
-#pragma unroll
-  for (int c = 0; c < NL; ++c) {
-    const int t = threadIdx.x + kNT * c;
-    const int k = t >> LOGT, jj = t & (TJZ - 1);
-    if (jj < nj) base[(long)k * ny + jj] = sm[pad8(k) * ES + jj];
-  }
+  fftz_body<V, INV, NZ>(spec, g, tpz, blockIdx.x, blockIdx.y, smz);
 }
 
 template <typename V, int NZ>
@@ -103,8 +77,6 @@ void launch_fftz(float2 *spec, const GridK &g, const float2 *tpz, bool inverse, 
 // two right-hand sides and the two coefficient arrays.  The arithmetic is FP64
 // for both spectrum types (float2 spectra are widened on load).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
-__device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 
 // TM > 0: every lane holds at most TM rows and keeps their elimination
 // coefficients at_i, ct_i in registers (shared memory holds only the two
@@ -382,226 +354,14 @@ __global__ void __launch_bounds__(kWPB * 32) k_tridiag(V *__restrict__ spec, Gri
 // per lane and level (1/B, exchanged with the neighbours) in place of two
 // divisions.  The singular (0,0) system keeps the serial pinned path.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double rcp_nr(double x) {
-  double y;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  return fma(y, e, y);
-}
-
-template <int T>
-__host__ __device__ constexpr int tri_min_blocks() {
-  return T <= 6 ? 6 : (T <= 8 ? 4 : 3);
-}
-
 template <typename V, int T>
 __global__ void __launch_bounds__(kWPB * 32, tri_min_blocks<T>()) k_tridiag_t(
     V *__restrict__ spec, GridK g, const double *__restrict__ lamx, const double *__restrict__ lamz,
     const double *__restrict__ am, const double *__restrict__ ap, const double *__restrict__ dyf, double mean_c,
     double nxnz) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int W = 33 * T;
-  const int ny = g.ny, nz = g.nz;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double2 *d0 = reinterpret_cast<double2 *>(smraw) + warp * 2 * W;
-  double2 *d1 = d0 + W;
-  const int nzh = nz / 2 + 1;
-  const unsigned q = blockIdx.x * kWPB + warp;
-  if (q >= (unsigned)(g.nkx * nzh)) return;  // whole warp leaves; no block-level barrier follows
-  const int kx = (int)(q / (unsigned)nzh), kz = (int)(q - (unsigned)kx * nzh);
-  const int kz2 = (kz == 0) ? 0 : nz - kz;
-  const bool two = kz2 != kz;
-  V *S0 = spec + (long)kx * g.R + (long)kz * ny;
-  V *S1 = spec + (long)kx * g.R + (long)kz2 * ny;
-  using VT = decltype(V::x);
-  auto st = [](double2 v) { return mk<V>((VT)v.x, (VT)v.y); };
-  // row e lives in lane e / T at slot (e mod T)*33 + lane; padding rows are zero
-#pragma unroll
-  for (int c = 0; c < T; ++c) {
-    const int e = lane + 32 * c;
-    const int l = e / T, sl = (e - l * T) * 33 + l;
-    if (e < ny) {
-      if constexpr (sizeof(V) == sizeof(double2)) {
-        cp_async16(d0 + sl, S0 + e);
-        if (two) cp_async16(d1 + sl, S1 + e);
-      } else {
-        const V v0 = S0[e];
-        d0[sl] = mk<double2>((double)v0.x, (double)v0.y);
-        if (two) {
-          const V v1 = S1[e];
-          d1[sl] = mk<double2>((double)v1.x, (double)v1.y);
-        }
-      }
-    } else {
-      d0[sl] = mk<double2>(0.0, 0.0);
-      d1[sl] = mk<double2>(0.0, 0.0);
-    }
-  }
-  const double lam = lamx[kx + g.kx0] + lamz[kz];
-  const bool pin = (kx + g.kx0 == 0 && kz == 0);
-  const int s0 = lane * T;
-  if constexpr (sizeof(V) == sizeof(double2)) cp_async_wait_all();
-  __syncwarp();
-
-  if (pin) {  // single system: pinned serial Thomas (as k_tridiag), factors in d1
-    double *cpin = reinterpret_cast<double *>(d1);
-    auto slot = [&](int e) { return (e % T) * 33 + e / T; };
-    if (lane == 0) {
-      double ct_p = 0.0;
-      double2 dt_p = mk<double2>(0.0, 0.0);
-      for (int e = 0; e < ny; ++e) {
-        const int sl = slot(e);
-        double ct = 0.0;
-        double2 dt = mk<double2>(0.0, 0.0);
-        if (e < ny - 1) {
-          const double a = am[e], c = ap[e];
-          const double2 f = d0[sl];
-          const double gi = 1.0 / ((lam - a - c) - a * ct_p);
-          ct = c * gi;
-          dt = mk<double2>((f.x - a * dt_p.x) * gi, (f.y - a * dt_p.y) * gi);
-        }
-        cpin[sl] = ct;
-        d0[sl] = dt;
-        ct_p = ct;
-        dt_p = dt;
-      }
-      double2 xn = d0[slot(ny - 1)];
-      for (int e = ny - 2; e >= 0; --e) {
-        const int sl = slot(e);
-        const double c = cpin[sl];
-        xn = mk<double2>(d0[sl].x - c * xn.x, d0[sl].y - c * xn.y);
-        d0[sl] = xn;
-      }
-    }
-    __syncwarp();
-    double sx = 0.0, sy = 0.0;
-    for (int e = lane; e < ny; e += 32) {
-      const double2 v = d0[slot(e)];
-      sx += v.x * dyf[e];
-      sy += v.y * dyf[e];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      sx += __shfl_xor_sync(0xffffffffu, sx, o);
-      sy += __shfl_xor_sync(0xffffffffu, sy, o);
-    }
-    const double subx = sx * mean_c * nxnz, suby = sy * mean_c * nxnz;
-    for (int e = lane; e < ny; e += 32) {
-      const int sl = slot(e);
-      S0[e] = st(mk<double2>(d0[sl].x - subx, d0[sl].y - suby));
-    }
-    return;
-  }
-
-  // forward elimination within the lane's block (padding rows: diagonal one)
-  double at_r[T], ct_r[T];
-  double at_p = -1.0, ct_p = 0.0;
-  double2 p0 = mk<double2>(0.0, 0.0), p1 = mk<double2>(0.0, 0.0);
-#pragma unroll
-  for (int t = 0; t < T; ++t) {
-    const bool real = s0 + t < ny;  // off-diagonals zero, diagonal one on padding rows
-    const double a = real ? am[s0 + t] : 0.0, c = real ? ap[s0 + t] : 0.0;
-    const double dg = real ? lam : 1.0;
-    const int sl = t * 33 + lane;
-    const double gi = rcp_nr((dg - a - c) - a * ct_p);
-    const double2 f0 = d0[sl], f1 = d1[sl];
-    p0 = mk<double2>((f0.x - a * p0.x) * gi, (f0.y - a * p0.y) * gi);
-    p1 = mk<double2>((f1.x - a * p1.x) * gi, (f1.y - a * p1.y) * gi);
-    d0[sl] = p0;
-    d1[sl] = p1;
-    at_p = -a * at_p * gi;
-    ct_p = c * gi;
-    at_r[t] = at_p;
-    ct_r[t] = ct_p;
-  }
-  // running backward pass: x_s = hd - ha x_{s-1} - hc x_e
-  double ha = 0.0, hc = -1.0;
-  double2 h0 = mk<double2>(0.0, 0.0), h1 = mk<double2>(0.0, 0.0);
-  if constexpr (T >= 2) {
-    h0 = d0[(T - 2) * 33 + lane];
-    h1 = d1[(T - 2) * 33 + lane];
-    ha = at_r[T - 2];
-    hc = ct_r[T - 2];
-#pragma unroll
-    for (int t = T - 3; t >= 0; --t) {
-      const double2 v0 = d0[t * 33 + lane], v1 = d1[t * 33 + lane];
-      const double ct = ct_r[t];
-      h0 = mk<double2>(v0.x - ct * h0.x, v0.y - ct * h0.y);
-      h1 = mk<double2>(v1.x - ct * h1.x, v1.y - ct * h1.y);
-      ha = at_r[t] - ct * ha;
-      hc = -ct * hc;
-    }
-  }
-  // reduced equation of this lane: A y_{l-1} + B y_l + C y_{l+1} = D
-  const double ha_n = shdn(ha, 1), hc_n = shdn(hc, 1);
-  const double h0x = shdn(h0.x, 1), h0y = shdn(h0.y, 1), h1x = shdn(h1.x, 1), h1y = shdn(h1.y, 1);
-  const double at_e = at_r[T - 1], ct_e = ct_r[T - 1];
-  double A = at_e, B = 1.0, C = 0.0;
-  double D[4] = {p0.x, p0.y, p1.x, p1.y};
-  if (lane < 31) {
-    B = 1.0 - ct_e * ha_n;
-    C = -ct_e * hc_n;
-    D[0] -= ct_e * h0x;
-    D[1] -= ct_e * h0y;
-    D[2] -= ct_e * h1x;
-    D[3] -= ct_e * h1y;
-  }
-  // parallel cyclic reduction over the 32 reduced equations
-#pragma unroll
-  for (int h = 1; h < 32; h <<= 1) {
-    const double iB = rcp_nr(B);
-    double Am = shup(A, h), iBm = shup(iB, h), Cm = shup(C, h);
-    double Ap = shdn(A, h), iBp = shdn(iB, h), Cp = shdn(C, h);
-    double Dm[4], Dp[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      Dm[c] = shup(D[c], h);
-      Dp[c] = shdn(D[c], h);
-    }
-    const bool lo = lane < h, hi = lane + h >= 32;
-    const double k1 = lo ? 0.0 : A * iBm, k2 = hi ? 0.0 : C * iBp;
-    if (lo) Am = Cm = 0.0;
-    if (hi) Ap = Cp = 0.0;
-    B = B - k1 * Cm - k2 * Ap;
-    A = -k1 * Am;
-    C = -k2 * Cp;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) D[c] = D[c] - k1 * Dm[c] - k2 * Dp[c];
-  }
-  const double iBf = rcp_nr(B);
-  double y[4], ys[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) y[c] = D[c] * iBf;
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const double v = shup(y[c], 1);  // every lane takes part in the shuffle
-    ys[c] = (lane == 0) ? 0.0 : v;
-  }
-  double2 x0 = mk<double2>(y[0], y[1]), x1 = mk<double2>(y[2], y[3]);
-  d0[(T - 1) * 33 + lane] = x0;
-  d1[(T - 1) * 33 + lane] = x1;
-#pragma unroll
-  for (int t = T - 2; t >= 0; --t) {
-    const int sl = t * 33 + lane;
-    const double a = at_r[t], c = ct_r[t];
-    const double2 v0 = d0[sl], v1 = d1[sl];
-    x0 = mk<double2>(v0.x - a * ys[0] - c * x0.x, v0.y - a * ys[1] - c * x0.y);
-    x1 = mk<double2>(v1.x - a * ys[2] - c * x1.x, v1.y - a * ys[3] - c * x1.y);
-    d0[sl] = x0;
-    d1[sl] = x1;
-  }
-  __syncwarp();
-#pragma unroll
-  for (int c = 0; c < T; ++c) {
-    const int e = lane + 32 * c;
-    if (e < ny) {
-      const int l = e / T, sl = (e - l * T) * 33 + l;
-      S0[e] = st(d0[sl]);
-      if (two) S1[e] = st(d1[sl]);
-    }
-  }
+  const int warp = threadIdx.x >> 5;
+  tridiag_t_body<V, T>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, blockIdx.x * kWPB + warp, warp, smraw);
 }
 
 // shared memory of a k_tridiag<V, TM> block: the two right-hand sides per warp,

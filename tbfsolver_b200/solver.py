@@ -611,11 +611,17 @@ class PCG:
 
 class Ensemble:
     """Many independent channels on one GPU (tbfp_ensemble_*): each member has
-    its own grid; one call projects every member.  Plain FP64 members are run
-    as one replayed CUDA graph."""
+    its own grid; one call projects every member, either as a replayed CUDA
+    graph of every member's kernels on a pool of streams (mode "graph"), or as
+    one persistent launch that runs every stage of every member from a device
+    work queue (mode "persistent": FP64, out-of-place members up to
+    nx = 256, nz = 128, ny = 256).  Mode "auto" measures both on the first
+    call and keeps the faster, recorded in the tuning cache file."""
+
+    MODES = {"auto": 0, "graph": 1, "persistent": 2}
 
     def __init__(self, meshes, nstreams: int = 8, precision: str = "fp64", tol: float = 1e-10, max_iter: int = 8,
-                 device: int = -1):
+                 device: int = -1, mode: str = "auto", blocks_per_sm: int = 0):
         self.lib = load()
         self.meshes = list(meshes)
         self._m = [_metrics(g) for g in self.meshes]
@@ -624,6 +630,22 @@ class Ensemble:
         h = C.c_void_p()
         check(self.lib.tbfp_ensemble_create(len(self.meshes), descs, nstreams, C.byref(h)), None)
         self.h = h
+        if mode != "auto" or blocks_per_sm:
+            self.set_mode(mode, blocks_per_sm)
+
+    def set_mode(self, mode: str, blocks_per_sm: int = 0) -> None:
+        check(self.lib.tbfp_ensemble_set_mode(self.h, self.MODES[mode], blocks_per_sm), None)
+
+    def mode(self):
+        """(form in use, its parameter, measured ms of [graph, persistent x1, persistent x2])."""
+        m, p = C.c_int(), C.c_int()
+        ms = (C.c_float * 3)()
+        check(self.lib.tbfp_ensemble_get_mode(self.h, C.byref(m), C.byref(p), ms), None)
+        names = {0: None, 1: "graph", 2: "persistent"}
+        return names[m.value], p.value, [float(x) for x in ms]
+
+    def set_wait_limit(self, polls: int) -> None:
+        check(self.lib.tbfp_ensemble_set_wait_limit(self.h, int(polls)), None)
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -9,7 +9,7 @@
  *
  * Exit status 0 on success.  The grid metrics follow the reference's tanh
  * channel (grid.f90:288-330, gamma 1.5): faces yf(j) = 1 + tanh(g (2j/ny - 1))
- * / tanh(g), centres between faces, ghost centres mirrored across the walls. */
+ * / tanh(g), centres yc(j) = the same map at j - 1/2, j = 0..ny+1. */
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -38,9 +38,8 @@ static void metrics(double *dxf, double *dxc, double *dyf, double *dyc, double *
   for (i = 0; i < NZ; ++i) dzf[i] = *dz;
   for (i = 0; i <= NZ; ++i) dzc[i] = *dz;
   for (i = 0; i <= NY; ++i) yf[i] = 1.0 + tanh(g * (2.0 * i / NY - 1.0)) / tanh(g);
-  for (i = 1; i <= NY; ++i) yc[i] = 0.5 * (yf[i - 1] + yf[i]);
-  yc[0] = 2.0 * yf[0] - yc[1]; /* ghost centres: mirror images across the walls */
-  yc[NY + 1] = 2.0 * yf[NY] - yc[NY];
+  /* centres: the same map at half-integer indices, ghost centres included */
+  for (i = 0; i <= NY + 1; ++i) yc[i] = 1.0 + tanh(g * ((2.0 * i - 1.0) / NY - 1.0)) / tanh(g);
   for (i = 0; i < NY; ++i) dyf[i] = yf[i + 1] - yf[i];
   for (i = 0; i <= NY; ++i) dyc[i] = yc[i + 1] - yc[i];
 }

@@ -53,7 +53,7 @@ def test_ensemble_matches_single_channel_projections():
              synth.small_spec(96, 64, 48, nbubbles=3, rhog=0.05)]
     inps = _members(specs, 11)
     rho0 = 0.05
-    with Ensemble([i.grid for i in inps], nstreams=2) as ens:
+    with Ensemble([i.grid for i in inps], nstreams=2, mode="graph") as ens:
         for rep in range(3):
             if rep == 2:  # new arrays: the graph is captured again
                 inps = _members(specs, 21)
@@ -94,3 +94,91 @@ def test_mixed_ensemble_reaches_tolerance():
                 _, p64, _ = _reference(inp, 0.05)
                 c = p64.a.cpu().numpy()
                 assert np.max(np.abs(a - c)) / np.max(np.abs(c)) < 1e-8
+
+
+def _specs_small():
+    return [synth.small_spec(64, 48, 32, nbubbles=2, rhog=0.05), synth.small_spec(48, 40, 24, nbubbles=1, rhog=0.05),
+            synth.small_spec(96, 64, 48, nbubbles=3, rhog=0.05), synth.small_spec(128, 96, 64, nbubbles=2, rhog=0.05)]
+
+
+def _close(a, b, tol=1e-12):
+    a, b = a.detach().cpu().numpy(), b.detach().cpu().numpy()
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)) < tol
+
+
+def test_persistent_form_matches_single_channel_projections():
+    """One persistent launch (a device work queue over (member, stage, tile))
+    runs the same tile bodies as the standalone kernels, inlined into another
+    kernel: the compiler may contract and order the arithmetic differently, so
+    the results agree with the single-channel ones to rounding (the 1e-12
+    parity bar), on the first call, on a replay and after the arrays change."""
+    specs = _specs_small()
+    inps = _members(specs, 31)
+    with Ensemble([i.grid for i in inps], nstreams=2, mode="persistent") as ens:
+        for rep in range(3):
+            if rep == 2:
+                inps = _members(specs, 41)
+            members = [_io(i) for i in inps]
+            stats = ens.projection(members, inps[0].dt, inps[0].alpha, 0.05)
+            assert ens.mode()[0] == "persistent"
+            for inp, m, st in zip(inps, members, stats):
+                want_st, want_psi, want_u = _reference(inp, 0.05)
+                assert _close(m[0].a, want_psi.a)
+                for a, b in zip(m[5].components(), want_u.components()):
+                    assert _close(Field.like(a, a.a).interior(), Field.like(b, b.a).interior())
+                assert abs(st.max_div - want_st.max_div) < 1e-12 and st.max_div < 1e-9
+
+
+def test_auto_form_is_measured_once_and_cached(tmp_path, monkeypatch):
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("TBFP_TUNE_CACHE", str(cache))
+    specs = _specs_small()
+    inps = _members(specs, 51)
+    members = [_io(i) for i in inps]
+    with Ensemble([i.grid for i in inps], nstreams=2) as ens:
+        ens.projection(members, inps[0].dt, inps[0].alpha, 0.05)
+        form, param, ms = ens.mode()
+    assert form in ("graph", "persistent") and ms[0] > 0 and ms[1] > 0
+    lines = cache.read_text().split()
+    assert len(lines) == 4 and int(lines[1]) == {"graph": 1, "persistent": 2}[form]
+    with Ensemble([i.grid for i in inps], nstreams=2) as ens2:  # same sizes: the choice is read back
+        stats = ens2.projection(members, inps[0].dt, inps[0].alpha, 0.05)
+        f2, p2, ms2 = ens2.mode()
+    assert (f2, p2) == (form, param) and ms2 == [-1.0, -1.0, -1.0]
+    for inp, m, st in zip(inps, members, stats):
+        _, want_psi, _ = _reference(inp, 0.05)
+        assert _close(m[0].a, want_psi.a)
+
+
+def test_persistent_wait_limit_reports_a_timeout():
+    """Failure detection without a fault: with a zero poll budget the first
+    dependency wait of the persistent kernel runs out, the launch stops and the
+    call returns TBFP_ETIMEOUT; with the budget restored the same ensemble
+    projects correctly."""
+    from tbfsolver_b200._native import TBFP_ETIMEOUT, TbfpError
+
+    specs = _specs_small()
+    inps = _members(specs, 61)
+    members = [_io(i) for i in inps]
+    with Ensemble([i.grid for i in inps], nstreams=2, mode="persistent") as ens:
+        ens.set_wait_limit(0)
+        with pytest.raises(TbfpError) as ei:
+            ens.projection(members, inps[0].dt, inps[0].alpha, 0.05)
+        assert ei.value.code == TBFP_ETIMEOUT
+        ens.set_wait_limit(10_000_000)
+        stats = ens.projection(members, inps[0].dt, inps[0].alpha, 0.05)
+        for inp, m, st in zip(inps, members, stats):
+            _, want_psi, _ = _reference(inp, 0.05)
+            assert _close(m[0].a, want_psi.a)
+
+
+def test_persistent_form_needs_out_of_place_members():
+    from tbfsolver_b200._native import TBFP_EUNSUPPORTED, TbfpError
+
+    specs = _specs_small()[:2]
+    inps = _members(specs, 71)
+    members = [(psi, pn, pnm1, rho, u, u) for (psi, pn, pnm1, rho, u, _) in (_io(i) for i in inps)]
+    with Ensemble([i.grid for i in inps], nstreams=2, mode="persistent") as ens:
+        with pytest.raises(TbfpError) as ei:
+            ens.projection(members, inps[0].dt, inps[0].alpha, 0.05)
+        assert ei.value.code == TBFP_EUNSUPPORTED
