@@ -343,6 +343,29 @@ int tbfp_flow_rate_dev(tbfp_handle *h, const double *ux, double *q);
 int tbfp_add_ux(tbfp_handle *h, double *ux, double uf);
 int tbfp_add_ux_dev(tbfp_handle *h, double *ux, double uf);
 
+/* --- surface tension ---------------------------------------------------- */
+/* computeSurfaceTension (VOF.f90:1872-2002): the face force st = sigma * k_f *
+   (c(Q) - c(P)) / dc on every face, from the volume fraction c (a cell field
+   with rho's layout, hd_rho; ghosts not read: x and z wrap, the walls copy).
+   Interface cells as the reference's: mixed eps <= c <= 1-eps, full
+   c >= 1-eps (eps = 1e-12), a full cell with an empty 6-neighbour counts as
+   mixed with c = 1-2 eps; k_f is the mean curvature of the face's two cells if
+   both are mixed, else the mixed one's, else 0.  The curvature of a mixed cell
+   is the generalised height-function estimate (computeBlockCurvature,
+   :2070-2290) computed over the whole grid rather than per bubble block: nine
+   height columns across the cell in the largest normal direction (then the
+   second, the third), each walking at most 6 cells toward the full and the
+   empty phase and stopping at the walls; a cell with no valid direction gets
+   0 where the reference fits a parabola.  Positive for a bubble (c = 1 inside):
+   2/R on a sphere.  kappa: NULL, or the curvature as a cell field (rho's layout;
+   y ghost rows 0).  st_x, st_y, st_z: the staggered components with halo hd_st,
+   every element written (x and z halos periodic; wall faces and y ghost rows
+   0), ready for the st_n / st_nm1 arguments of the projection. */
+int tbfp_surface_tension(tbfp_handle *h, const double *c, double sigma, double *kappa, double *st_x, double *st_y,
+                         double *st_z);
+int tbfp_surface_tension_dev(tbfp_handle *h, const double *c, double sigma, double *kappa, double *st_x,
+                             double *st_y, double *st_z);
+
 /* --- slab form: one channel split over several GPUs --------------------- */
 /* One rank's share of a channel split over P ranks (the reference's pencil
    decomposition with py = 1, pencilDec.f90:359-562): in physical space the z

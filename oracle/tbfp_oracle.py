@@ -1211,3 +1211,223 @@ def momentum_predictor(mesh: Mesh, ux: FField, uy: FField, uz: FField, c: FField
         else:
             t[...] = t + invrho0 * r * s
     return phi
+
+
+# ---------------------------------------------------------------------------
+# Surface tension: height-function curvature and the face force
+# (computeSurfaceTension / computeBlockST, VOF.f90:1872-2002; curvature
+# computeBlockCurvature / hfColumn, VOF.f90:2070-2290, Popinet 2009).
+#
+# A grid-wide restatement.  The reference works on per-bubble blocks whose
+# bounds stop the height columns and falls back to a parabolic fit through
+# interface centroids when no direction gives nine valid columns; here the
+# columns walk at most L cells each way over the whole grid, and a cell with no
+# valid direction gets curvature 0.  The interface cells, the face force and the
+# averaging of the curvature onto the faces follow the reference:
+#   mixed: eps <= c <= 1-eps; full: c >= 1-eps (VOF.f90:1094-1108);
+#   a full cell with an empty 6-neighbour becomes mixed with c = 1-2 eps
+#   (search_full_interface_cells, :672-726);
+#   st_d = sigma * k_f * (c(Q) - c(P)) / dc on the face between P and Q, k_f the
+#   mean of the two cells' curvatures if both are mixed, else the mixed one's,
+#   else 0 (computeBlockST, :1904-1996).
+# Arrays are dense interior arrays [k, j, i] (0-based); dyf[0..ny-1] = dyf(1..ny),
+# dyc[0..ny] = dyc(1..ny+1) as in the library descriptor.
+# ---------------------------------------------------------------------------
+ST_EPS = 1e-12
+ST_COLUMN = 6  # cells a height column may walk from its start cell, each way
+
+
+def st_classify(c: np.ndarray, eps: float = ST_EPS):
+    """(c', mixed, full) after the promotion of full interface cells."""
+    mixed0 = (c >= 0.0 + eps) & (c <= 1.0 - eps)
+    full0 = c >= 1.0 - eps
+    empty0 = ~full0 & ~mixed0
+    nb_empty = np.zeros_like(full0)
+    for ax in (0, 2):  # z and x periodic
+        nb_empty |= np.roll(empty0, 1, axis=ax) | np.roll(empty0, -1, axis=ax)
+    # y: the ghost rows copy the wall cells, so a wall cell's outer neighbour is itself
+    up = np.concatenate([empty0[:, 1:, :], empty0[:, -1:, :]], axis=1)
+    dn = np.concatenate([empty0[:, :1, :], empty0[:, :-1, :]], axis=1)
+    nb_empty |= up | dn
+    promote = full0 & nb_empty
+    cp = np.where(promote, 1.0 - 2.0 * eps, c)
+    return cp, mixed0 | promote, full0 & ~promote
+
+
+def st_curvature(cp, mixed, full, dx, dz, dyf, dyc, L: int = ST_COLUMN):
+    """Height-function curvature at the mixed cells (0 elsewhere).  Positive for a
+    bubble (c = 1 inside): 2/R on a sphere of radius R."""
+    nz, ny, nx = cp.shape
+    n_ = (nx, ny, nz)
+    empty = ~mixed & ~full
+    yf0 = np.zeros(ny + 1)  # face positions, sequential sums of dyf
+    acc = 0.0
+    for m in range(ny):
+        acc = acc + dyf[m]
+        yf0[m + 1] = acc
+    w = (1.0, 2.0, 1.0)
+
+    def cell(ijk):  # wrap x, z; None outside the walls in y
+        i, j, k = ijk
+        if j < 0 or j >= ny:
+            return None
+        return (k % nz, j, i % nx)
+
+    def cyc(j):  # clamped y index
+        return min(max(j, 0), ny - 1)
+
+    def ydist(jm, jp):
+        s = 0.0
+        for J in range(jm + 1, jp + 1):
+            s = s + dyc[J]
+        return s
+
+    def face_pos(d, q):  # position of face q (0-based: lower face of cell q) along d
+        if d == 0:
+            return q * dx
+        if d == 2:
+            return q * dz
+        return yf0[q]
+
+    def width(d, q):
+        return dx if d == 0 else (dz if d == 2 else dyf[q])
+
+    kap = np.zeros_like(cp)
+    ks, js, is_ = np.nonzero(mixed)
+    for k, j, i in zip(ks, js, is_):
+        # normal: central differences smoothed over the transverse 3x3 (weights 1,2,1)
+        nx_ = 0.0
+        ny_ = 0.0
+        nz_ = 0.0
+        for b in range(3):
+            for e in range(3):
+                jj = cyc(j + b - 1)
+                nx_ = nx_ + w[b] * w[e] * (cp[(k + e - 1) % nz, jj, (i + 1) % nx] - cp[(k + e - 1) % nz, jj, (i - 1) % nx])
+        jm, jp = cyc(j - 1), cyc(j + 1)
+        for a in range(3):
+            for e in range(3):
+                ny_ = ny_ + w[a] * w[e] * (cp[(k + e - 1) % nz, jp, (i + a - 1) % nx] - cp[(k + e - 1) % nz, jm, (i + a - 1) % nx])
+        for a in range(3):
+            for b in range(3):
+                jj = cyc(j + b - 1)
+                nz_ = nz_ + w[a] * w[b] * (cp[(k + 1) % nz, jj, (i + a - 1) % nx] - cp[(k - 1) % nz, jj, (i + a - 1) % nx])
+        nvec = [nx_ / (2.0 * dx), (ny_ / ydist(jm, jp)) if jp > jm else 0.0, nz_ / (2.0 * dz)]
+        order = []
+        mag = [abs(v) for v in nvec]
+        for _ in range(3):  # maxloc: the first largest remaining
+            best = -1
+            for d in range(3):
+                if d in order:
+                    continue
+                if best < 0 or mag[d] > mag[best]:
+                    best = d
+            order.append(best)
+        P = (i, j, k)
+        for d in order:
+            s = 1 if nvec[d] >= 0.0 else -1
+            t1, t2 = [x for x in (0, 1, 2) if x != d]
+            F = np.zeros((3, 3))
+            ok = True
+            for a in (-1, 0, 1):
+                for b in (-1, 0, 1):
+                    st0 = list(P)
+                    st0[t1] += a
+                    st0[t2] += b
+                    if cell(tuple(st0)) is None:
+                        ok = False
+                        break
+                    q0 = st0[d]
+
+                    def at(t):
+                        x = list(st0)
+                        x[d] = q0 + s * t
+                        return cell(tuple(x))
+
+                    tf = te = -1
+                    for t in range(L + 1):
+                        cc = at(t)
+                        if cc is None:
+                            break
+                        if full[cc]:
+                            tf = t
+                            break
+                    for t in range(L + 1):
+                        cc = at(-t)
+                        if cc is None:
+                            break
+                        if empty[cc]:
+                            te = t
+                            break
+                    if tf < 0 or te < 0:
+                        ok = False
+                        break
+                    hsum = 0.0
+                    for t in range(-te, tf + 1):
+                        cc = at(t)
+                        qq = q0 + s * t
+                        hsum = hsum + cp[cc] * width(d, qq % n_[d] if d != 1 else qq)
+                    qf = q0 + s * tf
+                    xf_ = face_pos(d, qf + 1) if s > 0 else face_pos(d, qf)
+                    F[a + 1, b + 1] = xf_ - s * hsum
+                if not ok:
+                    break
+            if not ok:
+                continue
+
+            def spacing(tdir, p):
+                if tdir == 0:
+                    return dx, dx
+                if tdir == 2:
+                    return dz, dz
+                return dyc[p], dyc[p + 1]
+
+            h1m, h1p = spacing(t1, P[t1])
+            h2m, h2p = spacing(t2, P[t2])
+            den1 = h1p * h1m * (h1p + h1m)
+            den2 = h2p * h2m * (h2p + h2m)
+            d1 = (h1m * h1m * F[2, 1] - h1p * h1p * F[0, 1] + (h1p * h1p - h1m * h1m) * F[1, 1]) / den1
+            d11 = 2.0 * (h1m * F[2, 1] - (h1p + h1m) * F[1, 1] + h1p * F[0, 1]) / den1
+            d2 = (h2m * h2m * F[1, 2] - h2p * h2p * F[1, 0] + (h2p * h2p - h2m * h2m) * F[1, 1]) / den2
+            d22 = 2.0 * (h2m * F[1, 2] - (h2p + h2m) * F[1, 1] + h2p * F[1, 0]) / den2
+            d12 = (F[2, 2] - F[2, 0] - F[0, 2] + F[0, 0]) / ((h1p + h1m) * (h2p + h2m))
+            num = d11 * (1.0 + d2 * d2) + d22 * (1.0 + d1 * d1) - 2.0 * d1 * d2 * d12
+            g = 1.0 + d1 * d1 + d2 * d2
+            kap[k, j, i] = s * num / (g * np.sqrt(g))
+            break
+    return kap
+
+
+def st_faces(cp, mixed, kap, sigma, dx, dz, dyc):
+    """Face force of computeBlockST on every face: stx[k, j, f] for x faces
+    f = 0..nx (face f between cells f-1 and f, periodic), sty[k, f, i] for
+    f = 0..ny (zero on the walls), stz[f, j, i] for f = 0..nz."""
+    nz, ny, nx = cp.shape
+
+    def kf(kp, mp, kq, mq):
+        return np.where(mp & mq, 0.5 * (kq + kp), np.where(mq, kq, np.where(mp, kp, 0.0)))
+
+    def along(ax, n, dc):
+        lo = [slice(None)] * 3
+        idx_p = np.arange(-1, n) % n  # cell below face f
+        idx_q = np.arange(0, n + 1) % n
+        cp_p, cp_q = np.take(cp, idx_p, axis=ax), np.take(cp, idx_q, axis=ax)
+        mp, mq = np.take(mixed, idx_p, axis=ax), np.take(mixed, idx_q, axis=ax)
+        kp, kq = np.take(kap, idx_p, axis=ax), np.take(kap, idx_q, axis=ax)
+        del lo
+        return sigma * kf(kp, mp, kq, mq) * ((cp_q - cp_p) / dc)
+
+    stx = along(2, nx, dx)
+    stz = along(0, nz, dz)
+    sty = np.zeros((nz, ny + 1, nx))
+    for f in range(1, ny):
+        mp, mq = mixed[:, f - 1, :], mixed[:, f, :]
+        sty[:, f, :] = sigma * kf(kap[:, f - 1, :], mp, kap[:, f, :], mq) * ((cp[:, f, :] - cp[:, f - 1, :]) / dyc[f])
+    return stx, sty, stz
+
+
+def surface_tension(c, sigma, dx, dz, dyf, dyc, eps: float = ST_EPS, L: int = ST_COLUMN):
+    """computeSurfaceTension restated grid-wide: (curvature, stx, sty, stz) from
+    the interior volume fraction c[k, j, i]."""
+    cp, mixed, full = st_classify(c, eps)
+    kap = st_curvature(cp, mixed, full, dx, dz, np.asarray(dyf), np.asarray(dyc), L)
+    return (kap,) + st_faces(cp, mixed, kap, sigma, dx, dz, np.asarray(dyc))

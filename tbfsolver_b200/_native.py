@@ -153,6 +153,8 @@ PROTOTYPES = {
     "tbfp_projection_dev": (C.c_int, [_H, _P, _P, _P, _P, _P, _P, _P, _P, _P, _PP, _PP, _D, _D, _D, _P,
                                       C.POINTER(TbfpStats)]),
     "tbfp_solve_fps_noalloc": (C.c_int, [C.POINTER(TbfpDesc), _P, _P]),
+    "tbfp_surface_tension": (C.c_int, [_H, _P, C.c_double, _P, _P, _P, _P]),
+    "tbfp_surface_tension_dev": (C.c_int, [_H, _P, C.c_double, _P, _P, _P, _P]),
 }
 
 _lib = None

@@ -97,6 +97,9 @@ struct tbfp_handle {
   WallTabs wt{};                           // updateBoundariesV wall spacings and values
   // flow control: dxc(1..nx), dyf(1..ny), dzf(1..nz) on the device, ny*nz row partials + the sum
   double *d_fdxc = nullptr, *d_fdyf = nullptr, *d_fdzf = nullptr, *d_fpart = nullptr;
+  // surface tension (tbfp_surface_tension): tables and dense scratch, made on first use
+  double *d_st_dyc = nullptr, *d_st_yf = nullptr, *d_st_cp = nullptr, *d_st_kap = nullptr, *h_kap = nullptr;
+  unsigned char *d_st_fl = nullptr;
   MgSolver *mg = nullptr;   // MG_MODE hierarchy (tbfp_pcg_setup)
   std::vector<double> mdxf, mdxc, mdyf, mdyc, mdzf, mdzc;  // caller's metrics, kept for tbfp_pcg_setup
   double *h_beta = nullptr, *h_q = nullptr;                // device copies for tbfp_pcg_solve
@@ -1622,6 +1625,65 @@ int tbfp_add_ux(tbfp_handle *h, double *ux, double uf) {
   if ((rc = d2h(h, ux, h->h_ux, h->n_ux))) return rc;
   TBFP_CK(h, cudaStreamSynchronize(h->stream));
   return finish(h, "tbfp_add_ux");
+}
+
+// ---------------------------------------------------------------------------
+// surface tension (computeSurfaceTension, VOF.f90:1872-2002), grid-wide
+// ---------------------------------------------------------------------------
+int tbfp_surface_tension_dev(tbfp_handle *h, const double *c, double sigma, double *kappa, double *st_x,
+                             double *st_y, double *st_z) {
+  int rc = check_ptrs(h, {c, st_x, st_y, st_z});
+  if (rc) return rc;
+  if (h->slab) return set_err(h, TBFP_EINVAL, "tbfp_surface_tension: not available on a slab handle");
+  if (!std::isfinite(sigma)) return set_err(h, TBFP_EINVAL, "tbfp_surface_tension: sigma must be finite");
+  cudaSetDevice(h->device);
+  const long n = (long)h->nx * h->ny * h->nz;
+  if (!h->d_st_cp) {
+    std::vector<double> dyc(h->mdyc.begin(), h->mdyc.end()), yf(h->ny + 1, 0.0);
+    double acc = 0.0;
+    for (int m = 0; m < h->ny; ++m) {  // face positions: sequential sums of dyf
+      acc = acc + h->mdyf[m];
+      yf[m + 1] = acc;
+    }
+    if ((rc = upload(h, &h->d_st_dyc, dyc)) || (rc = upload(h, &h->d_st_yf, yf)) ||
+        (rc = dev_alloc(h, &h->d_st_cp, (size_t)n)) || (rc = dev_alloc(h, &h->d_st_kap, (size_t)n)) ||
+        (rc = dev_alloc(h, &h->d_st_fl, (size_t)n)))
+      return rc;
+  }
+  StGrid g{};
+  g.nx = h->nx;
+  g.ny = h->ny;
+  g.nz = h->nz;
+  g.dx = h->dx_fft;
+  g.dz = h->dz_fft;
+  g.dyf = h->d_dyf;
+  g.dyc = h->d_st_dyc;
+  g.yf = h->d_st_yf;
+  launch_surface_tension(c, h->Lrho, g, 1e-12, sigma, h->d_st_cp, h->d_st_fl, h->d_st_kap, kappa, h->Lrho,
+                         (long)h->n_rho, st_x, h->Lst[0], (long)h->n_st[0], st_y, h->Lst[1], (long)h->n_st[1], st_z,
+                         h->Lst[2], (long)h->n_st[2], h->stream);
+  return finish(h, "tbfp_surface_tension");
+}
+
+int tbfp_surface_tension(tbfp_handle *h, const double *c, double sigma, double *kappa, double *st_x, double *st_y,
+                         double *st_z) {
+  int rc = check_ptrs(h, {c, st_x, st_y, st_z});
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  if ((rc = ensure_host_bufs(h, true))) return rc;
+  if (kappa && !h->h_kap && (rc = dev_alloc(h, &h->h_kap, h->n_rho))) return rc;
+  if ((rc = h2d(h, h->h_rho, c, h->n_rho))) return rc;
+  const unsigned fl = h->flags;
+  h->flags |= TBFP_FLAG_ASYNC;
+  rc = tbfp_surface_tension_dev(h, h->h_rho, sigma, kappa ? h->h_kap : nullptr, h->h_st[0], h->h_st[1], h->h_st[2]);
+  h->flags = fl;
+  if (rc) return rc;
+  if ((rc = d2h(h, st_x, h->h_st[0], h->n_st[0])) || (rc = d2h(h, st_y, h->h_st[1], h->n_st[1])) ||
+      (rc = d2h(h, st_z, h->h_st[2], h->n_st[2])))
+    return rc;
+  if (kappa && (rc = d2h(h, kappa, h->h_kap, h->n_rho))) return rc;
+  TBFP_CK(h, cudaStreamSynchronize(h->stream));
+  return TBFP_OK;
 }
 
 int tbfp_pcg_setup(tbfp_handle *h, const tbfp_mg_params *p) {

@@ -373,6 +373,22 @@ void launch_add_pressure_grad(const double *uxi, const double *uyi, const double
                               Lay Lrho, const GridK &g, const double *idxc, const double *idzc, double dta,
                               cudaStream_t st);
 
+// Surface tension (tbfp_surface.cu): grid constants; dyf[0..ny-1] = dyf(1..ny),
+// dyc[0..ny] = dyc(1..ny+1), yf[0..ny] the y face positions as sequential sums
+// of dyf from yf[0] = 0 (device tables).
+struct StGrid {
+  int nx, ny, nz;
+  double dx, dz;
+  const double *dyf, *dyc, *yf;
+};
+// c: volume fraction (layout Lc); cp, fl, kap: dense scratch (c after the
+// promotion of full interface cells, class bits 1 mixed / 2 full, curvature);
+// kap_out (NULL or layout Lk, nk elements); sx, sy, sz: the three staggered
+// st arrays (nsx, nsy, nsz elements).
+void launch_surface_tension(const double *c, Lay Lc, const StGrid &g, double eps, double sigma, double *cp,
+                            unsigned char *fl, double *kap, double *kap_out, Lay Lk, long nk, double *sx, Lay Lx,
+                            long nsx, double *sy, Lay Ly, long nsy, double *sz, Lay Lz, long nsz, cudaStream_t st);
+
 // per-file parts of prepare_kernels()
 cudaError_t prepare_xfft_kernels();
 cudaError_t prepare_yz_kernels();

@@ -296,6 +296,19 @@ class VOF:
                                                   mu.address() if mu is not None else None), sv.h)
 
 
+def compute_surface_tension(solver: FastPoissonSolver, c: Field, sigma: float, st: VField,
+                            kappa: Field | None = None) -> None:
+    """computeSurfaceTension (VOF.f90:1872-2002) on the grid: the face force
+    sigma * k_f * grad c into st (the three staggered components with halo
+    hd_st), from the volume fraction c (rho's layout) and the height-function
+    curvature (also into kappa when given).  See include/tbfp.h for the method."""
+    fields = [c, *st.components()] + ([kappa] if kappa is not None else [])
+    dev = _placement(fields)
+    fn = solver.lib.tbfp_surface_tension_dev if dev else solver.lib.tbfp_surface_tension
+    check(fn(solver.h, c.address(), float(sigma), kappa.address() if kappa is not None else None, st.ux.address(),
+             st.uy.address(), st.uz.address()), solver.h)
+
+
 class MomentumEqn:
     """The momentum predictor of FAST_MODE (momentumEqnCTOR, momentumEqn.f90:98-157;
     solveMomentumEqn :161-194 without its closing updateBoundariesV) on a
