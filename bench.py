@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-mg", action="store_true", help="skip the MG_MODE leg")
     ap.add_argument("--no-vof", action="store_true", help="skip the material-properties leg")
     ap.add_argument("--no-momentum", action="store_true", help="skip the momentum-predictor leg")
+    ap.add_argument("--no-st", action="store_true", help="skip the surface-tension leg")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the legs on the other workloads (mixed 1024x512x512, MG 256x256x128, ensemble)")
     return ap.parse_args()
@@ -770,6 +771,31 @@ def main_line(args, world, rank, local):
                           "rho, flux history, write u, fluxes"}
         del mu_, mu_u
 
+    # surface tension from the sharp volume fraction (interface cells, height-function
+    # curvature, face force), and the projection that reads it (st_n = st_nm1)
+    stres = None
+    if not args.no_st:
+        from tbfsolver_b200.fields import field_shape
+        from tbfsolver_b200.solver import compute_surface_tension
+        stf = VField(*[Field(k, 1, g.nx, g.ny, g.nz, torch.zeros(field_shape(k, 1, g.nx, g.ny, g.nz),
+                                                                dtype=torch.float64, device="cuda"))
+                       for k in ("sx", "sy", "sz")])
+        stn = list(stf.components())
+        sigma = 5e-3  # channel_18/specs/parameters
+        st_ms = _stream_timer(stream, lambda: compute_surface_tension(eqn.solver, inp.c, sigma, stf), args.steps,
+                              args.warmup)
+        pst_ms = _stream_timer(stream, lambda: eqn.projection(psi, pn, pnm1, inp.rho, u_in, dt, alpha, stn, stn,
+                                                              u_out=u_out, want_stats=False),
+                               args.steps, args.warmup)
+        pk0, _ = peaks()
+        sbytes = 32.0 * g.ncells  # read c, write the three face components
+        stres = {"value": g.ncells / (st_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": st_ms,
+                 "alg_bytes": sbytes, "frac": sbytes / (st_ms * 1e-3) / 1e9 / pk0, "launches_per_step": 3,
+                 "projection_with_st_ms": pst_ms,
+                 "note": "interface cells, height-function curvature and st = sigma k_f grad c on every face "
+                         "(200 bubbles); bytes: read c, write st; then one projection reading st at both levels"}
+        del stf, stn
+
     # one whole FAST substep on the device (material properties, setPressGrad,
     # solveMomentumEqn, projection, updateBoundariesV, setFlowRate): what a
     # time step costs once u* stays on the GPU
@@ -880,6 +906,7 @@ def main_line(args, world, rank, local):
         "material_props": vofres,
         "momentum": momres,
         "substep": subres,
+        "surface_tension": stres,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk, "unit": "GB/s",

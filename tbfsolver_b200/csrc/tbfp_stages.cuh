@@ -1,9 +1,14 @@
 // Tile bodies of the FP64/FP32 projection kernels as device functions.
 //
-// Each kernel of the projection (tbfp_xfft.cu, tbfp_yz.cu, tbfp_correct.cu) is
-// a thin __global__ wrapper that calls one of these bodies with its block
+// The z transform, y solve and correction kernels (tbfp_yz.cu, tbfp_correct.cu)
+// are thin __global__ wrappers that call these bodies with their block
 // coordinates; the persistent ensemble kernel (tbfp_ensemble.cu) calls the
-// same bodies for the tiles it takes from its work queue.  COH = true reads
+// same bodies for the tiles it takes from its work queue.  The RHS and the two
+// x transforms (tbfp_xfft.cu) keep kernel-form copies of the same code: called
+// as device functions they ran 15-25 % slower at 512x384x256 (same box, CUDA
+// events; explicit read-only loads did not recover it), so the x-direction
+// bodies below serve the persistent kernel only and must be kept equal to the
+// kernels there.  COH = true reads
 // the buffers that are written during the same launch (1/rho, s, the spectrum,
 // psi) through L2 (ld.global.cg): a persistent kernel consumes data that other
 // blocks of the same launch produced, which the read-only and L1 paths of a
@@ -15,8 +20,18 @@
 
 namespace tbfp {
 
+// Loads of data that the standalone kernel only reads: the read-only path
+// (__ldg; a kernel parameter declared const __restrict__ got it implicitly, a
+// device function's parameter does not).  COH: through L2 (the persistent
+// kernel, where another block of the launch may have written the data).
 template <bool COH, typename X>
 __device__ __forceinline__ X ldc(const X *p) {
+  if constexpr (COH) return __ldcg(p);
+  else return __ldg(p);
+}
+// Loads of data the kernel itself writes elsewhere (the in-place z transform).
+template <bool COH, typename X>
+__device__ __forceinline__ X ldw(const X *p) {
   if constexpr (COH) return __ldcg(p);
   else return *p;
 }
@@ -39,14 +54,15 @@ __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_syn
 template <typename V, int M, int MODE, bool COH = false>
 __device__ __forceinline__ void fftx_fwd_body(XSrc src, GridK g, const V *__restrict__ twx,
                                               const V *__restrict__ tpx, V *__restrict__ spec, int bx,
-                                              unsigned char *smx) {
+                                              unsigned char * /*dynamic shared memory: named below*/) {
+  extern __shared__ __align__(16) unsigned char smx[];  // the launch's dynamic shared memory
   using T = decltype(V::x);
   constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
   constexpr int LD = x_row_stride(M), NX = 2 * M, NXC = (NX + 31) / 32;
   V *sm = reinterpret_cast<V *>(smx);
   V *tw = sm + TJ * LD;
   __shared__ double red[kNW][3];
-  for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = tpx[t];
+  for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = __ldg(tpx + t);
   const int r0 = bx << LOGTJ;
   const int nrows = min(TJ, (int)g.R - r0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -153,7 +169,7 @@ __device__ __forceinline__ void fftx_fwd_body(XSrc src, GridK g, const V *__rest
       } else {
         const int km = M - kk;
         const V a = Z[pad8(kk)], b = Z[pad8(km)];
-        const V wa = twx[kk], wb = twx[km];
+        const V wa = __ldg(twx + kk), wb = __ldg(twx + km);
         V ep = mk<V>(a.x + b.x, a.y - b.y);  // Z_k + conj Z_{M-k}
         V em = mk<V>(a.x - b.x, a.y + b.y);  // Z_k - conj Z_{M-k}
         V t1 = cmul(wa, em);                  // W^k * em
@@ -202,14 +218,14 @@ __device__ __forceinline__ void rhs_body(RhsArgs a, GridK g, double *__restrict_
   const double h = a.rho0 * 0.5;
   const double idxf = g.idxf1, idzf = g.idzf1, idxc = g.idxc1, idzc = g.idzc1;
   // carried along j: centre values and the lower y face
-  double irc = ldc<COH>(ir + (oq)), pc = pn[op], oc = po[op];
-  double irm = ldc<COH>(ir + (oq - rjs)), pm = pn[op - pjs], om = po[op - pjs];
-  double uym = uy[oy - yjs];
+  double irc = ldc<COH>(ir + (oq)), pc = __ldg(pn + (op)), oc = __ldg(po + (op));
+  double irm = ldc<COH>(ir + (oq - rjs)), pm = __ldg(pn + (op - pjs)), om = __ldg(po + (op - pjs));
+  double uym = __ldg(uy + (oy - yjs));
   for (int j = j0; j <= j1; ++j) {
-    const double uxc = ux[ox], uxm = ux[ox - 1], uyc = uy[oy], uzc = uz[oz], uzm = uz[oz - zks];
+    const double uxc = __ldg(ux + (ox)), uxm = __ldg(ux + (ox - 1)), uyc = __ldg(uy + (oy)), uzc = __ldg(uz + (oz)), uzm = __ldg(uz + (oz - zks));
     const double irxp = ldc<COH>(ir + (oq + 1)), irxm = ldc<COH>(ir + (oq - 1)), iryp = ldc<COH>(ir + (oq + rjs)), irzp = ldc<COH>(ir + (oq + rks)), irzm = ldc<COH>(ir + (oq - rks));
-    const double pxp = pn[op + 1], pxm = pn[op - 1], pyp = pn[op + pjs], pzp = pn[op + pks], pzm = pn[op - pks];
-    const double oxp = po[op + 1], oxm = po[op - 1], oyp = po[op + pjs], ozp = po[op + pks], ozm = po[op - pks];
+    const double pxp = __ldg(pn + (op + 1)), pxm = __ldg(pn + (op - 1)), pyp = __ldg(pn + (op + pjs)), pzp = __ldg(pn + (op + pks)), pzm = __ldg(pn + (op - pks));
+    const double oxp = __ldg(po + (op + 1)), oxm = __ldg(po + (op - 1)), oyp = __ldg(po + (op + pjs)), ozp = __ldg(po + (op + pks)), ozm = __ldg(po + (op - pks));
     const double idyf = g.idyf[j - 1], idycp = g.idyc[j], idycm = g.idyc[j - 1];
 
     const double ddx = (uxc - uxm) * idxf;
@@ -263,13 +279,14 @@ __device__ __forceinline__ void rhs_body(RhsArgs a, GridK g, double *__restrict_
 template <typename V, int M, bool ACC, bool COH = false>
 __device__ __forceinline__ void fftx_inv_body(const V *__restrict__ spec, double *__restrict__ psi, Lay Lp, int hd,
                                               GridK g, const V *__restrict__ twx, const V *__restrict__ tpx,
-                                              double scale, int bx, unsigned char *smx) {
+                                              double scale, int bx, unsigned char * /*dynamic shared memory: named below*/) {
+  extern __shared__ __align__(16) unsigned char smx[];  // the launch's dynamic shared memory
   using T = decltype(V::x);
   constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
   constexpr int LD = x_row_stride(M), NX = 2 * M, NXC = (NX + 31) / 32;
   V *sm = reinterpret_cast<V *>(smx);
   V *tw = sm + TJ * LD;
-  for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = tpx[t];
+  for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = __ldg(tpx + t);
   const int r0 = bx << LOGTJ;
   const int nrows = min(TJ, (int)g.R - r0);
   constexpr int NLD = ((M + 1) << LOGTJ);
@@ -296,7 +313,7 @@ __device__ __forceinline__ void fftx_inv_body(const V *__restrict__ spec, double
       } else {
         const int km = M - kk;
         const V a = X[pad8(kk)], b = X[pad8(km)];
-        const V wa = cconj(twx[kk]), wb = cconj(twx[km]);
+        const V wa = cconj(__ldg(twx + kk)), wb = cconj(__ldg(twx + km));
         V ep = mk<V>(a.x + b.x, a.y - b.y);
         V em = mk<V>(a.x - b.x, a.y + b.y);
         V t1 = cmul(wa, em);
@@ -373,7 +390,8 @@ __host__ __device__ constexpr int tri_min_blocks() {
 
 template <typename V, bool INV, int NZ, bool COH = false>
 __device__ __forceinline__ void fftz_body(V *__restrict__ spec, GridK g, const V *__restrict__ tpz, int bx, int by,
-                                          unsigned char *smz) {
+                                          unsigned char * /*dynamic shared memory: named below*/) {
+  extern __shared__ __align__(16) unsigned char smz[];  // the launch's dynamic shared memory
   constexpr int LOGCPW = ct_lognb(NZ), LOGT = LOGCPW + 3, TJZ = 1 << LOGT;
   constexpr int ES = z_row_stride(NZ), ROWS = pad8(NZ - 1) + 1;
   constexpr int NL = (NZ << LOGT) / kNT;  // elements per thread (NZ*TJZ is a multiple of kNT)
@@ -390,7 +408,7 @@ __device__ __forceinline__ void fftz_body(V *__restrict__ spec, GridK g, const V
   for (int c = 0; c < NL; ++c) {
     const int t = threadIdx.x + kNT * c;
     const int k = t >> LOGT, jj = t & (TJZ - 1);
-    sm[pad8(k) * ES + jj] = (jj < nj) ? ldc<COH>(base + ((long)k * ny + jj)) : mk<V>(0, 0);
+    sm[pad8(k) * ES + jj] = (jj < nj) ? ldw<COH>(base + ((long)k * ny + jj)) : mk<V>(0, 0);
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -409,7 +427,8 @@ __device__ __forceinline__ void tridiag_t_body(V *__restrict__ spec, GridK g, co
                                                const double *__restrict__ lamz, const double *__restrict__ am,
                                                const double *__restrict__ ap, const double *__restrict__ dyf,
                                                double mean_c, double nxnz, unsigned q, int warp,
-                                               unsigned char *smraw) {
+                                               unsigned char * /*dynamic shared memory: named below*/) {
+  extern __shared__ __align__(16) unsigned char smraw[];  // the launch's dynamic shared memory
   constexpr int W = 33 * T;
   const int ny = g.ny, nz = g.nz;
   const int lane = threadIdx.x & 31;
@@ -692,38 +711,38 @@ __device__ __forceinline__ void correct_div_body(CorrArgs a, GridK g, unsigned l
   };
 
   // centre values of the current cell, carried along j
-  double psc = ldc<COH>(ps + (op)), pnc = pn[op], poc = po[op], irc = ldc<COH>(ir + (oq));
+  double psc = ldc<COH>(ps + (op)), pnc = __ldg(pn + (op)), poc = __ldg(po + (op)), irc = ldc<COH>(ir + (oq));
   double uym;
   if (j0 > 1) {
-    uym = face_update(uyi[oy - yjs], r, ir0, irc, ldc<COH>(ir + (oq - rjs)), g.idyc[j0 - 1], psc, ldc<COH>(ps + (op - pjs)), pnc,
-                      pn[op - pjs], poc, po[op - pjs], stf(1, ic, j0 - 1, k));
+    uym = face_update(__ldg(uyi + (oy - yjs)), r, ir0, irc, ldc<COH>(ir + (oq - rjs)), g.idyc[j0 - 1], psc, ldc<COH>(ps + (op - pjs)), pnc,
+                      __ldg(pn + (op - pjs)), poc, __ldg(po + (op - pjs)), stf(1, ic, j0 - 1, k));
   } else {
-    uym = uyi[oy - yjs];
+    uym = __ldg(uyi + (oy - yjs));
     if (valid) uyo[oy - yjs] = uym;
   }
   double vmax = 0.0;
   for (int j = j0; j <= j1; ++j) {
     // every load of this step, issued together
     const int ow = op + xo, qw = oq + xo;
-    const double psx = ldc<COH>(ps + (op + 1)), pnx = pn[op + 1], pox = po[op + 1], irx = ldc<COH>(ir + (oq + 1));
+    const double psx = ldc<COH>(ps + (op + 1)), pnx = __ldg(pn + (op + 1)), pox = __ldg(po + (op + 1)), irx = ldc<COH>(ir + (oq + 1));
     // the lower x face is the upper face of lane - 1; lane 0 computes it
     const bool lead = (threadIdx.x & 31) == 0;
     double psw = 0.0, pnw = 0.0, pow_ = 0.0, irw = 0.0, psw1 = 0.0, pnw1 = 0.0, pow1 = 0.0, irw1 = 0.0, ux_w = 0.0;
     if (lead) {
       psw = ldc<COH>(ps + (ow));
-      pnw = pn[ow];
-      pow_ = po[ow];
+      pnw = __ldg(pn + (ow));
+      pow_ = __ldg(po + (ow));
       irw = ldc<COH>(ir + (qw));
       psw1 = ldc<COH>(ps + (ow + 1));
-      pnw1 = pn[ow + 1];
-      pow1 = po[ow + 1];
+      pnw1 = __ldg(pn + (ow + 1));
+      pow1 = __ldg(po + (ow + 1));
       irw1 = ldc<COH>(ir + (qw + 1));
-      ux_w = uxi[ox + xo];
+      ux_w = __ldg(uxi + (ox + xo));
     }
-    const double psy = ldc<COH>(ps + (op + pjs)), pny = pn[op + pjs], poy = po[op + pjs], iry = ldc<COH>(ir + (oq + rjs));
-    const double psz = ldc<COH>(ps + (op + pz)), pnz = pn[op + pz], poz = po[op + pz], irz = ldc<COH>(ir + (oq + qz));
-    const double psm = ldc<COH>(ps + (op + pm)), pnm = pn[op + pm], pom = po[op + pm], irm = ldc<COH>(ir + (oq + qm));
-    const double ux_c = uxi[ox], uy_c = uyi[oy], uz_c = uzi[oz], uz_m = uzi[oz + zm];
+    const double psy = ldc<COH>(ps + (op + pjs)), pny = __ldg(pn + (op + pjs)), poy = __ldg(po + (op + pjs)), iry = ldc<COH>(ir + (oq + rjs));
+    const double psz = ldc<COH>(ps + (op + pz)), pnz = __ldg(pn + (op + pz)), poz = __ldg(po + (op + pz)), irz = ldc<COH>(ir + (oq + qz));
+    const double psm = ldc<COH>(ps + (op + pm)), pnm = __ldg(pn + (op + pm)), pom = __ldg(po + (op + pm)), irm = ldc<COH>(ir + (oq + qm));
+    const double ux_c = __ldg(uxi + (ox)), uy_c = __ldg(uyi + (oy)), uz_c = __ldg(uzi + (oz)), uz_m = __ldg(uzi + (oz + zm));
 
     const double uxp = face_update(ux_c, r, ir0, irx, irc, idxc, psx, psc, pnx, pnc, pox, poc, stf(0, ic, j, k));
     const double uxl = lead ? face_update(ux_w, r, ir0, irw1, irw, idxc, psw1, psw, pnw1, pnw, pow1, pow_,

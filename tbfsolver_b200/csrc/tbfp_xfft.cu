@@ -37,8 +37,142 @@ void launch_recip(const double *rho, double *irho, long n, cudaStream_t st) {
 template <typename V, int M, int MODE>
 __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_fwd(XSrc src, GridK g, const V *__restrict__ twx,
                                                   const V *__restrict__ tpx, V *__restrict__ spec) {
+  using T = decltype(V::x);
+  constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
+  constexpr int LD = x_row_stride(M), NX = 2 * M, NXC = (NX + 31) / 32;
   extern __shared__ __align__(16) unsigned char smx[];
-  fftx_fwd_body<V, M, MODE>(src, g, twx, tpx, spec, blockIdx.x, smx);
+  V *sm = reinterpret_cast<V *>(smx);
+  V *tw = sm + TJ * LD;
+  __shared__ double red[kNW][3];
+  for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = tpx[t];
+  const int r0 = blockIdx.x << LOGTJ;
+  const int nrows = min(TJ, (int)g.R - r0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  V *wsm = sm + warp * RPW * LD;  // this warp's rows
+  T *wsr = reinterpret_cast<T *>(wsm);
+  const bool sums = (MODE == 0) ? src.acc != nullptr : true;
+  const double ctop = (MODE == 1) ? src.acc[0] * src.ctop_scale : 0.0;
+  double sum0 = 0.0, sum1 = 0.0, vmax = 0.0;
+
+#pragma unroll
+  for (int rl = 0; rl < RPW; ++rl) {
+    const int row = warp * RPW + rl;
+    T *dst = wsr + rl * 2 * LD;
+    if (row < nrows) {
+      const unsigned rr = (unsigned)(r0 + row);
+      const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
+      const double *srow = src.s + at(src.Ls, 0, j, k);
+      if constexpr (MODE == 0) {
+        const double wy = sums ? src.dyf[j - 1] : 0.0;
+#pragma unroll
+        for (int c = 0; c < NXC; ++c) {
+          const int ii = lane + 32 * c;
+          if (NX % 32 == 0 || ii < NX) {
+            const double v = srow[ii + 1];
+            sum0 += v * wy;
+            sum1 += v * v;
+            dst[2 * pad8(ii >> 1) + (ii & 1)] = (T)v;
+          }
+        }
+      } else {
+        // r = s - c [j == ny] - L psi (the operator whose eigenvectors the solve uses)
+        const double *p = src.psi + at(src.Lp, 0, j, k);
+        const long sj = src.Lp.sj, sk = src.Lp.sk;
+        const double amj = src.am[j - 1], apj = src.ap[j - 1];
+        const double cj = (j == g.ny) ? ctop : 0.0;
+#pragma unroll
+        for (int c = 0; c < NXC; ++c) {
+          const int ii = lane + 32 * c;
+          if (NX % 32 == 0 || ii < NX) {
+            const int i = ii + 1;
+            const double p0 = p[i];
+            const double lap = (p[i + 1] + p[i - 1] - 2.0 * p0) * src.idx2 + amj * (p[i - sj] - p0) +
+                               apj * (p[i + sj] - p0) + (p[i + sk] + p[i - sk] - 2.0 * p0) * src.idz2;
+            const double v = (srow[i] - cj) - lap;
+            sum1 += v * v;
+            vmax = nanmax_nonneg(vmax, v + cj);
+            dst[2 * pad8(ii >> 1) + (ii & 1)] = (T)v;
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < NXC; ++c) {
+        const int ii = lane + 32 * c;
+        if (NX % 32 == 0 || ii < NX) dst[2 * pad8(ii >> 1) + (ii & 1)] = T(0);
+      }
+    }
+  }
+  if (sums) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sum0 += __shfl_xor_sync(0xffffffffu, sum0, o);
+      sum1 += __shfl_xor_sync(0xffffffffu, sum1, o);
+      if constexpr (MODE == 1) vmax = nanmax_nonneg(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    }
+    if (lane == 0) {
+      red[warp][0] = sum0;
+      red[warp][1] = sum1;
+      red[warp][2] = vmax;
+    }
+  }
+  __syncthreads();  // twiddle table, rows and partial sums in place
+  if (sums && threadIdx.x == 0) {
+    double a0 = 0.0, a1 = 0.0, m = 0.0;
+    for (int w = 0; w < kNW; ++w) {
+      a0 += red[w][0];
+      a1 += red[w][1];
+      m = nanmax_nonneg(m, red[w][2]);
+    }
+    if constexpr (MODE == 0) {
+      atomicAdd(src.acc, a0);
+      atomicAdd(src.acc + 1, a1);
+    } else {
+      atomicAdd(src.acc_r, a1);
+      atomicMax(reinterpret_cast<unsigned long long *>(src.acc_r + 1), (unsigned long long)__double_as_longlong(m));
+    }
+  }
+  fft_warp<V, M, LOGRPW, 1, LD, false>(wsm, lane, tw);
+
+  // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx)
+  constexpr int NPAIR = M / 2 + 1, NPC = (NPAIR + 31) / 32;
+  const T half = T(0.5);
+#pragma unroll
+  for (int rl = 0; rl < RPW; ++rl) {
+    V *Z = wsm + rl * LD;
+#pragma unroll
+    for (int c = 0; c < NPC; ++c) {
+      const int kk = lane + 32 * c;
+      if (kk >= NPAIR) break;
+      if (kk == 0) {
+        const V z0 = Z[0];
+        Z[0] = mk<V>(z0.x + z0.y, T(0));
+        Z[pad8(M)] = mk<V>(z0.x - z0.y, T(0));
+      } else {
+        const int km = M - kk;
+        const V a = Z[pad8(kk)], b = Z[pad8(km)];
+        const V wa = twx[kk], wb = twx[km];
+        V ep = mk<V>(a.x + b.x, a.y - b.y);  // Z_k + conj Z_{M-k}
+        V em = mk<V>(a.x - b.x, a.y + b.y);  // Z_k - conj Z_{M-k}
+        V t1 = cmul(wa, em);                  // W^k * em
+        Z[pad8(kk)] = mk<V>(half * (ep.x + t1.y), half * (ep.y - t1.x));  // (ep - i t1)/2
+        if (km != kk) {
+          V fp = mk<V>(b.x + a.x, b.y - a.y);
+          V fm = mk<V>(b.x - a.x, b.y + a.y);
+          V t2 = cmul(wb, fm);
+          Z[pad8(km)] = mk<V>(half * (fp.x + t2.y), half * (fp.y - t2.x));
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // S[kx][r0 + row]: consecutive threads take consecutive rows of one kx
+  constexpr int NST = ((M + 1) << LOGTJ);
+#pragma unroll
+  for (int t = threadIdx.x; t < NST; t += kNT) {
+    const int kx = t >> LOGTJ, row = t & (TJ - 1);
+    if (row < nrows) spec[(long)kx * g.R + r0 + row] = sm[row * LD + pad8(kx)];
+  }
 }
 
 template <typename V, int M, int MODE>
@@ -136,7 +270,78 @@ void launch_mixed_decide(MixedCtl *ctl, const double *acc, double *acc_r, cudaGr
 
 template <bool ST>
 __global__ void __launch_bounds__(128, 6) k_rhs(RhsArgs a, GridK g, double *__restrict__ s, Lay Ls) {
-  rhs_body<ST>(a, g, s, Ls, blockIdx.x, blockIdx.y, blockIdx.z, threadIdx.x);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.z + 1;
+  const int j0 = blockIdx.y * kRJ + 1, j1 = min(j0 + kRJ - 1, g.ny);
+  if (i > g.nx) return;  // no block-level barrier in this kernel
+  const int pjs = (int)a.Lpsi.sj, pks = (int)a.Lpsi.sk, rjs = (int)a.Lrho.sj, rks = (int)a.Lrho.sk;
+  const int xjs = (int)a.Lux.sj, yjs = (int)a.Luy.sj, zjs = (int)a.Luz.sj, zks = (int)a.Luz.sk;
+  const int sjs = (int)Ls.sj;
+  int op = (int)at(a.Lpsi, i, j0, k), oq = (int)at(a.Lrho, i, j0, k);
+  int ox = (int)at(a.Lux, i, j0, k), oy = (int)at(a.Luy, i, j0, k), oz = (int)at(a.Luz, i, j0, k);
+  int os = (int)at(Ls, i, j0, k);
+  const double *__restrict__ ux = a.ux;
+  const double *__restrict__ uy = a.uy;
+  const double *__restrict__ uz = a.uz;
+  const double *__restrict__ ir = a.irho;
+  const double *__restrict__ pn = a.pn;
+  const double *__restrict__ po = a.pnm1;
+  const double h = a.rho0 * 0.5;
+  const double idxf = g.idxf1, idzf = g.idzf1, idxc = g.idxc1, idzc = g.idzc1;
+  // carried along j: centre values and the lower y face
+  double irc = ir[oq], pc = pn[op], oc = po[op];
+  double irm = ir[oq - rjs], pm = pn[op - pjs], om = po[op - pjs];
+  double uym = uy[oy - yjs];
+  for (int j = j0; j <= j1; ++j) {
+    const double uxc = ux[ox], uxm = ux[ox - 1], uyc = uy[oy], uzc = uz[oz], uzm = uz[oz - zks];
+    const double irxp = ir[oq + 1], irxm = ir[oq - 1], iryp = ir[oq + rjs], irzp = ir[oq + rks], irzm = ir[oq - rks];
+    const double pxp = pn[op + 1], pxm = pn[op - 1], pyp = pn[op + pjs], pzp = pn[op + pks], pzm = pn[op - pks];
+    const double oxp = po[op + 1], oxm = po[op - 1], oyp = po[op + pjs], ozp = po[op + pks], ozm = po[op - pks];
+    const double idyf = g.idyf[j - 1], idycp = g.idyc[j], idycm = g.idyc[j - 1];
+
+    const double ddx = (uxc - uxm) * idxf;
+    const double ddy = (uyc - uym) * idyf;
+    const double ddz = (uzc - uzm) * idzf;
+    double r = ((ddx + ddy) + ddz) * a.r * a.rho0;
+    const double apx = 1.0 - h * (irxp + irc);
+    const double amx = 1.0 - h * (irxm + irc);
+    const double apy = 1.0 - h * (iryp + irc);
+    const double amy = 1.0 - h * (irm + irc);
+    const double apz = 1.0 - h * (irzp + irc);
+    const double amz = 1.0 - h * (irzm + irc);
+    double dpxp = (2.0 * (pxp - pc) - (oxp - oc)) * idxc;
+    double dpxm = (2.0 * (pc - pxm) - (oc - oxm)) * idxc;
+    double dpyp = (2.0 * (pyp - pc) - (oyp - oc)) * idycp;
+    double dpym = (2.0 * (pc - pm) - (oc - om)) * idycm;
+    double dpzp = (2.0 * (pzp - pc) - (ozp - oc)) * idzc;
+    double dpzm = (2.0 * (pc - pzm) - (oc - ozm)) * idzc;
+    if constexpr (ST) {
+      const long x0 = at(a.Lst[0], i, j, k), y0 = at(a.Lst[1], i, j, k), z0 = at(a.Lst[2], i, j, k);
+      dpxp = dpxp - 2.0 * a.stn[0][x0] + a.sto[0][x0];
+      dpxm = dpxm - 2.0 * a.stn[0][x0 - 1] + a.sto[0][x0 - 1];
+      dpyp = dpyp - 2.0 * a.stn[1][y0] + a.sto[1][y0];
+      dpym = dpym - 2.0 * a.stn[1][y0 - a.Lst[1].sj] + a.sto[1][y0 - a.Lst[1].sj];
+      dpzp = dpzp - 2.0 * a.stn[2][z0] + a.sto[2][z0];
+      dpzm = dpzm - 2.0 * a.stn[2][z0 - a.Lst[2].sk] + a.sto[2][z0 - a.Lst[2].sk];
+    }
+    r = r + (apx * dpxp - amx * dpxm) * idxf;
+    r = r + (apy * dpyp - amy * dpym) * idyf;
+    r = r + (apz * dpzp - amz * dpzm) * idzf;
+    s[os] = r;
+    irm = irc;
+    pm = pc;
+    om = oc;
+    irc = iryp;
+    pc = pyp;
+    oc = oyp;
+    uym = uyc;
+    op += pjs;
+    oq += rjs;
+    ox += xjs;
+    oy += yjs;
+    oz += zjs;
+    os += sjs;
+  }
 }
 
 void launch_rhs(const RhsArgs &ra, bool has_st, const GridK &g, double *s, Lay Ls, cudaStream_t st) {
@@ -157,8 +362,94 @@ template <typename V, int M, bool ACC>
 __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_inv(const V *__restrict__ spec, double *__restrict__ psi, Lay Lp,
                                                   int hd, GridK g, const V *__restrict__ twx,
                                                   const V *__restrict__ tpx, double scale) {
+  using T = decltype(V::x);
+  constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
+  constexpr int LD = x_row_stride(M), NX = 2 * M, NXC = (NX + 31) / 32;
   extern __shared__ __align__(16) unsigned char smx[];
-  fftx_inv_body<V, M, ACC>(spec, psi, Lp, hd, g, twx, tpx, scale, blockIdx.x, smx);
+  V *sm = reinterpret_cast<V *>(smx);
+  V *tw = sm + TJ * LD;
+  for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = tpx[t];
+  const int r0 = blockIdx.x << LOGTJ;
+  const int nrows = min(TJ, (int)g.R - r0);
+  constexpr int NLD = ((M + 1) << LOGTJ);
+#pragma unroll
+  for (int t = threadIdx.x; t < NLD; t += kNT) {
+    const int kx = t >> LOGTJ, row = t & (TJ - 1);
+    sm[row * LD + pad8(kx)] = (row < nrows) ? spec[(long)kx * g.R + r0 + row] : mk<V>(T(0), T(0));
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  V *wsm = sm + warp * RPW * LD;
+  // Z[k] = (X_k + conj X_{M-k}) + i conj(W^k) (X_k - conj X_{M-k}),  k = 0..M-1
+  constexpr int NPAIR = M / 2 + 1, NPC = (NPAIR + 31) / 32;
+#pragma unroll
+  for (int rl = 0; rl < RPW; ++rl) {
+    V *X = wsm + rl * LD;
+#pragma unroll
+    for (int c = 0; c < NPC; ++c) {
+      const int kk = lane + 32 * c;
+      if (kk >= NPAIR) break;
+      if (kk == 0) {
+        const T a = X[0].x, b = X[pad8(M)].x;
+        X[0] = mk<V>(a + b, a - b);
+      } else {
+        const int km = M - kk;
+        const V a = X[pad8(kk)], b = X[pad8(km)];
+        const V wa = cconj(twx[kk]), wb = cconj(twx[km]);
+        V ep = mk<V>(a.x + b.x, a.y - b.y);
+        V em = mk<V>(a.x - b.x, a.y + b.y);
+        V t1 = cmul(wa, em);
+        X[pad8(kk)] = mk<V>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
+        if (km != kk) {
+          V fp = mk<V>(b.x + a.x, b.y - a.y);
+          V fm = mk<V>(b.x - a.x, b.y + a.y);
+          V t2 = cmul(wb, fm);
+          X[pad8(km)] = mk<V>(fp.x - t2.y, fp.y + t2.x);
+        }
+      }
+    }
+  }
+  __syncwarp();
+  fft_warp<V, M, LOGRPW, 1, LD, true>(wsm, lane, tw);
+  const T *wsr = reinterpret_cast<const T *>(wsm);
+#pragma unroll
+  for (int rl = 0; rl < RPW; ++rl) {
+    const int row = warp * RPW + rl;
+    if (row >= nrows) break;
+    const unsigned rr = (unsigned)(r0 + row);
+    const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
+    // ghost images of the row: first y ghost layer (wall copy), periodic z
+    const int jg = (j == 1) ? 0 : (j == g.ny ? g.ny + 1 : -1);
+    const int kg = g.slab ? kNoGhost : ((k <= hd) ? k + g.nz : (k > g.nz - hd ? k - g.nz : kNoGhost));
+    double *p00 = psi + at(Lp, 0, j, k);
+    double *p10 = (jg >= 0) ? psi + at(Lp, 0, jg, k) : nullptr;
+    double *p01 = (kg != kNoGhost) ? psi + at(Lp, 0, j, kg) : nullptr;
+    double *p11 = (p10 && p01) ? psi + at(Lp, 0, jg, kg) : nullptr;
+    const T *src = wsr + rl * 2 * LD;
+#pragma unroll
+    for (int c = 0; c < NXC; ++c) {
+      const int ii = lane + 32 * c;
+      if (NX % 32 != 0 && ii >= NX) break;
+      const int i = ii + 1;
+      double v = (double)src[2 * pad8(ii >> 1) + (ii & 1)] * scale;
+      if constexpr (ACC) v += p00[i];  // refinement: psi += correction
+      const int ig = (i <= hd) ? i + NX : (i > NX - hd ? i - NX : kNoGhost);
+      p00[i] = v;
+      if (ig != kNoGhost) p00[ig] = v;
+      if (p10) {
+        p10[i] = v;
+        if (ig != kNoGhost) p10[ig] = v;
+      }
+      if (p01) {
+        p01[i] = v;
+        if (ig != kNoGhost) p01[ig] = v;
+      }
+      if (p11) {
+        p11[i] = v;
+        if (ig != kNoGhost) p11[ig] = v;
+      }
+    }
+  }
 }
 
 template <typename V, int M, bool ACC>

@@ -343,6 +343,7 @@ class ProjectionInputs:
     dt: float
     alpha: float
     rho0: float
+    c: Field | None = None  # the sharp volume fraction before smoothVF (surface tension reads it)
 
 
 def make_inputs(spec: ChannelSpec, seed: int = 1234, device="cpu", hd_u: int = 2, hd_psi: int = 1,
@@ -358,7 +359,7 @@ def make_inputs(spec: ChannelSpec, seed: int = 1234, device="cpu", hd_u: int = 2
     z = lambda: Field("cl", hd_psi, nx, ny, nz, torch.zeros(field_shape("cl", hd_psi, nx, ny, nz),  # noqa: E731
                                                             dtype=torch.float64, device=device))
     return ProjectionInputs(spec, g, u, Field("cl", hd_rho, nx, ny, nz, rho), Field("cl", hd_rho, nx, ny, nz, cs),
-                            z(), z(), spec.dt, 1.0, min(spec.rhol, spec.rhog))
+                            z(), z(), spec.dt, 1.0, min(spec.rhol, spec.rhog), Field("cl", hd_rho, nx, ny, nz, c))
 
 
 def small_spec(nx=32, ny=24, nz=16, stretched=True, nbubbles=3, radius=0.3, rhog=0.05, **kw) -> ChannelSpec:
