@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-vof", action="store_true", help="skip the material-properties leg")
     ap.add_argument("--no-momentum", action="store_true", help="skip the momentum-predictor leg")
     ap.add_argument("--no-st", action="store_true", help="skip the surface-tension leg")
+    ap.add_argument("--slabs", action="store_true",
+                    help="one channel split over the ranks (z/kx slabs, two all-to-alls) instead of replicas")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the legs on the other workloads (mixed 1024x512x512, MG 256x256x128, ensemble)")
     return ap.parse_args()
@@ -548,6 +550,92 @@ def extra_legs(args):
     return legs
 
 
+def run_slabs(args, world, rank, local):
+    """One channel split over the ranks (the reference's pencil decomposition
+    with py = 1): z slabs in physical space, kx slabs in spectral space, two
+    all-to-alls per solve (library packing, zero-copy send / receive buffers)
+    and the z ghost planes of psi.  A step: split RHS, solveFPS, correction,
+    every rank on its slab.  Strong scaling: the channel is the same at every
+    N.  The inputs' ghost planes come from the whole-channel synthesis on each
+    rank, so only the exchanges of a step run inside the timed region."""
+    import torch
+    import torch.distributed as dist
+
+    from tbfsolver_b200 import synth
+    from tbfsolver_b200.dist import SlabChannel
+    from tbfsolver_b200.fields import Field, VField
+    from tbfsolver_b200.solver import PoissonEqn, make_velocity_div_free
+
+    torch.cuda.set_device(local)
+    group = None
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    spec = synth.CONFIGS[args.config]
+    inp = synth.make_inputs(spec, seed=args.seed, device="cuda")
+    g = inp.grid
+    chan = SlabChannel(g, world, rank, device=local)
+    k0, nzl = chan.s.k0, chan.s.nz_loc
+
+    def zslice(f):
+        extra = 1 if f.kind == "sz" else 0
+        return Field(f.kind, f.hd, f.nx, f.ny, nzl, f.a[k0:k0 + nzl + extra + 2 * f.hd].clone())
+
+    u = VField(*[zslice(f) for f in inp.u.components()])
+    rho, pn, pnm1 = zslice(inp.rho), zslice(inp.psi_n), zslice(inp.psi_nm1)
+    del inp
+    torch.cuda.empty_cache()
+    s_loc = Field("cl", 1, g.nx, g.ny, nzl, torch.zeros_like(pn.a))
+    psi = Field("cl", 1, g.nx, g.ny, nzl, torch.zeros_like(pn.a))
+
+    class _Eqn:  # the slab handle behind PoissonEqn's RHS and correction wrappers
+        solver = chan
+        rho0 = min(spec.rhol, spec.rhog)
+
+    e = _Eqn()
+
+    def step():
+        PoissonEqn.compute_source(e, s_loc, pn, pnm1, rho, u, spec.dt, 1.0)
+        chan.solve_fps(psi, s_loc, group)
+        make_velocity_div_free(e, u, psi, pn, pnm1, rho, spec.dt, 1.0)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(local)
+    clk.start()
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    chan.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": g.ncells / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": spec.name, "cells": g.ncells, "precision": "fp64",
+                   "parallelism": f"one channel in z/kx slabs x{world} (two all-to-alls per solve)",
+                   "l2": "inputs larger than L2"},
+        "e2e": None, "gpu_launches": 9 * args.steps, "clocks": clocks, "cpu_baseline": None,
+        "note": "split RHS + solveFPS (forward x, all-to-all, z/y/z, all-to-all, inverse x, psi ghost planes) + "
+                "correction per rank; synchronous library calls, events on the default stream",
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
@@ -556,6 +644,9 @@ def main():
         return
     if args.config == "c4":
         run_ensemble(args, world, rank, local)
+        return
+    if args.slabs:
+        run_slabs(args, world, rank, local)
         return
     line = main_line(args, world, rank, local)
     if line is None:

@@ -383,6 +383,18 @@ int tbfp_slab_create(const tbfp_desc *d, int nz_total, int k0, int kx0, int nkx_
 int tbfp_slab_forward_x(tbfp_handle *h, const double *s, double *spec_z);
 int tbfp_slab_spectral(tbfp_handle *h, double *spec_x);
 int tbfp_slab_inverse_x(tbfp_handle *h, const double *spec_z, double *psi);
+/* The packing of the two all-to-alls (no counterpart in the reference, whose
+   pencil transposes pack with loops, pencilDec.f90:359-562).  z_start[0..world]:
+   the first z plane of every rank's slab in rank order (z_start[world] = the
+   channel's nz).  In the first exchange rank p sends S_z[kx range of q][nz_p][ny]
+   to rank q -- contiguous slices of its S_z, so S_z is the send buffer as it
+   is -- and tbfp_slab_unpack_kx turns the received chunks (in rank order, each
+   [nkx_loc][nz_p][ny]) into S_x[nkx_loc][nz][ny].  In the second exchange
+   tbfp_slab_pack_z writes S_x as the chunks for every destination q
+   ([nkx_loc][nz_q][ny], in rank order); what rank q receives, in rank order, is
+   its S_z as it is.  One strided copy on the device each way. */
+int tbfp_slab_unpack_kx(tbfp_handle *h, int world, const int *z_start, const double *recv, double *spec_x);
+int tbfp_slab_pack_z(tbfp_handle *h, int world, const int *z_start, const double *spec_x, double *send);
 
 /* --- ensemble: many independent channels per GPU ----------------------- */
 /* No counterpart in the reference, which runs one channel per job.  Each

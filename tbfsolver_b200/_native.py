@@ -110,6 +110,8 @@ PROTOTYPES = {
     "tbfp_slab_forward_x": (C.c_int, [_H, _P, _P]),
     "tbfp_slab_spectral": (C.c_int, [_H, _P]),
     "tbfp_slab_inverse_x": (C.c_int, [_H, _P, _P]),
+    "tbfp_slab_unpack_kx": (C.c_int, [_H, C.c_int, C.POINTER(C.c_int), _P, _P]),
+    "tbfp_slab_pack_z": (C.c_int, [_H, C.c_int, C.POINTER(C.c_int), _P, _P]),
     "tbfp_ensemble_create": (C.c_int, [C.c_int, C.POINTER(TbfpDesc), C.c_int, C.POINTER(C.c_void_p)]),
     "tbfp_ensemble_destroy": (C.c_int, [_H]),
     "tbfp_ensemble_size": (C.c_int, [_H]),

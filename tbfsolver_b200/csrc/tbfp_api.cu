@@ -998,6 +998,44 @@ int tbfp_slab_inverse_x(tbfp_handle *h, const double *spec_z, double *psi) {
   return finish(h, "tbfp_slab_inverse_x");
 }
 
+}  // extern "C"
+
+namespace {
+
+int slab_chunks(tbfp_handle *h, int world, const int *z_start, bool to_x, const double *src, double *dst,
+                const char *where) {
+  int rc = check_ptrs(h, {z_start, src, dst});
+  if (rc) return rc;
+  if (!h->slab) return set_err(h, TBFP_EINVAL, std::string(where) + ": not a slab handle");
+  if (world < 1 || world > kSlabMaxRanks)
+    return set_err(h, TBFP_EINVAL, std::string(where) + ": world must be 1..64");
+  SlabParts parts{};
+  parts.n = world;
+  if (z_start[0] != 0 || z_start[world] != h->nz_total)
+    return set_err(h, TBFP_EINVAL, std::string(where) + ": z_start must run from 0 to the channel's nz");
+  for (int r = 0; r <= world; ++r) {
+    if (r > 0 && z_start[r] <= z_start[r - 1])
+      return set_err(h, TBFP_EINVAL, std::string(where) + ": every rank needs at least one z plane");
+    parts.zs[r] = z_start[r];
+  }
+  cudaSetDevice(h->device);
+  launch_slab_chunks(h->gs, parts, to_x, reinterpret_cast<const double2 *>(src), reinterpret_cast<double2 *>(dst),
+                     h->stream);
+  return finish(h, where);
+}
+
+}  // namespace
+
+extern "C" {
+
+int tbfp_slab_unpack_kx(tbfp_handle *h, int world, const int *z_start, const double *recv, double *spec_x) {
+  return slab_chunks(h, world, z_start, true, recv, spec_x, "tbfp_slab_unpack_kx");
+}
+
+int tbfp_slab_pack_z(tbfp_handle *h, int world, const int *z_start, const double *spec_x, double *send) {
+  return slab_chunks(h, world, z_start, false, spec_x, send, "tbfp_slab_pack_z");
+}
+
 // ---------------------------------------------------------------------------
 int tbfp_solve_fps_dev(tbfp_handle *h, const double *s, double *psi) {
   return solve_fps_core(h, s, psi, !(h && (h->flags & TBFP_FLAG_ASYNC)));

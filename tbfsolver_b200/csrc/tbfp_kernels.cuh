@@ -389,6 +389,19 @@ void launch_surface_tension(const double *c, Lay Lc, const StGrid &g, double eps
                             unsigned char *fl, double *kap, double *kap_out, Lay Lk, long nk, double *sx, Lay Lx,
                             long nsx, double *sy, Lay Ly, long nsy, double *sz, Lay Lz, long nsz, cudaStream_t st);
 
+// The all-to-all chunks of a channel split over ranks (z slabs <-> kx slabs).
+// zs[0..n]: the z-slab starts of the n ranks (zs[n] = nz of the channel).
+constexpr int kSlabMaxRanks = 64;
+struct SlabParts {
+  int n;
+  int zs[kSlabMaxRanks + 1];
+};
+// to_x: chunks[p] = [nkx_loc][nz_p][ny] in rank order -> S_x[nkx_loc][nz][ny];
+// else the inverse (S_x -> the chunks for every destination).  g: the slab
+// handle's spectral grid (nkx = nkx_loc, nz = the channel's nz).
+void launch_slab_chunks(const GridK &g, const SlabParts &parts, bool to_x, const double2 *src, double2 *dst,
+                        cudaStream_t st);
+
 // per-file parts of prepare_kernels()
 cudaError_t prepare_xfft_kernels();
 cudaError_t prepare_yz_kernels();

@@ -404,6 +404,37 @@ void launch_tridiag(float2 *spec, const GridK &g, const double *lamx, const doub
   launch_tridiag_t(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, st);
 }
 
+// ---------------------------------------------------------------------------
+// The kx-slab spectrum S_x[kx][k][j] of a split channel and the chunks that
+// the all-to-alls move: the chunk of rank p (source in the first exchange,
+// destination in the second) is [kx][k - zs[p]][j] for its planes k.  One
+// thread per complex entry, j fastest in both layouts (coalesced).
+// ---------------------------------------------------------------------------
+__global__ void k_slab_chunks(GridK g, SlabParts parts, int to_x, const double2 *__restrict__ src,
+                              double2 *__restrict__ dst) {
+  const int ny = g.ny, nz = g.nz;
+  const long n = (long)g.nkx * nz * ny;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int j = (int)(t % ny);
+    const long r = t / ny;
+    const int k = (int)(r % nz), kx = (int)(r / nz);
+    int p = 0;
+    while (k >= parts.zs[p + 1]) ++p;  // the rank that owns plane k (parts.n is small)
+    const int z0 = parts.zs[p], nzp = parts.zs[p + 1] - z0;
+    const long c = (long)g.nkx * ny * z0 + ((long)kx * nzp + (k - z0)) * ny + j;
+    if (to_x) dst[t] = src[c];
+    else dst[c] = src[t];
+  }
+}
+
+void launch_slab_chunks(const GridK &g, const SlabParts &parts, bool to_x, const double2 *src, double2 *dst,
+                        cudaStream_t st) {
+  const long n = (long)g.nkx * g.nz * g.ny;
+  long nb = (n + 255) / 256;
+  if (nb > 148L * 32) nb = 148L * 32;
+  k_slab_chunks<<<(unsigned)(nb < 1 ? 1 : nb), 256, 0, st>>>(g, parts, to_x ? 1 : 0, src, dst);
+}
+
 cudaError_t prepare_yz_kernels() {
   cudaError_t e = cudaSuccess;
   auto set = [&](const void *fn, size_t bytes) {

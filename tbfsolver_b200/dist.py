@@ -103,9 +103,27 @@ def _all_to_all(chunks: list, sizes_in: list, group) -> list:
     return list(torch.split(recv, sizes_in))
 
 
-def to_kx_slabs(sz: torch.Tensor, s: Slabs, group=None) -> torch.Tensor:
-    """S_z[nkx, nz_loc, ny] -> S_x[nkx_loc, nz, ny] (the first all-to-all of a solve)."""
+def z_starts(s: Slabs) -> list:
+    """First z plane of every rank's slab, and the channel's nz last."""
+    return [s.zslab(r)[0] for r in range(s.world)] + [s.nz]
+
+
+def to_kx_slabs(sz: torch.Tensor, s: Slabs, group=None, chan=None) -> torch.Tensor:
+    """S_z[nkx, nz_loc, ny] -> S_x[nkx_loc, nz, ny] (the first all-to-all of a solve).
+    With chan (the rank's SlabChannel) and device tensors, S_z is the send
+    buffer as it is and one library kernel unpacks the received chunks."""
     ny = sz.shape[2]
+    if chan is not None and sz.is_cuda:
+        recv = sz.contiguous()
+        if s.world > 1:
+            recv = torch.empty(s.nkx_loc * s.nz * ny, dtype=sz.dtype, device=sz.device)
+            ins = [s.nkx_loc * s.zslab(p)[1] * ny * 2 for p in range(s.world)]
+            outs = [s.kxslab(q)[1] * s.nz_loc * ny * 2 for q in range(s.world)]
+            dist.all_to_all_single(torch.view_as_real(recv).reshape(-1),
+                                   torch.view_as_real(sz.contiguous()).reshape(-1), ins, outs, group=group)
+        sx = torch.empty((s.nkx_loc, s.nz, ny), dtype=sz.dtype, device=sz.device)
+        chan.unpack_kx(recv, sx)
+        return sx
     chunks = kx_send_chunks(sz, s)
     if s.world > 1:
         per = 2 if sz.is_complex() else 1
@@ -113,9 +131,22 @@ def to_kx_slabs(sz: torch.Tensor, s: Slabs, group=None) -> torch.Tensor:
     return kx_assemble(chunks, s, ny, sz.is_complex())
 
 
-def to_z_slabs(sx: torch.Tensor, s: Slabs, group=None) -> torch.Tensor:
-    """S_x[nkx_loc, nz, ny] -> S_z[nkx, nz_loc, ny] (the second all-to-all)."""
+def to_z_slabs(sx: torch.Tensor, s: Slabs, group=None, chan=None) -> torch.Tensor:
+    """S_x[nkx_loc, nz, ny] -> S_z[nkx, nz_loc, ny] (the second all-to-all).  With
+    chan and device tensors one library kernel packs the chunks and what the
+    rank receives is S_z as it is."""
     ny = sx.shape[2]
+    if chan is not None and sx.is_cuda:
+        send = torch.empty(s.nkx_loc * s.nz * ny, dtype=sx.dtype, device=sx.device)
+        chan.pack_z(sx, send)
+        if s.world == 1:
+            return send.reshape(s.nkx, s.nz_loc, ny)
+        sz = torch.empty((s.nkx, s.nz_loc, ny), dtype=sx.dtype, device=sx.device)
+        ins = [s.kxslab(p)[1] * s.nz_loc * ny * 2 for p in range(s.world)]
+        outs = [s.nkx_loc * s.zslab(q)[1] * ny * 2 for q in range(s.world)]
+        dist.all_to_all_single(torch.view_as_real(sz).reshape(-1), torch.view_as_real(send).reshape(-1), ins, outs,
+                               group=group)
+        return sz
     chunks = z_send_chunks(sx, s)
     if s.world > 1:
         per = 2 if sx.is_complex() else 1
@@ -308,10 +339,29 @@ class SlabChannel:
         from ._native import check
         check(self.lib.tbfp_slab_inverse_x(self.h, spec_z.contiguous().data_ptr(), psi.address()), self.h)
 
+    def _zs(self):
+        import ctypes as C
+
+        if not hasattr(self, "_zs_arr"):
+            zs = z_starts(self.s)
+            self._zs_arr = (C.c_int * len(zs))(*zs)
+        return self._zs_arr
+
+    def unpack_kx(self, recv: torch.Tensor, spec_x: torch.Tensor) -> None:
+        """The chunks received in the first all-to-all (rank order) -> S_x (tbfp_slab_unpack_kx)."""
+        from ._native import check
+        check(self.lib.tbfp_slab_unpack_kx(self.h, self.world, self._zs(), recv.data_ptr(), spec_x.data_ptr()),
+              self.h)
+
+    def pack_z(self, spec_x: torch.Tensor, send: torch.Tensor) -> None:
+        """S_x -> the chunks for every destination of the second all-to-all (tbfp_slab_pack_z)."""
+        from ._native import check
+        check(self.lib.tbfp_slab_pack_z(self.h, self.world, self._zs(), spec_x.data_ptr(), send.data_ptr()), self.h)
+
     def solve_fps(self, psi, s_field, group=None) -> None:
         """solveFPS on this rank's slab (a collective: every rank calls it)."""
         sz = self.forward_x(s_field)
-        sx = to_kx_slabs(sz, self.s, group).contiguous()
+        sx = to_kx_slabs(sz, self.s, group, chan=self)
         self.spectral(sx)
-        self.inverse_x(to_z_slabs(sx, self.s, group), psi)
+        self.inverse_x(to_z_slabs(sx, self.s, group, chan=self), psi)
         exchange_z_ghosts(psi.a, self.s, self.hd_psi, group)

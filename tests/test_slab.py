@@ -124,3 +124,64 @@ def test_slab_projection_is_the_whole_channel_projection():
     finally:
         for c in chans:
             c.close()
+
+
+@pytest.mark.parametrize("P,dims", [(1, (32, 24, 16)), (3, (48, 40, 16)), (4, (64, 24, 24))])
+def test_library_packing_matches_the_torch_packing(P, dims):
+    """tbfp_slab_unpack_kx / tbfp_slab_pack_z against the torch chunk functions,
+    uneven partitions included: bit for bit, and the whole split solve through
+    the library packing equals the whole-channel solve."""
+    nx, ny, nz = dims
+    g = Grid(nx, ny, nz, 2 * np.pi, 2.0, np.pi, True, 1.5)
+    chans = [SlabChannel(g, P, r) for r in range(P)]
+    try:
+        gen = torch.Generator(device="cuda").manual_seed(P)
+        sz = [torch.randn((c.s.nkx, c.s.nz_loc, ny), dtype=torch.complex128, device="cuda", generator=gen)
+              for c in chans]
+        sends = [kx_send_chunks(z, c.s) for z, c in zip(sz, chans)]
+        recv = all_to_all_local(sends)
+        for r, c in zip(recv, chans):
+            want = kx_assemble(r, c.s, ny, True)
+            flat = torch.view_as_complex(torch.cat(r).reshape(-1, 2))
+            got = torch.empty_like(want)
+            c.unpack_kx(flat, got)
+            assert torch.equal(got, want)
+            send = torch.empty(c.s.nkx_loc * nz * ny, dtype=torch.complex128, device="cuda")
+            c.pack_z(want.contiguous(), send)
+            chunks = z_send_chunks(want.contiguous(), c.s)
+            assert torch.equal(torch.view_as_real(send).reshape(-1), torch.cat(chunks))
+        # a whole solve with the library packing and local exchanges
+        m = mesh_of(g)
+        rng = np.random.default_rng(7)
+        s = Field("cl", 1, nx, ny, nz)
+        s.interior()[...] = rng.standard_normal((nz, ny, nx))
+        s.interior()[...] -= np.sum(s.interior() * m.volume()) / m.s_Vg
+        s = Field.like(s, torch.from_numpy(s.a).cuda())
+        with FastPoissonSolver(g) as fps:
+            whole = Field.like(s, torch.zeros_like(s.a))
+            fps.solve_fps(whole, s)
+        s_loc = [_zslice(s, c.s.k0, c.s.nz_loc) for c in chans]
+        psi_loc = [Field("cl", 1, nx, ny, c.s.nz_loc, torch.zeros_like(x.a)) for c, x in zip(chans, s_loc)]
+        spec_z = [c.forward_x(x).clone() for c, x in zip(chans, s_loc)]
+        recv = all_to_all_local([[z[c2.s.kx0:c2.s.kx0 + c2.s.nkx_loc].reshape(-1) for c2 in chans] for z in spec_z])
+        spec_x = []
+        for r, c in zip(recv, chans):
+            sx = torch.empty((c.s.nkx_loc, nz, ny), dtype=torch.complex128, device="cuda")
+            c.unpack_kx(torch.cat(r), sx)
+            c.spectral(sx)
+            spec_x.append(sx)
+        sends = []
+        for x, c in zip(spec_x, chans):
+            send = torch.empty(c.s.nkx_loc * nz * ny, dtype=torch.complex128, device="cuda")
+            c.pack_z(x, send)
+            offs = [c.s.nkx_loc * ny * c2.s.k0 for c2 in chans] + [c.s.nkx_loc * ny * nz]
+            sends.append([send[offs[q]:offs[q + 1]] for q in range(P)])
+        recv = all_to_all_local(sends)
+        for r, c, p in zip(recv, chans, psi_loc):
+            c.inverse_x(torch.cat(r).reshape(c.s.nkx, c.s.nz_loc, ny), p)
+        exchange_z_ghosts_local([p.a for p in psi_loc], [c.s for c in chans], chans[0].hd_psi)
+        for c, p in zip(chans, psi_loc):
+            assert torch.equal(p.a, _zslice(whole, c.s.k0, c.s.nz_loc).a), c.rank
+    finally:
+        for c in chans:
+            c.close()
