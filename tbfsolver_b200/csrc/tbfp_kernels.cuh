@@ -271,6 +271,9 @@ void launch_recip(const double *rho, double *irho, long n, cudaStream_t st);
 void launch_fftx_fwd_from_s(const double *s, Lay Ls, const GridK &g, const double2 *twx, const double2 *tpx,
                             double2 *spec, cudaStream_t st);
 void launch_rhs(const RhsArgs &ra, bool has_st, const GridK &g, double *s, Lay Ls, cudaStream_t st);
+// the right-hand side computed into the forward x transform's tiles (s is not stored)
+void launch_rhs_fftx(const RhsArgs &ra, bool has_st, const GridK &g, const double2 *twx, const double2 *tpx,
+                     double2 *spec, cudaStream_t st);
 void launch_fftz(double2 *spec, const GridK &g, const double2 *tpz, bool inverse, cudaStream_t st);
 void launch_fftz(float2 *spec, const GridK &g, const float2 *tpz, bool inverse, cudaStream_t st);
 void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,

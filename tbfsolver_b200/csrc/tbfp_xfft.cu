@@ -351,6 +351,192 @@ void launch_rhs(const RhsArgs &ra, bool has_st, const GridK &g, double *s, Lay L
 }
 
 // ---------------------------------------------------------------------------
+// The split right-hand side and the forward x transform in one kernel (the
+// FP64 direct solve).  The CTA computes the right-hand side of its TJ rows
+// straight into its x tile in shared memory, so s never goes through HBM
+// (403 MB written and read back at 512x384x256).  Threads own columns and
+// march along the tile's rows with the centre values and lower y neighbours
+// carried from row to row, the arithmetic of k_rhs term for term; a row at
+// j = 1 (the start of a z plane) reloads them.  The transform, the r2c
+// post-processing and the transposed store are those of k_fftx_fwd.
+// ---------------------------------------------------------------------------
+template <int M, bool ST>
+__global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3))
+    k_rhs_fftx(RhsArgs a, GridK g, const double2 *__restrict__ twx, const double2 *__restrict__ tpx,
+               double2 *__restrict__ spec) {
+  using V = double2;
+  constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
+  constexpr int LD = x_row_stride(M), NX = 2 * M;
+  // column ownership: NG groups of NX threads (NX <= kNT), each marching RG
+  // rows, or one group with NCOL columns per thread
+  constexpr int NG = NX <= kNT ? kNT / NX : 1;
+  constexpr int NCOL = NX <= kNT ? 1 : (NX + kNT - 1) / kNT;
+  constexpr int RG = (TJ + NG - 1) / NG;
+  extern __shared__ __align__(16) unsigned char smx[];
+  V *sm = reinterpret_cast<V *>(smx);
+  double *smr = reinterpret_cast<double *>(smx);
+  V *tw = sm + TJ * LD;
+  for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = __ldg(tpx + t);
+  const int r0 = blockIdx.x << LOGTJ;
+  const int nrows = min(TJ, (int)g.R - r0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  const int grp = NX <= kNT ? (int)threadIdx.x / NX : 0;
+  if (grp < NG) {
+    const int col0 = (int)threadIdx.x - grp * (NX <= kNT ? NX : 0);
+    const int rl0 = grp * RG, rl1 = min(rl0 + RG, TJ);
+    const int pjs = (int)a.Lpsi.sj, pks = (int)a.Lpsi.sk, rjs = (int)a.Lrho.sj, rks = (int)a.Lrho.sk;
+    const int yjs = (int)a.Luy.sj, zks = (int)a.Luz.sk;
+    const double *__restrict__ ux = a.ux;
+    const double *__restrict__ uy = a.uy;
+    const double *__restrict__ uz = a.uz;
+    const double *__restrict__ ir = a.irho;
+    const double *__restrict__ pn = a.pn;
+    const double *__restrict__ po = a.pnm1;
+    const double h = a.rho0 * 0.5;
+    const double idxf = g.idxf1, idzf = g.idzf1, idxc = g.idxc1, idzc = g.idzc1;
+#pragma unroll 1
+    for (int c = 0; c < NCOL; ++c) {
+      const int ii = col0 + c * kNT;
+      if (NCOL > 1 && ii >= NX) break;
+      const int i = ii + 1;
+      double *dst = smr + 2 * pad8(ii >> 1) + (ii & 1);
+      double irc = 0.0, pc = 0.0, oc = 0.0, irm = 0.0, pm = 0.0, om = 0.0, uym = 0.0;
+      int jprev = -1;
+#pragma unroll
+      for (int rl = rl0; rl < rl1; ++rl) {
+        double r = 0.0;
+        if (rl < nrows) {
+          const unsigned rr = (unsigned)(r0 + rl);
+          const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
+          const int op = (int)at(a.Lpsi, i, j, k), oq = (int)at(a.Lrho, i, j, k);
+          const int ox = (int)at(a.Lux, i, j, k), oy = (int)at(a.Luy, i, j, k), oz = (int)at(a.Luz, i, j, k);
+          if (j != jprev + 1) {  // first row of the march or of a z plane
+            irc = __ldg(ir + oq);
+            pc = __ldg(pn + op);
+            oc = __ldg(po + op);
+            irm = __ldg(ir + (oq - rjs));
+            pm = __ldg(pn + (op - pjs));
+            om = __ldg(po + (op - pjs));
+            uym = __ldg(uy + (oy - yjs));
+          }
+          jprev = j;
+          const double uxc = __ldg(ux + ox), uyc = __ldg(uy + oy), uzc = __ldg(uz + oz), uzm = __ldg(uz + (oz - zks));
+          const double iryp = __ldg(ir + (oq + rjs)), irzp = __ldg(ir + (oq + rks)), irzm = __ldg(ir + (oq - rks));
+          const double pyp = __ldg(pn + (op + pjs)), pzp = __ldg(pn + (op + pks)), pzm = __ldg(pn + (op - pks));
+          const double oyp = __ldg(po + (op + pjs)), ozp = __ldg(po + (op + pks)), ozm = __ldg(po + (op - pks));
+          const double uxm = __ldg(ux + (ox - 1));
+          const double irxm = __ldg(ir + (oq - 1)), irxp = __ldg(ir + (oq + 1));
+          const double pxm = __ldg(pn + (op - 1)), pxp = __ldg(pn + (op + 1));
+          const double oxm = __ldg(po + (op - 1)), oxp = __ldg(po + (op + 1));
+          const double idyf = g.idyf[j - 1], idycp = g.idyc[j], idycm = g.idyc[j - 1];
+
+          const double ddx = (uxc - uxm) * idxf;
+          const double ddy = (uyc - uym) * idyf;
+          const double ddz = (uzc - uzm) * idzf;
+          r = ((ddx + ddy) + ddz) * a.r * a.rho0;
+          const double apx = 1.0 - h * (irxp + irc);
+          const double amx = 1.0 - h * (irxm + irc);
+          const double apy = 1.0 - h * (iryp + irc);
+          const double amy = 1.0 - h * (irm + irc);
+          const double apz = 1.0 - h * (irzp + irc);
+          const double amz = 1.0 - h * (irzm + irc);
+          double dpxp = (2.0 * (pxp - pc) - (oxp - oc)) * idxc;
+          double dpxm = (2.0 * (pc - pxm) - (oc - oxm)) * idxc;
+          double dpyp = (2.0 * (pyp - pc) - (oyp - oc)) * idycp;
+          double dpym = (2.0 * (pc - pm) - (oc - om)) * idycm;
+          double dpzp = (2.0 * (pzp - pc) - (ozp - oc)) * idzc;
+          double dpzm = (2.0 * (pc - pzm) - (oc - ozm)) * idzc;
+          if constexpr (ST) {
+            const long x0 = at(a.Lst[0], i, j, k), y0 = at(a.Lst[1], i, j, k), z0 = at(a.Lst[2], i, j, k);
+            dpxp = dpxp - 2.0 * a.stn[0][x0] + a.sto[0][x0];
+            dpxm = dpxm - 2.0 * a.stn[0][x0 - 1] + a.sto[0][x0 - 1];
+            dpyp = dpyp - 2.0 * a.stn[1][y0] + a.sto[1][y0];
+            dpym = dpym - 2.0 * a.stn[1][y0 - a.Lst[1].sj] + a.sto[1][y0 - a.Lst[1].sj];
+            dpzp = dpzp - 2.0 * a.stn[2][z0] + a.sto[2][z0];
+            dpzm = dpzm - 2.0 * a.stn[2][z0 - a.Lst[2].sk] + a.sto[2][z0 - a.Lst[2].sk];
+          }
+          r = r + (apx * dpxp - amx * dpxm) * idxf;
+          r = r + (apy * dpyp - amy * dpym) * idyf;
+          r = r + (apz * dpzp - amz * dpzm) * idzf;
+          irm = irc;
+          pm = pc;
+          om = oc;
+          irc = iryp;
+          pc = pyp;
+          oc = oyp;
+          uym = uyc;
+        }
+        dst[rl * 2 * LD] = r;
+      }
+    }
+  }
+  __syncthreads();  // twiddle table and rows in place
+  V *wsm = sm + warp * RPW * LD;  // this warp's rows
+  fft_warp<V, M, LOGRPW, 1, LD, false>(wsm, lane, tw);
+
+  // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx)
+  constexpr int NPAIR = M / 2 + 1, NPC = (NPAIR + 31) / 32;
+#pragma unroll
+  for (int rl = 0; rl < RPW; ++rl) {
+    V *Z = wsm + rl * LD;
+#pragma unroll
+    for (int c = 0; c < NPC; ++c) {
+      const int kk = lane + 32 * c;
+      if (kk >= NPAIR) break;
+      if (kk == 0) {
+        const V z0 = Z[0];
+        Z[0] = make_double2(z0.x + z0.y, 0.0);
+        Z[pad8(M)] = make_double2(z0.x - z0.y, 0.0);
+      } else {
+        const int km = M - kk;
+        const V za = Z[pad8(kk)], zb = Z[pad8(km)];
+        const V wa = twx[kk], wb = twx[km];
+        const V ep = make_double2(za.x + zb.x, za.y - zb.y);  // Z_k + conj Z_{M-k}
+        const V em = make_double2(za.x - zb.x, za.y + zb.y);  // Z_k - conj Z_{M-k}
+        const V t1 = cmul(wa, em);                             // W^k * em
+        Z[pad8(kk)] = make_double2(0.5 * (ep.x + t1.y), 0.5 * (ep.y - t1.x));  // (ep - i t1)/2
+        if (km != kk) {
+          const V fp = make_double2(zb.x + za.x, zb.y - za.y);
+          const V fm = make_double2(zb.x - za.x, zb.y + za.y);
+          const V t2 = cmul(wb, fm);
+          Z[pad8(km)] = make_double2(0.5 * (fp.x + t2.y), 0.5 * (fp.y - t2.x));
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // S[kx][r0 + row]: consecutive threads take consecutive rows of one kx
+  constexpr int NST = ((M + 1) << LOGTJ);
+#pragma unroll
+  for (int t = threadIdx.x; t < NST; t += kNT) {
+    const int kx = t >> LOGTJ, row = t & (TJ - 1);
+    if (row < nrows) spec[(long)kx * g.R + r0 + row] = sm[row * LD + pad8(kx)];
+  }
+}
+
+template <int M>
+static void launch_rhs_fftx_n(const RhsArgs &ra, bool has_st, const GridK &g, const double2 *twx,
+                              const double2 *tpx, double2 *spec, cudaStream_t st) {
+  constexpr int TJ = fftx_rows_per_cta(M);
+  const unsigned nblk = (unsigned)((g.R + TJ - 1) / TJ);
+  const size_t smem = fftx_smem_bytes(M, 16);
+  if (has_st) k_rhs_fftx<M, true><<<nblk, kNT, smem, st>>>(ra, g, twx, tpx, spec);
+  else k_rhs_fftx<M, false><<<nblk, kNT, smem, st>>>(ra, g, twx, tpx, spec);
+}
+
+void launch_rhs_fftx(const RhsArgs &ra, bool has_st, const GridK &g, const double2 *twx, const double2 *tpx,
+                     double2 *spec, cudaStream_t st) {
+  switch (g.M) {
+#define TBFP_CASE(L) \
+  case L: launch_rhs_fftx_n<L>(ra, has_st, g, twx, tpx, spec, st); break;
+    TBFP_FFT_LENGTHS(TBFP_CASE)
+#undef TBFP_CASE
+    default: break;  // lengths are validated by tbfp_create
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Inverse x transform of a tile of rows: S[kx][row] -> c2r -> psi rows scaled
 // by 1/(nx*nz) (fastPoissonSolver.f90:371-378), written with every ghost image
 // of updateBoundaries (field.f90:950-974 on one rank): the first y ghost layer
@@ -496,7 +682,9 @@ cudaError_t prepare_xfft_kernels() {
   set((const void *)k_fftx_fwd<float2, L, 1>, fftx_smem_bytes(L, 8));        \
   set((const void *)k_fftx_inv<double2, L, false>, fftx_smem_bytes(L, 16));  \
   set((const void *)k_fftx_inv<float2, L, false>, fftx_smem_bytes(L, 8));    \
-  set((const void *)k_fftx_inv<float2, L, true>, fftx_smem_bytes(L, 8));
+  set((const void *)k_fftx_inv<float2, L, true>, fftx_smem_bytes(L, 8));     \
+  set((const void *)k_rhs_fftx<L, false>, fftx_smem_bytes(L, 16));           \
+  set((const void *)k_rhs_fftx<L, true>, fftx_smem_bytes(L, 16));
   TBFP_FFT_LENGTHS(TBFP_CASE)
 #undef TBFP_CASE
   return e;
