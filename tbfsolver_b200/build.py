@@ -19,7 +19,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "lib", "libtbfp.so")
-SOURCES = ["tbfp_api.cu", "tbfp_xfft.cu", "tbfp_yz.cu", "tbfp_correct.cu", "tbfp_mg.cu", "tbfp_noalloc.cu", "tbfp_vof.cu", "tbfp_momentum.cu", "tbfp_flow.cu", "tbfp_ensemble.cu", "tbfp_surface.cu"]
+SOURCES = ["tbfp_api.cu", "tbfp_xfft.cu", "tbfp_yz.cu", "tbfp_correct.cu", "tbfp_mg.cu", "tbfp_noalloc.cu", "tbfp_vof.cu", "tbfp_momentum.cu", "tbfp_flow.cu", "tbfp_ensemble.cu", "tbfp_surface.cu", "tbfp_correct_tma.cu"]
 HEADERS = ["tbfp_kernels.cuh", "tbfp_stages.cuh", "fft_smem.cuh", "tbfp_mg.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

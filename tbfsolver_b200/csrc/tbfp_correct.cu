@@ -59,6 +59,12 @@ __global__ void __launch_bounds__(128, 8) k_correct_div(CorrArgs a, GridK g, uns
 
 void launch_correct_div(const CorrArgs &ca, bool has_st, const GridK &g, unsigned long long *maxdiv,
                         cudaStream_t st) {
+  if (!has_st) {  // the TMA-staged z march (tbfp_correct_tma.cu) wherever tensor maps describe the arrays
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        launch_correct_div_tma(ca, g, maxdiv, sms, st))
+      return;
+  }
   dim3 grid((g.nx + 127) / 128, (g.ny + kJC - 1) / kJC, g.nz);
   if (has_st) k_correct_div<true><<<grid, 128, 0, st>>>(ca, g, maxdiv);
   else k_correct_div<false><<<grid, 128, 0, st>>>(ca, g, maxdiv);
@@ -114,6 +120,8 @@ void launch_div(const double *ux, const double *uy, const double *uz, Lay Lux, L
 // Raise the dynamic shared-memory limits of every transform kernel; once per device.
 cudaError_t prepare_kernels() {
   cudaError_t e = prepare_xfft_kernels();
+  const cudaError_t e3 = prepare_correct_tma_kernel();
+  if (e == cudaSuccess) e = e3;
   const cudaError_t e2 = prepare_yz_kernels();
   return e != cudaSuccess ? e : e2;
 }

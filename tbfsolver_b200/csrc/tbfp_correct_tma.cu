@@ -1,0 +1,441 @@
+// Velocity correction with the continuity check (makeVelocityDivFree FAST,
+// momentumEqn.f90:999-1127, and computeContinuityError,
+// auxiliaryRoutines.f90:42-91), with its inputs staged by the tensor memory
+// accelerator (TMA).
+//
+// A CTA owns an x-y tile of kCTX x kCTY cells and marches a chunk of z planes.
+// For every plane, one thread issues seven tiled bulk copies
+// (cp.async.bulk.tensor, no multicast): psi, psi^n, psi^(n-1) and 1/rho with a
+// one-cell halo in x and y, and the tile's ux, uy (with the face below the
+// tile) and uz.  The copies complete on an mbarrier.  Three plane slots form a
+// ring: while the threads correct plane k from the slots of planes k and k+1,
+// the copies of plane k+2 are in flight, so the load parallelism comes from
+// the copy engine instead of from resident warps.  The lower z face of a plane
+// is the upper face of the plane before (carried in registers); the chunk's
+// first plane computes it from one extra plane.  The x face below cell i = 1
+// is the upper face of cell nx (the periodic image), whose nine inputs per row
+// come in by 8-byte cp.async copies in the same ring.
+//
+// Every face is computed with the arguments and in the operation order of
+// correct_div_body (the kernel form, which serves surface tension and arrays
+// that a tensor map cannot describe).  A wait on a copy is bounded: past the
+// limit the CTA waits (bounded again) for its copies in flight, folds NaN into
+// *maxdiv, which the host reports as a non-finite divergence, and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "tbfp_kernels.cuh"
+#include "tbfp_stages.cuh"
+
+namespace tbfp {
+
+namespace {
+
+constexpr int kCTX = 128, kCTY = 8, kCNT = 256;
+constexpr int kCRows = kCTX * kCTY / kCNT;           // rows per thread (consecutive)
+constexpr int kPer = 9;                               // periodic inputs per row
+constexpr long long kTmaWaitCycles = 4000000000LL;    // about 2 s of SM clock
+constexpr int kCorrTmaMaxSmem = 220 * 1024;  // under the opt-in limit with the static reduction buffer
+
+__host__ __device__ constexpr int align128(int b) { return (b + 127) & ~127; }
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kTmaWaitCycles) return false;
+  return true;
+}
+__device__ __forceinline__ void tma_load2(unsigned dst, const CUtensorMap *map, int x, int y, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load3(unsigned dst, const CUtensorMap *map, int x, int y, int z, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
+// Box geometry of one array: the first box column/row (array indices, for the
+// tile at the origin), the offset of the first needed column inside the box
+// (the box starts on an even index: 16-byte rule), the box width, and the
+// array index of plane 0.
+struct BoxGeom {
+  int xo, dx, w, yo, zo;
+};
+// ux rows are nx + 1 + 2 halo long (odd), so its row stride is no multiple of
+// 16 bytes: its tensor map is 2-D (the flattened x-y plane, z) and each tile
+// row is its own box of kUxW values starting on an even element.
+constexpr int kUxW = kCTX + 2;
+constexpr int kUxLd = 144;  // shared-memory row slot of ux: kUxW values, 1152 bytes (a copy lands on 128 bytes)
+struct UxGeom {
+  int fx, yo, zo, sj;  // x index of face i0-1 at the origin tile, row index of row j0 = 1, plane 0, row stride
+};
+struct CorrTmaGeom {
+  BoxGeom ps, ir, uy, uz;  // psi, psi^n, psi^(n-1) share the psi layout
+  UxGeom ux;
+  int nzc;  // planes per chunk
+};
+
+// shared-memory carve-up (bytes), from the box widths
+struct CorrTmaSmem {
+  int sps, sir, ss;       // one psi-layout plane, one 1/rho plane, a scalar slot
+  int sux, suy, suz, us;  // velocity boxes and a velocity slot
+  int ps;                 // a periodic slot
+  int total;
+};
+__host__ __device__ inline CorrTmaSmem corr_tma_smem(const CorrTmaGeom &q) {
+  CorrTmaSmem m;
+  m.sps = align128(q.ps.w * (kCTY + 2) * 8);
+  m.sir = align128(q.ir.w * (kCTY + 2) * 8);
+  m.ss = 3 * m.sps + m.sir;
+  m.sux = kUxLd * kCTY * 8;
+  m.suy = align128(q.uy.w * (kCTY + 1) * 8);
+  m.suz = align128(q.uz.w * kCTY * 8);
+  m.us = m.sux + m.suy + m.suz;
+  m.ps = align128(kPer * kCTY * 8);
+  m.total = 3 * m.ss + 3 * m.us + 3 * m.ps + 3 * 8;
+  return m;
+}
+
+__global__ void __launch_bounds__(kCNT, 1)
+    k_correct_tma(const __grid_constant__ CUtensorMap m_ps, const __grid_constant__ CUtensorMap m_pn,
+                  const __grid_constant__ CUtensorMap m_po, const __grid_constant__ CUtensorMap m_ir,
+                  const __grid_constant__ CUtensorMap m_ux, const __grid_constant__ CUtensorMap m_uy,
+                  const __grid_constant__ CUtensorMap m_uz, CorrArgs a, GridK g, CorrTmaGeom q,
+                  unsigned long long *__restrict__ maxdiv) {
+  extern __shared__ __align__(128) unsigned char smc[];
+  const int tid = threadIdx.x, tx = tid & (kCTX - 1), tg = tid / kCTX;
+  const int bx = blockIdx.x, by = blockIdx.y;
+  const int i0 = 1 + kCTX * bx, j0 = 1 + kCTY * by;
+  const int k0 = 1 + q.nzc * (int)blockIdx.z;
+  if (k0 > g.nz) return;  // whole CTA
+  const int k1 = min(k0 + q.nzc - 1, g.nz);
+  const int km0 = (k0 == 1 && !g.slab) ? g.nz : k0 - 1;
+  const CorrTmaSmem L = corr_tma_smem(q);
+  // copy destinations on 128-byte boundaries (the launch adds 128 bytes of slack)
+  // 3 scalar slots (psi, psi^n, psi^(n-1), 1/rho)
+  unsigned char *sc = smc + ((128u - (smem_u32(smc) & 127u)) & 127u);
+  unsigned char *su = sc + 3 * L.ss;        // 3 velocity slots: ux, uy, uz
+  double *sp = reinterpret_cast<double *>(su + 3 * L.us);  // 3 periodic slots [value][row]
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(su + 3 * L.us + 3 * L.ps);
+  const int PSD = L.ps / 8;
+  const unsigned bps = (unsigned)(q.ps.w * (kCTY + 2) * 8), bir = (unsigned)(q.ir.w * (kCTY + 2) * 8);
+  const unsigned bux = (unsigned)(kUxW * kCTY * 8), buy = (unsigned)(q.uy.w * (kCTY + 1) * 8),
+                 buz = (unsigned)(q.uz.w * kCTY * 8);
+
+  if (tid == 0) {
+    for (int m = 0; m < 3; ++m) mbar_init(smem_u32(bars + m), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+
+  // stage t: scalars of plane p_t into scalar slot (t+1)%3 and, for t >= 0,
+  // the velocities of p_t into velocity slot t%3 (stage -1: uz only, slot 2),
+  // all on mbarrier (t+1)%3; p_{-1} = km0, p_t = k0 + t
+  auto issue = [&](int t) {
+    const int pl = (t < 0) ? km0 : k0 + t;
+    const int S = (t + 1) % 3, U = (t + 3) % 3;
+    if (tid == 0) {
+      const unsigned bar = smem_u32(bars + S);
+      mbar_expect_tx(bar, 3 * bps + bir + buz + (t >= 0 ? bux + buy : 0u));
+      unsigned char *s = sc + S * L.ss;
+      const int xs = q.ps.xo + kCTX * bx, ys = q.ps.yo + kCTY * by, zs = q.ps.zo + pl;
+      tma_load3(smem_u32(s), &m_ps, xs, ys, zs, bar);
+      tma_load3(smem_u32(s + L.sps), &m_pn, xs, ys, zs, bar);
+      tma_load3(smem_u32(s + 2 * L.sps), &m_po, xs, ys, zs, bar);
+      tma_load3(smem_u32(s + 3 * L.sps), &m_ir, q.ir.xo + kCTX * bx, q.ir.yo + kCTY * by, q.ir.zo + pl, bar);
+      unsigned char *u = su + U * L.us;
+      if (t >= 0) {
+        for (int r = 0; r < kCTY; ++r) {
+          const int e = (q.ux.yo + kCTY * by + r) * q.ux.sj + q.ux.fx + kCTX * bx;
+          tma_load2(smem_u32(u + r * kUxLd * 8), &m_ux, e & ~1, q.ux.zo + pl, bar);
+        }
+        tma_load3(smem_u32(u + L.sux), &m_uy, q.uy.xo + kCTX * bx, q.uy.yo + kCTY * by, q.uy.zo + pl, bar);
+      }
+      tma_load3(smem_u32(u + L.sux + L.suy), &m_uz, q.uz.xo + kCTX * bx, q.uz.yo + kCTY * by, q.uz.zo + pl, bar);
+    }
+    if (bx == 0 && t >= 0 && tid < kPer * kCTY) {
+      // inputs of the upper x face of cell nx, row j (clamped into the array)
+      const int r = tid / kPer, v = tid - r * kPer, j = min(j0 + r, g.ny);
+      const int ic = g.nx + (v < 8 ? (v & 1) : 0);
+      const double *src;
+      if (v < 2) src = a.psi + at(a.Lpsi, ic, j, pl);
+      else if (v < 4) src = a.pn + at(a.Lpsi, ic, j, pl);
+      else if (v < 6) src = a.pnm1 + at(a.Lpsi, ic, j, pl);
+      else if (v < 8) src = a.irho + at(a.Lrho, ic, j, pl);
+      else src = a.uxi + at(a.Lux, g.nx, j, pl);
+      cp_async8(sp + S * PSD + v * kCTY + r, src);
+    }
+    cp_async_commit();
+  };
+
+  const int nlast = k1 - k0, tmax = nlast + 1;
+  int waited = 0;  // stages -1 .. waited-1 have been waited for
+  int issued = 1;  // stages up to this one are issued
+  issue(-1);
+  issue(0);
+  issue(1);
+  auto drain_and_fail = [&]() {
+    if (tid == 0) {
+      for (int t = waited; t <= issued; ++t) {
+        const int m = (t + 1) % 3;
+        mbar_wait_bounded(smem_u32(bars + m), (unsigned)(((t + 1) / 3) & 1));
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (tid == 0) atomicMax(maxdiv, 0x7ff8000000000000ull);  // NaN: a copy did not complete in time
+  };
+
+  const double R = a.r, ir0 = a.invrho0, idxc = g.idxc1, idzc = g.idzc1;
+  const int i = i0 + tx;
+  const bool col = i <= g.nx;
+  const double idx = col ? g.idxf[i - 1] : 0.0;
+
+  // the lower z face of the chunk's first plane, from planes km0 (slot 0) and k0 (slot 1)
+  double uzq[kCRows];
+  {
+    bool bad = !mbar_wait_bounded(smem_u32(bars + 0), 0u);
+    bad = !mbar_wait_bounded(smem_u32(bars + 1), 0u) || bad;
+    cp_async_wait_group<1>();
+    if (__syncthreads_or(bad)) {
+      waited = -1;
+      drain_and_fail();
+      return;
+    }
+    waited = 1;
+    const double *P0 = reinterpret_cast<const double *>(sc), *P1 = reinterpret_cast<const double *>(sc + L.ss);
+    const double *Uzm = reinterpret_cast<const double *>(su + 2 * L.us + L.sux + L.suy);
+#pragma unroll
+    for (int qq = 0; qq < kCRows; ++qq) {
+      const int r = kCRows * tg + qq;
+      const int rs = (r + 1) * q.ps.w + q.ps.dx + 1 + tx, ri = (r + 1) * q.ir.w + q.ir.dx + 1 + tx;
+      const int so = L.sps / 8, io = 3 * L.sps / 8;
+      uzq[qq] = face_update(Uzm[r * q.uz.w + q.uz.dx + tx], R, ir0, P1[io + ri], P0[io + ri], idzc, P1[rs], P0[rs],
+                            P1[so + rs], P0[so + rs], P1[2 * so + rs], P0[2 * so + rs], 0.0);
+    }
+  }
+
+  double vmax = 0.0;
+  for (int n = 0; n <= nlast; ++n) {
+    const int k = k0 + n;
+    {
+      const int t = n + 1;  // scalars of plane k+1
+      const bool bad = !mbar_wait_bounded(smem_u32(bars + (t + 1) % 3), (unsigned)(((t + 1) / 3) & 1));
+      cp_async_wait_group<1>();  // the periodic column of plane k
+      if (__syncthreads_or(bad)) {
+        drain_and_fail();
+        return;
+      }
+      waited = t + 1;
+    }
+    if (n + 2 <= tmax) {
+      issue(n + 2);
+      issued = n + 2;
+    } else {
+      cp_async_commit();  // keeps one group per plane
+    }
+    const int K = (n + 1) % 3, K1 = (n + 2) % 3, U = n % 3;
+    const double *Sps = reinterpret_cast<const double *>(sc + K * L.ss);
+    const double *Spn = Sps + L.sps / 8, *Spo = Sps + 2 * (L.sps / 8), *Sir = Sps + 3 * (L.sps / 8);
+    const double *Tps = reinterpret_cast<const double *>(sc + K1 * L.ss);
+    const double *Tpn = Tps + L.sps / 8, *Tpo = Tps + 2 * (L.sps / 8), *Tir = Tps + 3 * (L.sps / 8);
+    const double *Ux = reinterpret_cast<const double *>(su + U * L.us);
+    const double *Uy = reinterpret_cast<const double *>(su + U * L.us + L.sux);
+    const double *Uz = reinterpret_cast<const double *>(su + U * L.us + L.sux + L.suy);
+    const double *Pe = sp + K * PSD;
+    const double idz = g.idzf[k - 1];
+    double uym = 0.0;
+#pragma unroll
+    for (int qq = 0; qq < kCRows; ++qq) {
+      const int r = kCRows * tg + qq, j = j0 + r;
+      const int rs = (r + 1) * q.ps.w + q.ps.dx + 1 + tx, ri = (r + 1) * q.ir.w + q.ir.dx + 1 + tx;
+      const double psc = Sps[rs], pnc = Spn[rs], poc = Spo[rs], irc = Sir[ri];
+      // upper and lower x faces (ux(i) at column rx + 1 of the row's box)
+      const int rx = r * kUxLd + (((q.ux.yo + kCTY * by + r) * q.ux.sj + q.ux.fx) & 1) + tx;
+      const double uxp = face_update(Ux[rx + 1], R, ir0, Sir[ri + 1], irc, idxc, Sps[rs + 1], psc, Spn[rs + 1], pnc,
+                                     Spo[rs + 1], poc, 0.0);
+      double uxm;
+      if (i == 1) {
+        uxm = face_update(Pe[8 * kCTY + r], R, ir0, Pe[7 * kCTY + r], Pe[6 * kCTY + r], idxc, Pe[1 * kCTY + r],
+                          Pe[0 * kCTY + r], Pe[3 * kCTY + r], Pe[2 * kCTY + r], Pe[5 * kCTY + r], Pe[4 * kCTY + r], 0.0);
+      } else {
+        uxm = face_update(Ux[rx], R, ir0, irc, Sir[ri - 1], idxc, psc, Sps[rs - 1], pnc, Spn[rs - 1], poc,
+                          Spo[rs - 1], 0.0);
+      }
+      // upper y face (the top wall face is copied), lower y face
+      const double uyc = Uy[(r + 1) * q.uy.w + q.uy.dx + tx];
+      const double uyp = (j < g.ny) ? face_update(uyc, R, ir0, Sir[ri + q.ir.w], irc, g.idyc[j], Sps[rs + q.ps.w],
+                                                  psc, Spn[rs + q.ps.w], pnc, Spo[rs + q.ps.w], poc, 0.0)
+                                    : uyc;
+      if (qq == 0) {
+        const double uyb = Uy[r * q.uy.w + q.uy.dx + tx];
+        if (j > 1) {
+          uym = face_update(uyb, R, ir0, irc, Sir[ri - q.ir.w], g.idyc[j - 1], psc, Sps[rs - q.ps.w], pnc,
+                            Spn[rs - q.ps.w], poc, Spo[rs - q.ps.w], 0.0);
+        } else {
+          uym = uyb;
+          if (col) a.uyo[at(a.Luy, i, 0, k)] = uyb;  // the wall face below row 1
+        }
+      }
+      // upper z face; the lower one is the previous plane's upper face
+      const double uzp = face_update(Uz[r * q.uz.w + q.uz.dx + tx], R, ir0, Tir[ri], irc, idzc, Tps[rs], psc,
+                                     Tpn[rs], pnc, Tpo[rs], poc, 0.0);
+      const double uzl = uzq[qq];
+      uzq[qq] = uzp;
+      if (col && j <= g.ny) {
+        const long ox = at(a.Lux, i, j, k);
+        a.uxo[ox] = uxp;
+        if (i == g.nx) a.uxo[ox - i] = uxp;  // ux(0, j, k)
+        a.uyo[at(a.Luy, i, j, k)] = uyp;
+        const long oz = at(a.Luz, i, j, k);
+        a.uzo[oz] = uzp;
+        if (k == g.nz && !g.slab) a.uzo[oz - (long)k * a.Luz.sk] = uzp;  // uz(i, j, 0)
+        double dv = (uxp - uxm) * idx;
+        dv = dv + (uyp - uym) * g.idyf[j - 1];
+        dv = dv + (uzp - uzl) * idz;
+        vmax = nanmax_nonneg(vmax, dv);
+      }
+      uym = uyp;
+    }
+    __syncthreads();  // the slots of plane k are free for the copies of plane k+3
+  }
+  cp_async_wait_all();  // the last stage's periodic copies (not read)
+  block_max_atomic(vmax, maxdiv);
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = []() -> EncodeTiledFn {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &qr) != cudaSuccess ||
+        qr != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// Box geometry of an array with layout Ly: needed columns start at x index
+// fx (first cell or face minus ilo) and span nx_need, rows at fy and span
+// ny_need; nk_nom planes around the nominal first plane klo_nom.
+bool box_geom(const Lay &Ly, int first_i, int nx_need, int first_j, int ny_need, int klo_nom, BoxGeom *b) {
+  const int fx = first_i - Ly.ilo;
+  if (fx < 0 || first_j - Ly.jlo < 0 || klo_nom - Ly.klo < 1) return false;  // needs a halo on every side
+  b->xo = fx & ~1;
+  b->dx = fx & 1;
+  b->w = (b->dx + nx_need + 1) & ~1;
+  b->yo = first_j - Ly.jlo;
+  b->zo = -Ly.klo;
+  return b->w <= 256 && ny_need <= 256;
+}
+
+bool encode_box(CUtensorMap *m, const double *base, const Lay &Ly, long nk, const BoxGeom &b, int box_h) {
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (Ly.sj & 1) != 0 || (Ly.sk & 1) != 0) return false;
+  const EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)Ly.sj, (cuuint64_t)(Ly.sk / Ly.sj), (cuuint64_t)nk};
+  cuuint64_t strides[2] = {(cuuint64_t)Ly.sj * 8, (cuuint64_t)Ly.sk * 8};
+  cuuint32_t box[3] = {(cuuint32_t)b.w, (cuuint32_t)box_h, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the 2-D map of ux: dims (plane of sk values, planes), boxes of one row of kUxW
+bool encode_rows(CUtensorMap *m, const double *base, const Lay &Ly, long nk) {
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (Ly.sk & 1) != 0) return false;
+  const EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)Ly.sk, (cuuint64_t)nk};
+  cuuint64_t strides[1] = {(cuuint64_t)Ly.sk * 8};
+  cuuint32_t box[2] = {(cuuint32_t)kUxW, 1};
+  cuuint32_t es[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// planes per chunk: the chunk count that best fills whole waves of one CTA
+// per SM, counting the extra plane each chunk loads
+int pick_chunk(int tiles, int nz, int sms) {
+  int best = nz;
+  double best_eff = -1.0;
+  for (int c = 1; c <= 32 && c <= nz; ++c) {
+    const int len = (nz + c - 1) / c, chunks = (nz + len - 1) / len;
+    const long ctas = (long)tiles * chunks, waves = (ctas + sms - 1) / sms;
+    const double eff = (double)ctas / (double)(waves * sms) * (double)len / (double)(len + 1);
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = len;
+    }
+  }
+  return best;
+}
+
+}  // namespace
+
+cudaError_t prepare_correct_tma_kernel() {
+  return cudaFuncSetAttribute((const void *)k_correct_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kCorrTmaMaxSmem);
+}
+
+bool launch_correct_div_tma(const CorrArgs &ca, const GridK &g, unsigned long long *maxdiv, int sms,
+                            cudaStream_t st) {
+  CorrTmaGeom q{};
+  if (!box_geom(ca.Lpsi, 0, kCTX + 2, 0, kCTY + 2, 1, &q.ps) || !box_geom(ca.Lrho, 0, kCTX + 2, 0, kCTY + 2, 1, &q.ir) ||
+      !box_geom(ca.Luy, 1, kCTX, 0, kCTY + 1, 1, &q.uy) || !box_geom(ca.Luz, 1, kCTX, 1, kCTY, 0, &q.uz))
+    return false;
+  q.ux.fx = 0 - ca.Lux.ilo;  // face i0 - 1 of the origin tile
+  q.ux.yo = 1 - ca.Lux.jlo;
+  q.ux.zo = -ca.Lux.klo;
+  q.ux.sj = (int)ca.Lux.sj;
+  if (q.ux.fx < 1 || q.ux.yo < 1 || q.ux.zo < 0 || (ca.Lux.sk & 1) != 0) return false;  // a halo on every side
+  const CorrTmaSmem L = corr_tma_smem(q);
+  if (L.total + 128 > kCorrTmaMaxSmem) return false;
+  // planes in each array: the nominal range plus the halo on both sides
+  const long nk_s = g.nz + 2L * (1 - ca.Lpsi.klo), nk_r = g.nz + 2L * (1 - ca.Lrho.klo);
+  const long nk_u = g.nz + 2L * (1 - ca.Lux.klo), nk_v = g.nz + 2L * (1 - ca.Luy.klo);
+  const long nk_w = g.nz + 1 + 2L * (0 - ca.Luz.klo);
+  CUtensorMap m[7];
+  if (!encode_box(&m[0], ca.psi, ca.Lpsi, nk_s, q.ps, kCTY + 2) || !encode_box(&m[1], ca.pn, ca.Lpsi, nk_s, q.ps, kCTY + 2) ||
+      !encode_box(&m[2], ca.pnm1, ca.Lpsi, nk_s, q.ps, kCTY + 2) ||
+      !encode_box(&m[3], ca.irho, ca.Lrho, nk_r, q.ir, kCTY + 2) || !encode_rows(&m[4], ca.uxi, ca.Lux, nk_u) ||
+      !encode_box(&m[5], ca.uyi, ca.Luy, nk_v, q.uy, kCTY + 1) || !encode_box(&m[6], ca.uzi, ca.Luz, nk_w, q.uz, kCTY))
+    return false;
+  const int nbx = (g.nx + kCTX - 1) / kCTX, nby = (g.ny + kCTY - 1) / kCTY;
+  q.nzc = pick_chunk(nbx * nby, g.nz, sms > 0 ? sms : 148);
+  const dim3 grid((unsigned)nbx, (unsigned)nby, (unsigned)((g.nz + q.nzc - 1) / q.nzc));
+  k_correct_tma<<<grid, kCNT, (size_t)L.total + 128, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], m[6], ca, g, q, maxdiv);
+  return true;
+}
+
+}  // namespace tbfp

@@ -271,6 +271,11 @@ void launch_recip(const double *rho, double *irho, long n, cudaStream_t st);
 void launch_fftx_fwd_from_s(const double *s, Lay Ls, const GridK &g, const double2 *twx, const double2 *tpx,
                             double2 *spec, cudaStream_t st);
 void launch_rhs(const RhsArgs &ra, bool has_st, const GridK &g, double *s, Lay Ls, cudaStream_t st);
+// the correction with its inputs staged by TMA; false when the arrays do not
+// suit a tensor map (then nothing is launched)
+bool launch_correct_div_tma(const CorrArgs &ca, const GridK &g, unsigned long long *maxdiv, int sms,
+                            cudaStream_t st);
+cudaError_t prepare_correct_tma_kernel();
 // the right-hand side computed into the forward x transform's tiles (s is not stored)
 void launch_rhs_fftx(const RhsArgs &ra, bool has_st, const GridK &g, const double2 *twx, const double2 *tpx,
                      double2 *spec, cudaStream_t st);
