@@ -3,18 +3,18 @@
 // auxiliaryRoutines.f90:42-91), with its inputs staged by the tensor memory
 // accelerator (TMA).
 //
-// A CTA owns an x-y tile of kCTX x kCTY cells and marches a chunk of z planes.
-// For every plane, one thread issues seven tiled bulk copies
+// A CTA owns an x-y tile of kCTX x TY cells and marches a chunk of z planes.
+// For every plane, one thread issues the tiled bulk copies
 // (cp.async.bulk.tensor, no multicast): psi, psi^n, psi^(n-1) and 1/rho with a
 // one-cell halo in x and y, and the tile's ux, uy (with the face below the
-// tile) and uz.  The copies complete on an mbarrier.  Three plane slots form a
-// ring: while the threads correct plane k from the slots of planes k and k+1,
-// the copies of plane k+2 are in flight, so the load parallelism comes from
-// the copy engine instead of from resident warps.  The lower z face of a plane
-// is the upper face of the plane before (carried in registers); the chunk's
-// first plane computes it from one extra plane.  The x face below cell i = 1
-// is the upper face of cell nx (the periodic image), whose nine inputs per row
-// come in by 8-byte cp.async copies in the same ring.
+// tile) and uz.  The copies of a plane complete on one mbarrier.  NS slots
+// form a ring: while the threads correct plane k from the slots of planes k
+// and k+1, the copies of planes k+2 .. k+NS-2 are in flight, so the load
+// parallelism comes from the copy engine instead of from resident warps.  The
+// lower z face of a plane is the upper face of the plane before (carried in
+// registers); the chunk's first plane computes it from one extra plane.  The x
+// face below cell i = 1 is the upper face of cell nx (the periodic image),
+// whose nine inputs per row come in by 8-byte cp.async copies in the same ring.
 //
 // Every face is computed with the arguments and in the operation order of
 // correct_div_body (the kernel form, which serves surface tension and arrays
@@ -31,8 +31,7 @@ namespace tbfp {
 
 namespace {
 
-constexpr int kCTX = 128, kCTY = 8, kCNT = 256;
-constexpr int kCRows = kCTX * kCTY / kCNT;           // rows per thread (consecutive)
+constexpr int kCTX = 128;  // tile width; a CTA's threads are 128 columns x NT/128 row groups
 constexpr int kPer = 9;                               // periodic inputs per row
 constexpr long long kTmaWaitCycles = 4000000000LL;    // about 2 s of SM clock
 constexpr int kCorrTmaMaxSmem = 220 * 1024;  // under the opt-in limit with the static reduction buffer
@@ -98,86 +97,85 @@ struct CorrTmaGeom {
   int nzc;  // planes per chunk
 };
 
-// shared-memory carve-up (bytes), from the box widths
+// shared-memory carve-up of one ring slot (bytes), from the box widths
 struct CorrTmaSmem {
-  int sps, sir, ss;       // one psi-layout plane, one 1/rho plane, a scalar slot
-  int sux, suy, suz, us;  // velocity boxes and a velocity slot
-  int ps;                 // a periodic slot
-  int total;
+  int sps, sir;             // one psi-layout plane, one 1/rho plane
+  int sux, suy, suz, sper;  // velocity boxes, the periodic column
+  int slot, total;
 };
-__host__ __device__ inline CorrTmaSmem corr_tma_smem(const CorrTmaGeom &q) {
+__host__ __device__ inline CorrTmaSmem corr_tma_smem(const CorrTmaGeom &q, int ty, int ns) {
   CorrTmaSmem m;
-  m.sps = align128(q.ps.w * (kCTY + 2) * 8);
-  m.sir = align128(q.ir.w * (kCTY + 2) * 8);
-  m.ss = 3 * m.sps + m.sir;
-  m.sux = kUxLd * kCTY * 8;
-  m.suy = align128(q.uy.w * (kCTY + 1) * 8);
-  m.suz = align128(q.uz.w * kCTY * 8);
-  m.us = m.sux + m.suy + m.suz;
-  m.ps = align128(kPer * kCTY * 8);
-  m.total = 3 * m.ss + 3 * m.us + 3 * m.ps + 3 * 8;
+  m.sps = align128(q.ps.w * (ty + 2) * 8);
+  m.sir = align128(q.ir.w * (ty + 2) * 8);
+  m.sux = kUxLd * ty * 8;
+  m.suy = align128(q.uy.w * (ty + 1) * 8);
+  m.suz = align128(q.uz.w * ty * 8);
+  m.sper = align128(kPer * ty * 8);
+  m.slot = 3 * m.sps + m.sir + m.sux + m.suy + m.suz + m.sper;
+  m.total = ns * m.slot + ns * 8;
   return m;
 }
 
-__global__ void __launch_bounds__(kCNT, 1)
+template <int TY, int NS, int NT>
+__global__ void __launch_bounds__(NT, 1)
     k_correct_tma(const __grid_constant__ CUtensorMap m_ps, const __grid_constant__ CUtensorMap m_pn,
                   const __grid_constant__ CUtensorMap m_po, const __grid_constant__ CUtensorMap m_ir,
                   const __grid_constant__ CUtensorMap m_ux, const __grid_constant__ CUtensorMap m_uy,
                   const __grid_constant__ CUtensorMap m_uz, CorrArgs a, GridK g, CorrTmaGeom q,
                   unsigned long long *__restrict__ maxdiv) {
+  constexpr int NG = NT / kCTX, RPT = TY / NG;  // row groups, consecutive rows per thread
+  static_assert(NT % kCTX == 0 && TY % NG == 0 && NS >= 3, "whole row groups; at least one plane in flight");
   extern __shared__ __align__(128) unsigned char smc[];
   const int tid = threadIdx.x, tx = tid & (kCTX - 1), tg = tid / kCTX;
   const int bx = blockIdx.x, by = blockIdx.y;
-  const int i0 = 1 + kCTX * bx, j0 = 1 + kCTY * by;
+  const int i0 = 1 + kCTX * bx, j0 = 1 + TY * by;
   const int k0 = 1 + q.nzc * (int)blockIdx.z;
   if (k0 > g.nz) return;  // whole CTA
   const int k1 = min(k0 + q.nzc - 1, g.nz);
   const int km0 = (k0 == 1 && !g.slab) ? g.nz : k0 - 1;
-  const CorrTmaSmem L = corr_tma_smem(q);
-  // copy destinations on 128-byte boundaries (the launch adds 128 bytes of slack)
-  // 3 scalar slots (psi, psi^n, psi^(n-1), 1/rho)
-  unsigned char *sc = smc + ((128u - (smem_u32(smc) & 127u)) & 127u);
-  unsigned char *su = sc + 3 * L.ss;        // 3 velocity slots: ux, uy, uz
-  double *sp = reinterpret_cast<double *>(su + 3 * L.us);  // 3 periodic slots [value][row]
-  unsigned long long *bars = reinterpret_cast<unsigned long long *>(su + 3 * L.us + 3 * L.ps);
-  const int PSD = L.ps / 8;
-  const unsigned bps = (unsigned)(q.ps.w * (kCTY + 2) * 8), bir = (unsigned)(q.ir.w * (kCTY + 2) * 8);
-  const unsigned bux = (unsigned)(kUxW * kCTY * 8), buy = (unsigned)(q.uy.w * (kCTY + 1) * 8),
-                 buz = (unsigned)(q.uz.w * kCTY * 8);
+  const CorrTmaSmem L = corr_tma_smem(q, TY, NS);
+  // NS slots [psi | psi^n | psi^(n-1) | 1/rho | ux | uy | uz | periodic], copy
+  // destinations on 128-byte boundaries (the launch adds 128 bytes of slack)
+  unsigned char *base = smc + ((128u - (smem_u32(smc) & 127u)) & 127u);
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(base + NS * L.slot);
+  const int o_pn = L.sps, o_po = 2 * L.sps, o_ir = 3 * L.sps, o_ux = o_ir + L.sir, o_uy = o_ux + L.sux,
+            o_uz = o_uy + L.suy, o_per = o_uz + L.suz;
+  const unsigned bps = (unsigned)(q.ps.w * (TY + 2) * 8), bir = (unsigned)(q.ir.w * (TY + 2) * 8);
+  const unsigned bux = (unsigned)(kUxW * TY * 8), buy = (unsigned)(q.uy.w * (TY + 1) * 8),
+                 buz = (unsigned)(q.uz.w * TY * 8);
 
   if (tid == 0) {
-    for (int m = 0; m < 3; ++m) mbar_init(smem_u32(bars + m), 1);
+    for (int m = 0; m < NS; ++m) mbar_init(smem_u32(bars + m), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
 
-  // stage t: scalars of plane p_t into scalar slot (t+1)%3 and, for t >= 0,
-  // the velocities of p_t into velocity slot t%3 (stage -1: uz only, slot 2),
-  // all on mbarrier (t+1)%3; p_{-1} = km0, p_t = k0 + t
+  // stage t: plane p_t (p_{-1} = km0, p_t = k0 + t) into slot (t+1)%NS on
+  // mbarrier (t+1)%NS: the four scalar boxes and uz, and for t >= 0 also ux,
+  // uy and the periodic column
   auto issue = [&](int t) {
     const int pl = (t < 0) ? km0 : k0 + t;
-    const int S = (t + 1) % 3, U = (t + 3) % 3;
+    const int S = (t + 1) % NS;
+    unsigned char *s = base + S * L.slot;
     if (tid == 0) {
       const unsigned bar = smem_u32(bars + S);
       mbar_expect_tx(bar, 3 * bps + bir + buz + (t >= 0 ? bux + buy : 0u));
-      unsigned char *s = sc + S * L.ss;
-      const int xs = q.ps.xo + kCTX * bx, ys = q.ps.yo + kCTY * by, zs = q.ps.zo + pl;
+      const int xs = q.ps.xo + kCTX * bx, ys = q.ps.yo + TY * by, zs = q.ps.zo + pl;
       tma_load3(smem_u32(s), &m_ps, xs, ys, zs, bar);
-      tma_load3(smem_u32(s + L.sps), &m_pn, xs, ys, zs, bar);
-      tma_load3(smem_u32(s + 2 * L.sps), &m_po, xs, ys, zs, bar);
-      tma_load3(smem_u32(s + 3 * L.sps), &m_ir, q.ir.xo + kCTX * bx, q.ir.yo + kCTY * by, q.ir.zo + pl, bar);
-      unsigned char *u = su + U * L.us;
+      tma_load3(smem_u32(s + o_pn), &m_pn, xs, ys, zs, bar);
+      tma_load3(smem_u32(s + o_po), &m_po, xs, ys, zs, bar);
+      tma_load3(smem_u32(s + o_ir), &m_ir, q.ir.xo + kCTX * bx, q.ir.yo + TY * by, q.ir.zo + pl, bar);
       if (t >= 0) {
-        for (int r = 0; r < kCTY; ++r) {
-          const int e = (q.ux.yo + kCTY * by + r) * q.ux.sj + q.ux.fx + kCTX * bx;
-          tma_load2(smem_u32(u + r * kUxLd * 8), &m_ux, e & ~1, q.ux.zo + pl, bar);
+        for (int r = 0; r < TY; ++r) {
+          const int e = (q.ux.yo + TY * by + r) * q.ux.sj + q.ux.fx + kCTX * bx;
+          tma_load2(smem_u32(s + o_ux + r * kUxLd * 8), &m_ux, e & ~1, q.ux.zo + pl, bar);
         }
-        tma_load3(smem_u32(u + L.sux), &m_uy, q.uy.xo + kCTX * bx, q.uy.yo + kCTY * by, q.uy.zo + pl, bar);
+        tma_load3(smem_u32(s + o_uy), &m_uy, q.uy.xo + kCTX * bx, q.uy.yo + TY * by, q.uy.zo + pl, bar);
       }
-      tma_load3(smem_u32(u + L.sux + L.suy), &m_uz, q.uz.xo + kCTX * bx, q.uz.yo + kCTY * by, q.uz.zo + pl, bar);
+      tma_load3(smem_u32(s + o_uz), &m_uz, q.uz.xo + kCTX * bx, q.uz.yo + TY * by, q.uz.zo + pl, bar);
     }
-    if (bx == 0 && t >= 0 && tid < kPer * kCTY) {
+    if (bx == 0 && t >= 0 && tid < kPer * TY) {
       // inputs of the upper x face of cell nx, row j (clamped into the array)
       const int r = tid / kPer, v = tid - r * kPer, j = min(j0 + r, g.ny);
       const int ic = g.nx + (v < 8 ? (v & 1) : 0);
@@ -187,24 +185,26 @@ __global__ void __launch_bounds__(kCNT, 1)
       else if (v < 6) src = a.pnm1 + at(a.Lpsi, ic, j, pl);
       else if (v < 8) src = a.irho + at(a.Lrho, ic, j, pl);
       else src = a.uxi + at(a.Lux, g.nx, j, pl);
-      cp_async8(sp + S * PSD + v * kCTY + r, src);
+      cp_async8(reinterpret_cast<double *>(s + o_per) + v * TY + r, src);
     }
     cp_async_commit();
   };
 
   const int nlast = k1 - k0, tmax = nlast + 1;
-  int waited = 0;  // stages -1 .. waited-1 have been waited for
-  int issued = 1;  // stages up to this one are issued
-  issue(-1);
-  issue(0);
-  issue(1);
-  auto drain_and_fail = [&]() {
-    if (tid == 0) {
-      for (int t = waited; t <= issued; ++t) {
-        const int m = (t + 1) % 3;
-        mbar_wait_bounded(smem_u32(bars + m), (unsigned)(((t + 1) / 3) & 1));
-      }
+  int waited = -1;  // the next stage to wait for
+  int issued = -1;  // the last stage issued
+  for (int t = -1; t <= NS - 2; ++t) {  // one cp.async group per stage, issued or not
+    if (t <= tmax) {
+      issue(t);
+      issued = t;
+    } else {
+      cp_async_commit();
     }
+  }
+  auto drain_and_fail = [&]() {
+    if (tid == 0)
+      for (int t = waited; t <= issued; ++t)
+        mbar_wait_bounded(smem_u32(bars + (t + 1) % NS), (unsigned)(((t + 1) / NS) & 1));
     cp_async_wait_all();
     __syncthreads();
     if (tid == 0) atomicMax(maxdiv, 0x7ff8000000000000ull);  // NaN: a copy did not complete in time
@@ -214,26 +214,25 @@ __global__ void __launch_bounds__(kCNT, 1)
   const int i = i0 + tx;
   const bool col = i <= g.nx;
   const double idx = col ? g.idxf[i - 1] : 0.0;
+  auto dslot = [&](int S, int off) { return reinterpret_cast<const double *>(base + S * L.slot + off); };
 
   // the lower z face of the chunk's first plane, from planes km0 (slot 0) and k0 (slot 1)
-  double uzq[kCRows];
+  double uzq[RPT];
   {
     bool bad = !mbar_wait_bounded(smem_u32(bars + 0), 0u);
     bad = !mbar_wait_bounded(smem_u32(bars + 1), 0u) || bad;
-    cp_async_wait_group<1>();
+    cp_async_wait_group<NS - 2>();
     if (__syncthreads_or(bad)) {
-      waited = -1;
       drain_and_fail();
       return;
     }
     waited = 1;
-    const double *P0 = reinterpret_cast<const double *>(sc), *P1 = reinterpret_cast<const double *>(sc + L.ss);
-    const double *Uzm = reinterpret_cast<const double *>(su + 2 * L.us + L.sux + L.suy);
+    const double *P0 = dslot(0, 0), *P1 = dslot(1, 0), *Uzm = dslot(0, o_uz);
+    const int so = L.sps / 8, io = o_ir / 8;
 #pragma unroll
-    for (int qq = 0; qq < kCRows; ++qq) {
-      const int r = kCRows * tg + qq;
+    for (int qq = 0; qq < RPT; ++qq) {
+      const int r = RPT * tg + qq;
       const int rs = (r + 1) * q.ps.w + q.ps.dx + 1 + tx, ri = (r + 1) * q.ir.w + q.ir.dx + 1 + tx;
-      const int so = L.sps / 8, io = 3 * L.sps / 8;
       uzq[qq] = face_update(Uzm[r * q.uz.w + q.uz.dx + tx], R, ir0, P1[io + ri], P0[io + ri], idzc, P1[rs], P0[rs],
                             P1[so + rs], P0[so + rs], P1[2 * so + rs], P0[2 * so + rs], 0.0);
     }
@@ -243,45 +242,40 @@ __global__ void __launch_bounds__(kCNT, 1)
   for (int n = 0; n <= nlast; ++n) {
     const int k = k0 + n;
     {
-      const int t = n + 1;  // scalars of plane k+1
-      const bool bad = !mbar_wait_bounded(smem_u32(bars + (t + 1) % 3), (unsigned)(((t + 1) / 3) & 1));
-      cp_async_wait_group<1>();  // the periodic column of plane k
+      const int t = n + 1;  // plane k+1
+      const bool bad = !mbar_wait_bounded(smem_u32(bars + (t + 1) % NS), (unsigned)(((t + 1) / NS) & 1));
+      cp_async_wait_group<NS - 2>();  // the periodic column of plane k
       if (__syncthreads_or(bad)) {
         drain_and_fail();
         return;
       }
       waited = t + 1;
     }
-    if (n + 2 <= tmax) {
-      issue(n + 2);
-      issued = n + 2;
+    if (n + NS - 1 <= tmax) {  // into the slot of plane k-1, free since the last barrier
+      issue(n + NS - 1);
+      issued = n + NS - 1;
     } else {
-      cp_async_commit();  // keeps one group per plane
+      cp_async_commit();
     }
-    const int K = (n + 1) % 3, K1 = (n + 2) % 3, U = n % 3;
-    const double *Sps = reinterpret_cast<const double *>(sc + K * L.ss);
-    const double *Spn = Sps + L.sps / 8, *Spo = Sps + 2 * (L.sps / 8), *Sir = Sps + 3 * (L.sps / 8);
-    const double *Tps = reinterpret_cast<const double *>(sc + K1 * L.ss);
-    const double *Tpn = Tps + L.sps / 8, *Tpo = Tps + 2 * (L.sps / 8), *Tir = Tps + 3 * (L.sps / 8);
-    const double *Ux = reinterpret_cast<const double *>(su + U * L.us);
-    const double *Uy = reinterpret_cast<const double *>(su + U * L.us + L.sux);
-    const double *Uz = reinterpret_cast<const double *>(su + U * L.us + L.sux + L.suy);
-    const double *Pe = sp + K * PSD;
+    const int K = (n + 1) % NS, K1 = (n + 2) % NS;
+    const double *Sps = dslot(K, 0), *Spn = dslot(K, o_pn), *Spo = dslot(K, o_po), *Sir = dslot(K, o_ir);
+    const double *Tps = dslot(K1, 0), *Tpn = dslot(K1, o_pn), *Tpo = dslot(K1, o_po), *Tir = dslot(K1, o_ir);
+    const double *Ux = dslot(K, o_ux), *Uy = dslot(K, o_uy), *Uz = dslot(K, o_uz), *Pe = dslot(K, o_per);
     const double idz = g.idzf[k - 1];
     double uym = 0.0;
 #pragma unroll
-    for (int qq = 0; qq < kCRows; ++qq) {
-      const int r = kCRows * tg + qq, j = j0 + r;
+    for (int qq = 0; qq < RPT; ++qq) {
+      const int r = RPT * tg + qq, j = j0 + r;
       const int rs = (r + 1) * q.ps.w + q.ps.dx + 1 + tx, ri = (r + 1) * q.ir.w + q.ir.dx + 1 + tx;
       const double psc = Sps[rs], pnc = Spn[rs], poc = Spo[rs], irc = Sir[ri];
       // upper and lower x faces (ux(i) at column rx + 1 of the row's box)
-      const int rx = r * kUxLd + (((q.ux.yo + kCTY * by + r) * q.ux.sj + q.ux.fx) & 1) + tx;
+      const int rx = r * kUxLd + (((q.ux.yo + TY * by + r) * q.ux.sj + q.ux.fx) & 1) + tx;
       const double uxp = face_update(Ux[rx + 1], R, ir0, Sir[ri + 1], irc, idxc, Sps[rs + 1], psc, Spn[rs + 1], pnc,
                                      Spo[rs + 1], poc, 0.0);
       double uxm;
       if (i == 1) {
-        uxm = face_update(Pe[8 * kCTY + r], R, ir0, Pe[7 * kCTY + r], Pe[6 * kCTY + r], idxc, Pe[1 * kCTY + r],
-                          Pe[0 * kCTY + r], Pe[3 * kCTY + r], Pe[2 * kCTY + r], Pe[5 * kCTY + r], Pe[4 * kCTY + r], 0.0);
+        uxm = face_update(Pe[8 * TY + r], R, ir0, Pe[7 * TY + r], Pe[6 * TY + r], idxc, Pe[1 * TY + r],
+                          Pe[0 * TY + r], Pe[3 * TY + r], Pe[2 * TY + r], Pe[5 * TY + r], Pe[4 * TY + r], 0.0);
       } else {
         uxm = face_update(Ux[rx], R, ir0, irc, Sir[ri - 1], idxc, psc, Sps[rs - 1], pnc, Spn[rs - 1], poc,
                           Spo[rs - 1], 0.0);
@@ -321,9 +315,9 @@ __global__ void __launch_bounds__(kCNT, 1)
       }
       uym = uyp;
     }
-    __syncthreads();  // the slots of plane k are free for the copies of plane k+3
+    __syncthreads();  // the slot of plane k is free for the copies of plane k+NS-1
   }
-  cp_async_wait_all();  // the last stage's periodic copies (not read)
+  cp_async_wait_all();  // the periodic copies of stages past the chunk (not read)
   block_max_atomic(vmax, maxdiv);
 }
 
@@ -403,38 +397,41 @@ int pick_chunk(int tiles, int nz, int sms) {
 
 }  // namespace
 
+// tile height and ring depth of the launch
+constexpr int kTY = 8, kNS = 3, kCNT = 512;
+
 cudaError_t prepare_correct_tma_kernel() {
-  return cudaFuncSetAttribute((const void *)k_correct_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute((const void *)k_correct_tma<kTY, kNS, kCNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kCorrTmaMaxSmem);
 }
 
 bool launch_correct_div_tma(const CorrArgs &ca, const GridK &g, unsigned long long *maxdiv, int sms,
                             cudaStream_t st) {
   CorrTmaGeom q{};
-  if (!box_geom(ca.Lpsi, 0, kCTX + 2, 0, kCTY + 2, 1, &q.ps) || !box_geom(ca.Lrho, 0, kCTX + 2, 0, kCTY + 2, 1, &q.ir) ||
-      !box_geom(ca.Luy, 1, kCTX, 0, kCTY + 1, 1, &q.uy) || !box_geom(ca.Luz, 1, kCTX, 1, kCTY, 0, &q.uz))
+  if (!box_geom(ca.Lpsi, 0, kCTX + 2, 0, kTY + 2, 1, &q.ps) || !box_geom(ca.Lrho, 0, kCTX + 2, 0, kTY + 2, 1, &q.ir) ||
+      !box_geom(ca.Luy, 1, kCTX, 0, kTY + 1, 1, &q.uy) || !box_geom(ca.Luz, 1, kCTX, 1, kTY, 0, &q.uz))
     return false;
   q.ux.fx = 0 - ca.Lux.ilo;  // face i0 - 1 of the origin tile
   q.ux.yo = 1 - ca.Lux.jlo;
   q.ux.zo = -ca.Lux.klo;
   q.ux.sj = (int)ca.Lux.sj;
   if (q.ux.fx < 1 || q.ux.yo < 1 || q.ux.zo < 0 || (ca.Lux.sk & 1) != 0) return false;  // a halo on every side
-  const CorrTmaSmem L = corr_tma_smem(q);
+  const CorrTmaSmem L = corr_tma_smem(q, kTY, kNS);
   if (L.total + 128 > kCorrTmaMaxSmem) return false;
   // planes in each array: the nominal range plus the halo on both sides
   const long nk_s = g.nz + 2L * (1 - ca.Lpsi.klo), nk_r = g.nz + 2L * (1 - ca.Lrho.klo);
   const long nk_u = g.nz + 2L * (1 - ca.Lux.klo), nk_v = g.nz + 2L * (1 - ca.Luy.klo);
   const long nk_w = g.nz + 1 + 2L * (0 - ca.Luz.klo);
   CUtensorMap m[7];
-  if (!encode_box(&m[0], ca.psi, ca.Lpsi, nk_s, q.ps, kCTY + 2) || !encode_box(&m[1], ca.pn, ca.Lpsi, nk_s, q.ps, kCTY + 2) ||
-      !encode_box(&m[2], ca.pnm1, ca.Lpsi, nk_s, q.ps, kCTY + 2) ||
-      !encode_box(&m[3], ca.irho, ca.Lrho, nk_r, q.ir, kCTY + 2) || !encode_rows(&m[4], ca.uxi, ca.Lux, nk_u) ||
-      !encode_box(&m[5], ca.uyi, ca.Luy, nk_v, q.uy, kCTY + 1) || !encode_box(&m[6], ca.uzi, ca.Luz, nk_w, q.uz, kCTY))
+  if (!encode_box(&m[0], ca.psi, ca.Lpsi, nk_s, q.ps, kTY + 2) || !encode_box(&m[1], ca.pn, ca.Lpsi, nk_s, q.ps, kTY + 2) ||
+      !encode_box(&m[2], ca.pnm1, ca.Lpsi, nk_s, q.ps, kTY + 2) ||
+      !encode_box(&m[3], ca.irho, ca.Lrho, nk_r, q.ir, kTY + 2) || !encode_rows(&m[4], ca.uxi, ca.Lux, nk_u) ||
+      !encode_box(&m[5], ca.uyi, ca.Luy, nk_v, q.uy, kTY + 1) || !encode_box(&m[6], ca.uzi, ca.Luz, nk_w, q.uz, kTY))
     return false;
-  const int nbx = (g.nx + kCTX - 1) / kCTX, nby = (g.ny + kCTY - 1) / kCTY;
+  const int nbx = (g.nx + kCTX - 1) / kCTX, nby = (g.ny + kTY - 1) / kTY;
   q.nzc = pick_chunk(nbx * nby, g.nz, sms > 0 ? sms : 148);
   const dim3 grid((unsigned)nbx, (unsigned)nby, (unsigned)((g.nz + q.nzc - 1) / q.nzc));
-  k_correct_tma<<<grid, kCNT, (size_t)L.total + 128, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], m[6], ca, g, q, maxdiv);
+  k_correct_tma<kTY, kNS, kCNT><<<grid, kCNT, (size_t)L.total + 128, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], m[6], ca, g, q, maxdiv);
   return true;
 }
 
