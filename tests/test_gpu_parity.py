@@ -109,6 +109,47 @@ def test_golden_projection(path, mode):
         eqn.close()
 
 
+def _widen(f: Field, hd: int) -> Field:
+    """f re-embedded with halo hd >= f.hd; the extra outer layers hold NaN,
+    so any read of them shows up in the results."""
+    w = Field(f.kind, hd, f.nx, f.ny, f.nz, torch.full(
+        tuple(s + 2 * (hd - f.hd) for s in f.a.shape), float("nan"), dtype=f.a.dtype, device=f.a.device))
+    d = hd - f.hd
+    w.a[d:d + f.a.shape[0], d:d + f.a.shape[1], d:d + f.a.shape[2]] = f.a
+    return w
+
+
+@pytest.mark.gpu
+def test_projection_with_wider_halos_matches_default_halos():
+    """The out-of-place projection with psi and rho halos of 2 and velocity
+    halos of 3 against the same projection with the default halos (1 and 2).
+    Odd and even halos shift the tensor-map boxes of the staged correction by
+    one column (the 16-byte start rule), so both offsets of every box run here;
+    x tiles of 128 with a partial last tile, ny not a multiple of the tile
+    height.  The arithmetic is the same, so the interiors agree to the bit."""
+    spec = synth.small_spec(192, 20, 12, stretched=True, nbubbles=2, radius=0.3, rhog=0.05)
+    inp = synth.make_inputs(spec, seed=13, device="cuda")
+    g = inp.grid
+    out = []
+    for hps, hu in ((1, 2), (2, 3)):
+        rho, pn, pnm1 = (_widen(f, hps) for f in (inp.rho, inp.psi_n, inp.psi_nm1))
+        u = VField(*[_widen(f, hu) for f in inp.u.components()])
+        psi = Field("cl", hps, g.nx, g.ny, g.nz, torch.zeros(
+            tuple(s + 2 * (hps - 1) for s in inp.psi_n.a.shape), dtype=torch.float64, device="cuda"))
+        uo = VField(*[Field.like(f, torch.zeros_like(f.a)) for f in u.components()])
+        eqn = PoissonEqn(g, spec.rhol, spec.rhog, hd_psi=hps, hd_rho=hps, hd_u=hu)
+        try:
+            st = eqn.projection(psi, pn, pnm1, rho, u, inp.dt, inp.alpha, u_out=uo)
+        finally:
+            eqn.close()
+        out.append(([_np(psi).interior().copy()] + [_np(f).interior().copy() for f in uo.components()], st.max_div))
+    (a, mda), (b, mdb) = out
+    for x, y in zip(a, b):
+        assert np.isfinite(y).all()
+        assert np.array_equal(x, y)
+    assert mda == mdb and np.isfinite(mdb)
+
+
 # ---------------------------------------------------------------------------
 def _case(nx, ny, nz, stretched, nb=2, radius=0.3, seed=5, rhog=0.05):
     spec = synth.small_spec(nx, ny, nz, stretched=stretched, nbubbles=nb, radius=radius, rhog=rhog)
