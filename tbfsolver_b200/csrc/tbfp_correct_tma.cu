@@ -216,17 +216,19 @@ __global__ void __launch_bounds__(NT, 1)
   const double idx = col ? g.idxf[i - 1] : 0.0;
   auto dslot = [&](int S, int off) { return reinterpret_cast<const double *>(base + S * L.slot + off); };
 
-  // the lower z face of the chunk's first plane, from planes km0 (slot 0) and k0 (slot 1)
+  // the lower z face of the chunk's first plane, from planes km0 (slot 0) and
+  // k0 (slot 1); plane k0+1 (slot 2) is waited for as well
   double uzq[RPT];
   {
     bool bad = !mbar_wait_bounded(smem_u32(bars + 0), 0u);
     bad = !mbar_wait_bounded(smem_u32(bars + 1), 0u) || bad;
-    cp_async_wait_group<NS - 2>();
+    bad = !mbar_wait_bounded(smem_u32(bars + 2 % NS), (unsigned)((2 / NS) & 1)) || bad;
+    cp_async_wait_group<NS - 2>();  // the periodic columns of stages -1 and 0
     if (__syncthreads_or(bad)) {
       drain_and_fail();
       return;
     }
-    waited = 1;
+    waited = 2;
     const double *P0 = dslot(0, 0), *P1 = dslot(1, 0), *Uzm = dslot(0, o_uz);
     const int so = L.sps / 8, io = o_ir / 8;
 #pragma unroll
@@ -237,26 +239,20 @@ __global__ void __launch_bounds__(NT, 1)
                             P1[so + rs], P0[so + rs], P1[2 * so + rs], P0[2 * so + rs], 0.0);
     }
   }
+  __syncthreads();  // slot 0 (plane km0) is free
+  if (NS - 1 <= tmax) {
+    issue(NS - 1);
+    issued = NS - 1;
+  } else {
+    cp_async_commit();  // keeps one group per stage
+  }
 
+  // One barrier per plane: after plane k, wait for the copies of plane k+2
+  // and the periodic column of plane k+1, then one barrier both publishes
+  // them to every thread and frees the slot of plane k for plane k+NS.
   double vmax = 0.0;
   for (int n = 0; n <= nlast; ++n) {
     const int k = k0 + n;
-    {
-      const int t = n + 1;  // plane k+1
-      const bool bad = !mbar_wait_bounded(smem_u32(bars + (t + 1) % NS), (unsigned)(((t + 1) / NS) & 1));
-      cp_async_wait_group<NS - 2>();  // the periodic column of plane k
-      if (__syncthreads_or(bad)) {
-        drain_and_fail();
-        return;
-      }
-      waited = t + 1;
-    }
-    if (n + NS - 1 <= tmax) {  // into the slot of plane k-1, free since the last barrier
-      issue(n + NS - 1);
-      issued = n + NS - 1;
-    } else {
-      cp_async_commit();
-    }
     const int K = (n + 1) % NS, K1 = (n + 2) % NS;
     const double *Sps = dslot(K, 0), *Spn = dslot(K, o_pn), *Spo = dslot(K, o_po), *Sir = dslot(K, o_ir);
     const double *Tps = dslot(K1, 0), *Tpn = dslot(K1, o_pn), *Tpo = dslot(K1, o_po), *Tir = dslot(K1, o_ir);
@@ -315,7 +311,23 @@ __global__ void __launch_bounds__(NT, 1)
       }
       uym = uyp;
     }
-    __syncthreads();  // the slot of plane k is free for the copies of plane k+NS-1
+    if (n == nlast) break;
+    {
+      const int t = n + 2;  // plane k+2 (t <= tmax since n < nlast)
+      const bool bad = !mbar_wait_bounded(smem_u32(bars + (t + 1) % NS), (unsigned)(((t + 1) / NS) & 1));
+      cp_async_wait_group<NS - 2>();  // the periodic column of plane k+1
+      if (__syncthreads_or(bad)) {
+        drain_and_fail();
+        return;
+      }
+      waited = t + 1;
+    }
+    if (n + NS <= tmax) {  // into the slot of plane k
+      issue(n + NS);
+      issued = n + NS;
+    } else {
+      cp_async_commit();
+    }
   }
   cp_async_wait_all();  // the periodic copies of stages past the chunk (not read)
   block_max_atomic(vmax, maxdiv);
