@@ -151,45 +151,37 @@ __device__ __forceinline__ void fftx_fwd_body(XSrc src, GridK g, const V *__rest
     }
   }
   fft_warp<V, M, LOGRPW, 1, LD, false>(wsm, lane, tw);
+  __syncthreads();  // every row transformed
 
-  // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx)
-  constexpr int NPAIR = M / 2 + 1, NPC = (NPAIR + 31) / 32;
+  // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx),
+  // applied on the way out: a thread takes the pair Z_k, Z_{M-k} of one row and
+  // writes X_k and X_{M-k} to S
+  constexpr int NPAIR = M / 2 + 1, NST = NPAIR << LOGTJ;
   const T half = T(0.5);
 #pragma unroll
-  for (int rl = 0; rl < RPW; ++rl) {
-    V *Z = wsm + rl * LD;
-#pragma unroll
-    for (int c = 0; c < NPC; ++c) {
-      const int kk = lane + 32 * c;
-      if (kk >= NPAIR) break;
-      if (kk == 0) {
-        const V z0 = Z[0];
-        Z[0] = mk<V>(z0.x + z0.y, T(0));
-        Z[pad8(M)] = mk<V>(z0.x - z0.y, T(0));
-      } else {
-        const int km = M - kk;
-        const V a = Z[pad8(kk)], b = Z[pad8(km)];
-        const V wa = __ldg(twx + kk), wb = __ldg(twx + km);
-        V ep = mk<V>(a.x + b.x, a.y - b.y);  // Z_k + conj Z_{M-k}
-        V em = mk<V>(a.x - b.x, a.y + b.y);  // Z_k - conj Z_{M-k}
-        V t1 = cmul(wa, em);                  // W^k * em
-        Z[pad8(kk)] = mk<V>(half * (ep.x + t1.y), half * (ep.y - t1.x));  // (ep - i t1)/2
-        if (km != kk) {
-          V fp = mk<V>(b.x + a.x, b.y - a.y);
-          V fm = mk<V>(b.x - a.x, b.y + a.y);
-          V t2 = cmul(wb, fm);
-          Z[pad8(km)] = mk<V>(half * (fp.x + t2.y), half * (fp.y - t2.x));
-        }
+  for (int t = threadIdx.x; t < NST; t += kNT) {
+    const int kk = t >> LOGTJ, row = t & (TJ - 1), km = M - kk;
+    if (row >= nrows) continue;
+    const V *Z = sm + row * LD;
+    V *o = spec + r0 + row;
+    if (kk == 0) {
+      const V z0 = Z[0];
+      o[0] = mk<V>(z0.x + z0.y, T(0));
+      o[(long)M * g.R] = mk<V>(z0.x - z0.y, T(0));
+    } else {
+      const V a = Z[pad8(kk)], b = Z[pad8(km)];
+      const V wa = __ldg(twx + kk), wb = __ldg(twx + km);
+      V ep = mk<V>(a.x + b.x, a.y - b.y);  // Z_k + conj Z_{M-k}
+      V em = mk<V>(a.x - b.x, a.y + b.y);  // Z_k - conj Z_{M-k}
+      V t1 = cmul(wa, em);                  // W^k * em
+      o[(long)kk * g.R] = mk<V>(half * (ep.x + t1.y), half * (ep.y - t1.x));  // (ep - i t1)/2
+      if (km != kk) {
+        V fp = mk<V>(b.x + a.x, b.y - a.y);
+        V fm = mk<V>(b.x - a.x, b.y + a.y);
+        V t2 = cmul(wb, fm);
+        o[(long)km * g.R] = mk<V>(half * (fp.x + t2.y), half * (fp.y - t2.x));
       }
     }
-  }
-  __syncthreads();
-  // S[kx][r0 + row]: consecutive threads take consecutive rows of one kx
-  constexpr int NST = ((M + 1) << LOGTJ);
-#pragma unroll
-  for (int t = threadIdx.x; t < NST; t += kNT) {
-    const int kx = t >> LOGTJ, row = t & (TJ - 1);
-    if (row < nrows) spec[(long)kx * g.R + r0 + row] = sm[row * LD + pad8(kx)];
   }
 }
 
@@ -289,45 +281,37 @@ __device__ __forceinline__ void fftx_inv_body(const V *__restrict__ spec, double
   for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = __ldg(tpx + t);
   const int r0 = bx << LOGTJ;
   const int nrows = min(TJ, (int)g.R - r0);
-  constexpr int NLD = ((M + 1) << LOGTJ);
+  // Z[k] = (X_k + conj X_{M-k}) + i conj(W^k) (X_k - conj X_{M-k}),  k = 0..M-1,
+  // applied as the spectrum comes in (a thread loads the pair X_k, X_{M-k} of a row)
+  constexpr int NPAIR = M / 2 + 1, NLD = NPAIR << LOGTJ;
 #pragma unroll
   for (int t = threadIdx.x; t < NLD; t += kNT) {
-    const int kx = t >> LOGTJ, row = t & (TJ - 1);
-    sm[row * LD + pad8(kx)] = (row < nrows) ? ldc<COH>(spec + ((long)kx * g.R + r0 + row)) : mk<V>(T(0), T(0));
+    const int kk = t >> LOGTJ, row = t & (TJ - 1), km = M - kk;
+    V *X = sm + row * LD;
+    V a = mk<V>(T(0), T(0)), b = a;
+    if (row < nrows) {
+      a = ldc<COH>(spec + ((long)kk * g.R + r0 + row));
+      b = ldc<COH>(spec + ((long)km * g.R + r0 + row));
+    }
+    if (kk == 0) {
+      X[0] = mk<V>(a.x + b.x, a.x - b.x);  // the imaginary parts of X_0 and X_M are ignored
+    } else {
+      const V wa = cconj(__ldg(twx + kk)), wb = cconj(__ldg(twx + km));
+      V ep = mk<V>(a.x + b.x, a.y - b.y);
+      V em = mk<V>(a.x - b.x, a.y + b.y);
+      V t1 = cmul(wa, em);
+      X[pad8(kk)] = mk<V>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
+      if (km != kk) {
+        V fp = mk<V>(b.x + a.x, b.y - a.y);
+        V fm = mk<V>(b.x - a.x, b.y + a.y);
+        V t2 = cmul(wb, fm);
+        X[pad8(km)] = mk<V>(fp.x - t2.y, fp.y + t2.x);
+      }
+    }
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   V *wsm = sm + warp * RPW * LD;
-  // Z[k] = (X_k + conj X_{M-k}) + i conj(W^k) (X_k - conj X_{M-k}),  k = 0..M-1
-  constexpr int NPAIR = M / 2 + 1, NPC = (NPAIR + 31) / 32;
-#pragma unroll
-  for (int rl = 0; rl < RPW; ++rl) {
-    V *X = wsm + rl * LD;
-#pragma unroll
-    for (int c = 0; c < NPC; ++c) {
-      const int kk = lane + 32 * c;
-      if (kk >= NPAIR) break;
-      if (kk == 0) {
-        const T a = X[0].x, b = X[pad8(M)].x;
-        X[0] = mk<V>(a + b, a - b);
-      } else {
-        const int km = M - kk;
-        const V a = X[pad8(kk)], b = X[pad8(km)];
-        const V wa = cconj(__ldg(twx + kk)), wb = cconj(__ldg(twx + km));
-        V ep = mk<V>(a.x + b.x, a.y - b.y);
-        V em = mk<V>(a.x - b.x, a.y + b.y);
-        V t1 = cmul(wa, em);
-        X[pad8(kk)] = mk<V>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
-        if (km != kk) {
-          V fp = mk<V>(b.x + a.x, b.y - a.y);
-          V fm = mk<V>(b.x - a.x, b.y + a.y);
-          V t2 = cmul(wb, fm);
-          X[pad8(km)] = mk<V>(fp.x - t2.y, fp.y + t2.x);
-        }
-      }
-    }
-  }
-  __syncwarp();
   fft_warp<V, M, LOGRPW, 1, LD, true>(wsm, lane, tw);
   const T *wsr = reinterpret_cast<const T *>(wsm);
 #pragma unroll
