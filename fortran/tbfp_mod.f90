@@ -89,6 +89,9 @@ module tbfp_mod
     integer(c_int) function tbfp_get_stats(h, stats) bind(C, name='tbfp_get_stats')
       import; type(c_ptr), value :: h; type(tbfp_stats), intent(out) :: stats
     end function
+    integer(c_int) function tbfp_set_wait_limit(h, cycles) bind(C, name='tbfp_set_wait_limit')
+      import; type(c_ptr), value :: h; integer(c_long_long), value :: cycles
+    end function
 
     ! --- solveFPS, computeSource, makeVelocityDivFree, continuity error --------
     integer(c_int) function tbfp_solve_fps(h, s, psi) bind(C, name='tbfp_solve_fps')

@@ -56,7 +56,7 @@ extern "C" {
 #define TBFP_ENONFINITE (-7) /* a NaN or Inf reached a residual, the pressure or max|div u|: a
                                 non-finite input, or a breakdown (the reference aborts) */
 #define TBFP_ESINGULAR (-8)  /* MG_MODE: the coarsest-level system is singular (beta not positive) */
-#define TBFP_ETIMEOUT (-9)   /* a bounded device-side wait ran out (persistent ensemble kernel) */
+#define TBFP_ETIMEOUT (-9)   /* a bounded device-side wait ran out (persistent ensemble kernel, staged correction) */
 
 /* precision modes */
 #define TBFP_FP64 0  /* plain FP64: the drop-in for solveFPS */
@@ -431,6 +431,13 @@ int tbfp_ensemble_set_mode(tbfp_ensemble *e, int mode, int param);
 /* The form in use (0 before the first call) and its param; tuned_ms (NULL or 3 entries): the
    measured ms of the graph and of the persistent form at 1 and 2 blocks per SM (-1: not measured). */
 int tbfp_ensemble_get_mode(const tbfp_ensemble *e, int *mode, int *param, float *tuned_ms);
+/* Bound on each wait of the velocity correction for the bulk copies that stage its inputs in
+   shared memory (the FP64 out-of-place correction of tbfp_projection[_dev] and of each ensemble
+   member), in SM clock cycles; default 4e9 (about 2 s), 0: a copy not complete at the first look
+   counts as late.  A wait that runs out ends the kernel after its copies in flight have landed:
+   the call returns TBFP_ETIMEOUT and the handle stays usable.  No counterpart in the reference
+   (its loops run on the host and cannot wait on a copy engine). */
+int tbfp_set_wait_limit(tbfp_handle *h, long long cycles);
 /* Bound on each dependency wait of the persistent kernel, in polls of about 0.1 us (default 1e7,
    about a second).  A wait that runs out stops the launch: the call returns TBFP_ETIMEOUT. */
 int tbfp_ensemble_set_wait_limit(tbfp_ensemble *e, long long polls);

@@ -118,6 +118,7 @@ PROTOTYPES = {
     "tbfp_ensemble_set_mode": (C.c_int, [_H, C.c_int, C.c_int]),
     "tbfp_ensemble_get_mode": (C.c_int, [_H, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "tbfp_ensemble_set_wait_limit": (C.c_int, [_H, C.c_longlong]),
+    "tbfp_set_wait_limit": (C.c_int, [_H, C.c_longlong]),
     "tbfp_ensemble_projection_dev": (C.c_int, [_H, C.POINTER(TbfpMemberIO), C.c_double, C.c_double, C.c_double,
                                                C.POINTER(TbfpStats)]),
     "tbfp_pcg_setup": (C.c_int, [_H, C.POINTER(TbfpMgParams)]),

@@ -46,6 +46,7 @@ struct tbfp_handle {
   int nx = 0, ny = 0, nz = 0, nkx = 0;
   long R = 0;
   int hd_psi = 1, hd_u = 2, hd_rho = 1, hd_st = 1;
+  long long wait_cycles = kDefaultWaitCycles;  // bound on each copy wait of the staged correction
   Lay Lpsi{}, Lux{}, Luy{}, Luz{}, Lrho{}, Lst[3]{};
   size_t n_psi = 0, n_ux = 0, n_uy = 0, n_uz = 0, n_rho = 0, n_st[3]{};
   int device = 0;
@@ -288,6 +289,7 @@ CorrArgs corr_args(tbfp_handle *h, const double *uxi, const double *uyi, const d
   a.Lrho = h->Lrho;
   a.r = dt * alpha;  // momentumEqn.f90:1012
   a.invrho0 = 1.0 / rho0;
+  a.wait_cycles = h->wait_cycles;
   return a;
 }
 
@@ -628,6 +630,13 @@ int device_projection(tbfp_handle *h, const double *uxi, const double *uyi, cons
       out.iterations = c.iters;
       out.rel_residual = c.rel;
       solve_rc = c.status;
+    }
+    if (bits == kWaitTimeoutBits) {
+      h->last = out;
+      if (stats) *stats = out;
+      return set_err(h, TBFP_ETIMEOUT,
+                     "tbfp_projection: a staged copy of the velocity correction did not complete within the wait "
+                     "limit (tbfp_set_wait_limit)");
     }
     if (!std::isfinite(md) || solve_rc == TBFP_ENONFINITE) {
       h->last = out;
@@ -2290,6 +2299,13 @@ int tbfp_ensemble_get_mode(const tbfp_ensemble *e, int *mode, int *param, float 
   if (param) *param = e->use_param;
   if (tuned_ms)
     for (int c = 0; c < 3; ++c) tuned_ms[c] = e->tuned_ms[c];
+  return TBFP_OK;
+}
+
+int tbfp_set_wait_limit(tbfp_handle *h, long long cycles) {
+  if (!h) return TBFP_ENULL;
+  if (cycles < 0) return set_err(h, TBFP_EINVAL, "tbfp_set_wait_limit: negative limit");
+  h->wait_cycles = cycles;
   return TBFP_OK;
 }
 

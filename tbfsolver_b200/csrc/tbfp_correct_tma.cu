@@ -18,9 +18,10 @@
 //
 // Every face is computed with the arguments and in the operation order of
 // correct_div_body (the kernel form, which serves surface tension and arrays
-// that a tensor map cannot describe).  A wait on a copy is bounded: past the
-// limit the CTA waits (bounded again) for its copies in flight, folds NaN into
-// *maxdiv, which the host reports as a non-finite divergence, and returns.
+// that a tensor map cannot describe).  A wait on a copy is bounded
+// (CorrArgs::wait_cycles): past the limit the CTA waits (with the default
+// bound) for its copies in flight, folds kWaitTimeoutBits into *maxdiv, which
+// the host reports as TBFP_ETIMEOUT, and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -33,7 +34,6 @@ namespace {
 
 constexpr int kCTX = 128;  // tile width; a CTA's threads are 128 columns x NT/128 row groups
 constexpr int kPer = 9;                               // periodic inputs per row
-constexpr long long kTmaWaitCycles = 4000000000LL;    // about 2 s of SM clock
 constexpr int kCorrTmaMaxSmem = 220 * 1024;  // under the opt-in limit with the static reduction buffer
 
 __host__ __device__ constexpr int align128(int b) { return (b + 127) & ~127; }
@@ -55,10 +55,23 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-__device__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_test_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// A first look that does not block, then waits (try_wait suspends the thread
+// for a while inside the instruction) until the bound in SM cycles runs out.
+__device__ bool mbar_wait_bounded(unsigned bar, unsigned parity, long long limit) {
+  if (mbar_test_wait(bar, parity)) return true;
+  if (limit <= 0) return false;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity))
-    if (clock64() - t0 > kTmaWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   return true;
 }
 __device__ __forceinline__ void tma_load2(unsigned dst, const CUtensorMap *map, int x, int y, unsigned bar) {
@@ -202,13 +215,15 @@ __global__ void __launch_bounds__(NT, 1)
     }
   }
   auto drain_and_fail = [&]() {
+    // the copies in flight land before the CTA leaves (waits of the default bound)
     if (tid == 0)
       for (int t = waited; t <= issued; ++t)
-        mbar_wait_bounded(smem_u32(bars + (t + 1) % NS), (unsigned)(((t + 1) / NS) & 1));
+        mbar_wait_bounded(smem_u32(bars + (t + 1) % NS), (unsigned)(((t + 1) / NS) & 1), kDefaultWaitCycles);
     cp_async_wait_all();
     __syncthreads();
-    if (tid == 0) atomicMax(maxdiv, 0x7ff8000000000000ull);  // NaN: a copy did not complete in time
+    if (tid == 0) atomicMax(maxdiv, kWaitTimeoutBits);  // a copy did not complete within the bound
   };
+  const long long lim = a.wait_cycles;
 
   const double R = a.r, ir0 = a.invrho0, idxc = g.idxc1, idzc = g.idzc1;
   const int i = i0 + tx;
@@ -220,9 +235,9 @@ __global__ void __launch_bounds__(NT, 1)
   // k0 (slot 1); plane k0+1 (slot 2) is waited for as well
   double uzq[RPT];
   {
-    bool bad = !mbar_wait_bounded(smem_u32(bars + 0), 0u);
-    bad = !mbar_wait_bounded(smem_u32(bars + 1), 0u) || bad;
-    bad = !mbar_wait_bounded(smem_u32(bars + 2 % NS), (unsigned)((2 / NS) & 1)) || bad;
+    bool bad = !mbar_wait_bounded(smem_u32(bars + 0), 0u, lim);
+    bad = !mbar_wait_bounded(smem_u32(bars + 1), 0u, lim) || bad;
+    bad = !mbar_wait_bounded(smem_u32(bars + 2 % NS), (unsigned)((2 / NS) & 1), lim) || bad;
     cp_async_wait_group<NS - 2>();  // the periodic columns of stages -1 and 0
     if (__syncthreads_or(bad)) {
       drain_and_fail();
@@ -314,7 +329,7 @@ __global__ void __launch_bounds__(NT, 1)
     if (n == nlast) break;
     {
       const int t = n + 2;  // plane k+2 (t <= tmax since n < nlast)
-      const bool bad = !mbar_wait_bounded(smem_u32(bars + (t + 1) % NS), (unsigned)(((t + 1) / NS) & 1));
+      const bool bad = !mbar_wait_bounded(smem_u32(bars + (t + 1) % NS), (unsigned)(((t + 1) / NS) & 1), lim);
       cp_async_wait_group<NS - 2>();  // the periodic column of plane k+1
       if (__syncthreads_or(bad)) {
         drain_and_fail();

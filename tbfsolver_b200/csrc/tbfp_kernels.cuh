@@ -57,7 +57,12 @@ struct CorrArgs {
   Lay Lux, Luy, Luz, Lpsi, Lrho, Lst[3];
   double r;  // dt*alpha
   double invrho0;
+  long long wait_cycles;  // bound on each wait of the TMA-staged correction for its copies (SM cycles)
 };
+// The max|div u| word of a correction whose copy wait ran out: a NaN with its
+// own payload, above the canonical NaN, so the host tells it from NaN data.
+constexpr unsigned long long kWaitTimeoutBits = 0x7ff8dead00000001ull;
+constexpr long long kDefaultWaitCycles = 4000000000LL;  // about 2 s of SM clock
 
 // Source rows of the forward x transform.
 //   residual = false: s; with acc != nullptr also acc[0] += sum s*dyf(j) and

@@ -148,6 +148,12 @@ class FastPoissonSolver:
         check(self.lib.tbfp_get_stats(self.h, C.byref(st)), self.h)
         return st
 
+    def set_wait_limit(self, cycles: int) -> None:
+        """Bound, in SM clock cycles, on each wait of the velocity correction for the copies
+        that stage its inputs (tbfp_set_wait_limit; default 4e9, about 2 s).  A wait that runs
+        out makes the projection raise TbfpError with TBFP_ETIMEOUT; the handle stays usable."""
+        check(self.lib.tbfp_set_wait_limit(self.h, int(cycles)), self.h)
+
     # --- solveFPS ----------------------------------------------------------
     def solve_fps(self, p: Field, s: Field) -> int:
         """solveFPS (fastPoissonSolver.f90:337-384): p <- L^{-1} s with zero volume-weighted

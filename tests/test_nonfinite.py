@@ -102,3 +102,38 @@ def test_pcg_reports_a_nan_source():
         psi.a.zero_()
         st = pcg.solve_pcg(psi, bd, qd)
         assert st.rel_residual <= 1e-10
+
+
+def test_correction_copy_wait_limit_reports_a_timeout():
+    """The staged correction bounds each wait for the bulk copies of its input
+    planes.  With the bound at zero cycles a copy that has not landed at the
+    first look counts as late: the kernel lets its copies in flight land, ends,
+    and the call returns TBFP_ETIMEOUT (not a divergence error).  With the
+    default bound restored the same handle gives the same answer as before."""
+    from tbfsolver_b200._native import TBFP_ETIMEOUT
+
+    spec, inp = _inputs()
+    g = inp.grid
+    eqn = PoissonEqn(g, spec.rhol, spec.rhog)
+
+    def run():
+        psi = Field.like(inp.psi_n, torch.zeros_like(inp.psi_n.a))
+        uo = VField(*[Field.like(f, torch.zeros_like(f.a)) for f in inp.u.components()])
+        st = eqn.projection(psi, inp.psi_n, inp.psi_nm1, inp.rho, inp.u, inp.dt, inp.alpha, u_out=uo)
+        return [psi.a.clone()] + [f.a.clone() for f in uo.components()], st.max_div
+
+    try:
+        want, md = run()
+        eqn.solver.set_wait_limit(0)
+        with pytest.raises(TbfpError) as ei:
+            run()
+        assert ei.value.code == TBFP_ETIMEOUT
+        eqn.solver.set_wait_limit(4_000_000_000)
+        got, md2 = run()
+        assert md2 == md
+        for a, b in zip(want, got):
+            assert torch.equal(a, b)
+        with pytest.raises(TbfpError):
+            eqn.solver.set_wait_limit(-1)
+    finally:
+        eqn.close()
