@@ -565,39 +565,43 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_inv(const V *_
   for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = tpx[t];
   const int r0 = blockIdx.x << LOGTJ;
   const int nrows = min(TJ, (int)g.R - r0);
-  // Z[k] = (X_k + conj X_{M-k}) + i conj(W^k) (X_k - conj X_{M-k}),  k = 0..M-1,
-  // applied as the spectrum comes in: a thread loads the pair X_k, X_{M-k} of one
-  // row (eight rows of one k are 128 contiguous bytes) and writes both Z values
-  constexpr int NPAIR = M / 2 + 1, NLD = NPAIR << LOGTJ;
+  // Z[n] = (X_n + conj X_{M-n}) + i conj(W^n) (X_n - conj X_{M-n}),  n = 0..M-1,
+  // made as the spectrum comes in and fed straight into the first radix-R0
+  // pass: thread (b, row) loads X_n and X_{M-n} for its butterfly's inputs
+  // n = b + r M/R0 (eight rows of one n are 128 contiguous bytes), transforms
+  // them in registers and writes the pass's outputs
+  constexpr int R0 = ct_rad(M, 0), PER = M / R0, NB0 = PER << LOGTJ;
 #pragma unroll
-  for (int t = threadIdx.x; t < NLD; t += kNT) {
-    const int kk = t >> LOGTJ, row = t & (TJ - 1), km = M - kk;
-    V *X = sm + row * LD;
-    V a = mk<V>(T(0), T(0)), b = a;
-    if (row < nrows) {
-      a = spec[(long)kk * g.R + r0 + row];
-      b = spec[(long)km * g.R + r0 + row];
-    }
-    if (kk == 0) {
-      X[0] = mk<V>(a.x + b.x, a.x - b.x);  // the imaginary parts of X_0 and X_M are ignored
-    } else {
-      const V wa = cconj(twx[kk]), wb = cconj(twx[km]);
-      V ep = mk<V>(a.x + b.x, a.y - b.y);
-      V em = mk<V>(a.x - b.x, a.y + b.y);
-      V t1 = cmul(wa, em);
-      X[pad8(kk)] = mk<V>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
-      if (km != kk) {
-        V fp = mk<V>(b.x + a.x, b.y - a.y);
-        V fm = mk<V>(b.x - a.x, b.y + a.y);
-        V t2 = cmul(wb, fm);
-        X[pad8(km)] = mk<V>(fp.x - t2.y, fp.y + t2.x);
+  for (int t = threadIdx.x; t < NB0; t += kNT) {
+    const int jb = t >> LOGTJ, row = t & (TJ - 1);
+    V v[R0];
+#pragma unroll
+    for (int r = 0; r < R0; ++r) {
+      const int n = jb + r * PER, m = M - n;
+      V xa = mk<V>(T(0), T(0)), xb = xa;
+      if (row < nrows) {
+        xa = spec[(long)n * g.R + r0 + row];
+        xb = spec[(long)m * g.R + r0 + row];
+      }
+      if (n == 0) {
+        v[r] = mk<V>(xa.x + xb.x, xa.x - xb.x);  // the imaginary parts of X_0 and X_M are ignored
+      } else {
+        const V wa = cconj(twx[n]);
+        V ep = mk<V>(xa.x + xb.x, xa.y - xb.y);
+        V em = mk<V>(xa.x - xb.x, xa.y + xb.y);
+        V t1 = cmul(wa, em);
+        v[r] = mk<V>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
       }
     }
+    bfly<V, R0, true>(v);
+    V *X = sm + row * LD;
+#pragma unroll
+    for (int r = 0; r < R0; ++r) X[pad8(jb * R0 + r)] = v[r];
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   V *wsm = sm + warp * RPW * LD;
-  fft_warp<V, M, LOGRPW, 1, LD, true>(wsm, lane, tw);
+  fft_warp<V, M, LOGRPW, 1, LD, true, 1>(wsm, lane, tw);  // passes 1, 2, ...
   const T *wsr = reinterpret_cast<const T *>(wsm);
 #pragma unroll
   for (int rl = 0; rl < RPW; ++rl) {
