@@ -132,13 +132,13 @@ template <typename V, int R, bool INV> __device__ __forceinline__ void bfly(V *v
 // the reads of the late ones) free of bank conflicts for 16-byte elements.
 __host__ __device__ __forceinline__ constexpr int pad8(int e) { return e + (e >> 3); }
 
-// Pass P of a length-N transform of NB = 2^LOGNB sequences by one warp.
+// Passes P .. PEND-1 of a length-N transform of NB = 2^LOGNB sequences by one warp.
 // Butterfly b reads x[b + r*N/R], applies twiddle exp(-+2*pi*i*(b mod Ns)*r/(Ns*R)),
 // transforms, and writes y[(b/Ns)*Ns*R + b mod Ns + r*Ns].  Butterflies are
 // numbered sequence-fastest (b = jj*NB + sequence).
-template <typename V, int N, int LOGNB, int ES, int BS, bool INV, int P = 0>
+template <typename V, int N, int LOGNB, int ES, int BS, bool INV, int P = 0, int PEND = ct_nrad(N)>
 __device__ __forceinline__ void fft_warp(V *buf, int lane, const V *__restrict__ tw) {
-  if constexpr (P < ct_nrad(N)) {
+  if constexpr (P < PEND) {
     constexpr int R = ct_rad(N, P), NS = ct_ns(N, P), LNS = ct_log2(NS), PER = N / R;
     constexpr int NB = 1 << LOGNB, TOT = PER * NB, Q = (TOT + 31) / 32;
     constexpr int TWO = NS - ct_rad(N, 0);  // this pass's offset in the twiddle table
@@ -178,7 +178,7 @@ __device__ __forceinline__ void fft_warp(V *buf, int lane, const V *__restrict__
       }
     }
     __syncwarp();
-    fft_warp<V, N, LOGNB, ES, BS, INV, P + 1>(buf, lane, tw);
+    fft_warp<V, N, LOGNB, ES, BS, INV, P + 1, PEND>(buf, lane, tw);
   }
 }
 

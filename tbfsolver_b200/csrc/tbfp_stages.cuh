@@ -51,6 +51,73 @@ __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_syn
 // ---------------------------------------------------------------------------
 // Forward x transform (see k_fftx_fwd in tbfp_xfft.cu)
 // ---------------------------------------------------------------------------
+// The last Stockham pass of the forward half-length transforms of a tile of
+// TJ = 2^LOGTJ rows (the earlier passes done, rows at sm + row*LD in the pad8
+// layout), fused with the r2c pair step
+//   X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx)
+// and the store of S[kx][r0 + row].  Output k = b + r*NS of last-pass butterfly
+// b pairs with output M-k of butterfly NS-b, so thread (b, row) runs both
+// butterflies in registers and stores both halves of every pair: the last
+// pass's shared-memory writes and the pair step's reads are gone.
+template <typename V, int M, int LOGTJ>
+__device__ __forceinline__ void fwd_last_pass_r2c_store(const V *sm, const V *tw, const V *__restrict__ twx,
+                                                        V *__restrict__ spec, long R, int r0, int nrows) {
+  using T = decltype(V::x);
+  constexpr int TJ = 1 << LOGTJ, LD = x_row_stride(M);
+  constexpr int PL = ct_nrad(M) - 1, RL = ct_rad(M, PL), NS = ct_ns(M, PL), TWO = NS - ct_rad(M, 0);
+  constexpr int NITEM = NS == 1 ? 1 : NS / 2 + 1;  // butterflies b = 0 .. NS/2
+  const T half = T(0.5);
+  auto pair = [&](V zk, V zm, int k, int row) {  // X_k and X_{M-k} from Z_k, Z_{M-k}
+    V *o = spec + r0 + row;
+    const int m = M - k;
+    const V wa = twx[k], wb = twx[m];
+    V ep = mk<V>(zk.x + zm.x, zk.y - zm.y);  // Z_k + conj Z_{M-k}
+    V em = mk<V>(zk.x - zm.x, zk.y + zm.y);  // Z_k - conj Z_{M-k}
+    V t1 = cmul(wa, em);                      // W^k * em
+    o[(long)k * R] = mk<V>(half * (ep.x + t1.y), half * (ep.y - t1.x));  // (ep - i t1)/2
+    if (m != k) {
+      V fp = mk<V>(zm.x + zk.x, zm.y - zk.y);
+      V fm = mk<V>(zm.x - zk.x, zm.y + zk.y);
+      V t2 = cmul(wb, fm);
+      o[(long)m * R] = mk<V>(half * (fp.x + t2.y), half * (fp.y - t2.x));
+    }
+  };
+  auto butterfly = [&](const V *X, int b, V *v) {  // last-pass butterfly b of one row
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      V x = X[pad8(b + r * NS)];
+      if constexpr (NS > 1) {
+        if (r > 0) x = cmul(x, tw[TWO + b * (RL - 1) + (r - 1)]);
+      }
+      v[r] = x;
+    }
+    bfly<V, RL, false>(v);
+  };
+#pragma unroll
+  for (int t = threadIdx.x; t < (NITEM << LOGTJ); t += kNT) {
+    const int b = t >> LOGTJ, row = t & (TJ - 1);
+    if (row >= nrows) continue;
+    const V *X = sm + row * LD;
+    V u[RL];
+    butterfly(X, b, u);
+    if (b == 0) {  // outputs r*NS: Z_0 with Z_M (the Nyquist term), r with RL - r
+      V *o = spec + r0 + row;
+      o[0] = mk<V>(u[0].x + u[0].y, T(0));
+      o[(long)M * R] = mk<V>(u[0].x - u[0].y, T(0));
+#pragma unroll
+      for (int r = 1; r <= RL / 2; ++r) pair(u[r], u[RL - r], r * NS, row);
+    } else if (2 * b == NS) {  // outputs NS/2 + r*NS: r with RL - 1 - r
+#pragma unroll
+      for (int r = 0; 2 * r <= RL - 1; ++r) pair(u[r], u[RL - 1 - r], b + r * NS, row);
+    } else {  // with butterfly NS - b: r with RL - 1 - r
+      V w[RL];
+      butterfly(X, NS - b, w);
+#pragma unroll
+      for (int r = 0; r < RL; ++r) pair(u[r], w[RL - 1 - r], b + r * NS, row);
+    }
+  }
+}
+
 template <typename V, int M, int MODE, bool COH = false>
 __device__ __forceinline__ void fftx_fwd_body(XSrc src, GridK g, const V *__restrict__ twx,
                                               const V *__restrict__ tpx, V *__restrict__ spec, int bx,
@@ -150,39 +217,9 @@ __device__ __forceinline__ void fftx_fwd_body(XSrc src, GridK g, const V *__rest
       atomicMax(reinterpret_cast<unsigned long long *>(src.acc_r + 1), (unsigned long long)__double_as_longlong(m));
     }
   }
-  fft_warp<V, M, LOGRPW, 1, LD, false>(wsm, lane, tw);
-  __syncthreads();  // every row transformed
-
-  // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx),
-  // applied on the way out: a thread takes the pair Z_k, Z_{M-k} of one row and
-  // writes X_k and X_{M-k} to S
-  constexpr int NPAIR = M / 2 + 1, NST = NPAIR << LOGTJ;
-  const T half = T(0.5);
-#pragma unroll
-  for (int t = threadIdx.x; t < NST; t += kNT) {
-    const int kk = t >> LOGTJ, row = t & (TJ - 1), km = M - kk;
-    if (row >= nrows) continue;
-    const V *Z = sm + row * LD;
-    V *o = spec + r0 + row;
-    if (kk == 0) {
-      const V z0 = Z[0];
-      o[0] = mk<V>(z0.x + z0.y, T(0));
-      o[(long)M * g.R] = mk<V>(z0.x - z0.y, T(0));
-    } else {
-      const V a = Z[pad8(kk)], b = Z[pad8(km)];
-      const V wa = __ldg(twx + kk), wb = __ldg(twx + km);
-      V ep = mk<V>(a.x + b.x, a.y - b.y);  // Z_k + conj Z_{M-k}
-      V em = mk<V>(a.x - b.x, a.y + b.y);  // Z_k - conj Z_{M-k}
-      V t1 = cmul(wa, em);                  // W^k * em
-      o[(long)kk * g.R] = mk<V>(half * (ep.x + t1.y), half * (ep.y - t1.x));  // (ep - i t1)/2
-      if (km != kk) {
-        V fp = mk<V>(b.x + a.x, b.y - a.y);
-        V fm = mk<V>(b.x - a.x, b.y + a.y);
-        V t2 = cmul(wb, fm);
-        o[(long)km * g.R] = mk<V>(half * (fp.x + t2.y), half * (fp.y - t2.x));
-      }
-    }
-  }
+  fft_warp<V, M, LOGRPW, 1, LD, false, 0, ct_nrad(M) - 1>(wsm, lane, tw);  // all passes but the last
+  __syncthreads();
+  fwd_last_pass_r2c_store<V, M, LOGTJ>(sm, tw, twx, spec, g.R, r0, nrows);
 }
 
 // ---------------------------------------------------------------------------

@@ -157,39 +157,10 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_fwd(XSrc src, 
       atomicMax(reinterpret_cast<unsigned long long *>(src.acc_r + 1), (unsigned long long)__double_as_longlong(m));
     }
   }
-  fft_warp<V, M, LOGRPW, 1, LD, false>(wsm, lane, tw);
-  __syncthreads();  // every row transformed
-
-  // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx),
-  // applied on the way out: a thread takes the pair Z_k, Z_{M-k} of one row and
-  // writes X_k and X_{M-k} to S (eight rows of one k are 128 contiguous bytes)
-  constexpr int NPAIR = M / 2 + 1, NST = NPAIR << LOGTJ;
-  const T half = T(0.5);
-#pragma unroll
-  for (int t = threadIdx.x; t < NST; t += kNT) {
-    const int kk = t >> LOGTJ, row = t & (TJ - 1), km = M - kk;
-    if (row >= nrows) continue;
-    const V *Z = sm + row * LD;
-    V *o = spec + r0 + row;
-    if (kk == 0) {
-      const V z0 = Z[0];
-      o[0] = mk<V>(z0.x + z0.y, T(0));
-      o[(long)M * g.R] = mk<V>(z0.x - z0.y, T(0));
-    } else {
-      const V a = Z[pad8(kk)], b = Z[pad8(km)];
-      const V wa = twx[kk], wb = twx[km];
-      V ep = mk<V>(a.x + b.x, a.y - b.y);  // Z_k + conj Z_{M-k}
-      V em = mk<V>(a.x - b.x, a.y + b.y);  // Z_k - conj Z_{M-k}
-      V t1 = cmul(wa, em);                  // W^k * em
-      o[(long)kk * g.R] = mk<V>(half * (ep.x + t1.y), half * (ep.y - t1.x));  // (ep - i t1)/2
-      if (km != kk) {
-        V fp = mk<V>(b.x + a.x, b.y - a.y);
-        V fm = mk<V>(b.x - a.x, b.y + a.y);
-        V t2 = cmul(wb, fm);
-        o[(long)km * g.R] = mk<V>(half * (fp.x + t2.y), half * (fp.y - t2.x));
-      }
-    }
-  }
+  fft_warp<V, M, LOGRPW, 1, LD, false, 0, ct_nrad(M) - 1>(wsm, lane, tw);  // all passes but the last
+  __syncthreads();
+  // the last pass with the r2c pair step and the store of S[kx][r0 + row]
+  fwd_last_pass_r2c_store<V, M, LOGTJ>(sm, tw, twx, spec, g.R, r0, nrows);
 }
 
 template <typename V, int M, int MODE>
@@ -490,37 +461,10 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3))
   }
   __syncthreads();  // twiddle table and rows in place
   V *wsm = sm + warp * RPW * LD;  // this warp's rows
-  fft_warp<V, M, LOGRPW, 1, LD, false>(wsm, lane, tw);
-  __syncthreads();  // every row transformed
-
-  // X[k] = 1/2[(Z_k + conj Z_{M-k}) - i W^k (Z_k - conj Z_{M-k})], W = exp(-2 pi i/nx),
-  // applied on the way out (as in k_fftx_fwd)
-  constexpr int NPAIR = M / 2 + 1, NST = NPAIR << LOGTJ;
-#pragma unroll
-  for (int t = threadIdx.x; t < NST; t += kNT) {
-    const int kk = t >> LOGTJ, row = t & (TJ - 1), km = M - kk;
-    if (row >= nrows) continue;
-    const V *Z = sm + row * LD;
-    V *o = spec + r0 + row;
-    if (kk == 0) {
-      const V z0 = Z[0];
-      o[0] = make_double2(z0.x + z0.y, 0.0);
-      o[(long)M * g.R] = make_double2(z0.x - z0.y, 0.0);
-    } else {
-      const V za = Z[pad8(kk)], zb = Z[pad8(km)];
-      const V wa = twx[kk], wb = twx[km];
-      const V ep = make_double2(za.x + zb.x, za.y - zb.y);  // Z_k + conj Z_{M-k}
-      const V em = make_double2(za.x - zb.x, za.y + zb.y);  // Z_k - conj Z_{M-k}
-      const V t1 = cmul(wa, em);                             // W^k * em
-      o[(long)kk * g.R] = make_double2(0.5 * (ep.x + t1.y), 0.5 * (ep.y - t1.x));  // (ep - i t1)/2
-      if (km != kk) {
-        const V fp = make_double2(zb.x + za.x, zb.y - za.y);
-        const V fm = make_double2(zb.x - za.x, zb.y + za.y);
-        const V t2 = cmul(wb, fm);
-        o[(long)km * g.R] = make_double2(0.5 * (fp.x + t2.y), 0.5 * (fp.y - t2.x));
-      }
-    }
-  }
+  fft_warp<V, M, LOGRPW, 1, LD, false, 0, ct_nrad(M) - 1>(wsm, lane, tw);  // all passes but the last
+  __syncthreads();
+  // the last pass with the r2c pair step and the store of S[kx][r0 + row]
+  fwd_last_pass_r2c_store<V, M, LOGTJ>(sm, tw, twx, spec, g.R, r0, nrows);
 }
 
 template <int M>
