@@ -417,31 +417,72 @@ __device__ __forceinline__ void fftz_body(V *__restrict__ spec, GridK g, const V
   extern __shared__ __align__(16) unsigned char smz[];  // the launch's dynamic shared memory
   constexpr int LOGCPW = ct_lognb(NZ), LOGT = LOGCPW + 3, TJZ = 1 << LOGT;
   constexpr int ES = z_row_stride(NZ), ROWS = pad8(NZ - 1) + 1;
-  constexpr int NL = (NZ << LOGT) / kNT;  // elements per thread (NZ*TJZ is a multiple of kNT)
-  static_assert((NZ << LOGT) % kNT == 0, "z tile must split evenly over the CTA");
   V *sm = reinterpret_cast<V *>(smz);
   V *tw = sm + ES * ROWS;
-  for (int t = threadIdx.x; t < ct_twiddle_len(NZ); t += kNT) tw[t] = tpz[t];
   const int kx = by;
   const int j0 = bx << LOGT;
   const int nj = min(TJZ, g.ny - j0);
   const int ny = g.ny;
   V *base = spec + (long)kx * g.R + j0;
+  using T = decltype(V::x);
+  // The first pass reads its inputs from HBM and the last pass writes its
+  // outputs to HBM, so the tile goes through shared memory only between
+  // passes.  Thread (b, column): butterfly b of one column; eight columns of
+  // one k are 128 contiguous bytes.
+  constexpr int NP = ct_nrad(NZ), R0 = ct_rad(NZ, 0), PER0 = NZ / R0;
+  constexpr int RL = ct_rad(NZ, NP - 1), NSL = ct_ns(NZ, NP - 1), TWL = NSL - R0;
+  auto load_col = [&](int k, int jj) -> V {
+    return (jj < nj) ? ldw<COH>(base + ((long)k * ny + jj)) : mk<V>(T(0), T(0));
+  };
+  if constexpr (NP == 1) {  // one pass: HBM -> registers -> HBM
 #pragma unroll
-  for (int c = 0; c < NL; ++c) {
-    const int t = threadIdx.x + kNT * c;
-    const int k = t >> LOGT, jj = t & (TJZ - 1);
-    sm[pad8(k) * ES + jj] = (jj < nj) ? ldw<COH>(base + ((long)k * ny + jj)) : mk<V>(0, 0);
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  fft_warp<V, NZ, LOGCPW, ES, 1, INV>(sm + (warp << LOGCPW), lane, tw);
-  __syncthreads();
+    for (int t = threadIdx.x; t < TJZ; t += kNT) {
+      V v[R0];
 #pragma unroll
-  for (int c = 0; c < NL; ++c) {
-    const int t = threadIdx.x + kNT * c;
-    const int k = t >> LOGT, jj = t & (TJZ - 1);
-    if (jj < nj) base[(long)k * ny + jj] = sm[pad8(k) * ES + jj];
+      for (int r = 0; r < R0; ++r) v[r] = load_col(r, t);
+      bfly<V, R0, INV>(v);
+      if (t < nj) {
+#pragma unroll
+        for (int r = 0; r < R0; ++r) base[(long)r * ny + t] = v[r];
+      }
+    }
+    return;
+  } else {
+    for (int t = threadIdx.x; t < ct_twiddle_len(NZ); t += kNT) tw[t] = tpz[t];
+#pragma unroll
+    for (int t = threadIdx.x; t < (PER0 << LOGT); t += kNT) {
+      const int b = t >> LOGT, jj = t & (TJZ - 1);
+      V v[R0];
+#pragma unroll
+      for (int r = 0; r < R0; ++r) v[r] = load_col(b + r * PER0, jj);
+      bfly<V, R0, INV>(v);
+#pragma unroll
+      for (int r = 0; r < R0; ++r) sm[pad8(b * R0 + r) * ES + jj] = v[r];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    fft_warp<V, NZ, LOGCPW, ES, 1, INV, 1, NP - 1>(sm + (warp << LOGCPW), lane, tw);  // the middle passes
+    __syncthreads();
+#pragma unroll
+    for (int t = threadIdx.x; t < (NSL << LOGT); t += kNT) {
+      const int b = t >> LOGT, jj = t & (TJZ - 1);
+      V v[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        V x = sm[pad8(b + r * NSL) * ES + jj];
+        if (r > 0) {
+          V w = tw[TWL + b * (RL - 1) + (r - 1)];
+          if constexpr (INV) w.y = -w.y;
+          x = cmul(x, w);
+        }
+        v[r] = x;
+      }
+      bfly<V, RL, INV>(v);
+      if (jj < nj) {
+#pragma unroll
+        for (int r = 0; r < RL; ++r) base[(long)(b + r * NSL) * ny + jj] = v[r];
+      }
+    }
   }
 }
 
