@@ -305,6 +305,94 @@ __device__ __forceinline__ void rhs_body(RhsArgs a, GridK g, double *__restrict_
 // ---------------------------------------------------------------------------
 // Inverse x transform (see k_fftx_inv in tbfp_xfft.cu)
 // ---------------------------------------------------------------------------
+// The last Stockham pass of the inverse half-length transforms of a tile of
+// TJ = 2^LOGTJ rows (the earlier passes done, rows at sm + row*LD in the pad8
+// layout), fused with the store of the psi rows: complex output n of a row
+// holds psi at i = 2n+1 and 2n+2, scaled by 1/(nx*nz) (plus the old psi when
+// ACC), written with every ghost image of updateBoundaries (field.f90:950-974
+// on one rank): periodic x, the first y ghost layer copying the wall cell, and
+// periodic z unless the rows belong to a z slab.  Thread (b, row) runs
+// last-pass butterfly b of one row; 32 consecutive b write 512 contiguous
+// bytes.  For a one-pass length the tile is already transformed and is
+// stored as it stands.
+template <typename V, int M, int LOGTJ, bool ACC>
+__device__ __forceinline__ void inv_last_pass_store(const V *sm, const V *tw, double *__restrict__ psi, Lay Lp,
+                                                    int hd, const GridK &g, double scale, int r0, int nrows) {
+  using T = decltype(V::x);
+  constexpr int LD = x_row_stride(M), NX = 2 * M;
+  constexpr int NP = ct_nrad(M), RL = ct_rad(M, NP - 1), NSL = ct_ns(M, NP - 1), TWL = NSL - ct_rad(M, 0);
+  struct RowPtrs {
+    double *p00, *p10, *p01, *p11;
+  };
+  auto row_ptrs = [&](int row) {
+    const unsigned rr = (unsigned)(r0 + row);
+    const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
+    const int jg = (j == 1) ? 0 : (j == g.ny ? g.ny + 1 : -1);
+    const int kg = g.slab ? kNoGhost : ((k <= hd) ? k + g.nz : (k > g.nz - hd ? k - g.nz : kNoGhost));
+    RowPtrs q;
+    q.p00 = psi + at(Lp, 0, j, k);
+    q.p10 = (jg >= 0) ? psi + at(Lp, 0, jg, k) : nullptr;
+    q.p01 = (kg != kNoGhost) ? psi + at(Lp, 0, j, kg) : nullptr;
+    q.p11 = (q.p10 && q.p01) ? psi + at(Lp, 0, jg, kg) : nullptr;
+    return q;
+  };
+  auto put = [&](const RowPtrs &q, int i, double v) {
+    if constexpr (ACC) v += q.p00[i];  // refinement: psi += correction
+    const int ig = (i <= hd) ? i + NX : (i > NX - hd ? i - NX : kNoGhost);
+    q.p00[i] = v;
+    if (ig != kNoGhost) q.p00[ig] = v;
+    if (q.p10) {
+      q.p10[i] = v;
+      if (ig != kNoGhost) q.p10[ig] = v;
+    }
+    if (q.p01) {
+      q.p01[i] = v;
+      if (ig != kNoGhost) q.p01[ig] = v;
+    }
+    if (q.p11) {
+      q.p11[i] = v;
+      if (ig != kNoGhost) q.p11[ig] = v;
+    }
+  };
+  if constexpr (NP == 1) {
+    constexpr int LNX = ct_log2(NX);  // NX = 8 or 16
+#pragma unroll 1
+    for (int t = threadIdx.x; t < (NX << LOGTJ); t += kNT) {
+      const int ii = t & (NX - 1), row = t >> LNX;
+      if (row >= nrows) continue;
+      const T *src = reinterpret_cast<const T *>(sm + row * LD);
+      put(row_ptrs(row), ii + 1, (double)src[2 * pad8(ii >> 1) + (ii & 1)] * scale);
+    }
+  } else {
+    constexpr int LNSL = ct_log2(NSL);
+#pragma unroll 1
+    for (int t = threadIdx.x; t < (NSL << LOGTJ); t += kNT) {
+      const int b = t & (NSL - 1), row = t >> LNSL;
+      if (row >= nrows) continue;
+      const V *X = sm + row * LD;
+      V v[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        V x = X[pad8(b + r * NSL)];
+        if (r > 0) {
+          V w = tw[TWL + b * (RL - 1) + (r - 1)];
+          w.y = -w.y;
+          x = cmul(x, w);
+        }
+        v[r] = x;
+      }
+      bfly<V, RL, true>(v);
+      const RowPtrs q = row_ptrs(row);
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int n = b + r * NSL;
+        put(q, 2 * n + 1, (double)v[r].x * scale);
+        put(q, 2 * n + 2, (double)v[r].y * scale);
+      }
+    }
+  }
+}
+
 template <typename V, int M, bool ACC, bool COH = false>
 __device__ __forceinline__ void fftx_inv_body(const V *__restrict__ spec, double *__restrict__ psi, Lay Lp, int hd,
                                               GridK g, const V *__restrict__ twx, const V *__restrict__ tpx,
@@ -312,7 +400,7 @@ __device__ __forceinline__ void fftx_inv_body(const V *__restrict__ spec, double
   extern __shared__ __align__(16) unsigned char smx[];  // the launch's dynamic shared memory
   using T = decltype(V::x);
   constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
-  constexpr int LD = x_row_stride(M), NX = 2 * M, NXC = (NX + 31) / 32;
+  constexpr int LD = x_row_stride(M);
   V *sm = reinterpret_cast<V *>(smx);
   V *tw = sm + TJ * LD;
   for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = __ldg(tpx + t);
@@ -351,46 +439,9 @@ __device__ __forceinline__ void fftx_inv_body(const V *__restrict__ spec, double
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   V *wsm = sm + warp * RPW * LD;
-  fft_warp<V, M, LOGRPW, 1, LD, true, 1>(wsm, lane, tw);  // passes 1, 2, ...
-  const T *wsr = reinterpret_cast<const T *>(wsm);
-#pragma unroll
-  for (int rl = 0; rl < RPW; ++rl) {
-    const int row = warp * RPW + rl;
-    if (row >= nrows) break;
-    const unsigned rr = (unsigned)(r0 + row);
-    const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
-    // ghost images of the row: first y ghost layer (wall copy), periodic z
-    const int jg = (j == 1) ? 0 : (j == g.ny ? g.ny + 1 : -1);
-    const int kg = g.slab ? kNoGhost : ((k <= hd) ? k + g.nz : (k > g.nz - hd ? k - g.nz : kNoGhost));
-    double *p00 = psi + at(Lp, 0, j, k);
-    double *p10 = (jg >= 0) ? psi + at(Lp, 0, jg, k) : nullptr;
-    double *p01 = (kg != kNoGhost) ? psi + at(Lp, 0, j, kg) : nullptr;
-    double *p11 = (p10 && p01) ? psi + at(Lp, 0, jg, kg) : nullptr;
-    const T *src = wsr + rl * 2 * LD;
-#pragma unroll
-    for (int c = 0; c < NXC; ++c) {
-      const int ii = lane + 32 * c;
-      if (NX % 32 != 0 && ii >= NX) break;
-      const int i = ii + 1;
-      double v = (double)src[2 * pad8(ii >> 1) + (ii & 1)] * scale;
-      if constexpr (ACC) v += p00[i];  // refinement: psi += correction
-      const int ig = (i <= hd) ? i + NX : (i > NX - hd ? i - NX : kNoGhost);
-      p00[i] = v;
-      if (ig != kNoGhost) p00[ig] = v;
-      if (p10) {
-        p10[i] = v;
-        if (ig != kNoGhost) p10[ig] = v;
-      }
-      if (p01) {
-        p01[i] = v;
-        if (ig != kNoGhost) p01[ig] = v;
-      }
-      if (p11) {
-        p11[i] = v;
-        if (ig != kNoGhost) p11[ig] = v;
-      }
-    }
-  }
+  fft_warp<V, M, LOGRPW, 1, LD, true, 1, ct_nrad(M) - 1>(wsm, lane, tw);  // the middle passes
+  __syncthreads();
+  inv_last_pass_store<V, M, LOGTJ, ACC>(sm, tw, psi, Lp, hd, g, scale, r0, nrows);
 }
 
 // ---------------------------------------------------------------------------

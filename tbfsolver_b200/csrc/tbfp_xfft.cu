@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_inv(const V *_
                                                   const V *__restrict__ tpx, double scale) {
   using T = decltype(V::x);
   constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
-  constexpr int LD = x_row_stride(M), NX = 2 * M, NXC = (NX + 31) / 32;
+  constexpr int LD = x_row_stride(M);
   extern __shared__ __align__(16) unsigned char smx[];
   V *sm = reinterpret_cast<V *>(smx);
   V *tw = sm + TJ * LD;
@@ -545,46 +545,10 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_inv(const V *_
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   V *wsm = sm + warp * RPW * LD;
-  fft_warp<V, M, LOGRPW, 1, LD, true, 1>(wsm, lane, tw);  // passes 1, 2, ...
-  const T *wsr = reinterpret_cast<const T *>(wsm);
-#pragma unroll
-  for (int rl = 0; rl < RPW; ++rl) {
-    const int row = warp * RPW + rl;
-    if (row >= nrows) break;
-    const unsigned rr = (unsigned)(r0 + row);
-    const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
-    // ghost images of the row: first y ghost layer (wall copy), periodic z
-    const int jg = (j == 1) ? 0 : (j == g.ny ? g.ny + 1 : -1);
-    const int kg = g.slab ? kNoGhost : ((k <= hd) ? k + g.nz : (k > g.nz - hd ? k - g.nz : kNoGhost));
-    double *p00 = psi + at(Lp, 0, j, k);
-    double *p10 = (jg >= 0) ? psi + at(Lp, 0, jg, k) : nullptr;
-    double *p01 = (kg != kNoGhost) ? psi + at(Lp, 0, j, kg) : nullptr;
-    double *p11 = (p10 && p01) ? psi + at(Lp, 0, jg, kg) : nullptr;
-    const T *src = wsr + rl * 2 * LD;
-#pragma unroll
-    for (int c = 0; c < NXC; ++c) {
-      const int ii = lane + 32 * c;
-      if (NX % 32 != 0 && ii >= NX) break;
-      const int i = ii + 1;
-      double v = (double)src[2 * pad8(ii >> 1) + (ii & 1)] * scale;
-      if constexpr (ACC) v += p00[i];  // refinement: psi += correction
-      const int ig = (i <= hd) ? i + NX : (i > NX - hd ? i - NX : kNoGhost);
-      p00[i] = v;
-      if (ig != kNoGhost) p00[ig] = v;
-      if (p10) {
-        p10[i] = v;
-        if (ig != kNoGhost) p10[ig] = v;
-      }
-      if (p01) {
-        p01[i] = v;
-        if (ig != kNoGhost) p01[ig] = v;
-      }
-      if (p11) {
-        p11[i] = v;
-        if (ig != kNoGhost) p11[ig] = v;
-      }
-    }
-  }
+  fft_warp<V, M, LOGRPW, 1, LD, true, 1, ct_nrad(M) - 1>(wsm, lane, tw);  // the middle passes
+  __syncthreads();
+  // the last pass with the store of psi and its ghost images
+  inv_last_pass_store<V, M, LOGTJ, ACC>(sm, tw, psi, Lp, hd, g, scale, r0, nrows);
 }
 
 template <typename V, int M, bool ACC>
