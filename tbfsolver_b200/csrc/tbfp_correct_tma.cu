@@ -406,12 +406,15 @@ bool encode_rows(CUtensorMap *m, const double *base, const Lay &Ly, long nk) {
 }
 
 // planes per chunk: the chunk count that best fills whole waves of one CTA
-// per SM, counting the extra plane each chunk loads
+// per SM, counting the extra plane each chunk loads, with at least 8 planes a
+// chunk (small channels run several at once in an ensemble and need not fill
+// the GPU alone)
 int pick_chunk(int tiles, int nz, int sms) {
   int best = nz;
   double best_eff = -1.0;
   for (int c = 1; c <= 32 && c <= nz; ++c) {
     const int len = (nz + c - 1) / c, chunks = (nz + len - 1) / len;
+    if (len < 8 && len < nz) break;  // a chunk loads one plane more than it corrects
     const long ctas = (long)tiles * chunks, waves = (ctas + sms - 1) / sms;
     const double eff = (double)ctas / (double)(waves * sms) * (double)len / (double)(len + 1);
     if (eff > best_eff + 1e-9) {
