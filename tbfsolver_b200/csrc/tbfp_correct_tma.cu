@@ -265,6 +265,20 @@ __global__ void __launch_bounds__(NT, 1)
   // One barrier per plane: after plane k, wait for the copies of plane k+2
   // and the periodic column of plane k+1, then one barrier both publishes
   // them to every thread and frees the slot of plane k for plane k+NS.
+  // y metrics of the thread's rows, read once (a store to u may alias the
+  // tables as far as the compiler knows, so they would be reloaded per plane)
+  double m_idycp[RPT], m_idyf[RPT], m_idycm = 0.0;
+#pragma unroll
+  for (int qq = 0; qq < RPT; ++qq) {
+    const int j = j0 + RPT * tg + qq;
+    m_idycp[qq] = (j < g.ny) ? g.idyc[j] : 0.0;
+    m_idyf[qq] = (j <= g.ny) ? g.idyf[j - 1] : 0.0;
+  }
+  {
+    const int j = j0 + RPT * tg;
+    if (j > 1 && j <= g.ny) m_idycm = g.idyc[j - 1];
+  }
+
   double vmax = 0.0;
   for (int n = 0; n <= nlast; ++n) {
     const int k = k0 + n;
@@ -293,17 +307,19 @@ __global__ void __launch_bounds__(NT, 1)
       }
       // upper y face (the top wall face is copied), lower y face
       const double uyc = Uy[(r + 1) * q.uy.w + q.uy.dx + tx];
-      const double uyp = (j < g.ny) ? face_update(uyc, R, ir0, Sir[ri + q.ir.w], irc, g.idyc[j], Sps[rs + q.ps.w],
+      const double uyp = (j < g.ny) ? face_update(uyc, R, ir0, Sir[ri + q.ir.w], irc, m_idycp[qq], Sps[rs + q.ps.w],
                                                   psc, Spn[rs + q.ps.w], pnc, Spo[rs + q.ps.w], poc, 0.0)
                                     : uyc;
       if (qq == 0) {
         const double uyb = Uy[r * q.uy.w + q.uy.dx + tx];
-        if (j > 1) {
-          uym = face_update(uyb, R, ir0, irc, Sir[ri - q.ir.w], g.idyc[j - 1], psc, Sps[rs - q.ps.w], pnc,
-                            Spn[rs - q.ps.w], poc, Spo[rs - q.ps.w], 0.0);
-        } else {
+        if (j == 1) {
           uym = uyb;
           if (col) a.uyo[at(a.Luy, i, 0, k)] = uyb;  // the wall face below row 1
+        } else if (j <= g.ny) {
+          uym = face_update(uyb, R, ir0, irc, Sir[ri - q.ir.w], m_idycm, psc, Sps[rs - q.ps.w], pnc,
+                            Spn[rs - q.ps.w], poc, Spo[rs - q.ps.w], 0.0);
+        } else {
+          uym = 0.0;  // a row past ny: nothing is stored
         }
       }
       // upper z face; the lower one is the previous plane's upper face
@@ -320,7 +336,7 @@ __global__ void __launch_bounds__(NT, 1)
         a.uzo[oz] = uzp;
         if (k == g.nz && !g.slab) a.uzo[oz - (long)k * a.Luz.sk] = uzp;  // uz(i, j, 0)
         double dv = (uxp - uxm) * idx;
-        dv = dv + (uyp - uym) * g.idyf[j - 1];
+        dv = dv + (uyp - uym) * m_idyf[qq];
         dv = dv + (uzp - uzl) * idz;
         vmax = nanmax_nonneg(vmax, dv);
       }
