@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3))
     const int col0 = (int)threadIdx.x - grp * (NX <= kNT ? NX : 0);
     const int rl0 = grp * RG, rl1 = min(rl0 + RG, TJ);
     const int pjs = (int)a.Lpsi.sj, pks = (int)a.Lpsi.sk, rjs = (int)a.Lrho.sj, rks = (int)a.Lrho.sk;
-    const int yjs = (int)a.Luy.sj, zks = (int)a.Luz.sk;
+    const int xjs = (int)a.Lux.sj, yjs = (int)a.Luy.sj, zjs = (int)a.Luz.sj, zks = (int)a.Luz.sk;
     const double *__restrict__ ux = a.ux;
     const double *__restrict__ uy = a.uy;
     const double *__restrict__ uz = a.uz;
@@ -390,16 +390,18 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3))
       const int i = ii + 1;
       double *dst = smr + 2 * pad8(ii >> 1) + (ii & 1);
       double irc = 0.0, pc = 0.0, oc = 0.0, irm = 0.0, pm = 0.0, om = 0.0, uym = 0.0;
-      int jprev = -1;
+      // (j, k) and the element offsets of the march's first row; later rows step
+      // one row stride, a new z plane starts afresh
+      const unsigned rr0 = (unsigned)(r0 + rl0);
+      int k = (int)(rr0 / (unsigned)g.ny) + 1, j = (int)(rr0 - (unsigned)(k - 1) * g.ny) + 1;
+      int op = (int)at(a.Lpsi, i, j, k), oq = (int)at(a.Lrho, i, j, k);
+      int ox = (int)at(a.Lux, i, j, k), oy = (int)at(a.Luy, i, j, k), oz = (int)at(a.Luz, i, j, k);
+      bool fresh = true;
 #pragma unroll
       for (int rl = rl0; rl < rl1; ++rl) {
         double r = 0.0;
         if (rl < nrows) {
-          const unsigned rr = (unsigned)(r0 + rl);
-          const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
-          const int op = (int)at(a.Lpsi, i, j, k), oq = (int)at(a.Lrho, i, j, k);
-          const int ox = (int)at(a.Lux, i, j, k), oy = (int)at(a.Luy, i, j, k), oz = (int)at(a.Luz, i, j, k);
-          if (j != jprev + 1) {  // first row of the march or of a z plane
+          if (fresh) {  // first row of the march or of a z plane
             irc = __ldg(ir + oq);
             pc = __ldg(pn + op);
             oc = __ldg(po + op);
@@ -407,8 +409,8 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3))
             pm = __ldg(pn + (op - pjs));
             om = __ldg(po + (op - pjs));
             uym = __ldg(uy + (oy - yjs));
+            fresh = false;
           }
-          jprev = j;
           const double uxc = __ldg(ux + ox), uyc = __ldg(uy + oy), uzc = __ldg(uz + oz), uzm = __ldg(uz + (oz - zks));
           const double iryp = __ldg(ir + (oq + rjs)), irzp = __ldg(ir + (oq + rks)), irzm = __ldg(ir + (oq - rks));
           const double pyp = __ldg(pn + (op + pjs)), pzp = __ldg(pn + (op + pks)), pzm = __ldg(pn + (op - pks));
@@ -456,6 +458,22 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3))
           uym = uyc;
         }
         dst[rl * 2 * LD] = r;
+        if (++j > g.ny) {
+          j = 1;
+          ++k;
+          op = (int)at(a.Lpsi, i, j, k);
+          oq = (int)at(a.Lrho, i, j, k);
+          ox = (int)at(a.Lux, i, j, k);
+          oy = (int)at(a.Luy, i, j, k);
+          oz = (int)at(a.Luz, i, j, k);
+          fresh = true;
+        } else {
+          op += pjs;
+          oq += rjs;
+          ox += xjs;
+          oy += yjs;
+          oz += zjs;
+        }
       }
     }
   }
