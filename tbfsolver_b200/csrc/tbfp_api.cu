@@ -109,6 +109,8 @@ struct tbfp_handle {
   double *d_s = nullptr;  // split right-hand side, laid out like psi
   double *d_irho = nullptr;
   unsigned long long *d_maxdiv = nullptr;
+  unsigned *d_tri_ctl = nullptr;  // ticket and retire counts of the persistent y solve (zero between launches)
+  int sms = 0;                    // SMs of the handle's device
   // device copies used by the host-pointer entry points
   double *h_ux = nullptr, *h_uy = nullptr, *h_uz = nullptr;
   double *h_rho = nullptr, *h_pn = nullptr, *h_pnm1 = nullptr, *h_psi = nullptr, *h_s = nullptr;
@@ -296,7 +298,8 @@ CorrArgs corr_args(tbfp_handle *h, const double *uxi, const double *uyi, const d
 // solveFPS body on device data: spectrum already holds the forward x transform.
 void fps_spectral_solve(tbfp_handle *h) {
   launch_fftz(h->d_spec, h->g, h->d_tpz, false, h->stream);
-  launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, h->stream);
+  launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, h->d_tri_ctl,
+                 h->sms, h->stream);
   launch_fftz(h->d_spec, h->g, h->d_tpz, true, h->stream);
 }
 
@@ -573,7 +576,8 @@ int device_projection(tbfp_handle *h, const double *uxi, const double *uyi, cons
     mark(2);
     launch_fftz(h->d_spec, h->g, h->d_tpz, false, s);
     mark(3);
-    launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, s);
+    launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz,
+                   h->d_tri_ctl, h->sms, s);
     mark(4);
     launch_fftz(h->d_spec, h->g, h->d_tpz, true, s);
     mark(5);
@@ -932,8 +936,14 @@ int create_impl(const tbfp_desc *d, const SlabSpec *sl, tbfp_handle **out) {
     return fail(rc);
   if ((rc = dev_alloc(h, &h->d_spec, (size_t)h->nkx * h->R)) || (rc = dev_alloc(h, &h->d_irho, h->n_rho)) ||
       (rc = dev_alloc(h, &h->d_s, h->n_psi)) ||
-      (rc = dev_alloc(h, &h->d_maxdiv, 1)) || (rc = dev_alloc(h, &h->d_ctl, 1)))
+      (rc = dev_alloc(h, &h->d_maxdiv, 1)) || (rc = dev_alloc(h, &h->d_ctl, 1)) ||
+      (rc = dev_alloc(h, &h->d_tri_ctl, 2)))
     return fail(rc);
+  {
+    const cudaError_t e = cudaMemset(h->d_tri_ctl, 0, 2 * sizeof(unsigned));
+    if (e != cudaSuccess) return fail(cuda_err(h, e, "cudaMemset"));
+    if (cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess) h->sms = 0;
+  }
 
   GridK &g = h->g;
   g.nx = nx;
@@ -992,7 +1002,8 @@ int tbfp_slab_spectral(tbfp_handle *h, double *spec_x) {
   cudaSetDevice(h->device);
   double2 *sp = reinterpret_cast<double2 *>(spec_x);
   launch_fftz(sp, h->gs, h->d_tpz, false, h->stream);
-  launch_tridiag(sp, h->gs, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, h->stream);
+  launch_tridiag(sp, h->gs, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, h->d_tri_ctl, h->sms,
+                 h->stream);
   launch_fftz(sp, h->gs, h->d_tpz, true, h->stream);
   return finish(h, "tbfp_slab_spectral");
 }

@@ -288,6 +288,12 @@ void launch_fftz(double2 *spec, const GridK &g, const double2 *tpz, bool inverse
 void launch_fftz(float2 *spec, const GridK &g, const float2 *tpz, bool inverse, cudaStream_t st);
 void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st);
+// FP64 spectrum with a two-word control block (zero before the first launch;
+// every launch leaves it zero) and the device's SM count: the persistent
+// prefetching form for 9..12 rows per lane, k_tridiag_t otherwise
+void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
+                    const double *ap, const double *dyf, double mean_c, double nxnz, unsigned *ctl, int sms,
+                    cudaStream_t st);
 void launch_tridiag(float2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st);
 void launch_fftx_inv(const double2 *spec, double *psi, Lay Lp, int hd, const GridK &g, const double2 *twx,

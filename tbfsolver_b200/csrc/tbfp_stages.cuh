@@ -537,28 +537,13 @@ __device__ __forceinline__ void fftz_body(V *__restrict__ spec, GridK g, const V
   }
 }
 
+// Right-hand sides of the y systems (kx, kz) and (kx, nz - kz) into d0 / d1:
+// row e lives in lane e / T at slot (e mod T)*33 + lane, padding rows are zero.
+// FP64 rows go by cp.async (the caller waits for them); FP32 rows are widened
+// through registers.
 template <typename V, int T>
-__device__ __forceinline__ void tridiag_t_body(V *__restrict__ spec, GridK g, const double *__restrict__ lamx,
-                                               const double *__restrict__ lamz, const double *__restrict__ am,
-                                               const double *__restrict__ ap, const double *__restrict__ dyf,
-                                               double mean_c, double nxnz, unsigned q, int warp,
-                                               unsigned char * /*dynamic shared memory: named below*/) {
-  extern __shared__ __align__(16) unsigned char smraw[];  // the launch's dynamic shared memory
-  constexpr int W = 33 * T;
-  const int ny = g.ny, nz = g.nz;
-  const int lane = threadIdx.x & 31;
-  double2 *d0 = reinterpret_cast<double2 *>(smraw) + warp * 2 * W;
-  double2 *d1 = d0 + W;
-  const int nzh = nz / 2 + 1;
-  if (q >= (unsigned)(g.nkx * nzh)) return;  // whole warp leaves; no block-level barrier follows
-  const int kx = (int)(q / (unsigned)nzh), kz = (int)(q - (unsigned)kx * nzh);
-  const int kz2 = (kz == 0) ? 0 : nz - kz;
-  const bool two = kz2 != kz;
-  V *S0 = spec + (long)kx * g.R + (long)kz * ny;
-  V *S1 = spec + (long)kx * g.R + (long)kz2 * ny;
-  using VT = decltype(V::x);
-  auto st = [](double2 v) { return mk<V>((VT)v.x, (VT)v.y); };
-  // row e lives in lane e / T at slot (e mod T)*33 + lane; padding rows are zero
+__device__ __forceinline__ void tri_pair_fill(const V *S0, const V *S1, bool two, int ny, int lane, double2 *d0,
+                                              double2 *d1) {
 #pragma unroll
   for (int c = 0; c < T; ++c) {
     const int e = lane + 32 * c;
@@ -580,11 +565,57 @@ __device__ __forceinline__ void tridiag_t_body(V *__restrict__ spec, GridK g, co
       d1[sl] = mk<double2>(0.0, 0.0);
     }
   }
+}
+
+template <typename V, int T, bool SMC = false>
+__device__ __forceinline__ void tri_pair_solve(V *S0, V *S1, bool two, double lam, bool pin,
+                                               const double *__restrict__ am, const double *__restrict__ ap,
+                                               const double *__restrict__ dyf, double mean_c, double nxnz, int ny,
+                                               int lane, double2 *d0, double2 *d1, const double *cam = nullptr,
+                                               const double *cap = nullptr);
+
+template <typename V, int T>
+__device__ __forceinline__ void tridiag_t_body(V *__restrict__ spec, GridK g, const double *__restrict__ lamx,
+                                               const double *__restrict__ lamz, const double *__restrict__ am,
+                                               const double *__restrict__ ap, const double *__restrict__ dyf,
+                                               double mean_c, double nxnz, unsigned q, int warp,
+                                               unsigned char * /*dynamic shared memory: named below*/) {
+  extern __shared__ __align__(16) unsigned char smraw[];  // the launch's dynamic shared memory
+  constexpr int W = 33 * T;
+  const int ny = g.ny, nz = g.nz;
+  const int lane = threadIdx.x & 31;
+  double2 *d0 = reinterpret_cast<double2 *>(smraw) + warp * 2 * W;
+  double2 *d1 = d0 + W;
+  const int nzh = nz / 2 + 1;
+  if (q >= (unsigned)(g.nkx * nzh)) return;  // whole warp leaves; no block-level barrier follows
+  const int kx = (int)(q / (unsigned)nzh), kz = (int)(q - (unsigned)kx * nzh);
+  const int kz2 = (kz == 0) ? 0 : nz - kz;
+  const bool two = kz2 != kz;
+  V *S0 = spec + (long)kx * g.R + (long)kz * ny;
+  V *S1 = spec + (long)kx * g.R + (long)kz2 * ny;
+  tri_pair_fill<V, T>(S0, S1, two, ny, lane, d0, d1);
   const double lam = lamx[kx + g.kx0] + lamz[kz];
   const bool pin = (kx + g.kx0 == 0 && kz == 0);
-  const int s0 = lane * T;
   if constexpr (sizeof(V) == sizeof(double2)) cp_async_wait_all();
   __syncwarp();
+  tri_pair_solve<V, T>(S0, S1, two, lam, pin, am, ap, dyf, mean_c, nxnz, ny, lane, d0, d1);
+}
+
+// Solve of the pair whose right-hand sides tri_pair_fill put in d0 / d1 (every
+// lane's copies landed and a __syncwarp passed); the solutions go to S0 / S1.
+// The (0,0) system (pin) has no partner, so d1 serves it as scratch.  SMC: the
+// elimination reads the off-diagonals of the lane's rows from shared copies
+// cam / cap (row t of lane l at [t*33 + l], zero on padding rows) instead of
+// the global tables, whose lane-strided reads touch a cache line per lane.
+template <typename V, int T, bool SMC>
+__device__ __forceinline__ void tri_pair_solve(V *S0, V *S1, bool two, double lam, bool pin,
+                                               const double *__restrict__ am, const double *__restrict__ ap,
+                                               const double *__restrict__ dyf, double mean_c, double nxnz, int ny,
+                                               int lane, double2 *d0, double2 *d1, const double *cam,
+                                               const double *cap) {
+  using VT = decltype(V::x);
+  auto st = [](double2 v) { return mk<V>((VT)v.x, (VT)v.y); };
+  const int s0 = lane * T;
 
   if (pin) {  // single system: pinned serial Thomas (as k_tridiag), factors in d1
     double *cpin = reinterpret_cast<double *>(d1);
@@ -643,7 +674,14 @@ __device__ __forceinline__ void tridiag_t_body(V *__restrict__ spec, GridK g, co
 #pragma unroll
   for (int t = 0; t < T; ++t) {
     const bool real = s0 + t < ny;  // off-diagonals zero, diagonal one on padding rows
-    const double a = real ? am[s0 + t] : 0.0, c = real ? ap[s0 + t] : 0.0;
+    double a, c;
+    if constexpr (SMC) {
+      a = cam[t * 33 + lane];
+      c = cap[t * 33 + lane];
+    } else {
+      a = real ? am[s0 + t] : 0.0;
+      c = real ? ap[s0 + t] : 0.0;
+    }
     const double dg = real ? lam : 1.0;
     const int sl = t * 33 + lane;
     const double gi = rcp_nr((dg - a - c) - a * ct_p);

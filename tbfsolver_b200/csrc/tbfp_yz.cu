@@ -364,6 +364,113 @@ __global__ void __launch_bounds__(kWPB * 32, tri_min_blocks<T>()) k_tridiag_t(
   tridiag_t_body<V, T>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, blockIdx.x * kWPB + warp, warp, smraw);
 }
 
+// ---------------------------------------------------------------------------
+// The same solve (FP64 spectrum, 9 <= T <= 12) as a persistent grid whose
+// warps overlap the copies of their next pair with the solve of the current
+// one.  k_tridiag_t waits for each pair's 12 KB (T = 12) before its
+// latency-bound elimination starts, and its 168 registers hold it at 12 warps
+// per SM; here each warp owns two buffers of a pair and, while it solves the
+// pair in one, the cp.async copies of its next pair land in the other.  The
+// off-diagonals of every lane's rows are copied once per CTA into shared
+// memory (row t of lane l at [t*33 + l]): the elimination's reads of the
+// global tables are lane-strided (a cache line per lane) and sat on its
+// dependent chain.  Pairs are handed out by tickets: the first pair of warp w
+// is w, the next ones come from atomicAdd on ctl[0] (one ticket ahead, so its
+// latency hides behind the solve).  The warp that takes the (0,0) system and
+// its serial pinned sweep takes fewer of the others.  The last warp to retire
+// (ctl[1] counts them) returns both words to zero for the next launch on the
+// stream.  No warp waits on another: the grid needs no co-residency.
+// At T <= 8 the spectrum of the cases this library meets is small (it fits in
+// L2 at 256x256x128) and k_tridiag_t, at 16 warps per SM, is faster.
+// ---------------------------------------------------------------------------
+template <int T>
+__host__ __device__ constexpr int tri_pf_min_blocks() {
+  static_assert(T >= 9 && T <= 12, "the persistent y solve is built for 9..12 rows per lane");
+  return 2;
+}
+template <int T>
+__host__ __device__ constexpr size_t tri_pf_smem_bytes() {
+  return (size_t)kWPB * 4 * 33 * T * sizeof(double2) + 2 * 33 * T * sizeof(double);
+}
+
+template <int T>
+__global__ void __launch_bounds__(kWPB * 32, tri_pf_min_blocks<T>()) k_tridiag_pf(
+    double2 *__restrict__ spec, GridK g, const double *__restrict__ lamx, const double *__restrict__ lamz,
+    const double *__restrict__ am, const double *__restrict__ ap, const double *__restrict__ dyf, double mean_c,
+    double nxnz, unsigned *__restrict__ ctl) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int W = 33 * T;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *buf = reinterpret_cast<double2 *>(smraw) + warp * 4 * W;  // two buffers of (d0, d1)
+  double *cam = reinterpret_cast<double *>(reinterpret_cast<double2 *>(smraw) + kWPB * 4 * W);
+  double *cap = cam + W;
+  const int ny = g.ny, nz = g.nz, nzh = nz / 2 + 1;
+  // the off-diagonals of every lane's rows, once per CTA (zero on padding rows)
+  for (int i = threadIdx.x; i < W; i += kWPB * 32) {
+    const int t = i / 33, l = i - t * 33, r = l * T + t;
+    const bool real = l < 32 && r < ny;
+    cam[i] = real ? am[r] : 0.0;
+    cap[i] = real ? ap[r] : 0.0;
+  }
+  __syncthreads();
+  const unsigned ntask = (unsigned)(g.nkx * nzh);
+  const unsigned nw = gridDim.x * kWPB;
+  auto pair = [&](unsigned q, int &kx, int &kz, bool &two, double2 *&S0, double2 *&S1) {
+    kx = (int)(q / (unsigned)nzh);
+    kz = (int)(q - (unsigned)kx * nzh);
+    const int kz2 = (kz == 0) ? 0 : nz - kz;
+    two = kz2 != kz;
+    S0 = spec + (long)kx * g.R + (long)kz * ny;
+    S1 = spec + (long)kx * g.R + (long)kz2 * ny;
+  };
+  auto fill = [&](unsigned q, double2 *d) {
+    int kx, kz;
+    bool two;
+    double2 *S0, *S1;
+    pair(q, kx, kz, two, S0, S1);
+    tri_pair_fill<double2, T>(S0, S1, two, ny, lane, d, d + W);
+  };
+  unsigned q = blockIdx.x * kWPB + warp;
+  unsigned qn = ntask;
+  if (q < ntask) {
+    fill(q, buf);
+    cp_async_commit();
+    unsigned t = 0;
+    if (lane == 0) t = atomicAdd(ctl, 1u);
+    qn = __shfl_sync(0xffffffffu, t, 0) + nw;
+  }
+  for (int it = 0; q < ntask; ++it) {
+    double2 *cur = buf + (it & 1) * 2 * W, *nxt = buf + ((it + 1) & 1) * 2 * W;
+    const bool more = qn < ntask;
+    if (more) fill(qn, nxt);
+    cp_async_commit();  // one group per iteration (empty on the last)
+    unsigned t = 0;
+    if (more && lane == 0) t = atomicAdd(ctl, 1u);  // the pair after next; read after the solve
+    int kx, kz;
+    bool two;
+    double2 *S0, *S1;
+    pair(q, kx, kz, two, S0, S1);
+    const double lam = lamx[kx + g.kx0] + lamz[kz];
+    const bool pin = (kx + g.kx0 == 0 && kz == 0);
+    cp_async_wait_group<1>();  // this pair's copies have landed; the next pair's may be in flight
+    __syncwarp();
+    tri_pair_solve<double2, T, true>(S0, S1, two, lam, pin, am, ap, dyf, mean_c, nxnz, ny, lane, cur, cur + W, cam,
+                                     cap);
+    __syncwarp();  // every lane is done with cur before it is refilled
+    const unsigned b = __shfl_sync(0xffffffffu, t, 0);
+    q = qn;
+    qn = more ? b + nw : ntask;
+  }
+  cp_async_wait_all();
+  if (lane == 0) {
+    __threadfence();
+    if (atomicAdd(ctl + 1, 1u) == nw - 1) {  // every other warp has taken its last ticket
+      atomicExch(ctl, 0u);
+      atomicExch(ctl + 1, 0u);
+    }
+  }
+}
+
 // shared memory of a k_tridiag<V, TM> block: the two right-hand sides per warp,
 // plus the coefficient arrays when TM == 0
 static size_t tridiag_block_smem(int T, int TM) {
@@ -397,6 +504,34 @@ static void launch_tridiag_t(V *spec, const GridK &g, const double *lamx, const 
 }
 void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st) {
+  launch_tridiag_t(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, st);
+}
+
+template <int T>
+static void launch_tridiag_pf_n(double2 *spec, const GridK &g, const double *lamx, const double *lamz,
+                                const double *am, const double *ap, const double *dyf, double mean_c, double nxnz,
+                                unsigned *ctl, int sms, cudaStream_t st) {
+  const long npair = (long)g.nkx * (g.nz / 2 + 1);
+  long nblk = (npair + kWPB - 1) / kWPB;
+  const long resident = (long)sms * tri_pf_min_blocks<T>();
+  if (nblk > resident) nblk = resident;
+  k_tridiag_pf<T><<<(unsigned)nblk, kWPB * 32, tri_pf_smem_bytes<T>(), st>>>(spec, g, lamx, lamz, am, ap, dyf,
+                                                                           mean_c, nxnz, ctl);
+}
+
+void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
+                    const double *ap, const double *dyf, double mean_c, double nxnz, unsigned *ctl, int sms,
+                    cudaStream_t st) {
+  const int T = tri_rows_per_lane(g.ny);
+  if (ctl && sms > 0) {
+    switch (T) {
+#define TBFP_TRI_PF(TT) \
+  case TT: launch_tridiag_pf_n<TT>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl, sms, st); return;
+      TBFP_TRI_PF(9) TBFP_TRI_PF(10) TBFP_TRI_PF(11) TBFP_TRI_PF(12)
+#undef TBFP_TRI_PF
+      default: break;
+    }
+  }
   launch_tridiag_t(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, st);
 }
 void launch_tridiag(float2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
@@ -460,6 +595,9 @@ cudaError_t prepare_yz_kernels() {
   TBFP_TRI_T(8) TBFP_TRI_T(9) TBFP_TRI_T(10) TBFP_TRI_T(11) TBFP_TRI_T(12) TBFP_TRI_T(13) TBFP_TRI_T(14)
   TBFP_TRI_T(15) TBFP_TRI_T(16)
 #undef TBFP_TRI_T
+#define TBFP_TRI_PF(TT) set((const void *)k_tridiag_pf<TT>, tri_pf_smem_bytes<TT>());
+  TBFP_TRI_PF(9) TBFP_TRI_PF(10) TBFP_TRI_PF(11) TBFP_TRI_PF(12)
+#undef TBFP_TRI_PF
   return e;
 }
 

@@ -70,6 +70,11 @@ CONFIGS = {
                       radius=0.06, rhol=1.0, rhog=0.02),
     "c5": ChannelSpec("c5-256x256x128-tanh1.5", 256, 256, 128, y_stretched=True, gamma=1.5, nbubbles=60,
                       radius=0.15, rhol=1.0, rhog=0.01),
+    # half of c2's planes: the same x and y transforms and y-solve instance
+    # (384 rows) with a spectrum (202 MB) still larger than L2, for profiling
+    # captures that must stay small
+    "c6": ChannelSpec("c6-512x384x128-tanh1.5", 512, 384, 128, y_stretched=True, gamma=1.5, nbubbles=100,
+                      radius=0.1, rhol=1.0, rhog=0.02),
 }
 
 

@@ -179,6 +179,34 @@ def test_solve_fps_random_rhs(dims, stretched):
     assert rel_linf(got, want.a) < TOL_P
 
 
+@pytest.mark.parametrize("ny", [260, 300, 333, 384])
+def test_persistent_y_solve_against_the_oracle_and_across_calls(ny):
+    """ny in 257..384 puts 9..12 rows on each lane, which the persistent y
+    solve takes (its warps prefetch their next pair and take pairs by ticket).
+    256 x ny x 64 has 4257 pairs, several per warp.  Three solves on one handle
+    give the same bits (the ticket counters return to zero after each launch),
+    and the answer matches the oracle."""
+    nx, nz = 256, 64
+    g = Grid(nx, ny, nz, 2 * np.pi, 2.0, np.pi, True, 1.5)
+    m = mesh_of(g)
+    rng = np.random.default_rng(ny)
+    s = Field("cl", 1, nx, ny, nz)
+    s.interior()[...] = rng.standard_normal((nz, ny, nx))
+    s.interior()[...] -= np.sum(s.interior() * m.volume()) / m.s_Vg
+    want = O.FField("cl", 1, nx, ny, nz)
+    O.solve_fps(m, s.interior().copy(), want, tridiag="thomas")
+    sd = _cuda(s)
+    with FastPoissonSolver(g) as fps:
+        outs = []
+        for _ in range(3):
+            p = _cuda(Field("cl", 1, nx, ny, nz))
+            fps.solve_fps(p, sd)
+            outs.append(p.a.clone())
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
+    got = outs[0].cpu().numpy()
+    assert rel_linf(got, want.a) < TOL_P
+
+
 def test_solve_fps_two_layer_halo():
     """hd_psi = 2: the same interior as hd_psi = 1, with both x and z ghost
     layers periodic images and the first y ghost layer a copy of the wall cell

@@ -41,7 +41,7 @@ def _slab_solve(chans, s_loc, psi_loc):
     exchange_z_ghosts_local([p.a for p in psi_loc], [c.s for c in chans], chans[0].hd_psi)
 
 
-@pytest.mark.parametrize("P,dims", [(2, (64, 48, 32)), (3, (48, 40, 24)), (4, (32, 24, 16))])
+@pytest.mark.parametrize("P,dims", [(2, (64, 48, 32)), (3, (48, 40, 24)), (4, (32, 24, 16)), (2, (128, 300, 32))])
 def test_slab_solve_fps_is_the_whole_channel_solve(P, dims):
     nx, ny, nz = dims
     g = Grid(nx, ny, nz, 2 * np.pi, 2.0, np.pi, True, 1.5)
