@@ -569,6 +569,86 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_inv(const V *_
   inv_last_pass_store<V, M, LOGTJ, ACC>(sm, tw, psi, Lp, hd, g, scale, r0, nrows);
 }
 
+// The same transform (FP64, M <= 256) as a persistent grid of 3 CTAs per SM
+// that stages each tile's spectrum in shared memory by cp.async, one tile
+// ahead: the copies of tile t+1 (the (M+1) x TJ entries, 128 contiguous bytes
+// per kx) are issued as soon as the first pass of tile t has read its stage,
+// so they land while tile t's middle passes, last pass and psi stores run.
+// k_fftx_inv issues a tile's loads only when its CTA starts and then waits
+// for them.  Tiles go round-robin over the CTAs (every tile costs the same).
+template <int M>
+__host__ __device__ constexpr size_t fftx_inv_pf_smem_bytes() {
+  return fftx_smem_bytes(M, 16) + (size_t)(M + 1) * fftx_rows_per_cta(M) * 16;
+}
+
+template <int M>
+__global__ void __launch_bounds__(kNT, 3) k_fftx_inv_pf(const double2 *__restrict__ spec, double *__restrict__ psi,
+                                                       Lay Lp, int hd, GridK g, const double2 *__restrict__ twx,
+                                                       const double2 *__restrict__ tpx, double scale) {
+  using V = double2;
+  constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
+  constexpr int LD = x_row_stride(M);
+  static_assert(TJ == 8, "a stage row of one kx is 8 entries (128 bytes)");
+  extern __shared__ __align__(16) unsigned char smx[];
+  V *sm = reinterpret_cast<V *>(smx);
+  V *tw = sm + TJ * LD;
+  V *stg = tw + M;  // stage: entry (kx, row) at kx*TJ + row
+  for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = tpx[t];
+  const int ntile = (int)((g.R + TJ - 1) / TJ);
+  auto stage = [&](int tile) {
+    const int r0 = tile << LOGTJ, nrows = min(TJ, (int)g.R - r0);
+    for (int t = threadIdx.x; t < (M + 1) * TJ; t += kNT) {
+      const int kx = t >> LOGTJ, row = t & (TJ - 1);
+      if (row < nrows) cp_async16(stg + t, spec + (long)kx * g.R + r0 + row);
+    }
+    cp_async_commit();
+  };
+  int tile = blockIdx.x;
+  if (tile < ntile) stage(tile);
+  constexpr int R0 = ct_rad(M, 0), PER = M / R0, NB0 = PER << LOGTJ;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (; tile < ntile; tile += gridDim.x) {
+    const int r0 = tile << LOGTJ, nrows = min(TJ, (int)g.R - r0);
+    cp_async_wait_all();
+    __syncthreads();  // the stage holds this tile; the previous tile's stores have read sm
+    // first pass: Z[n] = (X_n + conj X_{M-n}) + i conj(W^n) (X_n - conj X_{M-n}), as in k_fftx_inv
+#pragma unroll
+    for (int t = threadIdx.x; t < NB0; t += kNT) {
+      const int jb = t >> LOGTJ, row = t & (TJ - 1);
+      V v[R0];
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int n = jb + r * PER, m = M - n;
+        V xa = mk<V>(0.0, 0.0), xb = xa;
+        if (row < nrows) {
+          xa = stg[(n << LOGTJ) + row];
+          xb = stg[(m << LOGTJ) + row];
+        }
+        if (n == 0) {
+          v[r] = mk<V>(xa.x + xb.x, xa.x - xb.x);  // the imaginary parts of X_0 and X_M are ignored
+        } else {
+          const V wa = cconj(twx[n]);
+          V ep = mk<V>(xa.x + xb.x, xa.y - xb.y);
+          V em = mk<V>(xa.x - xb.x, xa.y + xb.y);
+          V t1 = cmul(wa, em);
+          v[r] = mk<V>(ep.x - t1.y, ep.y + t1.x);  // ep + i t1
+        }
+      }
+      bfly<V, R0, true>(v);
+      V *X = sm + row * LD;
+#pragma unroll
+      for (int r = 0; r < R0; ++r) X[pad8(jb * R0 + r)] = v[r];
+    }
+    __syncthreads();  // the stage is free and the first pass is in sm
+    if (tile + (int)gridDim.x < ntile) stage(tile + gridDim.x);
+    V *wsm = sm + warp * RPW * LD;
+    fft_warp<V, M, LOGRPW, 1, LD, true, 1, ct_nrad(M) - 1>(wsm, lane, tw);  // the middle passes
+    __syncthreads();
+    inv_last_pass_store<V, M, LOGTJ, false>(sm, tw, psi, Lp, hd, g, scale, r0, nrows);
+  }
+  cp_async_wait_all();
+}
+
 template <typename V, int M, bool ACC>
 static void launch_fftx_inv_n(const V *spec, double *psi, Lay Lp, int hd, const GridK &g, const V *twx, const V *tpx,
                               double scale, cudaStream_t st) {
@@ -590,8 +670,23 @@ static void launch_fftx_inv_t(const V *spec, double *psi, Lay Lp, int hd, const 
   }
 }
 
+template <int M>
+static void launch_fftx_inv_pf(const double2 *spec, double *psi, Lay Lp, int hd, const GridK &g, const double2 *twx,
+                               const double2 *tpx, double scale, int sms, cudaStream_t st) {
+  constexpr int TJ = fftx_rows_per_cta(M);
+  long nblk = (g.R + TJ - 1) / TJ;
+  if (nblk > 3L * sms) nblk = 3L * sms;
+  k_fftx_inv_pf<M><<<(unsigned)nblk, kNT, fftx_inv_pf_smem_bytes<M>(), st>>>(spec, psi, Lp, hd, g, twx, tpx, scale);
+}
+
 void launch_fftx_inv(const double2 *spec, double *psi, Lay Lp, int hd, const GridK &g, const double2 *twx,
                      const double2 *tpx, double scale, cudaStream_t st) {
+  int dev = 0, sms = 0;
+  if (g.M == 256 && cudaGetDevice(&dev) == cudaSuccess &&
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0) {
+    launch_fftx_inv_pf<256>(spec, psi, Lp, hd, g, twx, tpx, scale, sms, st);
+    return;
+  }
   launch_fftx_inv_t<double2, false>(spec, psi, Lp, hd, g, twx, tpx, scale, st);
 }
 void launch_fftx_inv(const float2 *spec, double *psi, Lay Lp, int hd, const GridK &g, const float2 *twx,
@@ -618,6 +713,7 @@ cudaError_t prepare_xfft_kernels() {
   set((const void *)k_rhs_fftx<L, true>, fftx_smem_bytes(L, 16));
   TBFP_FFT_LENGTHS(TBFP_CASE)
 #undef TBFP_CASE
+  set((const void *)k_fftx_inv_pf<256>, fftx_inv_pf_smem_bytes<256>());
   return e;
 }
 
