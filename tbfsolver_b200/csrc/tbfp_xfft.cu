@@ -569,13 +569,15 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_inv(const V *_
   inv_last_pass_store<V, M, LOGTJ, ACC>(sm, tw, psi, Lp, hd, g, scale, r0, nrows);
 }
 
-// The same transform (FP64, M <= 256) as a persistent grid of 3 CTAs per SM
-// that stages each tile's spectrum in shared memory by cp.async, one tile
-// ahead: the copies of tile t+1 (the (M+1) x TJ entries, 128 contiguous bytes
-// per kx) are issued as soon as the first pass of tile t has read its stage,
-// so they land while tile t's middle passes, last pass and psi stores run.
-// k_fftx_inv issues a tile's loads only when its CTA starts and then waits
-// for them.  Tiles go round-robin over the CTAs (every tile costs the same).
+// The same transform (FP64, M = 128 or 256) as a persistent grid of 3 CTAs
+// per SM that stages each tile's spectrum in shared memory by cp.async, one
+// tile ahead: the copies of tile t+1 (the (M+1) x TJ entries, TJ*16 contiguous
+// bytes per kx) are issued as soon as the first pass of tile t has read its
+// stage, so they land while tile t's middle passes, last pass and psi stores
+// run.  k_fftx_inv issues a tile's loads only when its CTA starts and then
+// waits for them.  Tiles go round-robin over the CTAs (every tile costs the
+// same); the launcher takes this form only when every CTA gets two tiles or
+// more.
 template <int M>
 __host__ __device__ constexpr size_t fftx_inv_pf_smem_bytes() {
   return fftx_smem_bytes(M, 16) + (size_t)(M + 1) * fftx_rows_per_cta(M) * 16;
@@ -588,7 +590,6 @@ __global__ void __launch_bounds__(kNT, 3) k_fftx_inv_pf(const double2 *__restric
   using V = double2;
   constexpr int LOGRPW = ct_lognb(M), RPW = 1 << LOGRPW, LOGTJ = LOGRPW + 3, TJ = 1 << LOGTJ;
   constexpr int LD = x_row_stride(M);
-  static_assert(TJ == 8, "a stage row of one kx is 8 entries (128 bytes)");
   extern __shared__ __align__(16) unsigned char smx[];
   V *sm = reinterpret_cast<V *>(smx);
   V *tw = sm + TJ * LD;
@@ -682,10 +683,14 @@ static void launch_fftx_inv_pf(const double2 *spec, double *psi, Lay Lp, int hd,
 void launch_fftx_inv(const double2 *spec, double *psi, Lay Lp, int hd, const GridK &g, const double2 *twx,
                      const double2 *tpx, double scale, cudaStream_t st) {
   int dev = 0, sms = 0;
-  if (g.M == 256 && cudaGetDevice(&dev) == cudaSuccess &&
+  if ((g.M == 128 || g.M == 256) && cudaGetDevice(&dev) == cudaSuccess &&
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0) {
-    launch_fftx_inv_pf<256>(spec, psi, Lp, hd, g, twx, tpx, scale, sms, st);
-    return;
+    const long ntile = (g.R + fftx_rows_per_cta(g.M) - 1) / fftx_rows_per_cta(g.M);
+    if (ntile >= 6L * sms) {  // two tiles or more per CTA
+      if (g.M == 128) launch_fftx_inv_pf<128>(spec, psi, Lp, hd, g, twx, tpx, scale, sms, st);
+      else launch_fftx_inv_pf<256>(spec, psi, Lp, hd, g, twx, tpx, scale, sms, st);
+      return;
+    }
   }
   launch_fftx_inv_t<double2, false>(spec, psi, Lp, hd, g, twx, tpx, scale, st);
 }
@@ -713,6 +718,7 @@ cudaError_t prepare_xfft_kernels() {
   set((const void *)k_rhs_fftx<L, true>, fftx_smem_bytes(L, 16));
   TBFP_FFT_LENGTHS(TBFP_CASE)
 #undef TBFP_CASE
+  set((const void *)k_fftx_inv_pf<128>, fftx_inv_pf_smem_bytes<128>());
   set((const void *)k_fftx_inv_pf<256>, fftx_inv_pf_smem_bytes<256>());
   return e;
 }
