@@ -290,7 +290,8 @@ void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const dou
                     const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st);
 // FP64 spectrum with a two-word control block (zero before the first launch;
 // every launch leaves it zero) and the device's SM count: the persistent
-// prefetching form for 9..12 rows per lane, k_tridiag_t otherwise
+// prefetching forms for 257 <= ny <= 512 (one warp per pair up to 384 rows,
+// a two-warp team per pair above), k_tridiag_t otherwise
 void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, unsigned *ctl, int sms,
                     cudaStream_t st);

@@ -471,6 +471,333 @@ __global__ void __launch_bounds__(kWPB * 32, tri_pf_min_blocks<T>()) k_tridiag_p
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same solve split over a team of two warps per pair (FP64, persistent,
+// prefetching, off-diagonals in shared memory): team thread l = 0..63 owns the
+// U = ceil(ny/64) consecutive rows [l*U, l*U+U), so each thread's elimination
+// chain is half as long as with one warp per pair.  The 64 reduced equations
+// are two closed systems of 32, one per warp, once the couplings across the
+// warp boundary (C of equation 31 to y_32, A of equation 32 to y_31) move to a
+// fifth right-hand-side column (spike): warp 0 solves y = u + v y_32 and warp 1
+// y = u' + v' y_31 by the same cyclic reduction over shuffles, and the two
+// interface unknowns come from
+//   y_31 = (u_31 + v_31 u'_0) / (1 - v_31 v'_0),  y_32 = u'_0 + v'_0 y_31,
+// which is block Gaussian elimination of the reduced system.  The two warps
+// meet at named barriers (one per team): after the copies land, for the
+// neighbour terms of equation 31, for the interface values, and before a
+// buffer is refilled.  The (0,0) system keeps the serial pinned sweep (warp 0).
+// Tickets, retirement and the control block work as in k_tridiag_pf.
+// Used for 385 <= ny <= 512 (7 or 8 rows per thread), where one warp per pair
+// would hold 13..16 rows per lane and spill: at 1024 x 512 x 512 the y stage
+// went from 1.483 to 1.034 ms.  At 257 <= ny <= 384 k_tridiag_pf, whose warps
+// hold 8 pairs per SM in flight against 6 teams here, stays faster (0.190
+// against 0.209 ms at 512 x 384 x 256).
+// ---------------------------------------------------------------------------
+template <int U>
+__host__ __device__ constexpr size_t tri_team_smem_bytes(int teams) {
+  return (size_t)teams * 4 * 65 * U * sizeof(double2) + 2 * 65 * U * sizeof(double) +
+         (size_t)teams * 16 * sizeof(double) + (size_t)teams * 8;
+}
+
+__device__ __forceinline__ void team_bar(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
+
+template <int U, int TPC>
+__global__ void __launch_bounds__(TPC * 64, 3) k_tridiag_team(
+    double2 *__restrict__ spec, GridK g, const double *__restrict__ lamx, const double *__restrict__ lamz,
+    const double *__restrict__ am, const double *__restrict__ ap, const double *__restrict__ dyf, double mean_c,
+    double nxnz, unsigned *__restrict__ ctl) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int W = 65 * U;
+  const int team = threadIdx.x >> 6, l = threadIdx.x & 63, w = l >> 5, lane = threadIdx.x & 31;
+  const int bar = 1 + team;
+  double2 *buf = reinterpret_cast<double2 *>(smraw) + team * 4 * W;  // two buffers of (d0, d1)
+  double *cam = reinterpret_cast<double *>(reinterpret_cast<double2 *>(smraw) + TPC * 4 * W);
+  double *cap = cam + W;
+  double *xch = cap + W + team * 16;  // [0, 6): neighbour terms of equation 31; [6, 16): interface values
+  unsigned *tks = reinterpret_cast<unsigned *>(cap + W + TPC * 16) + 2 * team;
+  const int ny = g.ny, nz = g.nz, nzh = nz / 2 + 1;
+  const unsigned ntask = (unsigned)(g.nkx * nzh);
+  const unsigned nw = gridDim.x * TPC;
+  for (int i = threadIdx.x; i < W; i += TPC * 64) {
+    const int t = i / 65, o = i - t * 65, r = o * U + t;
+    const bool real = o < 64 && r < ny;
+    cam[i] = real ? am[r] : 0.0;
+    cap[i] = real ? ap[r] : 0.0;
+  }
+  __syncthreads();
+  auto pair = [&](unsigned q, int &kx, int &kz, bool &two, double2 *&S0, double2 *&S1) {
+    kx = (int)(q / (unsigned)nzh);
+    kz = (int)(q - (unsigned)kx * nzh);
+    const int kz2 = (kz == 0) ? 0 : nz - kz;
+    two = kz2 != kz;
+    S0 = spec + (long)kx * g.R + (long)kz * ny;
+    S1 = spec + (long)kx * g.R + (long)kz2 * ny;
+  };
+  // row e of the pair at team thread e / U, slot (e mod U)*65 + e / U
+  auto fill = [&](unsigned q, double2 *d0) {
+    int kx, kz;
+    bool two;
+    double2 *S0, *S1;
+    pair(q, kx, kz, two, S0, S1);
+    double2 *d1 = d0 + W;
+#pragma unroll
+    for (int c = 0; c < U; ++c) {
+      const int e = l + 64 * c;
+      const int o = e / U, sl = (e - o * U) * 65 + o;
+      if (e < ny) {
+        cp_async16(d0 + sl, S0 + e);
+        if (two) cp_async16(d1 + sl, S1 + e);
+      } else {
+        d0[sl] = mk<double2>(0.0, 0.0);
+        d1[sl] = mk<double2>(0.0, 0.0);
+      }
+    }
+  };
+  unsigned q = blockIdx.x * TPC + team;
+  unsigned qn = ntask;
+  if (q < ntask) {
+    fill(q, buf);
+    cp_async_commit();
+    if (l == 0) tks[0] = atomicAdd(ctl, 1u);
+    team_bar(bar);
+    qn = tks[0] + nw;
+  }
+  for (int it = 0; q < ntask; ++it) {
+    double2 *d0 = buf + (it & 1) * 2 * W, *d1 = d0 + W, *nxt = buf + ((it + 1) & 1) * 2 * W;
+    const bool more = qn < ntask;
+    if (more) fill(qn, nxt);
+    cp_async_commit();
+    unsigned tk = 0;
+    if (more && l == 0) tk = atomicAdd(ctl, 1u);
+    int kx, kz;
+    bool two;
+    double2 *S0, *S1;
+    pair(q, kx, kz, two, S0, S1);
+    const double lam = lamx[kx + g.kx0] + lamz[kz];
+    const bool pin = (kx + g.kx0 == 0 && kz == 0);
+    cp_async_wait_group<1>();
+    team_bar(bar);  // both warps' copies of this pair are visible
+    if (pin) {
+      if (w == 0) {  // serial pinned Thomas (as tri_pair_solve), factors in d1
+        double *cpin = reinterpret_cast<double *>(d1);
+        auto slot = [&](int e) { return (e % U) * 65 + e / U; };
+        if (lane == 0) {
+          double ct_p = 0.0;
+          double2 dt_p = mk<double2>(0.0, 0.0);
+          for (int e = 0; e < ny; ++e) {
+            const int sl = slot(e);
+            double ct = 0.0;
+            double2 dt = mk<double2>(0.0, 0.0);
+            if (e < ny - 1) {
+              const double a = am[e], c = ap[e];
+              const double2 f = d0[sl];
+              const double gi = 1.0 / ((lam - a - c) - a * ct_p);
+              ct = c * gi;
+              dt = mk<double2>((f.x - a * dt_p.x) * gi, (f.y - a * dt_p.y) * gi);
+            }
+            cpin[sl] = ct;
+            d0[sl] = dt;
+            ct_p = ct;
+            dt_p = dt;
+          }
+          double2 xn = d0[slot(ny - 1)];
+          for (int e = ny - 2; e >= 0; --e) {
+            const int sl = slot(e);
+            const double c = cpin[sl];
+            xn = mk<double2>(d0[sl].x - c * xn.x, d0[sl].y - c * xn.y);
+            d0[sl] = xn;
+          }
+        }
+        __syncwarp();
+        double sx = 0.0, sy = 0.0;
+        for (int e = lane; e < ny; e += 32) {
+          const double2 v = d0[slot(e)];
+          sx += v.x * dyf[e];
+          sy += v.y * dyf[e];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          sx += __shfl_xor_sync(0xffffffffu, sx, o);
+          sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        }
+        const double subx = sx * mean_c * nxnz, suby = sy * mean_c * nxnz;
+        for (int e = lane; e < ny; e += 32) {
+          const int sl = slot(e);
+          S0[e] = mk<double2>(d0[sl].x - subx, d0[sl].y - suby);
+        }
+      }
+    } else {
+      const int s0 = l * U;
+      // forward elimination within the thread's block (padding rows: diagonal one)
+      double at_r[U], ct_r[U];
+      double at_p = -1.0, ct_p = 0.0;
+      double2 p0 = mk<double2>(0.0, 0.0), p1 = mk<double2>(0.0, 0.0);
+#pragma unroll
+      for (int t = 0; t < U; ++t) {
+        const bool real = s0 + t < ny;
+        const double a = cam[t * 65 + l], c = cap[t * 65 + l];
+        const double dg = real ? lam : 1.0;
+        const int sl = t * 65 + l;
+        const double gi = rcp_nr((dg - a - c) - a * ct_p);
+        const double2 f0 = d0[sl], f1 = d1[sl];
+        p0 = mk<double2>((f0.x - a * p0.x) * gi, (f0.y - a * p0.y) * gi);
+        p1 = mk<double2>((f1.x - a * p1.x) * gi, (f1.y - a * p1.y) * gi);
+        d0[sl] = p0;
+        d1[sl] = p1;
+        at_p = -a * at_p * gi;
+        ct_p = c * gi;
+        at_r[t] = at_p;
+        ct_r[t] = ct_p;
+      }
+      // running backward pass: x_s = hd - ha x_{s-1} - hc x_e
+      double ha = 0.0, hc = -1.0;
+      double2 h0 = mk<double2>(0.0, 0.0), h1 = mk<double2>(0.0, 0.0);
+      if constexpr (U >= 2) {
+        h0 = d0[(U - 2) * 65 + l];
+        h1 = d1[(U - 2) * 65 + l];
+        ha = at_r[U - 2];
+        hc = ct_r[U - 2];
+#pragma unroll
+        for (int t = U - 3; t >= 0; --t) {
+          const double2 v0 = d0[t * 65 + l], v1 = d1[t * 65 + l];
+          const double ct = ct_r[t];
+          h0 = mk<double2>(v0.x - ct * h0.x, v0.y - ct * h0.y);
+          h1 = mk<double2>(v1.x - ct * h1.x, v1.y - ct * h1.y);
+          ha = at_r[t] - ct * ha;
+          hc = -ct * hc;
+        }
+      }
+      // the next thread's terms: by shuffle inside a warp, through xch across
+      if (w == 1 && lane == 0) {
+        xch[0] = ha;
+        xch[1] = hc;
+        xch[2] = h0.x;
+        xch[3] = h0.y;
+        xch[4] = h1.x;
+        xch[5] = h1.y;
+      }
+      double ha_n = shdn(ha, 1), hc_n = shdn(hc, 1);
+      double h0x = shdn(h0.x, 1), h0y = shdn(h0.y, 1), h1x = shdn(h1.x, 1), h1y = shdn(h1.y, 1);
+      team_bar(bar);
+      if (w == 0 && lane == 31) {
+        ha_n = xch[0];
+        hc_n = xch[1];
+        h0x = xch[2];
+        h0y = xch[3];
+        h1x = xch[4];
+        h1y = xch[5];
+      }
+      const double at_e = at_r[U - 1], ct_e = ct_r[U - 1];
+      double A = at_e, B = 1.0, C = 0.0;
+      double D[5] = {p0.x, p0.y, p1.x, p1.y, 0.0};
+      if (l < 63) {
+        B = 1.0 - ct_e * ha_n;
+        C = -ct_e * hc_n;
+        D[0] -= ct_e * h0x;
+        D[1] -= ct_e * h0y;
+        D[2] -= ct_e * h1x;
+        D[3] -= ct_e * h1y;
+      }
+      // the coupling across the warp boundary becomes the spike column
+      if (w == 0 && lane == 31) {
+        D[4] = -C;
+        C = 0.0;
+      }
+      if (w == 1 && lane == 0) {
+        D[4] = -A;
+        A = 0.0;
+      }
+#pragma unroll
+      for (int h = 1; h < 32; h <<= 1) {
+        const double iB = rcp_nr(B);
+        double Am = shup(A, h), iBm = shup(iB, h), Cm = shup(C, h);
+        double Ap = shdn(A, h), iBp = shdn(iB, h), Cp = shdn(C, h);
+        double Dm[5], Dp[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          Dm[c] = shup(D[c], h);
+          Dp[c] = shdn(D[c], h);
+        }
+        const bool lo = lane < h, hi = lane + h >= 32;
+        const double k1 = lo ? 0.0 : A * iBm, k2 = hi ? 0.0 : C * iBp;
+        if (lo) Am = Cm = 0.0;
+        if (hi) Ap = Cp = 0.0;
+        B = B - k1 * Cm - k2 * Ap;
+        A = -k1 * Am;
+        C = -k2 * Cp;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) D[c] = D[c] - k1 * Dm[c] - k2 * Dp[c];
+      }
+      const double iBf = rcp_nr(B);
+      double y[5];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) y[c] = D[c] * iBf;
+      // interface unknowns y_31 and y_32
+      if (w == 0 && lane == 31) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) xch[6 + c] = y[c];
+      }
+      if (w == 1 && lane == 0) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) xch[11 + c] = y[c];
+      }
+      team_bar(bar);
+      const double v31 = xch[10], v32 = xch[15];
+      const double den = 1.0 - v31 * v32;
+      double y31[4], y32[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        y31[c] = (xch[6 + c] + v31 * xch[11 + c]) / den;
+        y32[c] = xch[11 + c] + v32 * y31[c];
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) y[c] = y[c] + y[4] * (w == 0 ? y32[c] : y31[c]);
+      double ys[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const double v = shup(y[c], 1);  // every lane takes part in the shuffle
+        ys[c] = (lane == 0) ? (w == 0 ? 0.0 : y31[c]) : v;
+      }
+      double2 x0 = mk<double2>(y[0], y[1]), x1 = mk<double2>(y[2], y[3]);
+      d0[(U - 1) * 65 + l] = x0;
+      d1[(U - 1) * 65 + l] = x1;
+#pragma unroll
+      for (int t = U - 2; t >= 0; --t) {
+        const int sl = t * 65 + l;
+        const double a = at_r[t], c = ct_r[t];
+        const double2 v0 = d0[sl], v1 = d1[sl];
+        x0 = mk<double2>(v0.x - a * ys[0] - c * x0.x, v0.y - a * ys[1] - c * x0.y);
+        x1 = mk<double2>(v1.x - a * ys[2] - c * x1.x, v1.y - a * ys[3] - c * x1.y);
+        d0[sl] = x0;
+        d1[sl] = x1;
+      }
+      team_bar(bar);  // every row of the pair is solved
+#pragma unroll
+      for (int c = 0; c < U; ++c) {
+        const int e = l + 64 * c;
+        if (e < ny) {
+          const int o = e / U, sl = (e - o * U) * 65 + o;
+          S0[e] = d0[sl];
+          if (two) S1[e] = d1[sl];
+        }
+      }
+    }
+    if (l == 0) tks[0] = tk;
+    team_bar(bar);  // the buffer is free for the refill; the ticket is visible
+    const unsigned b = tks[0];
+    q = qn;
+    qn = more ? b + nw : ntask;
+  }
+  cp_async_wait_all();
+  if (l == 0) {
+    __threadfence();
+    if (atomicAdd(ctl + 1, 1u) == nw - 1) {  // every other team has taken its last ticket
+      atomicExch(ctl, 0u);
+      atomicExch(ctl + 1, 0u);
+    }
+  }
+}
+
 // shared memory of a k_tridiag<V, TM> block: the two right-hand sides per warp,
 // plus the coefficient arrays when TM == 0
 static size_t tridiag_block_smem(int T, int TM) {
@@ -519,11 +846,30 @@ static void launch_tridiag_pf_n(double2 *spec, const GridK &g, const double *lam
                                                                            mean_c, nxnz, ctl);
 }
 
+template <int U, int TPC>
+static void launch_tridiag_team_n(double2 *spec, const GridK &g, const double *lamx, const double *lamz,
+                                  const double *am, const double *ap, const double *dyf, double mean_c, double nxnz,
+                                  unsigned *ctl, int sms, cudaStream_t st) {
+  const long npair = (long)g.nkx * (g.nz / 2 + 1);
+  long nblk = (npair + TPC - 1) / TPC;
+  const size_t smem = tri_team_smem_bytes<U>(TPC);
+  long per_sm = (long)(233472 / (smem + 1024));  // shared memory per SM, 1 KB reserved per CTA
+  if (per_sm > 3) per_sm = 3;
+  if (per_sm < 1) per_sm = 1;
+  if (nblk > per_sm * sms) nblk = per_sm * sms;
+  k_tridiag_team<U, TPC><<<(unsigned)nblk, TPC * 64, smem, st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl);
+}
+
 void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, unsigned *ctl, int sms,
                     cudaStream_t st) {
   const int T = tri_rows_per_lane(g.ny);
   if (ctl && sms > 0) {
+    switch ((g.ny + 63) / 64) {  // 385 <= ny <= 512: two-warp teams
+      case 7: launch_tridiag_team_n<7, 2>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl, sms, st); return;
+      case 8: launch_tridiag_team_n<8, 2>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl, sms, st); return;
+      default: break;
+    }
     switch (T) {
 #define TBFP_TRI_PF(TT) \
   case TT: launch_tridiag_pf_n<TT>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl, sms, st); return;
@@ -595,6 +941,8 @@ cudaError_t prepare_yz_kernels() {
   TBFP_TRI_T(8) TBFP_TRI_T(9) TBFP_TRI_T(10) TBFP_TRI_T(11) TBFP_TRI_T(12) TBFP_TRI_T(13) TBFP_TRI_T(14)
   TBFP_TRI_T(15) TBFP_TRI_T(16)
 #undef TBFP_TRI_T
+  set((const void *)k_tridiag_team<7, 2>, tri_team_smem_bytes<7>(2));
+  set((const void *)k_tridiag_team<8, 2>, tri_team_smem_bytes<8>(2));
 #define TBFP_TRI_PF(TT) set((const void *)k_tridiag_pf<TT>, tri_pf_smem_bytes<TT>());
   TBFP_TRI_PF(9) TBFP_TRI_PF(10) TBFP_TRI_PF(11) TBFP_TRI_PF(12)
 #undef TBFP_TRI_PF

@@ -179,13 +179,15 @@ def test_solve_fps_random_rhs(dims, stretched):
     assert rel_linf(got, want.a) < TOL_P
 
 
-@pytest.mark.parametrize("ny", [260, 300, 333, 384])
+@pytest.mark.parametrize("ny", [260, 300, 333, 384, 420, 500])
 def test_persistent_y_solve_against_the_oracle_and_across_calls(ny):
-    """ny in 257..384 puts 9..12 rows on each lane, which the persistent y
-    solve takes (its warps prefetch their next pair and take pairs by ticket).
-    256 x ny x 64 has 4257 pairs, several per warp.  Three solves on one handle
-    give the same bits (the ticket counters return to zero after each launch),
-    and the answer matches the oracle."""
+    """ny in 257..384 takes the persistent one-warp-per-pair y solve (9..12
+    rows per lane), ny in 385..512 the two-warp team form (7 or 8 rows per
+    thread; the two warps' reduced systems meet through the spike column).
+    Both prefetch their next pair and take pairs by ticket.  256 x ny x 64 has
+    4257 pairs, several per warp or team.  Three solves on one handle give the
+    same bits (the ticket counters return to zero after each launch), and the
+    answer matches the oracle."""
     nx, nz = 256, 64
     g = Grid(nx, ny, nz, 2 * np.pi, 2.0, np.pi, True, 1.5)
     m = mesh_of(g)
