@@ -537,6 +537,56 @@ __device__ __forceinline__ void fftz_body(V *__restrict__ spec, GridK g, const V
   }
 }
 
+// Serial Thomas sweep of the pinned (0,0) y system on one thread: row e's
+// right-hand side at d0[slot(e)], its off-diagonals from am_at(e), ap_at(e);
+// the elimination factors go to cpin[slot(e)] and the solution back to d0.
+// The last unknown is pinned to zero (Neumann walls make the system
+// singular).  The next row's operands are loaded one step ahead, so the loads
+// stay off the dependent chain of the elimination, and the reciprocal is the
+// Newton-refined rcp_nr of the parallel elimination.
+template <typename SlotF, typename AmF, typename ApF>
+__device__ __forceinline__ void pinned_sweep(double2 *d0, double *cpin, double lam, int ny, SlotF slot, AmF am_at,
+                                             ApF ap_at) {
+  double ct_p = 0.0;
+  double2 dt_p = mk<double2>(0.0, 0.0);
+  double a_n = am_at(0), c_n = ap_at(0);
+  double2 f_n = d0[slot(0)];
+  for (int e = 0; e < ny - 1; ++e) {
+    const double a = a_n, c = c_n;
+    const double2 f = f_n;
+    const int sl = slot(e);
+    if (e + 1 < ny - 1) {
+      a_n = am_at(e + 1);
+      c_n = ap_at(e + 1);
+      f_n = d0[slot(e + 1)];
+    }
+    const double gi = rcp_nr((lam - a - c) - a * ct_p);
+    ct_p = c * gi;
+    dt_p = mk<double2>((f.x - a * dt_p.x) * gi, (f.y - a * dt_p.y) * gi);
+    cpin[sl] = ct_p;
+    d0[sl] = dt_p;
+  }
+  {
+    const int sl = slot(ny - 1);
+    cpin[sl] = 0.0;
+    d0[sl] = mk<double2>(0.0, 0.0);
+  }
+  double2 xn = mk<double2>(0.0, 0.0);
+  double c_b = cpin[slot(ny - 2)];
+  double2 d_b = d0[slot(ny - 2)];
+  for (int e = ny - 2; e >= 0; --e) {
+    const double c = c_b;
+    const double2 dv = d_b;
+    const int sl = slot(e);
+    if (e > 0) {
+      c_b = cpin[slot(e - 1)];
+      d_b = d0[slot(e - 1)];
+    }
+    xn = mk<double2>(dv.x - c * xn.x, dv.y - c * xn.y);
+    d0[sl] = xn;
+  }
+}
+
 // Right-hand sides of the y systems (kx, kz) and (kx, nz - kz) into d0 / d1:
 // row e lives in lane e / T at slot (e mod T)*33 + lane, padding rows are zero.
 // FP64 rows go by cp.async (the caller waits for them); FP32 rows are widened
@@ -617,35 +667,15 @@ __device__ __forceinline__ void tri_pair_solve(V *S0, V *S1, bool two, double la
   auto st = [](double2 v) { return mk<V>((VT)v.x, (VT)v.y); };
   const int s0 = lane * T;
 
-  if (pin) {  // single system: pinned serial Thomas (as k_tridiag), factors in d1
+  if (pin) {  // single system: pinned serial Thomas, factors in d1
     double *cpin = reinterpret_cast<double *>(d1);
     auto slot = [&](int e) { return (e % T) * 33 + e / T; };
     if (lane == 0) {
-      double ct_p = 0.0;
-      double2 dt_p = mk<double2>(0.0, 0.0);
-      for (int e = 0; e < ny; ++e) {
-        const int sl = slot(e);
-        double ct = 0.0;
-        double2 dt = mk<double2>(0.0, 0.0);
-        if (e < ny - 1) {
-          const double a = am[e], c = ap[e];
-          const double2 f = d0[sl];
-          const double gi = 1.0 / ((lam - a - c) - a * ct_p);
-          ct = c * gi;
-          dt = mk<double2>((f.x - a * dt_p.x) * gi, (f.y - a * dt_p.y) * gi);
-        }
-        cpin[sl] = ct;
-        d0[sl] = dt;
-        ct_p = ct;
-        dt_p = dt;
-      }
-      double2 xn = d0[slot(ny - 1)];
-      for (int e = ny - 2; e >= 0; --e) {
-        const int sl = slot(e);
-        const double c = cpin[sl];
-        xn = mk<double2>(d0[sl].x - c * xn.x, d0[sl].y - c * xn.y);
-        d0[sl] = xn;
-      }
+      if constexpr (SMC)  // the shared copies use the right-hand sides' slots
+        pinned_sweep(d0, cpin, lam, ny, slot, [&](int e) { return cam[slot(e)]; },
+                     [&](int e) { return cap[slot(e)]; });
+      else
+        pinned_sweep(d0, cpin, lam, ny, slot, [&](int e) { return am[e]; }, [&](int e) { return ap[e]; });
     }
     __syncwarp();
     double sx = 0.0, sy = 0.0;

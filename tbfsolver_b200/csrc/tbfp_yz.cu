@@ -581,33 +581,9 @@ __global__ void __launch_bounds__(TPC * 64, 3) k_tridiag_team(
       if (w == 0) {  // serial pinned Thomas (as tri_pair_solve), factors in d1
         double *cpin = reinterpret_cast<double *>(d1);
         auto slot = [&](int e) { return (e % U) * 65 + e / U; };
-        if (lane == 0) {
-          double ct_p = 0.0;
-          double2 dt_p = mk<double2>(0.0, 0.0);
-          for (int e = 0; e < ny; ++e) {
-            const int sl = slot(e);
-            double ct = 0.0;
-            double2 dt = mk<double2>(0.0, 0.0);
-            if (e < ny - 1) {
-              const double a = am[e], c = ap[e];
-              const double2 f = d0[sl];
-              const double gi = 1.0 / ((lam - a - c) - a * ct_p);
-              ct = c * gi;
-              dt = mk<double2>((f.x - a * dt_p.x) * gi, (f.y - a * dt_p.y) * gi);
-            }
-            cpin[sl] = ct;
-            d0[sl] = dt;
-            ct_p = ct;
-            dt_p = dt;
-          }
-          double2 xn = d0[slot(ny - 1)];
-          for (int e = ny - 2; e >= 0; --e) {
-            const int sl = slot(e);
-            const double c = cpin[sl];
-            xn = mk<double2>(d0[sl].x - c * xn.x, d0[sl].y - c * xn.y);
-            d0[sl] = xn;
-          }
-        }
+        if (lane == 0)  // the shared off-diagonals use the right-hand sides' slots
+          pinned_sweep(d0, cpin, lam, ny, slot, [&](int e) { return cam[slot(e)]; },
+                       [&](int e) { return cap[slot(e)]; });
         __syncwarp();
         double sx = 0.0, sy = 0.0;
         for (int e = lane; e < ny; e += 32) {

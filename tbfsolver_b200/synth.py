@@ -75,6 +75,10 @@ CONFIGS = {
     # captures that must stay small
     "c6": ChannelSpec("c6-512x384x128-tanh1.5", 512, 384, 128, y_stretched=True, gamma=1.5, nbubbles=100,
                       radius=0.1, rhol=1.0, rhog=0.02),
+    # c3's y-solve instance (512 rows) on a small grid whose spectrum (135 MB)
+    # is still larger than L2, for profiling captures
+    "c7": ChannelSpec("c7-256x512x128-tanh1.5", 256, 512, 128, y_stretched=True, gamma=1.5, nbubbles=60,
+                      radius=0.15, rhol=1.0, rhog=0.02),
 }
 
 
