@@ -110,6 +110,7 @@ struct tbfp_handle {
   double *d_irho = nullptr;
   unsigned long long *d_maxdiv = nullptr;
   unsigned *d_tri_ctl = nullptr;  // ticket and retire counts of the persistent y solve (zero between launches)
+  double *d_pinf = nullptr;       // elimination factors of the pinned (0,0) y system
   int sms = 0;                    // SMs of the handle's device
   // device copies used by the host-pointer entry points
   double *h_ux = nullptr, *h_uy = nullptr, *h_uz = nullptr;
@@ -299,7 +300,7 @@ CorrArgs corr_args(tbfp_handle *h, const double *uxi, const double *uyi, const d
 void fps_spectral_solve(tbfp_handle *h) {
   launch_fftz(h->d_spec, h->g, h->d_tpz, false, h->stream);
   launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, h->d_tri_ctl,
-                 h->sms, h->stream);
+                 h->sms, h->d_pinf, h->stream);
   launch_fftz(h->d_spec, h->g, h->d_tpz, true, h->stream);
 }
 
@@ -577,7 +578,7 @@ int device_projection(tbfp_handle *h, const double *uxi, const double *uyi, cons
     launch_fftz(h->d_spec, h->g, h->d_tpz, false, s);
     mark(3);
     launch_tridiag(h->d_spec, h->g, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz,
-                   h->d_tri_ctl, h->sms, s);
+                   h->d_tri_ctl, h->sms, h->d_pinf, s);
     mark(4);
     launch_fftz(h->d_spec, h->g, h->d_tpz, true, s);
     mark(5);
@@ -937,11 +938,13 @@ int create_impl(const tbfp_desc *d, const SlabSpec *sl, tbfp_handle **out) {
   if ((rc = dev_alloc(h, &h->d_spec, (size_t)h->nkx * h->R)) || (rc = dev_alloc(h, &h->d_irho, h->n_rho)) ||
       (rc = dev_alloc(h, &h->d_s, h->n_psi)) ||
       (rc = dev_alloc(h, &h->d_maxdiv, 1)) || (rc = dev_alloc(h, &h->d_ctl, 1)) ||
-      (rc = dev_alloc(h, &h->d_tri_ctl, 2)))
+      (rc = dev_alloc(h, &h->d_tri_ctl, 2)) || (rc = dev_alloc(h, &h->d_pinf, (size_t)2 * ny)))
     return fail(rc);
   {
-    const cudaError_t e = cudaMemset(h->d_tri_ctl, 0, 2 * sizeof(unsigned));
+    cudaError_t e = cudaMemset(h->d_tri_ctl, 0, 2 * sizeof(unsigned));
     if (e != cudaSuccess) return fail(cuda_err(h, e, "cudaMemset"));
+    launch_pin_factors(h->d_am, h->d_ap, h->d_lamx, h->d_lamz, ny, h->d_pinf, h->stream);
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return fail(cuda_err(h, e, "k_pin_factors"));
     if (cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess) h->sms = 0;
   }
 
@@ -1003,7 +1006,7 @@ int tbfp_slab_spectral(tbfp_handle *h, double *spec_x) {
   double2 *sp = reinterpret_cast<double2 *>(spec_x);
   launch_fftz(sp, h->gs, h->d_tpz, false, h->stream);
   launch_tridiag(sp, h->gs, h->d_lamx, h->d_lamz, h->d_am, h->d_ap, h->d_dyf, h->mean_c, h->nxnz, h->d_tri_ctl, h->sms,
-                 h->stream);
+                 h->d_pinf, h->stream);
   launch_fftz(sp, h->gs, h->d_tpz, true, h->stream);
   return finish(h, "tbfp_slab_spectral");
 }

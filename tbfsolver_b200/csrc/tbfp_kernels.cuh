@@ -294,7 +294,11 @@ void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const dou
 // a two-warp team per pair above), k_tridiag_t otherwise
 void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, unsigned *ctl, int sms,
-                    cudaStream_t st);
+                    const double *pinf, cudaStream_t st);
+// the pinned (0,0) system's elimination factors (2*(ny-1) doubles) for the
+// persistent forms; pinf == nullptr makes them compute the factors inline
+void launch_pin_factors(const double *am, const double *ap, const double *lamx, const double *lamz, int ny, double *f,
+                        cudaStream_t st);
 void launch_tridiag(float2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st);
 void launch_fftx_inv(const double2 *spec, double *psi, Lay Lp, int hd, const GridK &g, const double2 *twx,

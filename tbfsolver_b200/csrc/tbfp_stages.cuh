@@ -587,6 +587,45 @@ __device__ __forceinline__ void pinned_sweep(double2 *d0, double *cpin, double l
   }
 }
 
+// The same sweep with the elimination factors of the pinned system taken from
+// a table (fs[2e] = 1/pivot, fs[2e+1] = ct_e for e < ny-1, made once per
+// handle by k_pin_factors with the arithmetic above): the system's matrix does
+// not change between calls, so only the right-hand side's recurrence is left
+// on the dependent chain.
+template <typename SlotF, typename AmF>
+__device__ __forceinline__ void pinned_sweep_f(double2 *d0, const double *fs, int ny, SlotF slot, AmF am_at) {
+  double2 dt_p = mk<double2>(0.0, 0.0);
+  double a_n = am_at(0), g_n = fs[0];
+  double2 f_n = d0[slot(0)];
+  for (int e = 0; e < ny - 1; ++e) {
+    const double a = a_n, gi = g_n;
+    const double2 f = f_n;
+    const int sl = slot(e);
+    if (e + 1 < ny - 1) {
+      a_n = am_at(e + 1);
+      g_n = fs[2 * (e + 1)];
+      f_n = d0[slot(e + 1)];
+    }
+    dt_p = mk<double2>((f.x - a * dt_p.x) * gi, (f.y - a * dt_p.y) * gi);
+    d0[sl] = dt_p;
+  }
+  d0[slot(ny - 1)] = mk<double2>(0.0, 0.0);
+  double2 xn = mk<double2>(0.0, 0.0);
+  double c_b = fs[2 * (ny - 2) + 1];
+  double2 d_b = d0[slot(ny - 2)];
+  for (int e = ny - 2; e >= 0; --e) {
+    const double c = c_b;
+    const double2 dv = d_b;
+    const int sl = slot(e);
+    if (e > 0) {
+      c_b = fs[2 * (e - 1) + 1];
+      d_b = d0[slot(e - 1)];
+    }
+    xn = mk<double2>(dv.x - c * xn.x, dv.y - c * xn.y);
+    d0[sl] = xn;
+  }
+}
+
 // Right-hand sides of the y systems (kx, kz) and (kx, nz - kz) into d0 / d1:
 // row e lives in lane e / T at slot (e mod T)*33 + lane, padding rows are zero.
 // FP64 rows go by cp.async (the caller waits for them); FP32 rows are widened
@@ -622,14 +661,15 @@ __device__ __forceinline__ void tri_pair_solve(V *S0, V *S1, bool two, double la
                                                const double *__restrict__ am, const double *__restrict__ ap,
                                                const double *__restrict__ dyf, double mean_c, double nxnz, int ny,
                                                int lane, double2 *d0, double2 *d1, const double *cam = nullptr,
-                                               const double *cap = nullptr);
+                                               const double *cap = nullptr, const double *pinf = nullptr);
 
 template <typename V, int T>
 __device__ __forceinline__ void tridiag_t_body(V *__restrict__ spec, GridK g, const double *__restrict__ lamx,
                                                const double *__restrict__ lamz, const double *__restrict__ am,
                                                const double *__restrict__ ap, const double *__restrict__ dyf,
                                                double mean_c, double nxnz, unsigned q, int warp,
-                                               unsigned char * /*dynamic shared memory: named below*/) {
+                                               unsigned char * /*dynamic shared memory: named below*/,
+                                               const double *pinf = nullptr) {
   extern __shared__ __align__(16) unsigned char smraw[];  // the launch's dynamic shared memory
   constexpr int W = 33 * T;
   const int ny = g.ny, nz = g.nz;
@@ -648,7 +688,7 @@ __device__ __forceinline__ void tridiag_t_body(V *__restrict__ spec, GridK g, co
   const bool pin = (kx + g.kx0 == 0 && kz == 0);
   if constexpr (sizeof(V) == sizeof(double2)) cp_async_wait_all();
   __syncwarp();
-  tri_pair_solve<V, T>(S0, S1, two, lam, pin, am, ap, dyf, mean_c, nxnz, ny, lane, d0, d1);
+  tri_pair_solve<V, T>(S0, S1, two, lam, pin, am, ap, dyf, mean_c, nxnz, ny, lane, d0, d1, nullptr, nullptr, pinf);
 }
 
 // Solve of the pair whose right-hand sides tri_pair_fill put in d0 / d1 (every
@@ -662,7 +702,7 @@ __device__ __forceinline__ void tri_pair_solve(V *S0, V *S1, bool two, double la
                                                const double *__restrict__ am, const double *__restrict__ ap,
                                                const double *__restrict__ dyf, double mean_c, double nxnz, int ny,
                                                int lane, double2 *d0, double2 *d1, const double *cam,
-                                               const double *cap) {
+                                               const double *cap, const double *pinf) {
   using VT = decltype(V::x);
   auto st = [](double2 v) { return mk<V>((VT)v.x, (VT)v.y); };
   const int s0 = lane * T;
@@ -670,12 +710,21 @@ __device__ __forceinline__ void tri_pair_solve(V *S0, V *S1, bool two, double la
   if (pin) {  // single system: pinned serial Thomas, factors in d1
     double *cpin = reinterpret_cast<double *>(d1);
     auto slot = [&](int e) { return (e % T) * 33 + e / T; };
-    if (lane == 0) {
-      if constexpr (SMC)  // the shared copies use the right-hand sides' slots
+    if constexpr (SMC) {
+      if (pinf) {  // the factor table, copied by the warp into d1
+        for (int i = lane; i < 2 * (ny - 1); i += 32) cpin[i] = pinf[i];
+        __syncwarp();
+        if (lane == 0) pinned_sweep_f(d0, cpin, ny, slot, [&](int e) { return cam[slot(e)]; });
+      } else if (lane == 0) {  // the shared copies use the right-hand sides' slots
         pinned_sweep(d0, cpin, lam, ny, slot, [&](int e) { return cam[slot(e)]; },
                      [&](int e) { return cap[slot(e)]; });
-      else
-        pinned_sweep(d0, cpin, lam, ny, slot, [&](int e) { return am[e]; }, [&](int e) { return ap[e]; });
+      }
+    } else if (pinf) {  // the factor table, copied by the warp into d1
+      for (int i = lane; i < 2 * (ny - 1); i += 32) cpin[i] = pinf[i];
+      __syncwarp();
+      if (lane == 0) pinned_sweep_f(d0, cpin, ny, slot, [&](int e) { return am[e]; });
+    } else if (lane == 0) {
+      pinned_sweep(d0, cpin, lam, ny, slot, [&](int e) { return am[e]; }, [&](int e) { return ap[e]; });
     }
     __syncwarp();
     double sx = 0.0, sy = 0.0;

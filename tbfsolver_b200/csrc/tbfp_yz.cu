@@ -358,10 +358,10 @@ template <typename V, int T>
 __global__ void __launch_bounds__(kWPB * 32, tri_min_blocks<T>()) k_tridiag_t(
     V *__restrict__ spec, GridK g, const double *__restrict__ lamx, const double *__restrict__ lamz,
     const double *__restrict__ am, const double *__restrict__ ap, const double *__restrict__ dyf, double mean_c,
-    double nxnz) {
+    double nxnz, const double *__restrict__ pinf) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int warp = threadIdx.x >> 5;
-  tridiag_t_body<V, T>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, blockIdx.x * kWPB + warp, warp, smraw);
+  tridiag_t_body<V, T>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, blockIdx.x * kWPB + warp, warp, smraw, pinf);
 }
 
 // ---------------------------------------------------------------------------
@@ -397,7 +397,7 @@ template <int T>
 __global__ void __launch_bounds__(kWPB * 32, tri_pf_min_blocks<T>()) k_tridiag_pf(
     double2 *__restrict__ spec, GridK g, const double *__restrict__ lamx, const double *__restrict__ lamz,
     const double *__restrict__ am, const double *__restrict__ ap, const double *__restrict__ dyf, double mean_c,
-    double nxnz, unsigned *__restrict__ ctl) {
+    double nxnz, unsigned *__restrict__ ctl, const double *__restrict__ pinf) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int W = 33 * T;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -455,7 +455,7 @@ __global__ void __launch_bounds__(kWPB * 32, tri_pf_min_blocks<T>()) k_tridiag_p
     cp_async_wait_group<1>();  // this pair's copies have landed; the next pair's may be in flight
     __syncwarp();
     tri_pair_solve<double2, T, true>(S0, S1, two, lam, pin, am, ap, dyf, mean_c, nxnz, ny, lane, cur, cur + W, cam,
-                                     cap);
+                                     cap, pinf);
     __syncwarp();  // every lane is done with cur before it is refilled
     const unsigned b = __shfl_sync(0xffffffffu, t, 0);
     q = qn;
@@ -505,7 +505,7 @@ template <int U, int TPC>
 __global__ void __launch_bounds__(TPC * 64, 3) k_tridiag_team(
     double2 *__restrict__ spec, GridK g, const double *__restrict__ lamx, const double *__restrict__ lamz,
     const double *__restrict__ am, const double *__restrict__ ap, const double *__restrict__ dyf, double mean_c,
-    double nxnz, unsigned *__restrict__ ctl) {
+    double nxnz, unsigned *__restrict__ ctl, const double *__restrict__ pinf) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int W = 65 * U;
   const int team = threadIdx.x >> 6, l = threadIdx.x & 63, w = l >> 5, lane = threadIdx.x & 31;
@@ -581,9 +581,14 @@ __global__ void __launch_bounds__(TPC * 64, 3) k_tridiag_team(
       if (w == 0) {  // serial pinned Thomas (as tri_pair_solve), factors in d1
         double *cpin = reinterpret_cast<double *>(d1);
         auto slot = [&](int e) { return (e % U) * 65 + e / U; };
-        if (lane == 0)  // the shared off-diagonals use the right-hand sides' slots
+        if (pinf) {  // the factor table, copied by the warp into d1
+          for (int i = lane; i < 2 * (ny - 1); i += 32) cpin[i] = pinf[i];
+          __syncwarp();
+          if (lane == 0) pinned_sweep_f(d0, cpin, ny, slot, [&](int e) { return cam[slot(e)]; });
+        } else if (lane == 0) {  // the shared off-diagonals use the right-hand sides' slots
           pinned_sweep(d0, cpin, lam, ny, slot, [&](int e) { return cam[slot(e)]; },
                        [&](int e) { return cap[slot(e)]; });
+        }
         __syncwarp();
         double sx = 0.0, sy = 0.0;
         for (int e = lane; e < ny; e += 32) {
@@ -782,7 +787,8 @@ static size_t tridiag_block_smem(int T, int TM) {
 
 template <typename V>
 static void launch_tridiag_t(V *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
-                             const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st) {
+                             const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st,
+                             const double *pinf = nullptr) {
   const long nwarps = (long)g.nkx * (g.nz / 2 + 1);
   const unsigned nblk = (unsigned)((nwarps + kWPB - 1) / kWPB);
   const int T = tri_rows_per_lane(g.ny);
@@ -792,7 +798,7 @@ static void launch_tridiag_t(V *spec, const GridK &g, const double *lamx, const 
   const size_t sm2 = (size_t)kWPB * 2 * 33 * T * sizeof(double2);
   switch (T) {
 #define TBFP_TRI_T(TT) \
-  case TT: k_tridiag_t<V, TT><<<nblk, blk, sm2, st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz); return;
+  case TT: k_tridiag_t<V, TT><<<nblk, blk, sm2, st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, pinf); return;
     TBFP_TRI_T(1) TBFP_TRI_T(2) TBFP_TRI_T(3) TBFP_TRI_T(4) TBFP_TRI_T(5) TBFP_TRI_T(6) TBFP_TRI_T(7)
     TBFP_TRI_T(8) TBFP_TRI_T(9) TBFP_TRI_T(10) TBFP_TRI_T(11) TBFP_TRI_T(12) TBFP_TRI_T(13) TBFP_TRI_T(14)
     TBFP_TRI_T(15) TBFP_TRI_T(16)
@@ -813,19 +819,19 @@ void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const dou
 template <int T>
 static void launch_tridiag_pf_n(double2 *spec, const GridK &g, const double *lamx, const double *lamz,
                                 const double *am, const double *ap, const double *dyf, double mean_c, double nxnz,
-                                unsigned *ctl, int sms, cudaStream_t st) {
+                                unsigned *ctl, int sms, const double *pinf, cudaStream_t st) {
   const long npair = (long)g.nkx * (g.nz / 2 + 1);
   long nblk = (npair + kWPB - 1) / kWPB;
   const long resident = (long)sms * tri_pf_min_blocks<T>();
   if (nblk > resident) nblk = resident;
   k_tridiag_pf<T><<<(unsigned)nblk, kWPB * 32, tri_pf_smem_bytes<T>(), st>>>(spec, g, lamx, lamz, am, ap, dyf,
-                                                                           mean_c, nxnz, ctl);
+                                                                           mean_c, nxnz, ctl, pinf);
 }
 
 template <int U, int TPC>
 static void launch_tridiag_team_n(double2 *spec, const GridK &g, const double *lamx, const double *lamz,
                                   const double *am, const double *ap, const double *dyf, double mean_c, double nxnz,
-                                  unsigned *ctl, int sms, cudaStream_t st) {
+                                  unsigned *ctl, int sms, const double *pinf, cudaStream_t st) {
   const long npair = (long)g.nkx * (g.nz / 2 + 1);
   long nblk = (npair + TPC - 1) / TPC;
   const size_t smem = tri_team_smem_bytes<U>(TPC);
@@ -833,28 +839,29 @@ static void launch_tridiag_team_n(double2 *spec, const GridK &g, const double *l
   if (per_sm > 3) per_sm = 3;
   if (per_sm < 1) per_sm = 1;
   if (nblk > per_sm * sms) nblk = per_sm * sms;
-  k_tridiag_team<U, TPC><<<(unsigned)nblk, TPC * 64, smem, st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl);
+  k_tridiag_team<U, TPC><<<(unsigned)nblk, TPC * 64, smem, st>>>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl,
+                                                                  pinf);
 }
 
 void launch_tridiag(double2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, unsigned *ctl, int sms,
-                    cudaStream_t st) {
+                    const double *pinf, cudaStream_t st) {
   const int T = tri_rows_per_lane(g.ny);
   if (ctl && sms > 0) {
     switch ((g.ny + 63) / 64) {  // 385 <= ny <= 512: two-warp teams
-      case 7: launch_tridiag_team_n<7, 2>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl, sms, st); return;
-      case 8: launch_tridiag_team_n<8, 2>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl, sms, st); return;
+      case 7: launch_tridiag_team_n<7, 2>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl, sms, pinf, st); return;
+      case 8: launch_tridiag_team_n<8, 2>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl, sms, pinf, st); return;
       default: break;
     }
     switch (T) {
 #define TBFP_TRI_PF(TT) \
-  case TT: launch_tridiag_pf_n<TT>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl, sms, st); return;
+  case TT: launch_tridiag_pf_n<TT>(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, ctl, sms, pinf, st); return;
       TBFP_TRI_PF(9) TBFP_TRI_PF(10) TBFP_TRI_PF(11) TBFP_TRI_PF(12)
 #undef TBFP_TRI_PF
       default: break;
     }
   }
-  launch_tridiag_t(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, st);
+  launch_tridiag_t(spec, g, lamx, lamz, am, ap, dyf, mean_c, nxnz, st, pinf);
 }
 void launch_tridiag(float2 *spec, const GridK &g, const double *lamx, const double *lamz, const double *am,
                     const double *ap, const double *dyf, double mean_c, double nxnz, cudaStream_t st) {
@@ -890,6 +897,29 @@ void launch_slab_chunks(const GridK &g, const SlabParts &parts, bool to_x, const
   long nb = (n + 255) / 256;
   if (nb > 148L * 32) nb = 148L * 32;
   k_slab_chunks<<<(unsigned)(nb < 1 ? 1 : nb), 256, 0, st>>>(g, parts, to_x ? 1 : 0, src, dst);
+}
+
+// Elimination factors of the pinned (0,0) y system, once per handle (its
+// matrix does not change between calls): f[2e] = 1/pivot_e, f[2e+1] = ct_e for
+// e < ny-1, with the arithmetic of pinned_sweep.  One thread: ny steps.
+__global__ void k_pin_factors(const double *__restrict__ am, const double *__restrict__ ap,
+                              const double *__restrict__ lamx, const double *__restrict__ lamz, int ny,
+                              double *__restrict__ f) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double lam = lamx[0] + lamz[0];
+  double ct_p = 0.0;
+  for (int e = 0; e < ny - 1; ++e) {
+    const double a = am[e], c = ap[e];
+    const double gi = rcp_nr((lam - a - c) - a * ct_p);
+    ct_p = c * gi;
+    f[2 * e] = gi;
+    f[2 * e + 1] = ct_p;
+  }
+}
+
+void launch_pin_factors(const double *am, const double *ap, const double *lamx, const double *lamz, int ny, double *f,
+                        cudaStream_t st) {
+  k_pin_factors<<<1, 32, 0, st>>>(am, ap, lamx, lamz, ny, f);
 }
 
 cudaError_t prepare_yz_kernels() {
