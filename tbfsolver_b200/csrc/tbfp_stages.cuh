@@ -315,27 +315,34 @@ __device__ __forceinline__ void rhs_body(RhsArgs a, GridK g, double *__restrict_
 // last-pass butterfly b of one row; 32 consecutive b write 512 contiguous
 // bytes.  For a one-pass length the tile is already transformed and is
 // stored as it stands.
+// The psi row (x index 0) of spectrum row r0 + row and its ghost images
+// (y wall copy, periodic z), null where a row has none.
+struct RowPtrs {
+  double *p00, *p10, *p01, *p11;
+};
+__device__ __forceinline__ RowPtrs psi_row_ptrs(double *psi, Lay Lp, int hd, const GridK &g, int r0, int row) {
+  const unsigned rr = (unsigned)(r0 + row);
+  const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
+  const int jg = (j == 1) ? 0 : (j == g.ny ? g.ny + 1 : -1);
+  const int kg = g.slab ? kNoGhost : ((k <= hd) ? k + g.nz : (k > g.nz - hd ? k - g.nz : kNoGhost));
+  RowPtrs q;
+  q.p00 = psi + at(Lp, 0, j, k);
+  q.p10 = (jg >= 0) ? psi + at(Lp, 0, jg, k) : nullptr;
+  q.p01 = (kg != kNoGhost) ? psi + at(Lp, 0, j, kg) : nullptr;
+  q.p11 = (q.p10 && q.p01) ? psi + at(Lp, 0, jg, kg) : nullptr;
+  return q;
+}
+
+// rp: the tile's row pointers made beforehand (one per row, in shared
+// memory), or null to make them per butterfly
 template <typename V, int M, int LOGTJ, bool ACC>
 __device__ __forceinline__ void inv_last_pass_store(const V *sm, const V *tw, double *__restrict__ psi, Lay Lp,
-                                                    int hd, const GridK &g, double scale, int r0, int nrows) {
+                                                    int hd, const GridK &g, double scale, int r0, int nrows,
+                                                    const RowPtrs *rp = nullptr) {
   using T = decltype(V::x);
   constexpr int LD = x_row_stride(M), NX = 2 * M;
   constexpr int NP = ct_nrad(M), RL = ct_rad(M, NP - 1), NSL = ct_ns(M, NP - 1), TWL = NSL - ct_rad(M, 0);
-  struct RowPtrs {
-    double *p00, *p10, *p01, *p11;
-  };
-  auto row_ptrs = [&](int row) {
-    const unsigned rr = (unsigned)(r0 + row);
-    const int k = (int)(rr / (unsigned)g.ny) + 1, j = (int)(rr - (unsigned)(k - 1) * g.ny) + 1;
-    const int jg = (j == 1) ? 0 : (j == g.ny ? g.ny + 1 : -1);
-    const int kg = g.slab ? kNoGhost : ((k <= hd) ? k + g.nz : (k > g.nz - hd ? k - g.nz : kNoGhost));
-    RowPtrs q;
-    q.p00 = psi + at(Lp, 0, j, k);
-    q.p10 = (jg >= 0) ? psi + at(Lp, 0, jg, k) : nullptr;
-    q.p01 = (kg != kNoGhost) ? psi + at(Lp, 0, j, kg) : nullptr;
-    q.p11 = (q.p10 && q.p01) ? psi + at(Lp, 0, jg, kg) : nullptr;
-    return q;
-  };
+  auto row_ptrs = [&](int row) { return rp ? rp[row] : psi_row_ptrs(psi, Lp, hd, g, r0, row); };
   auto put = [&](const RowPtrs &q, int i, double v) {
     if constexpr (ACC) v += q.p00[i];  // refinement: psi += correction
     const int ig = (i <= hd) ? i + NX : (i > NX - hd ? i - NX : kNoGhost);

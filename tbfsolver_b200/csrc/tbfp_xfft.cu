@@ -594,6 +594,7 @@ __global__ void __launch_bounds__(kNT, 3) k_fftx_inv_pf(const double2 *__restric
   V *sm = reinterpret_cast<V *>(smx);
   V *tw = sm + TJ * LD;
   V *stg = tw + M;  // stage: entry (kx, row) at kx*TJ + row
+  __shared__ RowPtrs rp[TJ];  // the tile's psi rows and their ghost images
   for (int t = threadIdx.x; t < ct_twiddle_len(M); t += kNT) tw[t] = tpx[t];
   const int ntile = (int)((g.R + TJ - 1) / TJ);
   auto stage = [&](int tile) {
@@ -640,12 +641,13 @@ __global__ void __launch_bounds__(kNT, 3) k_fftx_inv_pf(const double2 *__restric
 #pragma unroll
       for (int r = 0; r < R0; ++r) X[pad8(jb * R0 + r)] = v[r];
     }
-    __syncthreads();  // the stage is free and the first pass is in sm
+    if (threadIdx.x < TJ && (int)threadIdx.x < nrows) rp[threadIdx.x] = psi_row_ptrs(psi, Lp, hd, g, r0, threadIdx.x);
+    __syncthreads();  // the stage is free, the first pass is in sm, the row pointers are in rp
     if (tile + (int)gridDim.x < ntile) stage(tile + gridDim.x);
     V *wsm = sm + warp * RPW * LD;
     fft_warp<V, M, LOGRPW, 1, LD, true, 1, ct_nrad(M) - 1>(wsm, lane, tw);  // the middle passes
     __syncthreads();
-    inv_last_pass_store<V, M, LOGTJ, false>(sm, tw, psi, Lp, hd, g, scale, r0, nrows);
+    inv_last_pass_store<V, M, LOGTJ, false>(sm, tw, psi, Lp, hd, g, scale, r0, nrows, rp);
   }
   cp_async_wait_all();
 }
