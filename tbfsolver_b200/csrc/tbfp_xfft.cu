@@ -560,13 +560,15 @@ __global__ void __launch_bounds__(kNT, (M >= 384 ? 2 : 3)) k_fftx_inv(const V *_
 #pragma unroll
     for (int r = 0; r < R0; ++r) X[pad8(jb * R0 + r)] = v[r];
   }
+  __shared__ RowPtrs rp[TJ];  // the tile's psi rows and their ghost images
+  for (int r = threadIdx.x; r < nrows; r += kNT) rp[r] = psi_row_ptrs(psi, Lp, hd, g, r0, r);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   V *wsm = sm + warp * RPW * LD;
   fft_warp<V, M, LOGRPW, 1, LD, true, 1, ct_nrad(M) - 1>(wsm, lane, tw);  // the middle passes
   __syncthreads();
   // the last pass with the store of psi and its ghost images
-  inv_last_pass_store<V, M, LOGTJ, ACC>(sm, tw, psi, Lp, hd, g, scale, r0, nrows);
+  inv_last_pass_store<V, M, LOGTJ, ACC>(sm, tw, psi, Lp, hd, g, scale, r0, nrows, rp);
 }
 
 // The same transform (FP64, M = 128 or 256) as a persistent grid of 3 CTAs
@@ -641,7 +643,7 @@ __global__ void __launch_bounds__(kNT, 3) k_fftx_inv_pf(const double2 *__restric
 #pragma unroll
       for (int r = 0; r < R0; ++r) X[pad8(jb * R0 + r)] = v[r];
     }
-    if (threadIdx.x < TJ && (int)threadIdx.x < nrows) rp[threadIdx.x] = psi_row_ptrs(psi, Lp, hd, g, r0, threadIdx.x);
+    for (int r = threadIdx.x; r < nrows; r += kNT) rp[r] = psi_row_ptrs(psi, Lp, hd, g, r0, r);
     __syncthreads();  // the stage is free, the first pass is in sm, the row pointers are in rp
     if (tile + (int)gridDim.x < ntile) stage(tile + gridDim.x);
     V *wsm = sm + warp * RPW * LD;
